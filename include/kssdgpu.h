@@ -1,0 +1,164 @@
+/*
+ * libkssdgpu — B200 (sm_100a) shared-context counting engine for KSSD3A's
+ * `kssd3a ani` / `kssd3a matrix`.  C ABI: plain pointers and sizes, status returns.
+ *
+ * The reference has no plugin or FFI layer; its replaceable seam is the pair of
+ * counting functions the drivers call per query block:
+ *
+ *   count_ctx_obj_frm_comb_sketch_section_with_unique  src/command_ani.h:463-624
+ *   count_ctx_obj_frm_comb_sketch_section_lower         src/command_ani.h:635-721
+ *
+ * called from src/command_ani.c:656,1698,1803 and src/command_matrix.c:489,573,845.
+ * Those functions take the sorted index (sortedcomb_ctxgid64obj32) in host memory,
+ * a block of query samples (comblco keys + comblco.index offsets) and caller-owned,
+ * zeroed dense counter blocks [block][R] of ctx_mut2_t / obj_section_t
+ * (src/command_ani.h:114-124).  The entry points below take the same arguments,
+ * in the same layouts, and fill the same counters bit for bit; the index lives on
+ * the device behind an opaque handle (built once, like the reference's
+ * read_from_file of the index), errors come back as status codes instead of
+ * err()/errx() process exits, and no global state (the reference's Bitslen) is used:
+ * object width is a parameter of the index.
+ */
+#ifndef KSSDGPU_H
+#define KSSDGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. */
+#define KSSDGPU_OK 0
+#define KSSDGPU_ERR_ARG 1          /* invalid argument (size, null pointer, width) */
+#define KSSDGPU_ERR_CUDA 2         /* CUDA runtime error (message via kssdgpu_last_error) */
+#define KSSDGPU_ERR_UNSORTED 3     /* index records or query keys not sorted */
+#define KSSDGPU_ERR_GID 4          /* record gid >= number of references */
+#define KSSDGPU_ERR_TIMEOUT 5      /* a bounded device loop gave up (never expected) */
+#define KSSDGPU_ERR_NOMEM 6        /* device allocation failed */
+#define KSSDGPU_ERR_CAPACITY 7     /* request exceeds a documented capacity limit */
+
+/* Counting flags. */
+#define KSSDGPU_IGNORECONFLICT 0x1u /* ani --ignoreconflict: skip ref (ctx,gid) runs with >1 object */
+#define KSSDGPU_UNIQUE 0x2u         /* also count reference-unique contexts (--unique-ctx) */
+#define KSSDGPU_PLAIN 0x4u          /* use the plain one-query-per-launch kernel (baseline) */
+#define KSSDGPU_GLOBAL_ACC 0x8u     /* force global-memory accumulators (no shared-memory rows) */
+
+/* Counter cells, identical in layout to the reference's ctx_mut2_t / obj_section_t. */
+typedef struct kssdgpu_ctx_mut2 {
+    uint32_t num_ctx;
+    uint32_t num_mut2_ctx;
+} kssdgpu_ctx_mut2_t;
+typedef struct kssdgpu_obj_section {
+    uint32_t diff_obj;
+    uint32_t diff_obj_section;
+} kssdgpu_obj_section_t;
+
+typedef struct kssdgpu_index kssdgpu_index_t;
+
+/* Message of the last failing call on this thread ("" if none). */
+const char *kssdgpu_last_error(void);
+
+/*
+ * Device-resident CSR from the reference's inverted index records
+ * (sortedcomb_ctxgid64obj32: n packed 12-byte {uint64 ctx<<20|gid; uint32 obj},
+ * sorted by (ctxgid, obj); host memory).  Replaces read_from_file of the index
+ * (src/command_ani.c:508-516) plus kssd_build_fenceposts_ctxgid (:3656-3678).
+ * nref = number of reference samples (gids must be < nref); obj_bits = object
+ * width (Bitslen.obj, src/sketch_rearrange.c:35; 20 for the default coden pattern).
+ */
+int kssdgpu_index_from_records(const void *records12, uint64_t n, int nref, int obj_bits,
+                               int device, kssdgpu_index_t **out);
+
+/*
+ * The same CSR built on the device directly from a sketch (comblco keys, each
+ * sample sorted ascending, and comblco.index offsets; host memory): the GPU
+ * version of gen_inverted_index4comblco (src/command_sketch.c:916-938) minus the
+ * file write.  Guards of the reference: total entries < UINT32_MAX, nref < 2^20.
+ */
+int kssdgpu_index_from_sketch(const uint64_t *keys, const uint64_t *offs, int nref, int obj_bits,
+                              int device, kssdgpu_index_t **out);
+
+void kssdgpu_index_free(kssdgpu_index_t *idx);
+
+/* Facts of a built index: records, unique contexts, references, object bits. */
+int kssdgpu_index_info(const kssdgpu_index_t *idx, uint64_t *records, uint64_t *contexts,
+                       int *nref, int *obj_bits);
+
+/*
+ * Copies the index back as reference-layout records (12-byte packed, sorted) and
+ * its unique-object bitset ((n+7)/8 bytes; src/command_sketch.c:856-914).  Either
+ * output may be NULL.
+ */
+int kssdgpu_index_export(const kssdgpu_index_t *idx, void *records12, uint8_t *unique_bits);
+
+/*
+ * Per-reference context counts (AF denominators).  With conflict != 0 a (ctx,gid)
+ * run of L > 1 objects counts once, or not at all with ignoreconflict
+ * (ref_ctx_counts_from_ctxgidobj, src/command_ani.c:351-370); otherwise the
+ * record count of each gid (:372-381).  unique_out (may be NULL) receives the
+ * reference-unique context totals (unique_ref_context_totals, :441-460).
+ */
+int kssdgpu_index_ref_ctx_counts(const kssdgpu_index_t *idx, int conflict, int ignoreconflict,
+                                 uint32_t *ctx_count_out, uint32_t *unique_out);
+
+/*
+ * count_ctx_obj_frm_comb_sketch_section_with_unique (src/command_ani.h:463-574),
+ * counting part.  Host buffers:
+ *   qry_keys   comblco keys of the block, keys of query i at
+ *              qry_keys[qry_offs[i] - qry_offs[0] .. qry_offs[i+1] - qry_offs[0])
+ *   qry_offs   nq + 1 absolute comblco.index offsets (section_skidx)
+ *   ctx, obj   caller-owned [nq][nref] counter blocks (overwritten; need not be zeroed)
+ *   uctx, uobj [nq][nref] reference-unique counters when flags has KSSDGPU_UNIQUE
+ * Every cell of the outputs is written.  Detail-mode filtering and ranking
+ * (src/command_ani.h:577-621) is host work on these counters.
+ */
+int kssdgpu_count_block(kssdgpu_index_t *idx, const uint64_t *qry_keys, const uint64_t *qry_offs,
+                        int nq, unsigned flags, kssdgpu_ctx_mut2_t *ctx, kssdgpu_obj_section_t *obj,
+                        kssdgpu_ctx_mut2_t *uctx, kssdgpu_obj_section_t *uobj);
+
+/*
+ * count_ctx_obj_frm_comb_sketch_section_lower (src/command_ani.h:635-721): as
+ * above without unique counters, counting only references with gid < qry_gid,
+ * where qry_gid = qry_gid_offset + i for query i of the block.
+ */
+int kssdgpu_count_lower(kssdgpu_index_t *idx, const uint64_t *qry_keys, const uint64_t *qry_offs,
+                        int nq, int qry_gid_offset, unsigned flags, kssdgpu_ctx_mut2_t *ctx,
+                        kssdgpu_obj_section_t *obj);
+
+/*
+ * Device-pointer forms of the two calls (inputs already in HBM; stream is a
+ * cudaStream_t or NULL for the legacy stream).  d_qry_offs are absolute offsets as
+ * above; outputs are device arrays of nq*nref cells.  Asynchronous: the counters
+ * are complete when the stream reaches this point; errors detected on the device
+ * are reported by the next kssdgpu_sync(idx, stream).
+ */
+int kssdgpu_count_block_dev(kssdgpu_index_t *idx, const uint64_t *d_qry_keys,
+                            const uint64_t *d_qry_offs, int nq, int qry_gid_offset, int lower,
+                            unsigned flags, kssdgpu_ctx_mut2_t *d_ctx, kssdgpu_obj_section_t *d_obj,
+                            kssdgpu_ctx_mut2_t *d_uctx, kssdgpu_obj_section_t *d_uobj, void *stream);
+int kssdgpu_sync(kssdgpu_index_t *idx, void *stream);
+
+/*
+ * Whole self lower triangle in one pass (the counting behind
+ * comb_sortedsketch64_indexed_self_full / _triangle, src/command_ani.c:1657-1842,
+ * and matrix_write_indexed_self_matrix, src/command_matrix.c:439-619), valid when
+ * the index was built from the same sketch that supplies the queries.  Output
+ * cells are packed lower-triangular: cell (q, r), r < q, at q*(q-1)/2 + r
+ * (ani_lower_offset, src/command_ani.c:1588-1591); nref*(nref-1)/2 cells each.
+ * Host-buffer form.
+ */
+int kssdgpu_self_lower(kssdgpu_index_t *idx, unsigned flags, kssdgpu_ctx_mut2_t *ctx_lower,
+                       kssdgpu_obj_section_t *obj_lower);
+/* Device form of kssdgpu_self_lower (outputs in HBM, stream-ordered). */
+int kssdgpu_self_lower_dev(kssdgpu_index_t *idx, unsigned flags, kssdgpu_ctx_mut2_t *d_ctx_lower,
+                           kssdgpu_obj_section_t *d_obj_lower, void *stream);
+
+/* Number of kernels launched by this library so far in this process. */
+uint64_t kssdgpu_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,1174 @@
+// libkssdgpu: device-resident KSSD3A inverted index and shared-context counting
+// kernels for B200 (sm_100a).  C ABI in include/kssdgpu.h.
+//
+// HBM layout of an index (N records, U unique contexts):
+//   post[N]   uint64  gid << 32 | obj, in the reference's (ctx, gid, obj) record order
+//   gkey[U]   uint64  unique contexts, ascending
+//   gbeg[U+1] uint32  postings range of each context
+//   table[C]  Slot    open-addressing hash of the U contexts (C = pow2 >= 2U),
+//                     16 B {ctx, begin | count << 32}: one sector per probe
+//
+// Counting semantics follow src/command_ani.h:463-721 (see walk_context below).
+#include "kssdgpu.h"
+#include "kssd_dev.cuh"
+
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <atomic>
+#include <cstdio>
+#include <cstring>
+#include <numeric>
+#include <string>
+#include <vector>
+
+using namespace kssd;
+
+namespace {
+
+thread_local std::string g_last_error;
+std::atomic<uint64_t> g_launches{0};
+
+int fail(int code, const std::string &msg)
+{
+    g_last_error = msg;
+    return code;
+}
+
+#define CUDA_TRY(expr)                                                                              \
+    do {                                                                                            \
+        cudaError_t e_ = (expr);                                                                    \
+        if (e_ != cudaSuccess)                                                                      \
+            return fail(e_ == cudaErrorMemoryAllocation ? KSSDGPU_ERR_NOMEM : KSSDGPU_ERR_CUDA,   \
+                        std::string(#expr) + ": " + cudaGetErrorString(e_));                        \
+    } while (0)
+
+inline void count_launch(uint64_t n = 1) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+// ------------------------------------------------------------------ index build kernels
+
+// Unpack reference records (packed 12 B) into postings; flag context heads and
+// check the (ctxgid, obj) order and the gid range.
+__global__ void k_unpack_records(const uint32_t *__restrict__ w, uint64_t n, int nref, uint64_t *__restrict__ post,
+                                 uint32_t *__restrict__ head, unsigned long long *__restrict__ ctx_of,
+                                 int *__restrict__ err)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const unsigned long long cg = (unsigned long long)w[3 * i] | ((unsigned long long)w[3 * i + 1] << 32);
+        const uint32_t obj = w[3 * i + 2];
+        const uint32_t gid = (uint32_t)(cg & ((1u << kGidBits) - 1));
+        const unsigned long long ctx = cg >> kGidBits;
+        post[i] = ((uint64_t)gid << 32) | obj;
+        ctx_of[i] = ctx;
+        uint32_t h = 1;
+        if (i > 0) {
+            const unsigned long long pcg = (unsigned long long)w[3 * (i - 1)] | ((unsigned long long)w[3 * (i - 1) + 1] << 32);
+            const uint32_t pobj = w[3 * (i - 1) + 2];
+            if (pcg > cg || (pcg == cg && pobj > obj))
+                atomicMax(err, (int)kDevUnsorted);
+            h = (pcg >> kGidBits) != ctx;
+        }
+        if ((int)gid >= nref)
+            atomicMax(err, (int)kDevGid);
+        head[i] = h;
+    }
+}
+
+// Sketch keys -> sort keys (ctx << 20 | gid) with obj values; checks that each
+// sample's keys ascend (comblco order), which makes one stable sort by ctxgid
+// produce the reference's (ctxgid, obj) order.
+__global__ void k_sketch_to_sortkeys(const uint64_t *__restrict__ keys, const uint64_t *__restrict__ offs, int nref,
+                                     int obj_bits, unsigned long long *__restrict__ skey, uint32_t *__restrict__ sval,
+                                     int *__restrict__ err)
+{
+    const uint64_t base = offs[0];
+    const uint64_t objmask = (obj_bits >= 64) ? ~0ull : ((1ull << obj_bits) - 1);
+    for (int g = blockIdx.x; g < nref; g += gridDim.x) {
+        const uint64_t b = offs[g] - base, e = offs[g + 1] - base;
+        for (uint64_t i = b + threadIdx.x; i < e; i += blockDim.x) {
+            const uint64_t k = keys[i];
+            if (i > b && keys[i - 1] > k)
+                atomicMax(err, (int)kDevUnsorted);
+            skey[i] = ((k >> obj_bits) << kGidBits) | (uint64_t)g;
+            sval[i] = (uint32_t)(k & objmask);
+        }
+    }
+}
+
+__global__ void k_sorted_to_post(const unsigned long long *__restrict__ skey, const uint32_t *__restrict__ sval, uint64_t n,
+                                 uint64_t *__restrict__ post, uint32_t *__restrict__ head,
+                                 unsigned long long *__restrict__ ctx_of)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const unsigned long long cg = skey[i];
+        const unsigned long long ctx = cg >> kGidBits;
+        post[i] = ((cg & ((1u << kGidBits) - 1)) << 32) | sval[i];
+        ctx_of[i] = ctx;
+        head[i] = (i == 0) || ((skey[i - 1] >> kGidBits) != ctx);
+    }
+}
+
+__global__ void k_scatter_groups(const uint32_t *__restrict__ head, const uint32_t *__restrict__ gidx,
+                                 const unsigned long long *__restrict__ ctx_of, uint64_t n,
+                                 unsigned long long *__restrict__ gkey, uint32_t *__restrict__ gbeg, uint64_t u)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        if (head[i]) {
+            gkey[gidx[i]] = ctx_of[i];
+            gbeg[gidx[i]] = (uint32_t)i;
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+        gbeg[u] = (uint32_t)n;
+}
+
+__global__ void k_table_insert(const unsigned long long *__restrict__ gkey, const uint32_t *__restrict__ gbeg, uint64_t u,
+                               Slot *__restrict__ t, uint32_t mask, int *__restrict__ err)
+{
+    for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < u; g += (uint64_t)gridDim.x * blockDim.x) {
+        const unsigned long long ctx = gkey[g];
+        const unsigned long long range = (unsigned long long)gbeg[g] | ((unsigned long long)(gbeg[g + 1] - gbeg[g]) << 32);
+        uint32_t i = (uint32_t)mix64(ctx) & mask;
+        bool done = false;
+        for (uint32_t probe = 0; probe <= mask; ++probe) {
+            const unsigned long long prev = atomicCAS(&t[i].ctx, kEmptyCtx, ctx);
+            if (prev == kEmptyCtx || prev == ctx) {
+                t[i].range = range;
+                done = true;
+                break;
+            }
+            i = (i + 1) & mask;
+        }
+        if (!done)
+            atomicMax(err, (int)kDevProbe);
+    }
+}
+
+// reference-layout records back out of the CSR
+__global__ void k_export_records(const unsigned long long *__restrict__ gkey, const uint32_t *__restrict__ gbeg, uint64_t u,
+                                 const uint64_t *__restrict__ post, uint32_t *__restrict__ w)
+{
+    for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < u; g += (uint64_t)gridDim.x * blockDim.x) {
+        const unsigned long long ctx = gkey[g];
+        for (uint32_t i = gbeg[g]; i < gbeg[g + 1]; ++i) {
+            const uint64_t p = post[i];
+            const unsigned long long cg = (ctx << kGidBits) | (p >> 32);
+            w[3 * (uint64_t)i] = (uint32_t)cg;
+            w[3 * (uint64_t)i + 1] = (uint32_t)(cg >> 32);
+            w[3 * (uint64_t)i + 2] = (uint32_t)p;
+        }
+    }
+}
+
+// bit i set when record i's object occurs once in its context group
+// (write_unique_marker_bits_from_sorted, src/command_sketch.c:856-914)
+__global__ void k_unique_bits(const uint32_t *__restrict__ gbeg, uint64_t u, const uint64_t *__restrict__ post,
+                              uint32_t *__restrict__ bits32)
+{
+    for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < u; g += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t b = gbeg[g], e = gbeg[g + 1];
+        for (uint32_t i = b; i < e; ++i) {
+            const uint32_t o = (uint32_t)post[i];
+            uint32_t same = 0;
+            for (uint32_t j = b; j < e && same < 2; ++j)
+                same += (uint32_t)post[j] == o;
+            if (same == 1)
+                atomicOr(&bits32[i >> 5], 1u << (i & 31));
+        }
+    }
+}
+
+// per-gid record counts, conflict adjustments and unique-context totals
+// (src/command_ani.c:351-381,441-460)
+__global__ void k_ref_counts(const uint32_t *__restrict__ gbeg, uint64_t u, const uint64_t *__restrict__ post,
+                             int conflict, int ignoreconflict, uint32_t *__restrict__ cnt, uint32_t *__restrict__ uniq)
+{
+    for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < u; g += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t b = gbeg[g], e = gbeg[g + 1];
+        uint32_t i = b;
+        bool single_owner = true;
+        while (i < e) {
+            const uint32_t gid = (uint32_t)(post[i] >> 32);
+            uint32_t j = i + 1;
+            while (j < e && (uint32_t)(post[j] >> 32) == gid)
+                ++j;
+            const uint32_t run = j - i;
+            uint32_t keep = run;
+            if (conflict && run > 1)
+                keep = ignoreconflict ? 0 : 1;
+            if (keep)
+                atomicAdd(&cnt[gid], keep);
+            if (i != b)
+                single_owner = false;
+            i = j;
+        }
+        if (uniq && single_owner && (!ignoreconflict || e - b == 1))
+            atomicAdd(&uniq[(uint32_t)(post[b] >> 32)], 1u);
+    }
+}
+
+// ------------------------------------------------------------------ counting kernels
+
+struct CountParams {
+    const Slot *table;
+    uint32_t mask;
+    const uint64_t *post;
+    const uint64_t *qkeys;  // keys of query i at qkeys[qoffs[i] - qoffs[0] ...]
+    const uint64_t *qoffs;  // absolute offsets, nq + 1
+    int nq;
+    int nref;
+    int qgid_offset;
+    int obj_bits;
+    int ignoreconflict;
+    unsigned long long *out_ctx;   // [nq][nref] ctx_mut2_t as u64 (num_mut2 << 32 | num_ctx)
+    unsigned long long *out_obj;   // [nq][nref] obj_section_t as u64 (section << 32 | diff_obj)
+    unsigned long long *out_uctx;
+    unsigned long long *out_uobj;
+    unsigned int *work;            // persistent-kernel work counter (zeroed before launch)
+    const int *order;              // query processing order (largest first), may be null
+    int *err;
+};
+
+// One counter update for a matched (query ctx, reference gid run) with minimum
+// object difference d: num_ctx += 1; d > 0: diff_obj += 1, section += d;
+// d > 1: num_mut2 += 1  (src/command_ani.h:536-561).
+__device__ __forceinline__ unsigned long long inc_ctx(int d) { return 1ull | ((unsigned long long)(d > 1) << 32); }
+__device__ __forceinline__ unsigned long long inc_obj(int d) { return 1ull | ((unsigned long long)d << 32); }
+
+struct SmemAcc {
+    unsigned long long *c, *o;
+    __device__ __forceinline__ void add(uint32_t gid, int d) const
+    {
+        atomicAdd(c + gid, inc_ctx(d));
+        if (d)
+            atomicAdd(o + gid, inc_obj(d));
+    }
+};
+
+struct GlobalAcc {
+    unsigned long long *c, *o;
+    __device__ __forceinline__ void add(uint32_t gid, int d) const
+    {
+        atomicAdd(c + gid, inc_ctx(d));
+        if (d)
+            atomicAdd(o + gid, inc_obj(d));
+    }
+};
+
+// min over the query run's objects x one reference object
+__device__ __forceinline__ int min_diff_obj(uint32_t robj, uint32_t q0, int s, const uint64_t *__restrict__ qrun,
+                                            uint64_t objmask, int cur)
+{
+    int d = dna_pop(q0 ^ robj);
+    for (int k = 1; k < s && d; ++k)
+        d = min(d, dna_pop((uint32_t)(__ldg(qrun + k) & objmask) ^ robj));
+    return min(cur, d);
+}
+
+// The postings walk for one query context run (objects qrun[0..s)) against the
+// context group [pb, pe): per reference gid run, count the context, take the
+// minimum object difference over the run cross product, and (UNIQUE) credit the
+// sole owner of the context when there is exactly one gid run
+// (src/command_ani.h:515-575; lower variant :694-716 stops at gid >= qgid).
+template <bool LOWER, bool UNIQUE, class Acc>
+__device__ __forceinline__ void walk_context(const uint64_t *__restrict__ post, uint32_t pb, uint32_t pe,
+                                             const uint64_t *__restrict__ qrun, int s, uint64_t objmask, int qgid,
+                                             int ignoreconflict, const Acc &acc, const Acc &uacc)
+{
+    const uint32_t q0 = (uint32_t)(__ldg(qrun) & objmask);
+    uint32_t p = pb;
+    uint32_t owners = 0, sole_gid = 0;
+    int sole_d = 0;
+    bool sole_ok = false;
+    while (p < pe) {
+        const uint64_t w = __ldg(post + p);
+        const uint32_t gid = (uint32_t)(w >> 32);
+        if (LOWER && (int)gid >= qgid)
+            break;
+        int d = min_diff_obj((uint32_t)w, q0, s, qrun, objmask, kMinInit);
+        const uint32_t rb = p++;
+        while (p < pe) {
+            const uint64_t w2 = __ldg(post + p);
+            if ((uint32_t)(w2 >> 32) != gid)
+                break;
+            d = min_diff_obj((uint32_t)w2, q0, s, qrun, objmask, d);
+            ++p;
+        }
+        ++owners;
+        sole_gid = gid;
+        if (ignoreconflict && p - rb > 1)
+            continue;
+        acc.add(gid, d);
+        sole_d = d;
+        sole_ok = true;
+    }
+    if (UNIQUE && owners == 1 && sole_ok)
+        uacc.add(sole_gid, sole_d);
+}
+
+// Process query entry i of [b, e): only the first entry of a context run works;
+// it takes the whole run (src/command_ani.h:498-505).
+template <bool LOWER, bool UNIQUE, class Acc>
+__device__ __forceinline__ void process_entry(const CountParams &P, uint64_t i, uint64_t b, uint64_t e, int qgid,
+                                              uint64_t objmask, const Acc &acc, const Acc &uacc)
+{
+    const uint64_t key = __ldg(P.qkeys + i);
+    const uint64_t ctx = key >> P.obj_bits;
+    if (i > b && (__ldg(P.qkeys + i - 1) >> P.obj_bits) == ctx)
+        return;
+    int s = 1;
+    while (i + s < e && (__ldg(P.qkeys + i + s) >> P.obj_bits) == ctx)
+        ++s;
+    uint32_t pb, pc;
+    if (!table_lookup(P.table, P.mask, ctx, pb, pc))
+        return;
+    walk_context<LOWER, UNIQUE>(P.post, pb, pb + pc, P.qkeys + i, s, objmask, qgid, P.ignoreconflict, acc, uacc);
+}
+
+// Batched persistent kernel: CTAs take whole queries from a work counter
+// (largest first); with SMEM the query's reference row is accumulated in shared
+// memory and written once, coalesced; without, counters go to the zeroed global
+// row with atomics.
+template <bool LOWER, bool UNIQUE, bool SMEM>
+__global__ void __launch_bounds__(512) k_count_batched(CountParams P)
+{
+    extern __shared__ unsigned long long sm[];
+    __shared__ int s_item;
+    const uint64_t objmask = (P.obj_bits >= 64) ? ~0ull : ((1ull << P.obj_bits) - 1);
+    const uint64_t base = P.qoffs[0];
+    const int nref = P.nref;
+    for (;;) {
+        if (threadIdx.x == 0)
+            s_item = (int)atomicAdd(P.work, 1u);
+        __syncthreads();
+        const int it = s_item;
+        if (it >= P.nq)
+            break;
+        const int q = P.order ? P.order[it] : it;
+        const int qgid = P.qgid_offset + q;
+        const size_t row = (size_t)q * nref;
+        unsigned long long *sc = sm, *so = sm + nref, *suc = sm + 2 * nref, *suo = sm + 3 * nref;
+        if (SMEM) {
+            for (int c = threadIdx.x; c < nref * (UNIQUE ? 4 : 2); c += blockDim.x)
+                sm[c] = 0;
+            __syncthreads();
+        }
+        const uint64_t b = P.qoffs[q] - base, e = P.qoffs[q + 1] - base;
+        if (SMEM) {
+            const SmemAcc acc{sc, so}, uacc{suc, suo};
+            for (uint64_t i = b + threadIdx.x; i < e; i += blockDim.x)
+                process_entry<LOWER, UNIQUE>(P, i, b, e, qgid, objmask, acc, uacc);
+        } else {
+            const GlobalAcc acc{P.out_ctx + row, P.out_obj + row};
+            const GlobalAcc uacc{UNIQUE ? P.out_uctx + row : nullptr, UNIQUE ? P.out_uobj + row : nullptr};
+            for (uint64_t i = b + threadIdx.x; i < e; i += blockDim.x)
+                process_entry<LOWER, UNIQUE>(P, i, b, e, qgid, objmask, acc, uacc);
+        }
+        __syncthreads();
+        if (SMEM) {
+            for (int g = threadIdx.x; g < nref; g += blockDim.x) {
+                P.out_ctx[row + g] = sc[g];
+                P.out_obj[row + g] = so[g];
+                if (UNIQUE) {
+                    P.out_uctx[row + g] = suc[g];
+                    P.out_uobj[row + g] = suo[g];
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Plain baseline: one launch per query, one thread per query entry, global atomics.
+template <bool LOWER, bool UNIQUE>
+__global__ void __launch_bounds__(256) k_count_plain(CountParams P, int q)
+{
+    const uint64_t objmask = (P.obj_bits >= 64) ? ~0ull : ((1ull << P.obj_bits) - 1);
+    const uint64_t base = P.qoffs[0];
+    const uint64_t b = P.qoffs[q] - base, e = P.qoffs[q + 1] - base;
+    const uint64_t i = b + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (i >= e)
+        return;
+    const size_t row = (size_t)q * P.nref;
+    const GlobalAcc acc{P.out_ctx + row, P.out_obj + row};
+    const GlobalAcc uacc{UNIQUE ? P.out_uctx + row : nullptr, UNIQUE ? P.out_uobj + row : nullptr};
+    process_entry<LOWER, UNIQUE>(P, i, b, e, P.qgid_offset + q, objmask, acc, uacc);
+}
+
+// ------------------------------------------------------------------ self lower triangle (join)
+
+// Pairs of a context group whose gid runs are all single objects: k(k-1)/2.
+// Groups holding a multi-object run are handled by k_self_conflict_groups.
+__global__ void k_self_pair_counts(const uint32_t *__restrict__ gbeg, uint64_t u, const uint64_t *__restrict__ post,
+                                   unsigned long long *__restrict__ npairs, uint32_t *__restrict__ conflict_flag)
+{
+    for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < u; g += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t b = gbeg[g], e = gbeg[g + 1], k = e - b;
+        bool conflict = false;
+        if (k >= 2) {
+            uint32_t prev = (uint32_t)(post[b] >> 32);
+            for (uint32_t i = b + 1; i < e; ++i) {
+                const uint32_t gid = (uint32_t)(post[i] >> 32);
+                conflict |= gid == prev;
+                prev = gid;
+            }
+        }
+        conflict_flag[g] = conflict;
+        npairs[g] = (k >= 2 && !conflict) ? (unsigned long long)k * (k - 1) / 2 : 0ull;
+    }
+}
+
+__device__ __forceinline__ size_t lower_cell(uint32_t row, uint32_t col) { return (size_t)row * (row - 1) / 2 + col; }
+
+// Each thread walks `per_thread` consecutive pairs of the global pair sequence
+// (groups in context order, pairs (i<j) by j then i); cell (gid_j, gid_i).
+__global__ void __launch_bounds__(256) k_self_pairs(const uint32_t *__restrict__ gbeg, uint64_t u,
+                                                    const uint64_t *__restrict__ post,
+                                                    const unsigned long long *__restrict__ incl,  // inclusive scan
+                                                    unsigned long long total, int per_thread,
+                                                    unsigned long long *__restrict__ oc, unsigned long long *__restrict__ oo)
+{
+    const unsigned long long t0 = (blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x) * per_thread;
+    if (t0 >= total)
+        return;
+    // group containing pair t0: first g with incl[g] > t0
+    uint64_t lo = 0, hi = u;
+    while (lo < hi) {
+        const uint64_t mid = (lo + hi) >> 1;
+        if (incl[mid] > t0)
+            hi = mid;
+        else
+            lo = mid + 1;
+    }
+    uint64_t g = lo;
+    unsigned long long local = t0 - (g ? incl[g - 1] : 0ull);
+    // decode local -> (j, i), local = j(j-1)/2 + i
+    uint32_t j = (uint32_t)((1.0 + sqrt(1.0 + 8.0 * (double)local)) * 0.5);
+    while ((unsigned long long)j * (j - 1) / 2 > local)
+        --j;
+    while ((unsigned long long)(j + 1) * j / 2 <= local)
+        ++j;
+    uint32_t i = (uint32_t)(local - (unsigned long long)j * (j - 1) / 2);
+    uint32_t b = gbeg[g], k = gbeg[g + 1] - b;
+    const unsigned long long end = min(total, t0 + (unsigned long long)per_thread);
+    for (unsigned long long t = t0; t < end; ++t) {
+        const uint64_t pi = __ldg(post + b + i), pj = __ldg(post + b + j);
+        const int d = min(kMinInit, dna_pop((uint32_t)pi ^ (uint32_t)pj));
+        const size_t cell = lower_cell((uint32_t)(pj >> 32), (uint32_t)(pi >> 32));
+        atomicAdd(oc + cell, inc_ctx(d));
+        if (d)
+            atomicAdd(oo + cell, inc_obj(d));
+        if (++i == j) {
+            i = 0;
+            if (++j == k) {
+                // next group with pairs
+                do {
+                    ++g;
+                } while (g < u && incl[g] == incl[g - 1]);
+                if (g >= u)
+                    break;
+                b = gbeg[g];
+                k = gbeg[g + 1] - b;
+                j = 1;
+            }
+        }
+    }
+}
+
+// Groups with multi-object gid runs: one thread per group walks run pairs with the
+// full min-over-cross-product rule; the lower-gid run is the reference side.
+__global__ void k_self_conflict_groups(const uint32_t *__restrict__ gbeg, uint64_t u, const uint64_t *__restrict__ post,
+                                       const uint32_t *__restrict__ conflict_flag, int ignoreconflict,
+                                       unsigned long long *__restrict__ oc, unsigned long long *__restrict__ oo)
+{
+    for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < u; g += (uint64_t)gridDim.x * blockDim.x) {
+        if (!conflict_flag[g])
+            continue;
+        const uint32_t b = gbeg[g], e = gbeg[g + 1];
+        // run (query side, higher gid) qb..qe
+        for (uint32_t qb = b; qb < e;) {
+            const uint32_t qg = (uint32_t)(post[qb] >> 32);
+            uint32_t qe = qb + 1;
+            while (qe < e && (uint32_t)(post[qe] >> 32) == qg)
+                ++qe;
+            for (uint32_t rb = b; rb < qb;) {
+                const uint32_t rg = (uint32_t)(post[rb] >> 32);
+                uint32_t re = rb + 1;
+                while (re < qb && (uint32_t)(post[re] >> 32) == rg)
+                    ++re;
+                if (!(ignoreconflict && re - rb > 1)) {
+                    int d = kMinInit;
+                    for (uint32_t x = qb; x < qe && d; ++x)
+                        for (uint32_t y = rb; y < re && d; ++y)
+                            d = min(d, dna_pop((uint32_t)post[x] ^ (uint32_t)post[y]));
+                    const size_t cell = lower_cell(qg, rg);
+                    atomicAdd(oc + cell, inc_ctx(d));
+                    if (d)
+                        atomicAdd(oo + cell, inc_obj(d));
+                }
+                rb = re;
+            }
+            qb = qe;
+        }
+    }
+}
+
+// ------------------------------------------------------------------ helpers
+
+template <class T>
+struct DevBuf {
+    T *p = nullptr;
+    size_t cap = 0;
+    cudaError_t ensure(size_t n)
+    {
+        if (n <= cap && p)
+            return cudaSuccess;
+        if (p)
+            cudaFree(p);
+        p = nullptr;
+        cap = 0;
+        cudaError_t e = cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T));
+        if (e == cudaSuccess)
+            cap = std::max<size_t>(n, 1);
+        return e;
+    }
+    void release()
+    {
+        if (p)
+            cudaFree(p);
+        p = nullptr;
+        cap = 0;
+    }
+};
+
+int grid_for(uint64_t n, int block = 256)
+{
+    uint64_t g = (n + block - 1) / block;
+    if (g < 1)
+        g = 1;
+    if (g > 148ull * 64)
+        g = 148ull * 64;
+    return (int)g;
+}
+
+}  // namespace
+
+struct kssdgpu_index {
+    int device = 0;
+    int nref = 0;
+    int obj_bits = 20;
+    uint64_t n = 0;
+    uint64_t u = 0;
+    uint64_t *post = nullptr;
+    unsigned long long *gkey = nullptr;
+    uint32_t *gbeg = nullptr;
+    Slot *table = nullptr;
+    uint32_t mask = 0;
+    int *err = nullptr;
+    unsigned int *work = nullptr;
+    int sms = 148;
+    // host-API staging
+    DevBuf<uint64_t> s_keys, s_offs;
+    DevBuf<unsigned long long> s_out;
+    DevBuf<int> s_order;
+    // self-join plan
+    DevBuf<unsigned long long> j_incl;
+    DevBuf<uint32_t> j_conflict;
+    unsigned long long j_total = 0;
+    bool j_ready = false;
+    bool j_any_conflict = false;
+};
+
+namespace {
+
+int finish_build(kssdgpu_index *ix, uint32_t *head, unsigned long long *ctx_of, cudaStream_t st)
+{
+    const uint64_t n = ix->n;
+    uint32_t *gidx = nullptr;
+    CUDA_TRY(cudaMalloc(&gidx, std::max<uint64_t>(n, 1) * sizeof(uint32_t)));
+    size_t tmp_bytes = 0;
+    CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, head, gidx, (int64_t)n, st));
+    void *tmp = nullptr;
+    CUDA_TRY(cudaMalloc(&tmp, std::max<size_t>(tmp_bytes, 1)));
+    CUDA_TRY(cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, head, gidx, (int64_t)n, st));
+    count_launch();
+    uint32_t last_idx = 0, last_head = 0;
+    if (n) {
+        CUDA_TRY(cudaMemcpyAsync(&last_idx, gidx + n - 1, 4, cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(cudaMemcpyAsync(&last_head, head + n - 1, 4, cudaMemcpyDeviceToHost, st));
+    }
+    CUDA_TRY(cudaStreamSynchronize(st));
+    ix->u = n ? (uint64_t)last_idx + last_head : 0;
+    CUDA_TRY(cudaMalloc(&ix->gkey, std::max<uint64_t>(ix->u, 1) * sizeof(unsigned long long)));
+    CUDA_TRY(cudaMalloc(&ix->gbeg, (ix->u + 1) * sizeof(uint32_t)));
+    k_scatter_groups<<<grid_for(n), 256, 0, st>>>(head, gidx, ctx_of, n, ix->gkey, ix->gbeg, ix->u);
+    count_launch();
+    uint64_t cap = 1024;
+    while (cap < 2 * ix->u)
+        cap <<= 1;
+    ix->mask = (uint32_t)(cap - 1);
+    CUDA_TRY(cudaMalloc(&ix->table, cap * sizeof(Slot)));
+    CUDA_TRY(cudaMemsetAsync(ix->table, 0xFF, cap * sizeof(Slot), st));
+    k_table_insert<<<grid_for(ix->u), 256, 0, st>>>(ix->gkey, ix->gbeg, ix->u, ix->table, ix->mask, ix->err);
+    count_launch();
+    CUDA_TRY(cudaStreamSynchronize(st));
+    cudaFree(tmp);
+    cudaFree(gidx);
+    int herr = 0;
+    CUDA_TRY(cudaMemcpy(&herr, ix->err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (herr == kDevUnsorted)
+        return fail(KSSDGPU_ERR_UNSORTED, "index records are not sorted by (ctxgid, obj)");
+    if (herr == kDevGid)
+        return fail(KSSDGPU_ERR_GID, "index record gid is not below the reference count");
+    if (herr == kDevProbe)
+        return fail(KSSDGPU_ERR_TIMEOUT, "context hash table insert did not terminate");
+    return KSSDGPU_OK;
+}
+
+int new_index(int nref, int obj_bits, int device, uint64_t n, kssdgpu_index **out)
+{
+    if (!out)
+        return fail(KSSDGPU_ERR_ARG, "null output handle");
+    *out = nullptr;
+    if (nref <= 0 || nref >= (1 << kGidBits))
+        return fail(KSSDGPU_ERR_ARG, "reference count must be in 1..2^20-1");
+    if (obj_bits <= 0 || obj_bits > 32)
+        return fail(KSSDGPU_ERR_ARG, "object width must be 1..32 bits");
+    if (n >= 0xFFFFFFFFull)
+        return fail(KSSDGPU_ERR_CAPACITY, "index entries must be below UINT32_MAX");
+    CUDA_TRY(cudaSetDevice(device));
+    auto *ix = new kssdgpu_index();
+    ix->device = device;
+    ix->nref = nref;
+    ix->obj_bits = obj_bits;
+    ix->n = n;
+    cudaDeviceGetAttribute(&ix->sms, cudaDevAttrMultiProcessorCount, device);
+    cudaError_t e = cudaMalloc(&ix->err, sizeof(int));
+    if (e == cudaSuccess)
+        e = cudaMalloc(&ix->work, sizeof(unsigned int));
+    if (e == cudaSuccess)
+        e = cudaMemset(ix->err, 0, sizeof(int));
+    if (e == cudaSuccess)
+        e = cudaMalloc(&ix->post, std::max<uint64_t>(n, 1) * sizeof(uint64_t));
+    if (e != cudaSuccess) {
+        kssdgpu_index_free(ix);
+        return fail(KSSDGPU_ERR_NOMEM, std::string("index allocation: ") + cudaGetErrorString(e));
+    }
+    *out = ix;
+    return KSSDGPU_OK;
+}
+
+int check_dev_err(kssdgpu_index *ix, cudaStream_t st)
+{
+    int herr = 0;
+    CUDA_TRY(cudaMemcpyAsync(&herr, ix->err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    if (herr) {
+        cudaMemsetAsync(ix->err, 0, sizeof(int), st);
+        return fail(KSSDGPU_ERR_TIMEOUT, "device probe loop exceeded its bound");
+    }
+    return KSSDGPU_OK;
+}
+
+template <bool LOWER, bool UNIQUE, bool SMEM>
+int launch_batched(kssdgpu_index *ix, const CountParams &P, size_t smem, cudaStream_t st)
+{
+    auto kern = k_count_batched<LOWER, UNIQUE, SMEM>;
+    if (smem > 48 * 1024)
+        CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 512, smem));
+    if (per_sm < 1)
+        return fail(KSSDGPU_ERR_CAPACITY, "shared-memory row does not fit one CTA");
+    int grid = ix->sms * per_sm;
+    if (grid > P.nq)
+        grid = std::max(P.nq, 1);
+    CUDA_TRY(cudaMemsetAsync(P.work, 0, sizeof(unsigned int), st));
+    kern<<<grid, 512, smem, st>>>(P);
+    count_launch();
+    CUDA_TRY(cudaGetLastError());
+    return KSSDGPU_OK;
+}
+
+template <bool LOWER, bool UNIQUE>
+int launch_plain(kssdgpu_index *ix, const CountParams &P, const std::vector<uint64_t> &sizes, cudaStream_t st)
+{
+    for (int q = 0; q < P.nq; ++q) {
+        if (!sizes[q])
+            continue;
+        const int grid = (int)((sizes[q] + 255) / 256);
+        k_count_plain<LOWER, UNIQUE><<<grid, 256, 0, st>>>(P, q);
+        count_launch();
+    }
+    CUDA_TRY(cudaGetLastError());
+    return KSSDGPU_OK;
+}
+
+// shared-memory row budget: 2 (or 4 with unique) u64 per reference
+constexpr size_t kSmemRowLimit = 112 * 1024;
+
+int count_dev_impl(kssdgpu_index *ix, const uint64_t *d_keys, const uint64_t *d_offs, int nq, int qgid_offset, bool lower,
+                   unsigned flags, unsigned long long *oc, unsigned long long *oo, unsigned long long *uc,
+                   unsigned long long *uo, const int *d_order, const std::vector<uint64_t> *sizes, cudaStream_t st)
+{
+    const bool unique = (flags & KSSDGPU_UNIQUE) != 0;
+    if (lower && unique)
+        return fail(KSSDGPU_ERR_ARG, "unique-context counting has no lower-triangle form");
+    if (unique && (!uc || !uo))
+        return fail(KSSDGPU_ERR_ARG, "unique counters requested without output buffers");
+    CountParams P{};
+    P.table = ix->table;
+    P.mask = ix->mask;
+    P.post = ix->post;
+    P.qkeys = d_keys;
+    P.qoffs = d_offs;
+    P.nq = nq;
+    P.nref = ix->nref;
+    P.qgid_offset = qgid_offset;
+    P.obj_bits = ix->obj_bits;
+    P.ignoreconflict = (flags & KSSDGPU_IGNORECONFLICT) ? 1 : 0;
+    P.out_ctx = oc;
+    P.out_obj = oo;
+    P.out_uctx = uc;
+    P.out_uobj = uo;
+    P.work = ix->work;
+    P.order = d_order;
+    P.err = ix->err;
+    const size_t cells = (size_t)nq * ix->nref;
+    if (nq == 0)
+        return KSSDGPU_OK;
+    const size_t smem = (size_t)ix->nref * sizeof(unsigned long long) * (unique ? 4 : 2);
+    const bool plain = (flags & KSSDGPU_PLAIN) != 0;
+    const bool use_smem = !plain && !(flags & KSSDGPU_GLOBAL_ACC) && smem <= kSmemRowLimit;
+    if (!use_smem) {
+        CUDA_TRY(cudaMemsetAsync(oc, 0, cells * 8, st));
+        CUDA_TRY(cudaMemsetAsync(oo, 0, cells * 8, st));
+        if (unique) {
+            CUDA_TRY(cudaMemsetAsync(uc, 0, cells * 8, st));
+            CUDA_TRY(cudaMemsetAsync(uo, 0, cells * 8, st));
+        }
+    }
+    if (plain) {
+        if (!sizes)
+            return fail(KSSDGPU_ERR_ARG, "plain kernel needs host-side query sizes");
+        if (lower)
+            return launch_plain<true, false>(ix, P, *sizes, st);
+        return unique ? launch_plain<false, true>(ix, P, *sizes, st) : launch_plain<false, false>(ix, P, *sizes, st);
+    }
+    if (use_smem) {
+        if (lower)
+            return launch_batched<true, false, true>(ix, P, smem, st);
+        return unique ? launch_batched<false, true, true>(ix, P, smem, st)
+                      : launch_batched<false, false, true>(ix, P, smem, st);
+    }
+    if (lower)
+        return launch_batched<true, false, false>(ix, P, 0, st);
+    return unique ? launch_batched<false, true, false>(ix, P, 0, st) : launch_batched<false, false, false>(ix, P, 0, st);
+}
+
+int count_host_impl(kssdgpu_index *ix, const uint64_t *qkeys, const uint64_t *qoffs, int nq, int qgid_offset, bool lower,
+                    unsigned flags, void *ctx, void *obj, void *uctx, void *uobj)
+{
+    if (!ix)
+        return fail(KSSDGPU_ERR_ARG, "null index");
+    if (nq < 0 || (nq > 0 && (!qoffs || !ctx || !obj)))
+        return fail(KSSDGPU_ERR_ARG, "invalid query block arguments");
+    if (nq == 0)
+        return KSSDGPU_OK;
+    const bool unique = (flags & KSSDGPU_UNIQUE) != 0;
+    if (unique && (!uctx || !uobj))
+        return fail(KSSDGPU_ERR_ARG, "unique counters requested without output buffers");
+    CUDA_TRY(cudaSetDevice(ix->device));
+    const uint64_t nkeys = qoffs[nq] - qoffs[0];
+    if (nkeys && !qkeys)
+        return fail(KSSDGPU_ERR_ARG, "null query keys");
+    std::vector<uint64_t> sizes(nq);
+    for (int i = 0; i < nq; ++i) {
+        if (qoffs[i + 1] < qoffs[i])
+            return fail(KSSDGPU_ERR_ARG, "query offsets are not monotone");
+        sizes[i] = qoffs[i + 1] - qoffs[i];
+    }
+    std::vector<int> order(nq);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return sizes[a] > sizes[b]; });
+    const size_t cells = (size_t)nq * ix->nref;
+    const int nout = unique ? 4 : 2;
+    CUDA_TRY(ix->s_keys.ensure(nkeys));
+    CUDA_TRY(ix->s_offs.ensure((size_t)nq + 1));
+    CUDA_TRY(ix->s_out.ensure(cells * nout));
+    CUDA_TRY(ix->s_order.ensure((size_t)nq));
+    cudaStream_t st = 0;
+    if (nkeys)
+        CUDA_TRY(cudaMemcpyAsync(ix->s_keys.p, qkeys, nkeys * 8, cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaMemcpyAsync(ix->s_offs.p, qoffs, ((size_t)nq + 1) * 8, cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaMemcpyAsync(ix->s_order.p, order.data(), (size_t)nq * sizeof(int), cudaMemcpyHostToDevice, st));
+    unsigned long long *oc = ix->s_out.p, *oo = oc + cells;
+    unsigned long long *uc = unique ? oo + cells : nullptr, *uo = unique ? uc + cells : nullptr;
+    int rc = count_dev_impl(ix, ix->s_keys.p, ix->s_offs.p, nq, qgid_offset, lower, flags, oc, oo, uc, uo, ix->s_order.p,
+                            &sizes, st);
+    if (rc)
+        return rc;
+    CUDA_TRY(cudaMemcpyAsync(ctx, oc, cells * 8, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaMemcpyAsync(obj, oo, cells * 8, cudaMemcpyDeviceToHost, st));
+    if (unique) {
+        CUDA_TRY(cudaMemcpyAsync(uctx, uc, cells * 8, cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(cudaMemcpyAsync(uobj, uo, cells * 8, cudaMemcpyDeviceToHost, st));
+    }
+    return check_dev_err(ix, st);
+}
+
+int self_plan(kssdgpu_index *ix, cudaStream_t st)
+{
+    if (ix->j_ready)
+        return KSSDGPU_OK;
+    const uint64_t u = ix->u;
+    CUDA_TRY(ix->j_incl.ensure(u));
+    CUDA_TRY(ix->j_conflict.ensure(u));
+    unsigned long long *np = nullptr;
+    CUDA_TRY(cudaMalloc(&np, std::max<uint64_t>(u, 1) * sizeof(unsigned long long)));
+    k_self_pair_counts<<<grid_for(u), 256, 0, st>>>(ix->gbeg, u, ix->post, np, ix->j_conflict.p);
+    count_launch();
+    size_t tb = 0;
+    CUDA_TRY(cub::DeviceScan::InclusiveSum(nullptr, tb, np, ix->j_incl.p, (int64_t)u, st));
+    void *tmp = nullptr;
+    CUDA_TRY(cudaMalloc(&tmp, std::max<size_t>(tb, 1)));
+    CUDA_TRY(cub::DeviceScan::InclusiveSum(tmp, tb, np, ix->j_incl.p, (int64_t)u, st));
+    count_launch();
+    unsigned long long total = 0;
+    if (u)
+        CUDA_TRY(cudaMemcpyAsync(&total, ix->j_incl.p + u - 1, 8, cudaMemcpyDeviceToHost, st));
+    uint32_t any = 0;
+    {
+        // any conflict group?  reduce with a max
+        uint32_t *d_any = nullptr;
+        CUDA_TRY(cudaMalloc(&d_any, sizeof(uint32_t)));
+        size_t rb = 0;
+        CUDA_TRY(cub::DeviceReduce::Max(nullptr, rb, ix->j_conflict.p, d_any, (int64_t)u, st));
+        void *rt = nullptr;
+        CUDA_TRY(cudaMalloc(&rt, std::max<size_t>(rb, 1)));
+        CUDA_TRY(cub::DeviceReduce::Max(rt, rb, ix->j_conflict.p, d_any, (int64_t)u, st));
+        count_launch();
+        CUDA_TRY(cudaMemcpyAsync(&any, d_any, 4, cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(cudaStreamSynchronize(st));
+        cudaFree(rt);
+        cudaFree(d_any);
+    }
+    CUDA_TRY(cudaStreamSynchronize(st));
+    cudaFree(tmp);
+    cudaFree(np);
+    ix->j_total = u ? total : 0;
+    ix->j_any_conflict = any != 0;
+    ix->j_ready = true;
+    return KSSDGPU_OK;
+}
+
+int self_lower_dev_impl(kssdgpu_index *ix, unsigned flags, unsigned long long *oc, unsigned long long *oo, cudaStream_t st)
+{
+    int rc = self_plan(ix, st);
+    if (rc)
+        return rc;
+    const size_t cells = (size_t)ix->nref * (ix->nref - 1) / 2;
+    CUDA_TRY(cudaMemsetAsync(oc, 0, std::max<size_t>(cells, 1) * 8, st));
+    CUDA_TRY(cudaMemsetAsync(oo, 0, std::max<size_t>(cells, 1) * 8, st));
+    const int per_thread = 16;
+    if (ix->j_total) {
+        const unsigned long long threads = (ix->j_total + per_thread - 1) / per_thread;
+        const unsigned long long blocks = (threads + 255) / 256;
+        k_self_pairs<<<(unsigned)blocks, 256, 0, st>>>(ix->gbeg, ix->u, ix->post, ix->j_incl.p, ix->j_total, per_thread,
+                                                       oc, oo);
+        count_launch();
+    }
+    if (ix->j_any_conflict) {
+        k_self_conflict_groups<<<grid_for(ix->u), 256, 0, st>>>(ix->gbeg, ix->u, ix->post, ix->j_conflict.p,
+                                                                (flags & KSSDGPU_IGNORECONFLICT) ? 1 : 0, oc, oo);
+        count_launch();
+    }
+    CUDA_TRY(cudaGetLastError());
+    return KSSDGPU_OK;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ C ABI
+
+extern "C" {
+
+const char *kssdgpu_last_error(void) { return g_last_error.c_str(); }
+
+uint64_t kssdgpu_launch_count(void) { return g_launches.load(); }
+
+int kssdgpu_index_from_records(const void *records12, uint64_t n, int nref, int obj_bits, int device,
+                               kssdgpu_index_t **out)
+{
+    if (n && !records12)
+        return fail(KSSDGPU_ERR_ARG, "null records");
+    kssdgpu_index *ix = nullptr;
+    int rc = new_index(nref, obj_bits, device, n, &ix);
+    if (rc)
+        return rc;
+    cudaStream_t st = 0;
+    uint32_t *w = nullptr, *head = nullptr;
+    unsigned long long *ctx_of = nullptr;
+    auto cleanup = [&]() {
+        cudaFree(w);
+        cudaFree(head);
+        cudaFree(ctx_of);
+    };
+    cudaError_t e = cudaMalloc(&w, std::max<uint64_t>(n, 1) * 12);
+    if (e == cudaSuccess)
+        e = cudaMalloc(&head, std::max<uint64_t>(n, 1) * 4);
+    if (e == cudaSuccess)
+        e = cudaMalloc(&ctx_of, std::max<uint64_t>(n, 1) * 8);
+    if (e == cudaSuccess && n)
+        e = cudaMemcpyAsync(w, records12, n * 12, cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) {
+        cleanup();
+        kssdgpu_index_free(ix);
+        return fail(KSSDGPU_ERR_CUDA, std::string("index upload: ") + cudaGetErrorString(e));
+    }
+    if (n) {
+        k_unpack_records<<<grid_for(n), 256, 0, st>>>(w, n, nref, ix->post, head, ctx_of, ix->err);
+        count_launch();
+    }
+    rc = finish_build(ix, head, ctx_of, st);
+    cleanup();
+    if (rc) {
+        kssdgpu_index_free(ix);
+        return rc;
+    }
+    *out = ix;
+    return KSSDGPU_OK;
+}
+
+int kssdgpu_index_from_sketch(const uint64_t *keys, const uint64_t *offs, int nref, int obj_bits, int device,
+                              kssdgpu_index_t **out)
+{
+    if (!offs)
+        return fail(KSSDGPU_ERR_ARG, "null offsets");
+    if (nref <= 0)
+        return fail(KSSDGPU_ERR_ARG, "reference count must be positive");
+    const uint64_t n = offs[nref] - offs[0];
+    if (n && !keys)
+        return fail(KSSDGPU_ERR_ARG, "null keys");
+    kssdgpu_index *ix = nullptr;
+    int rc = new_index(nref, obj_bits, device, n, &ix);
+    if (rc)
+        return rc;
+    cudaStream_t st = 0;
+    uint64_t *dk = nullptr, *doffs = nullptr;
+    unsigned long long *skey = nullptr, *skey2 = nullptr, *ctx_of = nullptr;
+    uint32_t *sval = nullptr, *sval2 = nullptr, *head = nullptr;
+    void *tmp = nullptr;
+    auto cleanup = [&]() {
+        cudaFree(dk);
+        cudaFree(doffs);
+        cudaFree(skey);
+        cudaFree(skey2);
+        cudaFree(ctx_of);
+        cudaFree(sval);
+        cudaFree(sval2);
+        cudaFree(head);
+        cudaFree(tmp);
+    };
+    const uint64_t nn = std::max<uint64_t>(n, 1);
+    cudaError_t e = cudaMalloc(&dk, nn * 8);
+    if (e == cudaSuccess) e = cudaMalloc(&doffs, ((uint64_t)nref + 1) * 8);
+    if (e == cudaSuccess) e = cudaMalloc(&skey, nn * 8);
+    if (e == cudaSuccess) e = cudaMalloc(&skey2, nn * 8);
+    if (e == cudaSuccess) e = cudaMalloc(&sval, nn * 4);
+    if (e == cudaSuccess) e = cudaMalloc(&sval2, nn * 4);
+    if (e == cudaSuccess) e = cudaMalloc(&head, nn * 4);
+    if (e == cudaSuccess) e = cudaMalloc(&ctx_of, nn * 8);
+    if (e == cudaSuccess && n) e = cudaMemcpyAsync(dk, keys, n * 8, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(doffs, offs, ((uint64_t)nref + 1) * 8, cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) {
+        cleanup();
+        kssdgpu_index_free(ix);
+        return fail(e == cudaErrorMemoryAllocation ? KSSDGPU_ERR_NOMEM : KSSDGPU_ERR_CUDA,
+                    std::string("sketch upload: ") + cudaGetErrorString(e));
+    }
+    if (n) {
+        k_sketch_to_sortkeys<<<std::min(nref, 148 * 16), 256, 0, st>>>(dk, doffs, nref, obj_bits, skey, sval, ix->err);
+        count_launch();
+        // stable LSD radix sort on the 64-bit ctxgid; equal keys keep comblco (obj ascending) order
+        int end_bit = 64;
+        size_t tb = 0;
+        e = cub::DeviceRadixSort::SortPairs(nullptr, tb, skey, skey2, sval, sval2, (int64_t)n, 0, end_bit, st);
+        if (e == cudaSuccess) e = cudaMalloc(&tmp, std::max<size_t>(tb, 1));
+        if (e == cudaSuccess)
+            e = cub::DeviceRadixSort::SortPairs(tmp, tb, skey, skey2, sval, sval2, (int64_t)n, 0, end_bit, st);
+        count_launch(4);
+        if (e != cudaSuccess) {
+            cleanup();
+            kssdgpu_index_free(ix);
+            return fail(KSSDGPU_ERR_CUDA, std::string("device sort: ") + cudaGetErrorString(e));
+        }
+        k_sorted_to_post<<<grid_for(n), 256, 0, st>>>(skey2, sval2, n, ix->post, head, ctx_of);
+        count_launch();
+    }
+    rc = finish_build(ix, head, ctx_of, st);
+    cleanup();
+    if (rc) {
+        kssdgpu_index_free(ix);
+        return rc;
+    }
+    *out = ix;
+    return KSSDGPU_OK;
+}
+
+void kssdgpu_index_free(kssdgpu_index_t *ix)
+{
+    if (!ix)
+        return;
+    cudaSetDevice(ix->device);
+    cudaFree(ix->post);
+    cudaFree(ix->gkey);
+    cudaFree(ix->gbeg);
+    cudaFree(ix->table);
+    cudaFree(ix->err);
+    cudaFree(ix->work);
+    ix->s_keys.release();
+    ix->s_offs.release();
+    ix->s_out.release();
+    ix->s_order.release();
+    ix->j_incl.release();
+    ix->j_conflict.release();
+    delete ix;
+}
+
+int kssdgpu_index_info(const kssdgpu_index_t *ix, uint64_t *records, uint64_t *contexts, int *nref, int *obj_bits)
+{
+    if (!ix)
+        return fail(KSSDGPU_ERR_ARG, "null index");
+    if (records) *records = ix->n;
+    if (contexts) *contexts = ix->u;
+    if (nref) *nref = ix->nref;
+    if (obj_bits) *obj_bits = ix->obj_bits;
+    return KSSDGPU_OK;
+}
+
+int kssdgpu_index_export(const kssdgpu_index_t *cix, void *records12, uint8_t *unique_bits)
+{
+    kssdgpu_index *ix = const_cast<kssdgpu_index *>(cix);
+    if (!ix)
+        return fail(KSSDGPU_ERR_ARG, "null index");
+    CUDA_TRY(cudaSetDevice(ix->device));
+    cudaStream_t st = 0;
+    const uint64_t n = ix->n;
+    if (records12 && n) {
+        uint32_t *w = nullptr;
+        CUDA_TRY(cudaMalloc(&w, n * 12));
+        k_export_records<<<grid_for(ix->u), 256, 0, st>>>(ix->gkey, ix->gbeg, ix->u, ix->post, w);
+        count_launch();
+        CUDA_TRY(cudaMemcpyAsync(records12, w, n * 12, cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(cudaStreamSynchronize(st));
+        cudaFree(w);
+    }
+    if (unique_bits && n) {
+        const uint64_t words = (n + 31) / 32;
+        uint32_t *b = nullptr;
+        CUDA_TRY(cudaMalloc(&b, words * 4));
+        CUDA_TRY(cudaMemsetAsync(b, 0, words * 4, st));
+        k_unique_bits<<<grid_for(ix->u), 256, 0, st>>>(ix->gbeg, ix->u, ix->post, b);
+        count_launch();
+        std::vector<uint32_t> hb(words);
+        CUDA_TRY(cudaMemcpyAsync(hb.data(), b, words * 4, cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(cudaStreamSynchronize(st));
+        cudaFree(b);
+        std::memcpy(unique_bits, hb.data(), (n + 7) / 8);
+    }
+    return KSSDGPU_OK;
+}
+
+int kssdgpu_index_ref_ctx_counts(const kssdgpu_index_t *cix, int conflict, int ignoreconflict, uint32_t *ctx_count_out,
+                                 uint32_t *unique_out)
+{
+    kssdgpu_index *ix = const_cast<kssdgpu_index *>(cix);
+    if (!ix || (!ctx_count_out && !unique_out))
+        return fail(KSSDGPU_ERR_ARG, "null argument");
+    CUDA_TRY(cudaSetDevice(ix->device));
+    cudaStream_t st = 0;
+    uint32_t *c = nullptr;
+    CUDA_TRY(cudaMalloc(&c, (size_t)ix->nref * 2 * sizeof(uint32_t)));
+    CUDA_TRY(cudaMemsetAsync(c, 0, (size_t)ix->nref * 2 * sizeof(uint32_t), st));
+    k_ref_counts<<<grid_for(ix->u), 256, 0, st>>>(ix->gbeg, ix->u, ix->post, conflict, ignoreconflict, c, c + ix->nref);
+    count_launch();
+    if (ctx_count_out)
+        CUDA_TRY(cudaMemcpyAsync(ctx_count_out, c, (size_t)ix->nref * 4, cudaMemcpyDeviceToHost, st));
+    if (unique_out)
+        CUDA_TRY(cudaMemcpyAsync(unique_out, c + ix->nref, (size_t)ix->nref * 4, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    cudaFree(c);
+    return KSSDGPU_OK;
+}
+
+int kssdgpu_count_block(kssdgpu_index_t *ix, const uint64_t *qry_keys, const uint64_t *qry_offs, int nq, unsigned flags,
+                        kssdgpu_ctx_mut2_t *ctx, kssdgpu_obj_section_t *obj, kssdgpu_ctx_mut2_t *uctx,
+                        kssdgpu_obj_section_t *uobj)
+{
+    return count_host_impl(ix, qry_keys, qry_offs, nq, 0, false, flags, ctx, obj, uctx, uobj);
+}
+
+int kssdgpu_count_lower(kssdgpu_index_t *ix, const uint64_t *qry_keys, const uint64_t *qry_offs, int nq,
+                        int qry_gid_offset, unsigned flags, kssdgpu_ctx_mut2_t *ctx, kssdgpu_obj_section_t *obj)
+{
+    if (flags & KSSDGPU_UNIQUE)
+        return fail(KSSDGPU_ERR_ARG, "unique-context counting has no lower-triangle form");
+    return count_host_impl(ix, qry_keys, qry_offs, nq, qry_gid_offset, true, flags, ctx, obj, nullptr, nullptr);
+}
+
+int kssdgpu_count_block_dev(kssdgpu_index_t *ix, const uint64_t *d_qry_keys, const uint64_t *d_qry_offs, int nq,
+                            int qry_gid_offset, int lower, unsigned flags, kssdgpu_ctx_mut2_t *d_ctx,
+                            kssdgpu_obj_section_t *d_obj, kssdgpu_ctx_mut2_t *d_uctx, kssdgpu_obj_section_t *d_uobj,
+                            void *stream)
+{
+    if (!ix || nq < 0 || (nq && (!d_qry_offs || !d_ctx || !d_obj)))
+        return fail(KSSDGPU_ERR_ARG, "invalid device count arguments");
+    if (flags & KSSDGPU_PLAIN)
+        return fail(KSSDGPU_ERR_ARG, "the plain kernel needs host offsets; use the host-buffer call");
+    CUDA_TRY(cudaSetDevice(ix->device));
+    return count_dev_impl(ix, d_qry_keys, d_qry_offs, nq, qry_gid_offset, lower != 0, flags,
+                          reinterpret_cast<unsigned long long *>(d_ctx), reinterpret_cast<unsigned long long *>(d_obj),
+                          reinterpret_cast<unsigned long long *>(d_uctx), reinterpret_cast<unsigned long long *>(d_uobj),
+                          nullptr, nullptr, (cudaStream_t)stream);
+}
+
+int kssdgpu_sync(kssdgpu_index_t *ix, void *stream)
+{
+    if (!ix)
+        return fail(KSSDGPU_ERR_ARG, "null index");
+    CUDA_TRY(cudaSetDevice(ix->device));
+    CUDA_TRY(cudaGetLastError());
+    return check_dev_err(ix, (cudaStream_t)stream);
+}
+
+int kssdgpu_self_lower(kssdgpu_index_t *ix, unsigned flags, kssdgpu_ctx_mut2_t *ctx_lower,
+                       kssdgpu_obj_section_t *obj_lower)
+{
+    if (!ix || !ctx_lower || !obj_lower)
+        return fail(KSSDGPU_ERR_ARG, "null argument");
+    CUDA_TRY(cudaSetDevice(ix->device));
+    const size_t cells = (size_t)ix->nref * (ix->nref - 1) / 2;
+    CUDA_TRY(ix->s_out.ensure(std::max<size_t>(cells, 1) * 2));
+    cudaStream_t st = 0;
+    int rc = self_lower_dev_impl(ix, flags, ix->s_out.p, ix->s_out.p + std::max<size_t>(cells, 1), st);
+    if (rc)
+        return rc;
+    if (cells) {
+        CUDA_TRY(cudaMemcpyAsync(ctx_lower, ix->s_out.p, cells * 8, cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(cudaMemcpyAsync(obj_lower, ix->s_out.p + cells, cells * 8, cudaMemcpyDeviceToHost, st));
+    }
+    return check_dev_err(ix, st);
+}
+
+int kssdgpu_self_lower_dev(kssdgpu_index_t *ix, unsigned flags, kssdgpu_ctx_mut2_t *d_ctx_lower,
+                           kssdgpu_obj_section_t *d_obj_lower, void *stream)
+{
+    if (!ix || !d_ctx_lower || !d_obj_lower)
+        return fail(KSSDGPU_ERR_ARG, "null argument");
+    CUDA_TRY(cudaSetDevice(ix->device));
+    return self_lower_dev_impl(ix, flags, reinterpret_cast<unsigned long long *>(d_ctx_lower),
+                               reinterpret_cast<unsigned long long *>(d_obj_lower), (cudaStream_t)stream);
+}
+
+}  // extern "C"

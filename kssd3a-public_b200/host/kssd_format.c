@@ -1,0 +1,257 @@
+/*
+ * Sketch directory and inverted-index I/O (formats described in kssd_format.h).
+ * Size checks follow the reference reader: comblco must hold exactly
+ * comblco.index[n] keys (src/global_basic.c:1110-1114), the index exactly as many
+ * 12-byte records (src/command_ani.c:516), sidecars exactly n records
+ * (src/command_ani.c:223-248).
+ */
+#define _GNU_SOURCE
+#include "kssd_format.h"
+
+#include <errno.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <sys/stat.h>
+#include <unistd.h>
+
+static __thread char g_err[1024];
+
+const char *kssd_host_last_error(void) { return g_err; }
+
+static void set_err(const char *fmt, ...)
+{
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof g_err, fmt, ap);
+    va_end(ap);
+}
+
+bool kssd_file_exists(const char *dir, const char *name)
+{
+    char p[4096];
+    snprintf(p, sizeof p, "%s/%s", dir, name);
+    return access(p, F_OK) == 0;
+}
+
+static void *read_all(const char *dir, const char *name, size_t *size)
+{
+    char p[4096];
+    snprintf(p, sizeof p, "%s/%s", dir, name);
+    FILE *f = fopen(p, "rb");
+    if (!f) {
+        set_err("cannot open %s: %s", p, strerror(errno));
+        return NULL;
+    }
+    if (fseeko(f, 0, SEEK_END) != 0) {
+        fclose(f);
+        set_err("cannot seek %s", p);
+        return NULL;
+    }
+    off_t len = ftello(f);
+    rewind(f);
+    void *buf = malloc(len > 0 ? (size_t)len : 1);
+    if (!buf) {
+        fclose(f);
+        set_err("out of memory reading %s (%lld bytes)", p, (long long)len);
+        return NULL;
+    }
+    if (len > 0 && fread(buf, 1, (size_t)len, f) != (size_t)len) {
+        free(buf);
+        fclose(f);
+        set_err("short read on %s", p);
+        return NULL;
+    }
+    fclose(f);
+    *size = (size_t)len;
+    return buf;
+}
+
+static int write_all(const char *dir, const char *name, const void *a, size_t an, const void *b,
+                     size_t bn)
+{
+    char p[4096];
+    snprintf(p, sizeof p, "%s/%s", dir, name);
+    FILE *f = fopen(p, "wb");
+    if (!f) {
+        set_err("cannot create %s: %s", p, strerror(errno));
+        return -1;
+    }
+    int ok = (an == 0 || fwrite(a, 1, an, f) == an) && (bn == 0 || fwrite(b, 1, bn, f) == bn);
+    ok = (fclose(f) == 0) && ok;
+    if (!ok) {
+        set_err("write failed on %s", p);
+        return -1;
+    }
+    return 0;
+}
+
+void kssd_stat_bits(const kssd_sketch_stat_t *st, int *ctx_bits, int *obj_bits)
+{
+    const int ctx = st->coden_len > 0 ? 4 * st->coden_len : 4 * st->hclen;
+    if (ctx_bits)
+        *ctx_bits = ctx;
+    if (obj_bits)
+        *obj_bits = 2 * st->klen - ctx;
+}
+
+int kssd_read_stat(const char *dir, kssd_sketch_stat_t *out)
+{
+    size_t sz = 0;
+    void *b = read_all(dir, "lcofiles.stat", &sz);
+    if (!b)
+        return -1;
+    if (sz < sizeof(kssd_sketch_stat_t)) {
+        free(b);
+        set_err("%s/lcofiles.stat has %zu bytes, expected at least %zu", dir, sz,
+                sizeof(kssd_sketch_stat_t));
+        return -1;
+    }
+    memcpy(out, b, sizeof *out);
+    free(b);
+    return 0;
+}
+
+kssd_sketch_t *kssd_sketch_load(const char *dir, unsigned flags)
+{
+    kssd_sketch_t *s = calloc(1, sizeof *s);
+    if (!s) {
+        set_err("out of memory");
+        return NULL;
+    }
+    size_t sz = 0;
+    char *stat = read_all(dir, "lcofiles.stat", &sz);
+    if (!stat)
+        goto fail;
+    if (sz < sizeof(kssd_sketch_stat_t)) {
+        set_err("%s/lcofiles.stat too short", dir);
+        free(stat);
+        goto fail;
+    }
+    memcpy(&s->stat, stat, sizeof s->stat);
+    s->n = s->stat.infile_num;
+    if (s->n < 0 || sz < sizeof(kssd_sketch_stat_t) + (size_t)s->n * KSSD_PATHLEN) {
+        set_err("%s/lcofiles.stat: %zu bytes cannot hold %d names", dir, sz, s->n);
+        free(stat);
+        goto fail;
+    }
+    s->names = malloc((size_t)(s->n ? s->n : 1) * KSSD_PATHLEN);
+    if (!s->names) {
+        free(stat);
+        set_err("out of memory");
+        goto fail;
+    }
+    memcpy(s->names, stat + sizeof(kssd_sketch_stat_t), (size_t)s->n * KSSD_PATHLEN);
+    for (int i = 0; i < s->n; i++)
+        s->names[i][KSSD_PATHLEN - 1] = '\0';
+    free(stat);
+    kssd_stat_bits(&s->stat, &s->ctx_bits, &s->obj_bits);
+
+    size_t isz = 0;
+    s->offs = read_all(dir, "comblco.index", &isz);
+    if (!s->offs)
+        goto fail;
+    if (isz < (size_t)(s->n + 1) * sizeof(uint64_t)) {
+        set_err("%s/comblco.index has %zu bytes, expected %zu", dir, isz,
+                (size_t)(s->n + 1) * sizeof(uint64_t));
+        goto fail;
+    }
+    for (int i = 0; i < s->n; i++)
+        if (s->offs[i + 1] < s->offs[i]) {
+            set_err("%s/comblco.index is not monotone at sample %d", dir, i);
+            goto fail;
+        }
+    size_t ksz = 0;
+    s->keys = read_all(dir, "comblco", &ksz);
+    if (!s->keys)
+        goto fail;
+    const size_t expect = (size_t)s->offs[s->n] * sizeof(uint64_t);
+    if (ksz != expect) {
+        set_err("%s/comblco has %zu bytes, expected %zu", dir, ksz, expect);
+        goto fail;
+    }
+    if ((flags & 1u) && kssd_file_exists(dir, "lcofiles.anno")) {
+        size_t asz = 0;
+        s->anno = read_all(dir, "lcofiles.anno", &asz);
+        if (!s->anno)
+            goto fail;
+        if (asz != (size_t)s->n * KSSD_PATHLEN) {
+            set_err("%s/lcofiles.anno has %zu bytes, expected %zu", dir, asz,
+                    (size_t)s->n * KSSD_PATHLEN);
+            goto fail;
+        }
+    }
+    if ((flags & 2u) && kssd_file_exists(dir, "lcofiles.infilemeta")) {
+        size_t msz = 0;
+        s->meta = read_all(dir, "lcofiles.infilemeta", &msz);
+        if (!s->meta)
+            goto fail;
+        if (msz != (size_t)s->n * sizeof(kssd_infile_meta_t)) {
+            set_err("%s/lcofiles.infilemeta has %zu bytes, expected %zu", dir, msz,
+                    (size_t)s->n * sizeof(kssd_infile_meta_t));
+            goto fail;
+        }
+    }
+    return s;
+fail:
+    kssd_sketch_free(s);
+    return NULL;
+}
+
+void kssd_sketch_free(kssd_sketch_t *s)
+{
+    if (!s)
+        return;
+    free(s->names);
+    free(s->keys);
+    free(s->offs);
+    free(s->anno);
+    free(s->meta);
+    free(s);
+}
+
+int kssd_sketch_write(const char *dir, const kssd_sketch_stat_t *stat, int n,
+                      const char (*names)[KSSD_PATHLEN], const uint64_t *keys,
+                      const uint64_t *offs)
+{
+    if (mkdir(dir, 0755) != 0 && errno != EEXIST) {
+        set_err("cannot create %s: %s", dir, strerror(errno));
+        return -1;
+    }
+    kssd_sketch_stat_t st = *stat;
+    st.infile_num = n;
+    if (write_all(dir, "lcofiles.stat", &st, sizeof st, names, (size_t)n * KSSD_PATHLEN))
+        return -1;
+    if (write_all(dir, "comblco", keys, (size_t)offs[n] * sizeof(uint64_t), NULL, 0))
+        return -1;
+    if (write_all(dir, "comblco.index", offs, (size_t)(n + 1) * sizeof(uint64_t), NULL, 0))
+        return -1;
+    return 0;
+}
+
+kssd_index_rec_t *kssd_index_load(const char *dir, size_t *n_out)
+{
+    size_t sz = 0;
+    kssd_index_rec_t *r = read_all(dir, "sortedcomb_ctxgid64obj32", &sz);
+    if (!r)
+        return NULL;
+    if (sz % sizeof(kssd_index_rec_t)) {
+        free(r);
+        set_err("%s/sortedcomb_ctxgid64obj32 size %zu is not a multiple of 12", dir, sz);
+        return NULL;
+    }
+    *n_out = sz / sizeof(kssd_index_rec_t);
+    return r;
+}
+
+int kssd_index_write(const char *dir, const kssd_index_rec_t *recs, size_t n,
+                     const uint8_t *unique_bits)
+{
+    if (write_all(dir, "sortedcomb_ctxgid64obj32", recs, n * sizeof(*recs), NULL, 0))
+        return -1;
+    if (unique_bits &&
+        write_all(dir, "sortedcomb_ctxgid64obj32.unique_bits", unique_bits, (n + 7) / 8, NULL, 0))
+        return -1;
+    return 0;
+}

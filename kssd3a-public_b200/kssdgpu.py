@@ -1,0 +1,348 @@
+"""ctypes binding of libkssdgpu (include/kssdgpu.h) and libkssdhost (sketch I/O and
+synthetic workloads), with numpy arrays on the host side and optional torch CUDA
+tensors for the device-pointer calls.
+
+The shared libraries are built in-tree (``make -C kssd3a-public_b200``).  There is
+no fallback: loading fails loudly when they are missing, and every call checks
+its status code and raises ``KssdGpuError`` with the library's message.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIBDIR = os.path.join(HERE, "lib")
+
+# flags (include/kssdgpu.h)
+IGNORECONFLICT = 0x1
+UNIQUE = 0x2
+PLAIN = 0x4
+GLOBAL_ACC = 0x8
+
+_u64p = np.ctypeslib.ndpointer(dtype=np.uint64, flags="C_CONTIGUOUS")
+_u32p = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
+_u8p = np.ctypeslib.ndpointer(dtype=np.uint8, flags="C_CONTIGUOUS")
+
+
+class KssdGpuError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"kssdgpu error {code}: {msg}")
+        self.code = code
+
+
+def _load(name: str) -> C.CDLL:
+    path = os.path.join(LIBDIR, name)
+    if not os.path.exists(path):
+        raise ImportError(f"{path} is missing: build it with `make -C {HERE}`")
+    return C.CDLL(path)
+
+
+_gpu = None
+_host = None
+
+
+def gpu_lib() -> C.CDLL:
+    global _gpu
+    if _gpu is None:
+        lib = _load("libkssdgpu.so")
+        vp = C.c_void_p
+        lib.kssdgpu_last_error.restype = C.c_char_p
+        lib.kssdgpu_launch_count.restype = C.c_uint64
+        lib.kssdgpu_index_from_records.argtypes = [vp, C.c_uint64, C.c_int, C.c_int, C.c_int, C.POINTER(vp)]
+        lib.kssdgpu_index_from_sketch.argtypes = [_u64p, _u64p, C.c_int, C.c_int, C.c_int, C.POINTER(vp)]
+        lib.kssdgpu_index_free.argtypes = [vp]
+        lib.kssdgpu_index_free.restype = None
+        lib.kssdgpu_index_info.argtypes = [vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
+                                           C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        lib.kssdgpu_index_export.argtypes = [vp, vp, vp]
+        lib.kssdgpu_index_ref_ctx_counts.argtypes = [vp, C.c_int, C.c_int, vp, vp]
+        lib.kssdgpu_count_block.argtypes = [vp, vp, _u64p, C.c_int, C.c_uint, vp, vp, vp, vp]
+        lib.kssdgpu_count_lower.argtypes = [vp, vp, _u64p, C.c_int, C.c_int, C.c_uint, vp, vp]
+        lib.kssdgpu_count_block_dev.argtypes = [vp, vp, vp, C.c_int, C.c_int, C.c_int, C.c_uint,
+                                                vp, vp, vp, vp, vp]
+        lib.kssdgpu_sync.argtypes = [vp, vp]
+        lib.kssdgpu_self_lower.argtypes = [vp, C.c_uint, vp, vp]
+        lib.kssdgpu_self_lower_dev.argtypes = [vp, C.c_uint, vp, vp, vp]
+        _gpu = lib
+    return _gpu
+
+
+class _SynthCfg(C.Structure):
+    _fields_ = [
+        ("seed", C.c_uint64), ("sample_seed", C.c_uint64), ("n_samples", C.c_int),
+        ("n_clusters", C.c_int), ("role", C.c_int), ("size_dist", C.c_int),
+        ("len_median", C.c_double), ("len_sigma", C.c_double), ("len_min", C.c_double),
+        ("len_max", C.c_double), ("sub_lo", C.c_double), ("sub_hi", C.c_double),
+        ("indel_rate", C.c_double), ("density", C.c_double), ("ctx_bits", C.c_int),
+        ("obj_bits", C.c_int), ("klen", C.c_int), ("ref_sample_seed", C.c_uint64),
+        ("ref_samples", C.c_int), ("reads_min_genomes", C.c_int), ("reads_max_genomes", C.c_int),
+        ("cov_lo", C.c_double), ("cov_hi", C.c_double), ("err_lo", C.c_double),
+        ("err_hi", C.c_double), ("threads", C.c_int),
+    ]
+
+
+class _SynthOut(C.Structure):
+    _fields_ = [("n", C.c_int), ("keys", C.POINTER(C.c_uint64)), ("offs", C.POINTER(C.c_uint64)),
+                ("lengths", C.POINTER(C.c_double))]
+
+
+def host_lib() -> C.CDLL:
+    global _host
+    if _host is None:
+        lib = _load("libkssdhost.so")
+        lib.kssd_host_last_error.restype = C.c_char_p
+        lib.kssd_synth_default.argtypes = [C.POINTER(_SynthCfg)]
+        lib.kssd_synth_default.restype = None
+        lib.kssd_synth_generate.argtypes = [C.POINTER(_SynthCfg)]
+        lib.kssd_synth_generate.restype = C.POINTER(_SynthOut)
+        lib.kssd_synth_free.argtypes = [C.POINTER(_SynthOut)]
+        lib.kssd_synth_free.restype = None
+        _host = lib
+    return _host
+
+
+def _check(rc: int):
+    if rc != 0:
+        raise KssdGpuError(rc, gpu_lib().kssdgpu_last_error().decode(errors="replace"))
+
+
+def launch_count() -> int:
+    """Kernels launched by libkssdgpu so far in this process."""
+    return int(gpu_lib().kssdgpu_launch_count())
+
+
+# ---------------------------------------------------------------- synthetic workloads
+
+ROLE_MEMBER, ROLE_OWNLEN, ROLE_READS = 0, 1, 2
+SIZE_FIXED, SIZE_LOGNORMAL, SIZE_LOGUNIFORM = 0, 1, 2
+
+
+@dataclass
+class Sketch:
+    """A sketch in memory: comblco keys, comblco.index offsets, sample names."""
+    keys: np.ndarray
+    offs: np.ndarray
+    names: list
+    conflict: bool = False
+    obj_bits: int = 20
+    lengths: np.ndarray | None = None
+
+    @property
+    def n(self) -> int:
+        return len(self.offs) - 1
+
+
+def synth(**kw) -> Sketch:
+    """Generate a synthetic sketch (see host/kssd_synth.h for the model and fields)."""
+    prefix = kw.pop("name_prefix", None)
+    lib = host_lib()
+    cfg = _SynthCfg()
+    lib.kssd_synth_default(C.byref(cfg))
+    for k, v in kw.items():
+        if not hasattr(cfg, k):
+            raise KeyError(k)
+        setattr(cfg, k, v)
+    out = lib.kssd_synth_generate(C.byref(cfg))
+    if not out:
+        raise ValueError("invalid synthetic workload configuration")
+    try:
+        n = out.contents.n
+        offs = np.ctypeslib.as_array(out.contents.offs, shape=(n + 1,)).copy()
+        keys = np.ctypeslib.as_array(out.contents.keys, shape=(max(int(offs[-1]), 1),))[: int(offs[-1])].copy()
+        lengths = np.ctypeslib.as_array(out.contents.lengths, shape=(max(n, 1),))[:n].copy()
+    finally:
+        lib.kssd_synth_free(out)
+    prefix = prefix or ("read" if cfg.role == ROLE_READS else "g")
+    names = [f"{prefix}{i}" for i in range(n)]
+    return Sketch(keys=keys, offs=offs, names=names, conflict=cfg.role == ROLE_READS,
+                  obj_bits=cfg.obj_bits, lengths=lengths)
+
+
+# ---------------------------------------------------------------- sketch directories
+
+STAT_DTYPE = np.dtype([("hash_id", "<u4"), ("koc", "u1"), ("conflict", "u1"), ("pad", "V2"),
+                       ("coden_len", "<i4"), ("klen", "<i4"), ("hclen", "<i4"), ("holen", "<i4"),
+                       ("drfold", "<i4"), ("infile_num", "<i4")])
+REC_DTYPE = np.dtype([("ctxgid", "<u8"), ("obj", "<u4")])  # packed 12 B
+DEFAULT_HASH_ID = 1772583717  # the reference sketcher's id for its default coden/k=32/f8 pattern
+
+
+def write_sketch_dir(path: str, sk: Sketch, coden_len: int = 11, klen: int = 32, drfold: int = 8,
+                     hash_id: int = DEFAULT_HASH_ID, with_index: bool = False):
+    """Write a sketch directory in the reference layout (lcofiles.stat, comblco, comblco.index);
+    with_index also writes sortedcomb_ctxgid64obj32 and its unique_bits."""
+    os.makedirs(path, exist_ok=True)
+    st = np.zeros(1, dtype=STAT_DTYPE)
+    st["hash_id"], st["koc"], st["conflict"] = hash_id, 0, int(sk.conflict)
+    st["coden_len"], st["klen"], st["hclen"], st["holen"] = coden_len, klen, 0, 0
+    st["drfold"], st["infile_num"] = drfold, sk.n
+    names = b"".join(nm.encode()[:255].ljust(256, b"\0") for nm in sk.names)
+    with open(os.path.join(path, "lcofiles.stat"), "wb") as f:
+        f.write(st.tobytes() + names)
+    sk.keys.astype("<u8").tofile(os.path.join(path, "comblco"))
+    sk.offs.astype("<u8").tofile(os.path.join(path, "comblco.index"))
+    if with_index:
+        recs = build_records_np(sk)
+        recs.tofile(os.path.join(path, "sortedcomb_ctxgid64obj32"))
+        unique_bits_np(recs).tofile(os.path.join(path, "sortedcomb_ctxgid64obj32.unique_bits"))
+
+
+def read_sketch_dir(path: str) -> Sketch:
+    raw = open(os.path.join(path, "lcofiles.stat"), "rb").read()
+    st = np.frombuffer(raw[:32], dtype=STAT_DTYPE)[0]
+    n = int(st["infile_num"])
+    names = [raw[32 + 256 * i: 32 + 256 * (i + 1)].split(b"\0")[0].decode(errors="replace") for i in range(n)]
+    offs = np.fromfile(os.path.join(path, "comblco.index"), dtype="<u8")[: n + 1].astype(np.uint64)
+    keys = np.fromfile(os.path.join(path, "comblco"), dtype="<u8").astype(np.uint64)
+    ctx_bits = 4 * int(st["coden_len"]) if st["coden_len"] > 0 else 4 * int(st["hclen"])
+    return Sketch(keys=keys, offs=offs, names=names, conflict=bool(st["conflict"]),
+                  obj_bits=2 * int(st["klen"]) - ctx_bits)
+
+
+def read_index_records(path: str) -> np.ndarray:
+    return np.fromfile(os.path.join(path, "sortedcomb_ctxgid64obj32"), dtype=REC_DTYPE)
+
+
+def build_records_np(sk: Sketch) -> np.ndarray:
+    """Reference index records of a sketch, built with numpy (host helper for fixtures)."""
+    counts = np.diff(sk.offs).astype(np.int64)
+    gid = np.repeat(np.arange(sk.n, dtype=np.uint64), counts)
+    ctxgid = ((sk.keys >> np.uint64(sk.obj_bits)) << np.uint64(20)) | gid
+    obj = (sk.keys & np.uint64((1 << sk.obj_bits) - 1)).astype(np.uint32)
+    order = np.lexsort((obj, ctxgid))
+    rec = np.zeros(len(order), dtype=REC_DTYPE)
+    rec["ctxgid"] = ctxgid[order]
+    rec["obj"] = obj[order]
+    return rec
+
+
+def unique_bits_np(rec: np.ndarray) -> np.ndarray:
+    ctx = rec["ctxgid"] >> np.uint64(20)
+    key = np.stack([ctx, rec["obj"].astype(np.uint64)], axis=1)
+    _, inv, cnt = np.unique(key, axis=0, return_inverse=True, return_counts=True)
+    uniq = cnt[inv.ravel()] == 1
+    return np.packbits(uniq.astype(np.uint8), bitorder="little")
+
+
+# ---------------------------------------------------------------- index and counting
+
+
+class Index:
+    """Device-resident CSR of a reference index (opaque libkssdgpu handle)."""
+
+    def __init__(self, handle: int, nref: int, obj_bits: int):
+        self._h = C.c_void_p(handle)
+        self.nref = nref
+        self.obj_bits = obj_bits
+
+    @classmethod
+    def from_records(cls, records: np.ndarray, nref: int, obj_bits: int = 20, device: int = 0) -> "Index":
+        rec = np.ascontiguousarray(records)
+        if rec.dtype.itemsize != 12:
+            raise ValueError("records must be packed 12-byte {u64 ctxgid; u32 obj}")
+        h = C.c_void_p()
+        _check(gpu_lib().kssdgpu_index_from_records(rec.ctypes.data if len(rec) else None, len(rec),
+                                                    nref, obj_bits, device, C.byref(h)))
+        return cls(h.value, nref, obj_bits)
+
+    @classmethod
+    def from_sketch(cls, sk: Sketch, device: int = 0) -> "Index":
+        h = C.c_void_p()
+        keys = np.ascontiguousarray(sk.keys, dtype=np.uint64)
+        if len(keys) == 0:
+            keys = np.zeros(1, dtype=np.uint64)
+        _check(gpu_lib().kssdgpu_index_from_sketch(keys, np.ascontiguousarray(sk.offs, dtype=np.uint64),
+                                                   sk.n, sk.obj_bits, device, C.byref(h)))
+        return cls(h.value, sk.n, sk.obj_bits)
+
+    def close(self):
+        if self._h and self._h.value:
+            gpu_lib().kssdgpu_index_free(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def info(self):
+        r, u, n, o = C.c_uint64(), C.c_uint64(), C.c_int(), C.c_int()
+        _check(gpu_lib().kssdgpu_index_info(self._h, C.byref(r), C.byref(u), C.byref(n), C.byref(o)))
+        return dict(records=r.value, contexts=u.value, nref=n.value, obj_bits=o.value)
+
+    def export(self):
+        info = self.info()
+        rec = np.zeros(info["records"], dtype=REC_DTYPE)
+        bits = np.zeros((info["records"] + 7) // 8, dtype=np.uint8)
+        _check(gpu_lib().kssdgpu_index_export(self._h, rec.ctypes.data if len(rec) else None,
+                                              bits.ctypes.data if len(bits) else None))
+        return rec, bits
+
+    def ref_ctx_counts(self, conflict: bool, ignoreconflict: bool):
+        c = np.zeros(self.nref, dtype=np.uint32)
+        u = np.zeros(self.nref, dtype=np.uint32)
+        _check(gpu_lib().kssdgpu_index_ref_ctx_counts(self._h, int(conflict), int(ignoreconflict),
+                                                      c.ctypes.data, u.ctypes.data))
+        return c, u
+
+    def count_block(self, qkeys: np.ndarray, qoffs: np.ndarray, flags: int = 0):
+        """Returns (ctx, obj[, uctx, uobj]) as uint32 arrays of shape [nq, nref, 2]."""
+        nq = len(qoffs) - 1
+        qk = np.ascontiguousarray(qkeys, dtype=np.uint64)
+        qo = np.ascontiguousarray(qoffs, dtype=np.uint64)
+        outs = [np.zeros((nq, self.nref, 2), dtype=np.uint32) for _ in range(4 if flags & UNIQUE else 2)]
+        ptr = [o.ctypes.data for o in outs] + [None] * (4 - len(outs))
+        _check(gpu_lib().kssdgpu_count_block(self._h, qk.ctypes.data if len(qk) else None, qo, nq, flags, *ptr))
+        return tuple(outs)
+
+    def count_lower(self, qkeys: np.ndarray, qoffs: np.ndarray, qry_gid_offset: int, flags: int = 0):
+        nq = len(qoffs) - 1
+        qk = np.ascontiguousarray(qkeys, dtype=np.uint64)
+        qo = np.ascontiguousarray(qoffs, dtype=np.uint64)
+        ctx = np.zeros((nq, self.nref, 2), dtype=np.uint32)
+        obj = np.zeros((nq, self.nref, 2), dtype=np.uint32)
+        _check(gpu_lib().kssdgpu_count_lower(self._h, qk.ctypes.data if len(qk) else None, qo, nq,
+                                             qry_gid_offset, flags, ctx.ctypes.data, obj.ctypes.data))
+        return ctx, obj
+
+    def self_lower(self, flags: int = 0):
+        """Packed lower triangle: arrays [nref*(nref-1)/2, 2] of (num_ctx, mut2) and (diff_obj, section)."""
+        cells = self.nref * (self.nref - 1) // 2
+        ctx = np.zeros((max(cells, 1), 2), dtype=np.uint32)
+        obj = np.zeros((max(cells, 1), 2), dtype=np.uint32)
+        _check(gpu_lib().kssdgpu_self_lower(self._h, flags, ctx.ctypes.data, obj.ctypes.data))
+        return ctx[:cells], obj[:cells]
+
+    # device-pointer forms (torch tensors or raw ints)
+    def count_block_dev(self, d_keys, d_offs, nq, d_ctx, d_obj, d_uctx=None, d_uobj=None, flags=0,
+                        lower=False, qry_gid_offset=0, stream=None):
+        _check(gpu_lib().kssdgpu_count_block_dev(self._h, _ptr(d_keys), _ptr(d_offs), nq, qry_gid_offset,
+                                                 int(lower), flags, _ptr(d_ctx), _ptr(d_obj), _ptr(d_uctx),
+                                                 _ptr(d_uobj), _ptr(stream)))
+
+    def self_lower_dev(self, d_ctx, d_obj, flags=0, stream=None):
+        _check(gpu_lib().kssdgpu_self_lower_dev(self._h, flags, _ptr(d_ctx), _ptr(d_obj), _ptr(stream)))
+
+    def sync(self, stream=None):
+        _check(gpu_lib().kssdgpu_sync(self._h, _ptr(stream)))
+
+
+def _ptr(x):
+    if x is None:
+        return None
+    if isinstance(x, int):
+        return x
+    if hasattr(x, "data_ptr"):
+        return x.data_ptr()
+    if hasattr(x, "cuda_stream"):
+        return x.cuda_stream
+    raise TypeError(type(x))

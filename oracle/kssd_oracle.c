@@ -1,0 +1,306 @@
+/*
+ * ORACLE — test infrastructure only (see kssd_oracle.h).  A CPU restatement of
+ * the reference's shared-context counting, written for clarity: plain binary
+ * search for each query context, then a walk of that context's postings.  The
+ * counting rules follow src/command_ani.h:463-721 exactly; every function cites
+ * the reference lines whose behaviour it restates.
+ */
+#include "kssd_oracle.h"
+
+#include <stdlib.h>
+#include <string.h>
+
+/* NUM_CODENS + 1 with the default NUM_CODENS = 11 (src/command_ani.h:547,684). */
+#define ORC_MIN_INIT 12
+
+typedef struct __attribute__((packed)) {
+    uint64_t ctxgid;
+    uint32_t obj;
+} orc_rec_t;
+
+int orc_dna_popcount(uint32_t x)
+{
+    /* a differing 2-bit base sets at least one of its two bits (src/dna_popcount.h:45-49) */
+    uint32_t any = (x | (x >> 1)) & 0x55555555u;
+    return __builtin_popcount(any);
+}
+
+static int rec_cmp(const void *pa, const void *pb)
+{
+    const orc_rec_t *a = pa, *b = pb;
+    if (a->ctxgid != b->ctxgid)
+        return a->ctxgid < b->ctxgid ? -1 : 1;
+    if (a->obj != b->obj)
+        return a->obj < b->obj ? -1 : 1;
+    return 0;
+}
+
+size_t orc_build_index(const uint64_t *keys, const uint64_t *offs, int nsamples, int obj_bits,
+                       void *out_records)
+{
+    orc_rec_t *r = out_records;
+    const uint64_t objmask = (obj_bits >= 64) ? ~0ull : ((1ull << obj_bits) - 1);
+    const uint64_t gidmask = (1ull << ORC_GID_BITS) - 1;
+    size_t n = 0;
+    for (int g = 0; g < nsamples; g++) {
+        for (uint64_t i = offs[g]; i < offs[g + 1]; i++) {
+            r[n].ctxgid = ((keys[i] >> obj_bits) << ORC_GID_BITS) | ((uint64_t)g & gidmask);
+            r[n].obj = (uint32_t)(keys[i] & objmask);
+            n++;
+        }
+    }
+    qsort(r, n, sizeof(orc_rec_t), rec_cmp);
+    return n;
+}
+
+uint64_t orc_unique_bits(const void *records, size_t len, uint8_t *bits)
+{
+    /* For each ctx group, an obj value that occurs exactly once marks its record. */
+    const orc_rec_t *r = records;
+    uint64_t marked = 0;
+    memset(bits, 0, (len + 7) / 8);
+    size_t i = 0;
+    while (i < len) {
+        const uint64_t ctx = r[i].ctxgid >> ORC_GID_BITS;
+        size_t j = i + 1;
+        while (j < len && (r[j].ctxgid >> ORC_GID_BITS) == ctx)
+            j++;
+        for (size_t a = i; a < j; a++) {
+            int count = 0;
+            for (size_t b = i; b < j; b++)
+                count += r[b].obj == r[a].obj;
+            if (count == 1) {
+                bits[a >> 3] |= (uint8_t)(1u << (a & 7));
+                marked++;
+            }
+        }
+        i = j;
+    }
+    return marked;
+}
+
+void orc_ref_ctx_counts(const void *records, size_t len, int nref, const uint64_t *ref_offs,
+                        int conflict, int ignoreconflict, uint32_t *out)
+{
+    const orc_rec_t *r = records;
+    for (int g = 0; g < nref; g++)
+        out[g] = (uint32_t)(ref_offs[g + 1] - ref_offs[g]);
+    if (!conflict)
+        return;
+    /* A (ctx,gid) run of length L > 1 is one context (L-1 removed), or none with
+     * --ignoreconflict (L removed). */
+    size_t i = 0;
+    while (i < len) {
+        size_t j = i + 1;
+        while (j < len && r[j].ctxgid == r[i].ctxgid)
+            j++;
+        const size_t run = j - i;
+        if (run > 1) {
+            const uint32_t gid = (uint32_t)(r[i].ctxgid & ((1ull << ORC_GID_BITS) - 1));
+            out[gid] -= (uint32_t)(ignoreconflict ? run : run - 1);
+        }
+        i = j;
+    }
+}
+
+void orc_sample_ctx_counts(const uint64_t *keys, const uint64_t *offs, int nsamples, int obj_bits,
+                           int conflict, int ignoreconflict, uint32_t *out)
+{
+    for (int g = 0; g < nsamples; g++) {
+        const uint64_t b = offs[g], e = offs[g + 1];
+        if (!conflict) {
+            out[g] = (uint32_t)(e - b);
+            continue;
+        }
+        uint32_t runs = 0;
+        uint64_t i = b;
+        while (i < e) {
+            const uint64_t ctx = keys[i] >> obj_bits;
+            uint64_t j = i + 1;
+            while (j < e && (keys[j] >> obj_bits) == ctx)
+                j++;
+            if (!ignoreconflict || j - i == 1)
+                runs++;
+            i = j;
+        }
+        out[g] = runs;
+    }
+}
+
+void orc_unique_ref_totals(const void *records, size_t len, int nref, int ignoreconflict,
+                           uint32_t *out)
+{
+    const orc_rec_t *r = records;
+    memset(out, 0, sizeof(uint32_t) * (size_t)nref);
+    size_t i = 0;
+    while (i < len) {
+        const uint64_t ctx = r[i].ctxgid >> ORC_GID_BITS;
+        size_t j = i + 1;
+        int single_owner = 1;
+        while (j < len && (r[j].ctxgid >> ORC_GID_BITS) == ctx) {
+            if (r[j].ctxgid != r[i].ctxgid)
+                single_owner = 0;
+            j++;
+        }
+        const uint32_t gid = (uint32_t)(r[i].ctxgid & ((1ull << ORC_GID_BITS) - 1));
+        if (single_owner && (!ignoreconflict || j - i == 1) && gid < (uint32_t)nref)
+            out[gid]++;
+        i = j;
+    }
+}
+
+/* first record index whose ctx >= target (records sorted by ctxgid) */
+static size_t lower_bound_ctx(const orc_rec_t *r, size_t len, uint64_t target)
+{
+    size_t lo = 0, hi = len;
+    while (lo < hi) {
+        size_t mid = lo + (hi - lo) / 2;
+        if ((r[mid].ctxgid >> ORC_GID_BITS) < target)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+static int min_diff(const uint64_t *q, size_t qn, uint64_t objmask, const orc_rec_t *r,
+                    size_t rb, size_t re)
+{
+    int best = ORC_MIN_INIT;
+    for (size_t a = 0; a < qn; a++)
+        for (size_t b = rb; b < re; b++) {
+            const uint32_t x = (uint32_t)(q[a] & objmask) ^ r[b].obj;
+            const int d = x ? orc_dna_popcount(x) : 0;
+            if (d < best)
+                best = d;
+        }
+    return best;
+}
+
+static inline void add_cell(uint32_t *ctx2, uint32_t *obj2, size_t cell, int d)
+{
+    ctx2[2 * cell] += 1;
+    if (d > 0) {
+        obj2[2 * cell] += 1;
+        obj2[2 * cell + 1] += (uint32_t)d;
+        if (d > 1)
+            ctx2[2 * cell + 1] += 1;
+    }
+}
+
+/* One query sample against the whole index.  lower_gid >= 0 restricts the walk to
+ * gid < lower_gid (the self lower triangle, src/command_ani.h:694-699). */
+static void count_one(const orc_rec_t *r, size_t len, int nref, const uint64_t *a, size_t an,
+                      int obj_bits, int ignoreconflict, int lower_gid, size_t row,
+                      uint32_t *ctx2, uint32_t *obj2, uint32_t *uctx2, uint32_t *uobj2)
+{
+    const uint64_t objmask = (obj_bits >= 64) ? ~0ull : ((1ull << obj_bits) - 1);
+    const uint64_t gidmask = (1ull << ORC_GID_BITS) - 1;
+    size_t j = 0;
+    while (j < an) {
+        const uint64_t ctx = a[j] >> obj_bits;
+        size_t s = 1;
+        while (j + s < an && (a[j + s] >> obj_bits) == ctx)
+            s++;
+        size_t d = lower_bound_ctx(r, len, ctx);
+        size_t owners = 0;
+        uint32_t sole_gid = 0;
+        int sole_diff = 0, sole_allowed = 0;
+        while (d < len && (r[d].ctxgid >> ORC_GID_BITS) == ctx) {
+            const uint64_t cg = r[d].ctxgid;
+            const uint32_t gid = (uint32_t)(cg & gidmask);
+            const size_t rb = d;
+            while (d < len && r[d].ctxgid == cg)
+                d++;
+            const size_t re = d;
+            owners++;
+            sole_gid = gid;
+            if (lower_gid >= 0 && (int)gid >= lower_gid)
+                break;
+            if (ignoreconflict && re - rb > 1)
+                continue;
+            const int md = min_diff(a + j, s, objmask, r, rb, re);
+            add_cell(ctx2, obj2, row * (size_t)nref + gid, md);
+            sole_diff = md;
+            sole_allowed = 1;
+        }
+        if (uctx2 && owners == 1 && sole_allowed)
+            add_cell(uctx2, uobj2, row * (size_t)nref + sole_gid, sole_diff);
+        j += s;
+    }
+}
+
+int orc_count_block(const void *records, size_t len, int nref,
+                    const uint64_t *qkeys, const uint64_t *qoffs, int nq,
+                    int obj_bits, int ignoreconflict, int want_unique, int threads,
+                    uint32_t *ctx2, uint32_t *obj2, uint32_t *uctx2, uint32_t *uobj2)
+{
+    const orc_rec_t *r = records;
+#pragma omp parallel for schedule(dynamic, 1) num_threads(threads > 0 ? threads : 1)
+    for (int q = 0; q < nq; q++) {
+        const uint64_t *a = qkeys + (qoffs[q] - qoffs[0]);
+        const size_t an = (size_t)(qoffs[q + 1] - qoffs[q]);
+        count_one(r, len, nref, a, an, obj_bits, ignoreconflict, -1, (size_t)q, ctx2, obj2,
+                  want_unique ? uctx2 : NULL, want_unique ? uobj2 : NULL);
+    }
+    return 0;
+}
+
+int orc_count_lower(const void *records, size_t len, int nref, int qry_gid_offset,
+                    const uint64_t *qkeys, const uint64_t *qoffs, int nq,
+                    int obj_bits, int ignoreconflict, int threads,
+                    uint32_t *ctx2, uint32_t *obj2)
+{
+    const orc_rec_t *r = records;
+#pragma omp parallel for schedule(dynamic, 1) num_threads(threads > 0 ? threads : 1)
+    for (int q = 0; q < nq; q++) {
+        const uint64_t *a = qkeys + (qoffs[q] - qoffs[0]);
+        const size_t an = (size_t)(qoffs[q + 1] - qoffs[q]);
+        count_one(r, len, nref, a, an, obj_bits, ignoreconflict, qry_gid_offset + q, (size_t)q,
+                  ctx2, obj2, NULL, NULL);
+    }
+    return 0;
+}
+
+void orc_pair_features(const uint64_t *a, size_t n, const uint64_t *b, size_t m, int obj_bits,
+                       int ignore_b_conflict, uint32_t out4[4])
+{
+    const uint64_t objmask = (obj_bits >= 64) ? ~0ull : ((1ull << obj_bits) - 1);
+    memset(out4, 0, 4 * sizeof(uint32_t));
+    size_t i = 0, j = 0;
+    while (i < n && j < m) {
+        const uint64_t ca = a[i] >> obj_bits, cb = b[j] >> obj_bits;
+        size_t ie = i + 1, je = j + 1;
+        while (ie < n && (a[ie] >> obj_bits) == ca)
+            ie++;
+        while (je < m && (b[je] >> obj_bits) == cb)
+            je++;
+        if (ca < cb) {
+            i = ie;
+            continue;
+        }
+        if (cb < ca) {
+            j = je;
+            continue;
+        }
+        if (!(ignore_b_conflict && je - j > 1)) {
+            int best = ORC_MIN_INIT;
+            for (size_t x = i; x < ie; x++)
+                for (size_t y = j; y < je; y++) {
+                    const uint32_t d32 = (uint32_t)(a[x] & objmask) ^ (uint32_t)(b[y] & objmask);
+                    const int d = d32 ? orc_dna_popcount(d32) : 0;
+                    if (d < best)
+                        best = d;
+                }
+            out4[0]++;
+            if (best > 0) {
+                out4[1]++;
+                out4[2] += (uint32_t)best;
+                if (best > 1)
+                    out4[3]++;
+            }
+        }
+        i = ie;
+        j = je;
+    }
+}

@@ -1,0 +1,192 @@
+"""CUDA counting path (through the C ABI) against the oracle, bit for bit."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import kssdgpu
+import oracle
+from fixtures import mutate_from, random_samples, samples_to_sketch
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def _fixture(seed, nref, nq, ctx_space, obj_space, conflict, max_len=40):
+    rng = np.random.default_rng(seed)
+    refs = random_samples(rng, nref, max_len, ctx_space, obj_space, conflict)
+    qrys = random_samples(rng, nq, max_len, ctx_space, obj_space, conflict)
+    for i in range(min(nq, nref)):
+        if refs[i] and rng.random() < 0.5:
+            qrys[i] = mutate_from(rng, refs[i], 0.05)
+    rk, ro = samples_to_sketch(refs)
+    qk, qo = samples_to_sketch(qrys)
+    return rk, ro, qk, qo
+
+
+CASES = [(s, 4, 2, 35, 256, True) for s in range(10)] + \
+        [(s, 40, 12, 300, 1 << 20, True) for s in range(10, 14)] + \
+        [(s, 300, 50, 5000, 1 << 20, False) for s in range(14, 16)]
+
+
+@pytest.mark.parametrize("case", CASES)
+@pytest.mark.parametrize("flags", [0, kssdgpu.IGNORECONFLICT, kssdgpu.PLAIN, kssdgpu.GLOBAL_ACC,
+                                   kssdgpu.PLAIN | kssdgpu.IGNORECONFLICT])
+def test_count_block_unique(case, flags):
+    rk, ro, qk, qo = _fixture(*case)
+    nref = len(ro) - 1
+    rec = oracle.build_index(rk, ro)
+    idx = kssdgpu.Index.from_records(rec, nref)
+    ign = bool(flags & kssdgpu.IGNORECONFLICT)
+    got = idx.count_block(qk, qo, flags | kssdgpu.UNIQUE)
+    want = oracle.count_block(rec, nref, qk, qo, ignoreconflict=ign, unique=True)
+    for g, w in zip(got, want):
+        np.testing.assert_array_equal(g, w)
+    got2 = idx.count_block(qk, qo, flags)
+    np.testing.assert_array_equal(got2[0], want[0])
+    np.testing.assert_array_equal(got2[1], want[1])
+
+
+@pytest.mark.parametrize("case", CASES[::2])
+@pytest.mark.parametrize("flags", [0, kssdgpu.IGNORECONFLICT, kssdgpu.PLAIN, kssdgpu.GLOBAL_ACC])
+def test_count_lower_blocks(case, flags):
+    rk, ro, _, _ = _fixture(*case)
+    nref = len(ro) - 1
+    rec = oracle.build_index(rk, ro)
+    idx = kssdgpu.Index.from_records(rec, nref)
+    ign = bool(flags & kssdgpu.IGNORECONFLICT)
+    for off in range(0, nref, 64):
+        nb = min(64, nref - off)
+        qo = ro[off: off + nb + 1]
+        qk = rk[int(qo[0]): int(qo[-1])]
+        got = idx.count_lower(qk, qo, off, flags)
+        want = oracle.count_lower(rec, nref, off, qk, qo, ignoreconflict=ign)
+        for g, w in zip(got, want):
+            np.testing.assert_array_equal(g, w)
+
+
+@pytest.mark.parametrize("case", CASES[::3])
+@pytest.mark.parametrize("ign", [False, True])
+def test_self_lower_join(case, ign):
+    rk, ro, _, _ = _fixture(*case)
+    rec = oracle.build_index(rk, ro)
+    nref = len(ro) - 1
+    idx = kssdgpu.Index.from_records(rec, nref)
+    got = idx.self_lower(kssdgpu.IGNORECONFLICT if ign else 0)
+    want = oracle.self_lower_all(rec, rk, ro, ignoreconflict=ign)
+    np.testing.assert_array_equal(got[0], want[0])
+    np.testing.assert_array_equal(got[1], want[1])
+
+
+@pytest.mark.parametrize("case", CASES[::4])
+def test_index_from_sketch_and_export(case):
+    rk, ro, _, _ = _fixture(*case)
+    nref = len(ro) - 1
+    rec = oracle.build_index(rk, ro)
+    sk = kssdgpu.Sketch(keys=rk, offs=ro, names=[str(i) for i in range(nref)], conflict=True)
+    idx = kssdgpu.Index.from_sketch(sk)
+    got_rec, got_bits = idx.export()
+    assert got_rec.tobytes() == rec.tobytes()
+    np.testing.assert_array_equal(got_bits, oracle.unique_bits(rec))
+    for ign in (False, True):
+        c, u = idx.ref_ctx_counts(conflict=True, ignoreconflict=ign)
+        np.testing.assert_array_equal(c, oracle.ref_ctx_counts(rec, nref, ro, True, ign))
+        np.testing.assert_array_equal(u, oracle.unique_ref_totals(rec, nref, ign))
+    c, _ = idx.ref_ctx_counts(conflict=False, ignoreconflict=False)
+    np.testing.assert_array_equal(c, np.diff(ro).astype(np.uint32))
+
+
+def test_synthetic_genomes_block_and_self():
+    """Seeded assembly-like genomes (sketch-space generator): block, lower and self join agree."""
+    sk = kssdgpu.synth(n_samples=96, n_clusters=8, len_median=3e5, len_min=1e5, len_max=1e6,
+                       size_dist=kssdgpu.SIZE_LOGNORMAL, sub_lo=0.001, sub_hi=0.1)
+    rec = oracle.build_index(sk.keys, sk.offs)
+    idx = kssdgpu.Index.from_records(rec, sk.n)
+    q = kssdgpu.synth(n_samples=20, n_clusters=8, role=kssdgpu.ROLE_OWNLEN, sample_seed=99,
+                      size_dist=kssdgpu.SIZE_LOGUNIFORM, len_min=5e4, len_max=1e6)
+    got = idx.count_block(q.keys, q.offs, kssdgpu.UNIQUE)
+    want = oracle.count_block(rec, sk.n, q.keys, q.offs, unique=True)
+    for g, w in zip(got, want):
+        np.testing.assert_array_equal(g, w)
+    assert want[0][:, :, 0].sum() > 0
+    got = idx.self_lower()
+    want = oracle.self_lower_all(rec, sk.keys, sk.offs)
+    np.testing.assert_array_equal(got[0], want[0])
+    np.testing.assert_array_equal(got[1], want[1])
+
+
+def test_read_sets_with_conflicts():
+    ref = kssdgpu.synth(n_samples=40, n_clusters=8, len_median=2e5, len_min=1e5, len_max=1e6)
+    reads = kssdgpu.synth(n_samples=6, n_clusters=8, role=kssdgpu.ROLE_READS, sample_seed=5,
+                          ref_sample_seed=20261203, ref_samples=40, len_median=2e5, len_min=1e5, len_max=1e6,
+                          cov_lo=5, cov_hi=20)
+    rec = oracle.build_index(ref.keys, ref.offs)
+    idx = kssdgpu.Index.from_records(rec, ref.n)
+    for flags in (0, kssdgpu.IGNORECONFLICT):
+        got = idx.count_block(reads.keys, reads.offs, flags | kssdgpu.UNIQUE)
+        want = oracle.count_block(rec, ref.n, reads.keys, reads.offs, unique=True,
+                                  ignoreconflict=bool(flags & kssdgpu.IGNORECONFLICT))
+        for g, w in zip(got, want):
+            np.testing.assert_array_equal(g, w)
+
+
+def test_golden_cli_counts_on_gpu():
+    for name in sorted(f for f in os.listdir(GOLDEN) if f.startswith("counts_")):
+        g = json.load(open(os.path.join(GOLDEN, name)))
+        rk, ro = samples_to_sketch([[tuple(p) for p in s] for s in g["refs"]])
+        qk, qo = samples_to_sketch([[tuple(p) for p in s] for s in g["queries"]])
+        rec = oracle.build_index(rk, ro)
+        idx = kssdgpu.Index.from_records(rec, len(ro) - 1)
+        flags = kssdgpu.UNIQUE | (kssdgpu.IGNORECONFLICT if g["ignoreconflict"] else 0)
+        ctx, obj, uctx, uobj = idx.count_block(qk, qo, flags)
+        for row in g["rows"]:
+            q, r = row["q"], row["r"]
+            assert (ctx[q, r, 0], obj[q, r, 0], obj[q, r, 1], ctx[q, r, 1]) == (
+                row["XnY_ctx"], row["N_diff_obj"], row["N_diff_obj_section"], row["N_mut2_ctx"])
+            assert (uctx[q, r, 0], uobj[q, r, 0], uobj[q, r, 1], uctx[q, r, 1]) == (
+                row["Unique_XnY_ctx"], row["Unique_N_diff_obj"], row["Unique_N_diff_obj_section"],
+                row["Unique_N_mut2_ctx"])
+        assert int((ctx[:, :, 0] > 0).sum()) == len(g["rows"])
+
+
+def test_edge_cases():
+    # empty queries, a query with no shared contexts, a reference with no entries
+    refs = [[(1, 0), (2, 3)], [], [(2, 3), (5, 1)]]
+    rk, ro = samples_to_sketch(refs)
+    rec = oracle.build_index(rk, ro)
+    idx = kssdgpu.Index.from_records(rec, 3)
+    qk, qo = samples_to_sketch([[], [(9, 9)], [(2, 0), (2, 3), (5, 2)]])
+    got = idx.count_block(qk, qo, kssdgpu.UNIQUE)
+    want = oracle.count_block(rec, 3, qk, qo, unique=True)
+    for g, w in zip(got, want):
+        np.testing.assert_array_equal(g, w)
+    # zero queries
+    out = idx.count_block(np.zeros(0, np.uint64), np.zeros(1, np.uint64))
+    assert out[0].shape == (0, 3, 2)
+    # gid at the top of the 20-bit range is rejected when nref is too small
+    bad = np.zeros(1, dtype=kssdgpu.REC_DTYPE)
+    bad["ctxgid"] = (5 << 20) | 7
+    with pytest.raises(kssdgpu.KssdGpuError):
+        kssdgpu.Index.from_records(bad, 3)
+    # unsorted records are rejected
+    two = np.zeros(2, dtype=kssdgpu.REC_DTYPE)
+    two["ctxgid"] = [(9 << 20) | 0, (3 << 20) | 0]
+    with pytest.raises(kssdgpu.KssdGpuError):
+        kssdgpu.Index.from_records(two, 1)
+
+
+def test_large_gid_and_max_object_width():
+    """gid near 2^20 (within nref) and 32-bit objects (min-difference cap of 12)."""
+    nref = (1 << 20) - 1
+    rec = np.zeros(3, dtype=kssdgpu.REC_DTYPE)
+    rec["ctxgid"] = [(4 << 20) | 5, (4 << 20) | (nref - 1), (6 << 20) | (nref - 1)]
+    rec["obj"] = [0xFFFFFFFF, 0x0, 0x12345678]
+    idx = kssdgpu.Index.from_records(rec, nref, obj_bits=32)
+    qk = np.array([(4 << 32) | 0x0, (6 << 32) | 0x12345679], dtype=np.uint64)
+    qo = np.array([0, 2], dtype=np.uint64)
+    ctx, obj = idx.count_block(qk, qo, kssdgpu.GLOBAL_ACC)
+    want = oracle.count_block(rec, nref, qk, qo, obj_bits=32)
+    np.testing.assert_array_equal(ctx, want[0])
+    np.testing.assert_array_equal(obj, want[1])
+    assert obj[0, 5, 1] == 12  # 16 differing bases, capped at NUM_CODENS + 1
