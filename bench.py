@@ -1,0 +1,411 @@
+#!/usr/bin/env python
+"""Benchmark: ANI genome-pairs/s of the all-vs-all self ANI matrix on one B200.
+
+Workload (the configuration the headline metric is quoted on): 2,000 synthetic
+genomes, lognormal sizes (median 4 Mbp, sigma 0.37, clipped to 1-12 Mbp), 200
+clusters, ancestor-to-member substitution ~U(0.1%, 20%), sketched at the default
+coden pattern (44-bit context, 20-bit object, ~1 key per 256 bp), generated in
+sketch space by the seeded generator (host/kssd_synth.c).  The path is the
+counting behind `kssd3a ani -q refs --format matrix --values ani` (indexed self
+full matrix): the lower triangle of shared-context counters for every pair;
+genome-pairs = n^2 matrix cells per step.
+
+Arms:
+  ours (default)   value: device-resident step (self join over the resident index,
+                   counters zeroed and rebuilt each step); e2e: the reference-facing
+                   C-ABI call kssdgpu_count_lower with pinned HOST buffers (query keys
+                   H2D, dense counters D2H) every step; plus the plain one-query-per-
+                   launch kernel and the batched persistent probe kernel beside it.
+  reference        the reference's own count_ctx_obj_frm_comb_sketch_section_lower
+                   (compiled from its sources into oracle/_ref) over blocks of 64
+                   queries with all host threads; rank 0 only.
+One JSON line on stdout (rank 0).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "kssd3a-public_b200"))
+
+WORKLOAD = dict(name="self-ani-matrix-2000-genomes", n_samples=2000, n_clusters=200, len_median=4e6,
+                len_sigma=0.37, len_min=1e6, len_max=12e6, sub_lo=0.001, sub_hi=0.2, seed=20261203 + 2)
+BLOCK = 64  # the reference's self-matrix query block (src/command_ani.c:1498-1531)
+
+
+def make_workload(n: int):
+    import kssdgpu
+    w = dict(WORKLOAD)
+    return kssdgpu.synth(n_samples=n, n_clusters=max(1, n // 10), size_dist=kssdgpu.SIZE_LOGNORMAL,
+                         len_median=w["len_median"], len_sigma=w["len_sigma"], len_min=w["len_min"],
+                         len_max=w["len_max"], sub_lo=w["sub_lo"], sub_hi=w["sub_hi"], seed=w["seed"],
+                         sample_seed=w["seed"])
+
+
+def cpu_count_lower_blocks(sk, rec, blocks, threads, use_ref):
+    """Runs count_lower over the given 64-query blocks on the host; returns (seconds, counters)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    n = sk.n
+    outs = []
+    t0 = time.perf_counter()
+    for b in blocks:
+        off = b * BLOCK
+        nb = min(BLOCK, n - off)
+        qo = np.ascontiguousarray(sk.offs[off: off + nb + 1])
+        qk = sk.keys[int(qo[0]): int(qo[-1])]
+        outs.append((off, oracle.count_lower(rec, n, off, qk, qo, threads=threads, ref=use_ref)))
+    return time.perf_counter() - t0, outs
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, device: int):
+        self.device = device
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+
+        def run():
+            while not self._stop.is_set():
+                try:
+                    out = subprocess.run(["nvidia-smi", "-i", str(self.device), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                         timeout=5).stdout.strip()
+                    if out:
+                        self.samples.append([x.strip() for x in out.split(",")])
+                except Exception:
+                    pass
+                self._stop.wait(0.2)
+
+        self._t = threading.Thread(target=run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if len(s) > 3 + i
+                          and s[3 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def measured_peak_hbm():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return 0
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    sk = make_workload(args.genomes)
+    rec = oracle.build_index(sk.keys, sk.offs)
+    use_ref = oracle.ref_available()
+    threads = os.cpu_count() or 1
+    nblocks = (sk.n + BLOCK - 1) // BLOCK
+    # size a step to a bounded sample: time one block (the heaviest, last) first
+    t1, _ = cpu_count_lower_blocks(sk, rec, [nblocks - 1], threads, use_ref)
+    per_step = max(1, min(nblocks, int(args.cpu_step_seconds / max(t1, 1e-3))))
+    order = list(range(nblocks))
+    times, pairs = [], []
+    for s in range(args.warmup + args.steps):
+        blocks = [order[(s * per_step + i) % nblocks] for i in range(per_step)]
+        dt, _ = cpu_count_lower_blocks(sk, rec, blocks, threads, use_ref)
+        if s >= args.warmup:
+            times.append(dt)
+            pairs.append(sum(min(BLOCK, sk.n - b * BLOCK) for b in blocks) * sk.n)
+    value = float(sum(pairs) / sum(times))
+    kind = "reference" if use_ref else "port"
+    line = {
+        "impl": "reference", "metric": "ANI genome-pairs/s", "value": value, "unit": "genome-pairs/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * float(np.mean(times)), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "config": {"workload": WORKLOAD["name"], "genomes": sk.n, "entries": int(sk.offs[-1]),
+                   "path": "count_ctx_obj_frm_comb_sketch_section_lower, 64-query blocks",
+                   "blocks_per_step": per_step},
+        "cpu_baseline": {"value": value, "unit": "genome-pairs/s", "cores": threads, "kind": kind,
+                         "sample": f"{per_step} of {nblocks} 64-query blocks per step, rotating"},
+        "e2e": {"value": value, "unit": "genome-pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import kssdgpu
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    stream = torch.cuda.current_stream()
+
+    sk = make_workload(args.genomes)
+    n = sk.n
+    idx = kssdgpu.Index.from_sketch(sk, device=local_rank)
+    info = idx.info()
+    plan = idx.self_plan_info()
+
+    d_keys = torch.from_numpy(sk.keys.view(np.int64)).to(dev)
+    d_offs = torch.from_numpy(sk.offs.view(np.int64)).to(dev)
+    lower_cells = n * (n - 1) // 2
+    d_lc = torch.zeros(lower_cells, dtype=torch.int64, device=dev)
+    d_lo = torch.zeros(lower_cells, dtype=torch.int64, device=dev)
+    d_c = torch.zeros(n * n, dtype=torch.int64, device=dev)
+    d_o = torch.zeros(n * n, dtype=torch.int64, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
+
+    def self_step(flags=0):
+        idx.self_lower_dev(d_lc, d_lo, flags=flags, stream=stream)
+
+    def probe_step():
+        idx.count_block_dev(d_keys, d_offs, n, d_c, d_o, lower=True, stream=stream)
+
+    def plain_step():
+        idx.count_plain_dev(d_keys, d_offs, sk.offs, d_c, d_o, lower=True, stream=stream)
+
+    # ---- parity on the benchmark's own inputs: self join == batched probe == plain
+    probe_step()
+    idx.sync(stream)
+    tri = torch.tril_indices(n, n, -1, device=dev)
+    dense_c = d_c.view(n, n)[tri[0], tri[1]].clone()
+    dense_o = d_o.view(n, n)[tri[0], tri[1]].clone()
+    self_step()
+    idx.sync(stream)
+    ok_join = bool(torch.equal(dense_c, d_lc) and torch.equal(dense_o, d_lo))
+    plain_step()
+    idx.sync(stream)
+    ok_plain = bool(torch.equal(d_c.view(n, n)[tri[0], tri[1]], dense_c) and
+                    torch.equal(d_o.view(n, n)[tri[0], tri[1]], dense_o))
+    if not (ok_join and ok_plain):
+        raise SystemExit(f"parity failure on the bench workload: join={ok_join} plain={ok_plain}")
+    del tri
+
+    def timed(fn, steps, warmup, flush_l2=True, pre=None):
+        for _ in range(warmup):
+            if pre:
+                pre()
+            fn()
+        torch.cuda.synchronize()
+        tot = 0.0
+        for _ in range(steps):
+            if flush_l2:
+                flush.fill_(1)
+            if pre:
+                pre()
+            s = torch.cuda.Event(enable_timing=True)
+            e = torch.cuda.Event(enable_timing=True)
+            s.record(stream)
+            fn()
+            e.record(stream)
+            e.synchronize()
+            tot += s.elapsed_time(e)
+        idx.sync(stream)
+        return tot / steps  # ms
+
+    # ---- headline: timed region bracketed by barrier + synchronize, max over ranks
+    launches0 = kssdgpu.launch_count()
+    self_step()
+    torch.cuda.synchronize()
+    launches_per_step = kssdgpu.launch_count() - launches0
+    with ClockSampler(local_rank) as clocks:
+        # the steps take milliseconds: keep the GPU on this workload until the sampler
+        # has readings, then run the timed region inside the same sampling window
+        t_end = time.time() + 1.5
+        while time.time() < t_end or len(clocks.samples) < 3:
+            for _ in range(50):
+                self_step()
+            torch.cuda.synchronize()
+            if time.time() > t_end + 10:
+                break
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        ms_step = timed(self_step, args.steps, args.warmup)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+    if dist:
+        t = torch.tensor([ms_step], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_step = float(t.item())
+    launches_timed = launches_per_step * args.steps
+    value = world * n * n / (ms_step / 1e3)
+
+    # ---- dominant kernel alone (join kernels, counters zeroed outside the events)
+    zero = lambda: (d_lc.zero_(), d_lo.zero_())  # noqa: E731
+    ms_join = timed(lambda: self_step(kssdgpu.NO_ZERO), args.steps, 2, pre=zero)
+    peak, peak_kind = measured_peak_hbm()
+    # algorithmic bytes of one join launch: each listed group's (begin,k) word and its
+    # postings read once, each lower-triangle cell's two counters read-modified-written once
+    join_bytes = 8 * plan["groups"] + 8 * plan["postings"] + 2 * 16 * lower_cells
+    achieved = join_bytes / (ms_join / 1e3) / 1e9
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "k_self_join_traffic.json")
+    if os.path.exists(tfile):
+        try:
+            traffic = json.load(open(tfile)).get("bytes_per_launch")
+        except Exception:
+            traffic = None
+
+    # ---- plain one-query-per-launch and batched probe kernels (same counters)
+    ms_probe = timed(probe_step, max(3, args.steps // 2), 2)
+    ms_plain = timed(plain_step, 3, 1)
+    # per-query probe model bytes: 8|q| + 12 * postings walked + 16 per output cell
+    probe_model_bytes = None
+
+    # ---- e2e through the host-buffer C ABI (pinned host inputs and outputs)
+    h_keys = torch.from_numpy(sk.keys.view(np.int64)).pin_memory()
+    h_offs_t = torch.from_numpy(sk.offs.view(np.int64)).pin_memory()
+    h_ctx = torch.empty(n * n * 2, dtype=torch.int32).pin_memory()
+    h_obj = torch.empty(n * n * 2, dtype=torch.int32).pin_memory()
+    lib = kssdgpu.gpu_lib()
+    h_offs_np = h_offs_t.numpy().view(np.uint64)
+
+    def e2e_call():
+        rc = lib.kssdgpu_count_lower(idx.handle, h_keys.data_ptr(), h_offs_np, n, 0, 0, h_ctx.data_ptr(),
+                                     h_obj.data_ptr())
+        if rc:
+            raise kssdgpu.KssdGpuError(rc, lib.kssdgpu_last_error().decode())
+
+    for _ in range(2):
+        e2e_call()
+    e2e_times = []
+    for _ in range(max(3, args.steps // 2)):
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e2e_call()
+        e2e_times.append(time.perf_counter() - t0)
+    e2e_s = float(np.median(e2e_times))
+    if dist:
+        t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = world * n * n / e2e_s
+    h2d = int(sk.keys.nbytes + sk.offs.nbytes + 4 * n)
+    d2h = int(n * n * 16)
+    # the e2e counters equal the device-resident ones
+    e2e_ok = bool(np.array_equal(h_ctx.numpy().view(np.int64), d_c.cpu().numpy()))
+
+    # ---- CPU baseline: the reference's counting function on host cores (rank 0, N=1)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+        # the reference-layout index records (input of the CPU function); byte-identical
+        # to the reference's own `sketch -i` output (tests/test_gpu_count.py)
+        rec, _ = idx.export()
+        use_ref = oracle.ref_available()
+        threads = os.cpu_count() or 1
+        nblocks = (n + BLOCK - 1) // BLOCK
+        t1, _ = cpu_count_lower_blocks(sk, rec, [nblocks - 1], threads, use_ref)
+        per = max(1, min(nblocks, int(args.cpu_seconds / max(t1, 1e-3))))
+        blocks = sorted(set(np.linspace(0, nblocks - 1, per).astype(int).tolist()))
+        dt, outs = cpu_count_lower_blocks(sk, rec, blocks, threads, use_ref)
+        pairs = sum(min(BLOCK, n - b * BLOCK) for b in blocks) * n
+        # parity of the sampled blocks against the device counters
+        dc = d_c.view(n, n).cpu().numpy()
+        same = all(np.array_equal(o[0][:, :, 0].astype(np.int64) | (o[0][:, :, 1].astype(np.int64) << 32),
+                                  dc[off: off + o[0].shape[0]]) for off, o in outs)
+        cpu = {"value": pairs / dt, "unit": "genome-pairs/s", "cores": threads,
+               "kind": "reference" if use_ref else "port",
+               "sample": f"{len(blocks)} of {nblocks} 64-query blocks (count_lower), spread over the matrix",
+               "counts_match_gpu": bool(same)}
+
+    if rank == 0:
+        line = {
+            "metric": "ANI genome-pairs/s", "value": value, "unit": "genome-pairs/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "config": {"workload": WORKLOAD["name"], "genomes": n, "entries": int(sk.offs[-1]),
+                       "unique_contexts": info["contexts"], "matrix_cells": n * n,
+                       "lower_pairs": lower_cells, "path": "self join (kssdgpu_self_lower_dev)",
+                       "l2": "flushed (256 MB write) before every timed step",
+                       "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
+            "e2e": {"value": e2e_value, "unit": "genome-pairs/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "call": "kssdgpu_count_lower (host buffers, pinned)",
+                    "ms_per_step": 1e3 * e2e_s, "counts_match_device": e2e_ok},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                         "kernel": "k_self_small/k_self_big (self join)", "ms_per_launch": ms_join,
+                         "algorithmic_bytes": join_bytes},
+            "kernels": {
+                "batched_probe": {"ms": ms_probe, "value": world * n * n / (ms_probe / 1e3)},
+                "plain_per_query": {"ms": ms_plain, "value": world * n * n / (ms_plain / 1e3), "launches": n},
+                "self_join_vs_plain": ms_plain / ms_step, "batched_probe_vs_plain": ms_plain / ms_probe,
+            },
+            "join_plan": plan,
+            "gpu_launches": int(launches_timed),
+            "clocks": clocks.summary(),
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    idx.close()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--genomes", type=int, default=WORKLOAD["n_samples"])
+    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline sample budget")
+    ap.add_argument("--cpu-step-seconds", type=float, default=8.0, help="reference arm: seconds per step")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local_rank))
+    try:
+        return run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

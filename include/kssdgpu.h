@@ -44,6 +44,7 @@ extern "C" {
 #define KSSDGPU_UNIQUE 0x2u         /* also count reference-unique contexts (--unique-ctx) */
 #define KSSDGPU_PLAIN 0x4u          /* use the plain one-query-per-launch kernel (baseline) */
 #define KSSDGPU_GLOBAL_ACC 0x8u     /* force global-memory accumulators (no shared-memory rows) */
+#define KSSDGPU_NO_ZERO 0x10u       /* device calls: outputs were zeroed by the caller (skip memset) */
 
 /* Counter cells, identical in layout to the reference's ctx_mut2_t / obj_section_t. */
 typedef struct kssdgpu_ctx_mut2 {
@@ -154,6 +155,23 @@ int kssdgpu_self_lower(kssdgpu_index_t *idx, unsigned flags, kssdgpu_ctx_mut2_t 
 /* Device form of kssdgpu_self_lower (outputs in HBM, stream-ordered). */
 int kssdgpu_self_lower_dev(kssdgpu_index_t *idx, unsigned flags, kssdgpu_ctx_mut2_t *d_ctx_lower,
                            kssdgpu_obj_section_t *d_obj_lower, void *stream);
+
+/*
+ * Facts of the self-join plan (built on first use): context groups holding >= 2
+ * postings (listed groups), postings inside them, and the reference-run pairs the
+ * join credits.  These size the join's algorithmic bytes.
+ */
+int kssdgpu_self_plan_info(kssdgpu_index_t *idx, uint64_t *groups, uint64_t *postings, uint64_t *pairs);
+
+/*
+ * Plain baseline kernel with device inputs: one launch per query (h_qry_offs is a
+ * host copy of d_qry_offs, used to size each launch).  Outputs are zeroed unless
+ * KSSDGPU_NO_ZERO.  Same counters as kssdgpu_count_block_dev.
+ */
+int kssdgpu_count_plain_dev(kssdgpu_index_t *idx, const uint64_t *d_qry_keys, const uint64_t *d_qry_offs,
+                            const uint64_t *h_qry_offs, int nq, int qry_gid_offset, int lower, unsigned flags,
+                            kssdgpu_ctx_mut2_t *d_ctx, kssdgpu_obj_section_t *d_obj,
+                            kssdgpu_ctx_mut2_t *d_uctx, kssdgpu_obj_section_t *d_uobj, void *stream);
 
 /* Number of kernels launched by this library so far in this process. */
 uint64_t kssdgpu_launch_count(void);

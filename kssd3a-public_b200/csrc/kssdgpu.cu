@@ -396,95 +396,112 @@ __global__ void __launch_bounds__(256) k_count_plain(CountParams P, int q)
 }
 
 // ------------------------------------------------------------------ self lower triangle (join)
+//
+// In the self case every query sample is also an index sample, so the query run of
+// sample q at context c IS the (c, q) run of c's postings.  count_lower(q) at c
+// therefore credits every ordered pair of runs (r < q) of c's group, and the whole
+// triangle is one pass over the groups that hold at least two postings: no lookups.
 
-// Pairs of a context group whose gid runs are all single objects: k(k-1)/2.
-// Groups holding a multi-object run are handled by k_self_conflict_groups.
-__global__ void k_self_pair_counts(const uint32_t *__restrict__ gbeg, uint64_t u, const uint64_t *__restrict__ post,
-                                   unsigned long long *__restrict__ npairs, uint32_t *__restrict__ conflict_flag)
+// Plan-time classes of a context group.
+enum : uint32_t { kJoinSmallMax = 32 };
+
+// Classify groups with >= 2 postings; append (begin | k << 32) to the small
+// (k <= 32, one gid per posting), big (k > 32) or conflict (a gid holds several
+// objects) list.  Totals: [0] postings in listed groups, [1] pairs.
+__global__ void k_self_classify(const uint32_t *__restrict__ gbeg, uint64_t u, const uint64_t *__restrict__ post,
+                                unsigned long long *__restrict__ small, unsigned long long *__restrict__ big,
+                                unsigned long long *__restrict__ conf, unsigned int *__restrict__ counts,
+                                unsigned long long *__restrict__ totals)
 {
     for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < u; g += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t b = gbeg[g], e = gbeg[g + 1], k = e - b;
+        if (k < 2)
+            continue;
         bool conflict = false;
-        if (k >= 2) {
-            uint32_t prev = (uint32_t)(post[b] >> 32);
-            for (uint32_t i = b + 1; i < e; ++i) {
-                const uint32_t gid = (uint32_t)(post[i] >> 32);
-                conflict |= gid == prev;
-                prev = gid;
-            }
+        uint32_t prev = (uint32_t)(post[b] >> 32);
+        for (uint32_t i = b + 1; i < e; ++i) {
+            const uint32_t gid = (uint32_t)(post[i] >> 32);
+            conflict |= gid == prev;
+            prev = gid;
         }
-        conflict_flag[g] = conflict;
-        npairs[g] = (k >= 2 && !conflict) ? (unsigned long long)k * (k - 1) / 2 : 0ull;
+        const unsigned long long item = (unsigned long long)b | ((unsigned long long)k << 32);
+        if (conflict)
+            conf[atomicAdd(counts + 2, 1u)] = item;
+        else if (k <= kJoinSmallMax)
+            small[atomicAdd(counts + 0, 1u)] = item;
+        else
+            big[atomicAdd(counts + 1, 1u)] = item;
+        atomicAdd(totals + 0, (unsigned long long)k);
+        atomicAdd(totals + 1, (unsigned long long)k * (k - 1) / 2);
     }
+}
+
+__global__ void k_small_keys(const unsigned long long *__restrict__ items, uint32_t n, uint32_t *__restrict__ keys)
+{
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
+        keys[t] = kJoinSmallMax - (uint32_t)(items[t] >> 32);
 }
 
 __device__ __forceinline__ size_t lower_cell(uint32_t row, uint32_t col) { return (size_t)row * (row - 1) / 2 + col; }
 
-// Each thread walks `per_thread` consecutive pairs of the global pair sequence
-// (groups in context order, pairs (i<j) by j then i); cell (gid_j, gid_i).
-__global__ void __launch_bounds__(256) k_self_pairs(const uint32_t *__restrict__ gbeg, uint64_t u,
-                                                    const uint64_t *__restrict__ post,
-                                                    const unsigned long long *__restrict__ incl,  // inclusive scan
-                                                    unsigned long long total, int per_thread,
-                                                    unsigned long long *__restrict__ oc, unsigned long long *__restrict__ oo)
+__device__ __forceinline__ void join_pair(uint64_t pi, uint64_t pj, unsigned long long *__restrict__ oc,
+                                          unsigned long long *__restrict__ oo)
 {
-    const unsigned long long t0 = (blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x) * per_thread;
-    if (t0 >= total)
+    const int d = min(kMinInit, dna_pop((uint32_t)pi ^ (uint32_t)pj));
+    const size_t cell = lower_cell((uint32_t)(pj >> 32), (uint32_t)(pi >> 32));
+    atomicAdd(oc + cell, inc_ctx(d));
+    if (d)
+        atomicAdd(oo + cell, inc_obj(d));
+}
+
+// One thread per small group (list sorted by size so warps stay balanced):
+// every pair i < j of its postings credits cell (gid_j, gid_i).
+__global__ void __launch_bounds__(256) k_self_small(const unsigned long long *__restrict__ list, uint32_t n,
+                                                    const uint64_t *__restrict__ post,
+                                                    unsigned long long *__restrict__ oc,
+                                                    unsigned long long *__restrict__ oo)
+{
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n)
         return;
-    // group containing pair t0: first g with incl[g] > t0
-    uint64_t lo = 0, hi = u;
-    while (lo < hi) {
-        const uint64_t mid = (lo + hi) >> 1;
-        if (incl[mid] > t0)
-            hi = mid;
-        else
-            lo = mid + 1;
+    const unsigned long long item = __ldg(list + t);
+    const uint32_t b = (uint32_t)item, k = (uint32_t)(item >> 32);
+    for (uint32_t j = 1; j < k; ++j) {
+        const uint64_t pj = __ldg(post + b + j);
+        for (uint32_t i = 0; i < j; ++i)
+            join_pair(__ldg(post + b + i), pj, oc, oo);
     }
-    uint64_t g = lo;
-    unsigned long long local = t0 - (g ? incl[g - 1] : 0ull);
-    // decode local -> (j, i), local = j(j-1)/2 + i
-    uint32_t j = (uint32_t)((1.0 + sqrt(1.0 + 8.0 * (double)local)) * 0.5);
-    while ((unsigned long long)j * (j - 1) / 2 > local)
-        --j;
-    while ((unsigned long long)(j + 1) * j / 2 <= local)
-        ++j;
-    uint32_t i = (uint32_t)(local - (unsigned long long)j * (j - 1) / 2);
-    uint32_t b = gbeg[g], k = gbeg[g + 1] - b;
-    const unsigned long long end = min(total, t0 + (unsigned long long)per_thread);
-    for (unsigned long long t = t0; t < end; ++t) {
-        const uint64_t pi = __ldg(post + b + i), pj = __ldg(post + b + j);
-        const int d = min(kMinInit, dna_pop((uint32_t)pi ^ (uint32_t)pj));
-        const size_t cell = lower_cell((uint32_t)(pj >> 32), (uint32_t)(pi >> 32));
-        atomicAdd(oc + cell, inc_ctx(d));
-        if (d)
-            atomicAdd(oo + cell, inc_obj(d));
-        if (++i == j) {
-            i = 0;
-            if (++j == k) {
-                // next group with pairs
-                do {
-                    ++g;
-                } while (g < u && incl[g] == incl[g - 1]);
-                if (g >= u)
-                    break;
-                b = gbeg[g];
-                k = gbeg[g + 1] - b;
-                j = 1;
-            }
-        }
+}
+
+// One warp per big group: lanes stride over its k(k-1)/2 pairs.
+__global__ void __launch_bounds__(256) k_self_big(const unsigned long long *__restrict__ list, uint32_t n,
+                                                  const uint64_t *__restrict__ post,
+                                                  unsigned long long *__restrict__ oc,
+                                                  unsigned long long *__restrict__ oo)
+{
+    const uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (w >= n)
+        return;
+    const unsigned long long item = __ldg(list + w);
+    const uint32_t b = (uint32_t)item, k = (uint32_t)(item >> 32);
+    // lane handles rows j = lane+1, lane+33, ... paired with every i < j; rows are
+    // dealt round-robin so lanes carry near-equal work
+    for (uint32_t j = 1 + lane; j < k; j += 32) {
+        const uint64_t pj = __ldg(post + b + j);
+        for (uint32_t i = 0; i < j; ++i)
+            join_pair(__ldg(post + b + i), pj, oc, oo);
     }
 }
 
 // Groups with multi-object gid runs: one thread per group walks run pairs with the
 // full min-over-cross-product rule; the lower-gid run is the reference side.
-__global__ void k_self_conflict_groups(const uint32_t *__restrict__ gbeg, uint64_t u, const uint64_t *__restrict__ post,
-                                       const uint32_t *__restrict__ conflict_flag, int ignoreconflict,
+__global__ void k_self_conflict_groups(const unsigned long long *__restrict__ list, uint32_t n,
+                                       const uint64_t *__restrict__ post, int ignoreconflict,
                                        unsigned long long *__restrict__ oc, unsigned long long *__restrict__ oo)
 {
-    for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < u; g += (uint64_t)gridDim.x * blockDim.x) {
-        if (!conflict_flag[g])
-            continue;
-        const uint32_t b = gbeg[g], e = gbeg[g + 1];
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        const unsigned long long item = list[t];
+        const uint32_t b = (uint32_t)item, e = b + (uint32_t)(item >> 32);
         // run (query side, higher gid) qb..qe
         for (uint32_t qb = b; qb < e;) {
             const uint32_t qg = (uint32_t)(post[qb] >> 32);
@@ -571,12 +588,11 @@ struct kssdgpu_index {
     DevBuf<uint64_t> s_keys, s_offs;
     DevBuf<unsigned long long> s_out;
     DevBuf<int> s_order;
-    // self-join plan
-    DevBuf<unsigned long long> j_incl;
-    DevBuf<uint32_t> j_conflict;
-    unsigned long long j_total = 0;
+    // self-join plan: group lists (begin | k << 32) by class
+    DevBuf<unsigned long long> j_small, j_big, j_conf;
+    uint32_t j_n[3] = {0, 0, 0};
+    unsigned long long j_postings = 0, j_pairs = 0;
     bool j_ready = false;
-    bool j_any_conflict = false;
 };
 
 namespace {
@@ -740,7 +756,7 @@ int count_dev_impl(kssdgpu_index *ix, const uint64_t *d_keys, const uint64_t *d_
     const size_t smem = (size_t)ix->nref * sizeof(unsigned long long) * (unique ? 4 : 2);
     const bool plain = (flags & KSSDGPU_PLAIN) != 0;
     const bool use_smem = !plain && !(flags & KSSDGPU_GLOBAL_ACC) && smem <= kSmemRowLimit;
-    if (!use_smem) {
+    if (!use_smem && !(flags & KSSDGPU_NO_ZERO)) {
         CUDA_TRY(cudaMemsetAsync(oc, 0, cells * 8, st));
         CUDA_TRY(cudaMemsetAsync(oo, 0, cells * 8, st));
         if (unique) {
@@ -822,42 +838,57 @@ int self_plan(kssdgpu_index *ix, cudaStream_t st)
     if (ix->j_ready)
         return KSSDGPU_OK;
     const uint64_t u = ix->u;
-    CUDA_TRY(ix->j_incl.ensure(u));
-    CUDA_TRY(ix->j_conflict.ensure(u));
-    unsigned long long *np = nullptr;
-    CUDA_TRY(cudaMalloc(&np, std::max<uint64_t>(u, 1) * sizeof(unsigned long long)));
-    k_self_pair_counts<<<grid_for(u), 256, 0, st>>>(ix->gbeg, u, ix->post, np, ix->j_conflict.p);
-    count_launch();
-    size_t tb = 0;
-    CUDA_TRY(cub::DeviceScan::InclusiveSum(nullptr, tb, np, ix->j_incl.p, (int64_t)u, st));
-    void *tmp = nullptr;
-    CUDA_TRY(cudaMalloc(&tmp, std::max<size_t>(tb, 1)));
-    CUDA_TRY(cub::DeviceScan::InclusiveSum(tmp, tb, np, ix->j_incl.p, (int64_t)u, st));
-    count_launch();
-    unsigned long long total = 0;
-    if (u)
-        CUDA_TRY(cudaMemcpyAsync(&total, ix->j_incl.p + u - 1, 8, cudaMemcpyDeviceToHost, st));
-    uint32_t any = 0;
-    {
-        // any conflict group?  reduce with a max
-        uint32_t *d_any = nullptr;
-        CUDA_TRY(cudaMalloc(&d_any, sizeof(uint32_t)));
-        size_t rb = 0;
-        CUDA_TRY(cub::DeviceReduce::Max(nullptr, rb, ix->j_conflict.p, d_any, (int64_t)u, st));
-        void *rt = nullptr;
-        CUDA_TRY(cudaMalloc(&rt, std::max<size_t>(rb, 1)));
-        CUDA_TRY(cub::DeviceReduce::Max(rt, rb, ix->j_conflict.p, d_any, (int64_t)u, st));
+    const uint64_t cap = std::max<uint64_t>(u, 1);
+    CUDA_TRY(ix->j_small.ensure(cap));
+    CUDA_TRY(ix->j_big.ensure(cap));
+    CUDA_TRY(ix->j_conf.ensure(cap));
+    unsigned int *cnt = nullptr;
+    unsigned long long *tot = nullptr;
+    CUDA_TRY(cudaMalloc(&cnt, 3 * sizeof(unsigned int)));
+    CUDA_TRY(cudaMalloc(&tot, 2 * sizeof(unsigned long long)));
+    CUDA_TRY(cudaMemsetAsync(cnt, 0, 3 * sizeof(unsigned int), st));
+    CUDA_TRY(cudaMemsetAsync(tot, 0, 2 * sizeof(unsigned long long), st));
+    if (u) {
+        k_self_classify<<<grid_for(u), 256, 0, st>>>(ix->gbeg, u, ix->post, ix->j_small.p, ix->j_big.p, ix->j_conf.p,
+                                                     cnt, tot);
         count_launch();
-        CUDA_TRY(cudaMemcpyAsync(&any, d_any, 4, cudaMemcpyDeviceToHost, st));
-        CUDA_TRY(cudaStreamSynchronize(st));
-        cudaFree(rt);
-        cudaFree(d_any);
     }
+    unsigned int hc[3];
+    unsigned long long ht[2];
+    CUDA_TRY(cudaMemcpyAsync(hc, cnt, sizeof hc, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaMemcpyAsync(ht, tot, sizeof ht, cudaMemcpyDeviceToHost, st));
     CUDA_TRY(cudaStreamSynchronize(st));
-    cudaFree(tmp);
-    cudaFree(np);
-    ix->j_total = u ? total : 0;
-    ix->j_any_conflict = any != 0;
+    cudaFree(cnt);
+    cudaFree(tot);
+    // small groups sorted by size (descending) so a warp's threads do equal work;
+    // the key is (32 - k) over 6 bits
+    if (hc[0] > 1) {
+        const uint32_t n = hc[0];
+        uint32_t *keys = nullptr, *keys2 = nullptr;
+        unsigned long long *vals2 = nullptr;
+        void *tmp = nullptr;
+        size_t tb = 0;
+        CUDA_TRY(cudaMalloc(&keys, n * 4ull));
+        CUDA_TRY(cudaMalloc(&keys2, n * 4ull));
+        CUDA_TRY(cudaMalloc(&vals2, n * 8ull));
+        k_small_keys<<<grid_for(n), 256, 0, st>>>(ix->j_small.p, n, keys);
+        count_launch();
+        CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, tb, keys, keys2, ix->j_small.p, vals2, n, 0, 6, st));
+        CUDA_TRY(cudaMalloc(&tmp, std::max<size_t>(tb, 1)));
+        CUDA_TRY(cub::DeviceRadixSort::SortPairs(tmp, tb, keys, keys2, ix->j_small.p, vals2, n, 0, 6, st));
+        count_launch();
+        CUDA_TRY(cudaMemcpyAsync(ix->j_small.p, vals2, n * 8ull, cudaMemcpyDeviceToDevice, st));
+        CUDA_TRY(cudaStreamSynchronize(st));
+        cudaFree(keys);
+        cudaFree(keys2);
+        cudaFree(vals2);
+        cudaFree(tmp);
+    }
+    ix->j_n[0] = hc[0];
+    ix->j_n[1] = hc[1];
+    ix->j_n[2] = hc[2];
+    ix->j_postings = ht[0];
+    ix->j_pairs = ht[1];
     ix->j_ready = true;
     return KSSDGPU_OK;
 }
@@ -868,19 +899,22 @@ int self_lower_dev_impl(kssdgpu_index *ix, unsigned flags, unsigned long long *o
     if (rc)
         return rc;
     const size_t cells = (size_t)ix->nref * (ix->nref - 1) / 2;
-    CUDA_TRY(cudaMemsetAsync(oc, 0, std::max<size_t>(cells, 1) * 8, st));
-    CUDA_TRY(cudaMemsetAsync(oo, 0, std::max<size_t>(cells, 1) * 8, st));
-    const int per_thread = 16;
-    if (ix->j_total) {
-        const unsigned long long threads = (ix->j_total + per_thread - 1) / per_thread;
-        const unsigned long long blocks = (threads + 255) / 256;
-        k_self_pairs<<<(unsigned)blocks, 256, 0, st>>>(ix->gbeg, ix->u, ix->post, ix->j_incl.p, ix->j_total, per_thread,
-                                                       oc, oo);
+    if (!(flags & KSSDGPU_NO_ZERO)) {
+        CUDA_TRY(cudaMemsetAsync(oc, 0, std::max<size_t>(cells, 1) * 8, st));
+        CUDA_TRY(cudaMemsetAsync(oo, 0, std::max<size_t>(cells, 1) * 8, st));
+    }
+    if (ix->j_n[0]) {
+        k_self_small<<<(ix->j_n[0] + 255) / 256, 256, 0, st>>>(ix->j_small.p, ix->j_n[0], ix->post, oc, oo);
         count_launch();
     }
-    if (ix->j_any_conflict) {
-        k_self_conflict_groups<<<grid_for(ix->u), 256, 0, st>>>(ix->gbeg, ix->u, ix->post, ix->j_conflict.p,
-                                                                (flags & KSSDGPU_IGNORECONFLICT) ? 1 : 0, oc, oo);
+    if (ix->j_n[1]) {
+        k_self_big<<<(unsigned)(((uint64_t)ix->j_n[1] * 32 + 255) / 256), 256, 0, st>>>(ix->j_big.p, ix->j_n[1], ix->post,
+                                                                                       oc, oo);
+        count_launch();
+    }
+    if (ix->j_n[2]) {
+        k_self_conflict_groups<<<grid_for(ix->j_n[2]), 256, 0, st>>>(ix->j_conf.p, ix->j_n[2], ix->post,
+                                                                     (flags & KSSDGPU_IGNORECONFLICT) ? 1 : 0, oc, oo);
         count_launch();
     }
     CUDA_TRY(cudaGetLastError());
@@ -1031,8 +1065,9 @@ void kssdgpu_index_free(kssdgpu_index_t *ix)
     ix->s_offs.release();
     ix->s_out.release();
     ix->s_order.release();
-    ix->j_incl.release();
-    ix->j_conflict.release();
+    ix->j_small.release();
+    ix->j_big.release();
+    ix->j_conf.release();
     delete ix;
 }
 
@@ -1131,6 +1166,37 @@ int kssdgpu_count_block_dev(kssdgpu_index_t *ix, const uint64_t *d_qry_keys, con
                           reinterpret_cast<unsigned long long *>(d_ctx), reinterpret_cast<unsigned long long *>(d_obj),
                           reinterpret_cast<unsigned long long *>(d_uctx), reinterpret_cast<unsigned long long *>(d_uobj),
                           nullptr, nullptr, (cudaStream_t)stream);
+}
+
+int kssdgpu_count_plain_dev(kssdgpu_index_t *ix, const uint64_t *d_qry_keys, const uint64_t *d_qry_offs,
+                            const uint64_t *h_qry_offs, int nq, int qry_gid_offset, int lower, unsigned flags,
+                            kssdgpu_ctx_mut2_t *d_ctx, kssdgpu_obj_section_t *d_obj, kssdgpu_ctx_mut2_t *d_uctx,
+                            kssdgpu_obj_section_t *d_uobj, void *stream)
+{
+    if (!ix || nq < 0 || (nq && (!d_qry_offs || !h_qry_offs || !d_ctx || !d_obj)))
+        return fail(KSSDGPU_ERR_ARG, "invalid plain count arguments");
+    CUDA_TRY(cudaSetDevice(ix->device));
+    std::vector<uint64_t> sizes(nq);
+    for (int i = 0; i < nq; ++i)
+        sizes[i] = h_qry_offs[i + 1] - h_qry_offs[i];
+    return count_dev_impl(ix, d_qry_keys, d_qry_offs, nq, qry_gid_offset, lower != 0, flags | KSSDGPU_PLAIN,
+                          reinterpret_cast<unsigned long long *>(d_ctx), reinterpret_cast<unsigned long long *>(d_obj),
+                          reinterpret_cast<unsigned long long *>(d_uctx), reinterpret_cast<unsigned long long *>(d_uobj),
+                          nullptr, &sizes, (cudaStream_t)stream);
+}
+
+int kssdgpu_self_plan_info(kssdgpu_index_t *ix, uint64_t *groups, uint64_t *postings, uint64_t *pairs)
+{
+    if (!ix)
+        return fail(KSSDGPU_ERR_ARG, "null index");
+    CUDA_TRY(cudaSetDevice(ix->device));
+    int rc = self_plan(ix, 0);
+    if (rc)
+        return rc;
+    if (groups) *groups = (uint64_t)ix->j_n[0] + ix->j_n[1] + ix->j_n[2];
+    if (postings) *postings = ix->j_postings;
+    if (pairs) *pairs = ix->j_pairs;
+    return KSSDGPU_OK;
 }
 
 int kssdgpu_sync(kssdgpu_index_t *ix, void *stream)

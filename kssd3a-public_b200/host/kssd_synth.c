@@ -107,20 +107,16 @@ static inline uint64_t mutate_obj(const kssd_synth_cfg_t *c, rng_t *r, uint64_t 
     return key;
 }
 
-static double ancestor_len(const kssd_synth_cfg_t *c, int cluster)
-{
-    rng_t ra = stream(c->seed, 0xA11CE, (uint64_t)cluster);
-    return draw_len(c, &ra);
-}
-
-/* ancestor keys of a cluster (unsorted), returns its length */
+/* ancestor keys of a cluster (unsorted), returns its length; the key stream is
+ * independent of the length stream, so ancestors of different lengths share a prefix */
 static double ancestor_keys(const kssd_synth_cfg_t *c, int cluster, vec_t *out)
 {
-    rng_t ra = stream(c->seed, 0xA11CE, (uint64_t)cluster);
-    const double L = draw_len(c, &ra);
+    rng_t rl = stream(c->seed, 0xA11CE, (uint64_t)cluster);
+    rng_t rk = stream(c->seed, 0xA11CF, (uint64_t)cluster);
+    const double L = draw_len(c, &rl);
     const uint64_t m = (uint64_t)llround(L * c->density);
     for (uint64_t i = 0; i < m; i++)
-        vpush(out, fresh_key(c, &ra));
+        vpush(out, fresh_key(c, &rk));
     return L;
 }
 
@@ -181,7 +177,7 @@ static double gen_ownlen(const kssd_synth_cfg_t *c, int idx, vec_t *out)
     const int cluster = idx % c->n_clusters;
     const double La = ancestor_keys(c, cluster, &anc);
     rng_t r = stream(c->sample_seed, 0x0E11, (uint64_t)idx);
-    const double Ls = draw_len(c, &r);
+    const double Ls = exp(log(c->own_len_min) + runif(&r) * (log(c->own_len_max) - log(c->own_len_min)));
     const double p = c->sub_lo + (c->sub_hi - c->sub_lo) * runif(&r);
     derive(c, &r, &anc, Ls < La ? Ls / La : 1.0, p, out);
     if (Ls > La) {
@@ -240,6 +236,8 @@ void kssd_synth_default(kssd_synth_cfg_t *c)
     c->len_sigma = 0.37;
     c->len_min = 1e6;
     c->len_max = 12e6;
+    c->own_len_min = 5e4;
+    c->own_len_max = 12e6;
     c->sub_lo = 0.005;
     c->sub_hi = 0.05;
     c->indel_rate = 0.001;
@@ -258,10 +256,9 @@ void kssd_synth_default(kssd_synth_cfg_t *c)
 
 kssd_synth_out_t *kssd_synth_generate(const kssd_synth_cfg_t *c)
 {
-    if (c->n_samples < 0 || c->n_clusters <= 0 || c->ctx_bits + c->obj_bits > 64 || c->obj_bits > 32 ||
+    if (c->n_samples < 0 || c->n_clusters <= 0 || c->own_len_min <= 0 || c->own_len_max < c->own_len_min || c->ctx_bits + c->obj_bits > 64 || c->obj_bits > 32 ||
         c->ctx_bits <= 0 || c->obj_bits <= 0)
         return NULL;
-    (void)ancestor_len;
     const int n = c->n_samples;
     vec_t *per = calloc((size_t)(n ? n : 1), sizeof(vec_t));
     kssd_synth_out_t *o = calloc(1, sizeof *o);

@@ -6,7 +6,9 @@
  * Model (per sample; every sample is an independent deterministic stream):
  *   - cluster c has an ancestor of length L_c drawn from the size distribution;
  *     its sampled k-mers are round(L_c * density) random (44-bit ctx, 20-bit obj)
- *     keys (density ~ 1/256 at DimRdcFold 8).
+ *     keys (density ~ 1/256 at DimRdcFold 8).  Lengths and keys come from two
+ *     streams of (seed, c) only, so every configuration sharing seed and cluster
+ *     count shares the ancestors (a query set and a reference set, say).
  *   - a member with substitution rate p keeps an ancestor key when none of its
  *     ctx_bits/2 context bases and no indel start in its klen window hit it,
  *     probability (1-p)^(ctx_bits/2) * (1-indel_rate)^klen; kept keys mutate each
@@ -35,8 +37,9 @@ typedef struct kssd_synth_cfg {
     int n_samples;
     int n_clusters;
     int role;               /* KSSD_ROLE_* */
-    int size_dist;          /* KSSD_SIZE_*: ancestor lengths, and own lengths for OWNLEN */
+    int size_dist;          /* KSSD_SIZE_*: ancestor lengths (members inherit them) */
     double len_median, len_sigma, len_min, len_max;
+    double own_len_min, own_len_max; /* KSSD_ROLE_OWNLEN: own length ~ log-uniform */
     double sub_lo, sub_hi;  /* member substitution rate ~ U(lo, hi) */
     double indel_rate;
     double density;         /* sampled keys per bp */

@@ -22,6 +22,7 @@ IGNORECONFLICT = 0x1
 UNIQUE = 0x2
 PLAIN = 0x4
 GLOBAL_ACC = 0x8
+NO_ZERO = 0x10
 
 _u64p = np.ctypeslib.ndpointer(dtype=np.uint64, flags="C_CONTIGUOUS")
 _u32p = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
@@ -67,6 +68,10 @@ def gpu_lib() -> C.CDLL:
         lib.kssdgpu_sync.argtypes = [vp, vp]
         lib.kssdgpu_self_lower.argtypes = [vp, C.c_uint, vp, vp]
         lib.kssdgpu_self_lower_dev.argtypes = [vp, C.c_uint, vp, vp, vp]
+        lib.kssdgpu_self_plan_info.argtypes = [vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
+                                               C.POINTER(C.c_uint64)]
+        lib.kssdgpu_count_plain_dev.argtypes = [vp, vp, vp, _u64p, C.c_int, C.c_int, C.c_int, C.c_uint,
+                                                vp, vp, vp, vp, vp]
         _gpu = lib
     return _gpu
 
@@ -76,7 +81,8 @@ class _SynthCfg(C.Structure):
         ("seed", C.c_uint64), ("sample_seed", C.c_uint64), ("n_samples", C.c_int),
         ("n_clusters", C.c_int), ("role", C.c_int), ("size_dist", C.c_int),
         ("len_median", C.c_double), ("len_sigma", C.c_double), ("len_min", C.c_double),
-        ("len_max", C.c_double), ("sub_lo", C.c_double), ("sub_hi", C.c_double),
+        ("len_max", C.c_double), ("own_len_min", C.c_double), ("own_len_max", C.c_double),
+        ("sub_lo", C.c_double), ("sub_hi", C.c_double),
         ("indel_rate", C.c_double), ("density", C.c_double), ("ctx_bits", C.c_int),
         ("obj_bits", C.c_int), ("klen", C.c_int), ("ref_sample_seed", C.c_uint64),
         ("ref_samples", C.c_int), ("reads_min_genomes", C.c_int), ("reads_max_genomes", C.c_int),
@@ -328,6 +334,18 @@ class Index:
         _check(gpu_lib().kssdgpu_count_block_dev(self._h, _ptr(d_keys), _ptr(d_offs), nq, qry_gid_offset,
                                                  int(lower), flags, _ptr(d_ctx), _ptr(d_obj), _ptr(d_uctx),
                                                  _ptr(d_uobj), _ptr(stream)))
+
+    def count_plain_dev(self, d_keys, d_offs, h_offs, d_ctx, d_obj, d_uctx=None, d_uobj=None, flags=0,
+                        lower=False, qry_gid_offset=0, stream=None):
+        h = np.ascontiguousarray(h_offs, dtype=np.uint64)
+        _check(gpu_lib().kssdgpu_count_plain_dev(self._h, _ptr(d_keys), _ptr(d_offs), h, len(h) - 1,
+                                                 qry_gid_offset, int(lower), flags, _ptr(d_ctx), _ptr(d_obj),
+                                                 _ptr(d_uctx), _ptr(d_uobj), _ptr(stream)))
+
+    def self_plan_info(self):
+        g, p, q = C.c_uint64(), C.c_uint64(), C.c_uint64()
+        _check(gpu_lib().kssdgpu_self_plan_info(self._h, C.byref(g), C.byref(p), C.byref(q)))
+        return dict(groups=g.value, postings=p.value, pairs=q.value)
 
     def self_lower_dev(self, d_ctx, d_obj, flags=0, stream=None):
         _check(gpu_lib().kssdgpu_self_lower_dev(self._h, flags, _ptr(d_ctx), _ptr(d_obj), _ptr(stream)))

@@ -104,7 +104,8 @@ def test_synthetic_genomes_block_and_self():
     rec = oracle.build_index(sk.keys, sk.offs)
     idx = kssdgpu.Index.from_records(rec, sk.n)
     q = kssdgpu.synth(n_samples=20, n_clusters=8, role=kssdgpu.ROLE_OWNLEN, sample_seed=99,
-                      size_dist=kssdgpu.SIZE_LOGUNIFORM, len_min=5e4, len_max=1e6)
+                      len_median=3e5, len_min=1e5, len_max=1e6, size_dist=kssdgpu.SIZE_LOGNORMAL,
+                      own_len_min=5e4, own_len_max=1e6)
     got = idx.count_block(q.keys, q.offs, kssdgpu.UNIQUE)
     want = oracle.count_block(rec, sk.n, q.keys, q.offs, unique=True)
     for g, w in zip(got, want):
