@@ -173,6 +173,37 @@ int kssdgpu_count_plain_dev(kssdgpu_index_t *idx, const uint64_t *d_qry_keys, co
                             kssdgpu_ctx_mut2_t *d_ctx, kssdgpu_obj_section_t *d_obj,
                             kssdgpu_ctx_mut2_t *d_uctx, kssdgpu_obj_section_t *d_uobj, void *stream);
 
+/*
+ * No-allocation form of kssdgpu_count_block_dev (no counterpart in the reference).
+ *
+ * For callers that must not allocate device memory during a count: a serving
+ * loop that reserved all device memory up front for its admission budget, or an
+ * embedding application whose own allocator owns the device and forbids other
+ * allocations.  The call runs the batched persistent counting kernel with its
+ * scratch (work counter, error word, and the largest-first query order it builds
+ * on the device) in a static device array of this library instead of memory from
+ * cudaMalloc; it calls no cudaMalloc, cudaFree or allocating library routine.
+ * The index (built earlier) and all inputs and outputs are the caller's device
+ * buffers, as for kssdgpu_count_block_dev.
+ *
+ * Limits and rules:
+ *   - at most KSSDGPU_NOALLOC_MAX_QUERIES queries per call; more returns
+ *     KSSDGPU_ERR_CAPACITY without launching anything;
+ *   - the array is KSSDGPU_NOALLOC_SCRATCH_BYTES, held by every GPU that loads the
+ *     library until the process exits;
+ *   - the first call on a device looks up the array's device address (set-up);
+ *     make that first call before any stream capture;
+ *   - every call shares the one array (it keeps the last call's contents and is
+ *     cleared where needed on each call), so calls that overlap on the GPU (other
+ *     streams, other threads) race: serialise them.
+ */
+#define KSSDGPU_NOALLOC_MAX_QUERIES 65536
+#define KSSDGPU_NOALLOC_SCRATCH_BYTES (512 + 4 * KSSDGPU_NOALLOC_MAX_QUERIES)
+int kssdgpu_count_block_noalloc(kssdgpu_index_t *idx, const uint64_t *d_qry_keys, const uint64_t *d_qry_offs,
+                                int nq, int qry_gid_offset, int lower, unsigned flags,
+                                kssdgpu_ctx_mut2_t *d_ctx, kssdgpu_obj_section_t *d_obj,
+                                kssdgpu_ctx_mut2_t *d_uctx, kssdgpu_obj_section_t *d_uobj, void *stream);
+
 /* Number of kernels launched by this library so far in this process. */
 uint64_t kssdgpu_launch_count(void);
 

@@ -18,6 +18,7 @@
 #include <atomic>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <numeric>
 #include <string>
 #include <vector>
@@ -923,6 +924,80 @@ int self_lower_dev_impl(kssdgpu_index *ix, unsigned flags, unsigned long long *o
 
 }  // namespace
 
+// ------------------------------------------------------------------ no-allocation counting
+//
+// Scratch of kssdgpu_count_block_noalloc, in the library's own static device
+// memory so that a call needs no cudaMalloc.  Layout (32-bit words):
+//   [0]       work counter of the persistent kernel
+//   [1]       error word
+//   [2, 34)   histogram of query size classes
+//   [34, 66)  scatter cursors of the size classes
+//   [128, ..) query order, largest size class first (KSSDGPU_NOALLOC_MAX_QUERIES ints)
+// The first 128 words are cleared at the start of every call; the order is fully
+// rewritten by every call before it is read.
+static __device__ __align__(256) unsigned int g_noalloc_scratch[KSSDGPU_NOALLOC_SCRATCH_BYTES / 4];
+
+namespace {
+
+constexpr int kNoallocHeaderWords = 128;
+static_assert(KSSDGPU_NOALLOC_SCRATCH_BYTES == 4 * (kNoallocHeaderWords + KSSDGPU_NOALLOC_MAX_QUERIES),
+              "scratch layout and its documented size disagree");
+
+// size class of a query, 0 for the largest: leading zeros of its entry count
+__device__ __forceinline__ uint32_t size_class(const uint64_t *__restrict__ offs, int q)
+{
+    const uint64_t size = offs[q + 1] - offs[q];
+    const uint32_t s = size > 0x7FFFFFFFull ? 0x7FFFFFFFu : (uint32_t)size;
+    return s ? (uint32_t)__clz(s) : 31u;
+}
+
+__global__ void k_noalloc_hist(const uint64_t *__restrict__ offs, int nq, unsigned int *__restrict__ scr)
+{
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += gridDim.x * blockDim.x)
+        atomicAdd(scr + 2 + size_class(offs, q), 1u);
+}
+
+__global__ void k_noalloc_scan(unsigned int *__restrict__ scr)
+{
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        unsigned int run = 0;
+        for (int c = 0; c < 32; ++c) {
+            scr[34 + c] = run;
+            run += scr[2 + c];
+        }
+    }
+}
+
+__global__ void k_noalloc_scatter(const uint64_t *__restrict__ offs, int nq, unsigned int *__restrict__ scr)
+{
+    int *order = reinterpret_cast<int *>(scr + kNoallocHeaderWords);
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += gridDim.x * blockDim.x)
+        order[atomicAdd(scr + 34 + size_class(offs, q), 1u)] = q;
+}
+
+std::mutex g_noalloc_mu;
+unsigned int *g_noalloc_addr[64] = {};
+
+// Device address of the scratch array on the current device (looked up once per device).
+int noalloc_scratch(int device, unsigned int **out)
+{
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (device < 0 || device >= 64)
+        return fail(KSSDGPU_ERR_ARG, "device ordinal out of range for the no-allocation scratch");
+    if (!g_noalloc_addr[device]) {
+        void *p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p)
+            return fail(KSSDGPU_ERR_CUDA, std::string("cudaGetSymbolAddress of the no-allocation scratch: ") +
+                                              cudaGetErrorString(e));
+        g_noalloc_addr[device] = static_cast<unsigned int *>(p);
+    }
+    *out = g_noalloc_addr[device];
+    return KSSDGPU_OK;
+}
+
+}  // namespace
+
 // ------------------------------------------------------------------ C ABI
 
 extern "C" {
@@ -1183,6 +1258,78 @@ int kssdgpu_count_plain_dev(kssdgpu_index_t *ix, const uint64_t *d_qry_keys, con
                           reinterpret_cast<unsigned long long *>(d_ctx), reinterpret_cast<unsigned long long *>(d_obj),
                           reinterpret_cast<unsigned long long *>(d_uctx), reinterpret_cast<unsigned long long *>(d_uobj),
                           nullptr, &sizes, (cudaStream_t)stream);
+}
+
+int kssdgpu_count_block_noalloc(kssdgpu_index_t *ix, const uint64_t *d_qry_keys, const uint64_t *d_qry_offs,
+                                int nq, int qry_gid_offset, int lower, unsigned flags, kssdgpu_ctx_mut2_t *d_ctx,
+                                kssdgpu_obj_section_t *d_obj, kssdgpu_ctx_mut2_t *d_uctx,
+                                kssdgpu_obj_section_t *d_uobj, void *stream)
+{
+    if (!ix || nq < 0 || (nq && (!d_qry_offs || !d_ctx || !d_obj)))
+        return fail(KSSDGPU_ERR_ARG, "invalid no-allocation count arguments");
+    if (nq > KSSDGPU_NOALLOC_MAX_QUERIES)
+        return fail(KSSDGPU_ERR_CAPACITY, "no-allocation count: " + std::to_string(nq) +
+                                              " queries exceed the maximum of " +
+                                              std::to_string(KSSDGPU_NOALLOC_MAX_QUERIES) + " per call");
+    if (flags & KSSDGPU_PLAIN)
+        return fail(KSSDGPU_ERR_ARG, "the no-allocation count runs the batched kernel only");
+    const bool unique = (flags & KSSDGPU_UNIQUE) != 0;
+    if (lower && unique)
+        return fail(KSSDGPU_ERR_ARG, "unique-context counting has no lower-triangle form");
+    if (unique && (!d_uctx || !d_uobj))
+        return fail(KSSDGPU_ERR_ARG, "unique counters requested without output buffers");
+    CUDA_TRY(cudaSetDevice(ix->device));
+    unsigned int *scr = nullptr;
+    int rc = noalloc_scratch(ix->device, &scr);
+    if (rc)
+        return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    CUDA_TRY(cudaMemsetAsync(scr, 0, kNoallocHeaderWords * sizeof(unsigned int), st));
+    if (nq == 0)
+        return KSSDGPU_OK;
+    const int grid = std::min((nq + 255) / 256, ix->sms * 8);
+    k_noalloc_hist<<<grid, 256, 0, st>>>(d_qry_offs, nq, scr);
+    k_noalloc_scan<<<1, 32, 0, st>>>(scr);
+    k_noalloc_scatter<<<grid, 256, 0, st>>>(d_qry_offs, nq, scr);
+    count_launch(3);
+    CountParams P{};
+    P.table = ix->table;
+    P.mask = ix->mask;
+    P.post = ix->post;
+    P.qkeys = d_qry_keys;
+    P.qoffs = d_qry_offs;
+    P.nq = nq;
+    P.nref = ix->nref;
+    P.qgid_offset = qry_gid_offset;
+    P.obj_bits = ix->obj_bits;
+    P.ignoreconflict = (flags & KSSDGPU_IGNORECONFLICT) ? 1 : 0;
+    P.out_ctx = reinterpret_cast<unsigned long long *>(d_ctx);
+    P.out_obj = reinterpret_cast<unsigned long long *>(d_obj);
+    P.out_uctx = reinterpret_cast<unsigned long long *>(d_uctx);
+    P.out_uobj = reinterpret_cast<unsigned long long *>(d_uobj);
+    P.work = scr;
+    P.err = reinterpret_cast<int *>(scr + 1);
+    P.order = reinterpret_cast<const int *>(scr + kNoallocHeaderWords);
+    const size_t cells = (size_t)nq * ix->nref;
+    const size_t smem = (size_t)ix->nref * sizeof(unsigned long long) * (unique ? 4 : 2);
+    const bool use_smem = !(flags & KSSDGPU_GLOBAL_ACC) && smem <= kSmemRowLimit;
+    if (!use_smem && !(flags & KSSDGPU_NO_ZERO)) {
+        CUDA_TRY(cudaMemsetAsync(d_ctx, 0, cells * 8, st));
+        CUDA_TRY(cudaMemsetAsync(d_obj, 0, cells * 8, st));
+        if (unique) {
+            CUDA_TRY(cudaMemsetAsync(d_uctx, 0, cells * 8, st));
+            CUDA_TRY(cudaMemsetAsync(d_uobj, 0, cells * 8, st));
+        }
+    }
+    if (use_smem) {
+        if (lower)
+            return launch_batched<true, false, true>(ix, P, smem, st);
+        return unique ? launch_batched<false, true, true>(ix, P, smem, st)
+                      : launch_batched<false, false, true>(ix, P, smem, st);
+    }
+    if (lower)
+        return launch_batched<true, false, false>(ix, P, 0, st);
+    return unique ? launch_batched<false, true, false>(ix, P, 0, st) : launch_batched<false, false, false>(ix, P, 0, st);
 }
 
 int kssdgpu_self_plan_info(kssdgpu_index_t *ix, uint64_t *groups, uint64_t *postings, uint64_t *pairs)
