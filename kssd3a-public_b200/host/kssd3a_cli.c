@@ -1,0 +1,1352 @@
+/*
+ * kssd3a — drop-in `kssd3a ani` front end over libkssdgpu.
+ *
+ * Options, defaults, validation messages and exit codes follow the reference's
+ * `ani` (src/command_ani_wrapper.c:74-638; usage errors exit 64 through argp);
+ * the path dispatcher follows run_sketch_ani (:1082-1230), and every output path
+ * keeps its reference semantics (which AF precision, which anicut comparison, which
+ * ordering) while all shared-context counting runs on the GPU:
+ *
+ *   mem_eff index path          src/command_ani.c:494-692 (+ counting filters src/command_ani.h:577-621)
+ *   indexed self full/triangle  src/command_ani.c:1657-1842
+ *   direct self / rect matrix   src/command_ani.c:3209-3365
+ *   one-query stream            src/command_ani.c:2110-2201,2490-2666
+ *   multi-query stream          src/command_ani.c:2792-3015
+ *   no-index hash detail        src/command_ani.c:3837-4000
+ *
+ * Inputs are sketch directories; FASTA/FASTQ inputs need a sketcher and are rejected.
+ */
+#define _GNU_SOURCE
+#include <argp.h>
+#include <err.h>
+#include <errno.h>
+#include <fcntl.h>
+#include <limits.h>
+#include <math.h>
+#include <omp.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <sys/stat.h>
+#include <unistd.h>
+
+#include "kssd_epilogue.h"
+#include "kssd_format.h"
+#include "kssdgpu.h"
+
+#define PATHLEN KSSD_PATHLEN
+
+const char *argp_program_version = "kssd3a (B200 counting engine) 3.2.0-rc.1";
+
+typedef struct cli {
+    kssd_ani_opt_t o;
+    char refdir[PATHLEN], qrydir[PATHLEN], outf[PATHLEN], unique_report[PATHLEN];
+    char reflist[PATHLEN], qrylist[PATHLEN], gl[PATHLEN], index[PATHLEN], model[PATHLEN], pipecmd[PATHLEN];
+    double c;
+    bool pair, estimate_coverage, unique_ctx;
+    int output_values, coden_seen, manual_seen;
+    bool sketch_coden;
+    int sketch_hclen, sketch_holen, sketch_iolen, sketch_drfold, sketch_kmerocrs, sketch_ncap;
+    double sketch_npercentile;
+    bool sketch_split_mfa;
+    int nrem;
+    char **rem;
+} cli_t;
+
+static cli_t g;
+
+/* ------------------------------------------------------------------ options */
+
+enum {
+    O_USE_CODEN = 781, O_CTXLEN, O_OUTEROBJLEN, O_INNEROBJLEN, O_DRFOLD, O_LSTKMER, O_NPERCENTILE, O_NCAP,
+    O_READSQC, O_ABUNDANCE, O_ANNO, O_CONFLICT, O_ASONE, O_SPLITMFA, O_PIPECMD, O_RAW_OUTPUT, O_UNIFIED,
+    O_COVERAGE, O_MAX_PDIST, O_MAX_DIFF, O_METRIC, O_FORMAT, O_VALUES, O_UNIQUE_REPORT, O_UNIQUE
+};
+
+static struct argp_option k_opts[] = {
+    {0, 0, 0, 0, "Input sketches:", 1},
+    {"ref", 'r', "<SKETCH>", 0, "Reference sketch directory.", 1},
+    {"query", 'q', "<SKETCH>", 0, "Query sketch directory.", 1},
+    {"qraw", 'x', "<SKETCH>", 0, "Raw-read query sketch directory; enables naive ANI mode.", 1},
+    {"reflist", 779, "<FILE>", 0, "Reference path list for auto ANI (needs a sketcher; not in this build).", 1},
+    {"qrylist", 780, "<FILE>", 0, "Query path list for auto ANI (needs a sketcher; not in this build).", 1},
+    {"index", 'i', "<FILE>", OPTION_HIDDEN, "Reserved; currently unused.", 2},
+    {0, 0, 0, 0, "ANI mode and conflict handling:", 2},
+    {"naive", 'v', 0, 0, "Use naive distance/ANI calculation.", 2},
+    {"ignoreconflict", 778, 0, 0, "Ignore reference-side contexts that contain conflicting objects.", 2},
+    {"unique-ctx", O_UNIQUE, 0, 0, "Adaptive read-to-reference naive ANI on reference-unique contexts "
+                                  "(>= 5% of full reference contexts); indexed -r and --qraw, detail only.", 2},
+    {0, 0, 0, 0, "Filtering and metrics:", 3},
+    {"afcut", 'f', "<0..1>", 0, "Skip reports with max(Qry_align_fraction, Ref_align_fraction) below this fraction. [0.5; 0.2 for --qraw]", 3},
+    {"anicut", 'n', "<0..1>", 0, "Skip reports with ANI below this fraction. [0.95]", 3},
+    {"metric", O_METRIC, "<NAME>", 0, "best, recalibrated, ctx-moe, ctx-naive, p_dist, mash, aaf, mash-if-far, aaf-if-far. [best]", 3},
+    {"control", 'c', "<FLOAT>", 0, "Skip duplicated samples with distance below this value. [0]", 3},
+    {"ctxcut", 't', "<INT>", 0, "Skip reports with overlapped context count below this value. [3]", 3},
+    {"slmetrics", 's', "<+-1..9>", 0, "Metric number 1..9; in matrix mode positive reports distance, negative ANI. [1]", 3},
+    {"max-pdist", O_MAX_PDIST, "<FLOAT>", 0, "Close-only detail filter on p_dist. [off]", 3},
+    {"max-diff-section", O_MAX_DIFF, "<INT>", 0, "Close-only detail filter on object-section differences. [off]", 3},
+    {"unified-metric", O_UNIFIED, 0, 0, "In --qraw mode honor -s instead of forcing Naive.", 3},
+    {0, 0, 0, 0, "Reporting and output:", 4},
+    {"diagonal", 'd', 0, 0, "Set diagonal values.", 4},
+    {"exception", 'e', "<INT>", 0, "Missing/low-overlap matrix distance [1]; ANI uses 1-e.", 4},
+    {"glist", 'g', "<FILE>", 0, "Sample output file for KSSD set grouping.", 4},
+    {"outfmt", 'm', "<0/1/2>", 0, "Output format: detail(0), matrix(1), or triangle(2). [0]", 4},
+    {"format", O_FORMAT, "<NAME>", 0, "detail, matrix, or triangle; alias for -m. [detail]", 4},
+    {"values", O_VALUES, "<distance|ani>", 0, "Matrix/triangle values; overrides the sign of -s. [distance]", 4},
+    {"outfile", 'o', "<FILE>", 0, "Output file. [STDOUT]", 4},
+    {"raw-output", O_RAW_OUTPUT, 0, 0, "Skip calibrated/best ANI computation.", 4},
+    {"estimate-coverage", O_COVERAGE, 0, 0, "Coverage columns for --qraw detail (not in this build).", 4},
+    {"unique-ctx-report", O_UNIQUE_REPORT, "<FILE>", 0, "Write unfiltered unique-context counts to a new file.", 4},
+    {"top", 'N', "<INT>", 0, "Report at most top N references per query. [all]", 4},
+    {0, 0, 0, 0, "Execution:", 5},
+    {"threads", 'p', "<INT>", 0, "Number of host threads for the epilogue.", 5},
+    {0, 0, 0, 0, "Direct FASTA/FASTQ input mode (needs a sketcher; not in this build):", 6},
+    {"pair", 777, 0, 0, "Treat positional inputs as reference then query inputs.", 6},
+    {"pipecmd", O_PIPECMD, "<cmd>", 0, "Stream each raw input through command.", 6},
+    {"use_coden_ctxobj", O_USE_CODEN, 0, 0, "Use the coden context-object pattern. [default]", 7},
+    {"DimRdcFold", O_DRFOLD, "<INT>", 0, "K-mer space downsampling rate 1/2^f. [8]", 7},
+    {"ctxlen", O_CTXLEN, "<INT>", 0, "Manual half context length.", 7},
+    {"outerobjlen", O_OUTEROBJLEN, "<INT>", 0, "Manual half outer object length.", 7},
+    {"innerobjlen", O_INNEROBJLEN, "<INT>", 0, "Manual inner object length.", 7},
+    {"LstKmerOcrs", O_LSTKMER, "<INT>", 0, "Least k-mer occurrence required in FASTQ input. [1]", 7},
+    {"npercentile", O_NPERCENTILE, "<0..1>", 0, "Weighted lower-tail count percentile.", 7},
+    {"ncap", O_NCAP, "<INT>", OPTION_HIDDEN, "Cap for effective lower k-mer occurrence cutoff. [0]", 7},
+    {"readsQC", O_READSQC, 0, 0, "Infer and apply read-count QC filtering.", 7},
+    {"abundance", O_ABUNDANCE, 0, 0, "Use abundance-estimation mode.", 7},
+    {"anno", O_ANNO, 0, 0, "Write FASTA/FASTQ header annotations.", 7},
+    {"conflict", O_CONFLICT, 0, 0, "Keep conflicting context-objects.", 7},
+    {"asone", O_ASONE, 0, 0, "Treat each raw input path as one final genome.", 7},
+    {"splitmfa", O_SPLITMFA, 0, 0, "Treat each multi-FASTA record as one genome.", 7},
+    {0}};
+
+static int parse_int_range(struct argp_state *st, const char *name, const char *arg, int lo, int hi)
+{
+    char *end = NULL;
+    errno = 0;
+    long v = strtol(arg, &end, 10);
+    if (errno || end == arg || *end || v < lo || v > hi)
+        argp_error(st, "%s requires an integer in range %d..%d", name, lo, hi);
+    return (int)v;
+}
+
+static double parse_double_range(struct argp_state *st, const char *name, const char *arg, double lo, double hi)
+{
+    char *end = NULL;
+    errno = 0;
+    double v = strtod(arg, &end);
+    if (errno || end == arg || *end || !isfinite(v) || v < lo || v > hi)
+        argp_error(st, "%s requires a number in range %.6g..%.6g", name, lo, hi);
+    return v;
+}
+
+static void copy_path(struct argp_state *st, const char *name, char *dst, const char *arg)
+{
+    if (strlen(arg) >= PATHLEN)
+        argp_error(st, "%s path is too long; maximum supported length is %d bytes", name, PATHLEN - 1);
+    snprintf(dst, PATHLEN, "%s", arg);
+}
+
+static error_t parse_ani(int key, char *arg, struct argp_state *st)
+{
+    kssd_ani_opt_t *o = &g.o;
+    switch (key) {
+    case O_UNIQUE: g.unique_ctx = o->unique_ctx = true; break;
+    case O_UNIQUE_REPORT: copy_path(st, "--unique-ctx-report", g.unique_report, arg); break;
+    case O_METRIC: {
+        static const char *names[] = {"best", "recalibrated", "ctx-moe", "ctx-naive", "mash", "aaf",
+                                      "mash-if-far", "aaf-if-far", "p_dist"};
+        int m = 0;
+        for (int i = 0; i < 9; ++i)
+            if (!strcmp(arg, names[i]))
+                m = i + 1;
+        if (!strcmp(arg, "naive")) m = 4;
+        if (!strcmp(arg, "pdist")) m = 9;
+        if (!m)
+            argp_error(st, "unknown --metric '%s'; use best, recalibrated, ctx-moe, ctx-naive, p_dist, mash, aaf, "
+                           "mash-if-far, or aaf-if-far", arg);
+        o->s = o->s < 0 ? -m : m;
+        break;
+    }
+    case O_FORMAT:
+        if (!strcmp(arg, "detail")) o->fmt = 0;
+        else if (!strcmp(arg, "matrix")) o->fmt = 1;
+        else if (!strcmp(arg, "triangle")) o->fmt = 2;
+        else argp_error(st, "--format must be detail, matrix, or triangle");
+        break;
+    case O_VALUES:
+        if (!strcmp(arg, "distance")) g.output_values = 1;
+        else if (!strcmp(arg, "ani")) g.output_values = -1;
+        else argp_error(st, "--values must be distance or ani");
+        break;
+    case 'm': o->fmt = parse_int_range(st, "-m/--outfmt", arg, 0, 2); break;
+    case 'c': {
+        char *end = NULL;
+        errno = 0;
+        double v = strtod(arg, &end);
+        if (errno || end == arg || *end || !isfinite(v) || v < 0.0)
+            argp_error(st, "%s requires a non-negative number", "-c/--control");
+        g.c = v;
+        break;
+    }
+    case 'e': o->e = parse_int_range(st, "-e/--exception", arg, 1, INT_MAX); break;
+    case 's':
+        o->s = parse_int_range(st, "-s/--slmetrics", arg, -9, 9);
+        if (o->s == 0)
+            argp_error(st, "-s/--slmetrics accepts -9..-1 or 1..9, but not 0");
+        break;
+    case 'p': o->p = parse_int_range(st, "-p/--threads", arg, 1, 65536); break;
+    case O_USE_CODEN: g.coden_seen = 1; g.sketch_coden = true; break;
+    case O_CTXLEN: g.manual_seen = 1; g.sketch_coden = false; g.sketch_hclen = parse_int_range(st, "--ctxlen", arg, 4, 16); break;
+    case O_OUTEROBJLEN: g.manual_seen = 1; g.sketch_coden = false; g.sketch_holen = parse_int_range(st, "--outerobjlen", arg, 0, 8); break;
+    case O_INNEROBJLEN: g.manual_seen = 1; g.sketch_coden = false; g.sketch_iolen = parse_int_range(st, "--innerobjlen", arg, 0, 8); break;
+    case O_DRFOLD: g.sketch_drfold = parse_int_range(st, "--DimRdcFold", arg, 0, 24); break;
+    case O_LSTKMER: g.sketch_kmerocrs = parse_int_range(st, "--LstKmerOcrs", arg, 1, 65536); break;
+    case O_NPERCENTILE: g.sketch_npercentile = parse_double_range(st, "--npercentile", arg, 0.0, 1.0); break;
+    case O_NCAP: g.sketch_ncap = parse_int_range(st, "--ncap", arg, 0, 65536); break;
+    case O_READSQC: if (g.sketch_kmerocrs < 2) g.sketch_kmerocrs = 2; break;
+    case O_ABUNDANCE: case O_ANNO: case O_CONFLICT: case O_ASONE: break;
+    case O_SPLITMFA: g.sketch_split_mfa = true; break;
+    case O_PIPECMD: copy_path(st, "--pipecmd", g.pipecmd, arg); break;
+    case O_RAW_OUTPUT: o->raw_output = true; break;
+    case O_UNIFIED: o->unified_metric = true; break;
+    case O_COVERAGE: g.estimate_coverage = true; break;
+    case O_MAX_PDIST: o->max_pdist = parse_double_range(st, "--max-pdist", arg, 0.0, 1.0); o->max_pdist_set = true; break;
+    case O_MAX_DIFF: o->max_diff_obj_section = parse_int_range(st, "--max-diff-section", arg, 0, INT_MAX); break;
+    case 't': o->ctxcut = parse_int_range(st, "-t/--ctxcut", arg, 0, INT_MAX); break;
+    case 'f':
+        o->afcut = (float)parse_double_range(st, "-f/--afcut (fraction, e.g. 0.8, not 80)", arg, 0.0, 1.0);
+        o->afcut_set = true;
+        break;
+    case 'n': o->anicut = (float)parse_double_range(st, "-n/--anicut (fraction, e.g. 0.95, not 95)", arg, 0.0, 1.0); break;
+    case 'N': o->ntop = parse_int_range(st, "-N/--top", arg, 1, INT_MAX); break;
+    case 'i': copy_path(st, "-i/--index", g.index, arg); break;
+    case 'M': copy_path(st, "-M/--model", g.model, arg); break;
+    case 'q': copy_path(st, "-q/--query", g.qrydir, arg); break;
+    case 780: copy_path(st, "--qrylist", g.qrylist, arg); break;
+    case 'r': copy_path(st, "-r/--ref", g.refdir, arg); break;
+    case 779: copy_path(st, "--reflist", g.reflist, arg); break;
+    case 'o': copy_path(st, "-o/--outfile", g.outf, arg); break;
+    case 'g': copy_path(st, "-g/--glist", g.gl, arg); break;
+    case 'd': o->d = true; break;
+    case 'v': o->v = true; break;
+    case 778: o->ignoreconflict = true; break;
+    case 'x':
+        copy_path(st, "--qraw", g.qrydir, arg);
+        o->unassembled = true;
+        o->v = true;
+        break;
+    case 777: g.pair = true; break;
+    case ARGP_KEY_ARGS:
+        g.nrem = st->argc - st->next;
+        g.rem = st->argv + st->next;
+        break;
+    case ARGP_KEY_END: {
+        /* validation, src/command_ani_wrapper.c:536-621 */
+        if (g.output_values)
+            o->s = abs(o->s) * g.output_values;
+        const bool has_reflist = g.reflist[0], has_qrylist = g.qrylist[0];
+        if (g.unique_ctx || g.unique_report[0]) {
+            if (!o->unassembled || o->fmt != 0 || !g.refdir[0] || !g.qrydir[0] || has_reflist || has_qrylist || g.nrem)
+                argp_error(st, "unique-context options require explicit -r/--qraw inputs and detail output");
+            if (g.unique_ctx && (o->unified_metric || o->raw_output || abs(o->s) > 4 || o->max_pdist_set ||
+                                 o->max_diff_obj_section >= 0))
+                argp_error(st, "--unique-ctx uses calibrated read-mode Naive ANI; incompatible metric, raw-output, "
+                               "unified-metric or close-pair filter");
+            if (g.unique_report[0] && !strcmp(g.unique_report, g.outf))
+                argp_error(st, "--unique-ctx-report must differ from the ordinary output path");
+        }
+        if (g.coden_seen && g.manual_seen)
+            argp_error(st, "--use_coden_ctxobj selects the coden pattern; do not combine it with --ctxlen, "
+                           "--outerobjlen, or --innerobjlen.");
+        if (!g.sketch_coden) {
+            int k = g.sketch_iolen + 2 * (g.sketch_holen + g.sketch_hclen);
+            if (k > 32)
+                argp_error(st, "auto-sketch k-mer length %d should be at most 32", k);
+        }
+        if (g.pipecmd[0] && g.sketch_split_mfa)
+            argp_error(st, "--splitmfa does not support --pipecmd streaming inputs");
+        if (g.estimate_coverage && o->fmt != 0)
+            argp_error(st, "--estimate-coverage is supported only with detail output (-m0).");
+        if (g.estimate_coverage && !o->unassembled)
+            argp_error(st, "--estimate-coverage currently requires --qraw raw/unassembled query mode.");
+        if ((o->max_pdist_set || o->max_diff_obj_section >= 0) && o->fmt != 0)
+            argp_error(st, "--max-pdist/--max-diff-section are supported only with detail output (-m0).");
+        if (has_reflist || has_qrylist) {
+            if (!has_reflist || !has_qrylist)
+                argp_error(st, "--reflist and --qrylist must be used together");
+            if (g.refdir[0] || g.qrydir[0])
+                argp_error(st, "--reflist/--qrylist cannot be combined with -r, -q, or --qraw");
+            if (g.pair || g.nrem > 0)
+                argp_error(st, "--reflist/--qrylist cannot be combined with --pair or positional inputs");
+        } else if (g.pair) {
+            if (g.refdir[0] || g.qrydir[0])
+                argp_error(st, "--pair cannot be combined with -r, -q, or --qraw");
+            if (g.nrem < 2)
+                argp_error(st, "--pair requires one reference input followed by at least one query input");
+        } else if (!g.refdir[0] && !g.qrydir[0] && g.nrem >= 2) {
+            g.pair = true;
+        } else if (!g.refdir[0] && !g.qrydir[0] && g.nrem == 1 && o->fmt != 0) {
+            copy_path(st, "sketch", g.qrydir, g.rem[0]);
+        } else if (!g.qrydir[0]) {
+            argp_error(st, "missing query: use -q, --qraw, or positional reference and query inputs");
+        } else if (!g.refdir[0] && o->fmt == 0) {
+            argp_error(st, "-r/--ref is required for detail output; use -m1 or -m2 for one-sketch self matrices");
+        }
+        if (o->s < -9 || o->s > 9 || o->s == 0)
+            argp_error(st, "-s option should be within range 1..9 or -9..-1");
+        break;
+    }
+    default:
+        return ARGP_ERR_UNKNOWN;
+    }
+    return 0;
+}
+
+static struct argp k_argp = {
+    k_opts, parse_ani,
+    "[-r REF_SKETCH -q QRY | -r REF_SKETCH --qraw RAW_QRY | SELF_SKETCH with -m1/-m2]",
+    "\nEstimate average nucleotide identity (ANI) between sketches; shared-context counting on the GPU."
+    "\vOutputs are byte-identical to the reference `kssd3a ani` on the same sketch directories."};
+
+/* ------------------------------------------------------------------ helpers */
+
+static int env_int(const char *name, int dflt, int lo, const char *what)
+{
+    const char *e = getenv(name);
+    if (!e || !e[0])
+        return dflt;
+    char *end = NULL;
+    errno = 0;
+    long v = strtol(e, &end, 10);
+    if (errno || end == e || *end || v < lo || v > INT_MAX)
+        errx(EXIT_FAILURE, "invalid %s='%s' (use %s)", name, e, what);
+    return (int)v;
+}
+
+static bool force_ref_index(void)
+{
+    const char *e = getenv("KSSD3A_FORCE_REF_INDEX");
+    return e && e[0] && strcmp(e, "0") != 0;
+}
+
+static int matrix_direct_threshold(void)
+{
+    const char *name = "KSSD3A_ANI_MATRIX_DIRECT_THRESHOLD";
+    const char *e = getenv(name);
+    if (!e || !e[0]) {
+        name = "KSSD3A_ANI_M1_DIRECT_THRESHOLD";
+        e = getenv(name);
+    }
+    if (!e || !e[0])
+        return 1000;
+    char *end = NULL;
+    errno = 0;
+    long v = strtol(e, &end, 10);
+    if (errno || end == e || *end || v < 0 || v > INT_MAX)
+        errx(EXIT_FAILURE, "invalid %s='%s' (use non-negative integer)", name, e);
+    return (int)v;
+}
+
+static bool matrix_use_index(int nref, int nq, int direct)
+{
+    if (nref < 1 || nq < 1)
+        return false;
+    if (direct == 0)
+        return true;
+    return nref > direct || nq > direct;
+}
+
+static bool same_file(const char *a, const char *b)
+{
+    struct stat sa, sb;
+    return a && b && !stat(a, &sa) && !stat(b, &sb) && sa.st_dev == sb.st_dev && sa.st_ino == sb.st_ino;
+}
+
+static bool is_sketch_dir(const char *p)
+{
+    struct stat st;
+    if (stat(p, &st) || !S_ISDIR(st.st_mode))
+        return false;
+    return kssd_file_exists(p, "lcofiles.stat") && kssd_file_exists(p, "comblco") && kssd_file_exists(p, "comblco.index");
+}
+
+static kssd_sketch_t *load_sketch(const char *dir, unsigned flags)
+{
+    kssd_sketch_t *s = kssd_sketch_load(dir, flags);
+    if (!s)
+        errx(EXIT_FAILURE, "%s", kssd_host_last_error());
+    return s;
+}
+
+static void gpu_check(int rc, const char *what)
+{
+    if (rc != KSSDGPU_OK)
+        errx(EXIT_FAILURE, "%s: %s", what, kssdgpu_last_error());
+}
+
+static FILE *open_out(const char *path)
+{
+    FILE *f = path[0] ? fopen(path, "w") : stdout;
+    if (!f)
+        err(errno, "%s", path);
+    return f;
+}
+
+static void close_out(FILE *f)
+{
+    if (fflush(f) != 0 || ferror(f))
+        err(EXIT_FAILURE, "Cannot write ANI output");
+    if (f != stdout && fclose(f) != 0)
+        err(EXIT_FAILURE, "Cannot finish ANI output");
+}
+
+static void write_buf(FILE *f, const kssd_buf_t *b)
+{
+    if (b->l && fwrite(b->s, 1, b->l, f) != b->l)
+        err(EXIT_FAILURE, "Cannot write ANI output");
+}
+
+/* context runs of one sorted sample (count_ctx_runs_sorted_ctxobj64_local, src/command_ani.c:337-349) */
+static uint32_t ctx_runs(const uint64_t *a, size_t n, int obj_bits, bool ignoreconflict)
+{
+    uint32_t runs = 0;
+    for (size_t i = 0; i < n;) {
+        const uint64_t ctx = a[i] >> obj_bits;
+        const size_t b = i;
+        do {
+            ++i;
+        } while (i < n && (a[i] >> obj_bits) == ctx);
+        if (!ignoreconflict || i - b == 1)
+            runs++;
+    }
+    return runs;
+}
+
+static uint32_t *sample_ctx_counts(const kssd_sketch_t *s, bool use_runs, bool ignoreconflict)
+{
+    uint32_t *c = calloc((size_t)(s->n ? s->n : 1), sizeof(uint32_t));
+    if (!c)
+        err(EXIT_FAILURE, "calloc ctx counts");
+#pragma omp parallel for schedule(dynamic, 64) num_threads(g.o.p)
+    for (int i = 0; i < s->n; ++i) {
+        const size_t len = (size_t)(s->offs[i + 1] - s->offs[i]);
+        c[i] = use_runs ? ctx_runs(s->keys + s->offs[i] - s->offs[0], len, s->obj_bits, ignoreconflict) : (uint32_t)len;
+    }
+    return c;
+}
+
+static const char *anno_at(const kssd_sketch_t *s, uint32_t i)
+{
+    return s && s->anno && s->anno[i][0] ? s->anno[i] : "NA";
+}
+
+static bool best_guard_enabled(void) { return g.o.fmt == 0 && !g.o.unassembled && !g.o.v; }
+
+static unsigned ref_flags(void) { return (g.o.fmt == 0 ? 1u : 0u) | (best_guard_enabled() ? 2u : 0u); }
+static unsigned qry_flags(void) { return best_guard_enabled() ? 2u : 0u; }
+
+static void init_bits(const kssd_sketch_t *q)
+{
+    g.o.drfold = q->stat.drfold;
+    g.o.obj_bits = q->obj_bits;
+    g.o.ctx_bits = q->ctx_bits;
+}
+
+static kssdgpu_index_t *gpu_index_of_sketch(const kssd_sketch_t *s)
+{
+    kssdgpu_index_t *ix = NULL;
+    gpu_check(kssdgpu_index_from_sketch(s->keys, s->offs, s->n, s->obj_bits, 0, &ix), "device index");
+    return ix;
+}
+
+/* Counters of queries [q0, q0+nb) against the index: [nb][R] cells each. */
+typedef struct counts {
+    kssdgpu_ctx_mut2_t *ctx, *uctx;
+    kssdgpu_obj_section_t *obj, *uobj;
+} counts_t;
+
+static counts_t count_queries(kssdgpu_index_t *ix, int nref, const kssd_sketch_t *q, int q0, int nb, unsigned flags)
+{
+    counts_t c = {0};
+    const size_t cells = (size_t)nb * (size_t)nref;
+    c.ctx = malloc(cells * sizeof(*c.ctx) + 1);
+    c.obj = malloc(cells * sizeof(*c.obj) + 1);
+    if (flags & KSSDGPU_UNIQUE) {
+        c.uctx = malloc(cells * sizeof(*c.uctx) + 1);
+        c.uobj = malloc(cells * sizeof(*c.uobj) + 1);
+    }
+    if (!c.ctx || !c.obj || ((flags & KSSDGPU_UNIQUE) && (!c.uctx || !c.uobj)))
+        err(EXIT_FAILURE, "OOM counter block");
+    const uint64_t *keys = q->keys + (q->offs[q0] - q->offs[0]);
+    gpu_check(kssdgpu_count_block(ix, keys, q->offs + q0, nb, flags, c.ctx, c.obj, c.uctx, c.uobj), "device counting");
+    return c;
+}
+
+static void free_counts(counts_t *c)
+{
+    free(c->ctx);
+    free(c->obj);
+    free(c->uctx);
+    free(c->uobj);
+}
+
+static kssd_features_t feat_of(const kssdgpu_ctx_mut2_t *c, const kssdgpu_obj_section_t *o)
+{
+    kssd_features_t f = {0};
+    f.XnY_ctx = c->num_ctx;
+    f.N_mut2_ctx = c->num_mut2_ctx;
+    f.N_diff_obj = o->diff_obj;
+    f.N_diff_obj_section = o->diff_obj_section;
+    return f;
+}
+
+static double naive_of(const kssdgpu_ctx_mut2_t *c, const kssdgpu_obj_section_t *o)
+{
+    kssd_features_t f = feat_of(c, o);
+    return kssd_naive_dist(&f);
+}
+
+/* query blocks sized so that four counter blocks stay within ~2 GB of host memory */
+static int block_for(int nref, int nq)
+{
+    size_t per = (size_t)nref * 32;
+    size_t b = per ? (2ull << 30) / per : (size_t)nq;
+    if (b < 1)
+        b = 1;
+    if (b > 8192)
+        b = 8192;
+    return (int)(b < (size_t)nq ? b : (size_t)(nq ? nq : 1));
+}
+
+/* ------------------------------------------------------------------ ranking (detail pre-filter) */
+
+typedef struct {
+    uint32_t id;
+    float ani;
+} idani_t;
+
+static int cmp_idani_desc(const void *a, const void *b)
+{
+    const idani_t *x = a, *y = b;
+    return (x->ani < y->ani) - (x->ani > y->ani);
+}
+
+/* The reference keeps the top N by a partial min-heap before a final sort when N is
+ * well below the candidate count (src/command_ani.h:368-433); ties between equal
+ * ANIs are resolved by that exact sequence of swaps and sorts, so it is kept. */
+static void heap_sift_down(idani_t *h, int n, int i)
+{
+    for (;;) {
+        int l = 2 * i + 1, r = l + 1, s = i;
+        if (l < n && h[l].ani < h[s].ani) s = l;
+        if (r < n && h[r].ani < h[s].ani) s = r;
+        if (s == i) break;
+        idani_t t = h[i];
+        h[i] = h[s];
+        h[s] = t;
+        i = s;
+    }
+}
+
+static int select_topn(idani_t *a, int m, int topn)
+{
+    if (m <= 0 || topn <= 0)
+        return 0;
+    if (topn > m)
+        topn = m;
+    if (m <= 128 || topn >= m / 2) {
+        qsort(a, (size_t)m, sizeof *a, cmp_idani_desc);
+        return topn;
+    }
+    for (int i = (topn >> 1) - 1; i >= 0; --i)
+        heap_sift_down(a, topn, i);
+    for (int i = topn; i < m; ++i) {
+        if (a[i].ani <= a[0].ani)
+            continue;
+        idani_t t = a[i];
+        a[i] = a[0];
+        a[0] = t;
+        heap_sift_down(a, topn, 0);
+    }
+    qsort(a, (size_t)topn, sizeof *a, cmp_idani_desc);
+    return topn;
+}
+
+typedef struct {
+    double ani;
+    uint32_t id;
+} urank_t;
+
+static int cmp_urank(const void *a, const void *b)
+{
+    const urank_t *x = a, *y = b;
+    if (x->ani != y->ani)
+        return x->ani < y->ani ? 1 : -1;
+    return (x->id > y->id) - (x->id < y->id);
+}
+
+/* ------------------------------------------------------------------ mem_eff index path */
+
+static void print_unique_block(kssd_buf_t *b, int R, int q0, int nb, const uint32_t *rcnt, const uint32_t *qcnt,
+                               const uint32_t *uref, const counts_t *c, char (*refn)[PATHLEN], char (*qryn)[PATHLEN])
+{
+    /* print_unique_context_block, src/command_ani.c:462-492 */
+    for (int q = 0; q < nb; ++q)
+        for (int r = 0; r < R; ++r) {
+            const size_t cell = (size_t)q * R + r;
+            if (!c->ctx[cell].num_ctx)
+                continue;
+            const uint32_t shared = c->uctx[cell].num_ctx;
+            kssd_buf_printf(b, "%s\t%s\t%u\t%u\t%u\t%u\t%u\t%u\t%u\t%u\t%u\t%u\t%u", qryn[q0 + q], refn[r], qcnt[q0 + q],
+                            rcnt[r], c->ctx[cell].num_ctx, c->obj[cell].diff_obj, c->obj[cell].diff_obj_section,
+                            c->ctx[cell].num_mut2_ctx, uref[r], shared, c->uobj[cell].diff_obj,
+                            c->uobj[cell].diff_obj_section, c->uctx[cell].num_mut2_ctx);
+            if (shared) {
+                kssd_features_t f = feat_of(&c->uctx[cell], &c->uobj[cell]);
+                kssd_buf_printf(b, "\t%.6f", 1.0 - kssd_naive_dist(&f));
+            } else
+                kssd_buf_puts(b, "\tNA");
+            kssd_buf_printf(b, "\t%.6f", (double)shared / qcnt[q0 + q]);
+            if (uref[r])
+                kssd_buf_printf(b, "\t%.6f", (double)shared / uref[r]);
+            else
+                kssd_buf_puts(b, "\tNA");
+            kssd_buf_printf(b, "\t%.6f\n", (double)shared / rcnt[r]);
+        }
+}
+
+static FILE *open_out_with_report(const char *path, FILE *report)
+{
+    if (!report)
+        return path[0] ? fopen(path, "w") : stdout;
+    int fd = path[0] ? open(path, O_WRONLY | O_CREAT, 0666) : STDOUT_FILENO;
+    if (fd < 0)
+        err(errno, "%s", path);
+    struct stat out, diag;
+    if (fstat(fd, &out) || fstat(fileno(report), &diag))
+        err(errno, "Cannot check ANI output identity");
+    if (out.st_dev == diag.st_dev && out.st_ino == diag.st_ino)
+        errx(EXIT_FAILURE, "--unique-ctx-report must differ from the ordinary output path");
+    if (!path[0])
+        return stdout;
+    if (S_ISREG(out.st_mode) && ftruncate(fd, 0))
+        err(errno, "%s", path);
+    FILE *fp = fdopen(fd, "w");
+    if (!fp) {
+        close(fd);
+        err(errno, "%s", path);
+    }
+    return fp;
+}
+
+static int run_mem_eff(void)
+{
+    kssd_ani_opt_t *o = &g.o;
+    const bool count_unique = g.unique_ctx || g.unique_report[0];
+    kssd_sketch_t *ref = load_sketch(g.refdir, ref_flags());
+    kssd_sketch_t *qry = load_sketch(g.qrydir, qry_flags());
+    size_t nrec = 0;
+    kssd_index_rec_t *rec = kssd_index_load(g.refdir, &nrec);
+    if (!rec)
+        errx(EXIT_FAILURE, "%s", kssd_host_last_error());
+    if (nrec != (size_t)(ref->offs[ref->n] - ref->offs[0]))
+        errx(EXIT_FAILURE, "%s/sortedcomb_ctxgid64obj32: %zu records, expected %llu", g.refdir, nrec,
+             (unsigned long long)(ref->offs[ref->n] - ref->offs[0]));
+    if (qry->stat.hash_id != ref->stat.hash_id)
+        errx(EXIT_FAILURE, "hash_id mismatch between query and reference sketches");
+    const int R = ref->n;
+    kssdgpu_index_t *ix = NULL;
+    gpu_check(kssdgpu_index_from_records(rec, nrec, R, qry->obj_bits, 0, &ix), "device index");
+    free(rec);
+    uint32_t *rcnt = malloc((size_t)R * 4 + 4), *uref = malloc((size_t)R * 4 + 4);
+    if (ref->stat.conflict)
+        gpu_check(kssdgpu_index_ref_ctx_counts(ix, 1, o->ignoreconflict, rcnt, uref), "reference counts");
+    else {
+        for (int i = 0; i < R; ++i)
+            rcnt[i] = (uint32_t)(ref->offs[i + 1] - ref->offs[i]);
+        gpu_check(kssdgpu_index_ref_ctx_counts(ix, 0, o->ignoreconflict, NULL, uref), "reference counts");
+    }
+    uint32_t *qcnt = sample_ctx_counts(qry, qry->stat.conflict, false);
+
+    FILE *report = NULL;
+    if (g.unique_report[0]) {
+        report = fopen(g.unique_report, "wx");
+        if (!report)
+            err(errno, "%s", g.unique_report);
+        fprintf(report, "Qry\tRef\tQry_ctx\tRef_ctx\tXnY_ctx\tN_diff_obj\tN_diff_obj_section\tN_mut2_ctx\tUnique_Ref_ctx\t"
+                        "Unique_XnY_ctx\tUnique_N_diff_obj\tUnique_N_diff_obj_section\tUnique_N_mut2_ctx\tUnique_ANI\t"
+                        "Unique_QAF\tUnique_RAF\tUnique_RAF_fullref\n");
+    }
+    FILE *out = open_out_with_report(g.outf, report);
+    if (!out)
+        err(errno, "%s", g.outf);
+    kssd_buf_t hb = {0};
+    if (o->fmt) {
+        for (int i = 0; i < R; ++i) {
+            kssd_buf_putc(&hb, '\t');
+            kssd_buf_puts(&hb, ref->names[i]);
+        }
+        kssd_buf_putc(&hb, '\n');
+    } else {
+        kssd_buf_puts(&hb, kssd_detail_header);
+        kssd_buf_putc(&hb, '\n');
+    }
+    write_buf(out, &hb);
+    kssd_buf_free(&hb);
+
+    const unsigned flags = (o->ignoreconflict ? KSSDGPU_IGNORECONFLICT : 0) | (count_unique ? KSSDGPU_UNIQUE : 0);
+    const int ntop = o->ntop > 0 ? o->ntop : R;
+    const int B = block_for(R, qry->n);
+    for (int q0 = 0; q0 < qry->n; q0 += B) {
+        const int nb = qry->n - q0 < B ? qry->n - q0 : B;
+        counts_t c = count_queries(ix, R, qry, q0, nb, flags);
+        if (report) {
+            kssd_buf_t rb = {0};
+            print_unique_block(&rb, R, q0, nb, rcnt, qcnt, uref, &c, ref->names, qry->names);
+            write_buf(report, &rb);
+            kssd_buf_free(&rb);
+        }
+        kssd_buf_t *rows = calloc((size_t)nb, sizeof(kssd_buf_t));
+#pragma omp parallel for schedule(dynamic, 1) num_threads(o->p)
+        for (int i = 0; i < nb; ++i) {
+            const int qg = q0 + i;
+            const size_t a_size = (size_t)(qry->offs[qg + 1] - qry->offs[qg]);
+            kssd_buf_t *b = &rows[i];
+            const kssdgpu_ctx_mut2_t *cx = c.ctx + (size_t)i * R;
+            const kssdgpu_obj_section_t *ob = c.obj + (size_t)i * R;
+            const kssdgpu_ctx_mut2_t *ucx = c.uctx ? c.uctx + (size_t)i * R : NULL;
+            const kssdgpu_obj_section_t *uob = c.uobj ? c.uobj + (size_t)i * R : NULL;
+            uint32_t *ids = NULL;
+            int out_n = 0;
+            if (!o->fmt) {
+                /* detail candidates and ranking, src/command_ani.h:577-621 */
+                if (a_size) {
+                    idani_t *cand = malloc((size_t)R * sizeof(idani_t) + 8);
+                    urank_t *ranks = o->unique_ctx ? malloc((size_t)R * sizeof(urank_t) + 16) : NULL;
+                    int m = 0;
+                    for (int j = 0; j < R; ++j) {
+                        const uint32_t shared = cx[j].num_ctx;
+                        if (shared < (uint32_t)o->ctxcut)
+                            continue;
+                        if (rcnt[j] == 0 || qcnt[qg] == 0 ||
+                            !kssd_af_pass(o, (double)shared / (double)qcnt[qg], (double)shared / (double)rcnt[j]))
+                            continue;
+                        float dist = (float)ob[j].diff_obj / cx[j].num_ctx / 7;
+                        double ani = (float)(1 - dist);
+                        if (ranks) {
+                            const bool use_u = kssd_use_unique_context(ucx[j].num_ctx, rcnt[j]);
+                            ani = 1.0 - (use_u ? naive_of(&ucx[j], &uob[j]) : naive_of(&cx[j], &ob[j]));
+                        }
+                        if (ani < o->anicut)
+                            continue;
+                        if (ranks)
+                            ranks[m] = (urank_t){ani, (uint32_t)j};
+                        cand[m].id = (uint32_t)j;
+                        cand[m].ani = (float)ani;
+                        m++;
+                    }
+                    ids = malloc((size_t)(m ? m : 1) * sizeof(uint32_t));
+                    if (ranks) {
+                        qsort(ranks, (size_t)m, sizeof *ranks, cmp_urank);
+                        out_n = m < ntop ? m : ntop;
+                        for (int r = 0; r < out_n; ++r)
+                            ids[r] = ranks[r].id;
+                        free(ranks);
+                    } else {
+                        out_n = select_topn(cand, m, ntop);
+                        for (int r = 0; r < out_n; ++r)
+                            ids[r] = cand[r].id;
+                    }
+                    free(cand);
+                }
+            } else {
+                kssd_buf_puts(b, qry->names[qg]);
+            }
+            const int loop = o->fmt ? R : out_n;
+            const int qsize = (int)qcnt[qg];
+            for (int n = 0; n < loop; ++n) {
+                const int j = o->fmt ? n : (int)ids[n];
+                kssd_features_t f = feat_of(&cx[j], &ob[j]);
+                const int rsize = (int)rcnt[j];
+                if (qsize == 0 || rsize == 0) {
+                    if (o->fmt)
+                        kssd_buf_printf(b, "\t%lf", kssd_matrix_exception_value(o));
+                    continue;
+                }
+                /* this path reports single-precision align fractions (src/command_ani.c:3489-3494) */
+                const float af_q = (float)f.XnY_ctx / qsize;
+                const float af_r = (float)f.XnY_ctx / rsize;
+                f.X_ctx = (uint32_t)qsize;
+                const float bq = (float)kssd_af_anib(&f, o->drfold);
+                f.X_ctx = (uint32_t)rsize;
+                const float br = (float)kssd_af_anib(&f, o->drfold);
+                kssd_row_t row = kssd_make_row((uint32_t)j, &f, o, (uint32_t)qsize, (uint32_t)rsize, af_q, bq, af_r, br,
+                                               qry->meta ? &qry->meta[qg] : NULL, ref->meta ? &ref->meta[j] : NULL);
+                if (o->unique_ctx) {
+                    row.unique_ctx_selected = kssd_use_unique_context(ucx[j].num_ctx, rcnt[j]);
+                    row.naive_dist = row.unique_ctx_selected ? naive_of(&ucx[j], &uob[j]) : naive_of(&cx[j], &ob[j]);
+                    kssd_finalize_row(&row, o);
+                }
+                const double metric = o->s < 0 ? row.selected_ani : row.metric;
+                if (o->fmt)
+                    kssd_buf_printf(b, "\t%lf", metric);
+                else if (row.selected_ani >= o->anicut)
+                    kssd_append_detail_row(b, o, qry->names[qg], ref->names[j], &row, anno_at(ref, (uint32_t)j));
+            }
+            if (o->fmt)
+                kssd_buf_putc(b, '\n');
+            free(ids);
+        }
+        for (int i = 0; i < nb; ++i) {
+            write_buf(out, &rows[i]);
+            kssd_buf_free(&rows[i]);
+        }
+        free(rows);
+        free_counts(&c);
+    }
+    if (report && fclose(report) != 0)
+        err(errno, "Cannot finish unique-context report");
+    close_out(out);
+    kssdgpu_index_free(ix);
+    free(rcnt);
+    free(uref);
+    free(qcnt);
+    kssd_sketch_free(ref);
+    kssd_sketch_free(qry);
+    return 0;
+}
+
+/* ------------------------------------------------------------------ self matrices */
+
+/* Writes sortedcomb_ctxgid64obj32 and its unique bits from the device index, as
+ * `kssd3a sketch -i` does (gen_inverted_index4comblco, src/command_sketch.c:916-938). */
+static void write_index_files(const char *dir, kssdgpu_index_t *ix, uint64_t n)
+{
+    kssd_index_rec_t *rec = malloc(n * sizeof(*rec) + 12);
+    uint8_t *bits = malloc((n + 7) / 8 + 1);
+    if (!rec || !bits)
+        err(EXIT_FAILURE, "OOM index export");
+    gpu_check(kssdgpu_index_export(ix, rec, bits), "index export");
+    if (kssd_index_write(dir, rec, n, bits))
+        errx(EXIT_FAILURE, "%s", kssd_host_last_error());
+    uint64_t marked = 0;
+    for (uint64_t i = 0; i < n; ++i)
+        marked += (bits[i >> 3] >> (i & 7)) & 1u;
+    fprintf(stderr, "sketch unique-index: wrote %s/sortedcomb_ctxgid64obj32.unique_bits (%llu bytes; %llu unique markers / %llu records)\n",
+            dir, (unsigned long long)((n + 7) / 8), (unsigned long long)marked, (unsigned long long)n);
+    free(rec);
+    free(bits);
+}
+
+/* Lower-triangle counters of a self sketch: with an index file, the reference's
+ * index (probe kernel over query blocks); without, the self join over the index the
+ * device builds from the sketch. */
+static void self_lower_counts(const kssd_sketch_t *s, const char *dir, bool index_file, kssdgpu_ctx_mut2_t **pc,
+                              kssdgpu_obj_section_t **po)
+{
+    const int n = s->n;
+    const size_t cells = (size_t)n * (n - 1) / 2;
+    kssdgpu_ctx_mut2_t *lc = malloc(cells * sizeof(*lc) + 8);
+    kssdgpu_obj_section_t *lo = malloc(cells * sizeof(*lo) + 8);
+    if (!lc || !lo)
+        err(EXIT_FAILURE, "OOM lower triangle");
+    const unsigned flags = g.o.ignoreconflict ? KSSDGPU_IGNORECONFLICT : 0;
+    if (index_file) {
+        size_t nrec = 0;
+        kssd_index_rec_t *rec = kssd_index_load(dir, &nrec);
+        if (!rec)
+            errx(EXIT_FAILURE, "%s", kssd_host_last_error());
+        if (nrec != (size_t)(s->offs[n] - s->offs[0]))
+            errx(EINVAL, "load_self_sorted_index_or_build(): sorted index size mismatch");
+        kssdgpu_index_t *ix = NULL;
+        gpu_check(kssdgpu_index_from_records(rec, nrec, n, s->obj_bits, 0, &ix), "device index");
+        free(rec);
+        const int B = block_for(n, n);
+        for (int q0 = 0; q0 < n; q0 += B) {
+            const int nb = n - q0 < B ? n - q0 : B;
+            kssdgpu_ctx_mut2_t *c = malloc((size_t)nb * n * sizeof(*c) + 8);
+            kssdgpu_obj_section_t *o = malloc((size_t)nb * n * sizeof(*o) + 8);
+            if (!c || !o)
+                err(EXIT_FAILURE, "OOM counter block");
+            gpu_check(kssdgpu_count_lower(ix, s->keys + (s->offs[q0] - s->offs[0]), s->offs + q0, nb, q0, flags, c, o),
+                      "device counting");
+#pragma omp parallel for schedule(static) num_threads(g.o.p)
+            for (int i = 0; i < nb; ++i) {
+                const int q = q0 + i;
+                if (q == 0)
+                    continue;
+                memcpy(lc + (size_t)q * (q - 1) / 2, c + (size_t)i * n, (size_t)q * sizeof(*c));
+                memcpy(lo + (size_t)q * (q - 1) / 2, o + (size_t)i * n, (size_t)q * sizeof(*o));
+            }
+            free(c);
+            free(o);
+        }
+        kssdgpu_index_free(ix);
+    } else {
+        if (force_ref_index())
+            errx(EXIT_FAILURE, "KSSD3A_FORCE_REF_INDEX requires reference index '%s/%s'", dir,
+                 "sortedcomb_ctxgid64obj32");
+        kssdgpu_index_t *ix = gpu_index_of_sketch(s);
+        if (cells)
+            gpu_check(kssdgpu_self_lower(ix, flags, lc, lo), "device self join");
+        kssdgpu_index_free(ix);
+    }
+    *pc = lc;
+    *po = lo;
+}
+
+/* metric values of every lower pair (q > r), rows in parallel */
+static double *self_lower_metrics(const kssd_sketch_t *s, const kssdgpu_ctx_mut2_t *lc, const kssdgpu_obj_section_t *lo)
+{
+    const int n = s->n;
+    const size_t cells = (size_t)n * (n - 1) / 2;
+    uint32_t *qcnt = sample_ctx_counts(s, s->stat.conflict, false);
+    uint32_t *rcnt = g.o.ignoreconflict ? sample_ctx_counts(s, s->stat.conflict, true) : qcnt;
+    double *m = malloc(cells * sizeof(double) + 8);
+    if (!m)
+        err(EXIT_FAILURE, "OOM metrics");
+#pragma omp parallel for schedule(dynamic, 16) num_threads(g.o.p)
+    for (int q = 1; q < n; ++q) {
+        const size_t base = (size_t)q * (q - 1) / 2;
+        for (int r = 0; r < q; ++r) {
+            kssd_features_t f = feat_of(&lc[base + r], &lo[base + r]);
+            m[base + r] = kssd_pair_metric(&f, qcnt[q], rcnt[r], &g.o, s->meta ? &s->meta[q] : NULL,
+                                           s->meta ? &s->meta[r] : NULL);
+        }
+    }
+    if (rcnt != qcnt)
+        free(rcnt);
+    free(qcnt);
+    return m;
+}
+
+static void print_self_full_fixed6(const kssd_sketch_t *s, const double *m)
+{
+    /* comb_sortedsketch64_indexed_self_full printing, src/command_ani.c:1711-1746 */
+    const int n = s->n;
+    FILE *out = open_out(g.outf);
+    kssd_buf_t h = {0};
+    for (int r = 0; r < n; ++r) {
+        kssd_buf_putc(&h, '\t');
+        kssd_buf_puts(&h, s->names[r]);
+    }
+    kssd_buf_putc(&h, '\n');
+    write_buf(out, &h);
+    kssd_buf_free(&h);
+    const int32_t diag = kssd_scale_fixed6(kssd_matrix_diagonal_value(&g.o));
+    const int chunk = 256;
+    for (int q0 = 0; q0 < n; q0 += chunk) {
+        const int nb = n - q0 < chunk ? n - q0 : chunk;
+        kssd_buf_t *rows = calloc((size_t)nb, sizeof(kssd_buf_t));
+#pragma omp parallel for schedule(dynamic, 1) num_threads(g.o.p)
+        for (int i = 0; i < nb; ++i) {
+            const int q = q0 + i;
+            kssd_buf_t *b = &rows[i];
+            kssd_buf_reserve(b, (size_t)n * 10 + PATHLEN);
+            kssd_buf_puts(b, s->names[q]);
+            for (int r = 0; r < n; ++r) {
+                int32_t v = diag;
+                if (q > r)
+                    v = kssd_scale_fixed6(m[(size_t)q * (q - 1) / 2 + r]);
+                else if (q < r)
+                    v = kssd_scale_fixed6(m[(size_t)r * (r - 1) / 2 + q]);
+                kssd_buf_putc(b, '\t');
+                kssd_put_scaled6(b, v);
+            }
+            kssd_buf_putc(b, '\n');
+        }
+        for (int i = 0; i < nb; ++i) {
+            write_buf(out, &rows[i]);
+            kssd_buf_free(&rows[i]);
+        }
+        free(rows);
+    }
+    close_out(out);
+}
+
+static void print_self_lf(const kssd_sketch_t *s, const double *m, bool full)
+{
+    /* "%lf" matrices: direct full (src/command_ani.c:3320-3343) and triangles (:1809-1822,:3346-3357) */
+    const int n = s->n;
+    FILE *out = open_out(g.outf);
+    if (full) {
+        kssd_buf_t h = {0};
+        for (int r = 0; r < n; ++r) {
+            kssd_buf_putc(&h, '\t');
+            kssd_buf_puts(&h, s->names[r]);
+        }
+        kssd_buf_putc(&h, '\n');
+        write_buf(out, &h);
+        kssd_buf_free(&h);
+    }
+    const double diag = kssd_matrix_diagonal_value(&g.o);
+    const int chunk = 256;
+    for (int q0 = 0; q0 < n; q0 += chunk) {
+        const int nb = n - q0 < chunk ? n - q0 : chunk;
+        kssd_buf_t *rows = calloc((size_t)nb, sizeof(kssd_buf_t));
+#pragma omp parallel for schedule(dynamic, 1) num_threads(g.o.p)
+        for (int i = 0; i < nb; ++i) {
+            const int q = q0 + i;
+            kssd_buf_t *b = &rows[i];
+            kssd_buf_puts(b, s->names[q]);
+            const int end = full ? n : q;
+            for (int r = 0; r < end; ++r) {
+                double v = diag;
+                if (q > r)
+                    v = m[(size_t)q * (q - 1) / 2 + r];
+                else if (q < r)
+                    v = m[(size_t)r * (r - 1) / 2 + q];
+                kssd_buf_printf(b, "\t%lf", v);
+            }
+            if (!full && g.o.d)
+                kssd_buf_printf(b, "\t%lf", diag);
+            kssd_buf_putc(b, '\n');
+        }
+        for (int i = 0; i < nb; ++i) {
+            write_buf(out, &rows[i]);
+            kssd_buf_free(&rows[i]);
+        }
+        free(rows);
+    }
+    close_out(out);
+}
+
+/* kind: 0 indexed full (fixed6), 1 indexed triangle, 2 direct (full or triangle per fmt) */
+static int run_self(int kind)
+{
+    kssd_sketch_t *s = load_sketch(g.qrydir, 0);
+    init_bits(s);
+    bool index_file = false;
+    if (kind == 0) {
+        /* ensure_sorted_ref_index_for_ani_m1 (src/command_ani_wrapper.c:708-716): write the index when absent */
+        if (!kssd_file_exists(g.qrydir, "sortedcomb_ctxgid64obj32")) {
+            kssdgpu_index_t *ix = gpu_index_of_sketch(s);
+            write_index_files(g.qrydir, ix, s->offs[s->n] - s->offs[0]);
+            kssdgpu_index_free(ix);
+        }
+        index_file = true;
+    } else if (kind == 1) {
+        index_file = kssd_file_exists(g.qrydir, "sortedcomb_ctxgid64obj32");
+    }
+    kssdgpu_ctx_mut2_t *lc = NULL;
+    kssdgpu_obj_section_t *lo = NULL;
+    self_lower_counts(s, g.qrydir, index_file, &lc, &lo);
+    double *m = self_lower_metrics(s, lc, lo);
+    free(lc);
+    free(lo);
+    if (kind == 0)
+        print_self_full_fixed6(s, m);
+    else if (kind == 1)
+        print_self_lf(s, m, false);
+    else
+        print_self_lf(s, m, g.o.fmt == 1);
+    free(m);
+    kssd_sketch_free(s);
+    return 0;
+}
+
+/* ------------------------------------------------------------------ direct rectangular matrix */
+
+static int run_rect_matrix(void)
+{
+    kssd_sketch_t *qry = load_sketch(g.qrydir, qry_flags());
+    kssd_sketch_t *ref = load_sketch(g.refdir, ref_flags());
+    kssd_ani_opt_t *o = &g.o;
+    uint32_t *qcnt = sample_ctx_counts(qry, qry->stat.conflict, false);
+    uint32_t *rcnt = sample_ctx_counts(ref, ref->stat.conflict, o->ignoreconflict);
+    kssdgpu_index_t *ix = gpu_index_of_sketch(ref);
+    const unsigned flags = (o->ignoreconflict && ref->stat.conflict) ? KSSDGPU_IGNORECONFLICT : 0;
+    FILE *out = open_out(g.outf);
+    kssd_buf_t h = {0};
+    for (int r = 0; r < ref->n; ++r) {
+        kssd_buf_putc(&h, '\t');
+        kssd_buf_puts(&h, ref->names[r]);
+    }
+    kssd_buf_putc(&h, '\n');
+    write_buf(out, &h);
+    kssd_buf_free(&h);
+    const int R = ref->n, B = block_for(R, qry->n);
+    for (int q0 = 0; q0 < qry->n; q0 += B) {
+        const int nb = qry->n - q0 < B ? qry->n - q0 : B;
+        counts_t c = count_queries(ix, R, qry, q0, nb, flags);
+        kssd_buf_t *rows = calloc((size_t)nb, sizeof(kssd_buf_t));
+#pragma omp parallel for schedule(dynamic, 1) num_threads(o->p)
+        for (int i = 0; i < nb; ++i) {
+            const int q = q0 + i;
+            kssd_buf_puts(&rows[i], qry->names[q]);
+            for (int r = 0; r < R; ++r) {
+                kssd_features_t f = feat_of(&c.ctx[(size_t)i * R + r], &c.obj[(size_t)i * R + r]);
+                kssd_buf_printf(&rows[i], "\t%lf",
+                                kssd_pair_metric(&f, qcnt[q], rcnt[r], o, qry->meta ? &qry->meta[q] : NULL,
+                                                 ref->meta ? &ref->meta[r] : NULL));
+            }
+            kssd_buf_putc(&rows[i], '\n');
+        }
+        for (int i = 0; i < nb; ++i) {
+            write_buf(out, &rows[i]);
+            kssd_buf_free(&rows[i]);
+        }
+        free(rows);
+        free_counts(&c);
+    }
+    close_out(out);
+    kssdgpu_index_free(ix);
+    free(qcnt);
+    free(rcnt);
+    kssd_sketch_free(qry);
+    kssd_sketch_free(ref);
+    return 0;
+}
+
+/* ------------------------------------------------------------------ detail paths without an index */
+
+enum { DETAIL_STREAM_ONE = 0, DETAIL_STREAM_MULTI = 1, DETAIL_HASH = 2 };
+
+static int run_detail_scan(int kind)
+{
+    kssd_ani_opt_t *o = &g.o;
+    kssd_sketch_t *qry = load_sketch(g.qrydir, qry_flags());
+    kssd_sketch_t *ref = load_sketch(g.refdir, ref_flags());
+    if (ref->stat.hash_id != qry->stat.hash_id)
+        errx(EXIT_FAILURE, "hash_id mismatch between query and reference sketches");
+    const int R = ref->n;
+    const bool ref_conflict = ref->stat.conflict;
+    /* per-path context counts */
+    uint32_t *qcnt, *rcnt, *rtotal;
+    if (kind == DETAIL_HASH) {
+        qcnt = sample_ctx_counts(qry, qry->stat.conflict, false);
+        rcnt = sample_ctx_counts(ref, ref_conflict, o->ignoreconflict);
+        rtotal = rcnt;
+    } else {
+        qcnt = sample_ctx_counts(qry, true, false);
+        rcnt = sample_ctx_counts(ref, true, o->ignoreconflict);
+        rtotal = kind == DETAIL_STREAM_ONE ? sample_ctx_counts(ref, ref_conflict, o->ignoreconflict) : rcnt;
+    }
+    kssdgpu_index_t *ix = gpu_index_of_sketch(ref);
+    const unsigned flags = kind == DETAIL_HASH ? ((o->ignoreconflict && ref_conflict) ? KSSDGPU_IGNORECONFLICT : 0)
+                                               : (o->ignoreconflict ? KSSDGPU_IGNORECONFLICT : 0);
+    FILE *out = open_out(g.outf);
+    kssd_buf_t h = {0};
+    kssd_buf_puts(&h, kssd_detail_header);
+    kssd_buf_putc(&h, '\n');
+    write_buf(out, &h);
+    kssd_buf_free(&h);
+    const int B = block_for(R, qry->n);
+    for (int q0 = 0; q0 < qry->n; q0 += B) {
+        const int nb = qry->n - q0 < B ? qry->n - q0 : B;
+        counts_t c = count_queries(ix, R, qry, q0, nb, flags);
+        kssd_buf_t *rows = calloc((size_t)nb, sizeof(kssd_buf_t));
+#pragma omp parallel for schedule(dynamic, 1) num_threads(o->p)
+        for (int i = 0; i < nb; ++i) {
+            const int q = q0 + i;
+            kssd_row_t *surv = malloc((size_t)(R ? R : 1) * sizeof(kssd_row_t));
+            size_t ns = 0;
+            const uint32_t qctx = qcnt[q];
+            for (int r = 0; r < R && qctx; ++r) {
+                const size_t rlen = (size_t)(ref->offs[r + 1] - ref->offs[r]);
+                kssd_features_t f = feat_of(&c.ctx[(size_t)i * R + r], &c.obj[(size_t)i * R + r]);
+                const uint32_t rctx = rcnt[r];
+                if (kind == DETAIL_STREAM_ONE) {
+                    /* compute_streamed_ref_row_one_qry, src/command_ani.c:2110-2201 */
+                    if (rlen == 0 || rtotal[r] == 0)
+                        continue;
+                    const uint32_t need = kssd_af_needed_ctx(o, qctx, rtotal[r]);
+                    if (rctx == 0 || f.XnY_ctx < (uint32_t)o->ctxcut || f.XnY_ctx < need)
+                        continue;
+                } else if (kind == DETAIL_STREAM_MULTI) {
+                    /* src/command_ani.c:2933-2960 */
+                    if (rctx == 0 || f.XnY_ctx < (uint32_t)o->ctxcut)
+                        continue;
+                } else {
+                    /* comb_manysmall_...: src/command_ani.c:3945-3968 */
+                    if (rctx == 0)
+                        continue;
+                    if (f.XnY_ctx < kssd_af_needed_ctx(o, qctx, rctx))
+                        continue;
+                }
+                const double af_q = (double)f.XnY_ctx / (double)qctx;
+                const double af_r = (double)f.XnY_ctx / (double)rctx;
+                if (!kssd_af_pass(o, af_q, af_r))
+                    continue;
+                kssd_features_t t = f;
+                t.X_ctx = qctx;
+                const double bq = kssd_af_anib(&t, o->drfold);
+                t = f;
+                t.X_ctx = rctx;
+                const double br = kssd_af_anib(&t, o->drfold);
+                kssd_row_t row = kssd_make_row((uint32_t)r, &f, o, qctx, rctx, af_q, bq, af_r, br,
+                                               qry->meta ? &qry->meta[q] : NULL, ref->meta ? &ref->meta[r] : NULL);
+                if (kind != DETAIL_STREAM_MULTI && !kssd_row_passes_close_filter(&row, o))
+                    continue;
+                if (kind == DETAIL_HASH ? row.selected_ani <= o->anicut : row.selected_ani < o->anicut)
+                    continue;
+                surv[ns++] = row;
+            }
+            if (ns)
+                qsort(surv, ns, sizeof *surv, kssd_cmp_row_desc);
+            size_t out_n = ns;
+            if (kind != DETAIL_HASH && o->ntop > 0 && (size_t)o->ntop < out_n)
+                out_n = (size_t)o->ntop;
+            for (size_t k = 0; k < out_n; ++k)
+                kssd_append_detail_row(&rows[i], o, qry->names[q], ref->names[surv[k].rn], &surv[k],
+                                       anno_at(ref, surv[k].rn));
+            free(surv);
+        }
+        for (int i = 0; i < nb; ++i) {
+            write_buf(out, &rows[i]);
+            kssd_buf_free(&rows[i]);
+        }
+        free(rows);
+        free_counts(&c);
+    }
+    close_out(out);
+    kssdgpu_index_free(ix);
+    if (rtotal != rcnt)
+        free(rtotal);
+    free(qcnt);
+    free(rcnt);
+    kssd_sketch_free(qry);
+    kssd_sketch_free(ref);
+    return 0;
+}
+
+/* ------------------------------------------------------------------ dispatcher */
+
+static void gen_index(const char *dir)
+{
+    kssd_sketch_t *s = load_sketch(dir, 0);
+    if ((uint64_t)(s->offs[s->n] - s->offs[0]) >= 0xFFFFFFFFull)
+        errx(EXIT_FAILURE, "gen_inverted_index4comblco():sketch_index maximun exceed UINT32_MAX");
+    kssdgpu_index_t *ix = gpu_index_of_sketch(s);
+    write_index_files(dir, ix, s->offs[s->n] - s->offs[0]);
+    kssdgpu_index_free(ix);
+    kssd_sketch_free(s);
+}
+
+/* run_sketch_ani, src/command_ani_wrapper.c:1082-1230 */
+static int run_sketch_ani(void)
+{
+    kssd_ani_opt_t *o = &g.o;
+    if ((g.unique_ctx || g.unique_report[0]) && !kssd_file_exists(g.refdir, "sortedcomb_ctxgid64obj32"))
+        errx(EXIT_FAILURE, "unique-context options require an existing unfiltered reference inverted index; run "
+                           "sketch -i on the reference sketch");
+    if (o->unassembled && !o->afcut_set)
+        o->afcut = 0.2f;
+    kssd_sketch_stat_t qst;
+    if (kssd_read_stat(g.qrydir, &qst))
+        errx(EXIT_FAILURE, "%s", kssd_host_last_error());
+    const int nq = qst.infile_num;
+    o->drfold = qst.drfold;
+    kssd_stat_bits(&qst, &o->ctx_bits, &o->obj_bits);
+    const bool force = force_ref_index() || g.unique_ctx || g.unique_report[0];
+    const int direct_n = o->fmt ? matrix_direct_threshold() : 0;
+    const bool self = !g.refdir[0] || (o->fmt && same_file(g.refdir, g.qrydir));
+    if (self) {
+        if (!g.refdir[0] && o->fmt == 0)
+            errx(EXIT_FAILURE, "one-sketch ANI detail output is not supported; use -m1 full matrix or -m2 triangle");
+        if (o->fmt == 1 && (force || matrix_use_index(nq, nq, direct_n))) {
+            if (force && !kssd_file_exists(g.qrydir, "sortedcomb_ctxgid64obj32"))
+                errx(EXIT_FAILURE, "KSSD3A_FORCE_REF_INDEX requires reference index '%s/%s'", g.qrydir,
+                     "sortedcomb_ctxgid64obj32");
+            return run_self(0);
+        }
+        if (o->fmt == 2 && (force || matrix_use_index(nq, nq, direct_n)))
+            return run_self(1);
+        return run_self(2);
+    }
+    if (o->fmt == 2)
+        errx(EXIT_FAILURE, "ANI triangle output requires one sketch or identical -r/-q sketches");
+    kssd_sketch_stat_t rst;
+    if (kssd_read_stat(g.refdir, &rst))
+        errx(EXIT_FAILURE, "%s", kssd_host_last_error());
+    const int nref = rst.infile_num;
+    const bool small_stream = !force && o->fmt == 0 && nref > 0 && nq < nref;
+    if (small_stream && nq == 1) {
+        const char *lk = getenv("KSSD3A_QRAW_LOOKUP");
+        if (lk && lk[0] && strcmp(lk, "sorted") && strcmp(lk, "fence") && strcmp(lk, "fencepost") && strcmp(lk, "hash"))
+            errx(EXIT_FAILURE, "stream_ref_sketches_one_qraw_lookup(): invalid KSSD3A_QRAW_LOOKUP='%s' (use hash or sorted)", lk);
+        return run_detail_scan(DETAIL_STREAM_ONE);
+    }
+    const char *multi = getenv("KSSD3A_QRAW_MULTI");
+    if (o->fmt == 0 && nq > 1) {
+        bool use_q = small_stream && nq <= env_int("KSSD3A_QRAW_MULTI_THRESHOLD", 20, 1, "positive integer");
+        if (o->unassembled && !force && multi && multi[0]) {
+            if (!strcmp(multi, "sortedindex"))
+                use_q = true;
+            else if (!strcmp(multi, "legacy") || !strcmp(multi, "refindex"))
+                use_q = false;
+            else
+                errx(EXIT_FAILURE, "invalid KSSD3A_QRAW_MULTI='%s' (use sortedindex, refindex, or legacy)", multi);
+        }
+        if (use_q)
+            return run_detail_scan(DETAIL_STREAM_MULTI);
+    }
+    const bool has_index = kssd_file_exists(g.refdir, "sortedcomb_ctxgid64obj32");
+    if (o->fmt == 1) {
+        if (force) {
+            if (!has_index)
+                errx(EXIT_FAILURE, "KSSD3A_FORCE_REF_INDEX requires reference index '%s/%s'", g.refdir,
+                     "sortedcomb_ctxgid64obj32");
+            return run_mem_eff();
+        }
+        if (matrix_use_index(nref, nq, direct_n)) {
+            if (!has_index)
+                gen_index(g.refdir);
+            return run_mem_eff();
+        }
+    } else if (has_index)
+        return run_mem_eff();
+    const int auto_n = env_int("KSSD3A_AUTO_REF_INDEX_THRESHOLD", 100, 0, "non-negative integer; 0 disables");
+    if (!o->v && !o->unassembled && o->fmt == 0 && auto_n > 0 && nref > auto_n) {
+        gen_index(g.refdir);
+        return run_mem_eff();
+    }
+    if (force)
+        errx(EXIT_FAILURE, "KSSD3A_FORCE_REF_INDEX requires reference index '%s/%s'", g.refdir,
+             "sortedcomb_ctxgid64obj32");
+    if (o->fmt)
+        return run_rect_matrix();
+    return run_detail_scan(DETAIL_HASH);
+}
+
+static int cmd_ani(int argc, char **argv)
+{
+    memset(&g, 0, sizeof g);
+    kssd_opt_defaults(&g.o);
+    g.sketch_coden = true;
+    g.sketch_hclen = 11;
+    g.sketch_drfold = 8;
+    g.sketch_kmerocrs = 1;
+    argp_parse(&k_argp, argc, argv, ARGP_IN_ORDER, NULL, NULL);
+    g.o.unique_ctx = g.unique_ctx;
+    if (g.o.p < 1)
+        g.o.p = 1;
+    if (g.reflist[0] || g.qrylist[0] || g.pair)
+        errx(EXIT_FAILURE, "FASTA/FASTQ and list inputs need the sketcher, which this build does not include; "
+                           "sketch with `kssd3a sketch` first");
+    if (g.estimate_coverage)
+        errx(EXIT_FAILURE, "--estimate-coverage is not supported by this build");
+    if (!is_sketch_dir(g.qrydir))
+        errx(EXIT_FAILURE, "%s is not a sketch directory; FASTA/FASTQ inputs need the sketcher, which this build "
+                           "does not include", g.qrydir);
+    run_sketch_ani();
+    return 0;
+}
+
+int main(int argc, char **argv)
+{
+    setvbuf(stdout, NULL, _IOFBF, 1 << 20);
+    if (argc < 2) {
+        fprintf(stderr, "Usage: %s ani [OPTION...]\n", argv[0]);
+        return 64;
+    }
+    if (!strcmp(argv[1], "ani"))
+        return cmd_ani(argc - 1, argv + 1);
+    if (!strcmp(argv[1], "--version") || !strcmp(argv[1], "-V")) {
+        printf("%s\n", argp_program_version);
+        return 0;
+    }
+    fprintf(stderr, "%s: subcommand '%s' is not part of the counting engine; use the reference binary\n", argv[0],
+            argv[1]);
+    return 64;
+}

@@ -113,3 +113,33 @@ int refh_pair_features(const uint64_t *a, size_t n, const uint64_t *b, size_t m,
 	out4[3] = f.N_mut2_ctx;
 	return 0;
 }
+
+/* The reference's FP64 model functions (src/model_ani.h, src/model_refaf_hgb.h,
+ * src/command_ani.h:200-232, src/command_matrix.c:26-33), for bit-exact tests of the
+ * host epilogue.  f5 = {XnY, X_ctx, section, mut2, diff_obj} as ani_features_t. */
+extern double get_mashD(uint32_t K, uint32_t X, uint32_t Y, uint32_t XnY);
+extern double get_aafD(uint32_t K, uint32_t X, uint32_t Y, uint32_t XnY);
+
+void refh_models(const uint32_t *f5, int drfold, int obj_bits, double out[6])
+{
+	set_bits(obj_bits);
+	ani_model_drfold = drfold;
+	ani_features_t f;
+	memcpy(&f, f5, sizeof f);
+	ani_features_t t = f;
+	out[0] = lm3ways_dist_from_features(&t);
+	t = f;
+	out[1] = lm3ways_af_ANIb_from_features(&t);
+	t = f;
+	out[2] = get_naive_dist(&t);
+	t = f;
+	out[3] = get_p_dist(&t);
+	out[4] = get_mashD(Bitslen.ctx / 2, f.X_ctx, f.XnY_ctx + 7, f.XnY_ctx);
+	out[5] = get_aafD(Bitslen.ctx / 2, f.X_ctx, f.XnY_ctx + 7, f.XnY_ctx);
+}
+
+double refh_hgb(double raw_ani, double ref_af, unsigned xny, unsigned dobj, unsigned sect, unsigned mut2, int drfold)
+{
+	ani_model_drfold = drfold;
+	return refaf_hgb_predict_ani(raw_ani, ref_af, xny, dobj, sect, mut2);
+}

@@ -1,0 +1,95 @@
+"""Command-line parity cases shared by tests/test_gpu_cli.py and tests/golden/make_golden.py.
+
+Each case names seeded synthetic sketch directories (generated on demand by the host
+library's sketch-space generator) and an `ani` command line; the reference CLI and
+bin/kssd3a must print the same bytes.  The cases walk the reference dispatcher
+(src/command_ani_wrapper.c:1082-1230): indexed mem_eff detail/matrix, one- and
+multi-query streams, the no-index hash path, direct and indexed self matrices and
+triangles, the rectangular direct matrix, read sets with --unique-ctx.
+"""
+import os
+import shutil
+
+import kssdgpu
+
+FIXTURES = {
+    # 120 references: above the auto-index threshold (100) for detail output
+    "refs120": dict(n_samples=120, n_clusters=12, len_median=3e5, len_sigma=0.3, len_min=1e5, len_max=8e5,
+                    size_dist=kssdgpu.SIZE_LOGNORMAL, sub_lo=0.001, sub_hi=0.06, seed=11, sample_seed=11),
+    "qry30": dict(n_samples=30, n_clusters=12, role=kssdgpu.ROLE_OWNLEN, len_median=3e5, len_sigma=0.3,
+                  len_min=1e5, len_max=8e5, size_dist=kssdgpu.SIZE_LOGNORMAL, own_len_min=5e4, own_len_max=9e5,
+                  sub_lo=0.001, sub_hi=0.06, seed=11, sample_seed=12, name_prefix="q"),
+    "refs40": dict(n_samples=40, n_clusters=5, len_median=2e5, len_sigma=0.3, len_min=1e5, len_max=6e5,
+                   size_dist=kssdgpu.SIZE_LOGNORMAL, sub_lo=0.001, sub_hi=0.04, seed=21, sample_seed=21),
+    "qry1": dict(n_samples=1, n_clusters=5, role=kssdgpu.ROLE_OWNLEN, len_median=2e5, len_sigma=0.3, len_min=1e5,
+                 len_max=6e5, size_dist=kssdgpu.SIZE_LOGNORMAL, own_len_min=1.5e5, own_len_max=3e5, sub_lo=0.002,
+                 sub_hi=0.01, seed=21, sample_seed=22, name_prefix="one"),
+    "qry8": dict(n_samples=8, n_clusters=5, role=kssdgpu.ROLE_OWNLEN, len_median=2e5, len_sigma=0.3, len_min=1e5,
+                 len_max=6e5, size_dist=kssdgpu.SIZE_LOGNORMAL, own_len_min=5e4, own_len_max=4e5, sub_lo=0.001,
+                 sub_hi=0.03, seed=21, sample_seed=23, name_prefix="few"),
+    "qry50": dict(n_samples=50, n_clusters=5, role=kssdgpu.ROLE_OWNLEN, len_median=2e5, len_sigma=0.3,
+                  len_min=1e5, len_max=6e5, size_dist=kssdgpu.SIZE_LOGNORMAL, own_len_min=5e4, own_len_max=4e5,
+                  sub_lo=0.001, sub_hi=0.03, seed=21, sample_seed=24, name_prefix="many"),
+    "reads6": dict(n_samples=6, n_clusters=12, role=kssdgpu.ROLE_READS, len_median=3e5, len_sigma=0.3,
+                   len_min=1e5, len_max=8e5, size_dist=kssdgpu.SIZE_LOGNORMAL, sub_lo=0.001, sub_hi=0.06, seed=11,
+                   sample_seed=31, ref_sample_seed=11, ref_samples=120, cov_lo=5, cov_hi=20, err_lo=0.001,
+                   err_hi=0.005, name_prefix="reads"),
+}
+INDEXED = {"refs120i"}  # refs120 with sortedcomb_ctxgid64obj32 written up front
+
+# (case name, argv after `kssd3a`, extra environment)
+CASES = [
+    ("memeff_detail", ["ani", "-r", "{refs120}", "-q", "{qry30}"], {}),
+    ("memeff_detail_top3", ["ani", "-r", "{refs120}", "-q", "{qry30}", "-N", "3", "-n", "0.9", "-f", "0.3"], {}),
+    ("memeff_detail_metrics", ["ani", "-r", "{refs120}", "-q", "{qry30}", "--metric", "p_dist", "-n", "0.5"], {}),
+    ("memeff_detail_moe_raw", ["ani", "-r", "{refs120}", "-q", "{qry30}", "-s", "3", "--raw-output", "-t", "10"], {}),
+    ("memeff_detail_close", ["ani", "-r", "{refs120}", "-q", "{qry30}", "--max-pdist", "0.02", "-n", "0.8"], {}),
+    ("memeff_detail_naive", ["ani", "-r", "{refs120}", "-q", "{qry30}", "-v"], {}),
+    ("memeff_matrix_ani", ["ani", "-r", "{refs120}", "-q", "{qry30}", "--format", "matrix", "--values", "ani"],
+     {"KSSD3A_ANI_MATRIX_DIRECT_THRESHOLD": "0"}),
+    ("rect_matrix_direct", ["ani", "-r", "{refs40}", "-q", "{qry8}", "--format", "matrix"], {}),
+    ("rect_matrix_ani_direct", ["ani", "-r", "{refs40}", "-q", "{qry50}", "--format", "matrix", "-s", "-5"], {}),
+    ("stream_one", ["ani", "-r", "{refs40}", "-q", "{qry1}", "-n", "0.9"], {}),
+    ("stream_multi", ["ani", "-r", "{refs40}", "-q", "{qry8}", "-n", "0.9", "-N", "4"], {}),
+    ("hash_detail", ["ani", "-r", "{refs40}", "-q", "{qry50}", "-n", "0.9"], {}),
+    ("self_full_direct", ["ani", "-q", "{refs120}", "--format", "matrix", "--values", "ani"], {}),
+    ("self_full_indexed", ["ani", "-q", "{refs120}", "--format", "matrix", "--values", "ani"],
+     {"KSSD3A_ANI_MATRIX_DIRECT_THRESHOLD": "0"}),
+    ("self_full_indexed_dist", ["ani", "-q", "{refs40}", "-m1"], {"KSSD3A_ANI_MATRIX_DIRECT_THRESHOLD": "0"}),
+    ("self_triangle_direct", ["ani", "-q", "{refs40}", "-m2", "-d", "-s", "-1"], {}),
+    ("self_triangle_indexed", ["ani", "-q", "{refs120}", "-m2"], {"KSSD3A_ANI_MATRIX_DIRECT_THRESHOLD": "0"}),
+    ("reads_qraw", ["ani", "-r", "{refs120i}", "--qraw", "{reads6}", "-n", "0.8"], {}),
+    ("reads_qraw_unique", ["ani", "-r", "{refs120i}", "--qraw", "{reads6}", "-n", "0.95", "--unique-ctx"], {}),
+    ("reads_qraw_ignoreconflict", ["ani", "-r", "{refs120i}", "--qraw", "{reads6}", "-n", "0.5", "--ignoreconflict"],
+     {}),
+    ("reads_qraw_stream", ["ani", "-r", "{refs120}", "--qraw", "{reads6}", "-n", "0.5"], {}),
+]
+
+
+def make_fixture(root: str, name: str) -> str:
+    """Writes fixture `name` under root (idempotent) and returns its directory."""
+    path = os.path.join(root, name)
+    if os.path.isdir(path):
+        return path
+    base = name[:-1] if name in INDEXED else name
+    spec = dict(FIXTURES[base])
+    sk = kssdgpu.synth(**spec)
+    kssdgpu.write_sketch_dir(path, sk, with_index=name in INDEXED)
+    return path
+
+
+def materialize(root: str, argv, fresh_tag: str):
+    """argv with fixture placeholders replaced by fresh copies (so side effects such
+    as automatic index creation start from the same state for every binary)."""
+    out = []
+    for a in argv:
+        if a.startswith("{") and a.endswith("}"):
+            name = a[1:-1]
+            src = make_fixture(os.path.join(root, "_src"), name)
+            dst = os.path.join(root, fresh_tag, name)
+            if not os.path.isdir(dst):
+                shutil.copytree(src, dst)
+            out.append(dst)
+        else:
+            out.append(a)
+    return out

@@ -6,8 +6,8 @@ small seeded fixtures.  Run from the repository root:
 
 counts_*.json : fixture samples + every row of `ani --unique-ctx-report` (the
                 reference's full per-cell counters, src/command_ani.c:462-492)
-cli_*/        : fixture sketch directories + the reference's stdout for a set of
-                `kssd3a ani` / `kssd3a matrix` command lines (cmds.json)
+cli/*.out.gz  : the reference CLI's stdout for every case of tests/cli_cases.py
+                (seeded synthetic sketch directories, regenerated on demand)
 """
 import csv
 import io
@@ -77,6 +77,25 @@ def counts_case(name, seed, nref, nq, ctx_space, obj_space, ignoreconflict):
     print(name, len(rows), "rows")
 
 
+def cli_cases():
+    """stdout of the reference CLI for every tests/cli_cases.py case, gzip-compressed."""
+    import gzip
+    from cli_cases import CASES, materialize
+    out_dir = os.path.join(HERE, "cli")
+    os.makedirs(out_dir, exist_ok=True)
+    root = tempfile.mkdtemp(prefix="golden-cli-")
+    try:
+        for name, argv, env in CASES:
+            a = materialize(root, argv, "ref_" + name)
+            e = dict(os.environ, OMP_NUM_THREADS="4", **env)
+            r = subprocess.run([REF, *a, "-p", "4"], capture_output=True, env=e, check=True)
+            with gzip.GzipFile(os.path.join(out_dir, name + ".out.gz"), "wb", mtime=0) as f:
+                f.write(r.stdout)
+            print(name, len(r.stdout), "bytes")
+    finally:
+        shutil.rmtree(root)
+
+
 def main():
     if not os.path.exists(REF):
         sys.exit(f"{REF} missing: run `make -C oracle ref` first")
@@ -85,6 +104,7 @@ def main():
     counts_case("s2", 2, 12, 6, 60, 1 << 20, False)
     counts_case("s3", 3, 12, 6, 60, 1 << 20, True)
     counts_case("s4", 4, 30, 10, 400, 1 << 20, False)
+    cli_cases()
 
 
 if __name__ == "__main__":
