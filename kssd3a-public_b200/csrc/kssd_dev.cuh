@@ -9,12 +9,15 @@ constexpr int kGidBits = 20;
 // Initial value of the per-context minimum object difference: NUM_CODENS + 1 with
 // the reference's default NUM_CODENS = 11 (src/command_ani.h:547,684).
 constexpr int kMinInit = 12;
-constexpr unsigned long long kEmptyCtx = ~0ull;  // contexts are at most 44 bits
+constexpr unsigned long long kEmptyCtx = ~0ull;      // contexts are at most 44 bits
+constexpr unsigned long long kInlineBit = 1ull << 62;  // slot holds its only posting
 
-// Hash-table slot of one unique context: key and its postings range.
+// Hash-table slot of one unique context: the key, and either its postings range
+// or, for a context with a single posting, that posting itself (one random line
+// per probe for the common single-owner context).
 struct __align__(16) Slot {
-    unsigned long long ctx;    // kEmptyCtx when free
-    unsigned long long range;  // begin (low 32) | count (high 32)
+    unsigned long long ctx;    // context | kInlineBit when inline; kEmptyCtx when free
+    unsigned long long range;  // begin (low 32) | count (high 32), or the inline posting
 };
 
 // Error flag values written by kernels (host maps them to status codes).
@@ -34,16 +37,17 @@ __host__ __device__ __forceinline__ unsigned long long mix64(unsigned long long 
 __device__ __forceinline__ int dna_pop(uint32_t x) { return __popc((x | (x >> 1)) & 0x55555555u); }
 
 // Probe the open-addressing table; bounded by the table size (load <= 1/2, so an
-// empty slot always ends the probe).
+// empty slot always ends the probe).  Returns the slot's payload and whether it is
+// an inline single posting.
 __device__ __forceinline__ bool table_lookup(const Slot *__restrict__ t, uint32_t mask, unsigned long long ctx,
-                                             uint32_t &begin, uint32_t &count)
+                                             unsigned long long &payload, bool &single)
 {
     uint32_t i = (uint32_t)mix64(ctx) & mask;
     for (uint32_t probe = 0; probe <= mask; ++probe) {
         const ulonglong2 s = __ldg(reinterpret_cast<const ulonglong2 *>(t + i));
-        if (s.x == ctx) {
-            begin = (uint32_t)s.y;
-            count = (uint32_t)(s.y >> 32);
+        if ((s.x & ~kInlineBit) == ctx) {
+            payload = s.y;
+            single = (s.x & kInlineBit) != 0;
             return true;
         }
         if (s.x == kEmptyCtx)

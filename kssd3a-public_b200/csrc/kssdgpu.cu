@@ -124,16 +124,21 @@ __global__ void k_scatter_groups(const uint32_t *__restrict__ head, const uint32
 }
 
 __global__ void k_table_insert(const unsigned long long *__restrict__ gkey, const uint32_t *__restrict__ gbeg, uint64_t u,
-                               Slot *__restrict__ t, uint32_t mask, int *__restrict__ err)
+                               const uint64_t *__restrict__ post, Slot *__restrict__ t, uint32_t mask,
+                               int *__restrict__ err)
 {
     for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < u; g += (uint64_t)gridDim.x * blockDim.x) {
         const unsigned long long ctx = gkey[g];
-        const unsigned long long range = (unsigned long long)gbeg[g] | ((unsigned long long)(gbeg[g + 1] - gbeg[g]) << 32);
+        const uint32_t cnt = gbeg[g + 1] - gbeg[g];
+        // a context with one posting keeps it in the slot
+        const unsigned long long word = cnt == 1 ? (ctx | kInlineBit) : ctx;
+        const unsigned long long range =
+            cnt == 1 ? post[gbeg[g]] : ((unsigned long long)gbeg[g] | ((unsigned long long)cnt << 32));
         uint32_t i = (uint32_t)mix64(ctx) & mask;
         bool done = false;
         for (uint32_t probe = 0; probe <= mask; ++probe) {
-            const unsigned long long prev = atomicCAS(&t[i].ctx, kEmptyCtx, ctx);
-            if (prev == kEmptyCtx || prev == ctx) {
+            const unsigned long long prev = atomicCAS(&t[i].ctx, kEmptyCtx, word);
+            if (prev == kEmptyCtx || prev == word) {
                 t[i].range = range;
                 done = true;
                 break;
@@ -320,9 +325,23 @@ __device__ __forceinline__ void process_entry(const CountParams &P, uint64_t i, 
     int s = 1;
     while (i + s < e && (__ldg(P.qkeys + i + s) >> P.obj_bits) == ctx)
         ++s;
-    uint32_t pb, pc;
-    if (!table_lookup(P.table, P.mask, ctx, pb, pc))
+    unsigned long long payload;
+    bool single;
+    if (!table_lookup(P.table, P.mask, ctx, payload, single))
         return;
+    if (single) {
+        // the context's only posting, held in the slot: one gid run of one object
+        const uint32_t gid = (uint32_t)(payload >> 32);
+        if (LOWER && (int)gid >= qgid)
+            return;
+        const uint32_t q0 = (uint32_t)(P.qkeys[i] & objmask);
+        const int d = min_diff_obj((uint32_t)payload, q0, s, P.qkeys + i, objmask, kMinInit);
+        acc.add(gid, d);
+        if (UNIQUE)
+            uacc.add(gid, d);
+        return;
+    }
+    const uint32_t pb = (uint32_t)payload, pc = (uint32_t)(payload >> 32);
     walk_context<LOWER, UNIQUE>(P.post, pb, pb + pc, P.qkeys + i, s, objmask, qgid, P.ignoreconflict, acc, uacc);
 }
 
@@ -406,41 +425,102 @@ __global__ void __launch_bounds__(256) k_count_plain(CountParams P, int q)
 // Plan-time classes of a context group.
 enum : uint32_t { kJoinSmallMax = 32 };
 
-// Classify groups with >= 2 postings; append (begin | k << 32) to the small
-// (k <= 32, one gid per posting), big (k > 32) or conflict (a gid holds several
-// objects) list.  Totals: [0] postings in listed groups, [1] pairs.
-__global__ void k_self_classify(const uint32_t *__restrict__ gbeg, uint64_t u, const uint64_t *__restrict__ post,
-                                unsigned long long *__restrict__ small, unsigned long long *__restrict__ big,
-                                unsigned long long *__restrict__ conf, unsigned int *__restrict__ counts,
-                                unsigned long long *__restrict__ totals)
+// Warp-aggregated append of this lane's item when `want` (all 32 lanes call it).
+__device__ __forceinline__ uint32_t warp_slot(unsigned int *counter, bool want, unsigned lane)
 {
-    for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < u; g += (uint64_t)gridDim.x * blockDim.x) {
-        const uint32_t b = gbeg[g], e = gbeg[g + 1], k = e - b;
-        if (k < 2)
-            continue;
-        bool conflict = false;
-        uint32_t prev = (uint32_t)(post[b] >> 32);
-        for (uint32_t i = b + 1; i < e; ++i) {
-            const uint32_t gid = (uint32_t)(post[i] >> 32);
-            conflict |= gid == prev;
-            prev = gid;
+    const unsigned m = __ballot_sync(0xffffffffu, want);
+    unsigned base = 0;
+    if (m && lane == (unsigned)(__ffs(m) - 1))
+        base = atomicAdd(counter, (unsigned)__popc(m));
+    base = __shfl_sync(0xffffffffu, base, m ? __ffs(m) - 1 : 0);
+    return base + (unsigned)__popc(m & ((1u << lane) - 1u));
+}
+
+// Classify the groups with >= 2 postings (one thread per group, whole warps):
+//   small   (k <= 32, one object per gid) -> (sort key, group) for the compact plan;
+//             key = (32 - k, gid0, gid1, gid2 >> 2) so equal-size groups over the same
+//             genomes end up side by side
+//   big     (k > 32, one object per gid)  -> begin | k << 32
+//   conflict (a gid holds several objects) -> begin | k << 32
+// totals: [0] postings in listed groups, [1] pairs.
+__global__ void __launch_bounds__(256) k_self_classify(const uint32_t *__restrict__ gbeg, uint64_t u,
+                                                       const uint64_t *__restrict__ post,
+                                                       unsigned long long *__restrict__ skey,
+                                                       uint32_t *__restrict__ sval,
+                                                       unsigned long long *__restrict__ big,
+                                                       unsigned long long *__restrict__ conf,
+                                                       unsigned int *__restrict__ counts,
+                                                       unsigned long long *__restrict__ totals)
+{
+    const uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    const unsigned lane = threadIdx.x & 31;
+    uint32_t b = 0, k = 0;
+    bool conflict = false;
+    unsigned long long key = 0;
+    if (g < u) {
+        b = gbeg[g];
+        k = gbeg[g + 1] - b;
+        if (k >= 2) {
+            uint32_t prev = (uint32_t)(post[b] >> 32);
+            const uint32_t g0 = prev, g1 = (uint32_t)(post[b + 1] >> 32);
+            const uint32_t g2 = k >= 3 ? (uint32_t)(post[b + 2] >> 32) : 0u;
+            for (uint32_t i = b + 1; i < b + k; ++i) {
+                const uint32_t gid = (uint32_t)(post[i] >> 32);
+                conflict |= gid == prev;
+                prev = gid;
+            }
+            key = ((unsigned long long)(kJoinSmallMax - min(k, kJoinSmallMax)) << 58) |
+                  ((unsigned long long)g0 << 38) | ((unsigned long long)g1 << 18) | (g2 >> 2);
+        } else {
+            k = 0;
         }
-        const unsigned long long item = (unsigned long long)b | ((unsigned long long)k << 32);
-        if (conflict)
-            conf[atomicAdd(counts + 2, 1u)] = item;
-        else if (k <= kJoinSmallMax)
-            small[atomicAdd(counts + 0, 1u)] = item;
-        else
-            big[atomicAdd(counts + 1, 1u)] = item;
-        atomicAdd(totals + 0, (unsigned long long)k);
-        atomicAdd(totals + 1, (unsigned long long)k * (k - 1) / 2);
+    }
+    const bool is_small = k >= 2 && !conflict && k <= kJoinSmallMax;
+    const bool is_big = k > kJoinSmallMax && !conflict;
+    const bool is_conf = k >= 2 && conflict;
+    const uint32_t s0 = warp_slot(counts + 0, is_small, lane);
+    const uint32_t s1 = warp_slot(counts + 1, is_big, lane);
+    const uint32_t s2 = warp_slot(counts + 2, is_conf, lane);
+    const unsigned long long item = (unsigned long long)b | ((unsigned long long)k << 32);
+    if (is_small) {
+        skey[s0] = key;
+        sval[s0] = (uint32_t)g;
+    }
+    if (is_big)
+        big[s1] = item;
+    if (is_conf)
+        conf[s2] = item;
+    unsigned long long np = k, npairs = k >= 2 ? (unsigned long long)k * (k - 1) / 2 : 0ull;
+    for (int o = 16; o; o >>= 1) {
+        np += __shfl_down_sync(0xffffffffu, np, o);
+        npairs += __shfl_down_sync(0xffffffffu, npairs, o);
+    }
+    if (lane == 0 && np) {
+        atomicAdd(totals + 0, np);
+        atomicAdd(totals + 1, npairs);
     }
 }
 
-__global__ void k_small_keys(const unsigned long long *__restrict__ items, uint32_t n, uint32_t *__restrict__ keys)
+// sizes of the sorted small groups, for the offsets of the compact posting array
+__global__ void k_self_sizes(const uint32_t *__restrict__ sval, uint32_t n, const uint32_t *__restrict__ gbeg,
+                             uint32_t *__restrict__ ks)
 {
     for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
-        keys[t] = kJoinSmallMax - (uint32_t)(items[t] >> 32);
+        ks[t] = gbeg[sval[t] + 1] - gbeg[sval[t]];
+}
+
+// descriptor (offset | k << 32) and the group's postings copied to jp[offset ..)
+__global__ void k_self_gather(const uint32_t *__restrict__ sval, const uint32_t *__restrict__ ks,
+                              const uint32_t *__restrict__ offs, uint32_t n, const uint32_t *__restrict__ gbeg,
+                              const uint64_t *__restrict__ post, unsigned long long *__restrict__ desc,
+                              uint64_t *__restrict__ jp)
+{
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        const uint32_t b = gbeg[sval[t]], k = ks[t], o = offs[t];
+        desc[t] = (unsigned long long)o | ((unsigned long long)k << 32);
+        for (uint32_t i = 0; i < k; ++i)
+            jp[o + i] = post[b + i];
+    }
 }
 
 __device__ __forceinline__ size_t lower_cell(uint32_t row, uint32_t col) { return (size_t)row * (row - 1) / 2 + col; }
@@ -455,22 +535,62 @@ __device__ __forceinline__ void join_pair(uint64_t pi, uint64_t pj, unsigned lon
         atomicAdd(oo + cell, inc_obj(d));
 }
 
-// One thread per small group (list sorted by size so warps stay balanced):
-// every pair i < j of its postings credits cell (gid_j, gid_i).
-__global__ void __launch_bounds__(256) k_self_small(const unsigned long long *__restrict__ list, uint32_t n,
-                                                    const uint64_t *__restrict__ post,
+// One thread per small group of the compact plan; the warp steps through pair
+// slots in lockstep (groups sorted by size, so lanes carry equal work) and, at
+// every step, lanes holding the same counter cell as their neighbours add their
+// increments with a segmented warp scan: one atomic per run of equal cells.
+__global__ void __launch_bounds__(256) k_self_small(const unsigned long long *__restrict__ desc, uint32_t n,
+                                                    const uint64_t *__restrict__ jp,
                                                     unsigned long long *__restrict__ oc,
                                                     unsigned long long *__restrict__ oo)
 {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n)
-        return;
-    const unsigned long long item = __ldg(list + t);
-    const uint32_t b = (uint32_t)item, k = (uint32_t)(item >> 32);
-    for (uint32_t j = 1; j < k; ++j) {
-        const uint64_t pj = __ldg(post + b + j);
-        for (uint32_t i = 0; i < j; ++i)
-            join_pair(__ldg(post + b + i), pj, oc, oo);
+    const unsigned lane = threadIdx.x & 31;
+    uint32_t off = 0, k = 0;
+    if (t < n) {
+        const unsigned long long d = __ldg(desc + t);
+        off = (uint32_t)d;
+        k = (uint32_t)(d >> 32);
+    }
+    const uint32_t npairs = k >= 2 ? k * (k - 1) / 2 : 0u;
+    const uint32_t maxp = __reduce_max_sync(0xffffffffu, npairs);
+    uint32_t j = 1, i = 0;
+    uint64_t pj = npairs ? __ldg(jp + off + 1) : 0ull;
+    const unsigned below = (1u << lane) - 1u;
+    for (uint32_t p = 0; p < maxp; ++p) {
+        const bool act = p < npairs;
+        unsigned long long cell = ~0ull - lane;  // inactive lanes never join a run
+        unsigned long long ic = 0, io = 0;
+        if (act) {
+            const uint64_t pi = __ldg(jp + off + i);
+            const int d = min(kMinInit, dna_pop((uint32_t)pi ^ (uint32_t)pj));
+            cell = lower_cell((uint32_t)(pj >> 32), (uint32_t)(pi >> 32));
+            ic = inc_ctx(d);
+            io = d ? inc_obj(d) : 0ull;
+            if (++i == j) {
+                i = 0;
+                if (++j < k)
+                    pj = __ldg(jp + off + j);
+            }
+        }
+        const unsigned long long prev = __shfl_up_sync(0xffffffffu, cell, 1);
+        const unsigned heads = __ballot_sync(0xffffffffu, lane == 0 || prev != cell);
+        const int seg_start = 31 - __clz(heads & (below | (1u << lane)));
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned long long uc = __shfl_up_sync(0xffffffffu, ic, o);
+            const unsigned long long uo = __shfl_up_sync(0xffffffffu, io, o);
+            if ((int)lane - o >= seg_start) {
+                ic += uc;
+                io += uo;
+            }
+        }
+        const bool tail = lane == 31 || ((heads >> (lane + 1)) & 1u);
+        if (act && tail) {
+            atomicAdd(oc + cell, ic);
+            if (io)
+                atomicAdd(oo + cell, io);
+        }
     }
 }
 
@@ -589,8 +709,10 @@ struct kssdgpu_index {
     DevBuf<uint64_t> s_keys, s_offs;
     DevBuf<unsigned long long> s_out;
     DevBuf<int> s_order;
-    // self-join plan: group lists (begin | k << 32) by class
+    // self-join plan: compact small groups (descriptor offset | k << 32 into j_post),
+    // big and conflict groups (begin | k << 32 into post)
     DevBuf<unsigned long long> j_small, j_big, j_conf;
+    DevBuf<uint64_t> j_post;
     uint32_t j_n[3] = {0, 0, 0};
     unsigned long long j_postings = 0, j_pairs = 0;
     bool j_ready = false;
@@ -626,7 +748,8 @@ int finish_build(kssdgpu_index *ix, uint32_t *head, unsigned long long *ctx_of, 
     ix->mask = (uint32_t)(cap - 1);
     CUDA_TRY(cudaMalloc(&ix->table, cap * sizeof(Slot)));
     CUDA_TRY(cudaMemsetAsync(ix->table, 0xFF, cap * sizeof(Slot), st));
-    k_table_insert<<<grid_for(ix->u), 256, 0, st>>>(ix->gkey, ix->gbeg, ix->u, ix->table, ix->mask, ix->err);
+    k_table_insert<<<grid_for(ix->u), 256, 0, st>>>(ix->gkey, ix->gbeg, ix->u, ix->post, ix->table, ix->mask,
+                                                     ix->err);
     count_launch();
     CUDA_TRY(cudaStreamSynchronize(st));
     cudaFree(tmp);
@@ -839,52 +962,74 @@ int self_plan(kssdgpu_index *ix, cudaStream_t st)
     if (ix->j_ready)
         return KSSDGPU_OK;
     const uint64_t u = ix->u;
-    const uint64_t cap = std::max<uint64_t>(u, 1);
-    CUDA_TRY(ix->j_small.ensure(cap));
+    const uint64_t cap = std::max<uint64_t>(ix->n / 2 + 1, 1);  // a listed group holds >= 2 postings
     CUDA_TRY(ix->j_big.ensure(cap));
     CUDA_TRY(ix->j_conf.ensure(cap));
+    unsigned long long *skey = nullptr, *skey2 = nullptr;
+    uint32_t *sval = nullptr, *sval2 = nullptr, *ks = nullptr, *offs = nullptr;
     unsigned int *cnt = nullptr;
     unsigned long long *tot = nullptr;
-    CUDA_TRY(cudaMalloc(&cnt, 3 * sizeof(unsigned int)));
-    CUDA_TRY(cudaMalloc(&tot, 2 * sizeof(unsigned long long)));
-    CUDA_TRY(cudaMemsetAsync(cnt, 0, 3 * sizeof(unsigned int), st));
-    CUDA_TRY(cudaMemsetAsync(tot, 0, 2 * sizeof(unsigned long long), st));
+    void *tmp = nullptr;
+    auto cleanup = [&]() {
+        cudaFree(skey); cudaFree(skey2); cudaFree(sval); cudaFree(sval2);
+        cudaFree(ks); cudaFree(offs); cudaFree(cnt); cudaFree(tot); cudaFree(tmp);
+    };
+    cudaError_t e = cudaMalloc(&skey, cap * 8);
+    if (e == cudaSuccess) e = cudaMalloc(&sval, cap * 4);
+    if (e == cudaSuccess) e = cudaMalloc(&cnt, 3 * sizeof(unsigned int));
+    if (e == cudaSuccess) e = cudaMalloc(&tot, 2 * sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMemsetAsync(cnt, 0, 3 * sizeof(unsigned int), st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(tot, 0, 2 * sizeof(unsigned long long), st);
+    if (e != cudaSuccess) {
+        cleanup();
+        return fail(KSSDGPU_ERR_NOMEM, std::string("self-join plan: ") + cudaGetErrorString(e));
+    }
     if (u) {
-        k_self_classify<<<grid_for(u), 256, 0, st>>>(ix->gbeg, u, ix->post, ix->j_small.p, ix->j_big.p, ix->j_conf.p,
-                                                     cnt, tot);
+        k_self_classify<<<(unsigned)((u + 255) / 256), 256, 0, st>>>(ix->gbeg, u, ix->post, skey, sval, ix->j_big.p,
+                                                                     ix->j_conf.p, cnt, tot);
         count_launch();
     }
     unsigned int hc[3];
     unsigned long long ht[2];
-    CUDA_TRY(cudaMemcpyAsync(hc, cnt, sizeof hc, cudaMemcpyDeviceToHost, st));
-    CUDA_TRY(cudaMemcpyAsync(ht, tot, sizeof ht, cudaMemcpyDeviceToHost, st));
-    CUDA_TRY(cudaStreamSynchronize(st));
-    cudaFree(cnt);
-    cudaFree(tot);
-    // small groups sorted by size (descending) so a warp's threads do equal work;
-    // the key is (32 - k) over 6 bits
-    if (hc[0] > 1) {
-        const uint32_t n = hc[0];
-        uint32_t *keys = nullptr, *keys2 = nullptr;
-        unsigned long long *vals2 = nullptr;
-        void *tmp = nullptr;
-        size_t tb = 0;
-        CUDA_TRY(cudaMalloc(&keys, n * 4ull));
-        CUDA_TRY(cudaMalloc(&keys2, n * 4ull));
-        CUDA_TRY(cudaMalloc(&vals2, n * 8ull));
-        k_small_keys<<<grid_for(n), 256, 0, st>>>(ix->j_small.p, n, keys);
-        count_launch();
-        CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, tb, keys, keys2, ix->j_small.p, vals2, n, 0, 6, st));
-        CUDA_TRY(cudaMalloc(&tmp, std::max<size_t>(tb, 1)));
-        CUDA_TRY(cub::DeviceRadixSort::SortPairs(tmp, tb, keys, keys2, ix->j_small.p, vals2, n, 0, 6, st));
-        count_launch();
-        CUDA_TRY(cudaMemcpyAsync(ix->j_small.p, vals2, n * 8ull, cudaMemcpyDeviceToDevice, st));
-        CUDA_TRY(cudaStreamSynchronize(st));
-        cudaFree(keys);
-        cudaFree(keys2);
-        cudaFree(vals2);
-        cudaFree(tmp);
+    e = cudaMemcpyAsync(hc, cnt, sizeof hc, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(ht, tot, sizeof ht, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    const uint32_t n = e == cudaSuccess ? hc[0] : 0;
+    // small groups: sort by (size desc, leading gids), then lay their postings out contiguously
+    if (e == cudaSuccess && n) {
+        e = cudaMalloc(&skey2, (size_t)n * 8);
+        if (e == cudaSuccess) e = cudaMalloc(&sval2, (size_t)n * 4);
+        if (e == cudaSuccess) e = cudaMalloc(&ks, (size_t)n * 4);
+        if (e == cudaSuccess) e = cudaMalloc(&offs, (size_t)n * 4);
+        size_t tb = 0, tb2 = 0;
+        if (e == cudaSuccess) e = cub::DeviceRadixSort::SortPairs(nullptr, tb, skey, skey2, sval, sval2, n, 0, 64, st);
+        if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(nullptr, tb2, ks, offs, n, st);
+        if (e == cudaSuccess) e = cudaMalloc(&tmp, std::max<size_t>(std::max(tb, tb2), 1));
+        if (e == cudaSuccess) e = cub::DeviceRadixSort::SortPairs(tmp, tb, skey, skey2, sval, sval2, n, 0, 64, st);
+        count_launch(8);
+        if (e == cudaSuccess) {
+            k_self_sizes<<<grid_for(n), 256, 0, st>>>(sval2, n, ix->gbeg, ks);
+            count_launch();
+            e = cub::DeviceScan::ExclusiveSum(tmp, tb2, ks, offs, n, st);
+            count_launch(2);
+        }
+        uint32_t last_off = 0, last_k = 0;
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&last_off, offs + n - 1, 4, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&last_k, ks + n - 1, 4, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e == cudaSuccess) e = ix->j_small.ensure(n);
+        if (e == cudaSuccess) e = ix->j_post.ensure((size_t)last_off + last_k);
+        if (e == cudaSuccess) {
+            k_self_gather<<<grid_for(n), 256, 0, st>>>(sval2, ks, offs, n, ix->gbeg, ix->post, ix->j_small.p,
+                                                       ix->j_post.p);
+            count_launch();
+            e = cudaStreamSynchronize(st);
+        }
     }
+    cleanup();
+    if (e != cudaSuccess)
+        return fail(e == cudaErrorMemoryAllocation ? KSSDGPU_ERR_NOMEM : KSSDGPU_ERR_CUDA,
+                    std::string("self-join plan: ") + cudaGetErrorString(e));
     ix->j_n[0] = hc[0];
     ix->j_n[1] = hc[1];
     ix->j_n[2] = hc[2];
@@ -905,7 +1050,7 @@ int self_lower_dev_impl(kssdgpu_index *ix, unsigned flags, unsigned long long *o
         CUDA_TRY(cudaMemsetAsync(oo, 0, std::max<size_t>(cells, 1) * 8, st));
     }
     if (ix->j_n[0]) {
-        k_self_small<<<(ix->j_n[0] + 255) / 256, 256, 0, st>>>(ix->j_small.p, ix->j_n[0], ix->post, oc, oo);
+        k_self_small<<<(ix->j_n[0] + 255) / 256, 256, 0, st>>>(ix->j_small.p, ix->j_n[0], ix->j_post.p, oc, oo);
         count_launch();
     }
     if (ix->j_n[1]) {
@@ -1141,6 +1286,7 @@ void kssdgpu_index_free(kssdgpu_index_t *ix)
     ix->s_out.release();
     ix->s_order.release();
     ix->j_small.release();
+    ix->j_post.release();
     ix->j_big.release();
     ix->j_conf.release();
     delete ix;
