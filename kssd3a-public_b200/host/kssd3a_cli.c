@@ -306,7 +306,8 @@ static struct argp k_argp = {
     k_opts, parse_ani,
     "[-r REF_SKETCH -q QRY | -r REF_SKETCH --qraw RAW_QRY | SELF_SKETCH with -m1/-m2]",
     "\nEstimate average nucleotide identity (ANI) between sketches; shared-context counting on the GPU."
-    "\vOutputs are byte-identical to the reference `kssd3a ani` on the same sketch directories."};
+    "\vOutputs are byte-identical to the reference `kssd3a ani` on the same sketch directories.",
+    NULL, NULL, NULL};
 
 /* ------------------------------------------------------------------ helpers */
 
@@ -841,8 +842,8 @@ static void write_index_files(const char *dir, kssdgpu_index_t *ix, uint64_t n)
 /* Lower-triangle counters of a self sketch: with an index file, the reference's
  * index (probe kernel over query blocks); without, the self join over the index the
  * device builds from the sketch. */
-static void self_lower_counts(const kssd_sketch_t *s, const char *dir, bool index_file, kssdgpu_ctx_mut2_t **pc,
-                              kssdgpu_obj_section_t **po)
+static void self_lower_counts(const kssd_sketch_t *s, const char *dir, bool index_file, bool forced_needs_file,
+                              kssdgpu_ctx_mut2_t **pc, kssdgpu_obj_section_t **po)
 {
     const int n = s->n;
     const size_t cells = (size_t)n * (n - 1) / 2;
@@ -883,7 +884,7 @@ static void self_lower_counts(const kssd_sketch_t *s, const char *dir, bool inde
         }
         kssdgpu_index_free(ix);
     } else {
-        if (force_ref_index())
+        if (forced_needs_file && force_ref_index())
             errx(EXIT_FAILURE, "KSSD3A_FORCE_REF_INDEX requires reference index '%s/%s'", dir,
                  "sortedcomb_ctxgid64obj32");
         kssdgpu_index_t *ix = gpu_index_of_sketch(s);
@@ -1030,7 +1031,7 @@ static int run_self(int kind)
     }
     kssdgpu_ctx_mut2_t *lc = NULL;
     kssdgpu_obj_section_t *lo = NULL;
-    self_lower_counts(s, g.qrydir, index_file, &lc, &lo);
+    self_lower_counts(s, g.qrydir, index_file, kind != 2, &lc, &lo);
     double *m = self_lower_metrics(s, lc, lo);
     free(lc);
     free(lo);
@@ -1333,6 +1334,523 @@ static int cmd_ani(int argc, char **argv)
     return 0;
 }
 
+/* ------------------------------------------------------------------ `kssd3a matrix`
+ * Full and triangle reports of one sketch (matrix_write_indexed_self_matrix,
+ * src/command_matrix.c:439-619) and the rectangular full report
+ * (matrix_compute_dense, :258-315); options and validation of
+ * src/command_matrix_wrapper.c:53-533.  The sparse graph formats (edges, clusters,
+ * dedup-plan), --query-sketch-list and the legacy --ani matrix are not part of the
+ * counting engine and are rejected. */
+
+enum { MF_AUTO = 0, MF_FULL, MF_TRIANGLE, MF_EDGES, MF_CLUSTERS, MF_DEDUP };
+enum { MM_MOE = 0, MM_NAIVE, MM_PDIST, MM_MASH, MM_AAF };
+
+typedef struct matrix_cli {
+    int metric, metric_count, format, phylip, d, threads;
+    double e, diag;
+    bool cut_set, ani;
+    char refdir[PATHLEN], qrydir[PATHLEN], qrylist[PATHLEN], outf[PATHLEN], gl[PATHLEN], idmap[PATHLEN];
+    char edge_out[PATHLEN], keep_out[PATHLEN], remove_out[PATHLEN], keep_matrix_out[PATHLEN], keep_idmap[PATHLEN];
+    int keep_matrix_fmt, dedup_seen, nrem;
+    char **rem;
+} matrix_cli_t;
+
+static matrix_cli_t gm;
+
+enum {
+    MK_FORMAT = 900, MK_SPARSE, MK_CUT, MK_MAX_AFCUT, MK_CTXCUT, MK_DIAG_VALUE, MK_EDGE_OUT, MK_KEEP_OUT, MK_REMOVE_OUT,
+    MK_MATRIX_FORMAT, MK_MATRIX_IDMAP, MK_KEEP_MATRIX_OUT, MK_KEEP_MATRIX_FORMAT, MK_KEEP_MATRIX_IDMAP,
+    MK_MAX_CTX_FREQ, MK_MIN_VOTES, MK_SAMPLE_STEP, MK_QUERY_LIST, MK_PROGRESS, MK_DEDUP
+};
+
+static struct argp_option k_matrix_opts[] = {
+    {"ref", 'r', "<DIR>", 0, "Reference sketches. Omit for triangle mode.", 9},
+    {"query", 'q', "<DIR>", 0, "Query sketches.", 1},
+    {"query-sketch-list", MK_QUERY_LIST, "<FILE>", 0, "Query sketch directories, one per line (not in this build).", 1},
+    {"metric", 'm', "<METRIC>", 0, "ctx-moe, ctx-naive, p_dist, mash, or aaf; 0/1 alias mash/aaf. [ctx-naive]", 2},
+    {"format", MK_FORMAT, "<FORMAT>", 0, "full or triangle (edges, clusters and dedup-plan are not in this build). "
+                                         "[full for -r/-q; triangle for one sketch]", 2},
+    {"sparse", MK_SPARSE, 0, 0, "Alias for --format edges (not in this build).", 2},
+    {"cut", MK_CUT, "<FLOAT>", 0, "Distance cutoff for sparse reports.", 3},
+    {"dedup-strategy", MK_DEDUP, "<greedy|full-linkage>", 0, "Dedup-plan grouping strategy.", 3},
+    {"control", 'c', "<FLOAT>", OPTION_HIDDEN, "Compatibility alias for --cut.", 3},
+    {"max-afcut", MK_MAX_AFCUT, "<FLOAT>", 0, "Minimum max align fraction for sparse edges.", 3},
+    {"ctxcut", MK_CTXCUT, "<INT>", 0, "Minimum shared context count for sparse edges.", 3},
+    {"index-max-ctx-freq", MK_MAX_CTX_FREQ, "<INT>", 0, "Indexed sparse candidate mode option.", 3},
+    {"index-min-votes", MK_MIN_VOTES, "<INT>", 0, "Indexed sparse candidate mode option.", 3},
+    {"index-sample-step", MK_SAMPLE_STEP, "<INT>", 0, "Indexed sparse candidate mode option.", 3},
+    {"progress", MK_PROGRESS, "<auto|on|off>", 0, "Progress on stderr (accepted; no progress is printed).", 3},
+    {"glist", 'g', "<FILE>", 0, "Sample output file for KSSD set grouping.", 4},
+    {"outfile", 'o', "<FILE>", 0, "Matrix output file. [STDOUT]", 5},
+    {"matrix-format", MK_MATRIX_FORMAT, "<tsv|phylip>", 0, "Output format for --format full. [tsv]", 5},
+    {"matrix-idmap", MK_MATRIX_IDMAP, "<FILE>", 0, "With --matrix-format phylip, write short-ID to sample-name map.", 5},
+    {"edge-out", MK_EDGE_OUT, "<FILE>", 0, "Sparse edge TSV (not in this build).", 5},
+    {"keep-out", MK_KEEP_OUT, "<FILE>", 0, "Dedup-plan output (not in this build).", 5},
+    {"remove-out", MK_REMOVE_OUT, "<FILE>", 0, "Dedup-plan output (not in this build).", 5},
+    {"keep-matrix-out", MK_KEEP_MATRIX_OUT, "<FILE>", 0, "Dedup-plan output (not in this build).", 5},
+    {"keep-matrix-format", MK_KEEP_MATRIX_FORMAT, "<tsv|phylip>", 0, "Dedup-plan output format.", 5},
+    {"keep-matrix-idmap", MK_KEEP_MATRIX_IDMAP, "<FILE>", 0, "Dedup-plan id map.", 5},
+    {"threads", 'p', "<INT>", 0, "Number of host threads to use.", 6},
+    {"diagonal", 'd', 0, 0, "Print diagonal values in triangle mode. [0]", 7},
+    {"diagonal-value", MK_DIAG_VALUE, "<FLOAT>", 0, "Set diagonal value and enable diagonal output.", 7},
+    {"exception", 'e', "<FLOAT>", 0, "Distance value to use when XnY == 0. [1]", 8},
+    {"ani", 'n', 0, OPTION_HIDDEN, "Use context-object ANI mode.", 9},
+    {0}};
+
+static double parse_nonneg(struct argp_state *st, const char *name, const char *arg)
+{
+    char *end = NULL;
+    errno = 0;
+    double v = strtod(arg, &end);
+    if (errno || end == arg || *end || !isfinite(v) || v < 0.0)
+        argp_error(st, "%s requires a non-negative number", name);
+    return v;
+}
+
+static bool matrix_metric_from(const char *arg, int *m)
+{
+    /* pairwise_metric_from_string, src/pairwise_graph.c:70-99 */
+    static const struct { const char *name; int m; } names[] = {
+        {"ctx-moe", MM_MOE}, {"moe", MM_MOE}, {"ctx-naive", MM_NAIVE}, {"naive", MM_NAIVE}, {"p_dist", MM_PDIST},
+        {"pdist", MM_PDIST}, {"p-distance", MM_PDIST}, {"micro-obj", MM_PDIST}, {"micro_obj_rate", MM_PDIST},
+        {"mash", MM_MASH}, {"mashd", MM_MASH}, {"0", MM_MASH}, {"aaf", MM_AAF}, {"aafd", MM_AAF}, {"1", MM_AAF}};
+    for (size_t i = 0; i < sizeof names / sizeof names[0]; ++i)
+        if (!strcmp(arg, names[i].name)) {
+            *m = names[i].m;
+            return true;
+        }
+    return false;
+}
+
+static error_t parse_matrix(int key, char *arg, struct argp_state *st)
+{
+    switch (key) {
+    case 'm': {
+        /* whitespace-free metric, or an A&B / A|B expression of such */
+        char compact[128];
+        size_t n = 0;
+        for (const char *p = arg; *p; ++p)
+            if (*p != ' ' && *p != '\t' && *p != '\n' && *p != '\r' && n + 1 < sizeof compact)
+                compact[n++] = *p;
+        compact[n] = '\0';
+        int count = 0, m = 0;
+        const bool has_and = strchr(compact, '&') != NULL, has_or = strchr(compact, '|') != NULL;
+        bool ok = n > 0 && !(has_and && has_or);
+        if (ok) {
+            const char *delim = has_and ? "&" : (has_or ? "|" : "");
+            if ((has_and || has_or) && (compact[0] == delim[0] || compact[n - 1] == delim[0] || strstr(compact, has_and ? "&&" : "||")))
+                ok = false;
+            char *save = NULL;
+            for (char *tok = (has_and || has_or) ? strtok_r(compact, delim, &save) : compact; ok && tok;
+                 tok = (has_and || has_or) ? strtok_r(NULL, delim, &save) : NULL) {
+                int mm;
+                if (count >= 5 || !matrix_metric_from(tok, &mm))
+                    ok = false;
+                else if (count++ == 0)
+                    m = mm;
+            }
+        }
+        if (!ok || count == 0)
+            argp_error(st, "-m/--metric must be one metric such as ctx-naive, p_dist, mash, or aaf, or an expression "
+                           "like 'ctx-naive&aaf' or 'ctx-moe|mash'");
+        gm.metric = m;
+        gm.metric_count = count;
+        break;
+    }
+    case MK_FORMAT:
+        if (!strcmp(arg, "full") || !strcmp(arg, "matrix")) gm.format = MF_FULL;
+        else if (!strcmp(arg, "triangle") || !strcmp(arg, "tri")) gm.format = MF_TRIANGLE;
+        else if (!strcmp(arg, "edges") || !strcmp(arg, "edge") || !strcmp(arg, "sparse")) gm.format = MF_EDGES;
+        else if (!strcmp(arg, "clusters") || !strcmp(arg, "cluster") || !strcmp(arg, "components")) gm.format = MF_CLUSTERS;
+        else if (!strcmp(arg, "dedup-plan") || !strcmp(arg, "dedup")) gm.format = MF_DEDUP;
+        else argp_error(st, "--format must be one of full, triangle, edges/sparse, clusters, or dedup-plan");
+        break;
+    case MK_SPARSE: gm.format = MF_EDGES; break;
+    case 'c':
+    case MK_CUT: parse_nonneg(st, "--cut", arg); gm.cut_set = true; break;
+    case MK_MAX_AFCUT: parse_double_range(st, "--max-afcut", arg, 0.0, 1.0); break;
+    case MK_CTXCUT: parse_int_range(st, "--ctxcut", arg, 0, INT32_MAX); break;
+    case MK_MAX_CTX_FREQ: parse_int_range(st, "--index-max-ctx-freq", arg, 0, INT32_MAX); break;
+    case MK_MIN_VOTES: parse_int_range(st, "--index-min-votes", arg, 1, INT32_MAX); break;
+    case MK_SAMPLE_STEP: parse_int_range(st, "--index-sample-step", arg, 1, INT32_MAX); break;
+    case MK_PROGRESS:
+        if (strcmp(arg, "auto") && strcmp(arg, "on") && strcmp(arg, "off"))
+            argp_error(st, "--progress must be auto, on, or off");
+        break;
+    case MK_DEDUP: gm.dedup_seen = 1; break;
+    case 'e': gm.e = parse_nonneg(st, "-e/--exception", arg); break;
+    case 'p': gm.threads = parse_int_range(st, "-p/--threads", arg, 1, 65536); break;
+    case 'q': copy_path(st, "-q/--query", gm.qrydir, arg); break;
+    case MK_QUERY_LIST: copy_path(st, "--query-sketch-list", gm.qrylist, arg); break;
+    case 'r': copy_path(st, "-r/--ref", gm.refdir, arg); break;
+    case 'o': copy_path(st, "-o/--outfile", gm.outf, arg); break;
+    case 'g': copy_path(st, "-g/--glist", gm.gl, arg); break;
+    case MK_EDGE_OUT: copy_path(st, "--edge-out", gm.edge_out, arg); break;
+    case MK_KEEP_OUT: copy_path(st, "--keep-out", gm.keep_out, arg); break;
+    case MK_REMOVE_OUT: copy_path(st, "--remove-out", gm.remove_out, arg); break;
+    case MK_MATRIX_FORMAT:
+    case MK_KEEP_MATRIX_FORMAT: {
+        int ph;
+        if (!strcmp(arg, "tsv") || !strcmp(arg, "table")) ph = 0;
+        else if (!strcmp(arg, "phylip") || !strcmp(arg, "phy")) ph = 1;
+        else { argp_error(st, "matrix format must be tsv or phylip"); ph = 0; }
+        if (key == MK_MATRIX_FORMAT) gm.phylip = ph; else gm.keep_matrix_fmt = ph;
+        break;
+    }
+    case MK_MATRIX_IDMAP: copy_path(st, "--matrix-idmap", gm.idmap, arg); break;
+    case MK_KEEP_MATRIX_OUT: copy_path(st, "--keep-matrix-out", gm.keep_matrix_out, arg); break;
+    case MK_KEEP_MATRIX_IDMAP: copy_path(st, "--keep-matrix-idmap", gm.keep_idmap, arg); break;
+    case 'd': gm.d = 1; break;
+    case MK_DIAG_VALUE: gm.diag = parse_nonneg(st, "--diagonal-value", arg); gm.d = 1; break;
+    case 'n': gm.ani = true; break;
+    case ARGP_KEY_ARGS:
+        gm.nrem = st->argc - st->next;
+        gm.rem = st->argv + st->next;
+        break;
+    case ARGP_KEY_END: {
+        /* src/command_matrix_wrapper.c:399-430 (the checks that concern full/triangle reports) */
+        if (gm.qrydir[0] && gm.qrylist[0])
+            argp_error(st, "-q/--query and --query-sketch-list are mutually exclusive");
+        if (gm.qrylist[0] && gm.nrem > 0)
+            argp_error(st, "--query-sketch-list cannot be combined with a positional sketch argument");
+        if (!gm.qrydir[0] && !gm.qrylist[0] && gm.nrem == 1)
+            copy_path(st, "sketch", gm.qrydir, gm.rem[0]);
+        else if (gm.nrem > 0)
+            argp_error(st, "matrix accepts at most one positional sketch argument; use -r/-q for rectangular reports");
+        if (!gm.qrydir[0] && !gm.qrylist[0])
+            argp_error(st, "missing sketch input; provide one sketch argument, -q/--query, or --query-sketch-list");
+        if (gm.qrylist[0] && !gm.refdir[0])
+            argp_error(st, "--query-sketch-list requires -r/--ref");
+        if (gm.refdir[0] && gm.format == MF_TRIANGLE)
+            argp_error(st, "--format triangle is only valid for one sketch");
+        const int eff = gm.format != MF_AUTO ? gm.format : (gm.refdir[0] ? MF_FULL : MF_TRIANGLE);
+        if (gm.metric_count > 1 && (eff == MF_FULL || eff == MF_TRIANGLE))
+            argp_error(st, "combined --metric expressions are only valid for --sparse/--format edges, clusters, or "
+                           "dedup-plan");
+        if ((gm.format == MF_EDGES || gm.format == MF_CLUSTERS || gm.format == MF_DEDUP) && !gm.cut_set)
+            argp_error(st, "--sparse/--format edges, clusters, or dedup-plan requires --cut");
+        if ((gm.format == MF_CLUSTERS || gm.format == MF_DEDUP) && gm.refdir[0])
+            argp_error(st, "--format clusters/dedup-plan requires one sketch, not -r/-q");
+        if ((gm.keep_out[0] || gm.remove_out[0] || gm.keep_matrix_out[0] || gm.keep_idmap[0]) && eff != MF_DEDUP)
+            argp_error(st, "--keep-out/--remove-out/--keep-matrix-out/--keep-matrix-idmap require --format dedup-plan");
+        if (gm.dedup_seen && eff != MF_DEDUP)
+            argp_error(st, "--dedup-strategy requires --format dedup-plan");
+        if (gm.phylip && eff != MF_FULL)
+            argp_error(st, "--matrix-format phylip requires --format full");
+        if (gm.phylip && gm.refdir[0])
+            argp_error(st, "--matrix-format phylip requires one square sketch, not -r/-q");
+        if (gm.qrylist[0] && (eff != MF_FULL || gm.ani))
+            argp_error(st, "--query-sketch-list currently supports rectangular --format full without --ani");
+        if (gm.idmap[0] && !gm.phylip)
+            argp_error(st, "--matrix-idmap requires --matrix-format phylip");
+        if (gm.idmap[0] && gm.outf[0] && !strcmp(gm.idmap, gm.outf))
+            argp_error(st, "--matrix-idmap must differ from --outfile");
+        break;
+    }
+    default:
+        return ARGP_ERR_UNKNOWN;
+    }
+    return 0;
+}
+
+static struct argp k_matrix_argp = {k_matrix_opts, parse_matrix, 0,
+                                    "\nReport pairwise sketch distance matrices; shared-context counting on the GPU.",
+                                    NULL, NULL, NULL};
+
+/* matrix_kput_fixed6, src/command_matrix.c:103-124 */
+static void put_fixed6(kssd_buf_t *b, double v)
+{
+    if (!isfinite(v) || v > 900000000000.0 || v < -900000000000.0) {
+        kssd_buf_printf(b, "%lf", v);
+        return;
+    }
+    if (v < 0.0) {
+        kssd_buf_putc(b, '-');
+        v = -v;
+    }
+    const uint64_t scaled = (uint64_t)(v * 1000000.0 + 0.5);
+    uint32_t frac = (uint32_t)(scaled % 1000000ULL);
+    kssd_buf_printf(b, "%ld.", (long)(scaled / 1000000ULL));
+    char f6[7];
+    for (int i = 5; i >= 0; --i) {
+        f6[i] = (char)('0' + frac % 10);
+        frac /= 10;
+    }
+    f6[6] = '\0';
+    kssd_buf_puts(b, f6);
+}
+
+/* matrix_scale_fixed6 / matrix_kput_scaled6, src/command_matrix.c:126-149 */
+static uint32_t scale_u6(double v)
+{
+    if (!isfinite(v))
+        v = 1.0;
+    if (v < 0.0)
+        v = 0.0;
+    if (v > 4294.0)
+        v = 4294.0;
+    return (uint32_t)(v * 1000000.0 + 0.5);
+}
+
+static void put_u6(kssd_buf_t *b, uint32_t scaled)
+{
+    char f6[8];
+    uint32_t frac = scaled % 1000000U;
+    for (int i = 5; i >= 0; --i) {
+        f6[i] = (char)('0' + frac % 10);
+        frac /= 10;
+    }
+    f6[6] = '\0';
+    kssd_buf_printf(b, "%u.%s", scaled / 1000000U, f6);
+}
+
+/* matrix_context_feature_value with one metric, src/command_matrix.c:400-424,621-661 */
+static double matrix_context_value(const kssd_features_t *f, uint32_t qc, uint32_t rc, const kssd_ani_opt_t *o)
+{
+    if (f->XnY_ctx == 0 || qc == 0 || rc == 0)
+        return gm.e;
+    kssd_features_t t = *f;
+    double d;
+    switch (gm.metric) {
+    case MM_NAIVE: d = kssd_naive_dist(&t); break;
+    case MM_MOE: d = kssd_lm3ways_dist(&t, o->drfold); break;
+    case MM_PDIST: d = kssd_p_dist(&t, o->obj_bits); break;
+    case MM_MASH: d = kssd_mashD((uint32_t)(o->ctx_bits / 2), rc, qc, f->XnY_ctx); break;
+    default: d = kssd_aafD((uint32_t)(o->ctx_bits / 2), rc, qc, f->XnY_ctx); break;
+    }
+    if (!isfinite(d))
+        return gm.e;
+    if (d < 0.0) d = 0.0;
+    if (d > 1.0) d = 1.0;
+    return d;
+}
+
+/* pairwise_eval_arrays distances, src/pairwise_graph.c:13-49,301-360 */
+static double clean_dist(double d) { return !isfinite(d) ? 1.0 : (d < 0.0 ? 0.0 : d); }
+
+static double matrix_pair_value(const kssd_features_t *f, uint32_t qc, uint32_t rc, size_t qlen, size_t rlen,
+                                const kssd_ani_opt_t *o)
+{
+    if (qlen == 0 || rlen == 0 || f->XnY_ctx == 0)
+        return gm.e;
+    kssd_features_t t = *f;
+    const int k = o->ctx_bits > 0 ? o->ctx_bits / 2 : 32;
+    switch (gm.metric) {
+    case MM_MASH: {
+        const double denom = (double)qc + (double)rc - (double)f->XnY_ctx;
+        if (denom <= 0.0) return 1.0;
+        const double j = (double)f->XnY_ctx / denom, tr = (2.0 * j) / (1.0 + j);
+        if (tr <= 0.0) return 1.0;
+        return clean_dist(-log(tr) / (double)k);
+    }
+    case MM_AAF: {
+        const uint32_t m = qc < rc ? qc : rc;
+        if (m == 0) return 1.0;
+        const double c = (double)f->XnY_ctx / (double)m;
+        if (c <= 0.0) return 1.0;
+        return clean_dist(-log(c) / (double)k);
+    }
+    case MM_NAIVE: return clean_dist(kssd_naive_dist(&t));
+    case MM_PDIST: return clean_dist(kssd_p_dist(&t, o->obj_bits));
+    default: return clean_dist(kssd_lm3ways_dist(&t, o->drfold));
+    }
+}
+
+static void matrix_glist(const kssd_sketch_t *s)
+{
+    if (!gm.gl[0])
+        return;
+    FILE *f = fopen(gm.gl, "w");
+    if (!f)
+        err(errno, "matrix_write_glist(): Failed to open file:%s\n", gm.gl);
+    for (int i = 0; i < s->n; ++i)
+        fprintf(f, "%d\t%s\n", i + 1, s->names[i]);
+    fclose(f);
+}
+
+static int matrix_self(int fmt)
+{
+    kssd_sketch_t *s = load_sketch(gm.qrydir, 0);
+    init_bits(s);
+    const int n = s->n;
+    g.o.ignoreconflict = false;
+    g.o.p = gm.threads;
+    kssdgpu_ctx_mut2_t *lc = NULL;
+    kssdgpu_obj_section_t *lo = NULL;
+    self_lower_counts(s, gm.qrydir, kssd_file_exists(gm.qrydir, "sortedcomb_ctxgid64obj32"), false, &lc, &lo);
+    uint32_t *cnt = sample_ctx_counts(s, s->stat.conflict, false);
+    const size_t cells = (size_t)n * (n - 1) / 2;
+    double *v = malloc(cells * sizeof(double) + 8);
+    if (!v)
+        err(EXIT_FAILURE, "OOM matrix values");
+#pragma omp parallel for schedule(dynamic, 16) num_threads(gm.threads)
+    for (int q = 1; q < n; ++q) {
+        const size_t base = (size_t)q * (q - 1) / 2;
+        for (int r = 0; r < q; ++r) {
+            kssd_features_t f = feat_of(&lc[base + r], &lo[base + r]);
+            v[base + r] = matrix_context_value(&f, cnt[q], cnt[r], &g.o);
+        }
+    }
+    free(lc);
+    free(lo);
+    FILE *out = open_out(gm.outf);
+    kssd_buf_t h = {0};
+    if (fmt == MF_FULL) {
+        if (gm.phylip) {
+            if (gm.idmap[0]) {
+                FILE *im = open_out(gm.idmap);
+                for (int i = 0; i < n; ++i)
+                    fprintf(im, "S%09d\t%s\n", i + 1, s->names[i]);
+                if (im != stdout)
+                    fclose(im);
+            }
+            kssd_buf_printf(&h, "%d\n", n);
+        } else {
+            for (int r = 0; r < n; ++r) {
+                kssd_buf_putc(&h, '\t');
+                kssd_buf_puts(&h, s->names[r]);
+            }
+            kssd_buf_putc(&h, '\n');
+        }
+        write_buf(out, &h);
+        kssd_buf_free(&h);
+    }
+    const uint32_t diag_u6 = scale_u6(gm.diag);
+    const int chunk = 256;
+    for (int q0 = 0; q0 < n; q0 += chunk) {
+        const int nb = n - q0 < chunk ? n - q0 : chunk;
+        kssd_buf_t *rows = calloc((size_t)nb, sizeof(kssd_buf_t));
+#pragma omp parallel for schedule(dynamic, 1) num_threads(gm.threads)
+        for (int i = 0; i < nb; ++i) {
+            const int q = q0 + i;
+            kssd_buf_t *b = &rows[i];
+            if (fmt == MF_FULL && gm.phylip) {
+                char id[16];
+                snprintf(id, sizeof id, "S%09d", q + 1);
+                kssd_buf_printf(b, "%-10s", id);
+            } else {
+                kssd_buf_puts(b, s->names[q]);
+            }
+            if (fmt == MF_FULL) {
+                for (int r = 0; r < n; ++r) {
+                    uint32_t u = diag_u6;
+                    if (q > r)
+                        u = scale_u6(v[(size_t)q * (q - 1) / 2 + r]);
+                    else if (q < r)
+                        u = scale_u6(v[(size_t)r * (r - 1) / 2 + q]);
+                    kssd_buf_putc(b, gm.phylip ? ' ' : '\t');
+                    put_u6(b, u);
+                }
+            } else {
+                for (int r = 0; r < q; ++r) {
+                    kssd_buf_putc(b, '\t');
+                    put_fixed6(b, v[(size_t)q * (q - 1) / 2 + r]);
+                }
+                if (gm.d) {
+                    kssd_buf_putc(b, '\t');
+                    put_fixed6(b, gm.diag);
+                }
+            }
+            kssd_buf_putc(b, '\n');
+        }
+        for (int i = 0; i < nb; ++i) {
+            write_buf(out, &rows[i]);
+            kssd_buf_free(&rows[i]);
+        }
+        free(rows);
+    }
+    close_out(out);
+    matrix_glist(s);
+    free(v);
+    free(cnt);
+    kssd_sketch_free(s);
+    return 0;
+}
+
+static int matrix_rect(void)
+{
+    kssd_sketch_t *ref = load_sketch(gm.refdir, 0);
+    kssd_sketch_t *qry = load_sketch(gm.qrydir, 0);
+    if (ref->stat.hash_id != qry->stat.hash_id)
+        errx(EXIT_FAILURE, "pairwise_check_compatible(): ref hash_id %u != qry %u", ref->stat.hash_id,
+             qry->stat.hash_id);
+    init_bits(ref);
+    g.o.p = gm.threads;
+    const bool same = !strcmp(gm.refdir, gm.qrydir);
+    uint32_t *qc = sample_ctx_counts(qry, qry->stat.conflict, false);
+    uint32_t *rc = sample_ctx_counts(ref, ref->stat.conflict, false);
+    kssdgpu_index_t *ix = gpu_index_of_sketch(ref);
+    FILE *out = open_out(gm.outf);
+    kssd_buf_t h = {0};
+    for (int r = 0; r < ref->n; ++r) {
+        kssd_buf_putc(&h, '\t');
+        kssd_buf_puts(&h, ref->names[r]);
+    }
+    kssd_buf_putc(&h, '\n');
+    write_buf(out, &h);
+    kssd_buf_free(&h);
+    const int R = ref->n, B = block_for(R, qry->n);
+    for (int q0 = 0; q0 < qry->n; q0 += B) {
+        const int nb = qry->n - q0 < B ? qry->n - q0 : B;
+        counts_t c = count_queries(ix, R, qry, q0, nb, 0);
+        kssd_buf_t *rows = calloc((size_t)nb, sizeof(kssd_buf_t));
+#pragma omp parallel for schedule(dynamic, 1) num_threads(gm.threads)
+        for (int i = 0; i < nb; ++i) {
+            const int q = q0 + i;
+            const size_t qlen = (size_t)(qry->offs[q + 1] - qry->offs[q]);
+            kssd_buf_puts(&rows[i], qry->names[q]);
+            for (int r = 0; r < R; ++r) {
+                double v = gm.diag;
+                if (!(same && q == r)) {
+                    kssd_features_t f = feat_of(&c.ctx[(size_t)i * R + r], &c.obj[(size_t)i * R + r]);
+                    v = matrix_pair_value(&f, qc[q], rc[r], qlen, (size_t)(ref->offs[r + 1] - ref->offs[r]), &g.o);
+                }
+                kssd_buf_printf(&rows[i], "\t%lf", v);
+            }
+            kssd_buf_putc(&rows[i], '\n');
+        }
+        for (int i = 0; i < nb; ++i) {
+            write_buf(out, &rows[i]);
+            kssd_buf_free(&rows[i]);
+        }
+        free(rows);
+        free_counts(&c);
+    }
+    close_out(out);
+    kssdgpu_index_free(ix);
+    free(qc);
+    free(rc);
+    kssd_sketch_free(ref);
+    kssd_sketch_free(qry);
+    return 0;
+}
+
+static int cmd_matrix(int argc, char **argv)
+{
+    memset(&gm, 0, sizeof gm);
+    memset(&g, 0, sizeof g);
+    kssd_opt_defaults(&g.o);
+    gm.metric = MM_NAIVE;
+    gm.metric_count = 1;
+    gm.threads = 1;
+    gm.e = 1.0;
+    argp_parse(&k_matrix_argp, argc, argv, ARGP_IN_ORDER, NULL, NULL);
+    if (gm.qrylist[0])
+        errx(EXIT_FAILURE, "--query-sketch-list is not supported by this build");
+    const int fmt = gm.format != MF_AUTO ? gm.format : (gm.refdir[0] ? MF_FULL : MF_TRIANGLE);
+    if (fmt == MF_EDGES || fmt == MF_CLUSTERS || fmt == MF_DEDUP)
+        errx(EXIT_FAILURE, "sparse matrix formats (edges, clusters, dedup-plan) are not supported by this build");
+    if (gm.refdir[0] && gm.ani)
+        errx(EXIT_FAILURE, "the legacy --ani matrix is not supported by this build; use `kssd3a ani --format matrix`");
+    if (!is_sketch_dir(gm.qrydir) || (gm.refdir[0] && !is_sketch_dir(gm.refdir)))
+        errx(EXIT_FAILURE, "matrix inputs must be sketch directories");
+    if (!gm.refdir[0])
+        return matrix_self(fmt);
+    if (fmt != MF_FULL)
+        errx(EINVAL, "compute_matrix(): --format clusters, dedup-plan, and triangle require one sketch");
+    return matrix_rect();
+}
+
 int main(int argc, char **argv)
 {
     setvbuf(stdout, NULL, _IOFBF, 1 << 20);
@@ -1342,6 +1860,8 @@ int main(int argc, char **argv)
     }
     if (!strcmp(argv[1], "ani"))
         return cmd_ani(argc - 1, argv + 1);
+    if (!strcmp(argv[1], "matrix"))
+        return cmd_matrix(argc - 1, argv + 1);
     if (!strcmp(argv[1], "--version") || !strcmp(argv[1], "-V")) {
         printf("%s\n", argp_program_version);
         return 0;

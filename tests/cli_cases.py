@@ -1,11 +1,12 @@
 """Command-line parity cases shared by tests/test_gpu_cli.py and tests/golden/make_golden.py.
 
 Each case names seeded synthetic sketch directories (generated on demand by the host
-library's sketch-space generator) and an `ani` command line; the reference CLI and
+library's sketch-space generator) and a `kssd3a` command line; the reference CLI and
 bin/kssd3a must print the same bytes.  The cases walk the reference dispatcher
 (src/command_ani_wrapper.c:1082-1230): indexed mem_eff detail/matrix, one- and
 multi-query streams, the no-index hash path, direct and indexed self matrices and
-triangles, the rectangular direct matrix, read sets with --unique-ctx.
+triangles, the rectangular direct matrix, read sets with --unique-ctx; and the
+`matrix` command's one-sketch full/triangle and rectangular full reports.
 """
 import os
 import shutil
@@ -63,6 +64,16 @@ CASES = [
     ("reads_qraw_ignoreconflict", ["ani", "-r", "{refs120i}", "--qraw", "{reads6}", "-n", "0.5", "--ignoreconflict"],
      {}),
     ("reads_qraw_stream", ["ani", "-r", "{refs120}", "--qraw", "{reads6}", "-n", "0.5"], {}),
+    # `kssd3a matrix`: one-sketch full/triangle (indexed self path) and rectangular full (per-pair path)
+    ("matrix_triangle", ["matrix", "{refs40}"], {}),
+    ("matrix_triangle_d_mash", ["matrix", "-q", "{refs120}", "--format", "triangle", "-d", "-m", "mash"], {}),
+    ("matrix_full_moe", ["matrix", "--format", "full", "-m", "ctx-moe", "{refs40}"], {}),
+    ("matrix_full_phylip_pdist", ["matrix", "--format", "full", "--matrix-format", "phylip", "-m", "p_dist",
+                                  "{refs120i}"], {}),
+    ("matrix_full_diag_value", ["matrix", "--format", "full", "--diagonal-value", "0.5", "-m", "1", "{refs40}"], {}),
+    ("matrix_rect_aaf", ["matrix", "-r", "{refs40}", "-q", "{qry8}", "-m", "aaf"], {}),
+    ("matrix_rect_naive_e2", ["matrix", "-r", "{refs120}", "-q", "{qry30}", "-e", "2"], {}),
+    ("matrix_reads_triangle", ["matrix", "-m", "ctx-moe", "-d", "{reads6}"], {}),
 ]
 
 
@@ -76,6 +87,11 @@ def make_fixture(root: str, name: str) -> str:
     sk = kssdgpu.synth(**spec)
     kssdgpu.write_sketch_dir(path, sk, with_index=name in INDEXED)
     return path
+
+
+def with_threads(argv, threads=4):
+    """-p right after the subcommand: positional sketch arguments must come last."""
+    return [argv[0], "-p", str(threads), *argv[1:]]
 
 
 def materialize(root: str, argv, fresh_tag: str):

@@ -80,7 +80,7 @@ def counts_case(name, seed, nref, nq, ctx_space, obj_space, ignoreconflict):
 def cli_cases():
     """stdout of the reference CLI for every tests/cli_cases.py case, gzip-compressed."""
     import gzip
-    from cli_cases import CASES, materialize
+    from cli_cases import CASES, materialize, with_threads
     out_dir = os.path.join(HERE, "cli")
     os.makedirs(out_dir, exist_ok=True)
     root = tempfile.mkdtemp(prefix="golden-cli-")
@@ -88,7 +88,7 @@ def cli_cases():
         for name, argv, env in CASES:
             a = materialize(root, argv, "ref_" + name)
             e = dict(os.environ, OMP_NUM_THREADS="4", **env)
-            r = subprocess.run([REF, *a, "-p", "4"], capture_output=True, env=e, check=True)
+            r = subprocess.run([REF, *with_threads(a)], capture_output=True, env=e, check=True)
             with gzip.GzipFile(os.path.join(out_dir, name + ".out.gz"), "wb", mtime=0) as f:
                 f.write(r.stdout)
             print(name, len(r.stdout), "bytes")

@@ -8,7 +8,7 @@ import subprocess
 import pytest
 
 import oracle
-from cli_cases import CASES, materialize
+from cli_cases import CASES, materialize, with_threads
 
 pytestmark = pytest.mark.gpu
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -21,7 +21,7 @@ def _run(binary, argv, env_extra):
     for k in ("KSSD3A_FORCE_REF_INDEX", "KSSD3A_ANI_MATRIX_DIRECT_THRESHOLD", "KSSD3A_ANI_M1_DIRECT_THRESHOLD"):
         env.pop(k, None)
     env.update(env_extra)
-    return subprocess.run([binary, *argv, "-p", "4"], capture_output=True, env=env, timeout=600)
+    return subprocess.run([binary, *with_threads(argv)], capture_output=True, env=env, timeout=600)
 
 
 @pytest.fixture(scope="module")
