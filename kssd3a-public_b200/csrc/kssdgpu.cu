@@ -312,6 +312,28 @@ __device__ __forceinline__ void walk_context(const uint64_t *__restrict__ post, 
         uacc.add(sole_gid, sole_d);
 }
 
+// Handle a found context: the inline single posting, or a walk of its group.
+template <bool LOWER, bool UNIQUE, class Acc>
+__device__ __forceinline__ void credit_context(const CountParams &P, uint64_t i, int s, unsigned long long payload,
+                                               bool single, int qgid, uint64_t objmask, const Acc &acc,
+                                               const Acc &uacc)
+{
+    if (single) {
+        // the context's only posting, held in the slot: one gid run of one object
+        const uint32_t gid = (uint32_t)(payload >> 32);
+        if (LOWER && (int)gid >= qgid)
+            return;
+        const uint32_t q0 = (uint32_t)(P.qkeys[i] & objmask);
+        const int d = min_diff_obj((uint32_t)payload, q0, s, P.qkeys + i, objmask, kMinInit);
+        acc.add(gid, d);
+        if (UNIQUE)
+            uacc.add(gid, d);
+        return;
+    }
+    const uint32_t pb = (uint32_t)payload, pc = (uint32_t)(payload >> 32);
+    walk_context<LOWER, UNIQUE>(P.post, pb, pb + pc, P.qkeys + i, s, objmask, qgid, P.ignoreconflict, acc, uacc);
+}
+
 // Process query entry i of [b, e): only the first entry of a context run works;
 // it takes the whole run (src/command_ani.h:498-505).
 template <bool LOWER, bool UNIQUE, class Acc>
@@ -329,20 +351,66 @@ __device__ __forceinline__ void process_entry(const CountParams &P, uint64_t i, 
     bool single;
     if (!table_lookup(P.table, P.mask, ctx, payload, single))
         return;
-    if (single) {
-        // the context's only posting, held in the slot: one gid run of one object
-        const uint32_t gid = (uint32_t)(payload >> 32);
-        if (LOWER && (int)gid >= qgid)
-            return;
-        const uint32_t q0 = (uint32_t)(P.qkeys[i] & objmask);
-        const int d = min_diff_obj((uint32_t)payload, q0, s, P.qkeys + i, objmask, kMinInit);
-        acc.add(gid, d);
-        if (UNIQUE)
-            uacc.add(gid, d);
-        return;
+    credit_context<LOWER, UNIQUE>(P, i, s, payload, single, qgid, objmask, acc, uacc);
+}
+
+// Entries b + t, b + t + T, ... of one query, kProbeBatch per thread at a time:
+// their first hash slots are loaded back to back so several random lines are in
+// flight per thread, then each probe is resolved (rarely a second slot) and credited.
+constexpr int kProbeBatch = 4;
+
+template <bool LOWER, bool UNIQUE, class Acc>
+__device__ __forceinline__ void process_query(const CountParams &P, uint64_t b, uint64_t e, int qgid,
+                                              uint64_t objmask, const Acc &acc, const Acc &uacc)
+{
+    const uint64_t T = blockDim.x;
+    for (uint64_t base = b + threadIdx.x; base < e; base += T * kProbeBatch) {
+        unsigned long long ctx[kProbeBatch];
+        uint32_t slot[kProbeBatch];
+        int s[kProbeBatch];
+        ulonglong2 first[kProbeBatch];
+#pragma unroll
+        for (int u = 0; u < kProbeBatch; ++u) {
+            const uint64_t i = base + u * T;
+            s[u] = 0;
+            if (i < e) {
+                const uint64_t key = __ldg(P.qkeys + i);
+                ctx[u] = key >> P.obj_bits;
+                if (!(i > b && (__ldg(P.qkeys + i - 1) >> P.obj_bits) == ctx[u])) {
+                    int run = 1;
+                    while (i + run < e && (__ldg(P.qkeys + i + run) >> P.obj_bits) == ctx[u])
+                        ++run;
+                    s[u] = run;
+                    slot[u] = (uint32_t)mix64(ctx[u]) & P.mask;
+                }
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kProbeBatch; ++u)
+            if (s[u])
+                first[u] = __ldg(reinterpret_cast<const ulonglong2 *>(P.table + slot[u]));
+#pragma unroll
+        for (int u = 0; u < kProbeBatch; ++u) {
+            if (!s[u])
+                continue;
+            ulonglong2 sl = first[u];
+            uint32_t at = slot[u];
+            bool found = false;
+            for (uint32_t probe = 0; probe <= P.mask; ++probe) {
+                if ((sl.x & ~kInlineBit) == ctx[u]) {
+                    found = true;
+                    break;
+                }
+                if (sl.x == kEmptyCtx)
+                    break;
+                at = (at + 1) & P.mask;
+                sl = __ldg(reinterpret_cast<const ulonglong2 *>(P.table + at));
+            }
+            if (found)
+                credit_context<LOWER, UNIQUE>(P, base + u * T, s[u], sl.y, (sl.x & kInlineBit) != 0, qgid, objmask,
+                                              acc, uacc);
+        }
     }
-    const uint32_t pb = (uint32_t)payload, pc = (uint32_t)(payload >> 32);
-    walk_context<LOWER, UNIQUE>(P.post, pb, pb + pc, P.qkeys + i, s, objmask, qgid, P.ignoreconflict, acc, uacc);
 }
 
 // Batched persistent kernel: CTAs take whole queries from a work counter
@@ -376,13 +444,11 @@ __global__ void __launch_bounds__(512) k_count_batched(CountParams P)
         const uint64_t b = P.qoffs[q] - base, e = P.qoffs[q + 1] - base;
         if (SMEM) {
             const SmemAcc acc{sc, so}, uacc{suc, suo};
-            for (uint64_t i = b + threadIdx.x; i < e; i += blockDim.x)
-                process_entry<LOWER, UNIQUE>(P, i, b, e, qgid, objmask, acc, uacc);
+            process_query<LOWER, UNIQUE>(P, b, e, qgid, objmask, acc, uacc);
         } else {
             const GlobalAcc acc{P.out_ctx + row, P.out_obj + row};
             const GlobalAcc uacc{UNIQUE ? P.out_uctx + row : nullptr, UNIQUE ? P.out_uobj + row : nullptr};
-            for (uint64_t i = b + threadIdx.x; i < e; i += blockDim.x)
-                process_entry<LOWER, UNIQUE>(P, i, b, e, qgid, objmask, acc, uacc);
+            process_query<LOWER, UNIQUE>(P, b, e, qgid, objmask, acc, uacc);
         }
         __syncthreads();
         if (SMEM) {
@@ -538,7 +604,9 @@ __device__ __forceinline__ void join_pair(uint64_t pi, uint64_t pj, unsigned lon
 // One thread per small group of the compact plan; the warp steps through pair
 // slots in lockstep (groups sorted by size, so lanes carry equal work) and, at
 // every step, lanes holding the same counter cell as their neighbours add their
-// increments with a segmented warp scan: one atomic per run of equal cells.
+// increments with a segmented warp scan: one atomic per run of equal cells.  The
+// four increments of a pair travel packed in 16-bit fields of one word (a run sums
+// at most 32 pairs, so no field exceeds 32 * 12).
 __global__ void __launch_bounds__(256) k_self_small(const unsigned long long *__restrict__ desc, uint32_t n,
                                                     const uint64_t *__restrict__ jp,
                                                     unsigned long long *__restrict__ oc,
@@ -560,13 +628,13 @@ __global__ void __launch_bounds__(256) k_self_small(const unsigned long long *__
     for (uint32_t p = 0; p < maxp; ++p) {
         const bool act = p < npairs;
         unsigned long long cell = ~0ull - lane;  // inactive lanes never join a run
-        unsigned long long ic = 0, io = 0;
+        unsigned long long inc = 0;              // num_ctx | mut2 << 16 | diff_obj << 32 | section << 48
         if (act) {
             const uint64_t pi = __ldg(jp + off + i);
             const int d = min(kMinInit, dna_pop((uint32_t)pi ^ (uint32_t)pj));
             cell = lower_cell((uint32_t)(pj >> 32), (uint32_t)(pi >> 32));
-            ic = inc_ctx(d);
-            io = d ? inc_obj(d) : 0ull;
+            inc = 1ull | ((unsigned long long)(d > 1) << 16) | ((unsigned long long)(d > 0) << 32) |
+                  ((unsigned long long)d << 48);
             if (++i == j) {
                 i = 0;
                 if (++j < k)
@@ -575,21 +643,22 @@ __global__ void __launch_bounds__(256) k_self_small(const unsigned long long *__
         }
         const unsigned long long prev = __shfl_up_sync(0xffffffffu, cell, 1);
         const unsigned heads = __ballot_sync(0xffffffffu, lane == 0 || prev != cell);
-        const int seg_start = 31 - __clz(heads & (below | (1u << lane)));
+        if (heads != 0xffffffffu) {  // some neighbours share a cell: sum their runs
+            const int seg_start = 31 - __clz(heads & (below | (1u << lane)));
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const unsigned long long uc = __shfl_up_sync(0xffffffffu, ic, o);
-            const unsigned long long uo = __shfl_up_sync(0xffffffffu, io, o);
-            if ((int)lane - o >= seg_start) {
-                ic += uc;
-                io += uo;
+            for (int o = 1; o < 32; o <<= 1) {
+                const unsigned long long up = __shfl_up_sync(0xffffffffu, inc, o);
+                if ((int)lane - o >= seg_start)
+                    inc += up;
             }
         }
         const bool tail = lane == 31 || ((heads >> (lane + 1)) & 1u);
         if (act && tail) {
-            atomicAdd(oc + cell, ic);
-            if (io)
-                atomicAdd(oo + cell, io);
+            const unsigned long long nctx = inc & 0xFFFFull, mut2 = (inc >> 16) & 0xFFFFull;
+            const unsigned long long dobj = (inc >> 32) & 0xFFFFull, sect = inc >> 48;
+            atomicAdd(oc + cell, nctx | (mut2 << 32));
+            if (dobj)
+                atomicAdd(oo + cell, dobj | (sect << 32));
         }
     }
 }

@@ -407,6 +407,23 @@ static void write_buf(FILE *f, const kssd_buf_t *b)
         err(EXIT_FAILURE, "Cannot write ANI output");
 }
 
+/* KSSD3A_TIMING=1: phase timings on stderr */
+static double g_t_last = -1.0;
+static void phase(const char *what)
+{
+    static int on = -1;
+    if (on < 0) {
+        const char *e = getenv("KSSD3A_TIMING");
+        on = e && e[0] && strcmp(e, "0");
+    }
+    if (!on)
+        return;
+    const double now = omp_get_wtime();
+    if (g_t_last >= 0)
+        fprintf(stderr, "[kssd3a] %-28s %8.1f ms\n", what, 1e3 * (now - g_t_last));
+    g_t_last = now;
+}
+
 /* context runs of one sorted sample (count_ctx_runs_sorted_ctxobj64_local, src/command_ani.c:337-349) */
 static uint32_t ctx_runs(const uint64_t *a, size_t n, int obj_bits, bool ignoreconflict)
 {
@@ -839,9 +856,44 @@ static void write_index_files(const char *dir, kssdgpu_index_t *ix, uint64_t n)
     free(bits);
 }
 
-/* Lower-triangle counters of a self sketch: with an index file, the reference's
- * index (probe kernel over query blocks); without, the self join over the index the
- * device builds from the sketch. */
+/* Order-independent checksum of (ctxgid, obj) over index records or over a sketch's
+ * entries: equal sums (with equal counts) show the index file was built from this
+ * sketch, so the self join over it gives count_lower's counters. */
+static uint64_t mix_rec(uint64_t ctxgid, uint32_t obj)
+{
+    uint64_t x = ctxgid * 0x9E3779B97F4A7C15ull ^ ((uint64_t)obj + 0x632BE59BD9B4E019ull);
+    x ^= x >> 31;
+    x *= 0xBF58476D1CE4E5B9ull;
+    x ^= x >> 29;
+    return x;
+}
+
+static uint64_t records_checksum(const kssd_index_rec_t *rec, size_t n)
+{
+    uint64_t sum = 0;
+#pragma omp parallel for reduction(+ : sum) schedule(static) num_threads(g.o.p)
+    for (size_t i = 0; i < n; ++i)
+        sum += mix_rec(rec[i].ctxgid, rec[i].obj);
+    return sum;
+}
+
+static uint64_t sketch_checksum(const kssd_sketch_t *s)
+{
+    uint64_t sum = 0;
+    const uint64_t objmask = s->obj_bits >= 64 ? ~0ull : ((1ull << s->obj_bits) - 1);
+#pragma omp parallel for reduction(+ : sum) schedule(dynamic, 16) num_threads(g.o.p)
+    for (int gid = 0; gid < s->n; ++gid)
+        for (uint64_t i = s->offs[gid]; i < s->offs[gid + 1]; ++i) {
+            const uint64_t k = s->keys[i - s->offs[0]];
+            sum += mix_rec(((k >> s->obj_bits) << KSSD_GID_BITS) | (uint64_t)gid, (uint32_t)(k & objmask));
+        }
+    return sum;
+}
+
+/* Lower-triangle counters of a self sketch.  With an index file the reference reads
+ * that index: when its records are the sketch's own (checksum), the self join over it
+ * gives the same counters; otherwise the probe kernel runs the sketch's queries
+ * against it.  Without a file, the self join over the index the device builds. */
 static void self_lower_counts(const kssd_sketch_t *s, const char *dir, bool index_file, bool forced_needs_file,
                               kssdgpu_ctx_mut2_t **pc, kssdgpu_obj_section_t **po)
 {
@@ -859,28 +911,40 @@ static void self_lower_counts(const kssd_sketch_t *s, const char *dir, bool inde
             errx(EXIT_FAILURE, "%s", kssd_host_last_error());
         if (nrec != (size_t)(s->offs[n] - s->offs[0]))
             errx(EINVAL, "load_self_sorted_index_or_build(): sorted index size mismatch");
+        phase("read index file");
+        const bool own = records_checksum(rec, nrec) == sketch_checksum(s);
+        phase("index/sketch checksum");
         kssdgpu_index_t *ix = NULL;
         gpu_check(kssdgpu_index_from_records(rec, nrec, n, s->obj_bits, 0, &ix), "device index");
         free(rec);
-        const int B = block_for(n, n);
-        for (int q0 = 0; q0 < n; q0 += B) {
-            const int nb = n - q0 < B ? n - q0 : B;
-            kssdgpu_ctx_mut2_t *c = malloc((size_t)nb * n * sizeof(*c) + 8);
-            kssdgpu_obj_section_t *o = malloc((size_t)nb * n * sizeof(*o) + 8);
-            if (!c || !o)
-                err(EXIT_FAILURE, "OOM counter block");
-            gpu_check(kssdgpu_count_lower(ix, s->keys + (s->offs[q0] - s->offs[0]), s->offs + q0, nb, q0, flags, c, o),
-                      "device counting");
+        phase("device index from records");
+        if (own) {
+            if (cells)
+                gpu_check(kssdgpu_self_lower(ix, flags, lc, lo), "device self join");
+            phase("self join + D2H");
+        } else {
+            const int B = block_for(n, n);
+            for (int q0 = 0; q0 < n; q0 += B) {
+                const int nb = n - q0 < B ? n - q0 : B;
+                kssdgpu_ctx_mut2_t *c = malloc((size_t)nb * n * sizeof(*c) + 8);
+                kssdgpu_obj_section_t *o = malloc((size_t)nb * n * sizeof(*o) + 8);
+                if (!c || !o)
+                    err(EXIT_FAILURE, "OOM counter block");
+                gpu_check(kssdgpu_count_lower(ix, s->keys + (s->offs[q0] - s->offs[0]), s->offs + q0, nb, q0, flags, c,
+                                              o),
+                          "device counting");
 #pragma omp parallel for schedule(static) num_threads(g.o.p)
-            for (int i = 0; i < nb; ++i) {
-                const int q = q0 + i;
-                if (q == 0)
-                    continue;
-                memcpy(lc + (size_t)q * (q - 1) / 2, c + (size_t)i * n, (size_t)q * sizeof(*c));
-                memcpy(lo + (size_t)q * (q - 1) / 2, o + (size_t)i * n, (size_t)q * sizeof(*o));
+                for (int i = 0; i < nb; ++i) {
+                    const int q = q0 + i;
+                    if (q == 0)
+                        continue;
+                    memcpy(lc + (size_t)q * (q - 1) / 2, c + (size_t)i * n, (size_t)q * sizeof(*c));
+                    memcpy(lo + (size_t)q * (q - 1) / 2, o + (size_t)i * n, (size_t)q * sizeof(*o));
+                }
+                free(c);
+                free(o);
             }
-            free(c);
-            free(o);
+            phase("probe count_lower + D2H");
         }
         kssdgpu_index_free(ix);
     } else {
@@ -888,8 +952,10 @@ static void self_lower_counts(const kssd_sketch_t *s, const char *dir, bool inde
             errx(EXIT_FAILURE, "KSSD3A_FORCE_REF_INDEX requires reference index '%s/%s'", dir,
                  "sortedcomb_ctxgid64obj32");
         kssdgpu_index_t *ix = gpu_index_of_sketch(s);
+        phase("device index from sketch");
         if (cells)
             gpu_check(kssdgpu_self_lower(ix, flags, lc, lo), "device self join");
+        phase("self join + D2H");
         kssdgpu_index_free(ix);
     }
     *pc = lc;
@@ -906,15 +972,22 @@ static double *self_lower_metrics(const kssd_sketch_t *s, const kssdgpu_ctx_mut2
     double *m = malloc(cells * sizeof(double) + 8);
     if (!m)
         err(EXIT_FAILURE, "OOM metrics");
+    double zero_metric = 0;
+    const bool zero_const = kssd_zero_overlap_metric(&g.o, &zero_metric);
 #pragma omp parallel for schedule(dynamic, 16) num_threads(g.o.p)
     for (int q = 1; q < n; ++q) {
         const size_t base = (size_t)q * (q - 1) / 2;
         for (int r = 0; r < q; ++r) {
+            if (zero_const && lc[base + r].num_ctx == 0 && qcnt[q] && rcnt[r]) {
+                m[base + r] = zero_metric;
+                continue;
+            }
             kssd_features_t f = feat_of(&lc[base + r], &lo[base + r]);
             m[base + r] = kssd_pair_metric(&f, qcnt[q], rcnt[r], &g.o, s->meta ? &s->meta[q] : NULL,
                                            s->meta ? &s->meta[r] : NULL);
         }
     }
+    phase("epilogue (host FP64)");
     if (rcnt != qcnt)
         free(rcnt);
     free(qcnt);
@@ -1015,8 +1088,10 @@ static void print_self_lf(const kssd_sketch_t *s, const double *m, bool full)
 /* kind: 0 indexed full (fixed6), 1 indexed triangle, 2 direct (full or triangle per fmt) */
 static int run_self(int kind)
 {
+    phase("start");
     kssd_sketch_t *s = load_sketch(g.qrydir, 0);
     init_bits(s);
+    phase("read sketch");
     bool index_file = false;
     if (kind == 0) {
         /* ensure_sorted_ref_index_for_ani_m1 (src/command_ani_wrapper.c:708-716): write the index when absent */
@@ -1041,6 +1116,7 @@ static int run_self(int kind)
         print_self_lf(s, m, false);
     else
         print_self_lf(s, m, g.o.fmt == 1);
+    phase("format + write");
     free(m);
     kssd_sketch_free(s);
     return 0;
@@ -1071,15 +1147,19 @@ static int run_rect_matrix(void)
         const int nb = qry->n - q0 < B ? qry->n - q0 : B;
         counts_t c = count_queries(ix, R, qry, q0, nb, flags);
         kssd_buf_t *rows = calloc((size_t)nb, sizeof(kssd_buf_t));
+        double zero_metric = 0;
+        const bool zero_const = kssd_zero_overlap_metric(o, &zero_metric);
 #pragma omp parallel for schedule(dynamic, 1) num_threads(o->p)
         for (int i = 0; i < nb; ++i) {
             const int q = q0 + i;
             kssd_buf_puts(&rows[i], qry->names[q]);
             for (int r = 0; r < R; ++r) {
                 kssd_features_t f = feat_of(&c.ctx[(size_t)i * R + r], &c.obj[(size_t)i * R + r]);
-                kssd_buf_printf(&rows[i], "\t%lf",
-                                kssd_pair_metric(&f, qcnt[q], rcnt[r], o, qry->meta ? &qry->meta[q] : NULL,
-                                                 ref->meta ? &ref->meta[r] : NULL));
+                const double v = (zero_const && f.XnY_ctx == 0 && qcnt[q] && rcnt[r])
+                                     ? zero_metric
+                                     : kssd_pair_metric(&f, qcnt[q], rcnt[r], o, qry->meta ? &qry->meta[q] : NULL,
+                                                        ref->meta ? &ref->meta[r] : NULL);
+                kssd_buf_printf(&rows[i], "\t%lf", v);
             }
             kssd_buf_putc(&rows[i], '\n');
         }
@@ -1854,6 +1934,7 @@ static int cmd_matrix(int argc, char **argv)
 int main(int argc, char **argv)
 {
     setvbuf(stdout, NULL, _IOFBF, 1 << 20);
+    phase("start");
     if (argc < 2) {
         fprintf(stderr, "Usage: %s ani [OPTION...]\n", argv[0]);
         return 64;

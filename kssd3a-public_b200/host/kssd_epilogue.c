@@ -444,6 +444,15 @@ double kssd_pair_metric(const kssd_features_t *f, uint32_t qry_ctx, uint32_t ref
     return o->s < 0 ? r.selected_ani : r.metric;
 }
 
+bool kssd_zero_overlap_metric(const kssd_ani_opt_t *o, double *value)
+{
+    if (!(o->afcut > 0.0f))
+        return false;
+    const kssd_features_t zero = {0, 0, 0, 0, 0};
+    *value = kssd_pair_metric(&zero, 1, 1, o, NULL, NULL);
+    return true;
+}
+
 int kssd_cmp_row_desc(const void *pa, const void *pb)
 {
     const kssd_row_t *a = pa, *b = pb;

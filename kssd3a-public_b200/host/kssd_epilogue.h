@@ -99,6 +99,10 @@ void kssd_finalize_row(kssd_row_t *r, const kssd_ani_opt_t *o);
 double kssd_pair_metric(const kssd_features_t *f, uint32_t qry_ctx, uint32_t ref_ctx, const kssd_ani_opt_t *o,
                         const kssd_infile_meta_t *qry_meta, const kssd_infile_meta_t *ref_meta);
 double kssd_matrix_exception_value(const kssd_ani_opt_t *o);
+/* The metric of every pair with no shared context (XnY = 0) and non-empty sketches,
+ * which is one constant whenever afcut > 0: such a pair never passes the AF gate, so
+ * no model depends on its sketch sizes.  Returns false (no constant) when afcut is 0. */
+bool kssd_zero_overlap_metric(const kssd_ani_opt_t *o, double *value);
 double kssd_matrix_diagonal_value(const kssd_ani_opt_t *o);
 
 /* printing */

@@ -98,3 +98,42 @@ def test_hgb_table_shape():
     src = os.path.join(os.path.dirname(kssdgpu.__file__), "host", "hgb_t11_model.c")
     text = open(src).read()
     assert text.count("\n    {") == 9760
+
+
+class Opt(C.Structure):
+    _fields_ = [("fmt", C.c_int), ("p", C.c_int), ("d", C.c_bool), ("v", C.c_bool), ("unassembled", C.c_bool),
+                ("unified_metric", C.c_bool), ("ignoreconflict", C.c_bool), ("raw_output", C.c_bool),
+                ("max_pdist_set", C.c_bool), ("max_pdist", C.c_double), ("max_diff_obj_section", C.c_int),
+                ("e", C.c_int), ("s", C.c_int), ("ntop", C.c_int), ("ctxcut", C.c_int), ("afcut", C.c_float),
+                ("afcut_set", C.c_bool), ("anicut", C.c_float), ("unique_ctx", C.c_bool), ("obj_bits", C.c_int),
+                ("ctx_bits", C.c_int), ("drfold", C.c_int)]
+
+
+def test_zero_overlap_constant_equals_full_evaluation():
+    """The CLI's shortcut for pairs with no shared context gives exactly the value the
+    full row evaluation gives, for every metric, sign, exception value and AF cut."""
+    lib = _host()
+    lib.kssd_opt_defaults.argtypes = [C.POINTER(Opt)]
+    lib.kssd_zero_overlap_metric.argtypes = [C.POINTER(Opt), C.POINTER(C.c_double)]
+    lib.kssd_zero_overlap_metric.restype = C.c_bool
+    lib.kssd_pair_metric.argtypes = [C.POINTER(Feat), C.c_uint32, C.c_uint32, C.POINTER(Opt), C.c_void_p,
+                                     C.c_void_p]
+    lib.kssd_pair_metric.restype = C.c_double
+    rng = np.random.default_rng(3)
+    zero = Feat(0, 0, 0, 0, 0)
+    for s in list(range(1, 10)) + list(range(-9, 0)):
+        for afcut in (0.5, 0.2, 1e-6, 0.0):
+            for flags in ((False, False, False), (True, True, False), (False, False, True)):
+                o = Opt()
+                lib.kssd_opt_defaults(C.byref(o))
+                o.s, o.afcut, o.e = s, afcut, int(rng.integers(1, 3))
+                o.v, o.unassembled, o.raw_output = flags
+                const = C.c_double()
+                ok = lib.kssd_zero_overlap_metric(C.byref(o), C.byref(const))
+                assert ok == (afcut > 0)
+                if not ok:
+                    continue
+                for _ in range(20):
+                    qc, rc = (int(x) for x in rng.integers(1, 200000, size=2))
+                    full = lib.kssd_pair_metric(C.byref(zero), qc, rc, C.byref(o), None, None)
+                    assert _same(full, const.value), (s, afcut, flags, qc, rc, full, const.value)
