@@ -61,6 +61,11 @@ typedef struct kssdgpu_index kssdgpu_index_t;
 /* Message of the last failing call on this thread ("" if none). */
 const char *kssdgpu_last_error(void);
 
+/* Creates the CUDA context of `device` (otherwise created by the first call that
+ * needs it).  A front end can call it from a helper thread while it reads its input
+ * files, so context creation overlaps the I/O. */
+int kssdgpu_init(int device);
+
 /*
  * Device-resident CSR from the reference's inverted index records
  * (sortedcomb_ctxgid64obj32: n packed 12-byte {uint64 ctx<<20|gid; uint32 obj},
@@ -203,6 +208,49 @@ int kssdgpu_count_block_noalloc(kssdgpu_index_t *idx, const uint64_t *d_qry_keys
                                 int nq, int qry_gid_offset, int lower, unsigned flags,
                                 kssdgpu_ctx_mut2_t *d_ctx, kssdgpu_obj_section_t *d_obj,
                                 kssdgpu_ctx_mut2_t *d_uctx, kssdgpu_obj_section_t *d_uobj, void *stream);
+
+/*
+ * Continuous-batching query server over a resident index (the serving loop; the
+ * reference has no server: its per-request equivalent is one `kssd3a ani -r R -q one`
+ * run).  Each request is one query sample; its result is the list of nonzero counter
+ * cells kssdgpu_count_block gives for that query alone, sorted by reference id.
+ * Device memory for two batch slots is reserved at creation (the admission budget):
+ * a slot admits the oldest queued requests up to max_batch_queries queries and
+ * max_batch_keys keys, and the two slots' batches overlap on the device.
+ */
+typedef struct kssdgpu_hit {
+    uint32_t query; /* 0 in results (each request is one query) */
+    uint32_t ref;
+    uint32_t num_ctx, num_mut2_ctx, diff_obj, diff_obj_section;
+    uint32_t u_num_ctx, u_num_mut2_ctx, u_diff_obj, u_diff_obj_section; /* KSSDGPU_UNIQUE */
+} kssdgpu_hit_t;
+
+typedef struct kssdgpu_server_config {
+    int max_batch_queries;   /* queries per batch slot */
+    uint64_t max_batch_keys; /* keys per batch slot (larger single queries are rejected) */
+    uint64_t max_hits;       /* nonzero cells per batch (0: batch queries x references) */
+    unsigned flags;          /* KSSDGPU_IGNORECONFLICT | KSSDGPU_UNIQUE */
+} kssdgpu_server_config_t;
+
+typedef struct kssdgpu_server_stats {
+    uint64_t completed, batches, pending, max_inflight, overlapped_batches, reserved_bytes;
+    double p50_ms, p99_ms, max_ms, mean_ms; /* submit -> result latency */
+} kssdgpu_server_stats_t;
+
+typedef struct kssdgpu_server kssdgpu_server_t;
+
+int kssdgpu_server_create(kssdgpu_index_t *idx, const kssdgpu_server_config_t *cfg, kssdgpu_server_t **out);
+/* Copies the query's keys (sorted comblco keys of one sample) and queues it. */
+int kssdgpu_server_submit(kssdgpu_server_t *srv, const uint64_t *keys, uint64_t n_keys, uint64_t *ticket);
+/* Waits (timeout_ms < 0: no limit) for a request; gives its hit count and latency. */
+int kssdgpu_server_wait(kssdgpu_server_t *srv, uint64_t ticket, int timeout_ms, uint32_t *n_hits,
+                        double *latency_ms);
+/* Copies a finished request's hits (cap entries at most) and forgets the ticket. */
+int kssdgpu_server_take(kssdgpu_server_t *srv, uint64_t ticket, kssdgpu_hit_t *hits, uint32_t cap);
+int kssdgpu_server_stats(kssdgpu_server_t *srv, kssdgpu_server_stats_t *out);
+int kssdgpu_server_reset_stats(kssdgpu_server_t *srv);
+/* Finishes queued and running batches, then frees the server (not the index). */
+void kssdgpu_server_destroy(kssdgpu_server_t *srv);
 
 /* Number of kernels launched by this library so far in this process. */
 uint64_t kssdgpu_launch_count(void);

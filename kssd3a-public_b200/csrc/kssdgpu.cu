@@ -241,13 +241,19 @@ struct CountParams {
 __device__ __forceinline__ unsigned long long inc_ctx(int d) { return 1ull | ((unsigned long long)(d > 1) << 32); }
 __device__ __forceinline__ unsigned long long inc_obj(int d) { return 1ull | ((unsigned long long)d << 32); }
 
+// Shared-memory row: four 32-bit counters per reference (native shared atomics;
+// hot cells of similar genomes contend less than on 64-bit words).
 struct SmemAcc {
-    unsigned long long *c, *o;
+    uint32_t *nc, *m2, *dobj, *sect;
     __device__ __forceinline__ void add(uint32_t gid, int d) const
     {
-        atomicAdd(c + gid, inc_ctx(d));
-        if (d)
-            atomicAdd(o + gid, inc_obj(d));
+        atomicAdd(nc + gid, 1u);
+        if (d) {
+            atomicAdd(dobj + gid, 1u);
+            atomicAdd(sect + gid, (uint32_t)d);
+            if (d > 1)
+                atomicAdd(m2 + gid, 1u);
+        }
     }
 };
 
@@ -357,7 +363,10 @@ __device__ __forceinline__ void process_entry(const CountParams &P, uint64_t i, 
 // Entries b + t, b + t + T, ... of one query, kProbeBatch per thread at a time:
 // their first hash slots are loaded back to back so several random lines are in
 // flight per thread, then each probe is resolved (rarely a second slot) and credited.
-constexpr int kProbeBatch = 4;
+#ifndef KSSD_PROBE_BATCH
+#define KSSD_PROBE_BATCH 1
+#endif
+constexpr int kProbeBatch = KSSD_PROBE_BATCH;
 
 template <bool LOWER, bool UNIQUE, class Acc>
 __device__ __forceinline__ void process_query(const CountParams &P, uint64_t b, uint64_t e, int qgid,
@@ -420,7 +429,7 @@ __device__ __forceinline__ void process_query(const CountParams &P, uint64_t b, 
 template <bool LOWER, bool UNIQUE, bool SMEM>
 __global__ void __launch_bounds__(512) k_count_batched(CountParams P)
 {
-    extern __shared__ unsigned long long sm[];
+    extern __shared__ uint32_t sm[];
     __shared__ int s_item;
     const uint64_t objmask = (P.obj_bits >= 64) ? ~0ull : ((1ull << P.obj_bits) - 1);
     const uint64_t base = P.qoffs[0];
@@ -435,15 +444,17 @@ __global__ void __launch_bounds__(512) k_count_batched(CountParams P)
         const int q = P.order ? P.order[it] : it;
         const int qgid = P.qgid_offset + q;
         const size_t row = (size_t)q * nref;
-        unsigned long long *sc = sm, *so = sm + nref, *suc = sm + 2 * nref, *suo = sm + 3 * nref;
+        // rows: [nc | m2 | dobj | sect] x nref, then the unique-context row
+        uint32_t *row0 = sm, *row1 = sm + 4 * (size_t)nref;
         if (SMEM) {
-            for (int c = threadIdx.x; c < nref * (UNIQUE ? 4 : 2); c += blockDim.x)
+            for (int c = threadIdx.x; c < nref * (UNIQUE ? 8 : 4); c += blockDim.x)
                 sm[c] = 0;
             __syncthreads();
         }
         const uint64_t b = P.qoffs[q] - base, e = P.qoffs[q + 1] - base;
         if (SMEM) {
-            const SmemAcc acc{sc, so}, uacc{suc, suo};
+            const SmemAcc acc{row0, row0 + nref, row0 + 2 * nref, row0 + 3 * nref};
+            const SmemAcc uacc{row1, row1 + nref, row1 + 2 * nref, row1 + 3 * nref};
             process_query<LOWER, UNIQUE>(P, b, e, qgid, objmask, acc, uacc);
         } else {
             const GlobalAcc acc{P.out_ctx + row, P.out_obj + row};
@@ -453,11 +464,12 @@ __global__ void __launch_bounds__(512) k_count_batched(CountParams P)
         __syncthreads();
         if (SMEM) {
             for (int g = threadIdx.x; g < nref; g += blockDim.x) {
-                P.out_ctx[row + g] = sc[g];
-                P.out_obj[row + g] = so[g];
+                P.out_ctx[row + g] = (unsigned long long)row0[g] | ((unsigned long long)row0[nref + g] << 32);
+                P.out_obj[row + g] = (unsigned long long)row0[2 * nref + g] | ((unsigned long long)row0[3 * nref + g] << 32);
                 if (UNIQUE) {
-                    P.out_uctx[row + g] = suc[g];
-                    P.out_uobj[row + g] = suo[g];
+                    P.out_uctx[row + g] = (unsigned long long)row1[g] | ((unsigned long long)row1[nref + g] << 32);
+                    P.out_uobj[row + g] =
+                        (unsigned long long)row1[2 * nref + g] | ((unsigned long long)row1[3 * nref + g] << 32);
                 }
             }
         }
@@ -1218,6 +1230,13 @@ extern "C" {
 
 const char *kssdgpu_last_error(void) { return g_last_error.c_str(); }
 
+int kssdgpu_init(int device)
+{
+    CUDA_TRY(cudaSetDevice(device));
+    CUDA_TRY(cudaFree(nullptr));
+    return KSSDGPU_OK;
+}
+
 uint64_t kssdgpu_launch_count(void) { return g_launches.load(); }
 
 int kssdgpu_index_from_records(const void *records12, uint64_t n, int nref, int obj_bits, int device,
@@ -1600,3 +1619,6 @@ int kssdgpu_self_lower_dev(kssdgpu_index_t *ix, unsigned flags, kssdgpu_ctx_mut2
 }
 
 }  // extern "C"
+
+// continuous-batching server (same translation unit: it launches k_count_batched)
+#include "kssd_server.cuh"

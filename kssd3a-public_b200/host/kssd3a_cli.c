@@ -28,6 +28,7 @@
 #include <stdlib.h>
 #include <string.h>
 #include <sys/stat.h>
+#include <pthread.h>
 #include <unistd.h>
 
 #include "kssd_epilogue.h"
@@ -383,6 +384,23 @@ static void gpu_check(int rc, const char *what)
 {
     if (rc != KSSDGPU_OK)
         errx(EXIT_FAILURE, "%s: %s", what, kssdgpu_last_error());
+}
+
+/* CUDA context creation takes a sizeable fraction of a short run: start it on a
+ * helper thread while the sketches and the index are read (the runtime makes a later
+ * first call from the main thread wait for it). */
+static void *gpu_warmup(void *arg)
+{
+    (void)arg;
+    kssdgpu_init(0);
+    return NULL;
+}
+
+static void start_gpu_warmup(void)
+{
+    pthread_t t;
+    if (pthread_create(&t, NULL, gpu_warmup, NULL) == 0)
+        pthread_detach(t);
 }
 
 static FILE *open_out(const char *path)
@@ -1410,6 +1428,7 @@ static int cmd_ani(int argc, char **argv)
     if (!is_sketch_dir(g.qrydir))
         errx(EXIT_FAILURE, "%s is not a sketch directory; FASTA/FASTQ inputs need the sketcher, which this build "
                            "does not include", g.qrydir);
+    start_gpu_warmup();
     run_sketch_ani();
     return 0;
 }
@@ -1924,6 +1943,7 @@ static int cmd_matrix(int argc, char **argv)
         errx(EXIT_FAILURE, "the legacy --ani matrix is not supported by this build; use `kssd3a ani --format matrix`");
     if (!is_sketch_dir(gm.qrydir) || (gm.refdir[0] && !is_sketch_dir(gm.refdir)))
         errx(EXIT_FAILURE, "matrix inputs must be sketch directories");
+    start_gpu_warmup();
     if (!gm.refdir[0])
         return matrix_self(fmt);
     if (fmt != MF_FULL)

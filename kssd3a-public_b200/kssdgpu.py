@@ -72,8 +72,33 @@ def gpu_lib() -> C.CDLL:
                                                C.POINTER(C.c_uint64)]
         lib.kssdgpu_count_plain_dev.argtypes = [vp, vp, vp, _u64p, C.c_int, C.c_int, C.c_int, C.c_uint,
                                                 vp, vp, vp, vp, vp]
+        lib.kssdgpu_init.argtypes = [C.c_int]
+        lib.kssdgpu_server_create.argtypes = [vp, C.POINTER(_ServerConfig), C.POINTER(vp)]
+        lib.kssdgpu_server_submit.argtypes = [vp, vp, C.c_uint64, C.POINTER(C.c_uint64)]
+        lib.kssdgpu_server_wait.argtypes = [vp, C.c_uint64, C.c_int, C.POINTER(C.c_uint32), C.POINTER(C.c_double)]
+        lib.kssdgpu_server_take.argtypes = [vp, C.c_uint64, vp, C.c_uint32]
+        lib.kssdgpu_server_stats.argtypes = [vp, C.POINTER(_ServerStats)]
+        lib.kssdgpu_server_reset_stats.argtypes = [vp]
+        lib.kssdgpu_server_destroy.argtypes = [vp]
+        lib.kssdgpu_server_destroy.restype = None
         _gpu = lib
     return _gpu
+
+
+class _ServerConfig(C.Structure):
+    _fields_ = [("max_batch_queries", C.c_int), ("max_batch_keys", C.c_uint64), ("max_hits", C.c_uint64),
+                ("flags", C.c_uint)]
+
+
+class _ServerStats(C.Structure):
+    _fields_ = [("completed", C.c_uint64), ("batches", C.c_uint64), ("pending", C.c_uint64),
+                ("max_inflight", C.c_uint64), ("overlapped_batches", C.c_uint64), ("reserved_bytes", C.c_uint64),
+                ("p50_ms", C.c_double), ("p99_ms", C.c_double), ("max_ms", C.c_double), ("mean_ms", C.c_double)]
+
+
+HIT_DTYPE = np.dtype([("query", "<u4"), ("ref", "<u4"), ("num_ctx", "<u4"), ("num_mut2_ctx", "<u4"),
+                      ("diff_obj", "<u4"), ("diff_obj_section", "<u4"), ("u_num_ctx", "<u4"),
+                      ("u_num_mut2_ctx", "<u4"), ("u_diff_obj", "<u4"), ("u_diff_obj_section", "<u4")])
 
 
 class _SynthCfg(C.Structure):
@@ -352,6 +377,50 @@ class Index:
 
     def sync(self, stream=None):
         _check(gpu_lib().kssdgpu_sync(self._h, _ptr(stream)))
+
+
+class Server:
+    """Continuous-batching query server over a resident Index (libkssdgpu kssdgpu_server_*)."""
+
+    def __init__(self, index: Index, max_batch_queries=256, max_batch_keys=1 << 26, max_hits=0, flags=0):
+        self.index = index  # keep the index alive
+        cfg = _ServerConfig(max_batch_queries, max_batch_keys, max_hits, flags)
+        h = C.c_void_p()
+        _check(gpu_lib().kssdgpu_server_create(index.handle, C.byref(cfg), C.byref(h)))
+        self._h = h
+
+    def submit(self, keys: np.ndarray) -> int:
+        k = np.ascontiguousarray(keys, dtype=np.uint64)
+        t = C.c_uint64()
+        _check(gpu_lib().kssdgpu_server_submit(self._h, k.ctypes.data if len(k) else None, len(k), C.byref(t)))
+        return t.value
+
+    def result(self, ticket: int, timeout_ms: int = -1):
+        """(hits structured array sorted by ref, latency ms)."""
+        n, lat = C.c_uint32(), C.c_double()
+        _check(gpu_lib().kssdgpu_server_wait(self._h, ticket, timeout_ms, C.byref(n), C.byref(lat)))
+        hits = np.zeros(max(n.value, 1), dtype=HIT_DTYPE)
+        _check(gpu_lib().kssdgpu_server_take(self._h, ticket, hits.ctypes.data, n.value))
+        return hits[: n.value], lat.value
+
+    def stats(self):
+        st = _ServerStats()
+        _check(gpu_lib().kssdgpu_server_stats(self._h, C.byref(st)))
+        return {f: getattr(st, f) for f, _ in st._fields_}
+
+    def reset_stats(self):
+        _check(gpu_lib().kssdgpu_server_reset_stats(self._h))
+
+    def close(self):
+        if self._h and self._h.value:
+            gpu_lib().kssdgpu_server_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def _ptr(x):
