@@ -84,6 +84,7 @@ struct ServerSlot {
     kssdgpu_hit_t *d_hits = nullptr;
     unsigned int *d_count = nullptr, *d_work = nullptr;
     uint64_t *h_keys = nullptr, *h_offs = nullptr;
+    WorkItem *d_items = nullptr, *h_items = nullptr;
     unsigned int *h_count = nullptr;
     kssdgpu_hit_t *h_hits = nullptr;
     cudaStream_t st = nullptr;
@@ -115,6 +116,12 @@ struct kssdgpu_server {
 
 namespace {
 
+// chunks of a full batch: every query may end in a partial chunk
+size_t server_item_cap(const kssdgpu_server_config_t &c)
+{
+    return (size_t)(c.max_batch_keys / kChunkKeys) + (size_t)c.max_batch_queries + 1;
+}
+
 int server_slot_alloc(kssdgpu_server *s, ServerSlot &sl)
 {
     const auto &c = s->cfg;
@@ -122,6 +129,7 @@ int server_slot_alloc(kssdgpu_server *s, ServerSlot &sl)
     const bool uq = (c.flags & KSSDGPU_UNIQUE) != 0;
     CUDA_TRY(cudaMalloc(&sl.d_keys, std::max<uint64_t>(c.max_batch_keys, 1) * 8));
     CUDA_TRY(cudaMalloc(&sl.d_offs, ((size_t)c.max_batch_queries + 1) * 8));
+    CUDA_TRY(cudaMalloc(&sl.d_items, server_item_cap(c) * sizeof(WorkItem)));
     CUDA_TRY(cudaMalloc(&sl.d_rc, cells * 8));
     CUDA_TRY(cudaMalloc(&sl.d_ro, cells * 8));
     CUDA_TRY(cudaMemset(sl.d_rc, 0, cells * 8));
@@ -137,6 +145,7 @@ int server_slot_alloc(kssdgpu_server *s, ServerSlot &sl)
     CUDA_TRY(cudaMalloc(&sl.d_work, sizeof(unsigned int)));
     CUDA_TRY(cudaMallocHost(&sl.h_keys, std::max<uint64_t>(c.max_batch_keys, 1) * 8));
     CUDA_TRY(cudaMallocHost(&sl.h_offs, ((size_t)c.max_batch_queries + 1) * 8));
+    CUDA_TRY(cudaMallocHost(&sl.h_items, server_item_cap(c) * sizeof(WorkItem)));
     CUDA_TRY(cudaMallocHost(&sl.h_count, sizeof(unsigned int)));
     CUDA_TRY(cudaMallocHost(&sl.h_hits, (size_t)s->hit_cap * sizeof(kssdgpu_hit_t)));
     CUDA_TRY(cudaStreamCreateWithFlags(&sl.st, cudaStreamNonBlocking));
@@ -148,6 +157,7 @@ void server_slot_free(ServerSlot &sl)
 {
     cudaFree(sl.d_keys);
     cudaFree(sl.d_offs);
+    cudaFree(sl.d_items);
     cudaFree(sl.d_rc);
     cudaFree(sl.d_ro);
     cudaFree(sl.d_urc);
@@ -157,6 +167,7 @@ void server_slot_free(ServerSlot &sl)
     cudaFree(sl.d_work);
     cudaFreeHost(sl.h_keys);
     cudaFreeHost(sl.h_offs);
+    cudaFreeHost(sl.h_items);
     cudaFreeHost(sl.h_count);
     cudaFreeHost(sl.h_hits);
     if (sl.st)
@@ -171,17 +182,23 @@ int server_launch(kssdgpu_server *s, ServerSlot &sl)
 {
     const int nq = (int)sl.batch.size();
     uint64_t nk = 0;
+    size_t nitems = 0;
     sl.h_offs[0] = 0;
     for (int i = 0; i < nq; ++i) {
         const auto &k = sl.batch[i]->keys;
         if (!k.empty())
             std::memcpy(sl.h_keys + nk, k.data(), k.size() * 8);
+        // key-range chunks: a large request spreads over many SMs
+        for (uint64_t c = nk; c < nk + k.size(); c += kChunkKeys)
+            sl.h_items[nitems++] = WorkItem{(uint32_t)i, 0u, c, std::min<uint64_t>(nk + k.size(), c + kChunkKeys)};
         nk += k.size();
         sl.h_offs[i + 1] = nk;
     }
     if (nk)
         CUDA_TRY(cudaMemcpyAsync(sl.d_keys, sl.h_keys, nk * 8, cudaMemcpyHostToDevice, sl.st));
     CUDA_TRY(cudaMemcpyAsync(sl.d_offs, sl.h_offs, ((size_t)nq + 1) * 8, cudaMemcpyHostToDevice, sl.st));
+    if (nitems)
+        CUDA_TRY(cudaMemcpyAsync(sl.d_items, sl.h_items, nitems * sizeof(WorkItem), cudaMemcpyHostToDevice, sl.st));
     CUDA_TRY(cudaMemsetAsync(sl.d_count, 0, sizeof(unsigned int), sl.st));
     CountParams P{};
     P.table = s->ix->table;
@@ -199,6 +216,8 @@ int server_launch(kssdgpu_server *s, ServerSlot &sl)
     P.out_uobj = sl.d_uro;
     P.work = sl.d_work;
     P.order = nullptr;
+    P.items = sl.d_items;
+    P.nitems = (int)nitems;
     P.err = s->ix->err;
     int rc = (s->cfg.flags & KSSDGPU_UNIQUE) ? launch_batched<false, true, false>(s->ix, P, 0, sl.st)
                                              : launch_batched<false, false, false>(s->ix, P, 0, sl.st);

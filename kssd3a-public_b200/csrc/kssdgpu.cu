@@ -215,6 +215,15 @@ __global__ void k_ref_counts(const uint32_t *__restrict__ gbeg, uint64_t u, cons
 
 // ------------------------------------------------------------------ counting kernels
 
+// One unit of work of the global-row batched kernel: entries [b, e) (relative to
+// qoffs[0]) of query q.  Context runs that straddle a chunk boundary are taken by
+// the chunk holding the run's first entry, so chunks of one query never double count.
+struct WorkItem {
+    uint32_t q, pad;
+    uint64_t b, e;
+};
+constexpr uint64_t kChunkKeys = 4096;
+
 struct CountParams {
     const Slot *table;
     uint32_t mask;
@@ -232,8 +241,11 @@ struct CountParams {
     unsigned long long *out_uobj;
     unsigned int *work;            // persistent-kernel work counter (zeroed before launch)
     const int *order;              // query processing order (largest first), may be null
+    const WorkItem *items;         // global-row mode: key-range chunks of queries, may be null
+    int nitems;
     int *err;
 };
+
 
 // One counter update for a matched (query ctx, reference gid run) with minimum
 // object difference d: num_ctx += 1; d > 0: diff_obj += 1, section += d;
@@ -369,11 +381,11 @@ __device__ __forceinline__ void process_entry(const CountParams &P, uint64_t i, 
 constexpr int kProbeBatch = KSSD_PROBE_BATCH;
 
 template <bool LOWER, bool UNIQUE, class Acc>
-__device__ __forceinline__ void process_query(const CountParams &P, uint64_t b, uint64_t e, int qgid,
-                                              uint64_t objmask, const Acc &acc, const Acc &uacc)
+__device__ __forceinline__ void process_query(const CountParams &P, uint64_t b, uint64_t e, uint64_t cb, uint64_t ce,
+                                              int qgid, uint64_t objmask, const Acc &acc, const Acc &uacc)
 {
     const uint64_t T = blockDim.x;
-    for (uint64_t base = b + threadIdx.x; base < e; base += T * kProbeBatch) {
+    for (uint64_t base = cb + threadIdx.x; base < ce; base += T * kProbeBatch) {
         unsigned long long ctx[kProbeBatch];
         uint32_t slot[kProbeBatch];
         int s[kProbeBatch];
@@ -382,7 +394,7 @@ __device__ __forceinline__ void process_query(const CountParams &P, uint64_t b, 
         for (int u = 0; u < kProbeBatch; ++u) {
             const uint64_t i = base + u * T;
             s[u] = 0;
-            if (i < e) {
+            if (i < ce) {
                 const uint64_t key = __ldg(P.qkeys + i);
                 ctx[u] = key >> P.obj_bits;
                 if (!(i > b && (__ldg(P.qkeys + i - 1) >> P.obj_bits) == ctx[u])) {
@@ -425,7 +437,8 @@ __device__ __forceinline__ void process_query(const CountParams &P, uint64_t b, 
 // Batched persistent kernel: CTAs take whole queries from a work counter
 // (largest first); with SMEM the query's reference row is accumulated in shared
 // memory and written once, coalesced; without, counters go to the zeroed global
-// row with atomics.
+// row with atomics, and the work may be split into key-range chunks (P.items) so
+// that one large query (a read set) spreads over many SMs.
 template <bool LOWER, bool UNIQUE, bool SMEM>
 __global__ void __launch_bounds__(512) k_count_batched(CountParams P)
 {
@@ -439,9 +452,9 @@ __global__ void __launch_bounds__(512) k_count_batched(CountParams P)
             s_item = (int)atomicAdd(P.work, 1u);
         __syncthreads();
         const int it = s_item;
-        if (it >= P.nq)
+        if (it >= (!SMEM && P.items ? P.nitems : P.nq))
             break;
-        const int q = P.order ? P.order[it] : it;
+        const int q = (!SMEM && P.items) ? (int)P.items[it].q : P.order ? P.order[it] : it;
         const int qgid = P.qgid_offset + q;
         const size_t row = (size_t)q * nref;
         // rows: [nc | m2 | dobj | sect] x nref, then the unique-context row
@@ -455,11 +468,12 @@ __global__ void __launch_bounds__(512) k_count_batched(CountParams P)
         if (SMEM) {
             const SmemAcc acc{row0, row0 + nref, row0 + 2 * nref, row0 + 3 * nref};
             const SmemAcc uacc{row1, row1 + nref, row1 + 2 * nref, row1 + 3 * nref};
-            process_query<LOWER, UNIQUE>(P, b, e, qgid, objmask, acc, uacc);
+            process_query<LOWER, UNIQUE>(P, b, e, b, e, qgid, objmask, acc, uacc);
         } else {
             const GlobalAcc acc{P.out_ctx + row, P.out_obj + row};
             const GlobalAcc uacc{UNIQUE ? P.out_uctx + row : nullptr, UNIQUE ? P.out_uobj + row : nullptr};
-            process_query<LOWER, UNIQUE>(P, b, e, qgid, objmask, acc, uacc);
+            const uint64_t cb = P.items ? P.items[it].b : b, ce = P.items ? P.items[it].e : e;
+            process_query<LOWER, UNIQUE>(P, b, e, cb, ce, qgid, objmask, acc, uacc);
         }
         __syncthreads();
         if (SMEM) {
@@ -790,6 +804,7 @@ struct kssdgpu_index {
     DevBuf<uint64_t> s_keys, s_offs;
     DevBuf<unsigned long long> s_out;
     DevBuf<int> s_order;
+    DevBuf<WorkItem> s_items;
     // self-join plan: compact small groups (descriptor offset | k << 32 into j_post),
     // big and conflict groups (begin | k << 32 into post)
     DevBuf<unsigned long long> j_small, j_big, j_conf;
@@ -902,8 +917,9 @@ int launch_batched(kssdgpu_index *ix, const CountParams &P, size_t smem, cudaStr
     if (per_sm < 1)
         return fail(KSSDGPU_ERR_CAPACITY, "shared-memory row does not fit one CTA");
     int grid = ix->sms * per_sm;
-    if (grid > P.nq)
-        grid = std::max(P.nq, 1);
+    const int units = (!SMEM && P.items) ? P.nitems : P.nq;
+    if (grid > units)
+        grid = std::max(units, 1);
     CUDA_TRY(cudaMemsetAsync(P.work, 0, sizeof(unsigned int), st));
     kern<<<grid, 512, smem, st>>>(P);
     count_launch();
@@ -925,12 +941,32 @@ int launch_plain(kssdgpu_index *ix, const CountParams &P, const std::vector<uint
     return KSSDGPU_OK;
 }
 
-// shared-memory row budget: 2 (or 4 with unique) u64 per reference
+// shared-memory row budget: four 32-bit counters per reference (eight with unique)
 constexpr size_t kSmemRowLimit = 112 * 1024;
+
+bool uses_smem_row(const kssdgpu_index *ix, unsigned flags)
+{
+    const size_t smem = (size_t)ix->nref * sizeof(unsigned long long) * ((flags & KSSDGPU_UNIQUE) ? 4 : 2);
+    return !(flags & (KSSDGPU_PLAIN | KSSDGPU_GLOBAL_ACC)) && smem <= kSmemRowLimit;
+}
+
+// Key-range chunks of at most kChunkKeys entries for the global-row kernel, the
+// queries taken in the given order (offsets relative or absolute).
+void build_chunks(const uint64_t *offs, int nq, const int *order, std::vector<WorkItem> &items)
+{
+    items.clear();
+    for (int k = 0; k < nq; ++k) {
+        const int q = order ? order[k] : k;
+        const uint64_t b = offs[q] - offs[0], e = offs[q + 1] - offs[0];
+        for (uint64_t c = b; c < e; c += kChunkKeys)
+            items.push_back(WorkItem{(uint32_t)q, 0u, c, std::min(e, c + kChunkKeys)});
+    }
+}
 
 int count_dev_impl(kssdgpu_index *ix, const uint64_t *d_keys, const uint64_t *d_offs, int nq, int qgid_offset, bool lower,
                    unsigned flags, unsigned long long *oc, unsigned long long *oo, unsigned long long *uc,
-                   unsigned long long *uo, const int *d_order, const std::vector<uint64_t> *sizes, cudaStream_t st)
+                   unsigned long long *uo, const int *d_order, const std::vector<uint64_t> *sizes, cudaStream_t st,
+                   const WorkItem *d_items = nullptr, int nitems = 0)
 {
     const bool unique = (flags & KSSDGPU_UNIQUE) != 0;
     if (lower && unique)
@@ -960,7 +996,11 @@ int count_dev_impl(kssdgpu_index *ix, const uint64_t *d_keys, const uint64_t *d_
         return KSSDGPU_OK;
     const size_t smem = (size_t)ix->nref * sizeof(unsigned long long) * (unique ? 4 : 2);
     const bool plain = (flags & KSSDGPU_PLAIN) != 0;
-    const bool use_smem = !plain && !(flags & KSSDGPU_GLOBAL_ACC) && smem <= kSmemRowLimit;
+    const bool use_smem = uses_smem_row(ix, flags);
+    if (!use_smem && d_items) {
+        P.items = d_items;
+        P.nitems = nitems;
+    }
     if (!use_smem && !(flags & KSSDGPU_NO_ZERO)) {
         CUDA_TRY(cudaMemsetAsync(oc, 0, cells * 8, st));
         CUDA_TRY(cudaMemsetAsync(oo, 0, cells * 8, st));
@@ -1012,21 +1052,28 @@ int count_host_impl(kssdgpu_index *ix, const uint64_t *qkeys, const uint64_t *qo
     std::vector<int> order(nq);
     std::iota(order.begin(), order.end(), 0);
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return sizes[a] > sizes[b]; });
+    std::vector<WorkItem> items;
+    if (!uses_smem_row(ix, flags) && !(flags & KSSDGPU_PLAIN))
+        build_chunks(qoffs, nq, order.data(), items);
     const size_t cells = (size_t)nq * ix->nref;
     const int nout = unique ? 4 : 2;
     CUDA_TRY(ix->s_keys.ensure(nkeys));
     CUDA_TRY(ix->s_offs.ensure((size_t)nq + 1));
     CUDA_TRY(ix->s_out.ensure(cells * nout));
     CUDA_TRY(ix->s_order.ensure((size_t)nq));
+    CUDA_TRY(ix->s_items.ensure(items.size()));
     cudaStream_t st = 0;
     if (nkeys)
         CUDA_TRY(cudaMemcpyAsync(ix->s_keys.p, qkeys, nkeys * 8, cudaMemcpyHostToDevice, st));
     CUDA_TRY(cudaMemcpyAsync(ix->s_offs.p, qoffs, ((size_t)nq + 1) * 8, cudaMemcpyHostToDevice, st));
     CUDA_TRY(cudaMemcpyAsync(ix->s_order.p, order.data(), (size_t)nq * sizeof(int), cudaMemcpyHostToDevice, st));
+    if (!items.empty())
+        CUDA_TRY(cudaMemcpyAsync(ix->s_items.p, items.data(), items.size() * sizeof(WorkItem), cudaMemcpyHostToDevice,
+                                 st));
     unsigned long long *oc = ix->s_out.p, *oo = oc + cells;
     unsigned long long *uc = unique ? oo + cells : nullptr, *uo = unique ? uc + cells : nullptr;
     int rc = count_dev_impl(ix, ix->s_keys.p, ix->s_offs.p, nq, qgid_offset, lower, flags, oc, oo, uc, uo, ix->s_order.p,
-                            &sizes, st);
+                            &sizes, st, items.empty() ? nullptr : ix->s_items.p, (int)items.size());
     if (rc)
         return rc;
     CUDA_TRY(cudaMemcpyAsync(ctx, oc, cells * 8, cudaMemcpyDeviceToHost, st));
@@ -1373,6 +1420,7 @@ void kssdgpu_index_free(kssdgpu_index_t *ix)
     ix->s_offs.release();
     ix->s_out.release();
     ix->s_order.release();
+    ix->s_items.release();
     ix->j_small.release();
     ix->j_post.release();
     ix->j_big.release();

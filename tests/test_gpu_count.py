@@ -191,3 +191,33 @@ def test_large_gid_and_max_object_width():
     np.testing.assert_array_equal(ctx, want[0])
     np.testing.assert_array_equal(obj, want[1])
     assert obj[0, 5, 1] == 12  # 16 differing bases, capped at NUM_CODENS + 1
+
+
+def test_chunked_global_rows_with_runs_across_chunks():
+    """Global-row mode splits each query into 4,096-entry chunks; context runs
+    (conflicting objects) that straddle a chunk boundary are counted once, by the
+    chunk holding the run's first entry."""
+    ref = kssdgpu.synth(n_samples=40, n_clusters=4, len_median=1e6, len_min=5e5, len_max=2e6)
+    reads = kssdgpu.synth(n_samples=6, n_clusters=4, role=kssdgpu.ROLE_READS, sample_seed=7,
+                          ref_sample_seed=20261203, ref_samples=40, len_median=1e6, len_min=5e5, len_max=2e6,
+                          cov_lo=10, cov_hi=30)
+    keys = np.unique(reads.keys)
+    # widen the run at every chunk boundary: extra objects on the boundary entry's context
+    extra = []
+    for b in range(4096, len(keys), 4096):
+        ctx = int(keys[b]) >> 20
+        extra += [(ctx << 20) | int(o) for o in np.random.default_rng(b).integers(0, 1 << 20, 6)]
+    keys = np.unique(np.concatenate([keys, np.array(extra, dtype=np.uint64)]))
+    assert len(keys) > 3 * 4096
+    qk = np.concatenate([keys, ref.keys[ref.offs[3]:ref.offs[4]]])
+    qo = np.array([0, len(keys), len(qk)], dtype=np.uint64)
+    rec = oracle.build_index(ref.keys, ref.offs)
+    idx = kssdgpu.Index.from_records(rec, ref.n)
+    for flags in (0, kssdgpu.IGNORECONFLICT):
+        want = oracle.count_block(rec, ref.n, qk, qo, unique=True,
+                                  ignoreconflict=bool(flags & kssdgpu.IGNORECONFLICT))
+        for mode in (0, kssdgpu.GLOBAL_ACC):
+            got = idx.count_block(qk, qo, flags | mode | kssdgpu.UNIQUE)
+            for g, w in zip(got, want):
+                np.testing.assert_array_equal(g, w)
+        assert want[0][0, :, 0].sum() > 0
