@@ -169,6 +169,15 @@ int kssdgpu_self_lower_dev(kssdgpu_index_t *idx, unsigned flags, kssdgpu_ctx_mut
 int kssdgpu_self_plan_info(kssdgpu_index_t *idx, uint64_t *groups, uint64_t *postings, uint64_t *pairs);
 
 /*
+ * The self-join plan's autotuned setting (built on first use, like the plan):
+ * groups per set-major chunk, whether chunks run largest first, how many
+ * candidates the tuner timed (0: defaults kept) and the chosen candidate's join
+ * time in ms.  No reference counterpart (the CPU path has no tunables).
+ */
+int kssdgpu_self_plan_tuning(kssdgpu_index_t *idx, uint32_t *chunk_groups, int *sorted, int *candidates,
+                             float *join_ms);
+
+/*
  * Plain baseline kernel with device inputs: one launch per query (h_qry_offs is a
  * host copy of d_qry_offs, used to size each launch).  Outputs are zeroed unless
  * KSSDGPU_NO_ZERO.  Same counters as kssdgpu_count_block_dev.

@@ -17,6 +17,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <numeric>
@@ -530,8 +531,9 @@ __device__ __forceinline__ uint32_t warp_slot(unsigned int *counter, bool want, 
 
 // Classify the groups with >= 2 postings (one thread per group, whole warps):
 //   small   (k <= 32, one object per gid) -> (sort key, group) for the compact plan;
-//             key = (32 - k, gid0, gid1, gid2 >> 2) so equal-size groups over the same
-//             genomes end up side by side
+//             key = (32 - k, hash of the group's gid set) so that groups over the same
+//             genome set end up side by side (equal keys: the set-major join compares
+//             the gid lists themselves)
 //   big     (k > 32, one object per gid)  -> begin | k << 32
 //   conflict (a gid holds several objects) -> begin | k << 32
 // totals: [0] postings in listed groups, [1] pairs.
@@ -554,15 +556,14 @@ __global__ void __launch_bounds__(256) k_self_classify(const uint32_t *__restric
         k = gbeg[g + 1] - b;
         if (k >= 2) {
             uint32_t prev = (uint32_t)(post[b] >> 32);
-            const uint32_t g0 = prev, g1 = (uint32_t)(post[b + 1] >> 32);
-            const uint32_t g2 = k >= 3 ? (uint32_t)(post[b + 2] >> 32) : 0u;
+            unsigned long long h = mix64(prev + 1ull);
             for (uint32_t i = b + 1; i < b + k; ++i) {
                 const uint32_t gid = (uint32_t)(post[i] >> 32);
                 conflict |= gid == prev;
                 prev = gid;
+                h = mix64(h ^ (gid + 1ull));
             }
-            key = ((unsigned long long)(kJoinSmallMax - min(k, kJoinSmallMax)) << 58) |
-                  ((unsigned long long)g0 << 38) | ((unsigned long long)g1 << 18) | (g2 >> 2);
+            key = ((unsigned long long)(kJoinSmallMax - min(k, kJoinSmallMax)) << 58) | (h >> 6);
         } else {
             k = 0;
         }
@@ -627,66 +628,148 @@ __device__ __forceinline__ void join_pair(uint64_t pi, uint64_t pj, unsigned lon
         atomicAdd(oo + cell, inc_obj(d));
 }
 
-// One thread per small group of the compact plan; the warp steps through pair
-// slots in lockstep (groups sorted by size, so lanes carry equal work) and, at
-// every step, lanes holding the same counter cell as their neighbours add their
-// increments with a segmented warp scan: one atomic per run of equal cells.  The
-// four increments of a pair travel packed in 16-bit fields of one word (a run sums
-// at most 32 pairs, so no field exceeds 32 * 12).
-__global__ void __launch_bounds__(256) k_self_small(const unsigned long long *__restrict__ desc, uint32_t n,
-                                                    const uint64_t *__restrict__ jp,
-                                                    unsigned long long *__restrict__ oc,
-                                                    unsigned long long *__restrict__ oo)
+// Zero two 16-byte aligned arrays of `words` 8-byte counters.
+__global__ void __launch_bounds__(256) k_zero_pair(unsigned long long *__restrict__ a, unsigned long long *__restrict__ b,
+                                                   size_t words)
+{
+    const size_t n16 = words / 2;
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    ulonglong2 *a2 = reinterpret_cast<ulonglong2 *>(a), *b2 = reinterpret_cast<ulonglong2 *>(b);
+    const ulonglong2 z = make_ulonglong2(0ull, 0ull);
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n16; i += stride) {
+        a2[i] = z;
+        b2[i] = z;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0 && (words & 1)) {
+        a[words - 1] = 0;
+        b[words - 1] = 0;
+    }
+}
+
+// Set-major plan of the small groups.  Sorted groups with the same gid list form
+// a run (their pairs all land on the same k(k-1)/2 counter cells); runs are cut
+// into chunks of at most `csize` groups, and every (chunk, pair) is one work item
+// of the join: the item sums its pair's increments over the chunk's groups in
+// registers and adds them with one atomic per counter word.  Chunks are ordered by
+// size (largest first) so that the lanes of a warp loop over equal group counts.
+
+// heads[t] = 1 where sorted small group t starts a new run (size or gid list differs)
+__global__ void k_set_heads(const unsigned long long *__restrict__ desc, uint32_t n, const uint64_t *__restrict__ jp,
+                            uint32_t *__restrict__ heads)
+{
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        uint32_t h = 1;
+        if (t > 0) {
+            const unsigned long long d = desc[t], d0 = desc[t - 1];
+            const uint32_t k = (uint32_t)(d >> 32);
+            if (k == (uint32_t)(d0 >> 32)) {
+                h = 0;
+                const uint64_t *a = jp + (uint32_t)d, *b = jp + (uint32_t)d0;
+                for (uint32_t i = 0; i < k && !h; ++i)
+                    h = (uint32_t)(a[i] >> 32) != (uint32_t)(b[i] >> 32);
+            }
+        }
+        heads[t] = h;
+    }
+}
+
+// run starts: first[run] = t for every head (run = inclusive head count - 1)
+__global__ void k_set_run_first(const uint32_t *__restrict__ heads, const uint32_t *__restrict__ runs_incl, uint32_t n,
+                                uint32_t *__restrict__ first)
+{
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
+        if (heads[t])
+            first[runs_incl[t] - 1] = t;
+}
+
+// chunk heads: every csize-th group of a run, counted from the run's start
+__global__ void k_set_chunk_heads(const uint32_t *__restrict__ runs_incl, const uint32_t *__restrict__ first, uint32_t n,
+                                  uint32_t csize, uint32_t *__restrict__ cheads)
+{
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
+        cheads[t] = ((t - first[runs_incl[t] - 1]) % csize) == 0;
+}
+
+// chunk records {offset of the first group's postings, m | k << 32} and pair counts
+__global__ void k_set_chunks(const uint32_t *__restrict__ cheads, const uint32_t *__restrict__ cpos, uint32_t n,
+                             uint32_t csize, const unsigned long long *__restrict__ desc,
+                             ulonglong2 *__restrict__ chunks, uint32_t *__restrict__ skey, uint32_t *__restrict__ sval)
+{
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        if (!cheads[t])
+            continue;
+        const uint32_t c = cpos[t];
+        // the chunk ends at the next chunk head (every run start is one)
+        uint32_t e = t + 1;
+        while (e < n && e - t < csize && !cheads[e])
+            ++e;
+        const unsigned long long d = desc[t];
+        const uint32_t k = (uint32_t)(d >> 32);
+        chunks[c] = make_ulonglong2((unsigned long long)(uint32_t)d, (unsigned long long)(e - t) | ((unsigned long long)k << 32));
+        skey[c] = csize - (e - t);  // ascending key = descending group count
+        sval[c] = c;
+    }
+}
+
+// chunks in sorted order, with their pair counts
+__global__ void k_set_permute(const uint32_t *__restrict__ order, uint32_t nchunks, const ulonglong2 *__restrict__ in,
+                              ulonglong2 *__restrict__ out, uint32_t *__restrict__ npairs)
+{
+    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < nchunks; c += gridDim.x * blockDim.x) {
+        const ulonglong2 ch = in[order[c]];
+        const uint32_t k = (uint32_t)(ch.y >> 32);
+        out[c] = ch;
+        npairs[c] = k * (k - 1) / 2;
+    }
+}
+
+// items[item_off[c] + p] = c | i << 32 | j << 40 for the chunk's pairs (i < j)
+__global__ void k_set_items(const ulonglong2 *__restrict__ chunks, const uint32_t *__restrict__ item_off, uint32_t nchunks,
+                            unsigned long long *__restrict__ items)
+{
+    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < nchunks; c += gridDim.x * blockDim.x) {
+        const uint32_t k = (uint32_t)(chunks[c].y >> 32);
+        uint32_t o = item_off[c];
+        for (uint32_t j = 1; j < k; ++j)
+            for (uint32_t i = 0; i < j; ++i)
+                items[o++] = (unsigned long long)c | ((unsigned long long)i << 32) | ((unsigned long long)j << 40);
+    }
+}
+
+// The set-major join: one thread per (chunk, pair) item.  The m groups of the chunk
+// share their gid list, so the pair's counter cell is the same for all of them:
+// sum num_ctx (= m), mut2, diff_obj and section over the groups, then one atomic
+// per counter word.  The chunk's postings (m x k, contiguous) are read by all its
+// items, from L1.
+__global__ void __launch_bounds__(256) k_self_sets(const unsigned long long *__restrict__ items, uint32_t nitems,
+                                                   const ulonglong2 *__restrict__ chunks,
+                                                   const uint64_t *__restrict__ jp, unsigned long long *__restrict__ oc,
+                                                   unsigned long long *__restrict__ oo)
 {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    const unsigned lane = threadIdx.x & 31;
-    uint32_t off = 0, k = 0;
-    if (t < n) {
-        const unsigned long long d = __ldg(desc + t);
-        off = (uint32_t)d;
-        k = (uint32_t)(d >> 32);
+    if (t >= nitems)
+        return;
+    const unsigned long long it = __ldg(items + t);
+    const ulonglong2 ch = __ldg(chunks + (uint32_t)it);
+    const uint32_t i = (uint32_t)(it >> 32) & 0xFFu, j = (uint32_t)(it >> 40) & 0xFFu;
+    const uint32_t m = (uint32_t)ch.y, k = (uint32_t)(ch.y >> 32);
+    const uint64_t *g = jp + ch.x;
+    const uint32_t gi = (uint32_t)(__ldg(g + i) >> 32), gj = (uint32_t)(__ldg(g + j) >> 32);
+    // low (object) words of the postings
+    const uint32_t *w = reinterpret_cast<const uint32_t *>(g);
+    uint32_t mut2 = 0, dobj = 0, sect = 0;
+#pragma unroll 4
+    for (uint32_t x = 0; x < m; ++x) {
+        const uint32_t oi = __ldg(w + 2 * (x * k + i)), oj = __ldg(w + 2 * (x * k + j));
+        const uint32_t d = (uint32_t)min(kMinInit, dna_pop(oi ^ oj));
+        mut2 += d > 1;
+        dobj += d > 0;
+        sect += d;
     }
-    const uint32_t npairs = k >= 2 ? k * (k - 1) / 2 : 0u;
-    const uint32_t maxp = __reduce_max_sync(0xffffffffu, npairs);
-    uint32_t j = 1, i = 0;
-    uint64_t pj = npairs ? __ldg(jp + off + 1) : 0ull;
-    const unsigned below = (1u << lane) - 1u;
-    for (uint32_t p = 0; p < maxp; ++p) {
-        const bool act = p < npairs;
-        unsigned long long cell = ~0ull - lane;  // inactive lanes never join a run
-        unsigned long long inc = 0;              // num_ctx | mut2 << 16 | diff_obj << 32 | section << 48
-        if (act) {
-            const uint64_t pi = __ldg(jp + off + i);
-            const int d = min(kMinInit, dna_pop((uint32_t)pi ^ (uint32_t)pj));
-            cell = lower_cell((uint32_t)(pj >> 32), (uint32_t)(pi >> 32));
-            inc = 1ull | ((unsigned long long)(d > 1) << 16) | ((unsigned long long)(d > 0) << 32) |
-                  ((unsigned long long)d << 48);
-            if (++i == j) {
-                i = 0;
-                if (++j < k)
-                    pj = __ldg(jp + off + j);
-            }
-        }
-        const unsigned long long prev = __shfl_up_sync(0xffffffffu, cell, 1);
-        const unsigned heads = __ballot_sync(0xffffffffu, lane == 0 || prev != cell);
-        if (heads != 0xffffffffu) {  // some neighbours share a cell: sum their runs
-            const int seg_start = 31 - __clz(heads & (below | (1u << lane)));
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const unsigned long long up = __shfl_up_sync(0xffffffffu, inc, o);
-                if ((int)lane - o >= seg_start)
-                    inc += up;
-            }
-        }
-        const bool tail = lane == 31 || ((heads >> (lane + 1)) & 1u);
-        if (act && tail) {
-            const unsigned long long nctx = inc & 0xFFFFull, mut2 = (inc >> 16) & 0xFFFFull;
-            const unsigned long long dobj = (inc >> 32) & 0xFFFFull, sect = inc >> 48;
-            atomicAdd(oc + cell, nctx | (mut2 << 32));
-            if (dobj)
-                atomicAdd(oo + cell, dobj | (sect << 32));
-        }
-    }
+    const size_t cell = lower_cell(gj, gi);
+    atomicAdd(oc + cell, (unsigned long long)m | ((unsigned long long)mut2 << 32));
+    if (dobj)
+        atomicAdd(oo + cell, (unsigned long long)dobj | ((unsigned long long)sect << 32));
 }
 
 // One warp per big group: lanes stride over its k(k-1)/2 pairs.
@@ -809,6 +892,13 @@ struct kssdgpu_index {
     // big and conflict groups (begin | k << 32 into post)
     DevBuf<unsigned long long> j_small, j_big, j_conf;
     DevBuf<uint64_t> j_post;
+    DevBuf<ulonglong2> j_chunks;            // set-major chunks of the small groups
+    DevBuf<unsigned long long> j_items;     // (chunk, pair) work items
+    uint32_t j_nchunks = 0, j_nitems = 0;
+    uint32_t j_chunk_size = 32;             // groups per set-major chunk (1..255)
+    bool j_sort_chunks = true;              // chunks ordered by group count, largest first
+    int j_tune_tried = 0;                   // autotuner candidates timed (0: defaults kept)
+    float j_tune_ms = 0;                    // the chosen candidate's join time
     uint32_t j_n[3] = {0, 0, 0};
     unsigned long long j_postings = 0, j_pairs = 0;
     bool j_ready = false;
@@ -1085,6 +1175,188 @@ int count_host_impl(kssdgpu_index *ix, const uint64_t *qkeys, const uint64_t *qo
     return check_dev_err(ix, st);
 }
 
+// Runs of equal gid lists among the n sorted small groups -> chunks -> (chunk, pair)
+// items (j_chunks, j_items); the per-group descriptors are released afterwards.
+// Plan knobs, overridable for tuning: KSSDGPU_JOIN_CHUNK (groups per chunk, 1..255)
+// and KSSDGPU_JOIN_SORT (0: chunks in plan order).
+uint32_t env_u32(const char *name, uint32_t def, uint32_t lo, uint32_t hi)
+{
+    const char *v = std::getenv(name);
+    if (!v || !*v)
+        return def;
+    const unsigned long x = std::strtoul(v, nullptr, 10);
+    return x < lo ? lo : x > hi ? hi : (uint32_t)x;
+}
+
+cudaError_t set_major_plan(kssdgpu_index *ix, uint32_t n, cudaStream_t st)
+{
+    ix->j_chunk_size = env_u32("KSSDGPU_JOIN_CHUNK", ix->j_chunk_size, 1, 255);
+    ix->j_sort_chunks = env_u32("KSSDGPU_JOIN_SORT", ix->j_sort_chunks ? 1 : 0, 0, 1) != 0;
+    const uint32_t csize = ix->j_chunk_size;
+    uint32_t *heads = nullptr, *runs = nullptr, *first = nullptr, *cheads = nullptr, *cpos = nullptr;
+    uint32_t *skey = nullptr, *skey2 = nullptr, *sval = nullptr, *sval2 = nullptr, *npairs = nullptr, *ioff = nullptr;
+    ulonglong2 *chunks0 = nullptr;
+    void *tmp = nullptr;
+    auto cleanup = [&]() {
+        cudaFree(heads); cudaFree(runs); cudaFree(first); cudaFree(cheads); cudaFree(cpos);
+        cudaFree(skey); cudaFree(skey2); cudaFree(sval); cudaFree(sval2); cudaFree(npairs); cudaFree(ioff);
+        cudaFree(chunks0); cudaFree(tmp);
+    };
+    size_t tb1 = 0, tb2 = 0, tb3 = 0;
+    cudaError_t e = cudaMalloc(&heads, (size_t)n * 4);
+    if (e == cudaSuccess) e = cudaMalloc(&runs, (size_t)n * 4);
+    if (e == cudaSuccess) e = cudaMalloc(&first, (size_t)n * 4);
+    if (e == cudaSuccess) e = cudaMalloc(&cheads, (size_t)n * 4);
+    if (e == cudaSuccess) e = cudaMalloc(&cpos, (size_t)n * 4);
+    if (e == cudaSuccess) e = cudaMalloc(&skey, (size_t)n * 4);
+    if (e == cudaSuccess) e = cudaMalloc(&skey2, (size_t)n * 4);
+    if (e == cudaSuccess) e = cudaMalloc(&sval, (size_t)n * 4);
+    if (e == cudaSuccess) e = cudaMalloc(&sval2, (size_t)n * 4);
+    if (e == cudaSuccess) e = cudaMalloc(&npairs, (size_t)n * 4);
+    if (e == cudaSuccess) e = cudaMalloc(&ioff, (size_t)n * 4);
+    if (e == cudaSuccess) e = cudaMalloc(&chunks0, (size_t)n * sizeof(ulonglong2));
+    if (e == cudaSuccess) e = cub::DeviceScan::InclusiveSum(nullptr, tb1, heads, runs, n, st);
+    if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(nullptr, tb2, cheads, cpos, n, st);
+    if (e == cudaSuccess) e = cub::DeviceRadixSort::SortPairs(nullptr, tb3, skey, skey2, sval, sval2, n, 0, 16, st);
+    const size_t tb = std::max<size_t>(std::max(std::max(tb1, tb2), tb3), 1);
+    if (e == cudaSuccess) e = cudaMalloc(&tmp, tb);
+    if (e == cudaSuccess) {
+        k_set_heads<<<grid_for(n), 256, 0, st>>>(ix->j_small.p, n, ix->j_post.p, heads);
+        count_launch();
+        size_t b = tb;
+        e = cub::DeviceScan::InclusiveSum(tmp, b, heads, runs, n, st);
+        count_launch(2);
+    }
+    if (e == cudaSuccess) {
+        k_set_run_first<<<grid_for(n), 256, 0, st>>>(heads, runs, n, first);
+        k_set_chunk_heads<<<grid_for(n), 256, 0, st>>>(runs, first, n, csize, cheads);
+        count_launch(2);
+        size_t b = tb;
+        e = cub::DeviceScan::ExclusiveSum(tmp, b, cheads, cpos, n, st);
+        count_launch(2);
+    }
+    uint32_t last_pos = 0, last_head = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&last_pos, cpos + n - 1, 4, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&last_head, cheads + n - 1, 4, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    const uint32_t nchunks = last_pos + last_head;
+    if (e == cudaSuccess) e = ix->j_chunks.ensure(nchunks);
+    if (e == cudaSuccess) {
+        k_set_chunks<<<grid_for(n), 256, 0, st>>>(cheads, cpos, n, csize, ix->j_small.p, chunks0, skey, sval);
+        count_launch();
+        const uint32_t *order = sval;
+        if (ix->j_sort_chunks) {
+            size_t b = tb;
+            e = cub::DeviceRadixSort::SortPairs(tmp, b, skey, skey2, sval, sval2, nchunks, 0, 16, st);
+            count_launch(4);
+            order = sval2;
+        }
+        if (e == cudaSuccess) {
+            k_set_permute<<<grid_for(nchunks), 256, 0, st>>>(order, nchunks, chunks0, ix->j_chunks.p, npairs);
+            count_launch();
+            size_t b = tb;
+            e = cub::DeviceScan::ExclusiveSum(tmp, b, npairs, ioff, nchunks, st);
+            count_launch(2);
+        }
+    }
+    uint32_t last_off = 0, last_np = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&last_off, ioff + nchunks - 1, 4, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&last_np, npairs + nchunks - 1, 4, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    const uint64_t nitems = (uint64_t)last_off + last_np;
+    if (e == cudaSuccess && nitems >= (1ull << 32))
+        e = cudaErrorMemoryAllocation;  // more join items than one 32-bit launch index covers
+    if (e == cudaSuccess) e = ix->j_items.ensure(nitems);
+    if (e == cudaSuccess) {
+        k_set_items<<<grid_for(nchunks), 256, 0, st>>>(ix->j_chunks.p, ioff, nchunks, ix->j_items.p);
+        count_launch();
+        e = cudaStreamSynchronize(st);
+    }
+    cleanup();
+    if (e == cudaSuccess) {
+        ix->j_nchunks = nchunks;
+        ix->j_nitems = (uint32_t)nitems;
+    }
+    return e;
+}
+
+// Autotuner of the set-major join: every candidate (groups per chunk, chunk order)
+// is planned and timed on scratch counters (CUDA events, best of three after one
+// warm-up run; the scratch is zeroed once: accumulating into nonzero counters
+// costs the same); the fastest stays.  Skipped, keeping the defaults, when
+// KSSDGPU_TUNE=0, when a knob is pinned by its environment variable, or when the
+// scratch counters would take more than a quarter of the free device memory.
+cudaError_t tune_join(kssdgpu_index *ix, uint32_t n, cudaStream_t st)
+{
+    const bool pinned = std::getenv("KSSDGPU_JOIN_CHUNK") || std::getenv("KSSDGPU_JOIN_SORT");
+    if (!env_u32("KSSDGPU_TUNE", 1, 0, 1) || pinned)
+        return set_major_plan(ix, n, st);
+    const size_t cells = std::max<size_t>((size_t)ix->nref * (ix->nref - 1) / 2, 1);
+    size_t free_b = 0, total_b = 0;
+    cudaError_t e = cudaMemGetInfo(&free_b, &total_b);
+    if (e != cudaSuccess || cells * 16 > free_b / 4)
+        return set_major_plan(ix, n, st);
+    unsigned long long *oc = nullptr, *oo = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    e = cudaMalloc(&oc, cells * 8);
+    if (e == cudaSuccess) e = cudaMalloc(&oo, cells * 8);
+    if (e == cudaSuccess) e = cudaEventCreate(&ev0);
+    if (e == cudaSuccess) e = cudaEventCreate(&ev1);
+    // chunk order: largest first for every size; plan order once, at the default size
+    static const struct { uint32_t size; bool sorted; } kCands[] = {
+        {8, true}, {16, true}, {32, true}, {64, true}, {128, true}, {32, false}};
+    float best = 1e30f;
+    uint32_t best_size = ix->j_chunk_size;
+    bool best_sort = ix->j_sort_chunks;
+    int tried = 0;
+    if (e == cudaSuccess) e = cudaMemsetAsync(oc, 0, cells * 8, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(oo, 0, cells * 8, st);
+    for (const auto &cand : kCands) {
+        if (e != cudaSuccess)
+            break;
+        const uint32_t cs = cand.size;
+        const int srt = cand.sorted ? 1 : 0;
+        ix->j_chunk_size = cs;
+        ix->j_sort_chunks = srt != 0;
+        e = set_major_plan(ix, n, st);
+        float t_min = 1e30f;
+        for (int r = 0; r < 4 && e == cudaSuccess; ++r) {
+            e = cudaEventRecord(ev0, st);
+            if (e == cudaSuccess && ix->j_nitems) {
+                k_self_sets<<<(ix->j_nitems + 255) / 256, 256, 0, st>>>(ix->j_items.p, ix->j_nitems, ix->j_chunks.p,
+                                                                        ix->j_post.p, oc, oo);
+                count_launch();
+                e = cudaGetLastError();
+            }
+            if (e == cudaSuccess) e = cudaEventRecord(ev1, st);
+            if (e == cudaSuccess) e = cudaEventSynchronize(ev1);
+            float ms = 0;
+            if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, ev0, ev1);
+            if (e == cudaSuccess && r > 0)
+                t_min = std::min(t_min, ms);
+        }
+        if (e != cudaSuccess)
+            break;
+        ++tried;
+        if (t_min < best) {
+            best = t_min;
+            best_size = cs;
+            best_sort = srt != 0;
+        }
+    }
+    cudaFree(oc);
+    cudaFree(oo);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (e != cudaSuccess)
+        return e;
+    ix->j_chunk_size = best_size;
+    ix->j_sort_chunks = best_sort;
+    ix->j_tune_tried = tried;
+    ix->j_tune_ms = best;
+    return set_major_plan(ix, n, st);
+}
+
 int self_plan(kssdgpu_index *ix, cudaStream_t st)
 {
     if (ix->j_ready)
@@ -1153,6 +1425,9 @@ int self_plan(kssdgpu_index *ix, cudaStream_t st)
             count_launch();
             e = cudaStreamSynchronize(st);
         }
+        if (e == cudaSuccess)
+            e = tune_join(ix, n, st);
+        ix->j_small.release();
     }
     cleanup();
     if (e != cudaSuccess)
@@ -1174,11 +1449,20 @@ int self_lower_dev_impl(kssdgpu_index *ix, unsigned flags, unsigned long long *o
         return rc;
     const size_t cells = (size_t)ix->nref * (ix->nref - 1) / 2;
     if (!(flags & KSSDGPU_NO_ZERO)) {
-        CUDA_TRY(cudaMemsetAsync(oc, 0, std::max<size_t>(cells, 1) * 8, st));
-        CUDA_TRY(cudaMemsetAsync(oo, 0, std::max<size_t>(cells, 1) * 8, st));
+        const size_t words = std::max<size_t>(cells, 1);
+        if ((((uintptr_t)oc | (uintptr_t)oo) & 15) == 0) {
+            // both counter arrays in one launch, 16-byte stores
+            k_zero_pair<<<ix->sms * 8, 256, 0, st>>>(oc, oo, words);
+            count_launch();
+            CUDA_TRY(cudaGetLastError());
+        } else {
+            CUDA_TRY(cudaMemsetAsync(oc, 0, words * 8, st));
+            CUDA_TRY(cudaMemsetAsync(oo, 0, words * 8, st));
+        }
     }
-    if (ix->j_n[0]) {
-        k_self_small<<<(ix->j_n[0] + 255) / 256, 256, 0, st>>>(ix->j_small.p, ix->j_n[0], ix->j_post.p, oc, oo);
+    if (ix->j_nitems) {
+        k_self_sets<<<(ix->j_nitems + 255) / 256, 256, 0, st>>>(ix->j_items.p, ix->j_nitems, ix->j_chunks.p,
+                                                                ix->j_post.p, oc, oo);
         count_launch();
     }
     if (ix->j_n[1]) {
@@ -1423,6 +1707,8 @@ void kssdgpu_index_free(kssdgpu_index_t *ix)
     ix->s_items.release();
     ix->j_small.release();
     ix->j_post.release();
+    ix->j_chunks.release();
+    ix->j_items.release();
     ix->j_big.release();
     ix->j_conf.release();
     delete ix;
@@ -1625,6 +1911,21 @@ int kssdgpu_self_plan_info(kssdgpu_index_t *ix, uint64_t *groups, uint64_t *post
     if (groups) *groups = (uint64_t)ix->j_n[0] + ix->j_n[1] + ix->j_n[2];
     if (postings) *postings = ix->j_postings;
     if (pairs) *pairs = ix->j_pairs;
+    return KSSDGPU_OK;
+}
+
+int kssdgpu_self_plan_tuning(kssdgpu_index_t *ix, uint32_t *chunk_groups, int *sorted, int *candidates, float *join_ms)
+{
+    if (!ix)
+        return fail(KSSDGPU_ERR_ARG, "null index");
+    CUDA_TRY(cudaSetDevice(ix->device));
+    int rc = self_plan(ix, 0);
+    if (rc)
+        return rc;
+    if (chunk_groups) *chunk_groups = ix->j_chunk_size;
+    if (sorted) *sorted = ix->j_sort_chunks ? 1 : 0;
+    if (candidates) *candidates = ix->j_tune_tried;
+    if (join_ms) *join_ms = ix->j_tune_ms;
     return KSSDGPU_OK;
 }
 
