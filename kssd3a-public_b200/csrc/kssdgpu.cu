@@ -897,6 +897,7 @@ struct kssdgpu_index {
     uint32_t j_nchunks = 0, j_nitems = 0;
     uint32_t j_chunk_size = 32;             // groups per set-major chunk (1..255)
     bool j_sort_chunks = true;              // chunks ordered by group count, largest first
+    bool j_tuned = false;                   // the autotuner ran for this index
     int j_tune_tried = 0;                   // autotuner candidates timed (0: defaults kept)
     float j_tune_ms = 0;                    // the chosen candidate's join time
     uint32_t j_n[3] = {0, 0, 0};
@@ -1283,14 +1284,16 @@ cudaError_t set_major_plan(kssdgpu_index *ix, uint32_t n, cudaStream_t st)
 // Autotuner of the set-major join: every candidate (groups per chunk, chunk order)
 // is planned and timed on scratch counters (CUDA events, best of three after one
 // warm-up run; the scratch is zeroed once: accumulating into nonzero counters
-// costs the same); the fastest stays.  Skipped, keeping the defaults, when
-// KSSDGPU_TUNE=0, when a knob is pinned by its environment variable, or when the
-// scratch counters would take more than a quarter of the free device memory.
+// costs the same); the fastest stays.  Runs once per index, on request
+// (kssdgpu_self_plan_tune) or at plan time with KSSDGPU_TUNE=1; keeps the defaults
+// when a knob is pinned by its environment variable or when the scratch counters
+// would take more than a quarter of the free device memory.
 cudaError_t tune_join(kssdgpu_index *ix, uint32_t n, cudaStream_t st)
 {
+    ix->j_tuned = true;
     const bool pinned = std::getenv("KSSDGPU_JOIN_CHUNK") || std::getenv("KSSDGPU_JOIN_SORT");
-    if (!env_u32("KSSDGPU_TUNE", 1, 0, 1) || pinned)
-        return set_major_plan(ix, n, st);
+    if (pinned || n == 0)
+        return n ? set_major_plan(ix, n, st) : cudaSuccess;
     const size_t cells = std::max<size_t>((size_t)ix->nref * (ix->nref - 1) / 2, 1);
     size_t free_b = 0, total_b = 0;
     cudaError_t e = cudaMemGetInfo(&free_b, &total_b);
@@ -1426,8 +1429,7 @@ int self_plan(kssdgpu_index *ix, cudaStream_t st)
             e = cudaStreamSynchronize(st);
         }
         if (e == cudaSuccess)
-            e = tune_join(ix, n, st);
-        ix->j_small.release();
+            e = env_u32("KSSDGPU_TUNE", 0, 0, 1) ? tune_join(ix, n, st) : set_major_plan(ix, n, st);
     }
     cleanup();
     if (e != cudaSuccess)
@@ -1914,7 +1916,7 @@ int kssdgpu_self_plan_info(kssdgpu_index_t *ix, uint64_t *groups, uint64_t *post
     return KSSDGPU_OK;
 }
 
-int kssdgpu_self_plan_tuning(kssdgpu_index_t *ix, uint32_t *chunk_groups, int *sorted, int *candidates, float *join_ms)
+int kssdgpu_self_plan_tune(kssdgpu_index_t *ix, uint32_t *chunk_groups, int *sorted, int *candidates, float *join_ms)
 {
     if (!ix)
         return fail(KSSDGPU_ERR_ARG, "null index");
@@ -1922,6 +1924,12 @@ int kssdgpu_self_plan_tuning(kssdgpu_index_t *ix, uint32_t *chunk_groups, int *s
     int rc = self_plan(ix, 0);
     if (rc)
         return rc;
+    if (!ix->j_tuned) {
+        const cudaError_t e = tune_join(ix, ix->j_n[0], 0);
+        if (e != cudaSuccess)
+            return fail(e == cudaErrorMemoryAllocation ? KSSDGPU_ERR_NOMEM : KSSDGPU_ERR_CUDA,
+                        std::string("self-join autotuner: ") + cudaGetErrorString(e));
+    }
     if (chunk_groups) *chunk_groups = ix->j_chunk_size;
     if (sorted) *sorted = ix->j_sort_chunks ? 1 : 0;
     if (candidates) *candidates = ix->j_tune_tried;

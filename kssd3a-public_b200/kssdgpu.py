@@ -68,7 +68,7 @@ def gpu_lib() -> C.CDLL:
         lib.kssdgpu_sync.argtypes = [vp, vp]
         lib.kssdgpu_self_lower.argtypes = [vp, C.c_uint, vp, vp]
         lib.kssdgpu_self_lower_dev.argtypes = [vp, C.c_uint, vp, vp, vp]
-        lib.kssdgpu_self_plan_tuning.argtypes = [vp, C.POINTER(C.c_uint32), C.POINTER(C.c_int),
+        lib.kssdgpu_self_plan_tune.argtypes = [vp, C.POINTER(C.c_uint32), C.POINTER(C.c_int),
                                                  C.POINTER(C.c_int), C.POINTER(C.c_float)]
         lib.kssdgpu_self_plan_info.argtypes = [vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
                                                C.POINTER(C.c_uint64)]
@@ -369,9 +369,10 @@ class Index:
                                                  qry_gid_offset, int(lower), flags, _ptr(d_ctx), _ptr(d_obj),
                                                  _ptr(d_uctx), _ptr(d_uobj), _ptr(stream)))
 
-    def self_plan_tuning(self):
+    def self_plan_tune(self):
+        """Autotune the self-join plan (once per index); returns the setting in use."""
         c, so, n, ms = C.c_uint32(), C.c_int(), C.c_int(), C.c_float()
-        _check(gpu_lib().kssdgpu_self_plan_tuning(self._h, C.byref(c), C.byref(so), C.byref(n), C.byref(ms)))
+        _check(gpu_lib().kssdgpu_self_plan_tune(self._h, C.byref(c), C.byref(so), C.byref(n), C.byref(ms)))
         return dict(chunk_groups=c.value, sorted=bool(so.value), candidates=n.value, join_ms=ms.value)
 
     def self_plan_info(self):
