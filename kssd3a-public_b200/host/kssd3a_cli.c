@@ -425,6 +425,82 @@ static void write_buf(FILE *f, const kssd_buf_t *b)
         err(EXIT_FAILURE, "Cannot write ANI output");
 }
 
+/* Ordered background writer: chunks of formatted rows handed over in order are
+ * written by one thread while the caller formats the next chunk (at most one chunk
+ * queued behind the one being written). */
+typedef struct {
+    kssd_buf_t *rows;
+    int nb;
+} wchunk_t;
+
+typedef struct {
+    FILE *f;
+    pthread_t th;
+    pthread_mutex_t mu;
+    pthread_cond_t cv;
+    wchunk_t q[2];
+    int head, count;
+    bool done;
+} owriter_t;
+
+static void *owriter_main(void *arg)
+{
+    owriter_t *w = arg;
+    for (;;) {
+        pthread_mutex_lock(&w->mu);
+        while (!w->count && !w->done)
+            pthread_cond_wait(&w->cv, &w->mu);
+        if (!w->count) {
+            pthread_mutex_unlock(&w->mu);
+            return NULL;
+        }
+        const wchunk_t c = w->q[w->head];
+        pthread_mutex_unlock(&w->mu);
+        for (int i = 0; i < c.nb; ++i) {
+            write_buf(w->f, &c.rows[i]);
+            kssd_buf_free(&c.rows[i]);
+        }
+        free(c.rows);
+        pthread_mutex_lock(&w->mu);
+        w->head = (w->head + 1) % 2;
+        w->count--;
+        pthread_cond_broadcast(&w->cv);
+        pthread_mutex_unlock(&w->mu);
+    }
+}
+
+static void owriter_start(owriter_t *w, FILE *f)
+{
+    memset(w, 0, sizeof *w);
+    w->f = f;
+    pthread_mutex_init(&w->mu, NULL);
+    pthread_cond_init(&w->cv, NULL);
+    if (pthread_create(&w->th, NULL, owriter_main, w) != 0)
+        errx(EXIT_FAILURE, "cannot start the output writer thread");
+}
+
+static void owriter_push(owriter_t *w, kssd_buf_t *rows, int nb)
+{
+    pthread_mutex_lock(&w->mu);
+    while (w->count == 2)
+        pthread_cond_wait(&w->cv, &w->mu);
+    w->q[(w->head + w->count) % 2] = (wchunk_t){rows, nb};
+    w->count++;
+    pthread_cond_broadcast(&w->cv);
+    pthread_mutex_unlock(&w->mu);
+}
+
+static void owriter_finish(owriter_t *w)
+{
+    pthread_mutex_lock(&w->mu);
+    w->done = true;
+    pthread_cond_broadcast(&w->cv);
+    pthread_mutex_unlock(&w->mu);
+    pthread_join(w->th, NULL);
+    pthread_mutex_destroy(&w->mu);
+    pthread_cond_destroy(&w->cv);
+}
+
 /* KSSD3A_TIMING=1: phase timings on stderr */
 static double g_t_last = -1.0;
 static void phase(const char *what)
@@ -921,6 +997,16 @@ static void self_lower_counts(const kssd_sketch_t *s, const char *dir, bool inde
     kssdgpu_obj_section_t *lo = malloc(cells * sizeof(*lo) + 8);
     if (!lc || !lo)
         err(EXIT_FAILURE, "OOM lower triangle");
+    /* map the pages on all cores before the device copies land there: a copy into
+     * untouched memory runs at page-fault speed */
+    const size_t pieces = (cells * sizeof(*lc) + (8u << 20) - 1) / (8u << 20);
+#pragma omp parallel for schedule(dynamic, 1) num_threads(g.o.p)
+    for (size_t k = 0; k < pieces; ++k) {
+        const size_t off = k * (8u << 20), len = cells * sizeof(*lc) - off < (8u << 20) ? cells * sizeof(*lc) - off
+                                                                                         : (8u << 20);
+        memset((char *)lc + off, 0, len);
+        memset((char *)lo + off, 0, len);
+    }
     const unsigned flags = g.o.ignoreconflict ? KSSDGPU_IGNORECONFLICT : 0;
     if (index_file) {
         size_t nrec = 0;
@@ -1014,7 +1100,11 @@ static double *self_lower_metrics(const kssd_sketch_t *s, const kssdgpu_ctx_mut2
 
 static void print_self_full_fixed6(const kssd_sketch_t *s, const double *m)
 {
-    /* comb_sortedsketch64_indexed_self_full printing, src/command_ani.c:1711-1746 */
+    /* comb_sortedsketch64_indexed_self_full printing, src/command_ani.c:1711-1746.
+     * Rows go out in chunks of B: the chunk's scaled values are first gathered into a
+     * B x n tile (the lower triangle read along rows for r < q and along columns for
+     * r > q, both contiguous), then rows are formatted in parallel from the tile while
+     * the previous chunk is being written. */
     const int n = s->n;
     FILE *out = open_out(g.outf);
     kssd_buf_t h = {0};
@@ -1026,33 +1116,61 @@ static void print_self_full_fixed6(const kssd_sketch_t *s, const double *m)
     write_buf(out, &h);
     kssd_buf_free(&h);
     const int32_t diag = kssd_scale_fixed6(kssd_matrix_diagonal_value(&g.o));
-    const int chunk = 256;
-    for (int q0 = 0; q0 < n; q0 += chunk) {
-        const int nb = n - q0 < chunk ? n - q0 : chunk;
+    const int B = 256;
+    int32_t *tile = malloc((size_t)B * (size_t)(n > 0 ? n : 1) * sizeof(int32_t));
+    if (!tile)
+        err(EXIT_FAILURE, "OOM output tile");
+    const int threads = g.o.p > 0 ? g.o.p : 1;
+    int cb = n / (threads * 4);
+    if (cb < 64)
+        cb = 64;
+    owriter_t w;
+    owriter_start(&w, out);
+    for (int q0 = 0; q0 < n; q0 += B) {
+        const int nb = n - q0 < B ? n - q0 : B;
+#pragma omp parallel for schedule(dynamic, 1) num_threads(g.o.p)
+        for (int rb = 0; rb < n; rb += cb) {
+            const int re = n - rb < cb ? n : rb + cb;
+            for (int i = 0; i < nb; ++i) {
+                /* r < q: row q of the triangle */
+                const int q = q0 + i;
+                int32_t *t = tile + (size_t)i * n;
+                const double *mq = m + (size_t)q * (size_t)(q > 0 ? q - 1 : 0) / 2;
+                const int e = re < q ? re : q;
+                for (int r = rb; r < e; ++r)
+                    t[r] = kssd_scale_fixed6(mq[r]);
+                if (q >= rb && q < re)
+                    t[q] = diag;
+            }
+            for (int r = rb; r < re; ++r) {
+                /* r > q: column q of the triangle, contiguous over the chunk's rows */
+                const int iend = r - q0 < nb ? r - q0 : nb;
+                if (iend <= 0)
+                    continue;
+                const double *mr = m + (size_t)r * (size_t)(r - 1) / 2 + q0;
+                for (int i = 0; i < iend; ++i)
+                    tile[(size_t)i * n + r] = kssd_scale_fixed6(mr[i]);
+            }
+        }
         kssd_buf_t *rows = calloc((size_t)nb, sizeof(kssd_buf_t));
+        if (!rows)
+            err(EXIT_FAILURE, "OOM output rows");
 #pragma omp parallel for schedule(dynamic, 1) num_threads(g.o.p)
         for (int i = 0; i < nb; ++i) {
-            const int q = q0 + i;
             kssd_buf_t *b = &rows[i];
+            const int32_t *t = tile + (size_t)i * n;
             kssd_buf_reserve(b, (size_t)n * 10 + PATHLEN);
-            kssd_buf_puts(b, s->names[q]);
+            kssd_buf_puts(b, s->names[q0 + i]);
             for (int r = 0; r < n; ++r) {
-                int32_t v = diag;
-                if (q > r)
-                    v = kssd_scale_fixed6(m[(size_t)q * (q - 1) / 2 + r]);
-                else if (q < r)
-                    v = kssd_scale_fixed6(m[(size_t)r * (r - 1) / 2 + q]);
                 kssd_buf_putc(b, '\t');
-                kssd_put_scaled6(b, v);
+                kssd_put_scaled6(b, t[r]);
             }
             kssd_buf_putc(b, '\n');
         }
-        for (int i = 0; i < nb; ++i) {
-            write_buf(out, &rows[i]);
-            kssd_buf_free(&rows[i]);
-        }
-        free(rows);
+        owriter_push(&w, rows, nb);
     }
+    owriter_finish(&w);
+    free(tile);
     close_out(out);
 }
 

@@ -9,6 +9,7 @@
 #include "kssd_format.h"
 
 #include <errno.h>
+#include <fcntl.h>
 #include <stdarg.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -35,36 +36,55 @@ bool kssd_file_exists(const char *dir, const char *name)
     return access(p, F_OK) == 0;
 }
 
+/* Whole file into memory; large files are read in 64 MB pieces by parallel pread
+ * (page-cache copies and first-touch page faults spread over the host cores). */
 static void *read_all(const char *dir, const char *name, size_t *size)
 {
     char p[4096];
     snprintf(p, sizeof p, "%s/%s", dir, name);
-    FILE *f = fopen(p, "rb");
-    if (!f) {
+    const int fd = open(p, O_RDONLY);
+    if (fd < 0) {
         set_err("cannot open %s: %s", p, strerror(errno));
         return NULL;
     }
-    if (fseeko(f, 0, SEEK_END) != 0) {
-        fclose(f);
-        set_err("cannot seek %s", p);
+    struct stat st;
+    if (fstat(fd, &st) != 0) {
+        close(fd);
+        set_err("cannot stat %s", p);
         return NULL;
     }
-    off_t len = ftello(f);
-    rewind(f);
-    void *buf = malloc(len > 0 ? (size_t)len : 1);
+    const size_t len = (size_t)st.st_size;
+    char *buf = malloc(len > 0 ? len : 1);
     if (!buf) {
-        fclose(f);
-        set_err("out of memory reading %s (%lld bytes)", p, (long long)len);
+        close(fd);
+        set_err("out of memory reading %s (%zu bytes)", p, len);
         return NULL;
     }
-    if (len > 0 && fread(buf, 1, (size_t)len, f) != (size_t)len) {
+    const size_t piece = (size_t)64 << 20;
+    const long npieces = (long)((len + piece - 1) / piece);
+    int bad = 0;
+#pragma omp parallel for schedule(dynamic, 1) reduction(| : bad) if (npieces > 1)
+    for (long c = 0; c < npieces; ++c) {
+        const size_t off = (size_t)c * piece, want = len - off < piece ? len - off : piece;
+        size_t got = 0;
+        while (got < want) {
+            const ssize_t r = pread(fd, buf + off + got, want - got, (off_t)(off + got));
+            if (r < 0 && errno == EINTR)
+                continue;
+            if (r <= 0) {
+                bad = 1;
+                break;
+            }
+            got += (size_t)r;
+        }
+    }
+    close(fd);
+    if (bad) {
         free(buf);
-        fclose(f);
         set_err("short read on %s", p);
         return NULL;
     }
-    fclose(f);
-    *size = (size_t)len;
+    *size = len;
     return buf;
 }
 
