@@ -381,7 +381,8 @@ def run_ours(args, rank, world, local_rank):
                               "frac": step_bytes / (ms_step / 1e3) / 1e9 / peak,
                               "what": "zero fill of the dense lower triangle + self join"},
             "kernels": {
-                "batched_probe": {"ms": ms_probe, "value": world * n * n / (ms_probe / 1e3)},
+                "batched_probe": {"ms": ms_probe, "value": world * n * n / (ms_probe / 1e3),
+                                  "contexts_probed_per_s": world * int(sk.offs[-1]) / (ms_probe / 1e3)},
                 "plain_per_query": {"ms": ms_plain, "value": world * n * n / (ms_plain / 1e3), "launches": n},
                 "self_join_vs_plain": ms_plain / ms_step, "batched_probe_vs_plain": ms_plain / ms_probe,
             },
@@ -602,7 +603,7 @@ def run_rect(args, rank):
             "config": {"queries": nq, "refs": nr, "query_keys": qkeys, "ref_entries": int(ref.offs[-1]),
                        "accumulators": "global (reference row exceeds shared memory)" if nr * 16 > 112 * 1024
                        else "shared"},
-            "graph_replay_ms": graph_ms,
+            "graph_replay_ms": graph_ms, "contexts_probed_per_s": qkeys / (ms_b / 1e3),
             "plain_per_query": {"ms": ms_p, "value": cells / (ms_p / 1e3), "launches": nq},
             "batched_vs_plain": ms_p / ms_b,
             "roofline_probe_model": {"bound": "hbm", "bytes": probe_bytes,
@@ -611,6 +612,89 @@ def run_rect(args, rank):
             "cpu_baseline": {"value": len(sample) * nr / cpu_s, "unit": "genome-pairs/s",
                              "cores": os.cpu_count(), "kind": "reference" if oracle.ref_available() else "port",
                              "sample": f"{len(sample)} queries", "counts_match_gpu": same}}
+    print(json.dumps(line), flush=True)
+    idx.close()
+    return 0
+
+
+def run_reads(args, rank):
+    """Read sets: --reads-samples samples, each a mix of 1-5 genomes of a --rect-refs
+    genome reference at 5-50x with 0.1-1% substitution errors (conflicts kept, as
+    `sketch --asone --conflict -A`), counted against the reference index with unique
+    contexts (`ani --qraw ... --unique-ctx`): one batched launch, key-range chunks
+    built on the device, vs the plain per-query kernel; the reference's own counting
+    function timed on a sample."""
+    import torch
+    import kssdgpu
+    if rank != 0:
+        return 0
+    nr, nq = args.rect_refs, args.reads_samples
+    seed = 20261203 + 4
+    clusters = max(1, nr // 10)
+    ref = kssdgpu.synth(n_samples=nr, n_clusters=clusters, size_dist=kssdgpu.SIZE_LOGNORMAL, len_median=4e6,
+                        len_sigma=0.37, len_min=1e6, len_max=12e6, sub_lo=0.001, sub_hi=0.2, seed=seed,
+                        sample_seed=seed, threads=os.cpu_count() or 8)
+    qry = kssdgpu.synth(n_samples=nq, n_clusters=clusters, role=kssdgpu.ROLE_READS, size_dist=kssdgpu.SIZE_LOGNORMAL,
+                        len_median=4e6, len_sigma=0.37, len_min=1e6, len_max=12e6, sub_lo=0.001, sub_hi=0.2,
+                        seed=seed, sample_seed=seed + 1, ref_sample_seed=seed, ref_samples=nr, cov_lo=5, cov_hi=50,
+                        err_lo=0.001, err_hi=0.01, threads=os.cpu_count() or 8)
+    idx = kssdgpu.Index.from_sketch(ref)
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.current_stream()
+    dk = torch.from_numpy(qry.keys.view(np.int64)).to(dev)
+    do = torch.from_numpy(qry.offs.view(np.int64)).to(dev)
+    cells = nq * nr
+    outs = [torch.zeros(cells, dtype=torch.int64, device=dev) for _ in range(4)]
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    flags = kssdgpu.UNIQUE
+
+    def timed(fn, steps, warm):
+        for _ in range(warm):
+            fn()
+        torch.cuda.synchronize()
+        tot = 0.0
+        for _ in range(steps):
+            flush.fill_(1)
+            s = torch.cuda.Event(enable_timing=True)
+            e = torch.cuda.Event(enable_timing=True)
+            s.record(stream)
+            fn()
+            e.record(stream)
+            e.synchronize()
+            tot += s.elapsed_time(e)
+        idx.sync(stream)
+        return tot / steps
+
+    ms_b = timed(lambda: idx.count_block_dev(dk, do, nq, *outs, flags=flags, stream=stream), args.steps,
+                 args.warmup)
+    sums = [int(o.sum().item()) for o in outs]
+    ms_p = timed(lambda: idx.count_plain_dev(dk, do, qry.offs, *outs, flags=flags, stream=stream), 1, 1)
+    assert [int(o.sum().item()) for o in outs] == sums
+    qkeys = int(qry.offs[-1])
+    # the reference's counting function (with unique contexts) on a sample of read sets
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    rec, _ = idx.export()
+    sample = list(range(0, nq, max(1, nq // 8)))[:8]
+    skeys = np.concatenate([qry.keys[int(qry.offs[q]):int(qry.offs[q + 1])] for q in sample])
+    soffs = np.concatenate([[0], np.cumsum([int(qry.offs[q + 1] - qry.offs[q]) for q in sample])]).astype(np.uint64)
+    t0 = time.perf_counter()
+    want = oracle.count_block(rec, nr, skeys, soffs, unique=True, threads=os.cpu_count() or 1,
+                              ref=oracle.ref_available())
+    cpu_s = time.perf_counter() - t0
+    rows = torch.tensor(sample, device=dev)
+    same = all(bool(np.array_equal(w[:, :, 0].astype(np.int64) | (w[:, :, 1].astype(np.int64) << 32),
+                                   o.view(nq, nr)[rows].cpu().numpy())) for w, o in zip(want, outs))
+    line = {"metric": "ANI genome-pairs/s", "workload": f"reads-{nq}x{nr}-unique-ctx", "unit": "genome-pairs/s",
+            "value": cells / (ms_b / 1e3), "ms_per_step": ms_b, "steps": args.steps, "data": "synthetic",
+            "contexts_probed_per_s": qkeys / (ms_b / 1e3),
+            "config": {"read_sets": nq, "refs": nr, "query_keys": qkeys, "ref_entries": int(ref.offs[-1]),
+                       "mean_keys_per_read_set": qkeys / nq, "flags": "unique contexts, conflicts kept"},
+            "plain_per_query": {"ms": ms_p, "value": cells / (ms_p / 1e3), "launches": nq},
+            "batched_vs_plain": ms_p / ms_b,
+            "cpu_baseline": {"value": len(sample) * nr / cpu_s, "unit": "genome-pairs/s",
+                             "cores": os.cpu_count(), "kind": "reference" if oracle.ref_available() else "port",
+                             "sample": f"{len(sample)} read sets", "counts_match_gpu": same}}
     print(json.dumps(line), flush=True)
     idx.close()
     return 0
@@ -626,9 +710,11 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline sample budget")
     ap.add_argument("--cpu-step-seconds", type=float, default=8.0, help="reference arm: seconds per step")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", choices=["self", "serve", "rect"], default="self",
+    ap.add_argument("--workload", choices=["self", "serve", "rect", "reads"], default="self",
                     help="self: the headline self matrix (default); serve: Poisson arrivals against a resident "
-                         "index (p50/p99); rect: uneven queries against a larger index, one batched launch")
+                         "index (p50/p99); rect: uneven queries against a larger index, one batched launch; "
+                         "reads: read sets with unique-context counting against the larger index")
+    ap.add_argument("--reads-samples", type=int, default=40)
     ap.add_argument("--serve-refs", type=int, default=50000, help="serve: resident index size (genomes)")
     ap.add_argument("--serve-rates", default="100,300,1000,3000,5000,10000,20000", help="serve: arrival rates (req/s)")
     ap.add_argument("--serve-seconds", type=float, default=3.0, help="serve: arrival window per rate")
@@ -646,6 +732,8 @@ def main():
         return run_serve(args, rank)
     if args.workload == "rect":
         return run_rect(args, rank)
+    if args.workload == "reads":
+        return run_reads(args, rank)
     if world > 1:
         import datetime
         import torch

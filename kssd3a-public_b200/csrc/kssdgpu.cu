@@ -244,6 +244,8 @@ struct CountParams {
     const int *order;              // query processing order (largest first), may be null
     const WorkItem *items;         // global-row mode: key-range chunks of queries, may be null
     int nitems;
+    const uint32_t *chunk_prefix;  // global-row mode without items: query q owns the kChunkKeys-entry
+                                   // chunks [prefix[q], prefix[q+1]) (nq + 1 words), may be null
     int *err;
 };
 
@@ -453,9 +455,26 @@ __global__ void __launch_bounds__(512) k_count_batched(CountParams P)
             s_item = (int)atomicAdd(P.work, 1u);
         __syncthreads();
         const int it = s_item;
-        if (it >= (!SMEM && P.items ? P.nitems : P.nq))
+        const bool vchunks = !SMEM && !P.items && P.chunk_prefix;
+        if (it >= (!SMEM && P.items ? P.nitems : vchunks ? (int)P.chunk_prefix[P.nq] : P.nq))
             break;
-        const int q = (!SMEM && P.items) ? (int)P.items[it].q : P.order ? P.order[it] : it;
+        int q;
+        if (!SMEM && P.items) {
+            q = (int)P.items[it].q;
+        } else if (vchunks) {
+            // the last query whose first chunk is <= it (queries without keys own no chunk)
+            int lo = 0, hi = P.nq - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (P.chunk_prefix[mid] <= (uint32_t)it)
+                    lo = mid;
+                else
+                    hi = mid - 1;
+            }
+            q = lo;
+        } else {
+            q = P.order ? P.order[it] : it;
+        }
         const int qgid = P.qgid_offset + q;
         const size_t row = (size_t)q * nref;
         // rows: [nc | m2 | dobj | sect] x nref, then the unique-context row
@@ -473,7 +492,14 @@ __global__ void __launch_bounds__(512) k_count_batched(CountParams P)
         } else {
             const GlobalAcc acc{P.out_ctx + row, P.out_obj + row};
             const GlobalAcc uacc{UNIQUE ? P.out_uctx + row : nullptr, UNIQUE ? P.out_uobj + row : nullptr};
-            const uint64_t cb = P.items ? P.items[it].b : b, ce = P.items ? P.items[it].e : e;
+            uint64_t cb = b, ce = e;
+            if (P.items) {
+                cb = P.items[it].b;
+                ce = P.items[it].e;
+            } else if (vchunks) {
+                cb = b + (uint64_t)(it - (int)P.chunk_prefix[q]) * kChunkKeys;
+                ce = min(e, cb + kChunkKeys);
+            }
             process_query<LOWER, UNIQUE>(P, b, e, cb, ce, qgid, objmask, acc, uacc);
         }
         __syncthreads();
@@ -489,6 +515,18 @@ __global__ void __launch_bounds__(512) k_count_batched(CountParams P)
             }
         }
         __syncthreads();
+    }
+}
+
+// counts[q] = kChunkKeys-entry chunks of query q; prefix[0] = 0 (a scan of counts fills
+// prefix[1..nq])
+__global__ void k_chunk_counts(const uint64_t *__restrict__ qoffs, int nq, uint32_t *__restrict__ counts,
+                               uint32_t *__restrict__ prefix)
+{
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += gridDim.x * blockDim.x) {
+        if (q == 0)
+            prefix[0] = 0;
+        counts[q] = (uint32_t)((qoffs[q + 1] - qoffs[q] + kChunkKeys - 1) / kChunkKeys);
     }
 }
 
@@ -723,16 +761,27 @@ __global__ void k_set_permute(const uint32_t *__restrict__ order, uint32_t nchun
     }
 }
 
-// items[item_off[c] + p] = c | i << 32 | j << 40 for the chunk's pairs (i < j)
+// Self-contained join items: offset of the chunk's first group in the compact
+// postings (34 bits) | m << 34 (8) | k << 42 (6) | i << 48 (5) | j << 53 (5).
+__host__ __device__ __forceinline__ unsigned long long set_item(uint64_t off, uint32_t m, uint32_t k, uint32_t i,
+                                                                uint32_t j)
+{
+    return off | ((unsigned long long)m << 34) | ((unsigned long long)k << 42) | ((unsigned long long)i << 48) |
+           ((unsigned long long)j << 53);
+}
+constexpr uint64_t kSetItemMaxOffset = 1ull << 34;
+
+// items[item_off[c] + p] for the chunk's pairs (i < j)
 __global__ void k_set_items(const ulonglong2 *__restrict__ chunks, const uint32_t *__restrict__ item_off, uint32_t nchunks,
                             unsigned long long *__restrict__ items)
 {
     for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < nchunks; c += gridDim.x * blockDim.x) {
-        const uint32_t k = (uint32_t)(chunks[c].y >> 32);
+        const ulonglong2 ch = chunks[c];
+        const uint32_t m = (uint32_t)ch.y, k = (uint32_t)(ch.y >> 32);
         uint32_t o = item_off[c];
         for (uint32_t j = 1; j < k; ++j)
             for (uint32_t i = 0; i < j; ++i)
-                items[o++] = (unsigned long long)c | ((unsigned long long)i << 32) | ((unsigned long long)j << 40);
+                items[o++] = set_item(ch.x, m, k, i, j);
     }
 }
 
@@ -741,8 +790,14 @@ __global__ void k_set_items(const ulonglong2 *__restrict__ chunks, const uint32_
 // sum num_ctx (= m), mut2, diff_obj and section over the groups, then one atomic
 // per counter word.  The chunk's postings (m x k, contiguous) are read by all its
 // items, from L1.
-__global__ void __launch_bounds__(256) k_self_sets(const unsigned long long *__restrict__ items, uint32_t nitems,
-                                                   const ulonglong2 *__restrict__ chunks,
+#ifndef KSSD_SET_UNROLL
+#define KSSD_SET_UNROLL 4
+#endif
+#ifndef KSSD_SET_MINB
+#define KSSD_SET_MINB 1
+#endif
+constexpr int kSetUnroll = KSSD_SET_UNROLL;
+__global__ void __launch_bounds__(256, KSSD_SET_MINB) k_self_sets(const unsigned long long *__restrict__ items, uint32_t nitems,
                                                    const uint64_t *__restrict__ jp, unsigned long long *__restrict__ oc,
                                                    unsigned long long *__restrict__ oo)
 {
@@ -750,18 +805,21 @@ __global__ void __launch_bounds__(256) k_self_sets(const unsigned long long *__r
     if (t >= nitems)
         return;
     const unsigned long long it = __ldg(items + t);
-    const ulonglong2 ch = __ldg(chunks + (uint32_t)it);
-    const uint32_t i = (uint32_t)(it >> 32) & 0xFFu, j = (uint32_t)(it >> 40) & 0xFFu;
-    const uint32_t m = (uint32_t)ch.y, k = (uint32_t)(ch.y >> 32);
-    const uint64_t *g = jp + ch.x;
-    const uint32_t gi = (uint32_t)(__ldg(g + i) >> 32), gj = (uint32_t)(__ldg(g + j) >> 32);
-    // low (object) words of the postings
+    const uint64_t off = it & (kSetItemMaxOffset - 1);
+    const uint32_t m = (uint32_t)(it >> 34) & 0xFFu, k = (uint32_t)(it >> 42) & 0x3Fu;
+    const uint32_t i = (uint32_t)(it >> 48) & 0x1Fu, j = (uint32_t)(it >> 53) & 0x1Fu;
+    const uint64_t *g = jp + off;
+    // the first group's postings give the gids (high words) and its objects
+    const uint64_t pi0 = __ldg(g + i), pj0 = __ldg(g + j);
+    const uint32_t gi = (uint32_t)(pi0 >> 32), gj = (uint32_t)(pj0 >> 32);
+    uint32_t d = (uint32_t)min(kMinInit, dna_pop((uint32_t)pi0 ^ (uint32_t)pj0));
+    uint32_t mut2 = d > 1, dobj = d > 0, sect = d;
+    // low (object) words of the other groups' postings
     const uint32_t *w = reinterpret_cast<const uint32_t *>(g);
-    uint32_t mut2 = 0, dobj = 0, sect = 0;
-#pragma unroll 4
-    for (uint32_t x = 0; x < m; ++x) {
+#pragma unroll kSetUnroll
+    for (uint32_t x = 1; x < m; ++x) {
         const uint32_t oi = __ldg(w + 2 * (x * k + i)), oj = __ldg(w + 2 * (x * k + j));
-        const uint32_t d = (uint32_t)min(kMinInit, dna_pop(oi ^ oj));
+        d = (uint32_t)min(kMinInit, dna_pop(oi ^ oj));
         mut2 += d > 1;
         dobj += d > 0;
         sect += d;
@@ -888,6 +946,8 @@ struct kssdgpu_index {
     DevBuf<unsigned long long> s_out;
     DevBuf<int> s_order;
     DevBuf<WorkItem> s_items;
+    DevBuf<uint32_t> s_prefix, s_counts;    // device-built chunk prefix of a query block
+    DevBuf<unsigned char> s_cubtmp;
     // self-join plan: compact small groups (descriptor offset | k << 32 into j_post),
     // big and conflict groups (begin | k << 32 into post)
     DevBuf<unsigned long long> j_small, j_big, j_conf;
@@ -1008,7 +1068,8 @@ int launch_batched(kssdgpu_index *ix, const CountParams &P, size_t smem, cudaStr
     if (per_sm < 1)
         return fail(KSSDGPU_ERR_CAPACITY, "shared-memory row does not fit one CTA");
     int grid = ix->sms * per_sm;
-    const int units = (!SMEM && P.items) ? P.nitems : P.nq;
+    // with device-built chunks the count of work units stays on the device
+    const int units = (!SMEM && P.items) ? P.nitems : (!SMEM && P.chunk_prefix) ? grid : P.nq;
     if (grid > units)
         grid = std::max(units, 1);
     CUDA_TRY(cudaMemsetAsync(P.work, 0, sizeof(unsigned int), st));
@@ -1091,6 +1152,19 @@ int count_dev_impl(kssdgpu_index *ix, const uint64_t *d_keys, const uint64_t *d_
     if (!use_smem && d_items) {
         P.items = d_items;
         P.nitems = nitems;
+    } else if (!use_smem && !plain && nq > 0) {
+        // device offsets only: chunk counts and their prefix on the device, so that a
+        // large query (a read set) spreads over many SMs
+        CUDA_TRY(ix->s_prefix.ensure((size_t)nq + 1));
+        CUDA_TRY(ix->s_counts.ensure((size_t)nq));
+        size_t tb = 0;
+        CUDA_TRY(cub::DeviceScan::InclusiveSum(nullptr, tb, ix->s_counts.p, ix->s_prefix.p + 1, nq, st));
+        CUDA_TRY(ix->s_cubtmp.ensure(tb));
+        k_chunk_counts<<<std::min((nq + 255) / 256, ix->sms * 8), 256, 0, st>>>(d_offs, nq, ix->s_counts.p,
+                                                                                ix->s_prefix.p);
+        CUDA_TRY(cub::DeviceScan::InclusiveSum(ix->s_cubtmp.p, tb, ix->s_counts.p, ix->s_prefix.p + 1, nq, st));
+        count_launch(3);
+        P.chunk_prefix = ix->s_prefix.p;
     }
     if (!use_smem && !(flags & KSSDGPU_NO_ZERO)) {
         CUDA_TRY(cudaMemsetAsync(oc, 0, cells * 8, st));
@@ -1326,8 +1400,8 @@ cudaError_t tune_join(kssdgpu_index *ix, uint32_t n, cudaStream_t st)
         for (int r = 0; r < 4 && e == cudaSuccess; ++r) {
             e = cudaEventRecord(ev0, st);
             if (e == cudaSuccess && ix->j_nitems) {
-                k_self_sets<<<(ix->j_nitems + 255) / 256, 256, 0, st>>>(ix->j_items.p, ix->j_nitems, ix->j_chunks.p,
-                                                                        ix->j_post.p, oc, oo);
+                k_self_sets<<<(ix->j_nitems + 255) / 256, 256, 0, st>>>(ix->j_items.p, ix->j_nitems, ix->j_post.p,
+                                                                        oc, oo);
                 count_launch();
                 e = cudaGetLastError();
             }
@@ -1463,8 +1537,8 @@ int self_lower_dev_impl(kssdgpu_index *ix, unsigned flags, unsigned long long *o
         }
     }
     if (ix->j_nitems) {
-        k_self_sets<<<(ix->j_nitems + 255) / 256, 256, 0, st>>>(ix->j_items.p, ix->j_nitems, ix->j_chunks.p,
-                                                                ix->j_post.p, oc, oo);
+        k_self_sets<<<(ix->j_nitems + 255) / 256, 256, 0, st>>>(ix->j_items.p, ix->j_nitems, ix->j_post.p, oc,
+                                                                oo);
         count_launch();
     }
     if (ix->j_n[1]) {
@@ -1707,6 +1781,9 @@ void kssdgpu_index_free(kssdgpu_index_t *ix)
     ix->s_out.release();
     ix->s_order.release();
     ix->s_items.release();
+    ix->s_prefix.release();
+    ix->s_counts.release();
+    ix->s_cubtmp.release();
     ix->j_small.release();
     ix->j_post.release();
     ix->j_chunks.release();

@@ -221,3 +221,19 @@ def test_chunked_global_rows_with_runs_across_chunks():
             for g, w in zip(got, want):
                 np.testing.assert_array_equal(g, w)
         assert want[0][0, :, 0].sum() > 0
+        # device-pointer form: the chunk table is built on the device from the offsets
+        import torch
+        dev = torch.device("cuda", 0)
+        d_keys = torch.from_numpy(qk.view(np.int64)).to(dev)
+        # absolute offsets that do not start at 0, an empty query in the middle
+        qo2 = np.array([5, 5 + len(keys), 5 + len(keys), 5 + len(qk)], dtype=np.uint64)
+        d_keys2 = torch.cat([torch.zeros(5, dtype=torch.int64, device=dev), d_keys])
+        d_offs = torch.from_numpy(qo2.view(np.int64)).to(dev)
+        outs = [torch.full((3 * ref.n,), -1, dtype=torch.int64, device=dev) for _ in range(4)]
+        idx.count_block_dev(d_keys2[5:], d_offs, 3, *outs, flags=flags | kssdgpu.GLOBAL_ACC | kssdgpu.UNIQUE)
+        idx.sync()
+        got = [o.cpu().numpy().view(np.uint32).reshape(3, ref.n, 2) for o in outs]
+        for g, w in zip(got, want):
+            np.testing.assert_array_equal(g[0], w[0])
+            np.testing.assert_array_equal(g[2], w[1])
+            assert not g[1].any()
