@@ -295,6 +295,7 @@ def run_ours(args, rank, world, local_rank):
             traffic = None
 
     # ---- plain one-query-per-launch and batched probe kernels (same counters)
+    probe_tuning = idx.count_tune(d_keys, d_offs, n, d_c, d_o, lower=True)  # accumulator mode / chunk size
     ms_probe = timed(probe_step, max(3, args.steps // 2), 2)
     ms_plain = timed(plain_step, 3, 1)
     # per-query probe model bytes: 8|q| + 12 * postings walked + 16 per output cell
@@ -382,7 +383,8 @@ def run_ours(args, rank, world, local_rank):
                               "what": "zero fill of the dense lower triangle + self join"},
             "kernels": {
                 "batched_probe": {"ms": ms_probe, "value": world * n * n / (ms_probe / 1e3),
-                                  "contexts_probed_per_s": world * int(sk.offs[-1]) / (ms_probe / 1e3)},
+                                  "contexts_probed_per_s": world * int(sk.offs[-1]) / (ms_probe / 1e3),
+                                  "tuning": probe_tuning},
                 "plain_per_query": {"ms": ms_plain, "value": world * n * n / (ms_plain / 1e3), "launches": n},
                 "self_join_vs_plain": ms_plain / ms_step, "batched_probe_vs_plain": ms_plain / ms_probe,
             },
@@ -564,6 +566,7 @@ def run_rect(args, rank):
         idx.sync(stream)
         return tot / steps
 
+    tuning = idx.count_tune(dk, do, nq, dc, dob)
     ms_b = timed(batched, args.steps, args.warmup)
     checksum = int(dc.sum().item())
     shared = int((dc & 0xFFFFFFFF).sum().item())  # = postings walked (conflict-free references)
@@ -603,7 +606,7 @@ def run_rect(args, rank):
             "config": {"queries": nq, "refs": nr, "query_keys": qkeys, "ref_entries": int(ref.offs[-1]),
                        "accumulators": "global (reference row exceeds shared memory)" if nr * 16 > 112 * 1024
                        else "shared"},
-            "graph_replay_ms": graph_ms, "contexts_probed_per_s": qkeys / (ms_b / 1e3),
+            "graph_replay_ms": graph_ms, "contexts_probed_per_s": qkeys / (ms_b / 1e3), "tuning": tuning,
             "plain_per_query": {"ms": ms_p, "value": cells / (ms_p / 1e3), "launches": nq},
             "batched_vs_plain": ms_p / ms_b,
             "roofline_probe_model": {"bound": "hbm", "bytes": probe_bytes,
@@ -665,6 +668,7 @@ def run_reads(args, rank):
         idx.sync(stream)
         return tot / steps
 
+    tuning = idx.count_tune(dk, do, nq, *outs, flags=flags)
     ms_b = timed(lambda: idx.count_block_dev(dk, do, nq, *outs, flags=flags, stream=stream), args.steps,
                  args.warmup)
     sums = [int(o.sum().item()) for o in outs]
@@ -687,7 +691,7 @@ def run_reads(args, rank):
                                    o.view(nq, nr)[rows].cpu().numpy())) for w, o in zip(want, outs))
     line = {"metric": "ANI genome-pairs/s", "workload": f"reads-{nq}x{nr}-unique-ctx", "unit": "genome-pairs/s",
             "value": cells / (ms_b / 1e3), "ms_per_step": ms_b, "steps": args.steps, "data": "synthetic",
-            "contexts_probed_per_s": qkeys / (ms_b / 1e3),
+            "contexts_probed_per_s": qkeys / (ms_b / 1e3), "tuning": tuning,
             "config": {"read_sets": nq, "refs": nr, "query_keys": qkeys, "ref_entries": int(ref.offs[-1]),
                        "mean_keys_per_read_set": qkeys / nq, "flags": "unique contexts, conflicts kept"},
             "plain_per_query": {"ms": ms_p, "value": cells / (ms_p / 1e3), "launches": nq},

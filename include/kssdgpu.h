@@ -45,6 +45,8 @@ extern "C" {
 #define KSSDGPU_PLAIN 0x4u          /* use the plain one-query-per-launch kernel (baseline) */
 #define KSSDGPU_GLOBAL_ACC 0x8u     /* force global-memory accumulators (no shared-memory rows) */
 #define KSSDGPU_NO_ZERO 0x10u       /* device calls: outputs were zeroed by the caller (skip memset) */
+#define KSSDGPU_SMEM_ACC 0x20u      /* force shared-memory accumulator rows (KSSDGPU_ERR_CAPACITY when a
+                                       row of the index's references does not fit) */
 
 /* Counter cells, identical in layout to the reference's ctx_mut2_t / obj_section_t. */
 typedef struct kssdgpu_ctx_mut2 {
@@ -145,6 +147,28 @@ int kssdgpu_count_block_dev(kssdgpu_index_t *idx, const uint64_t *d_qry_keys,
                             unsigned flags, kssdgpu_ctx_mut2_t *d_ctx, kssdgpu_obj_section_t *d_obj,
                             kssdgpu_ctx_mut2_t *d_uctx, kssdgpu_obj_section_t *d_uobj, void *stream);
 int kssdgpu_sync(kssdgpu_index_t *idx, void *stream);
+
+/*
+ * Autotune the batched count of this index on a representative block (arguments as
+ * kssdgpu_count_block_dev; flags select unique/ignoreconflict, lower selects the
+ * triangle form): shared-memory accumulator rows (where a row fits) and global rows
+ * in key-range chunks of 1,024 / 4,096 / 16,384 entries are each timed with CUDA
+ * events (best of three after a warm-up) on the legacy stream, and the fastest
+ * becomes the index's setting for later batched counts without KSSDGPU_SMEM_ACC /
+ * KSSDGPU_GLOBAL_ACC.  Synchronizes the device; the outputs hold the block's counters
+ * afterwards.  Without a call: global rows in 4,096-entry chunks.  No reference
+ * counterpart (the CPU path has no tunables).
+ */
+typedef struct kssdgpu_count_tuning {
+    int smem_rows;        /* 1: shared-memory accumulator rows; 0: global rows in chunks */
+    uint32_t chunk_keys;  /* entries per key-range chunk of the global-row mode */
+    int candidates;       /* settings timed */
+    float ms;             /* the chosen setting's time on the block */
+} kssdgpu_count_tuning_t;
+int kssdgpu_count_tune(kssdgpu_index_t *idx, const uint64_t *d_qry_keys, const uint64_t *d_qry_offs, int nq,
+                       int qry_gid_offset, int lower, unsigned flags, kssdgpu_ctx_mut2_t *d_ctx,
+                       kssdgpu_obj_section_t *d_obj, kssdgpu_ctx_mut2_t *d_uctx, kssdgpu_obj_section_t *d_uobj,
+                       kssdgpu_count_tuning_t *out);
 
 /*
  * Whole self lower triangle in one pass (the counting behind

@@ -216,6 +216,7 @@ int server_launch(kssdgpu_server *s, ServerSlot &sl)
     P.out_uobj = sl.d_uro;
     P.work = sl.d_work;
     P.order = nullptr;
+    P.chunk_keys = (uint32_t)kChunkKeys;
     P.items = sl.d_items;
     P.nitems = (int)nitems;
     P.err = s->ix->err;

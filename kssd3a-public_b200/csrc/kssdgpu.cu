@@ -244,8 +244,9 @@ struct CountParams {
     const int *order;              // query processing order (largest first), may be null
     const WorkItem *items;         // global-row mode: key-range chunks of queries, may be null
     int nitems;
-    const uint32_t *chunk_prefix;  // global-row mode without items: query q owns the kChunkKeys-entry
+    const uint32_t *chunk_prefix;  // global-row mode without items: query q owns the chunk_keys-entry
                                    // chunks [prefix[q], prefix[q+1]) (nq + 1 words), may be null
+    uint32_t chunk_keys;           // entries per chunk in that mode
     int *err;
 };
 
@@ -497,8 +498,8 @@ __global__ void __launch_bounds__(512) k_count_batched(CountParams P)
                 cb = P.items[it].b;
                 ce = P.items[it].e;
             } else if (vchunks) {
-                cb = b + (uint64_t)(it - (int)P.chunk_prefix[q]) * kChunkKeys;
-                ce = min(e, cb + kChunkKeys);
+                cb = b + (uint64_t)(it - (int)P.chunk_prefix[q]) * P.chunk_keys;
+                ce = min(e, cb + (uint64_t)P.chunk_keys);
             }
             process_query<LOWER, UNIQUE>(P, b, e, cb, ce, qgid, objmask, acc, uacc);
         }
@@ -518,15 +519,15 @@ __global__ void __launch_bounds__(512) k_count_batched(CountParams P)
     }
 }
 
-// counts[q] = kChunkKeys-entry chunks of query q; prefix[0] = 0 (a scan of counts fills
+// counts[q] = chunk-entry chunks of query q; prefix[0] = 0 (a scan of counts fills
 // prefix[1..nq])
-__global__ void k_chunk_counts(const uint64_t *__restrict__ qoffs, int nq, uint32_t *__restrict__ counts,
-                               uint32_t *__restrict__ prefix)
+__global__ void k_chunk_counts(const uint64_t *__restrict__ qoffs, int nq, uint32_t chunk,
+                               uint32_t *__restrict__ counts, uint32_t *__restrict__ prefix)
 {
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += gridDim.x * blockDim.x) {
         if (q == 0)
             prefix[0] = 0;
-        counts[q] = (uint32_t)((qoffs[q + 1] - qoffs[q] + kChunkKeys - 1) / kChunkKeys);
+        counts[q] = (uint32_t)((qoffs[q + 1] - qoffs[q] + chunk - 1) / chunk);
     }
 }
 
@@ -947,6 +948,12 @@ struct kssdgpu_index {
     DevBuf<int> s_order;
     DevBuf<WorkItem> s_items;
     DevBuf<uint32_t> s_prefix, s_counts;    // device-built chunk prefix of a query block
+    // batched-count setting (kssdgpu_count_tune): shared-memory rows where they fit, or
+    // global rows in key-range chunks of count_chunk_keys entries
+    bool count_smem = false;
+    uint32_t count_chunk_keys = 4096;
+    int count_tune_tried = 0;
+    float count_tune_ms = 0;
     DevBuf<unsigned char> s_cubtmp;
     // self-join plan: compact small groups (descriptor offset | k << 32 into j_post),
     // big and conflict groups (begin | k << 32 into post)
@@ -1096,22 +1103,31 @@ int launch_plain(kssdgpu_index *ix, const CountParams &P, const std::vector<uint
 // shared-memory row budget: four 32-bit counters per reference (eight with unique)
 constexpr size_t kSmemRowLimit = 112 * 1024;
 
-bool uses_smem_row(const kssdgpu_index *ix, unsigned flags)
+bool smem_row_fits(const kssdgpu_index *ix, unsigned flags)
 {
-    const size_t smem = (size_t)ix->nref * sizeof(unsigned long long) * ((flags & KSSDGPU_UNIQUE) ? 4 : 2);
-    return !(flags & (KSSDGPU_PLAIN | KSSDGPU_GLOBAL_ACC)) && smem <= kSmemRowLimit;
+    return (size_t)ix->nref * sizeof(unsigned long long) * ((flags & KSSDGPU_UNIQUE) ? 4 : 2) <= kSmemRowLimit;
 }
 
-// Key-range chunks of at most kChunkKeys entries for the global-row kernel, the
-// queries taken in the given order (offsets relative or absolute).
-void build_chunks(const uint64_t *offs, int nq, const int *order, std::vector<WorkItem> &items)
+// Accumulator mode of a batched count: global rows in key-range chunks unless the
+// caller forces shared-memory rows (KSSDGPU_SMEM_ACC) or the count autotuner chose
+// them for this index; shared rows only where a row fits.
+bool uses_smem_row(const kssdgpu_index *ix, unsigned flags)
+{
+    if (flags & (KSSDGPU_PLAIN | KSSDGPU_GLOBAL_ACC))
+        return false;
+    return smem_row_fits(ix, flags) && ((flags & KSSDGPU_SMEM_ACC) || ix->count_smem);
+}
+
+// Key-range chunks of at most `chunk` entries for the global-row kernel, the queries
+// taken in the given order (offsets relative or absolute).
+void build_chunks(const uint64_t *offs, int nq, const int *order, uint64_t chunk, std::vector<WorkItem> &items)
 {
     items.clear();
     for (int k = 0; k < nq; ++k) {
         const int q = order ? order[k] : k;
         const uint64_t b = offs[q] - offs[0], e = offs[q + 1] - offs[0];
-        for (uint64_t c = b; c < e; c += kChunkKeys)
-            items.push_back(WorkItem{(uint32_t)q, 0u, c, std::min(e, c + kChunkKeys)});
+        for (uint64_t c = b; c < e; c += chunk)
+            items.push_back(WorkItem{(uint32_t)q, 0u, c, std::min(e, c + chunk)});
     }
 }
 
@@ -1148,7 +1164,11 @@ int count_dev_impl(kssdgpu_index *ix, const uint64_t *d_keys, const uint64_t *d_
         return KSSDGPU_OK;
     const size_t smem = (size_t)ix->nref * sizeof(unsigned long long) * (unique ? 4 : 2);
     const bool plain = (flags & KSSDGPU_PLAIN) != 0;
+    if ((flags & KSSDGPU_SMEM_ACC) && !plain && !(flags & KSSDGPU_GLOBAL_ACC) && !smem_row_fits(ix, flags))
+        return fail(KSSDGPU_ERR_CAPACITY, "shared-memory accumulator rows requested, but a row of " +
+                                              std::to_string(ix->nref) + " references does not fit");
     const bool use_smem = uses_smem_row(ix, flags);
+    P.chunk_keys = ix->count_chunk_keys;
     if (!use_smem && d_items) {
         P.items = d_items;
         P.nitems = nitems;
@@ -1160,8 +1180,8 @@ int count_dev_impl(kssdgpu_index *ix, const uint64_t *d_keys, const uint64_t *d_
         size_t tb = 0;
         CUDA_TRY(cub::DeviceScan::InclusiveSum(nullptr, tb, ix->s_counts.p, ix->s_prefix.p + 1, nq, st));
         CUDA_TRY(ix->s_cubtmp.ensure(tb));
-        k_chunk_counts<<<std::min((nq + 255) / 256, ix->sms * 8), 256, 0, st>>>(d_offs, nq, ix->s_counts.p,
-                                                                                ix->s_prefix.p);
+        k_chunk_counts<<<std::min((nq + 255) / 256, ix->sms * 8), 256, 0, st>>>(d_offs, nq, ix->count_chunk_keys,
+                                                                                ix->s_counts.p, ix->s_prefix.p);
         CUDA_TRY(cub::DeviceScan::InclusiveSum(ix->s_cubtmp.p, tb, ix->s_counts.p, ix->s_prefix.p + 1, nq, st));
         count_launch(3);
         P.chunk_prefix = ix->s_prefix.p;
@@ -1219,7 +1239,7 @@ int count_host_impl(kssdgpu_index *ix, const uint64_t *qkeys, const uint64_t *qo
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return sizes[a] > sizes[b]; });
     std::vector<WorkItem> items;
     if (!uses_smem_row(ix, flags) && !(flags & KSSDGPU_PLAIN))
-        build_chunks(qoffs, nq, order.data(), items);
+        build_chunks(qoffs, nq, order.data(), ix->count_chunk_keys, items);
     const size_t cells = (size_t)nq * ix->nref;
     const int nout = unique ? 4 : 2;
     CUDA_TRY(ix->s_keys.ensure(nkeys));
@@ -1888,6 +1908,88 @@ int kssdgpu_count_block_dev(kssdgpu_index_t *ix, const uint64_t *d_qry_keys, con
                           reinterpret_cast<unsigned long long *>(d_ctx), reinterpret_cast<unsigned long long *>(d_obj),
                           reinterpret_cast<unsigned long long *>(d_uctx), reinterpret_cast<unsigned long long *>(d_uobj),
                           nullptr, nullptr, (cudaStream_t)stream);
+}
+
+int kssdgpu_count_tune(kssdgpu_index_t *ix, const uint64_t *d_qry_keys, const uint64_t *d_qry_offs, int nq,
+                       int qry_gid_offset, int lower, unsigned flags, kssdgpu_ctx_mut2_t *d_ctx,
+                       kssdgpu_obj_section_t *d_obj, kssdgpu_ctx_mut2_t *d_uctx, kssdgpu_obj_section_t *d_uobj,
+                       kssdgpu_count_tuning_t *out)
+{
+    if (!ix || nq < 1 || !d_qry_offs || !d_ctx || !d_obj)
+        return fail(KSSDGPU_ERR_ARG, "invalid count-tuning arguments");
+    CUDA_TRY(cudaSetDevice(ix->device));
+    const unsigned base = flags & (KSSDGPU_UNIQUE | KSSDGPU_IGNORECONFLICT);
+    struct Cand {
+        bool smem;
+        uint32_t chunk;
+    };
+    std::vector<Cand> cands = {{false, 1024}, {false, 4096}, {false, 16384}};
+    if (smem_row_fits(ix, base))
+        cands.push_back({true, 4096});
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    CUDA_TRY(cudaEventCreate(&ev0));
+    cudaError_t ce = cudaEventCreate(&ev1);
+    if (ce != cudaSuccess) {
+        cudaEventDestroy(ev0);
+        return fail(KSSDGPU_ERR_CUDA, cudaGetErrorString(ce));
+    }
+    const bool keep_smem = ix->count_smem;
+    const uint32_t keep_chunk = ix->count_chunk_keys;
+    float best = 1e30f;
+    Cand pick = {keep_smem, keep_chunk};
+    int rc = KSSDGPU_OK, tried = 0;
+    for (const Cand &c : cands) {
+        ix->count_chunk_keys = c.chunk;
+        const unsigned f = base | (c.smem ? KSSDGPU_SMEM_ACC : KSSDGPU_GLOBAL_ACC);
+        float t_min = 1e30f;
+        for (int r = 0; r < 4 && rc == KSSDGPU_OK; ++r) {
+            ce = cudaEventRecord(ev0, 0);
+            if (ce == cudaSuccess) {
+                rc = count_dev_impl(ix, d_qry_keys, d_qry_offs, nq, qry_gid_offset, lower != 0, f,
+                                    reinterpret_cast<unsigned long long *>(d_ctx),
+                                    reinterpret_cast<unsigned long long *>(d_obj),
+                                    reinterpret_cast<unsigned long long *>(d_uctx),
+                                    reinterpret_cast<unsigned long long *>(d_uobj), nullptr, nullptr, 0);
+                if (rc)
+                    break;
+            }
+            if (ce == cudaSuccess) ce = cudaEventRecord(ev1, 0);
+            if (ce == cudaSuccess) ce = cudaEventSynchronize(ev1);
+            float ms = 0;
+            if (ce == cudaSuccess) ce = cudaEventElapsedTime(&ms, ev0, ev1);
+            if (ce != cudaSuccess) {
+                rc = fail(KSSDGPU_ERR_CUDA, cudaGetErrorString(ce));
+                break;
+            }
+            if (r > 0)
+                t_min = std::min(t_min, ms);
+        }
+        if (rc)
+            break;
+        ++tried;
+        if (t_min < best) {
+            best = t_min;
+            pick = c;
+        }
+    }
+    cudaEventDestroy(ev0);
+    cudaEventDestroy(ev1);
+    if (rc) {
+        ix->count_smem = keep_smem;
+        ix->count_chunk_keys = keep_chunk;
+        return rc;
+    }
+    ix->count_smem = pick.smem;
+    ix->count_chunk_keys = pick.chunk;
+    ix->count_tune_tried = tried;
+    ix->count_tune_ms = best;
+    if (out) {
+        out->smem_rows = pick.smem ? 1 : 0;
+        out->chunk_keys = pick.chunk;
+        out->candidates = tried;
+        out->ms = best;
+    }
+    return check_dev_err(ix, 0);
 }
 
 int kssdgpu_count_plain_dev(kssdgpu_index_t *ix, const uint64_t *d_qry_keys, const uint64_t *d_qry_offs,

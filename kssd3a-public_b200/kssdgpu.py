@@ -23,6 +23,7 @@ UNIQUE = 0x2
 PLAIN = 0x4
 GLOBAL_ACC = 0x8
 NO_ZERO = 0x10
+SMEM_ACC = 0x20
 
 _u64p = np.ctypeslib.ndpointer(dtype=np.uint64, flags="C_CONTIGUOUS")
 _u32p = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
@@ -66,6 +67,8 @@ def gpu_lib() -> C.CDLL:
         lib.kssdgpu_count_block_dev.argtypes = [vp, vp, vp, C.c_int, C.c_int, C.c_int, C.c_uint,
                                                 vp, vp, vp, vp, vp]
         lib.kssdgpu_sync.argtypes = [vp, vp]
+        lib.kssdgpu_count_tune.argtypes = [vp, vp, vp, C.c_int, C.c_int, C.c_int, C.c_uint, vp, vp, vp, vp,
+                                           C.POINTER(_CountTuning)]
         lib.kssdgpu_self_lower.argtypes = [vp, C.c_uint, vp, vp]
         lib.kssdgpu_self_lower_dev.argtypes = [vp, C.c_uint, vp, vp, vp]
         lib.kssdgpu_self_plan_tune.argtypes = [vp, C.POINTER(C.c_uint32), C.POINTER(C.c_int),
@@ -90,6 +93,10 @@ def gpu_lib() -> C.CDLL:
 class _ServerConfig(C.Structure):
     _fields_ = [("max_batch_queries", C.c_int), ("max_batch_keys", C.c_uint64), ("max_hits", C.c_uint64),
                 ("flags", C.c_uint)]
+
+
+class _CountTuning(C.Structure):
+    _fields_ = [("smem_rows", C.c_int), ("chunk_keys", C.c_uint32), ("candidates", C.c_int), ("ms", C.c_float)]
 
 
 class _ServerStats(C.Structure):
@@ -361,6 +368,15 @@ class Index:
         _check(gpu_lib().kssdgpu_count_block_dev(self._h, _ptr(d_keys), _ptr(d_offs), nq, qry_gid_offset,
                                                  int(lower), flags, _ptr(d_ctx), _ptr(d_obj), _ptr(d_uctx),
                                                  _ptr(d_uobj), _ptr(stream)))
+
+    def count_tune(self, d_keys, d_offs, nq, d_ctx, d_obj, d_uctx=None, d_uobj=None, flags=0, lower=False,
+                   qry_gid_offset=0):
+        """Autotune this index's batched count on a block; returns the chosen setting."""
+        t = _CountTuning()
+        _check(gpu_lib().kssdgpu_count_tune(self._h, _ptr(d_keys), _ptr(d_offs), nq, qry_gid_offset, int(lower),
+                                            flags, _ptr(d_ctx), _ptr(d_obj), _ptr(d_uctx), _ptr(d_uobj),
+                                            C.byref(t)))
+        return {f: getattr(t, f) for f, _ in t._fields_}
 
     def count_plain_dev(self, d_keys, d_offs, h_offs, d_ctx, d_obj, d_uctx=None, d_uobj=None, flags=0,
                         lower=False, qry_gid_offset=0, stream=None):

@@ -32,7 +32,8 @@ CASES = [(s, 4, 2, 35, 256, True) for s in range(10)] + \
 
 @pytest.mark.parametrize("case", CASES)
 @pytest.mark.parametrize("flags", [0, kssdgpu.IGNORECONFLICT, kssdgpu.PLAIN, kssdgpu.GLOBAL_ACC,
-                                   kssdgpu.PLAIN | kssdgpu.IGNORECONFLICT])
+                                   kssdgpu.PLAIN | kssdgpu.IGNORECONFLICT, kssdgpu.SMEM_ACC,
+                                   kssdgpu.SMEM_ACC | kssdgpu.IGNORECONFLICT])
 def test_count_block_unique(case, flags):
     rk, ro, qk, qo = _fixture(*case)
     nref = len(ro) - 1
@@ -49,7 +50,7 @@ def test_count_block_unique(case, flags):
 
 
 @pytest.mark.parametrize("case", CASES[::2])
-@pytest.mark.parametrize("flags", [0, kssdgpu.IGNORECONFLICT, kssdgpu.PLAIN, kssdgpu.GLOBAL_ACC])
+@pytest.mark.parametrize("flags", [0, kssdgpu.IGNORECONFLICT, kssdgpu.PLAIN, kssdgpu.GLOBAL_ACC, kssdgpu.SMEM_ACC])
 def test_count_lower_blocks(case, flags):
     rk, ro, _, _ = _fixture(*case)
     nref = len(ro) - 1
@@ -237,3 +238,41 @@ def test_chunked_global_rows_with_runs_across_chunks():
             np.testing.assert_array_equal(g[0], w[0])
             np.testing.assert_array_equal(g[2], w[1])
             assert not g[1].any()
+
+
+def test_count_autotuner_keeps_counts():
+    """kssdgpu_count_tune times the accumulator settings on a block; its outputs and
+    every later count (under the chosen setting) equal the oracle's counters."""
+    import torch
+    ref = kssdgpu.synth(n_samples=64, n_clusters=8, len_median=3e5, len_min=1e5, len_max=1e6,
+                        size_dist=kssdgpu.SIZE_LOGNORMAL, sub_lo=0.001, sub_hi=0.1, seed=5, sample_seed=5)
+    qry = kssdgpu.synth(n_samples=24, n_clusters=8, role=kssdgpu.ROLE_OWNLEN, len_median=3e5, len_min=1e5,
+                        len_max=1e6, size_dist=kssdgpu.SIZE_LOGNORMAL, own_len_min=5e4, own_len_max=2e6,
+                        seed=5, sample_seed=6)
+    rec = oracle.build_index(ref.keys, ref.offs)
+    idx = kssdgpu.Index.from_records(rec, ref.n)
+    want = oracle.count_block(rec, ref.n, qry.keys, qry.offs, unique=True)
+    dev = torch.device("cuda", 0)
+    dk = torch.from_numpy(qry.keys.view(np.int64)).to(dev)
+    do = torch.from_numpy(qry.offs.view(np.int64)).to(dev)
+    outs = [torch.zeros(qry.n * ref.n, dtype=torch.int64, device=dev) for _ in range(4)]
+    t = idx.count_tune(dk, do, qry.n, *outs, flags=kssdgpu.UNIQUE)
+    assert t["candidates"] == 4 and t["chunk_keys"] in (1024, 4096, 16384) and t["ms"] > 0
+    for _ in range(2):
+        got = [o.cpu().numpy().view(np.uint32).reshape(qry.n, ref.n, 2) for o in outs]
+        for g, w in zip(got, want):
+            np.testing.assert_array_equal(g, w)
+        for o in outs:
+            o.fill_(-1)
+        idx.count_block_dev(dk, do, qry.n, *outs, flags=kssdgpu.UNIQUE)
+        idx.sync()
+    host = idx.count_block(qry.keys, qry.offs, kssdgpu.UNIQUE)
+    for g, w in zip(host, want):
+        np.testing.assert_array_equal(g, w)
+    # shared rows cannot be forced where a row does not fit
+    big = np.zeros(2, dtype=kssdgpu.REC_DTYPE)
+    big["ctxgid"] = [(1 << 20) | 0, (2 << 20) | 20000]
+    bidx = kssdgpu.Index.from_records(big, 20001)
+    with pytest.raises(kssdgpu.KssdGpuError) as e:
+        bidx.count_block(qry.keys[:10], np.array([0, 10], dtype=np.uint64), kssdgpu.SMEM_ACC)
+    assert e.value.code == 7
