@@ -181,6 +181,20 @@ int kssdgpu_count_tune(kssdgpu_index_t *idx, const uint64_t *d_qry_keys, const u
  */
 int kssdgpu_self_lower(kssdgpu_index_t *idx, unsigned flags, kssdgpu_ctx_mut2_t *ctx_lower,
                        kssdgpu_obj_section_t *obj_lower);
+/*
+ * Candidate votes of the indexed sparse scan behind `kssd3a matrix --format
+ * edges|clusters|dedup-plan` on one sketch (pairwise_indexed_self_scan,
+ * src/pairwise_graph.c:1148-1316; nomination at :1195-1246): for every sample q of the
+ * sketch (keys/offs: comblco keys and absolute comblco.index offsets, nref samples),
+ * the keys at positions 0, step, 2*step, ... that the index holds, in context groups of
+ * at most max_ctx_freq postings (0: any), vote once for every reference gid r < q of
+ * the group.  Outputs over the packed lower triangle (cell (q, r) at q*(q-1)/2 + r):
+ * votes, and first = the lowest sampled position index (position / step) that voted
+ * (UINT32_MAX without a vote) -- the scan's order of touching r within row q.
+ * Host buffers; synchronous.
+ */
+int kssdgpu_self_votes(kssdgpu_index_t *idx, const uint64_t *keys, const uint64_t *offs, uint32_t max_ctx_freq,
+                       uint32_t sample_step, uint32_t *votes, uint32_t *first);
 /* Device form of kssdgpu_self_lower (outputs in HBM, stream-ordered). */
 int kssdgpu_self_lower_dev(kssdgpu_index_t *idx, unsigned flags, kssdgpu_ctx_mut2_t *d_ctx_lower,
                            kssdgpu_obj_section_t *d_obj_lower, void *stream);

@@ -888,6 +888,61 @@ __global__ void k_self_conflict_groups(const unsigned long long *__restrict__ li
     }
 }
 
+// ------------------------------------------------------------------ sparse-scan candidate votes
+
+// Candidate nomination of the indexed sparse scan (src/pairwise_graph.c:1195-1246):
+// sample q's keys at positions 0, step, 2*step, ... (qi = position / step) that are
+// found in the index, in context groups of at most max_freq postings (0: any), vote
+// once for every posting's gid r < q: votes[(q, r)] += 1 and first[(q, r)] =
+// min(qi), the order in which the scan first touches r.  One thread per sketch key;
+// the key's sample comes from a binary search of the offsets.
+__global__ void __launch_bounds__(256) k_self_votes(const Slot *__restrict__ table, uint32_t mask,
+                                                    const uint64_t *__restrict__ post,
+                                                    const uint64_t *__restrict__ keys,
+                                                    const uint64_t *__restrict__ offs, int n, uint64_t nkeys,
+                                                    int obj_bits, uint32_t max_freq, uint32_t step,
+                                                    uint32_t *__restrict__ votes, uint32_t *__restrict__ first)
+{
+    const uint64_t base = offs[0];
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nkeys;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        // the sample holding absolute key base + i: the last q with offs[q] <= base + i
+        int lo = 0, hi = n - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (__ldg(offs + mid) <= base + i)
+                lo = mid;
+            else
+                hi = mid - 1;
+        }
+        const int q = lo;
+        const uint64_t pos = base + i - __ldg(offs + q);
+        if (q == 0 || pos % step)
+            continue;
+        const uint32_t qi = (uint32_t)(pos / step);
+        const unsigned long long ctx = __ldg(keys + i) >> obj_bits;
+        unsigned long long payload;
+        bool single;
+        if (!table_lookup(table, mask, ctx, payload, single))
+            continue;
+        uint32_t pb = 0, pc = 1;
+        if (!single) {
+            pb = (uint32_t)payload;
+            pc = (uint32_t)(payload >> 32);
+        }
+        if (max_freq && pc > max_freq)
+            continue;
+        for (uint32_t k = 0; k < pc; ++k) {
+            const uint32_t gid = single ? (uint32_t)(payload >> 32) : (uint32_t)(__ldg(post + pb + k) >> 32);
+            if ((int)gid >= q)
+                break;
+            const size_t cell = (size_t)q * (q - 1) / 2 + gid;
+            atomicAdd(votes + cell, 1u);
+            atomicMin(first + cell, qi);
+        }
+    }
+}
+
 // ------------------------------------------------------------------ helpers
 
 template <class T>
@@ -2141,6 +2196,49 @@ int kssdgpu_self_lower(kssdgpu_index_t *ix, unsigned flags, kssdgpu_ctx_mut2_t *
         CUDA_TRY(cudaMemcpyAsync(ctx_lower, ix->s_out.p, cells * 8, cudaMemcpyDeviceToHost, st));
         CUDA_TRY(cudaMemcpyAsync(obj_lower, ix->s_out.p + cells, cells * 8, cudaMemcpyDeviceToHost, st));
     }
+    return check_dev_err(ix, st);
+}
+
+int kssdgpu_self_votes(kssdgpu_index_t *ix, const uint64_t *keys, const uint64_t *offs, uint32_t max_ctx_freq,
+                       uint32_t sample_step, uint32_t *votes, uint32_t *first)
+{
+    if (!ix || !offs || !votes || !first || sample_step == 0)
+        return fail(KSSDGPU_ERR_ARG, "invalid vote arguments");
+    CUDA_TRY(cudaSetDevice(ix->device));
+    const int n = ix->nref;
+    const size_t cells = (size_t)n * (n > 0 ? n - 1 : 0) / 2;
+    if (!cells)
+        return KSSDGPU_OK;
+    const uint64_t nkeys = offs[n] - offs[0];
+    if (nkeys && !keys)
+        return fail(KSSDGPU_ERR_ARG, "null keys");
+    for (int i = 0; i < n; ++i)
+        if (offs[i + 1] < offs[i])
+            return fail(KSSDGPU_ERR_ARG, "sample offsets are not monotone");
+    cudaStream_t st = 0;
+    CUDA_TRY(ix->s_keys.ensure(nkeys));
+    CUDA_TRY(ix->s_offs.ensure((size_t)n + 1));
+    uint32_t *d = nullptr;
+    cudaError_t e = cudaMalloc(&d, cells * 8);
+    if (e != cudaSuccess)
+        return fail(KSSDGPU_ERR_NOMEM, std::string("vote counters: ") + cudaGetErrorString(e));
+    if (nkeys)
+        e = cudaMemcpyAsync(ix->s_keys.p, keys, nkeys * 8, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(ix->s_offs.p, offs, ((size_t)n + 1) * 8, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d, 0, cells * 4, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d + cells, 0xFF, cells * 4, st);
+    if (e == cudaSuccess && nkeys) {
+        k_self_votes<<<grid_for(nkeys), 256, 0, st>>>(ix->table, ix->mask, ix->post, ix->s_keys.p, ix->s_offs.p, n,
+                                                      nkeys, ix->obj_bits, max_ctx_freq, sample_step, d, d + cells);
+        count_launch();
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(votes, d, cells * 4, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(first, d + cells, cells * 4, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFree(d);
+    if (e != cudaSuccess)
+        return fail(KSSDGPU_ERR_CUDA, cudaGetErrorString(e));
     return check_dev_err(ix, st);
 }
 

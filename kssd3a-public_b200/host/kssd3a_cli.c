@@ -21,6 +21,7 @@
 #include <err.h>
 #include <errno.h>
 #include <fcntl.h>
+#include <inttypes.h>
 #include <limits.h>
 #include <math.h>
 #include <omp.h>
@@ -1562,10 +1563,16 @@ static int cmd_ani(int argc, char **argv)
 enum { MF_AUTO = 0, MF_FULL, MF_TRIANGLE, MF_EDGES, MF_CLUSTERS, MF_DEDUP };
 enum { MM_MOE = 0, MM_NAIVE, MM_PDIST, MM_MASH, MM_AAF };
 
+enum { MOP_SINGLE = 0, MOP_AND, MOP_OR };
+
 typedef struct matrix_cli {
     int metric, metric_count, format, phylip, d, threads;
-    double e, diag;
-    bool cut_set, ani;
+    int metrics[5], metric_op;   /* pairwise_metric_expr_t: up to 5 metrics joined by & or | */
+    char metric_label[128];
+    double e, diag, cut, max_afcut;
+    bool cut_set, ani, max_afcut_set;
+    uint32_t ctxcut, max_ctx_freq, min_votes, sample_step;
+    int dedup_strategy;          /* 0 greedy, 1 full-linkage */
     char refdir[PATHLEN], qrydir[PATHLEN], qrylist[PATHLEN], outf[PATHLEN], gl[PATHLEN], idmap[PATHLEN];
     char edge_out[PATHLEN], keep_out[PATHLEN], remove_out[PATHLEN], keep_matrix_out[PATHLEN], keep_idmap[PATHLEN];
     int keep_matrix_fmt, dedup_seen, nrem;
@@ -1663,8 +1670,11 @@ static error_t parse_matrix(int key, char *arg, struct argp_state *st)
                 int mm;
                 if (count >= 5 || !matrix_metric_from(tok, &mm))
                     ok = false;
-                else if (count++ == 0)
-                    m = mm;
+                else {
+                    if (count == 0)
+                        m = mm;
+                    gm.metrics[count++] = mm;
+                }
             }
         }
         if (!ok || count == 0)
@@ -1672,6 +1682,15 @@ static error_t parse_matrix(int key, char *arg, struct argp_state *st)
                            "like 'ctx-naive&aaf' or 'ctx-moe|mash'");
         gm.metric = m;
         gm.metric_count = count;
+        gm.metric_op = count == 1 ? MOP_SINGLE : (has_and ? MOP_AND : MOP_OR);
+        /* pairwise_expr_append_label, src/pairwise_graph.c:154-170 */
+        static const char *const names[] = {"ctx-moe", "ctx-naive", "p_dist", "mash", "aaf"};
+        gm.metric_label[0] = '\0';
+        for (int i = 0; i < count; ++i) {
+            const size_t used = strlen(gm.metric_label);
+            snprintf(gm.metric_label + used, sizeof gm.metric_label - used, "%s%s",
+                     i == 0 ? "" : (gm.metric_op == MOP_AND ? "&" : "|"), names[gm.metrics[i]]);
+        }
         break;
     }
     case MK_FORMAT:
@@ -1684,17 +1703,38 @@ static error_t parse_matrix(int key, char *arg, struct argp_state *st)
         break;
     case MK_SPARSE: gm.format = MF_EDGES; break;
     case 'c':
-    case MK_CUT: parse_nonneg(st, "--cut", arg); gm.cut_set = true; break;
-    case MK_MAX_AFCUT: parse_double_range(st, "--max-afcut", arg, 0.0, 1.0); break;
-    case MK_CTXCUT: parse_int_range(st, "--ctxcut", arg, 0, INT32_MAX); break;
-    case MK_MAX_CTX_FREQ: parse_int_range(st, "--index-max-ctx-freq", arg, 0, INT32_MAX); break;
-    case MK_MIN_VOTES: parse_int_range(st, "--index-min-votes", arg, 1, INT32_MAX); break;
-    case MK_SAMPLE_STEP: parse_int_range(st, "--index-sample-step", arg, 1, INT32_MAX); break;
-    case MK_PROGRESS:
-        if (strcmp(arg, "auto") && strcmp(arg, "on") && strcmp(arg, "off"))
-            argp_error(st, "--progress must be auto, on, or off");
+    case MK_CUT: gm.cut = parse_nonneg(st, "--cut", arg); gm.cut_set = true; break;
+    case MK_MAX_AFCUT:
+        gm.max_afcut = parse_double_range(st, "--max-afcut", arg, 0.0, 1.0);
+        gm.max_afcut_set = true;
         break;
-    case MK_DEDUP: gm.dedup_seen = 1; break;
+    case MK_CTXCUT: gm.ctxcut = (uint32_t)parse_int_range(st, "--ctxcut", arg, 0, INT32_MAX); break;
+    case MK_MAX_CTX_FREQ:
+        gm.max_ctx_freq = (uint32_t)parse_int_range(st, "--index-max-ctx-freq", arg, 0, INT32_MAX);
+        break;
+    case MK_MIN_VOTES: gm.min_votes = (uint32_t)parse_int_range(st, "--index-min-votes", arg, 1, INT32_MAX); break;
+    case MK_SAMPLE_STEP:
+        gm.sample_step = (uint32_t)parse_int_range(st, "--index-sample-step", arg, 1, INT32_MAX);
+        break;
+    case MK_PROGRESS:
+        /* parse_matrix_progress, src/command_matrix_wrapper.c:216-228; progress itself is not printed */
+        if (strcmp(arg, "auto") && strcmp(arg, "on") && strcmp(arg, "1") && strcmp(arg, "yes") && strcmp(arg, "off") &&
+            strcmp(arg, "0") && strcmp(arg, "no"))
+            argp_error(st, "--progress must be one of auto, on, or off");
+        break;
+    case MK_DEDUP:
+        /* pairwise_dedup_strategy_from_string, src/pairwise_graph.c:118-140 */
+        gm.dedup_seen = 1;
+        if (!strcmp(arg, "greedy") || !strcmp(arg, "rep") || !strcmp(arg, "representative") ||
+            !strcmp(arg, "rep-centric") || !strcmp(arg, "representative-centric"))
+            gm.dedup_strategy = 0;
+        else if (!strcmp(arg, "full") || !strcmp(arg, "full-linkage") || !strcmp(arg, "full_linkage") ||
+                 !strcmp(arg, "complete") || !strcmp(arg, "complete-linkage") || !strcmp(arg, "complete_linkage") ||
+                 !strcmp(arg, "clique"))
+            gm.dedup_strategy = 1;
+        else
+            argp_error(st, "--dedup-strategy must be one of greedy, full-linkage, complete-linkage, or clique");
+        break;
     case 'e': gm.e = parse_nonneg(st, "-e/--exception", arg); break;
     case 'p': gm.threads = parse_int_range(st, "-p/--threads", arg, 1, 65536); break;
     case 'q': copy_path(st, "-q/--query", gm.qrydir, arg); break;
@@ -1707,10 +1747,11 @@ static error_t parse_matrix(int key, char *arg, struct argp_state *st)
     case MK_REMOVE_OUT: copy_path(st, "--remove-out", gm.remove_out, arg); break;
     case MK_MATRIX_FORMAT:
     case MK_KEEP_MATRIX_FORMAT: {
+        /* parse_keep_matrix_format, src/command_matrix_wrapper.c:202-213 (both options) */
         int ph;
         if (!strcmp(arg, "tsv") || !strcmp(arg, "table")) ph = 0;
-        else if (!strcmp(arg, "phylip") || !strcmp(arg, "phy")) ph = 1;
-        else { argp_error(st, "matrix format must be tsv or phylip"); ph = 0; }
+        else if (!strcmp(arg, "phylip") || !strcmp(arg, "phy") || !strcmp(arg, "fillip")) ph = 1;
+        else { argp_error(st, "--keep-matrix-format must be one of tsv or phylip"); ph = 0; }
         if (key == MK_MATRIX_FORMAT) gm.phylip = ph; else gm.keep_matrix_fmt = ph;
         break;
     }
@@ -1760,8 +1801,41 @@ static error_t parse_matrix(int key, char *arg, struct argp_state *st)
             argp_error(st, "--query-sketch-list currently supports rectangular --format full without --ani");
         if (gm.idmap[0] && !gm.phylip)
             argp_error(st, "--matrix-idmap requires --matrix-format phylip");
-        if (gm.idmap[0] && gm.outf[0] && !strcmp(gm.idmap, gm.outf))
-            argp_error(st, "--matrix-idmap must differ from --outfile");
+        if (gm.keep_matrix_fmt && !gm.keep_matrix_out[0])
+            argp_error(st, "--keep-matrix-format requires --keep-matrix-out");
+        if (gm.keep_idmap[0] && !gm.keep_matrix_out[0])
+            argp_error(st, "--keep-matrix-idmap requires --keep-matrix-out");
+        if (gm.keep_idmap[0] && !gm.keep_matrix_fmt)
+            argp_error(st, "--keep-matrix-idmap requires --keep-matrix-format phylip");
+        /* output files must all differ, in the reference's order of checks */
+        static const struct { int a, b; const char *msg; } diff[] = {
+            {3, 4, "--keep-out and --remove-out must be different files"},
+            {3, 0, "--keep-out must differ from --outfile"},
+            {4, 0, "--remove-out must differ from --outfile"},
+            {5, 0, "--keep-matrix-out must differ from --outfile"},
+            {1, 0, "--matrix-idmap must differ from --outfile"},
+            {2, 0, "--edge-out must differ from --outfile"},
+            {3, 2, "--keep-out must differ from --edge-out"},
+            {4, 2, "--remove-out must differ from --edge-out"},
+            {5, 2, "--keep-matrix-out must differ from --edge-out"},
+            {5, 3, "--keep-matrix-out must differ from --keep-out"},
+            {5, 4, "--keep-matrix-out must differ from --remove-out"},
+            {6, 0, "--keep-matrix-idmap must differ from --outfile"},
+            {6, 2, "--keep-matrix-idmap must differ from --edge-out"},
+            {6, 3, "--keep-matrix-idmap must differ from --keep-out"},
+            {6, 4, "--keep-matrix-idmap must differ from --remove-out"},
+            {6, 5, "--keep-matrix-idmap must differ from --keep-matrix-out"},
+            {1, 2, "--matrix-idmap must differ from --edge-out"},
+            {1, 3, "--matrix-idmap must differ from --keep-out"},
+            {1, 4, "--matrix-idmap must differ from --remove-out"},
+            {1, 5, "--matrix-idmap must differ from --keep-matrix-out"},
+            {1, 6, "--matrix-idmap must differ from --keep-matrix-idmap"},
+        };
+        const char *files[7] = {gm.outf, gm.idmap, gm.edge_out, gm.keep_out, gm.remove_out, gm.keep_matrix_out,
+                                gm.keep_idmap};
+        for (size_t i = 0; i < sizeof diff / sizeof diff[0]; ++i)
+            if (files[diff[i].a][0] && files[diff[i].b][0] && !strcmp(files[diff[i].a], files[diff[i].b]))
+                argp_error(st, "%s", diff[i].msg);
         break;
     }
     default:
@@ -1821,38 +1895,50 @@ static void put_u6(kssd_buf_t *b, uint32_t scaled)
     kssd_buf_printf(b, "%u.%s", scaled / 1000000U, f6);
 }
 
-/* matrix_context_feature_value with one metric, src/command_matrix.c:400-424,621-661 */
+/* matrix_context_metric_distance, src/command_matrix.c:400-424 */
+static double matrix_metric_distance(int metric, const kssd_features_t *f, uint32_t qc, uint32_t rc,
+                                     const kssd_ani_opt_t *o)
+{
+    kssd_features_t t = *f;
+    switch (metric) {
+    case MM_NAIVE: return kssd_naive_dist(&t);
+    case MM_MOE: return kssd_lm3ways_dist(&t, o->drfold);
+    case MM_PDIST: return kssd_p_dist(&t, o->obj_bits);
+    case MM_MASH: return kssd_mashD((uint32_t)(o->ctx_bits / 2), rc, qc, f->XnY_ctx);
+    default: return kssd_aafD((uint32_t)(o->ctx_bits / 2), rc, qc, f->XnY_ctx);
+    }
+}
+
+/* matrix_context_feature_value, src/command_matrix.c:621-661: the metric expression
+ * over clamped distances (& keeps the largest, | the smallest) */
 static double matrix_context_value(const kssd_features_t *f, uint32_t qc, uint32_t rc, const kssd_ani_opt_t *o)
 {
     if (f->XnY_ctx == 0 || qc == 0 || rc == 0)
         return gm.e;
-    kssd_features_t t = *f;
-    double d;
-    switch (gm.metric) {
-    case MM_NAIVE: d = kssd_naive_dist(&t); break;
-    case MM_MOE: d = kssd_lm3ways_dist(&t, o->drfold); break;
-    case MM_PDIST: d = kssd_p_dist(&t, o->obj_bits); break;
-    case MM_MASH: d = kssd_mashD((uint32_t)(o->ctx_bits / 2), rc, qc, f->XnY_ctx); break;
-    default: d = kssd_aafD((uint32_t)(o->ctx_bits / 2), rc, qc, f->XnY_ctx); break;
+    double selected = 0.0;
+    for (int i = 0; i < gm.metric_count; ++i) {
+        double d = matrix_metric_distance(gm.metrics[i], f, qc, rc, o);
+        if (!isfinite(d))
+            return gm.e;
+        if (d < 0.0) d = 0.0;
+        if (d > 1.0) d = 1.0;
+        if (i == 0)
+            selected = d;
+        else if (gm.metric_op == MOP_AND ? d > selected : d < selected)
+            selected = d;
     }
-    if (!isfinite(d))
-        return gm.e;
-    if (d < 0.0) d = 0.0;
-    if (d > 1.0) d = 1.0;
-    return d;
+    return selected;
 }
 
 /* pairwise_eval_arrays distances, src/pairwise_graph.c:13-49,301-360 */
 static double clean_dist(double d) { return !isfinite(d) ? 1.0 : (d < 0.0 ? 0.0 : d); }
 
-static double matrix_pair_value(const kssd_features_t *f, uint32_t qc, uint32_t rc, size_t qlen, size_t rlen,
-                                const kssd_ani_opt_t *o)
+static double pair_metric_distance(int metric, const kssd_features_t *f, uint32_t qc, uint32_t rc,
+                                   const kssd_ani_opt_t *o)
 {
-    if (qlen == 0 || rlen == 0 || f->XnY_ctx == 0)
-        return gm.e;
     kssd_features_t t = *f;
     const int k = o->ctx_bits > 0 ? o->ctx_bits / 2 : 32;
-    switch (gm.metric) {
+    switch (metric) {
     case MM_MASH: {
         const double denom = (double)qc + (double)rc - (double)f->XnY_ctx;
         if (denom <= 0.0) return 1.0;
@@ -1871,6 +1957,50 @@ static double matrix_pair_value(const kssd_features_t *f, uint32_t qc, uint32_t 
     case MM_PDIST: return clean_dist(kssd_p_dist(&t, o->obj_bits));
     default: return clean_dist(kssd_lm3ways_dist(&t, o->drfold));
     }
+}
+
+/* pairwise_eval_t (src/pairwise_graph.h) of one (query, reference) pair */
+typedef struct pair_eval {
+    double distance, similarity, af_qry, af_ref, max_af;
+    uint32_t xny, n_diff_obj, n_diff_obj_section, n_mut2_ctx;
+    bool valid;
+} pair_eval_t;
+
+/* pairwise_eval_arrays + pairwise_eval_expr_merge (src/pairwise_graph.c:301-360,417-446):
+ * the features are the pair's shared-context counters; the metric expression keeps the
+ * largest (&) or smallest (|) distance, the first of equals. */
+static pair_eval_t pair_eval(const kssd_features_t *f, uint32_t qc, uint32_t rc, size_t qlen, size_t rlen,
+                             const kssd_ani_opt_t *o)
+{
+    pair_eval_t e = {.distance = 1.0};
+    if (qlen == 0 || rlen == 0)
+        return e;
+    e.xny = f->XnY_ctx;
+    e.n_diff_obj = f->N_diff_obj;
+    e.n_diff_obj_section = f->N_diff_obj_section;
+    e.n_mut2_ctx = f->N_mut2_ctx;
+    e.af_qry = qc > 0 ? (double)f->XnY_ctx / (double)qc : 0.0;
+    e.af_ref = rc > 0 ? (double)f->XnY_ctx / (double)rc : 0.0;
+    e.max_af = e.af_qry > e.af_ref ? e.af_qry : e.af_ref;
+    if (f->XnY_ctx == 0)
+        return e;
+    double sel = 1.0;
+    for (int i = 0; i < gm.metric_count; ++i) {
+        const double d = pair_metric_distance(gm.metrics[i], f, qc, rc, o);
+        if (i == 0 || (gm.metric_op == MOP_AND ? d > sel : d < sel))
+            sel = d;
+    }
+    e.distance = sel;
+    e.similarity = 1.0 - sel;
+    e.valid = true;
+    return e;
+}
+
+static double matrix_pair_value(const kssd_features_t *f, uint32_t qc, uint32_t rc, size_t qlen, size_t rlen,
+                                const kssd_ani_opt_t *o)
+{
+    const pair_eval_t e = pair_eval(f, qc, rc, qlen, rlen, o);
+    return e.valid ? e.distance : gm.e;
 }
 
 static void matrix_glist(const kssd_sketch_t *s)
@@ -1915,7 +2045,9 @@ static int matrix_self(int fmt)
     if (fmt == MF_FULL) {
         if (gm.phylip) {
             if (gm.idmap[0]) {
+                /* matrix_write_full_matrix_idmap, src/command_matrix.c:365-379 */
                 FILE *im = open_out(gm.idmap);
+                fputs("id\tsample\n", im);
                 for (int i = 0; i < n; ++i)
                     fprintf(im, "S%09d\t%s\n", i + 1, s->names[i]);
                 if (im != stdout)
@@ -2042,6 +2174,756 @@ static int matrix_rect(void)
     return 0;
 }
 
+/* ------------------------------------------------------------------ sparse reports
+ *
+ * `kssd3a matrix --format edges|clusters|dedup-plan` (src/command_matrix.c:660-1300,
+ * src/pairwise_graph.c:518-1316).  Every pair's features come from the GPU self join
+ * (one sketch) or block counts (-r/-q); with an index file and a conflict-free sketch
+ * the reference nominates candidate pairs by context votes (GPU: kssdgpu_self_votes) and
+ * reports edges row by row in the order its scan touches them; the union-find
+ * components, greedy and full-linkage dedup plans and every report are host code.
+ */
+
+typedef struct sp_edge {
+    int a, b;
+} sp_edge_t;
+
+typedef struct sp_edges {
+    sp_edge_t *e;
+    size_t n, cap;
+} sp_edges_t;
+
+static void sp_push(sp_edges_t *l, int a, int b)
+{
+    if (l->n == l->cap) {
+        l->cap = l->cap ? l->cap * 2 : 1024;
+        l->e = realloc(l->e, l->cap * sizeof(sp_edge_t));
+        if (!l->e)
+            err(EXIT_FAILURE, "OOM edge list");
+    }
+    l->e[l->n++] = (sp_edge_t){a, b};
+}
+
+/* matrix_print_edge_header / matrix_print_edge, src/command_matrix.c:87-101 */
+static void print_edge_header(FILE *f)
+{
+    fputs("Qry\tRef\tDistance\tSimilarity\tMetric\tXnY_ctx\tQry_align_fraction\tRef_align_fraction\tmax_AF\t"
+          "N_diff_obj\tN_diff_obj_section\tN_mut2_ctx\n",
+          f);
+}
+
+static void print_edge(FILE *f, const char *q, const char *r, const pair_eval_t *e)
+{
+    fprintf(f, "%s\t%s\t%.12g\t%.12g\t%s\t%u\t%.12g\t%.12g\t%.12g\t%u\t%u\t%u\n", q, r, e->distance, e->similarity,
+            gm.metric_label, e->xny, e->af_qry, e->af_ref, e->max_af, e->n_diff_obj, e->n_diff_obj_section,
+            e->n_mut2_ctx);
+}
+
+/* pairwise_eval_passes_edge and the reject counters around it (src/pairwise_graph.c:
+ * 518-530,1229-1245): 0 = no distance edge, 1 = shared-context reject, 2 = align-fraction
+ * reject, 3 = accepted */
+static int edge_class(const pair_eval_t *e)
+{
+    if (!e->valid || e->distance >= gm.cut)
+        return 0;
+    if (e->xny < gm.ctxcut)
+        return 1;
+    if (e->max_af < gm.max_afcut)
+        return 2;
+    return 3;
+}
+
+/* one sketch: lower-triangle counters, per-sample context counts */
+typedef struct sp_self {
+    const kssd_sketch_t *s;
+    const kssdgpu_ctx_mut2_t *lc;
+    const kssdgpu_obj_section_t *lo;
+    const uint32_t *cnt;
+} sp_self_t;
+
+static size_t sp_len(const kssd_sketch_t *s, int i) { return (size_t)(s->offs[i + 1] - s->offs[i]); }
+
+/* pairwise_eval_expr_samples(metric, sketch, qry, sketch, ref) from the pair's cell */
+static pair_eval_t sp_eval(const sp_self_t *c, int qry, int ref)
+{
+    const int hi = qry > ref ? qry : ref, lo = qry > ref ? ref : qry;
+    const size_t cell = (size_t)hi * (size_t)(hi - 1) / 2 + (size_t)lo;
+    const kssd_features_t f = feat_of(&c->lc[cell], &c->lo[cell]);
+    return pair_eval(&f, c->cnt[qry], c->cnt[ref], sp_len(c->s, qry), sp_len(c->s, ref), &g.o);
+}
+
+/* ---- sample quality (src/pairwise_graph.c:532-603) and representative rules
+ * (src/command_matrix.c:151-246) */
+
+static bool sp_meta_valid(const kssd_sketch_t *s, int i)
+{
+    return s->meta && i >= 0 && i < s->n && s->meta[i].meta_fmt_version == 1 && s->meta[i].total_length_bp > 0;
+}
+
+static double finite_or(double v, double fb) { return isfinite(v) ? v : fb; }
+
+static int positive_lower_u32_cmp(uint32_t a, uint32_t b)
+{
+    if (a == b) return 0;
+    if (a == 0) return -1;
+    if (b == 0) return 1;
+    return a < b ? 1 : -1;
+}
+
+/* > 0: a is the better representative */
+static int sp_quality_cmp(const kssd_sketch_t *s, int a, int b)
+{
+    if (a == b)
+        return 0;
+    const bool ra = sp_meta_valid(s, a), rb = sp_meta_valid(s, b);
+    if (ra != rb)
+        return ra ? 1 : -1;
+    if (ra && rb) {
+        const kssd_infile_meta_t *ma = &s->meta[a], *mb = &s->meta[b];
+        const bool fa = ma->infile_fmt == 1, fb = mb->infile_fmt == 1;
+        if (fa != fb)
+            return fa ? 1 : -1;
+        const double aa = finite_or((double)ma->asm_level, -1.0), ab = finite_or((double)mb->asm_level, -1.0);
+        if (aa != ab)
+            return aa > ab ? 1 : -1;
+        if (ma->total_length_bp != mb->total_length_bp)
+            return ma->total_length_bp > mb->total_length_bp ? 1 : -1;
+        const int rc = positive_lower_u32_cmp(ma->record_count, mb->record_count);
+        if (rc)
+            return rc;
+        if (ma->median_length_bp != mb->median_length_bp)
+            return ma->median_length_bp > mb->median_length_bp ? 1 : -1;
+        const double ca = finite_or((double)ma->length_cv, INFINITY), cb = finite_or((double)mb->length_cv, INFINITY);
+        if (ca != cb)
+            return ca < cb ? 1 : -1;
+    }
+    const size_t ea = sp_len(s, a), eb = sp_len(s, b);
+    if (ea != eb)
+        return ea > eb ? 1 : -1;
+    return a < b ? 1 : -1;
+}
+
+static const kssd_sketch_t *g_sp_sketch;
+static int sp_order_cmp(const void *x, const void *y)
+{
+    return -sp_quality_cmp(g_sp_sketch, *(const int *)x, *(const int *)y);
+}
+
+/* samples best first (the comparison is a total order, so any sort gives the reference's) */
+static int *sp_quality_order(const kssd_sketch_t *s)
+{
+    int *o = malloc((size_t)(s->n ? s->n : 1) * sizeof(int));
+    if (!o)
+        err(EXIT_FAILURE, "OOM quality order");
+    for (int i = 0; i < s->n; ++i)
+        o[i] = i;
+    g_sp_sketch = s;
+    qsort(o, (size_t)s->n, sizeof(int), sp_order_cmp);
+    return o;
+}
+
+static const char *sp_rep_rule(const kssd_sketch_t *s, int sample, int rep)
+{
+    if (sample == rep)
+        return "self";
+    const bool sv = sp_meta_valid(s, sample), rv = sp_meta_valid(s, rep);
+    if (sv != rv)
+        return rv ? "valid_metadata" : "sample_valid_metadata";
+    if (sv && rv) {
+        const kssd_infile_meta_t *sm = &s->meta[sample], *rm = &s->meta[rep];
+        const bool sf = sm->infile_fmt == 1, rf = rm->infile_fmt == 1;
+        if (sf != rf)
+            return rf ? "fasta_input" : "sample_fasta_input";
+        if (sm->asm_level != rm->asm_level)
+            return rm->asm_level > sm->asm_level ? "higher_asm_level" : "sample_higher_asm_level";
+        if (sm->total_length_bp != rm->total_length_bp)
+            return rm->total_length_bp > sm->total_length_bp ? "longer_total_length" : "sample_longer_total_length";
+        if (sm->record_count != rm->record_count) {
+            if (sm->record_count == 0)
+                return "sample_missing_record_count";
+            if (rm->record_count == 0)
+                return "rep_missing_record_count";
+            return rm->record_count < sm->record_count ? "fewer_records" : "sample_fewer_records";
+        }
+        if (sm->median_length_bp != rm->median_length_bp)
+            return rm->median_length_bp > sm->median_length_bp ? "longer_median_length"
+                                                               : "sample_longer_median_length";
+        if (sm->length_cv != rm->length_cv)
+            return rm->length_cv < sm->length_cv ? "lower_length_cv" : "sample_lower_length_cv";
+    }
+    const size_t se = sp_len(s, sample), re = sp_len(s, rep);
+    if (se != re)
+        return re > se ? "larger_sketch_entries" : "sample_larger_sketch_entries";
+    return rep < sample ? "earlier_sample_order" : "sample_earlier_sample_order";
+}
+
+static void sp_print_meta(FILE *f, const kssd_sketch_t *s, int i)
+{
+    if (!sp_meta_valid(s, i)) {
+        fputs("\tNA\tNA\tNA\tNA\tNA\tNA", f);
+        return;
+    }
+    const kssd_infile_meta_t *m = &s->meta[i];
+    fprintf(f, "\t%s\t%.6g\t%" PRIu64 "\t%u\t%u\t%.6g",
+            m->infile_fmt == 1 ? "FASTA" : m->infile_fmt == 2 ? "FASTQ" : "NA", (double)m->asm_level,
+            m->total_length_bp, m->record_count, m->median_length_bp, (double)m->length_cv);
+}
+
+/* ---- components and dedup plans (src/pairwise_graph.c:605-975) */
+
+typedef struct sp_comp {
+    int n;
+    int *parent, *size, *rep;
+    uint8_t *rank;
+    bool *removed;
+} sp_comp_t;
+
+static void sp_comp_init(sp_comp_t *c, int n)
+{
+    c->n = n;
+    c->parent = malloc((size_t)(n ? n : 1) * sizeof(int));
+    c->size = calloc((size_t)(n ? n : 1), sizeof(int));
+    c->rep = malloc((size_t)(n ? n : 1) * sizeof(int));
+    c->rank = calloc((size_t)(n ? n : 1), 1);
+    c->removed = calloc((size_t)(n ? n : 1), sizeof(bool));
+    if (!c->parent || !c->size || !c->rep || !c->rank || !c->removed)
+        err(EXIT_FAILURE, "OOM component bookkeeping");
+    for (int i = 0; i < n; ++i) {
+        c->parent[i] = i;
+        c->rep[i] = -1;
+    }
+}
+
+static void sp_comp_free(sp_comp_t *c)
+{
+    free(c->parent);
+    free(c->size);
+    free(c->rep);
+    free(c->rank);
+    free(c->removed);
+}
+
+static int sp_find(int *parent, int x)
+{
+    while (parent[x] != x) {
+        parent[x] = parent[parent[x]];
+        x = parent[x];
+    }
+    return x;
+}
+
+static void sp_union(sp_comp_t *c, int a, int b)
+{
+    int ra = sp_find(c->parent, a), rb = sp_find(c->parent, b);
+    if (ra == rb)
+        return;
+    if (c->rank[ra] < c->rank[rb])
+        c->parent[ra] = rb;
+    else if (c->rank[ra] > c->rank[rb])
+        c->parent[rb] = ra;
+    else {
+        c->parent[rb] = ra;
+        ++c->rank[ra];
+    }
+}
+
+/* pairwise_component_result_finalize: sizes, best-quality representative per component */
+static void sp_comp_finalize(sp_comp_t *c, const kssd_sketch_t *s)
+{
+    for (int i = 0; i < c->n; ++i) {
+        const int r = sp_find(c->parent, i);
+        c->parent[i] = r;
+        ++c->size[r];
+    }
+    for (int i = 0; i < c->n; ++i) {
+        const int r = c->parent[i];
+        if (c->rep[r] < 0 || sp_quality_cmp(s, i, c->rep[r]) > 0)
+            c->rep[r] = i;
+    }
+    for (int i = 0; i < c->n; ++i)
+        c->removed[i] = i != c->rep[c->parent[i]];
+}
+
+/* pairwise_greedy_dedup_from_edges: best sample first claims all its unclaimed neighbours */
+static void sp_dedup_greedy(sp_comp_t *c, const kssd_sketch_t *s, const sp_edges_t *edges)
+{
+    const int n = c->n;
+    size_t *off = calloc((size_t)n + 1, sizeof(size_t));
+    if (!off)
+        err(EXIT_FAILURE, "OOM dedup graph");
+    for (size_t e = 0; e < edges->n; ++e) {
+        ++off[edges->e[e].a + 1];
+        ++off[edges->e[e].b + 1];
+    }
+    for (int i = 0; i < n; ++i)
+        off[i + 1] += off[i];
+    int *adj = malloc((off[n] ? off[n] : 1) * sizeof(int));
+    size_t *cur = malloc(((size_t)n + 1) * sizeof(size_t));
+    if (!adj || !cur)
+        err(EXIT_FAILURE, "OOM dedup adjacency");
+    memcpy(cur, off, ((size_t)n + 1) * sizeof(size_t));
+    for (size_t e = 0; e < edges->n; ++e) {
+        adj[cur[edges->e[e].a]++] = edges->e[e].b;
+        adj[cur[edges->e[e].b]++] = edges->e[e].a;
+    }
+    int *order = sp_quality_order(s);
+    for (int oi = 0; oi < n; ++oi) {
+        const int rep = order[oi];
+        if (c->removed[rep])
+            continue;
+        c->parent[rep] = rep;
+        c->rep[rep] = rep;
+        c->size[rep] = 1;
+        for (size_t k = off[rep]; k < off[rep + 1]; ++k) {
+            const int x = adj[k];
+            if (x == rep || c->removed[x])
+                continue;
+            c->removed[x] = true;
+            c->parent[x] = rep;
+            c->rep[x] = rep;
+            ++c->size[rep];
+        }
+    }
+    for (int i = 0; i < n; ++i)
+        if (c->rep[i] < 0) {
+            c->rep[i] = i;
+            c->size[i] = 1;
+        }
+    free(order);
+    free(cur);
+    free(adj);
+    free(off);
+}
+
+/* pairwise_complete_linkage_dedup_from_edges: in quality order, a representative takes
+ * every unassigned sample linked to all members taken so far */
+static void sp_dedup_complete(sp_comp_t *c, const kssd_sketch_t *s, const sp_edges_t *edges)
+{
+    const int n = c->n;
+    const size_t words = ((size_t)n * (size_t)n + 63) / 64;
+    uint64_t *bits = calloc(words ? words : 1, sizeof(uint64_t));
+    int *members = malloc((size_t)(n ? n : 1) * sizeof(int));
+    bool *assigned = calloc((size_t)(n ? n : 1), sizeof(bool));
+    if (!bits || !members || !assigned)
+        err(EXIT_FAILURE, "OOM full-linkage dedup");
+    for (size_t e = 0; e < edges->n; ++e) {
+        const size_t a = (size_t)edges->e[e].a, b = (size_t)edges->e[e].b;
+        bits[(a * n + b) >> 6] |= 1ull << ((a * n + b) & 63);
+        bits[(b * n + a) >> 6] |= 1ull << ((b * n + a) & 63);
+    }
+    int *order = sp_quality_order(s);
+    for (int oi = 0; oi < n; ++oi) {
+        const int rep = order[oi];
+        if (assigned[rep])
+            continue;
+        assigned[rep] = true;
+        c->parent[rep] = rep;
+        c->rep[rep] = rep;
+        c->size[rep] = 1;
+        members[0] = rep;
+        int mn = 1;
+        for (int ci = 0; ci < n; ++ci) {
+            const int x = order[ci];
+            if (x == rep || assigned[x])
+                continue;
+            bool all = true;
+            for (int mi = 0; mi < mn && all; ++mi) {
+                const size_t pos = (size_t)x * n + (size_t)members[mi];
+                all = (bits[pos >> 6] >> (pos & 63)) & 1ull;
+            }
+            if (!all)
+                continue;
+            c->removed[x] = true;
+            assigned[x] = true;
+            c->parent[x] = rep;
+            c->rep[x] = rep;
+            ++c->size[rep];
+            members[mn++] = x;
+        }
+    }
+    for (int i = 0; i < n; ++i)
+        if (c->rep[i] < 0) {
+            c->rep[i] = i;
+            c->size[i] = 1;
+        }
+    free(order);
+    free(assigned);
+    free(members);
+    free(bits);
+}
+
+/* ---- reports (src/command_matrix.c:317-380,801-939,1056-1123) */
+
+static FILE *sp_open(const char *path)
+{
+    FILE *f = path[0] ? fopen(path, "w") : stdout;
+    if (!f)
+        err(errno, "matrix_open_output(): %s", path);
+    return f;
+}
+
+static void sp_close(FILE *f)
+{
+    if (f != stdout)
+        fclose(f);
+    else
+        fflush(f);
+}
+
+/* kept representatives' dense matrix from the lower counters (the indexed form,
+ * matrix_write_keep_matrix_indexed) */
+static void sp_keep_matrix(const sp_self_t *c, const sp_comp_t *comp)
+{
+    if (!gm.keep_matrix_out[0])
+        return;
+    const kssd_sketch_t *s = c->s;
+    int *kept = malloc((size_t)(s->n ? s->n : 1) * sizeof(int));
+    if (!kept)
+        err(EXIT_FAILURE, "OOM kept samples");
+    int kn = 0;
+    for (int i = 0; i < s->n; ++i)
+        if (!comp->removed[i])
+            kept[kn++] = i;
+    if (gm.keep_idmap[0]) {
+        FILE *im = sp_open(gm.keep_idmap);
+        fputs("id\tsample\n", im);
+        for (int i = 0; i < kn; ++i)
+            fprintf(im, "S%09d\t%s\n", i + 1, s->names[kept[i]]);
+        sp_close(im);
+    }
+    FILE *f = sp_open(gm.keep_matrix_out);
+    if (gm.keep_matrix_fmt) {
+        fprintf(f, "%d\n", kn);
+    } else {
+        for (int k = 0; k < kn; ++k)
+            fprintf(f, "\t%s", s->names[kept[k]]);
+        fputc('\n', f);
+    }
+    for (int qi = 0; qi < kn; ++qi) {
+        const int q = kept[qi];
+        if (gm.keep_matrix_fmt) {
+            char id[16];
+            snprintf(id, sizeof id, "S%09d", qi + 1);
+            fprintf(f, "%-10s", id);
+        } else {
+            fputs(s->names[q], f);
+        }
+        for (int k = 0; k < kn; ++k) {
+            const int r = kept[k];
+            double v = gm.diag;
+            if (q != r) {
+                const int hi = q > r ? q : r, lo = q > r ? r : q;
+                const size_t cell = (size_t)hi * (size_t)(hi - 1) / 2 + (size_t)lo;
+                const kssd_features_t ft = feat_of(&c->lc[cell], &c->lo[cell]);
+                v = matrix_context_value(&ft, c->cnt[q], c->cnt[r], &g.o);
+            }
+            if (gm.keep_matrix_fmt)
+                fprintf(f, " %.12g", v);
+            else
+                fprintf(f, "\t%lf", v);
+        }
+        fputc('\n', f);
+    }
+    sp_close(f);
+    free(kept);
+}
+
+/* matrix_write_component_report */
+static void sp_component_report(const sp_self_t *c, sp_comp_t *comp, bool dedup)
+{
+    const kssd_sketch_t *s = c->s;
+    const int n = s->n;
+    int *cid = calloc((size_t)(n ? n : 1), sizeof(int));
+    if (!cid)
+        err(EXIT_FAILURE, "OOM cluster ids");
+    int next = 1;
+    for (int i = 0; i < n; ++i) {
+        const int root = sp_find(comp->parent, i);
+        if (!cid[root])
+            cid[root] = next++;
+    }
+    FILE *out = sp_open(gm.outf);
+    FILE *keep = dedup && gm.keep_out[0] ? sp_open(gm.keep_out) : NULL;
+    FILE *rem = dedup && gm.remove_out[0] ? sp_open(gm.remove_out) : NULL;
+    if (dedup)
+        fputs("sample\tcomponent_id\taction\trepresentative\treason\trep_rule\tcomponent_size\tsample_sketch_entries\t"
+              "rep_sketch_entries\tsample_fmt\tsample_asm_level\tsample_total_length_bp\tsample_record_count\t"
+              "sample_median_length_bp\tsample_length_cv\trep_fmt\trep_asm_level\trep_total_length_bp\t"
+              "rep_record_count\trep_median_length_bp\trep_length_cv\n",
+              out);
+    else
+        fputs("sample\tcluster_id\tcomponent_size\trepresentative\n", out);
+    for (int i = 0; i < n; ++i) {
+        const int root = sp_find(comp->parent, i);
+        const int rep = comp->rep[root];
+        if (dedup) {
+            const bool single = comp->size[root] == 1, kept = i == rep;
+            if (kept && keep)
+                fprintf(keep, "%s\n", s->names[i]);
+            if (!kept && rem)
+                fprintf(rem, "%s\n", s->names[i]);
+            fprintf(out, "%s\tcluster_%06d\t%s\t%s\t%s\t%s\t%d\t%" PRIu64 "\t%" PRIu64, s->names[i], cid[root],
+                    kept ? "keep" : "remove", s->names[rep],
+                    single ? "singleton" : (kept ? "best_representative" : "duplicate"), sp_rep_rule(s, i, rep),
+                    comp->size[root], (uint64_t)sp_len(s, i), (uint64_t)sp_len(s, rep));
+            sp_print_meta(out, s, i);
+            sp_print_meta(out, s, rep);
+            fputc('\n', out);
+        } else {
+            fprintf(out, "%s\tcluster_%06d\t%d\t%s\n", s->names[i], cid[root], comp->size[root], s->names[rep]);
+        }
+    }
+    sp_close(out);
+    if (keep)
+        sp_close(keep);
+    if (rem)
+        sp_close(rem);
+    sp_keep_matrix(c, comp);
+    free(cid);
+}
+
+/* ---- one sketch */
+
+typedef struct sp_touch {
+    uint32_t first;
+    int r;
+} sp_touch_t;
+
+static int matrix_sparse_self(int fmt)
+{
+    const bool comps = fmt == MF_CLUSTERS || fmt == MF_DEDUP, dedup = fmt == MF_DEDUP;
+    /* matrix_parse_flags_for_format: component reports read the input metadata */
+    kssd_sketch_t *s = load_sketch(gm.qrydir, comps ? 2u : 0u);
+    init_bits(s);
+    g.o.p = gm.threads;
+    g.o.ignoreconflict = false;
+    if (dedup && !gm.max_afcut_set)
+        gm.max_afcut = 0.8;
+    const int n = s->n;
+    const size_t cells = (size_t)n * (size_t)(n > 0 ? n - 1 : 0) / 2;
+    /* exact features of every pair: the self join over the sketch's own index */
+    kssdgpu_ctx_mut2_t *lc = malloc(cells * sizeof(*lc) + 8);
+    kssdgpu_obj_section_t *lo = malloc(cells * sizeof(*lo) + 8);
+    if (!lc || !lo)
+        err(EXIT_FAILURE, "OOM lower triangle");
+    kssdgpu_index_t *ix = gpu_index_of_sketch(s);
+    if (cells)
+        gpu_check(kssdgpu_self_lower(ix, 0, lc, lo), "device self join");
+    uint32_t *cnt = sample_ctx_counts(s, s->stat.conflict, false);
+    const sp_self_t c = {s, lc, lo, cnt};
+    /* matrix_can_use_sorted_index: conflict-free sketch with an index file */
+    const bool indexed = !s->stat.conflict && kssd_file_exists(gm.qrydir, "sortedcomb_ctxgid64obj32");
+    FILE *edge_out = NULL;
+    if (comps) {
+        if (gm.edge_out[0]) {
+            edge_out = sp_open(gm.edge_out);
+            print_edge_header(edge_out);
+        }
+    } else {
+        edge_out = sp_open(gm.outf);
+        print_edge_header(edge_out);
+    }
+    sp_comp_t comp;
+    sp_comp_init(&comp, n);
+    sp_edges_t edges = {0};
+    if (indexed) {
+        /* pairwise_indexed_self_scan: votes over the index file's records */
+        size_t nrec = 0;
+        kssd_index_rec_t *rec = kssd_index_load(gm.qrydir, &nrec);
+        if (!rec)
+            errx(EXIT_FAILURE, "%s", kssd_host_last_error());
+        if (nrec != (size_t)(s->offs[n] - s->offs[0]))
+            errx(EINVAL, "pairwise_indexed_self_scan(): %s/sortedcomb_ctxgid64obj32 has %zu records, expected %llu",
+                 gm.qrydir, nrec, (unsigned long long)(s->offs[n] - s->offs[0]));
+        kssdgpu_index_t *vix = ix;
+        if (records_checksum(rec, nrec) != sketch_checksum(s))
+            gpu_check(kssdgpu_index_from_records(rec, nrec, n, s->obj_bits, 0, &vix), "device index");
+        free(rec);
+        uint32_t *votes = malloc(cells * sizeof(uint32_t) + 4), *first = malloc(cells * sizeof(uint32_t) + 4);
+        if (!votes || !first)
+            err(EXIT_FAILURE, "OOM votes");
+        if (cells)
+            gpu_check(kssdgpu_self_votes(vix, s->keys, s->offs, gm.max_ctx_freq, gm.sample_step, votes, first),
+                      "device votes");
+        if (vix != ix)
+            kssdgpu_index_free(vix);
+        /* rows in order; within a row, edges in the order the scan first touched them */
+        sp_edges_t *rows = calloc((size_t)(n ? n : 1), sizeof(sp_edges_t));
+        if (!rows)
+            err(EXIT_FAILURE, "OOM rows");
+#pragma omp parallel for schedule(dynamic, 16) num_threads(gm.threads)
+        for (int q = 1; q < n; ++q) {
+            const size_t base = (size_t)q * (size_t)(q - 1) / 2;
+            sp_touch_t *t = NULL;
+            size_t tn = 0, tc = 0;
+            for (int r = 0; r < q; ++r) {
+                if (!votes[base + r] || votes[base + r] < gm.min_votes)
+                    continue;
+                const pair_eval_t e = sp_eval(&c, q, r);
+                if (edge_class(&e) != 3)
+                    continue;
+                if (tn == tc) {
+                    tc = tc ? tc * 2 : 16;
+                    t = realloc(t, tc * sizeof(sp_touch_t));
+                    if (!t)
+                        err(EXIT_FAILURE, "OOM row edges");
+                }
+                t[tn++] = (sp_touch_t){first[base + r], r};
+            }
+            /* by first touch, then gid (the order of a context group's postings) */
+            for (size_t i = 1; i < tn; ++i) {
+                const sp_touch_t x = t[i];
+                size_t j = i;
+                while (j > 0 && (t[j - 1].first > x.first || (t[j - 1].first == x.first && t[j - 1].r > x.r))) {
+                    t[j] = t[j - 1];
+                    --j;
+                }
+                t[j] = x;
+            }
+            for (size_t i = 0; i < tn; ++i)
+                sp_push(&rows[q], q, t[i].r);
+            free(t);
+        }
+        for (int q = 1; q < n; ++q) {
+            for (size_t i = 0; i < rows[q].n; ++i) {
+                const int a = rows[q].e[i].a, b = rows[q].e[i].b;
+                if (comps && !dedup)
+                    sp_union(&comp, a, b);
+                if (dedup)
+                    sp_push(&edges, a, b);
+                if (edge_out) {
+                    const pair_eval_t e = sp_eval(&c, a, b);
+                    print_edge(edge_out, s->names[a], s->names[b], &e);
+                }
+            }
+            free(rows[q].e);
+        }
+        free(rows);
+        free(votes);
+        free(first);
+    } else if (!comps) {
+        /* matrix_compute_edges on one sketch: reference samples outer, later queries inner */
+        for (int rn = 0; rn < n; ++rn)
+            for (int qn = rn + 1; qn < n; ++qn) {
+                const pair_eval_t e = sp_eval(&c, qn, rn);
+                if (edge_class(&e) == 3)
+                    print_edge(edge_out, s->names[qn], s->names[rn], &e);
+            }
+    } else {
+        /* pairwise_build_components / pairwise_collect_dedup_edges: all pairs i < j */
+        for (int i = 0; i < n; ++i)
+            for (int j = i + 1; j < n; ++j) {
+                const pair_eval_t e = sp_eval(&c, i, j);
+                if (edge_class(&e) != 3)
+                    continue;
+                if (dedup)
+                    sp_push(&edges, i, j);
+                else
+                    sp_union(&comp, i, j);
+                if (edge_out)
+                    print_edge(edge_out, s->names[i], s->names[j], &e);
+            }
+    }
+    if (edge_out)
+        sp_close(edge_out);
+    if (comps) {
+        if (dedup) {
+            if (gm.dedup_strategy)
+                sp_dedup_complete(&comp, s, &edges);
+            else
+                sp_dedup_greedy(&comp, s, &edges);
+        } else {
+            sp_comp_finalize(&comp, s);
+        }
+        sp_component_report(&c, &comp, dedup);
+    }
+    matrix_glist(s);
+    free(edges.e);
+    sp_comp_free(&comp);
+    kssdgpu_index_free(ix);
+    free(cnt);
+    free(lc);
+    free(lo);
+    kssd_sketch_free(s);
+    return 0;
+}
+
+/* ---- -r/-q edges (matrix_compute_edges): reference samples outer, queries inner */
+
+typedef struct sp_redge {
+    int rn, qn;
+    pair_eval_t e;
+} sp_redge_t;
+
+static int matrix_sparse_rect(void)
+{
+    kssd_sketch_t *ref = load_sketch(gm.refdir, 0);
+    kssd_sketch_t *qry = load_sketch(gm.qrydir, 0);
+    if (ref->stat.hash_id != qry->stat.hash_id)
+        errx(EXIT_FAILURE, "pairwise_check_compatible(): ref hash_id %u != qry %u", ref->stat.hash_id,
+             qry->stat.hash_id);
+    init_bits(ref);
+    g.o.p = gm.threads;
+    const bool same = !strcmp(gm.refdir, gm.qrydir);
+    uint32_t *qc = sample_ctx_counts(qry, qry->stat.conflict, false);
+    uint32_t *rc = sample_ctx_counts(ref, ref->stat.conflict, false);
+    kssdgpu_index_t *ix = gpu_index_of_sketch(ref);
+    const int R = ref->n, B = block_for(R, qry->n);
+    sp_redge_t *all = NULL;
+    size_t an = 0, ac = 0;
+    for (int q0 = 0; q0 < qry->n; q0 += B) {
+        const int nb = qry->n - q0 < B ? qry->n - q0 : B;
+        counts_t cts = count_queries(ix, R, qry, q0, nb, 0);
+        for (int i = 0; i < nb; ++i) {
+            const int q = q0 + i;
+            for (int r = 0; r < R; ++r) {
+                if (same && q <= r)
+                    continue;
+                const kssdgpu_ctx_mut2_t *cc = &cts.ctx[(size_t)i * R + r];
+                if (!cc->num_ctx)
+                    continue;
+                const kssd_features_t f = feat_of(cc, &cts.obj[(size_t)i * R + r]);
+                const pair_eval_t e = pair_eval(&f, qc[q], rc[r], sp_len(qry, q), sp_len(ref, r), &g.o);
+                if (edge_class(&e) != 3)
+                    continue;
+                if (an == ac) {
+                    ac = ac ? ac * 2 : 1024;
+                    all = realloc(all, ac * sizeof(sp_redge_t));
+                    if (!all)
+                        err(EXIT_FAILURE, "OOM edges");
+                }
+                all[an++] = (sp_redge_t){r, q, e};
+            }
+        }
+        free_counts(&cts);
+    }
+    /* counting sort by reference sample; queries already ascend within one */
+    size_t *start = calloc((size_t)R + 1, sizeof(size_t));
+    sp_redge_t *sorted = malloc((an ? an : 1) * sizeof(sp_redge_t));
+    if (!start || !sorted)
+        err(EXIT_FAILURE, "OOM edge order");
+    for (size_t i = 0; i < an; ++i)
+        ++start[all[i].rn + 1];
+    for (int r = 0; r < R; ++r)
+        start[r + 1] += start[r];
+    for (size_t i = 0; i < an; ++i)
+        sorted[start[all[i].rn]++] = all[i];
+    FILE *out = sp_open(gm.outf);
+    print_edge_header(out);
+    for (size_t i = 0; i < an; ++i)
+        print_edge(out, qry->names[sorted[i].qn], ref->names[sorted[i].rn], &sorted[i].e);
+    sp_close(out);
+    free(sorted);
+    free(start);
+    free(all);
+    kssdgpu_index_free(ix);
+    free(qc);
+    free(rc);
+    kssd_sketch_free(ref);
+    kssd_sketch_free(qry);
+    return 0;
+}
+
 static int cmd_matrix(int argc, char **argv)
 {
     memset(&gm, 0, sizeof gm);
@@ -2049,21 +2931,27 @@ static int cmd_matrix(int argc, char **argv)
     kssd_opt_defaults(&g.o);
     gm.metric = MM_NAIVE;
     gm.metric_count = 1;
+    gm.metrics[0] = MM_NAIVE;
+    gm.metric_op = MOP_SINGLE;
+    snprintf(gm.metric_label, sizeof gm.metric_label, "ctx-naive");
     gm.threads = 1;
     gm.e = 1.0;
+    gm.max_ctx_freq = 256;
+    gm.min_votes = 1;
+    gm.sample_step = 1;
     argp_parse(&k_matrix_argp, argc, argv, ARGP_IN_ORDER, NULL, NULL);
     if (gm.qrylist[0])
         errx(EXIT_FAILURE, "--query-sketch-list is not supported by this build");
     const int fmt = gm.format != MF_AUTO ? gm.format : (gm.refdir[0] ? MF_FULL : MF_TRIANGLE);
-    if (fmt == MF_EDGES || fmt == MF_CLUSTERS || fmt == MF_DEDUP)
-        errx(EXIT_FAILURE, "sparse matrix formats (edges, clusters, dedup-plan) are not supported by this build");
     if (gm.refdir[0] && gm.ani)
         errx(EXIT_FAILURE, "the legacy --ani matrix is not supported by this build; use `kssd3a ani --format matrix`");
     if (!is_sketch_dir(gm.qrydir) || (gm.refdir[0] && !is_sketch_dir(gm.refdir)))
         errx(EXIT_FAILURE, "matrix inputs must be sketch directories");
     start_gpu_warmup();
     if (!gm.refdir[0])
-        return matrix_self(fmt);
+        return (fmt == MF_EDGES || fmt == MF_CLUSTERS || fmt == MF_DEDUP) ? matrix_sparse_self(fmt) : matrix_self(fmt);
+    if (fmt == MF_EDGES)
+        return matrix_sparse_rect();
     if (fmt != MF_FULL)
         errx(EINVAL, "compute_matrix(): --format clusters, dedup-plan, and triangle require one sketch");
     return matrix_rect();

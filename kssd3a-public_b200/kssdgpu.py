@@ -67,6 +67,7 @@ def gpu_lib() -> C.CDLL:
         lib.kssdgpu_count_block_dev.argtypes = [vp, vp, vp, C.c_int, C.c_int, C.c_int, C.c_uint,
                                                 vp, vp, vp, vp, vp]
         lib.kssdgpu_sync.argtypes = [vp, vp]
+        lib.kssdgpu_self_votes.argtypes = [vp, _u64p, _u64p, C.c_uint32, C.c_uint32, vp, vp]
         lib.kssdgpu_count_tune.argtypes = [vp, vp, vp, C.c_int, C.c_int, C.c_int, C.c_uint, vp, vp, vp, vp,
                                            C.POINTER(_CountTuning)]
         lib.kssdgpu_self_lower.argtypes = [vp, C.c_uint, vp, vp]
@@ -208,13 +209,18 @@ STAT_DTYPE = np.dtype([("hash_id", "<u4"), ("koc", "u1"), ("conflict", "u1"), ("
                        ("coden_len", "<i4"), ("klen", "<i4"), ("hclen", "<i4"), ("holen", "<i4"),
                        ("drfold", "<i4"), ("infile_num", "<i4")])
 REC_DTYPE = np.dtype([("ctxgid", "<u8"), ("obj", "<u4")])  # packed 12 B
+# infile_meta_t (src/global_basic.h:182-193): lcofiles.infilemeta records, 32 B
+META_DTYPE = np.dtype([("total_length_bp", "<u8"), ("record_count", "<u4"), ("median_length_bp", "<u4"),
+                       ("asm_level", "<f4"), ("length_cv", "<f4"), ("meta_fmt_version", "u1"), ("infile_fmt", "i1"),
+                       ("create_type", "i1"), ("infile_flags", "u1"), ("pad", "V4")])
 DEFAULT_HASH_ID = 1772583717  # the reference sketcher's id for its default coden/k=32/f8 pattern
 
 
 def write_sketch_dir(path: str, sk: Sketch, coden_len: int = 11, klen: int = 32, drfold: int = 8,
-                     hash_id: int = DEFAULT_HASH_ID, with_index: bool = False):
+                     hash_id: int = DEFAULT_HASH_ID, with_index: bool = False, meta: np.ndarray | None = None):
     """Write a sketch directory in the reference layout (lcofiles.stat, comblco, comblco.index);
-    with_index also writes sortedcomb_ctxgid64obj32 and its unique_bits."""
+    with_index also writes sortedcomb_ctxgid64obj32 and its unique_bits; meta (META_DTYPE,
+    one record per sample) writes lcofiles.infilemeta."""
     os.makedirs(path, exist_ok=True)
     st = np.zeros(1, dtype=STAT_DTYPE)
     st["hash_id"], st["koc"], st["conflict"] = hash_id, 0, int(sk.conflict)
@@ -225,6 +231,9 @@ def write_sketch_dir(path: str, sk: Sketch, coden_len: int = 11, klen: int = 32,
         f.write(st.tobytes() + names)
     sk.keys.astype("<u8").tofile(os.path.join(path, "comblco"))
     sk.offs.astype("<u8").tofile(os.path.join(path, "comblco.index"))
+    if meta is not None:
+        assert meta.dtype == META_DTYPE and len(meta) == sk.n
+        meta.tofile(os.path.join(path, "lcofiles.infilemeta"))
     if with_index:
         recs = build_records_np(sk)
         recs.tofile(os.path.join(path, "sortedcomb_ctxgid64obj32"))
@@ -384,6 +393,18 @@ class Index:
         _check(gpu_lib().kssdgpu_count_plain_dev(self._h, _ptr(d_keys), _ptr(d_offs), h, len(h) - 1,
                                                  qry_gid_offset, int(lower), flags, _ptr(d_ctx), _ptr(d_obj),
                                                  _ptr(d_uctx), _ptr(d_uobj), _ptr(stream)))
+
+    def self_votes(self, keys: np.ndarray, offs: np.ndarray, max_ctx_freq: int = 256, sample_step: int = 1):
+        """Sparse-scan candidate votes and first-touch positions over the packed lower triangle."""
+        n = self.nref
+        cells = n * (n - 1) // 2
+        votes = np.zeros(max(cells, 1), dtype=np.uint32)
+        first = np.zeros(max(cells, 1), dtype=np.uint32)
+        k = np.ascontiguousarray(keys, dtype=np.uint64)
+        _check(gpu_lib().kssdgpu_self_votes(self._h, k if len(k) else np.zeros(1, np.uint64),
+                                            np.ascontiguousarray(offs, dtype=np.uint64), max_ctx_freq, sample_step,
+                                            votes.ctypes.data, first.ctypes.data))
+        return votes[:cells], first[:cells]
 
     def self_plan_tune(self):
         """Autotune the self-join plan (once per index); returns the setting in use."""

@@ -304,3 +304,39 @@ void orc_pair_features(const uint64_t *a, size_t n, const uint64_t *b, size_t m,
         j = je;
     }
 }
+
+/* Candidate nomination of the indexed sparse scan, src/pairwise_graph.c:1195-1246:
+ * for sample q (its keys sorted), every step-th key (position qi*step) whose context
+ * the index holds in a group of at most max_freq records (0: any) gives one vote to
+ * each record gid < q of the group; first[(q, r)] is the smallest qi that voted for r
+ * (UINT32_MAX without a vote).  Cells packed lower-triangular (q*(q-1)/2 + r). */
+void orc_self_votes(const void *records, size_t len, const uint64_t *keys, const uint64_t *offs, int nsamples,
+                    int obj_bits, uint32_t max_freq, uint32_t step, uint32_t *votes, uint32_t *first)
+{
+    const orc_rec_t *r = records;
+    const size_t cells = (size_t)nsamples * (size_t)(nsamples > 0 ? nsamples - 1 : 0) / 2;
+    memset(votes, 0, cells * sizeof(uint32_t));
+    for (size_t c = 0; c < cells; c++)
+        first[c] = UINT32_MAX;
+    for (int q = 1; q < nsamples; q++) {
+        const uint64_t *a = keys + (offs[q] - offs[0]);
+        const size_t an = (size_t)(offs[q + 1] - offs[q]);
+        for (size_t pos = 0, qi = 0; pos < an; pos += step, qi++) {
+            const uint64_t ctx = a[pos] >> obj_bits;
+            size_t b = lower_bound_ctx(r, len, ctx), e = b;
+            while (e < len && (r[e].ctxgid >> ORC_GID_BITS) == ctx)
+                e++;
+            if (b == e || (max_freq && e - b > max_freq))
+                continue;
+            for (size_t k = b; k < e; k++) {
+                const uint32_t gid = (uint32_t)(r[k].ctxgid & ((1ull << ORC_GID_BITS) - 1));
+                if ((int)gid >= q)
+                    break;
+                const size_t cell = (size_t)q * (q - 1) / 2 + gid;
+                votes[cell]++;
+                if (qi < first[cell])
+                    first[cell] = (uint32_t)qi;
+            }
+        }
+    }
+}

@@ -50,6 +50,8 @@ void orc_pair_features(const uint64_t *a, size_t n, const uint64_t *b, size_t m,
                        int ignore_b_conflict, uint32_t out4[4]);
 /* src/dna_popcount.h:45-49. */
 int orc_dna_popcount(uint32_t x);
+void orc_self_votes(const void *records, size_t len, const uint64_t *keys, const uint64_t *offs, int nsamples,
+                    int obj_bits, uint32_t max_freq, uint32_t step, uint32_t *votes, uint32_t *first);
 
 #ifdef __cplusplus
 }

@@ -45,6 +45,8 @@ def oracle_lib() -> C.CDLL:
                                         C.c_int, C.c_int, _vp, _vp]
         lib.orc_pair_features.argtypes = [_u64p, C.c_size_t, _u64p, C.c_size_t, C.c_int, C.c_int, _u32p]
         lib.orc_dna_popcount.argtypes = [C.c_uint32]
+        lib.orc_self_votes.argtypes = [_vp, C.c_size_t, _u64p, _u64p, C.c_int, C.c_int, C.c_uint32, C.c_uint32,
+                                       _u32p, _u32p]
         _orc = lib
     return _orc
 
@@ -186,3 +188,14 @@ def self_lower_all(rec, sketch_keys, sketch_offs, obj_bits=20, ignoreconflict=Fa
             ctx[base: base + q] = c[i, :q]
             obj[base: base + q] = o[i, :q]
     return ctx, obj
+
+
+def self_votes(rec, keys, offs, obj_bits=20, max_freq=256, step=1):
+    """Sparse-scan candidate votes and first-touch order over the packed lower triangle."""
+    n = len(offs) - 1
+    cells = n * (n - 1) // 2
+    votes = np.zeros(max(cells, 1), dtype=np.uint32)
+    first = np.zeros(max(cells, 1), dtype=np.uint32)
+    oracle_lib().orc_self_votes(_rptr(rec), len(rec), _qk(keys), np.ascontiguousarray(offs, np.uint64), n, obj_bits,
+                                max_freq, step, votes, first)
+    return votes[:cells], first[:cells]

@@ -36,7 +36,23 @@ FIXTURES = {
                    sample_seed=31, ref_sample_seed=11, ref_samples=120, cov_lo=5, cov_hi=20, err_lo=0.001,
                    err_hi=0.005, name_prefix="reads"),
 }
-INDEXED = {"refs120i"}  # refs120 with sortedcomb_ctxgid64obj32 written up front
+INDEXED = {"refs120i", "refs120im"}  # with sortedcomb_ctxgid64obj32 written up front
+WITH_META = {"refs120im", "refs40m"}  # with lcofiles.infilemeta (per-sample input metadata)
+
+
+def synth_meta(sk, seed):
+    """Seeded per-sample input metadata (some records invalid, some FASTQ, ties on purpose)."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    m = np.zeros(sk.n, dtype=kssdgpu.META_DTYPE)
+    m["total_length_bp"] = (sk.lengths // 1000 * 1000).astype(np.uint64)  # ties between samples
+    m["record_count"] = rng.choice([0, 1, 2, 5, 40], sk.n)
+    m["median_length_bp"] = rng.choice([5000, 20000, 100000], sk.n)
+    m["asm_level"] = rng.choice([1.0, 2.0, 3.0, np.nan], sk.n).astype(np.float32)
+    m["length_cv"] = rng.choice([0.1, 0.5, np.inf], sk.n).astype(np.float32)
+    m["meta_fmt_version"] = rng.choice([1, 1, 1, 0], sk.n)
+    m["infile_fmt"] = rng.choice([1, 1, 2], sk.n)
+    return m
 
 # (case name, argv after `kssd3a`, extra environment)
 CASES = [
@@ -74,6 +90,31 @@ CASES = [
     ("matrix_rect_aaf", ["matrix", "-r", "{refs40}", "-q", "{qry8}", "-m", "aaf"], {}),
     ("matrix_rect_naive_e2", ["matrix", "-r", "{refs120}", "-q", "{qry30}", "-e", "2"], {}),
     ("matrix_reads_triangle", ["matrix", "-m", "ctx-moe", "-d", "{reads6}"], {}),
+    ("matrix_full_phylip_idmap", ["matrix", "--format", "full", "--matrix-format", "phylip", "--matrix-idmap",
+                                  "{out:ids.tsv}", "{refs40}"], {}),
+    # sparse reports: indexed scan (index file, conflict-free), direct pairs, -r/-q edges.
+    # The reference's indexed scan emits rows from several threads in any order: those
+    # cases compare the sorted lines ("_sorted").
+    ("matrix_edges_indexed", ["matrix", "--format", "edges", "--cut", "0.05", "{refs120i}"], {"_sorted": "1"}),
+    ("matrix_edges_indexed_votes", ["matrix", "--sparse", "--cut", "0.2", "--index-max-ctx-freq", "3",
+                                    "--index-min-votes", "2", "--index-sample-step", "2", "-m", "ctx-moe",
+                                    "{refs120i}"], {"_sorted": "1"}),
+    ("matrix_edges_direct_expr", ["matrix", "--format", "edges", "--cut", "0.1", "-m", "ctx-naive&aaf",
+                                  "--ctxcut", "50", "{refs40}"], {}),
+    ("matrix_edges_rect_or", ["matrix", "-r", "{refs40}", "-q", "{qry8}", "--format", "edges", "--cut", "0.3",
+                              "-m", "mash|p_dist", "--max-afcut", "0.2"], {}),
+    ("matrix_clusters_indexed", ["matrix", "--format", "clusters", "--cut", "0.05", "--edge-out",
+                                 "{out:edges.tsv}", "-g", "{out:glist.tsv}", "{refs120im}"], {"_sorted_out": "edges.tsv"}),
+    ("matrix_clusters_direct", ["matrix", "--format", "clusters", "--cut", "0.08", "-m", "p_dist",
+                                "--edge-out", "{out:edges.tsv}", "{refs40m}"], {}),
+    ("matrix_dedup_greedy", ["matrix", "--format", "dedup-plan", "--cut", "0.05", "--keep-out", "{out:keep.txt}",
+                             "--remove-out", "{out:remove.txt}", "--keep-matrix-out", "{out:keep.tsv}",
+                             "{refs120im}"], {}),
+    ("matrix_dedup_full_phylip", ["matrix", "--format", "dedup-plan", "--dedup-strategy", "full-linkage", "--cut",
+                                  "0.08", "--max-afcut", "0.5", "--keep-matrix-out", "{out:keep.phy}",
+                                  "--keep-matrix-format", "phylip", "--keep-matrix-idmap", "{out:keep.idmap}",
+                                  "--edge-out", "{out:edges.tsv}", "{refs40m}"], {}),
+    ("matrix_dedup_reads", ["matrix", "--format", "dedup-plan", "--cut", "0.5", "-m", "mash", "{reads6}"], {}),
 ]
 
 
@@ -82,10 +123,13 @@ def make_fixture(root: str, name: str) -> str:
     path = os.path.join(root, name)
     if os.path.isdir(path):
         return path
-    base = name[:-1] if name in INDEXED else name
+    base = name
+    while base not in FIXTURES:
+        base = base[:-1]
     spec = dict(FIXTURES[base])
     sk = kssdgpu.synth(**spec)
-    kssdgpu.write_sketch_dir(path, sk, with_index=name in INDEXED)
+    meta = synth_meta(sk, len(name)) if name in WITH_META else None
+    kssdgpu.write_sketch_dir(path, sk, with_index=name in INDEXED, meta=meta)
     return path
 
 
@@ -94,12 +138,21 @@ def with_threads(argv, threads=4):
     return [argv[0], "-p", str(threads), *argv[1:]]
 
 
+def out_files(argv):
+    """Names of the extra output files a case writes ({out:NAME} placeholders)."""
+    return [a[5:-1] for a in argv if a.startswith("{out:")]
+
+
 def materialize(root: str, argv, fresh_tag: str):
     """argv with fixture placeholders replaced by fresh copies (so side effects such
-    as automatic index creation start from the same state for every binary)."""
+    as automatic index creation start from the same state for every binary) and
+    {out:NAME} placeholders by files of this run."""
     out = []
     for a in argv:
-        if a.startswith("{") and a.endswith("}"):
+        if a.startswith("{out:"):
+            os.makedirs(os.path.join(root, fresh_tag), exist_ok=True)
+            out.append(os.path.join(root, fresh_tag, a[5:-1]))
+        elif a.startswith("{") and a.endswith("}"):
             name = a[1:-1]
             src = make_fixture(os.path.join(root, "_src"), name)
             dst = os.path.join(root, fresh_tag, name)

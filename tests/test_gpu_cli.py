@@ -8,7 +8,7 @@ import subprocess
 import pytest
 
 import oracle
-from cli_cases import CASES, materialize, with_threads
+from cli_cases import CASES, materialize, out_files, with_threads
 
 pytestmark = pytest.mark.gpu
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -20,7 +20,7 @@ def _run(binary, argv, env_extra):
     env = dict(os.environ, OMP_NUM_THREADS="4")
     for k in ("KSSD3A_FORCE_REF_INDEX", "KSSD3A_ANI_MATRIX_DIRECT_THRESHOLD", "KSSD3A_ANI_M1_DIRECT_THRESHOLD"):
         env.pop(k, None)
-    env.update(env_extra)
+    env.update({k: v for k, v in env_extra.items() if not k.startswith("_")})
     return subprocess.run([binary, *with_threads(argv)], capture_output=True, env=env, timeout=600)
 
 
@@ -43,12 +43,28 @@ def test_cli_bytes_match_reference(case, workdir):
         if not os.path.exists(path):
             pytest.skip("no reference binary and no golden output for this case")
         want = gzip.open(path).read()
-    if mine.stdout != want:
+    if env.get("_sorted"):
+        # header first, rows in any order
+        mine_lines, want_lines = mine.stdout.decode().splitlines(), want.decode().splitlines()
+        assert mine_lines[:1] == want_lines[:1]
+        assert sorted(mine_lines[1:]) == sorted(want_lines[1:])
+    elif mine.stdout != want:
         a, b = mine.stdout.decode().splitlines(), want.decode().splitlines()
         for i, (x, y) in enumerate(zip(a, b)):
             if x != y:
                 pytest.fail(f"first differing line {i}:\n ours: {x[:300]}\n want: {y[:300]}")
         pytest.fail(f"line counts differ: ours {len(a)} want {len(b)}")
+    # extra output files (edge lists, keep/remove lists, kept matrices, id maps, glists)
+    if oracle.ref_available():
+        for f in out_files(argv):
+            po = os.path.join(workdir, "ours_" + name, f)
+            pr = os.path.join(workdir, "ref_" + name, f)
+            assert os.path.exists(po) == os.path.exists(pr), f
+            if os.path.exists(po):
+                a, b = open(po, "rb").read(), open(pr, "rb").read()
+                if env.get("_sorted_out") == f:
+                    a, b = sorted(a.splitlines()), sorted(b.splitlines())
+                assert a == b, f
     # automatic index creation leaves identical files behind
     if oracle.ref_available():
         for a in argv:

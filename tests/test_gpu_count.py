@@ -276,3 +276,25 @@ def test_count_autotuner_keeps_counts():
     with pytest.raises(kssdgpu.KssdGpuError) as e:
         bidx.count_block(qry.keys[:10], np.array([0, 10], dtype=np.uint64), kssdgpu.SMEM_ACC)
     assert e.value.code == 7
+
+
+@pytest.mark.parametrize("max_freq,step", [(256, 1), (0, 1), (2, 1), (256, 3), (1, 2)])
+def test_sparse_scan_votes(max_freq, step):
+    """Candidate votes of the indexed sparse scan (and the scan's first-touch order)
+    equal the oracle's, on conflict-free genomes with shared and unshared contexts."""
+    sk = kssdgpu.synth(n_samples=60, n_clusters=6, len_median=3e5, len_min=1e5, len_max=1e6,
+                       size_dist=kssdgpu.SIZE_LOGNORMAL, sub_lo=0.001, sub_hi=0.1, seed=9, sample_seed=9)
+    rec = oracle.build_index(sk.keys, sk.offs)
+    idx = kssdgpu.Index.from_records(rec, sk.n)
+    v, f = idx.self_votes(sk.keys, sk.offs, max_freq, step)
+    wv, wf = oracle.self_votes(rec, sk.keys, sk.offs, max_freq=max_freq, step=step)
+    np.testing.assert_array_equal(v, wv)
+    np.testing.assert_array_equal(f, wf)
+    # a group of one posting holds no pair: max_freq 1 nominates nothing
+    assert (wv.sum() > 0) == (max_freq != 1)
+    # absolute offsets that do not start at 0
+    offs2 = sk.offs + np.uint64(7)
+    keys2 = sk.keys
+    v2, f2 = idx.self_votes(keys2, offs2, max_freq, step)
+    np.testing.assert_array_equal(v2, wv)
+    np.testing.assert_array_equal(f2, wf)
