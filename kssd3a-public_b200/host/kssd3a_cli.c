@@ -18,6 +18,7 @@
  */
 #define _GNU_SOURCE
 #include <argp.h>
+#include <ctype.h>
 #include <err.h>
 #include <errno.h>
 #include <fcntl.h>
@@ -1590,30 +1591,38 @@ enum {
 static struct argp_option k_matrix_opts[] = {
     {"ref", 'r', "<DIR>", 0, "Reference sketches. Omit for triangle mode.", 9},
     {"query", 'q', "<DIR>", 0, "Query sketches.", 1},
-    {"query-sketch-list", MK_QUERY_LIST, "<FILE>", 0, "Query sketch directories, one per line (not in this build).", 1},
+    {"query-sketch-list", MK_QUERY_LIST, "<FILE>", 0,
+     "One compatible -T query sketch directory per line; rectangular full matrix only.", 1},
     {"metric", 'm', "<METRIC>", 0, "ctx-moe, ctx-naive, p_dist, mash, or aaf; 0/1 alias mash/aaf. [ctx-naive]", 2},
-    {"format", MK_FORMAT, "<FORMAT>", 0, "full or triangle (edges, clusters and dedup-plan are not in this build). "
+    {"format", MK_FORMAT, "<FORMAT>", 0, "Report format: full, triangle, edges/sparse, clusters, or dedup-plan. "
                                          "[full for -r/-q; triangle for one sketch]", 2},
-    {"sparse", MK_SPARSE, 0, 0, "Alias for --format edges (not in this build).", 2},
-    {"cut", MK_CUT, "<FLOAT>", 0, "Distance cutoff for sparse reports.", 3},
-    {"dedup-strategy", MK_DEDUP, "<greedy|full-linkage>", 0, "Dedup-plan grouping strategy.", 3},
+    {"sparse", MK_SPARSE, 0, 0, "Alias for --format sparse/edges; requires --cut.", 2},
+    {"cut", MK_CUT, "<FLOAT>", 0, "Distance cutoff for sparse edge, cluster, and dedup-plan reports.", 3},
+    {"dedup-strategy", MK_DEDUP, "<greedy|full-linkage>", 0,
+     "Dedup-plan grouping strategy: greedy representative-neighbor or full-linkage clique. [greedy]", 3},
     {"control", 'c', "<FLOAT>", OPTION_HIDDEN, "Compatibility alias for --cut.", 3},
-    {"max-afcut", MK_MAX_AFCUT, "<FLOAT>", 0, "Minimum max align fraction for sparse edges.", 3},
-    {"ctxcut", MK_CTXCUT, "<INT>", 0, "Minimum shared context count for sparse edges.", 3},
-    {"index-max-ctx-freq", MK_MAX_CTX_FREQ, "<INT>", 0, "Indexed sparse candidate mode option.", 3},
-    {"index-min-votes", MK_MIN_VOTES, "<INT>", 0, "Indexed sparse candidate mode option.", 3},
-    {"index-sample-step", MK_SAMPLE_STEP, "<INT>", 0, "Indexed sparse candidate mode option.", 3},
+    {"max-afcut", MK_MAX_AFCUT, "<FLOAT>", 0,
+     "Minimum max(Qry_align_fraction, Ref_align_fraction) for sparse edges. [0; 0.8 for dedup-plan]", 3},
+    {"ctxcut", MK_CTXCUT, "<INT>", 0, "Minimum shared context count for sparse edges. [0]", 3},
+    {"index-max-ctx-freq", MK_MAX_CTX_FREQ, "<INT>", 0,
+     "Indexed sparse candidate mode: skip context groups above this frequency; 0 keeps all contexts. [256]", 3},
+    {"index-min-votes", MK_MIN_VOTES, "<INT>", 0,
+     "Indexed sparse candidate mode: exact-score pairs with at least this many candidate context votes. [1]", 3},
+    {"index-sample-step", MK_SAMPLE_STEP, "<INT>", 0,
+     "Indexed sparse candidate mode: use every Nth query context for nomination. [1]", 3},
     {"progress", MK_PROGRESS, "<auto|on|off>", 0, "Progress on stderr (accepted; no progress is printed).", 3},
     {"glist", 'g', "<FILE>", 0, "Sample output file for KSSD set grouping.", 4},
     {"outfile", 'o', "<FILE>", 0, "Matrix output file. [STDOUT]", 5},
     {"matrix-format", MK_MATRIX_FORMAT, "<tsv|phylip>", 0, "Output format for --format full. [tsv]", 5},
     {"matrix-idmap", MK_MATRIX_IDMAP, "<FILE>", 0, "With --matrix-format phylip, write short-ID to sample-name map.", 5},
-    {"edge-out", MK_EDGE_OUT, "<FILE>", 0, "Sparse edge TSV (not in this build).", 5},
-    {"keep-out", MK_KEEP_OUT, "<FILE>", 0, "Dedup-plan output (not in this build).", 5},
-    {"remove-out", MK_REMOVE_OUT, "<FILE>", 0, "Dedup-plan output (not in this build).", 5},
-    {"keep-matrix-out", MK_KEEP_MATRIX_OUT, "<FILE>", 0, "Dedup-plan output (not in this build).", 5},
-    {"keep-matrix-format", MK_KEEP_MATRIX_FORMAT, "<tsv|phylip>", 0, "Dedup-plan output format.", 5},
-    {"keep-matrix-idmap", MK_KEEP_MATRIX_IDMAP, "<FILE>", 0, "Dedup-plan id map.", 5},
+    {"edge-out", MK_EDGE_OUT, "<FILE>", 0, "Optional sparse edge TSV for cluster/dedup-plan reports.", 5},
+    {"keep-out", MK_KEEP_OUT, "<FILE>", 0, "Write one kept sample per line for dedup-plan reports.", 5},
+    {"remove-out", MK_REMOVE_OUT, "<FILE>", 0, "Write one removed sample per line for dedup-plan reports.", 5},
+    {"keep-matrix-out", MK_KEEP_MATRIX_OUT, "<FILE>", 0,
+     "With dedup-plan, write a dense distance matrix for kept representatives.", 5},
+    {"keep-matrix-format", MK_KEEP_MATRIX_FORMAT, "<tsv|phylip>", 0, "Output format for --keep-matrix-out. [tsv]", 5},
+    {"keep-matrix-idmap", MK_KEEP_MATRIX_IDMAP, "<FILE>", 0,
+     "With --keep-matrix-format phylip, write short-ID to sample-name map.", 5},
     {"threads", 'p', "<INT>", 0, "Number of host threads to use.", 6},
     {"diagonal", 'd', 0, 0, "Print diagonal values in triangle mode. [0]", 7},
     {"diagonal-value", MK_DIAG_VALUE, "<FLOAT>", 0, "Set diagonal value and enable diagonal output.", 7},
@@ -2116,16 +2125,97 @@ static int matrix_self(int fmt)
     return 0;
 }
 
+/* matrix_load_query_sketch_list (src/command_matrix.c:1350-1450): the listed sketch
+ * directories (one per line; blank lines and # comments skipped), compatible with the
+ * first, concatenated into one query sketch */
+static char *trim_line(char *line)
+{
+    while (*line && isspace((unsigned char)*line))
+        ++line;
+    char *end = line + strlen(line);
+    while (end > line && isspace((unsigned char)end[-1]))
+        *--end = '\0';
+    return line;
+}
+
+static kssd_sketch_t *load_query_list(const char *list_path)
+{
+    FILE *fp = fopen(list_path, "r");
+    if (!fp)
+        err(errno, "open failed for %s", list_path);
+    kssd_sketch_t **parts = NULL;
+    size_t np = 0, cap = 0, samples = 0, entries = 0;
+    char *line = NULL;
+    size_t lcap = 0;
+    while (getline(&line, &lcap, fp) >= 0) {
+        char *dir = trim_line(line);
+        if (!*dir || *dir == '#')
+            continue;
+        kssd_sketch_t *part = load_sketch(dir, 0);
+        if (np) {
+            const kssd_sketch_stat_t *e = &parts[0]->stat, *a = &part->stat;
+            if (e->hash_id != a->hash_id || e->koc != a->koc || e->conflict != a->conflict ||
+                e->coden_len != a->coden_len || e->klen != a->klen || e->hclen != a->hclen || e->holen != a->holen ||
+                e->drfold != a->drfold)
+                errx(EINVAL, "--query-sketch-list entry is incompatible with the first entry: %s", dir);
+        }
+        if (np == cap) {
+            cap = cap ? cap * 2 : 16;
+            parts = realloc(parts, cap * sizeof(*parts));
+            if (!parts)
+                err(EXIT_FAILURE, "realloc query sketch list");
+        }
+        parts[np++] = part;
+        samples += (size_t)part->n;
+        entries += (size_t)(part->offs[part->n] - part->offs[0]);
+    }
+    free(line);
+    fclose(fp);
+    if (np == 0)
+        errx(EINVAL, "no query sketch directories listed in %s", list_path);
+    if (samples > (size_t)INT_MAX)
+        errx(EOVERFLOW, "--query-sketch-list is too large");
+    kssd_sketch_t *m = calloc(1, sizeof *m);
+    if (!m)
+        err(EXIT_FAILURE, "allocate merged query sketch");
+    m->stat = parts[0]->stat;
+    m->stat.infile_num = (int32_t)samples;
+    m->n = (int)samples;
+    m->obj_bits = parts[0]->obj_bits;
+    m->ctx_bits = parts[0]->ctx_bits;
+    m->names = malloc((samples ? samples : 1) * KSSD_PATHLEN);
+    m->keys = malloc((entries ? entries : 1) * sizeof(uint64_t));
+    m->offs = calloc(samples + 1, sizeof(uint64_t));
+    if (!m->names || !m->keys || !m->offs)
+        err(EXIT_FAILURE, "allocate merged query sketch payload");
+    size_t so = 0, eo = 0;
+    for (size_t p = 0; p < np; ++p) {
+        const kssd_sketch_t *part = parts[p];
+        const size_t pe = (size_t)(part->offs[part->n] - part->offs[0]);
+        for (int i = 0; i < part->n; ++i) {
+            memcpy(m->names[so + (size_t)i], part->names[i], KSSD_PATHLEN);
+            m->offs[so + (size_t)i + 1] = eo + (part->offs[i + 1] - part->offs[0]);
+        }
+        if (pe)
+            memcpy(m->keys + eo, part->keys, pe * sizeof(uint64_t));
+        so += (size_t)part->n;
+        eo += pe;
+        kssd_sketch_free(parts[p]);
+    }
+    free(parts);
+    return m;
+}
+
 static int matrix_rect(void)
 {
     kssd_sketch_t *ref = load_sketch(gm.refdir, 0);
-    kssd_sketch_t *qry = load_sketch(gm.qrydir, 0);
+    kssd_sketch_t *qry = gm.qrylist[0] ? load_query_list(gm.qrylist) : load_sketch(gm.qrydir, 0);
     if (ref->stat.hash_id != qry->stat.hash_id)
         errx(EXIT_FAILURE, "pairwise_check_compatible(): ref hash_id %u != qry %u", ref->stat.hash_id,
              qry->stat.hash_id);
     init_bits(ref);
     g.o.p = gm.threads;
-    const bool same = !strcmp(gm.refdir, gm.qrydir);
+    const bool same = !gm.qrylist[0] && !strcmp(gm.refdir, gm.qrydir);
     uint32_t *qc = sample_ctx_counts(qry, qry->stat.conflict, false);
     uint32_t *rc = sample_ctx_counts(ref, ref->stat.conflict, false);
     kssdgpu_index_t *ix = gpu_index_of_sketch(ref);
@@ -2940,13 +3030,16 @@ static int cmd_matrix(int argc, char **argv)
     gm.min_votes = 1;
     gm.sample_step = 1;
     argp_parse(&k_matrix_argp, argc, argv, ARGP_IN_ORDER, NULL, NULL);
-    if (gm.qrylist[0])
-        errx(EXIT_FAILURE, "--query-sketch-list is not supported by this build");
     const int fmt = gm.format != MF_AUTO ? gm.format : (gm.refdir[0] ? MF_FULL : MF_TRIANGLE);
     if (gm.refdir[0] && gm.ani)
         errx(EXIT_FAILURE, "the legacy --ani matrix is not supported by this build; use `kssd3a ani --format matrix`");
-    if (!is_sketch_dir(gm.qrydir) || (gm.refdir[0] && !is_sketch_dir(gm.refdir)))
+    if ((!gm.qrylist[0] && !is_sketch_dir(gm.qrydir)) || (gm.refdir[0] && !is_sketch_dir(gm.refdir)))
         errx(EXIT_FAILURE, "matrix inputs must be sketch directories");
+    if (gm.qrylist[0]) {
+        /* compute_matrix_query_list: rectangular full matrix against the listed queries */
+        start_gpu_warmup();
+        return matrix_rect();
+    }
     start_gpu_warmup();
     if (!gm.refdir[0])
         return (fmt == MF_EDGES || fmt == MF_CLUSTERS || fmt == MF_DEDUP) ? matrix_sparse_self(fmt) : matrix_self(fmt);

@@ -115,6 +115,8 @@ CASES = [
                                   "--keep-matrix-format", "phylip", "--keep-matrix-idmap", "{out:keep.idmap}",
                                   "--edge-out", "{out:edges.tsv}", "{refs40m}"], {}),
     ("matrix_dedup_reads", ["matrix", "--format", "dedup-plan", "--cut", "0.5", "-m", "mash", "{reads6}"], {}),
+    ("matrix_query_list", ["matrix", "-r", "{refs40}", "--query-sketch-list", "{list:qry8,qry1}", "-m", "ctx-moe"],
+     {}),
 ]
 
 
@@ -149,7 +151,15 @@ def materialize(root: str, argv, fresh_tag: str):
     {out:NAME} placeholders by files of this run."""
     out = []
     for a in argv:
-        if a.startswith("{out:"):
+        if a.startswith("{list:"):
+            # a --query-sketch-list file naming fresh copies of the fixtures (with a
+            # comment, a blank line and surrounding blanks the parser must skip)
+            dirs = materialize(root, ["{" + n + "}" for n in a[6:-1].split(",")], fresh_tag)
+            path = os.path.join(root, fresh_tag, "query_list.txt")
+            with open(path, "w") as f:
+                f.write("# query sketches\n\n" + "".join(f"  {d} \n" for d in dirs))
+            out.append(path)
+        elif a.startswith("{out:"):
             os.makedirs(os.path.join(root, fresh_tag), exist_ok=True)
             out.append(os.path.join(root, fresh_tag, a[5:-1]))
         elif a.startswith("{") and a.endswith("}"):
