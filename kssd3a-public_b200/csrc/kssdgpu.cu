@@ -1003,6 +1003,8 @@ struct kssdgpu_index {
     DevBuf<int> s_order;
     DevBuf<WorkItem> s_items;
     DevBuf<uint32_t> s_prefix, s_counts;    // device-built chunk prefix of a query block
+    cudaStream_t pipe_st[3] = {nullptr, nullptr, nullptr};  // host-buffer pipeline: H2D, count, D2H
+    std::vector<cudaEvent_t> pipe_ev;
     // batched-count setting (kssdgpu_count_tune): shared-memory rows where they fit, or
     // global rows in key-range chunks of count_chunk_keys entries
     bool count_smem = false;
@@ -1267,6 +1269,113 @@ int count_dev_impl(kssdgpu_index *ix, const uint64_t *d_keys, const uint64_t *d_
     return unique ? launch_batched<false, true, false>(ix, P, 0, st) : launch_batched<false, false, false>(ix, P, 0, st);
 }
 
+// A host-buffer count is split into sub-blocks whose copies overlap the counting when
+// the block is large and the host buffers are page-locked (asynchronous copies need it).
+bool host_pinned(const void *p)
+{
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
+bool pipeline_worthwhile(kssdgpu_index *ix, int nq, uint64_t nkeys, const void *qkeys, const void *ctx)
+{
+    (void)ix;
+    return nq >= 16 && nkeys >= (8ull << 20) && host_pinned(qkeys) && host_pinned(ctx);
+}
+
+// Sub-blocks of about equal key counts; per sub-block: keys H2D on one stream, the
+// batched count on the compute stream (stream-ordered, so the index's scratch is
+// reused safely), counter rows D2H on a third stream.
+int count_host_pipelined(kssdgpu_index *ix, const uint64_t *qkeys, const uint64_t *qoffs, int nq, int qgid_offset,
+                         bool lower, unsigned flags, void *ctx, void *obj, void *uctx, void *uobj,
+                         const std::vector<uint64_t> &sizes)
+{
+    const bool unique = (flags & KSSDGPU_UNIQUE) != 0;
+    const uint64_t nkeys = qoffs[nq] - qoffs[0];
+    const int parts = std::min(8, nq / 2);
+    std::vector<int> cut(1, 0);
+    for (int p = 1; p < parts; ++p) {
+        const uint64_t target = qoffs[0] + nkeys * (uint64_t)p / (uint64_t)parts;
+        int q = (int)(std::upper_bound(qoffs, qoffs + nq + 1, target) - qoffs) - 1;
+        q = std::max(q, cut.back() + 1);
+        if (q < nq)
+            cut.push_back(q);
+    }
+    cut.push_back(nq);
+    const int np = (int)cut.size() - 1;
+    // per sub-block query order (largest first) and key-range chunks, relative to it
+    const bool smem = uses_smem_row(ix, flags);
+    std::vector<int> order_all(nq);
+    std::vector<WorkItem> items_all;
+    std::vector<size_t> item_off(np + 1, 0);
+    for (int p = 0; p < np; ++p) {
+        const int q0 = cut[p], nb = cut[p + 1] - q0;
+        int *ord = order_all.data() + q0;
+        std::iota(ord, ord + nb, 0);
+        std::stable_sort(ord, ord + nb, [&](int a, int b) { return sizes[q0 + a] > sizes[q0 + b]; });
+        if (!smem) {
+            std::vector<WorkItem> it;
+            build_chunks(qoffs + q0, nb, ord, ix->count_chunk_keys, it);
+            items_all.insert(items_all.end(), it.begin(), it.end());
+        }
+        item_off[p + 1] = items_all.size();
+    }
+    const size_t cells = (size_t)nq * ix->nref;
+    const int nout = unique ? 4 : 2;
+    CUDA_TRY(ix->s_keys.ensure(nkeys));
+    CUDA_TRY(ix->s_offs.ensure((size_t)nq + 1));
+    CUDA_TRY(ix->s_out.ensure(cells * nout));
+    CUDA_TRY(ix->s_order.ensure((size_t)nq));
+    CUDA_TRY(ix->s_items.ensure(items_all.size()));
+    for (int i = 0; i < 3; ++i)
+        if (!ix->pipe_st[i])
+            CUDA_TRY(cudaStreamCreateWithFlags(&ix->pipe_st[i], cudaStreamNonBlocking));
+    while ((int)ix->pipe_ev.size() < 2 * np) {
+        cudaEvent_t e;
+        CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        ix->pipe_ev.push_back(e);
+    }
+    cudaStream_t sin = ix->pipe_st[0], scomp = ix->pipe_st[1], sout = ix->pipe_st[2];
+    // small tables first, on the compute stream
+    CUDA_TRY(cudaMemcpyAsync(ix->s_offs.p, qoffs, ((size_t)nq + 1) * 8, cudaMemcpyHostToDevice, scomp));
+    CUDA_TRY(cudaMemcpyAsync(ix->s_order.p, order_all.data(), (size_t)nq * sizeof(int), cudaMemcpyHostToDevice, scomp));
+    if (!items_all.empty())
+        CUDA_TRY(cudaMemcpyAsync(ix->s_items.p, items_all.data(), items_all.size() * sizeof(WorkItem),
+                                 cudaMemcpyHostToDevice, scomp));
+    unsigned long long *oc = ix->s_out.p, *oo = oc + cells;
+    unsigned long long *uc = unique ? oo + cells : nullptr, *uo = unique ? uc + cells : nullptr;
+    void *hout[4] = {ctx, obj, uctx, uobj};
+    unsigned long long *dout[4] = {oc, oo, uc, uo};
+    for (int p = 0; p < np; ++p) {
+        const int q0 = cut[p], nb = cut[p + 1] - q0;
+        const uint64_t k0 = qoffs[q0] - qoffs[0], kn = qoffs[q0 + nb] - qoffs[q0];
+        if (kn)
+            CUDA_TRY(cudaMemcpyAsync(ix->s_keys.p + k0, qkeys + k0, kn * 8, cudaMemcpyHostToDevice, sin));
+        CUDA_TRY(cudaEventRecord(ix->pipe_ev[2 * p], sin));
+        CUDA_TRY(cudaStreamWaitEvent(scomp, ix->pipe_ev[2 * p], 0));
+        const size_t c0 = (size_t)q0 * ix->nref, cn = (size_t)nb * ix->nref;
+        std::vector<uint64_t> sub_sizes(sizes.begin() + q0, sizes.begin() + q0 + nb);
+        const size_t ni = item_off[p + 1] - item_off[p];
+        int rc = count_dev_impl(ix, ix->s_keys.p + k0, ix->s_offs.p + q0, nb, qgid_offset + q0, lower, flags, oc + c0,
+                                oo + c0, unique ? uc + c0 : nullptr, unique ? uo + c0 : nullptr, ix->s_order.p + q0,
+                                &sub_sizes, scomp, ni ? ix->s_items.p + item_off[p] : nullptr, (int)ni);
+        if (rc)
+            return rc;
+        CUDA_TRY(cudaEventRecord(ix->pipe_ev[2 * p + 1], scomp));
+        CUDA_TRY(cudaStreamWaitEvent(sout, ix->pipe_ev[2 * p + 1], 0));
+        for (int o = 0; o < nout; ++o)
+            CUDA_TRY(cudaMemcpyAsync(static_cast<unsigned long long *>(hout[o]) + c0, dout[o] + c0, cn * 8,
+                                     cudaMemcpyDeviceToHost, sout));
+    }
+    CUDA_TRY(cudaStreamSynchronize(sin));
+    CUDA_TRY(cudaStreamSynchronize(scomp));
+    return check_dev_err(ix, sout);
+}
+
 int count_host_impl(kssdgpu_index *ix, const uint64_t *qkeys, const uint64_t *qoffs, int nq, int qgid_offset, bool lower,
                     unsigned flags, void *ctx, void *obj, void *uctx, void *uobj)
 {
@@ -1289,6 +1398,8 @@ int count_host_impl(kssdgpu_index *ix, const uint64_t *qkeys, const uint64_t *qo
             return fail(KSSDGPU_ERR_ARG, "query offsets are not monotone");
         sizes[i] = qoffs[i + 1] - qoffs[i];
     }
+    if (!(flags & KSSDGPU_PLAIN) && pipeline_worthwhile(ix, nq, nkeys, qkeys, ctx))
+        return count_host_pipelined(ix, qkeys, qoffs, nq, qgid_offset, lower, flags, ctx, obj, uctx, uobj, sizes);
     std::vector<int> order(nq);
     std::iota(order.begin(), order.end(), 0);
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return sizes[a] > sizes[b]; });
@@ -1857,6 +1968,12 @@ void kssdgpu_index_free(kssdgpu_index_t *ix)
     ix->s_order.release();
     ix->s_items.release();
     ix->s_prefix.release();
+    for (int i = 0; i < 3; ++i)
+        if (ix->pipe_st[i])
+            cudaStreamDestroy(ix->pipe_st[i]);
+    for (cudaEvent_t e : ix->pipe_ev)
+        cudaEventDestroy(e);
+    ix->pipe_ev.clear();
     ix->s_counts.release();
     ix->s_cubtmp.release();
     ix->j_small.release();

@@ -298,3 +298,31 @@ def test_sparse_scan_votes(max_freq, step):
     v2, f2 = idx.self_votes(keys2, offs2, max_freq, step)
     np.testing.assert_array_equal(v2, wv)
     np.testing.assert_array_equal(f2, wf)
+
+
+@pytest.mark.parametrize("mode", ["block_unique", "lower"])
+def test_pinned_host_buffers_pipeline(mode):
+    """With page-locked host buffers a large block is split into sub-blocks whose copies
+    overlap the counting; the counters equal the single-pass ones (pageable buffers)."""
+    import torch
+    sk = kssdgpu.synth(n_samples=600, n_clusters=60, size_dist=kssdgpu.SIZE_LOGNORMAL, len_median=4e6,
+                       len_sigma=0.37, len_min=1e6, len_max=12e6, sub_lo=0.001, sub_hi=0.2, seed=3, sample_seed=3)
+    assert int(sk.offs[-1]) >= 8 << 20
+    idx = kssdgpu.Index.from_sketch(sk)
+    n = sk.n
+    lib = kssdgpu.gpu_lib()
+    h_keys = torch.from_numpy(sk.keys.view(np.int64)).pin_memory()
+    nout = 4 if mode == "block_unique" else 2
+    outs = [torch.empty(n * n * 2, dtype=torch.int32).pin_memory() for _ in range(nout)]
+    offs = np.ascontiguousarray(sk.offs)
+    if mode == "block_unique":
+        rc = lib.kssdgpu_count_block(idx.handle, h_keys.data_ptr(), offs, n, kssdgpu.UNIQUE,
+                                     *[o.data_ptr() for o in outs])
+        want = idx.count_block(sk.keys, sk.offs, kssdgpu.UNIQUE)
+    else:
+        rc = lib.kssdgpu_count_lower(idx.handle, h_keys.data_ptr(), offs, n, 0, 0, outs[0].data_ptr(),
+                                     outs[1].data_ptr())
+        want = idx.count_lower(sk.keys, sk.offs, 0)
+    assert rc == 0, lib.kssdgpu_last_error()
+    for g, w in zip(outs, want):
+        np.testing.assert_array_equal(g.numpy().view(np.uint32).reshape(n, n, 2), w)
