@@ -98,7 +98,9 @@ static struct argp_option k_opts[] = {
     {"values", O_VALUES, "<distance|ani>", 0, "Matrix/triangle values; overrides the sign of -s. [distance]", 4},
     {"outfile", 'o', "<FILE>", 0, "Output file. [STDOUT]", 4},
     {"raw-output", O_RAW_OUTPUT, 0, 0, "Skip calibrated/best ANI computation.", 4},
-    {"estimate-coverage", O_COVERAGE, 0, 0, "Coverage columns for --qraw detail (not in this build).", 4},
+    {"estimate-coverage", O_COVERAGE, 0, 0,
+     "Append abundance-derived coverage/depth columns for --qraw detail output when the query sketch has comblco.a.",
+     4},
     {"unique-ctx-report", O_UNIQUE_REPORT, "<FILE>", 0, "Write unfiltered unique-context counts to a new file.", 4},
     {"top", 'N', "<INT>", 0, "Report at most top N references per query. [all]", 4},
     {0, 0, 0, 0, "Execution:", 5},
@@ -753,6 +755,90 @@ static FILE *open_out_with_report(const char *path, FILE *report)
     return fp;
 }
 
+/* ---- --estimate-coverage inputs */
+
+/* load_coverage_unique_bits (src/command_ani.c:2209-2253): the reference database's
+ * marker bits when its index and .unique_bits are both present and sized right */
+typedef struct cov_db {
+    kssd_cov_refdb_t db;
+    uint8_t *bits;
+    kssd_index_rec_t *rec;
+    bool own_rec;
+} cov_db_t;
+
+static void cov_db_load(cov_db_t *c, const char *refdir, uint64_t entries, kssd_index_rec_t *rec)
+{
+    memset(c, 0, sizeof *c);
+    if (!kssd_file_exists(refdir, "sortedcomb_ctxgid64obj32.unique_bits"))
+        return;
+    if (!kssd_file_exists(refdir, "sortedcomb_ctxgid64obj32")) {
+        warnx("load_coverage_unique_bits(): ignoring %s/%s because %s is missing", refdir,
+              "sortedcomb_ctxgid64obj32.unique_bits", "sortedcomb_ctxgid64obj32");
+        return;
+    }
+    size_t nbits = 0;
+    c->bits = kssd_unique_bits_load(refdir, &nbits);
+    if (!c->bits || nbits != (size_t)((entries + 7u) >> 3)) {
+        warnx("load_coverage_unique_bits(): ignoring %s/%s: %zu bytes, expected %zu", refdir,
+              "sortedcomb_ctxgid64obj32.unique_bits", nbits, (size_t)((entries + 7u) >> 3));
+        free(c->bits);
+        c->bits = NULL;
+        return;
+    }
+    if (rec) {
+        c->rec = rec;
+    } else {
+        size_t n = 0;
+        c->rec = kssd_index_load(refdir, &n);
+        c->own_rec = true;
+        if (!c->rec || n != entries) {
+            warnx("load_coverage_unique_bits(): ignoring %s/%s: %zu records, expected %llu", refdir,
+                  "sortedcomb_ctxgid64obj32", n, (unsigned long long)entries);
+            free(c->rec);
+            free(c->bits);
+            memset(c, 0, sizeof *c);
+            return;
+        }
+    }
+    c->db.available = true;
+    c->db.entries = entries;
+    c->db.bits = c->bits;
+    c->db.sorted = c->rec;
+}
+
+static void cov_db_free(cov_db_t *c)
+{
+    free(c->bits);
+    if (c->own_rec)
+        free(c->rec);
+    memset(c, 0, sizeof *c);
+}
+
+/* the query's per-key counts: mem_eff reads comblco.a when present and sized right
+ * (src/command_ani.c:536-551); the streaming paths with the sketch when it was made
+ * with counting (SKETCH_PARSE_ABUNDANCE, src/global_basic.c:1123-1124) */
+static uint32_t *cov_query_counts(const kssd_sketch_t *q, const char *dir, bool required)
+{
+    const size_t entries = (size_t)(q->offs[q->n] - q->offs[0]);
+    if (!kssd_file_exists(dir, "comblco.a")) {
+        if (required)
+            errx(EXIT_FAILURE, "%s/comblco.a: missing abundances of a counted sketch", dir);
+        return NULL;
+    }
+    size_t n = 0;
+    uint32_t *a = kssd_abundance_load(dir, &n);
+    if (!a)
+        errx(EXIT_FAILURE, "%s", kssd_host_last_error());
+    if (n != entries) {
+        if (required)
+            errx(EXIT_FAILURE, "%s/comblco.a has %zu counts, expected %zu", dir, n, entries);
+        warnx("ani_mem_eff(): ignoring %s/comblco.a: %zu bytes, expected %zu", dir, n * 4, entries * 4);
+        free(a);
+        return NULL;
+    }
+    return a;
+}
+
 static int run_mem_eff(void)
 {
     kssd_ani_opt_t *o = &g.o;
@@ -771,7 +857,15 @@ static int run_mem_eff(void)
     const int R = ref->n;
     kssdgpu_index_t *ix = NULL;
     gpu_check(kssdgpu_index_from_records(rec, nrec, R, qry->obj_bits, 0, &ix), "device index");
-    free(rec);
+    const bool coverage = o->estimate_coverage && o->fmt == 0;
+    cov_db_t cov = {0};
+    uint32_t *qab = NULL;
+    if (coverage) {
+        cov_db_load(&cov, g.refdir, nrec, rec);
+        qab = cov_query_counts(qry, g.qrydir, false);
+    }
+    if (!cov.rec)
+        free(rec);
     uint32_t *rcnt = malloc((size_t)R * 4 + 4), *uref = malloc((size_t)R * 4 + 4);
     if (ref->stat.conflict)
         gpu_check(kssdgpu_index_ref_ctx_counts(ix, 1, o->ignoreconflict, rcnt, uref), "reference counts");
@@ -803,6 +897,10 @@ static int run_mem_eff(void)
         kssd_buf_putc(&hb, '\n');
     } else {
         kssd_buf_puts(&hb, kssd_detail_header);
+        if (coverage) {
+            kssd_buf_putc(&hb, '\t');
+            kssd_buf_puts(&hb, kssd_coverage_header);
+        }
         kssd_buf_putc(&hb, '\n');
     }
     write_buf(out, &hb);
@@ -878,6 +976,10 @@ static int run_mem_eff(void)
             }
             const int loop = o->fmt ? R : out_n;
             const int qsize = (int)qcnt[qg];
+            /* with coverage the reported rows are collected, their coverage computed
+             * together, then printed (ani_block_print_internal, src/command_ani.c:3452-3544) */
+            kssd_row_t *cov_rows = coverage ? malloc((size_t)(loop ? loop : 1) * sizeof(kssd_row_t)) : NULL;
+            size_t cov_n = 0;
             for (int n = 0; n < loop; ++n) {
                 const int j = o->fmt ? n : (int)ids[n];
                 kssd_features_t f = feat_of(&cx[j], &ob[j]);
@@ -904,9 +1006,22 @@ static int run_mem_eff(void)
                 const double metric = o->s < 0 ? row.selected_ani : row.metric;
                 if (o->fmt)
                     kssd_buf_printf(b, "\t%lf", metric);
-                else if (row.selected_ani >= o->anicut)
-                    kssd_append_detail_row(b, o, qry->names[qg], ref->names[j], &row, anno_at(ref, (uint32_t)j));
+                else if (row.selected_ani >= o->anicut) {
+                    if (coverage)
+                        cov_rows[cov_n++] = row;
+                    else
+                        kssd_append_detail_row(b, o, qry->names[qg], ref->names[j], &row, anno_at(ref, (uint32_t)j));
+                }
             }
+            if (coverage && cov_n) {
+                const size_t qb = (size_t)(qry->offs[qg] - qry->offs[0]);
+                kssd_coverage_rows(qry->keys + qb, qab ? qab + qb : NULL, a_size, ref->keys, ref->offs,
+                                   cov.db.available ? &cov.db : NULL, qry->obj_bits, cov_rows, cov_n);
+                for (size_t k = 0; k < cov_n; ++k)
+                    kssd_append_detail_row(b, o, qry->names[qg], ref->names[cov_rows[k].rn], &cov_rows[k],
+                                           anno_at(ref, cov_rows[k].rn));
+            }
+            free(cov_rows);
             if (o->fmt)
                 kssd_buf_putc(b, '\n');
             free(ids);
@@ -925,6 +1040,9 @@ static int run_mem_eff(void)
     free(rcnt);
     free(uref);
     free(qcnt);
+    free(qab);
+    free(cov.rec);
+    cov_db_free(&cov);
     kssd_sketch_free(ref);
     kssd_sketch_free(qry);
     return 0;
@@ -1344,9 +1462,23 @@ static int run_detail_scan(int kind)
     kssdgpu_index_t *ix = gpu_index_of_sketch(ref);
     const unsigned flags = kind == DETAIL_HASH ? ((o->ignoreconflict && ref_conflict) ? KSSDGPU_IGNORECONFLICT : 0)
                                                : (o->ignoreconflict ? KSSDGPU_IGNORECONFLICT : 0);
+    /* --estimate-coverage: the streaming paths fill the columns (src/command_ani.c:2519,
+     * 2641,2822,2989); the no-index hash path prints them as not computed */
+    cov_db_t cov = {0};
+    uint32_t *qab = NULL;
+    if (o->estimate_coverage) {
+        if (qry->stat.koc)
+            qab = cov_query_counts(qry, g.qrydir, true);
+        if (kind != DETAIL_HASH)
+            cov_db_load(&cov, g.refdir, (uint64_t)(ref->offs[R] - ref->offs[0]), NULL);
+    }
     FILE *out = open_out(g.outf);
     kssd_buf_t h = {0};
     kssd_buf_puts(&h, kssd_detail_header);
+    if (o->estimate_coverage) {
+        kssd_buf_putc(&h, '\t');
+        kssd_buf_puts(&h, kssd_coverage_header);
+    }
     kssd_buf_putc(&h, '\n');
     write_buf(out, &h);
     kssd_buf_free(&h);
@@ -1406,6 +1538,12 @@ static int run_detail_scan(int kind)
             size_t out_n = ns;
             if (kind != DETAIL_HASH && o->ntop > 0 && (size_t)o->ntop < out_n)
                 out_n = (size_t)o->ntop;
+            if (o->estimate_coverage && kind != DETAIL_HASH && out_n) {
+                const size_t qb = (size_t)(qry->offs[q] - qry->offs[0]);
+                kssd_coverage_rows(qry->keys + qb, qab ? qab + qb : NULL, (size_t)(qry->offs[q + 1] - qry->offs[q]),
+                                   ref->keys, ref->offs, cov.db.available ? &cov.db : NULL, qry->obj_bits, surv,
+                                   out_n);
+            }
             for (size_t k = 0; k < out_n; ++k)
                 kssd_append_detail_row(&rows[i], o, qry->names[q], ref->names[surv[k].rn], &surv[k],
                                        anno_at(ref, surv[k].rn));
@@ -1420,6 +1558,8 @@ static int run_detail_scan(int kind)
     }
     close_out(out);
     kssdgpu_index_free(ix);
+    free(qab);
+    cov_db_free(&cov);
     if (rtotal != rcnt)
         free(rtotal);
     free(qcnt);
@@ -1538,13 +1678,12 @@ static int cmd_ani(int argc, char **argv)
     g.sketch_kmerocrs = 1;
     argp_parse(&k_argp, argc, argv, ARGP_IN_ORDER, NULL, NULL);
     g.o.unique_ctx = g.unique_ctx;
+    g.o.estimate_coverage = g.estimate_coverage;
     if (g.o.p < 1)
         g.o.p = 1;
     if (g.reflist[0] || g.qrylist[0] || g.pair)
         errx(EXIT_FAILURE, "FASTA/FASTQ and list inputs need the sketcher, which this build does not include; "
                            "sketch with `kssd3a sketch` first");
-    if (g.estimate_coverage)
-        errx(EXIT_FAILURE, "--estimate-coverage is not supported by this build");
     if (!is_sketch_dir(g.qrydir))
         errx(EXIT_FAILURE, "%s is not a sketch directory; FASTA/FASTQ inputs need the sketcher, which this build "
                            "does not include", g.qrydir);

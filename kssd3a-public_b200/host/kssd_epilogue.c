@@ -532,6 +532,40 @@ static double bounded_af(double v)
     return v < 0.0 ? 0.0 : (v > 1.0 ? 1.0 : v);
 }
 
+/* append_coverage_double / coverage_estimator_label and the coverage columns of
+ * print_unified_detail_row (src/command_ani.c:1106-1126,1403-1429) */
+static void coverage_double(kssd_buf_t *b, double v)
+{
+    if (!isfinite(v))
+        kssd_buf_puts(b, "NA");
+    else if (fabs(v) >= 1000.0)
+        kssd_buf_printf(b, "%.3f", v);
+    else
+        kssd_buf_printf(b, "%.6g", v);
+}
+
+static void append_coverage(kssd_buf_t *b, const kssd_row_t *r)
+{
+    const char *label = r->coverage_status == 0   ? "NA:not_computed"
+                        : r->coverage_status == 2 ? "NA:query_missing_comblco.a"
+                        : r->coverage_status == 3 ? "NA:ref_read_error"
+                        : r->coverage_status == 4 ? "refdb_unique_ctxobj_bitset"
+                                                  : "reported_unique_ctxobj_sum";
+    if (r->coverage_status != 1 && r->coverage_status != 4) {
+        kssd_buf_printf(b, "\t%s\tNA\tNA\tNA\tNA\tNA\tNA\tNA\tNA\tNA\tNA\tNA", label);
+        return;
+    }
+    kssd_buf_printf(b, "\t%s\t%u\t%u\t", label, r->cov_ref_markers, r->cov_observed_markers);
+    const double v[8] = {r->cov_observed_fraction, r->cov_count_sum, r->est_depth, r->pos_mean_depth,
+                         r->pos_median_depth, r->count_cv, r->est_mass, r->est_fraction};
+    for (int i = 0; i < 8; ++i) {
+        if (i)
+            kssd_buf_putc(b, '\t');
+        coverage_double(b, v[i]);
+    }
+    kssd_buf_printf(b, "\t%s", r->coverage_status == 4 ? "refdb" : "reported_rows");
+}
+
 void kssd_append_detail_row(kssd_buf_t *b, const kssd_ani_opt_t *o, const char *qry_name, const char *ref_name,
                             const kssd_row_t *r, const char *annotation)
 {
@@ -551,10 +585,13 @@ void kssd_append_detail_row(kssd_buf_t *b, const kssd_ani_opt_t *o, const char *
     else
         conf = "raw";
     const char *anno = annotation && annotation[0] ? annotation : "NA";
-    kssd_buf_printf(b, "%s\t%s\t%lf\t%lf\t%s\t%s\t%d\t%f\t%f\t%f\t%f\t%d\t%d\t%d\t%s\n", qry_name, ref_name,
+    kssd_buf_printf(b, "%s\t%s\t%lf\t%lf\t%s\t%s\t%d\t%f\t%f\t%f\t%f\t%d\t%d\t%d\t%s", qry_name, ref_name,
                     r->selected_ani, r->metric, conf, name, r->XnY_ctx, r->af_qry, bounded_af(r->blastn_af_qry),
                     r->af_ref, bounded_af(r->blastn_af_ref), r->N_diff_obj, r->N_diff_obj_section, r->N_mut2_ctx,
                     anno);
+    if (o->estimate_coverage)
+        append_coverage(b, r);
+    kssd_buf_putc(b, '\n');
 }
 
 int32_t kssd_scale_fixed6(double value)

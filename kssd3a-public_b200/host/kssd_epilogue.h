@@ -51,6 +51,7 @@ typedef struct kssd_ani_opt {
     bool afcut_set;
     float anicut;
     bool unique_ctx;
+    bool estimate_coverage; /* --estimate-coverage: coverage columns on detail rows */
     /* sketch-derived globals of the reference (Bitslen, ani_model_drfold) */
     int obj_bits;
     int ctx_bits;
@@ -66,7 +67,33 @@ typedef struct kssd_row {
     bool unique_ctx_selected;
     double af_qry, blastn_af_qry, af_ref, blastn_af_ref;
     int XnY_ctx, N_diff_obj, N_diff_obj_section, N_mut2_ctx;
+    /* --estimate-coverage (src/command_ani.c:1071-1084): status 0 not computed, 1 markers
+     * unique among the reported rows, 2 query abundances missing, 4 reference-db unique bits */
+    unsigned char coverage_status;
+    uint32_t cov_ref_markers, cov_observed_markers;
+    double cov_observed_fraction, cov_count_sum, est_depth, pos_mean_depth, pos_median_depth, count_cv;
+    double est_mass, est_fraction;
 } kssd_row_t;
+
+/* Reference-database marker bits for coverage: the index records and their
+ * unique-object bitset (sortedcomb_ctxgid64obj32 + .unique_bits) */
+typedef struct kssd_cov_refdb {
+    bool available;
+    uint64_t entries;
+    const uint8_t *bits;
+    const kssd_index_rec_t *sorted;
+} kssd_cov_refdb_t;
+
+/* populate_selected_coverage_for_query_arrays (src/command_ani.c:2315-2455): coverage of
+ * the reported rows of one query from its abundances (q_keys sorted, q_counts parallel;
+ * NULL: abundances missing) and each row's reference keys (ref_keys at absolute
+ * ref_offs[rn] - ref_offs[0]); markers are reference keys unique in the reference db
+ * (refdb available) or among the rows' references. */
+void kssd_coverage_rows(const uint64_t *q_keys, const uint32_t *q_counts, size_t q_n, const uint64_t *ref_keys,
+                        const uint64_t *ref_offs, const kssd_cov_refdb_t *refdb, int obj_bits, kssd_row_t *rows,
+                        size_t n_rows);
+
+extern const char kssd_coverage_header[];
 
 void kssd_opt_defaults(kssd_ani_opt_t *o);
 

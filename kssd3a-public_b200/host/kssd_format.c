@@ -275,3 +275,28 @@ int kssd_index_write(const char *dir, const kssd_index_rec_t *recs, size_t n,
         return -1;
     return 0;
 }
+
+uint32_t *kssd_abundance_load(const char *dir, size_t *n_out)
+{
+    size_t sz = 0;
+    uint32_t *a = read_all(dir, "comblco.a", &sz);
+    if (!a)
+        return NULL;
+    *n_out = sz / sizeof(uint32_t);
+    if (sz % sizeof(uint32_t)) {
+        free(a);
+        set_err("%s/comblco.a size %zu is not a multiple of 4", dir, sz);
+        return NULL;
+    }
+    return a;
+}
+
+uint8_t *kssd_unique_bits_load(const char *dir, size_t *bytes_out)
+{
+    size_t sz = 0;
+    uint8_t *b = read_all(dir, "sortedcomb_ctxgid64obj32.unique_bits", &sz);
+    if (!b)
+        return NULL;
+    *bytes_out = sz;
+    return b;
+}

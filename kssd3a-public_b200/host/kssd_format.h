@@ -74,6 +74,10 @@ const char *kssd_host_last_error(void);
 /* Loads a sketch directory.  flags: 1 = annotations, 2 = infile meta.
  * Returns NULL on error (message via kssd_host_last_error). */
 kssd_sketch_t *kssd_sketch_load(const char *dir, unsigned flags);
+/* comblco.a: per-key k-mer counts of a sketch made with counting (stat.koc) */
+uint32_t *kssd_abundance_load(const char *dir, size_t *n_out);
+/* sortedcomb_ctxgid64obj32.unique_bits: one bit per index record */
+uint8_t *kssd_unique_bits_load(const char *dir, size_t *bytes_out);
 void kssd_sketch_free(kssd_sketch_t *s);
 int kssd_sketch_write(const char *dir, const kssd_sketch_stat_t *stat, int n,
                       const char (*names)[KSSD_PATHLEN], const uint64_t *keys,

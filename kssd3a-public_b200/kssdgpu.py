@@ -217,13 +217,15 @@ DEFAULT_HASH_ID = 1772583717  # the reference sketcher's id for its default code
 
 
 def write_sketch_dir(path: str, sk: Sketch, coden_len: int = 11, klen: int = 32, drfold: int = 8,
-                     hash_id: int = DEFAULT_HASH_ID, with_index: bool = False, meta: np.ndarray | None = None):
+                     hash_id: int = DEFAULT_HASH_ID, with_index: bool = False, meta: np.ndarray | None = None,
+                     abundance: np.ndarray | None = None):
     """Write a sketch directory in the reference layout (lcofiles.stat, comblco, comblco.index);
     with_index also writes sortedcomb_ctxgid64obj32 and its unique_bits; meta (META_DTYPE,
-    one record per sample) writes lcofiles.infilemeta."""
+    one record per sample) writes lcofiles.infilemeta; abundance (uint32 per key) writes
+    comblco.a and marks the sketch as made with k-mer counting (koc)."""
     os.makedirs(path, exist_ok=True)
     st = np.zeros(1, dtype=STAT_DTYPE)
-    st["hash_id"], st["koc"], st["conflict"] = hash_id, 0, int(sk.conflict)
+    st["hash_id"], st["koc"], st["conflict"] = hash_id, int(abundance is not None), int(sk.conflict)
     st["coden_len"], st["klen"], st["hclen"], st["holen"] = coden_len, klen, 0, 0
     st["drfold"], st["infile_num"] = drfold, sk.n
     names = b"".join(nm.encode()[:255].ljust(256, b"\0") for nm in sk.names)
@@ -231,6 +233,9 @@ def write_sketch_dir(path: str, sk: Sketch, coden_len: int = 11, klen: int = 32,
         f.write(st.tobytes() + names)
     sk.keys.astype("<u8").tofile(os.path.join(path, "comblco"))
     sk.offs.astype("<u8").tofile(os.path.join(path, "comblco.index"))
+    if abundance is not None:
+        assert len(abundance) == len(sk.keys)
+        abundance.astype("<u4").tofile(os.path.join(path, "comblco.a"))
     if meta is not None:
         assert meta.dtype == META_DTYPE and len(meta) == sk.n
         meta.tofile(os.path.join(path, "lcofiles.infilemeta"))

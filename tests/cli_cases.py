@@ -31,6 +31,10 @@ FIXTURES = {
     "qry50": dict(n_samples=50, n_clusters=5, role=kssdgpu.ROLE_OWNLEN, len_median=2e5, len_sigma=0.3,
                   len_min=1e5, len_max=6e5, size_dist=kssdgpu.SIZE_LOGNORMAL, own_len_min=5e4, own_len_max=4e5,
                   sub_lo=0.001, sub_hi=0.03, seed=21, sample_seed=24, name_prefix="many"),
+    "reads1": dict(n_samples=1, n_clusters=12, role=kssdgpu.ROLE_READS, len_median=3e5, len_sigma=0.3,
+                   len_min=1e5, len_max=8e5, size_dist=kssdgpu.SIZE_LOGNORMAL, sub_lo=0.001, sub_hi=0.06, seed=11,
+                   sample_seed=37, ref_sample_seed=11, ref_samples=120, cov_lo=10, cov_hi=30, err_lo=0.001,
+                   err_hi=0.003, name_prefix="single"),
     "reads6": dict(n_samples=6, n_clusters=12, role=kssdgpu.ROLE_READS, len_median=3e5, len_sigma=0.3,
                    len_min=1e5, len_max=8e5, size_dist=kssdgpu.SIZE_LOGNORMAL, sub_lo=0.001, sub_hi=0.06, seed=11,
                    sample_seed=31, ref_sample_seed=11, ref_samples=120, cov_lo=5, cov_hi=20, err_lo=0.001,
@@ -38,6 +42,17 @@ FIXTURES = {
 }
 INDEXED = {"refs120i", "refs120im"}  # with sortedcomb_ctxgid64obj32 written up front
 WITH_META = {"refs120im", "refs40m"}  # with lcofiles.infilemeta (per-sample input metadata)
+WITH_COUNTS = {"reads6a", "reads1a"}  # sketched with k-mer counts: comblco.a
+
+
+def synth_counts(sk, seed):
+    """Seeded per-key k-mer counts: a depth per sample, Poisson-like spread, some singletons."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    depth = np.repeat(rng.integers(3, 60, sk.n), np.diff(sk.offs).astype(np.int64))
+    counts = rng.poisson(depth).astype(np.uint32)
+    counts[rng.random(len(counts)) < 0.1] = 1
+    return np.maximum(counts, 1)
 
 
 def synth_meta(sk, seed):
@@ -117,6 +132,17 @@ CASES = [
     ("matrix_dedup_reads", ["matrix", "--format", "dedup-plan", "--cut", "0.5", "-m", "mash", "{reads6}"], {}),
     ("matrix_query_list", ["matrix", "-r", "{refs40}", "--query-sketch-list", "{list:qry8,qry1}", "-m", "ctx-moe"],
      {}),
+    # --estimate-coverage on read sets with k-mer counts: mem_eff with the reference
+    # database's marker bits, the multi-query stream (markers among reported rows), the
+    # one-query stream, and a query without counts
+    ("reads_coverage_memeff", ["ani", "-r", "{refs120i}", "--qraw", "{reads6a}", "-n", "0.8",
+                               "--estimate-coverage"], {}),
+    ("reads_coverage_stream_multi", ["ani", "-r", "{refs120}", "--qraw", "{reads6a}", "-n", "0.5", "-N", "5",
+                                     "--estimate-coverage"], {}),
+    ("reads_coverage_stream_one", ["ani", "-r", "{refs120i}", "--qraw", "{reads1a}", "-n", "0.5",
+                                   "--estimate-coverage"], {}),
+    ("reads_coverage_no_counts", ["ani", "-r", "{refs120i}", "--qraw", "{reads6}", "-n", "0.8",
+                                  "--estimate-coverage"], {}),
 ]
 
 
@@ -131,7 +157,8 @@ def make_fixture(root: str, name: str) -> str:
     spec = dict(FIXTURES[base])
     sk = kssdgpu.synth(**spec)
     meta = synth_meta(sk, len(name)) if name in WITH_META else None
-    kssdgpu.write_sketch_dir(path, sk, with_index=name in INDEXED, meta=meta)
+    counts = synth_counts(sk, len(name)) if name in WITH_COUNTS else None
+    kssdgpu.write_sketch_dir(path, sk, with_index=name in INDEXED, meta=meta, abundance=counts)
     return path
 
 
