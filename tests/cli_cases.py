@@ -40,7 +40,7 @@ FIXTURES = {
                    sample_seed=31, ref_sample_seed=11, ref_samples=120, cov_lo=5, cov_hi=20, err_lo=0.001,
                    err_hi=0.005, name_prefix="reads"),
 }
-INDEXED = {"refs120i", "refs120im"}  # with sortedcomb_ctxgid64obj32 written up front
+INDEXED = {"refs120i", "refs120im", "refs40i"}  # with sortedcomb_ctxgid64obj32 written up front
 WITH_META = {"refs120im", "refs40m"}  # with lcofiles.infilemeta (per-sample input metadata)
 WITH_COUNTS = {"reads6a", "reads1a"}  # sketched with k-mer counts: comblco.a
 
@@ -132,6 +132,19 @@ CASES = [
     ("matrix_dedup_reads", ["matrix", "--format", "dedup-plan", "--cut", "0.5", "-m", "mash", "{reads6}"], {}),
     ("matrix_query_list", ["matrix", "-r", "{refs40}", "--query-sketch-list", "{list:qry8,qry1}", "-m", "ctx-moe"],
      {}),
+    # the dispatcher's environment switches (src/command_ani_wrapper.c:1082-1230)
+    ("env_force_ref_index_one", ["ani", "-r", "{refs40i}", "-q", "{qry1}", "-n", "0.9"],
+     {"KSSD3A_FORCE_REF_INDEX": "1"}),
+    ("env_qraw_lookup_sorted", ["ani", "-r", "{refs120i}", "--qraw", "{reads1}", "-n", "0.5"],
+     {"KSSD3A_QRAW_LOOKUP": "sorted"}),
+    ("env_qraw_multi_legacy", ["ani", "-r", "{refs120i}", "--qraw", "{reads6}", "-n", "0.5", "-N", "4"],
+     {"KSSD3A_QRAW_MULTI": "legacy"}),
+    ("env_qraw_multi_sortedindex", ["ani", "-r", "{refs120i}", "--qraw", "{reads6}", "-n", "0.5", "-N", "4"],
+     {"KSSD3A_QRAW_MULTI": "sortedindex"}),
+    ("env_multi_threshold", ["ani", "-r", "{refs40}", "-q", "{qry8}", "-n", "0.9"],
+     {"KSSD3A_QRAW_MULTI_THRESHOLD": "3"}),
+    ("env_no_auto_index", ["ani", "-r", "{refs120}", "-q", "{qry30}", "-n", "0.9"],
+     {"KSSD3A_AUTO_REF_INDEX_THRESHOLD": "0"}),
     # --estimate-coverage on read sets with k-mer counts: mem_eff with the reference
     # database's marker bits, the multi-query stream (markers among reported rows), the
     # one-query stream, and a query without counts

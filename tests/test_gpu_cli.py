@@ -18,7 +18,7 @@ GOLDEN = os.path.join(ROOT, "tests", "golden", "cli")
 
 def _run(binary, argv, env_extra):
     env = dict(os.environ, OMP_NUM_THREADS="4")
-    for k in ("KSSD3A_FORCE_REF_INDEX", "KSSD3A_ANI_MATRIX_DIRECT_THRESHOLD", "KSSD3A_ANI_M1_DIRECT_THRESHOLD"):
+    for k in [k for k in env if k.startswith("KSSD3A_")]:
         env.pop(k, None)
     env.update({k: v for k, v in env_extra.items() if not k.startswith("_")})
     return subprocess.run([binary, *with_threads(argv)], capture_output=True, env=env, timeout=600)
