@@ -120,6 +120,23 @@ def measured_peak_hbm():
         return 6650.0, "fallback"
 
 
+def max_over_ranks(dist, x, device):
+    """The largest of x over all ranks (x itself without a process group): every
+    rank's timed region ends with the slowest one."""
+    if dist is None:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(world, units, seconds):
+    """Whole-job throughput of `world` replicas that each processed `units` in at
+    most `seconds` (weak scaling: per-GPU work fixed)."""
+    return world * units / seconds
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return 0
@@ -267,12 +284,9 @@ def run_ours(args, rank, world, local_rank):
         torch.cuda.synchronize()
         if dist:
             dist.barrier()
-    if dist:
-        t = torch.tensor([ms_step], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_step = float(t.item())
+    ms_step = max_over_ranks(dist, ms_step, dev)
     launches_timed = launches_per_step * args.steps
-    value = world * n * n / (ms_step / 1e3)
+    value = replica_value(world, n * n, ms_step / 1e3)
 
     # ---- dominant kernel alone (join kernels, counters zeroed outside the events)
     zero = lambda: (d_lc.zero_(), d_lo.zero_())  # noqa: E731
@@ -325,11 +339,8 @@ def run_ours(args, rank, world, local_rank):
         e2e_call()
         e2e_times.append(time.perf_counter() - t0)
     e2e_s = float(np.median(e2e_times))
-    if dist:
-        t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e_value = world * n * n / e2e_s
+    e2e_s = max_over_ranks(dist, e2e_s, dev)
+    e2e_value = replica_value(world, n * n, e2e_s)
     h2d = int(sk.keys.nbytes + sk.offs.nbytes + 4 * n)
     d2h = int(n * n * 16)
     # the e2e counters equal the device-resident ones
