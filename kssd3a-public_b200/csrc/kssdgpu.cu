@@ -750,16 +750,43 @@ __global__ void k_set_chunks(const uint32_t *__restrict__ cheads, const uint32_t
     }
 }
 
-// chunks in sorted order, with their pair counts
+// Small groups of at most kFlatMax genomes can be joined flat (one thread per group)
+// instead of as (chunk, pair) items; the plan chooses the largest flat size.
+constexpr uint32_t kFlatMax = 4;
+
+// chunks in sorted order, with their pair counts (none for chunks of flat-joined sizes)
 __global__ void k_set_permute(const uint32_t *__restrict__ order, uint32_t nchunks, const ulonglong2 *__restrict__ in,
-                              ulonglong2 *__restrict__ out, uint32_t *__restrict__ npairs)
+                              ulonglong2 *__restrict__ out, uint32_t *__restrict__ npairs, uint32_t flat_max)
 {
     for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < nchunks; c += gridDim.x * blockDim.x) {
         const ulonglong2 ch = in[order[c]];
         const uint32_t k = (uint32_t)(ch.y >> 32);
         out[c] = ch;
-        npairs[c] = k * (k - 1) / 2;
+        npairs[c] = k <= flat_max ? 0 : k * (k - 1) / 2;
     }
+}
+
+// first sorted small group of every size 2..flat_max (the groups are sorted by size,
+// largest first, so each size is one contiguous class and the smallest is the tail)
+__global__ void k_flat_firsts(const unsigned long long *__restrict__ desc, uint32_t n, uint32_t flat_max,
+                              uint32_t *__restrict__ firsts)
+{
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        const uint32_t k = (uint32_t)(desc[t] >> 32);
+        if (k <= flat_max && (t == 0 || (uint32_t)(desc[t - 1] >> 32) != k))
+            firsts[k] = t;
+    }
+}
+
+// run heads of one flat class, one 32-bit word per 32 groups (bit = lane)
+__global__ void k_flat_heads(const uint32_t *__restrict__ heads, uint32_t first, uint32_t cnt, uint32_t *__restrict__ out)
+{
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if ((t & ~31u) >= cnt)
+        return;  // whole warps only
+    const uint32_t b = __ballot_sync(0xFFFFFFFFu, t < cnt && heads[first + t]);
+    if ((t & 31) == 0)
+        out[t >> 5] = b;
 }
 
 // Self-contained join items: offset of the chunk's first group in the compact
@@ -772,13 +799,16 @@ __host__ __device__ __forceinline__ unsigned long long set_item(uint64_t off, ui
 }
 constexpr uint64_t kSetItemMaxOffset = 1ull << 34;
 
-// items[item_off[c] + p] for the chunk's pairs (i < j)
+// items[item_off[c] + p] for the chunk's pairs (i < j); chunks of flat-joined sizes
+// have none
 __global__ void k_set_items(const ulonglong2 *__restrict__ chunks, const uint32_t *__restrict__ item_off, uint32_t nchunks,
-                            unsigned long long *__restrict__ items)
+                            uint32_t flat_max, unsigned long long *__restrict__ items)
 {
     for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < nchunks; c += gridDim.x * blockDim.x) {
         const ulonglong2 ch = chunks[c];
         const uint32_t m = (uint32_t)ch.y, k = (uint32_t)(ch.y >> 32);
+        if (k <= flat_max)
+            continue;
         uint32_t o = item_off[c];
         for (uint32_t j = 1; j < k; ++j)
             for (uint32_t i = 0; i < j; ++i)
@@ -798,11 +828,10 @@ __global__ void k_set_items(const ulonglong2 *__restrict__ chunks, const uint32_
 #define KSSD_SET_MINB 1
 #endif
 constexpr int kSetUnroll = KSSD_SET_UNROLL;
-__global__ void __launch_bounds__(256, KSSD_SET_MINB) k_self_sets(const unsigned long long *__restrict__ items, uint32_t nitems,
-                                                   const uint64_t *__restrict__ jp, unsigned long long *__restrict__ oc,
-                                                   unsigned long long *__restrict__ oo)
+__device__ __forceinline__ void self_set_item(uint32_t t, const unsigned long long *__restrict__ items, uint32_t nitems,
+                                              const uint64_t *__restrict__ jp, unsigned long long *__restrict__ oc,
+                                              unsigned long long *__restrict__ oo)
 {
-    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= nitems)
         return;
     const unsigned long long it = __ldg(items + t);
@@ -829,6 +858,100 @@ __global__ void __launch_bounds__(256, KSSD_SET_MINB) k_self_sets(const unsigned
     atomicAdd(oc + cell, (unsigned long long)m | ((unsigned long long)mut2 << 32));
     if (dobj)
         atomicAdd(oo + cell, (unsigned long long)dobj | ((unsigned long long)sect << 32));
+}
+
+// Flat join of one size class: one thread per group of K genomes, lanes on
+// consecutive groups (a warp reads 32 x K postings, contiguous).  Groups of one run
+// share their K(K-1)/2 counter cells; per pair, a warp sums each run's increments by
+// a segmented reduction toward the run's first lane (run heads from the plan, bit =
+// lane) and that lane adds them with one atomic per counter word.  Threads of a warp
+// exit together (the shuffles span the full warp).
+template <int K>
+__device__ __forceinline__ void self_flat_group(uint32_t t, const uint64_t *__restrict__ pk, uint32_t nk,
+                                                const uint32_t *__restrict__ hk, unsigned long long *__restrict__ oc,
+                                                unsigned long long *__restrict__ oo)
+{
+    const uint32_t lane = t & 31, base = t - lane;
+    if (base >= nk)
+        return;
+    const uint32_t nv = min(nk - base, 32u);
+    const bool act = lane < nv;
+    uint64_t p[K];
+#pragma unroll
+    for (int x = 0; x < K; ++x)
+        p[x] = act ? __ldg(pk + (size_t)K * t + x) : 0;
+    // segments: the plan's run heads, lane 0, and every inactive lane on its own
+    const uint32_t valid = nv == 32 ? 0xFFFFFFFFu : (1u << nv) - 1;
+    const uint32_t heads = __ldg(hk + (t >> 5)) | 1u | ~valid;
+    const uint32_t above = lane == 31 ? 0u : heads & (0xFFFFFFFFu << (lane + 1));
+    const uint32_t end = above ? (uint32_t)__ffs(above) - 1 : 32u;
+    const bool lead = act && ((heads >> lane) & 1u);
+    const uint32_t m = end - lane;
+#pragma unroll
+    for (int j = 1; j < K; ++j) {
+#pragma unroll
+        for (int i = 0; i < j; ++i) {
+            const uint32_t d = (uint32_t)min(kMinInit, dna_pop((uint32_t)p[i] ^ (uint32_t)p[j]));
+            // sect (9 bits: at most 32 x 12) | dobj << 9 (6 bits) | mut2 << 15 (6 bits)
+            uint32_t v = act ? d | (uint32_t)(d > 0) << 9 | (uint32_t)(d > 1) << 15 : 0;
+#pragma unroll
+            for (uint32_t off = 1; off < 32; off <<= 1) {
+                const uint32_t x = __shfl_down_sync(0xFFFFFFFFu, v, off);
+                if (lane + off < end)
+                    v += x;
+            }
+            if (lead) {
+                const uint32_t sect = v & 511u, dobj = (v >> 9) & 63u, mut2 = v >> 15;
+                const size_t cell = lower_cell((uint32_t)(p[j] >> 32), (uint32_t)(p[i] >> 32));
+                atomicAdd(oc + cell, (unsigned long long)m | ((unsigned long long)mut2 << 32));
+                if (dobj)
+                    atomicAdd(oo + cell, (unsigned long long)dobj | ((unsigned long long)sect << 32));
+            }
+        }
+    }
+}
+
+// Flat classes of one join launch: class k (2..kFlatMax) has n[k] groups whose
+// postings start at off[k] in the compact postings, run-head words from hoff[k],
+// and blocks [block0[k], block0[k] + nblocks[k]) of the launch.
+struct FlatClasses {
+    uint32_t n[kFlatMax + 1];
+    uint64_t off[kFlatMax + 1];
+    uint32_t hoff[kFlatMax + 1];
+    uint32_t block0[kFlatMax + 1];
+    uint32_t nblocks[kFlatMax + 1];
+};
+
+template <int K>
+__device__ __forceinline__ bool flat_class_block(const FlatClasses &fc, const uint64_t *__restrict__ jp,
+                                                 const uint32_t *__restrict__ fheads,
+                                                 unsigned long long *__restrict__ oc, unsigned long long *__restrict__ oo)
+{
+    const uint32_t b = blockIdx.x - fc.block0[K];
+    if (b >= fc.nblocks[K])
+        return false;
+    self_flat_group<K>(b * blockDim.x + threadIdx.x, jp + fc.off[K], fc.n[K], fheads + fc.hoff[K], oc, oo);
+    return true;
+}
+
+// The join launch: the first set_blocks blocks run the (chunk, pair) items, the rest
+// the flat classes (largest size first), so that the latter fill the former's tail.
+__global__ void __launch_bounds__(256, KSSD_SET_MINB) k_self_sets(const unsigned long long *__restrict__ items, uint32_t nitems,
+                                                   uint32_t set_blocks, const uint64_t *__restrict__ jp,
+                                                   const FlatClasses fc, const uint32_t *__restrict__ fheads,
+                                                   unsigned long long *__restrict__ oc,
+                                                   unsigned long long *__restrict__ oo)
+{
+    if (blockIdx.x < set_blocks) {
+        self_set_item(blockIdx.x * blockDim.x + threadIdx.x, items, nitems, jp, oc, oo);
+        return;
+    }
+    static_assert(kFlatMax == 4, "one dispatch per flat class");
+    if (flat_class_block<4>(fc, jp, fheads, oc, oo))
+        return;
+    if (flat_class_block<3>(fc, jp, fheads, oc, oo))
+        return;
+    flat_class_block<2>(fc, jp, fheads, oc, oo);
 }
 
 // One warp per big group: lanes stride over its k(k-1)/2 pairs.
@@ -1021,6 +1144,9 @@ struct kssdgpu_index {
     uint32_t j_nchunks = 0, j_nitems = 0;
     uint32_t j_chunk_size = 32;             // groups per set-major chunk (1..255)
     bool j_sort_chunks = true;              // chunks ordered by group count, largest first
+    uint32_t j_flat_max = 2;                // small groups of up to this many genomes joined flat (1: none)
+    FlatClasses j_flat{};                   // the flat classes of the plan
+    DevBuf<uint32_t> j_fheads;              // their run heads, one word per 32 groups
     bool j_tuned = false;                   // the autotuner ran for this index
     int j_tune_tried = 0;                   // autotuner candidates timed (0: defaults kept)
     float j_tune_ms = 0;                    // the chosen candidate's join time
@@ -1439,7 +1565,8 @@ int count_host_impl(kssdgpu_index *ix, const uint64_t *qkeys, const uint64_t *qo
 // Runs of equal gid lists among the n sorted small groups -> chunks -> (chunk, pair)
 // items (j_chunks, j_items); the per-group descriptors are released afterwards.
 // Plan knobs, overridable for tuning: KSSDGPU_JOIN_CHUNK (groups per chunk, 1..255)
-// and KSSDGPU_JOIN_SORT (0: chunks in plan order).
+// , KSSDGPU_JOIN_SORT (0: chunks in plan order) and KSSDGPU_JOIN_FLAT (largest group
+// size joined flat, 1..4; 1: every small group as chunk items).
 uint32_t env_u32(const char *name, uint32_t def, uint32_t lo, uint32_t hi)
 {
     const char *v = std::getenv(name);
@@ -1449,22 +1576,45 @@ uint32_t env_u32(const char *name, uint32_t def, uint32_t lo, uint32_t hi)
     return x < lo ? lo : x > hi ? hi : (uint32_t)x;
 }
 
+// One launch of the set-major join: the plan's (chunk, pair) items, then its flat
+// classes, largest size first.
+cudaError_t launch_sets(kssdgpu_index *ix, unsigned long long *oc, unsigned long long *oo, cudaStream_t st)
+{
+    FlatClasses fc = ix->j_flat;
+    const uint32_t sb = (ix->j_nitems + 255) / 256;
+    uint32_t nb = sb;
+    for (uint32_t k = kFlatMax; k >= 2; --k) {
+        fc.block0[k] = nb;
+        fc.nblocks[k] = (fc.n[k] + 255) / 256;
+        nb += fc.nblocks[k];
+    }
+    if (!nb)
+        return cudaSuccess;
+    k_self_sets<<<nb, 256, 0, st>>>(ix->j_items.p, ix->j_nitems, sb, ix->j_post.p, fc, ix->j_fheads.p, oc, oo);
+    count_launch();
+    return cudaGetLastError();
+}
+
 cudaError_t set_major_plan(kssdgpu_index *ix, uint32_t n, cudaStream_t st)
 {
     ix->j_chunk_size = env_u32("KSSDGPU_JOIN_CHUNK", ix->j_chunk_size, 1, 255);
     ix->j_sort_chunks = env_u32("KSSDGPU_JOIN_SORT", ix->j_sort_chunks ? 1 : 0, 0, 1) != 0;
+    ix->j_flat_max = env_u32("KSSDGPU_JOIN_FLAT", ix->j_flat_max, 1, kFlatMax);
+    const uint32_t flat_max = ix->j_flat_max;
     const uint32_t csize = ix->j_chunk_size;
     uint32_t *heads = nullptr, *runs = nullptr, *first = nullptr, *cheads = nullptr, *cpos = nullptr;
     uint32_t *skey = nullptr, *skey2 = nullptr, *sval = nullptr, *sval2 = nullptr, *npairs = nullptr, *ioff = nullptr;
+    uint32_t *f2d = nullptr;
     ulonglong2 *chunks0 = nullptr;
     void *tmp = nullptr;
     auto cleanup = [&]() {
         cudaFree(heads); cudaFree(runs); cudaFree(first); cudaFree(cheads); cudaFree(cpos);
         cudaFree(skey); cudaFree(skey2); cudaFree(sval); cudaFree(sval2); cudaFree(npairs); cudaFree(ioff);
-        cudaFree(chunks0); cudaFree(tmp);
+        cudaFree(f2d); cudaFree(chunks0); cudaFree(tmp);
     };
     size_t tb1 = 0, tb2 = 0, tb3 = 0;
     cudaError_t e = cudaMalloc(&heads, (size_t)n * 4);
+    if (e == cudaSuccess) e = cudaMalloc(&f2d, (kFlatMax + 1) * 4);
     if (e == cudaSuccess) e = cudaMalloc(&runs, (size_t)n * 4);
     if (e == cudaSuccess) e = cudaMalloc(&first, (size_t)n * 4);
     if (e == cudaSuccess) e = cudaMalloc(&cheads, (size_t)n * 4);
@@ -1496,6 +1646,39 @@ cudaError_t set_major_plan(kssdgpu_index *ix, uint32_t n, cudaStream_t st)
         e = cub::DeviceScan::ExclusiveSum(tmp, b, cheads, cpos, n, st);
         count_launch(2);
     }
+    // flat classes 2..flat_max: where each starts, its first posting, its run heads
+    uint32_t fk[kFlatMax + 1];
+    unsigned long long dk[kFlatMax + 1] = {};
+    FlatClasses fc{};
+    if (e == cudaSuccess && flat_max >= 2) {
+        e = cudaMemsetAsync(f2d, 0xFF, sizeof fk, st);
+        if (e == cudaSuccess) {
+            k_flat_firsts<<<grid_for(n), 256, 0, st>>>(ix->j_small.p, n, flat_max, f2d);
+            count_launch();
+            e = cudaMemcpyAsync(fk, f2d, sizeof fk, cudaMemcpyDeviceToHost, st);
+        }
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        uint32_t words = 0;
+        for (uint32_t k = 2; e == cudaSuccess && k <= flat_max; ++k) {
+            if (fk[k] >= n)
+                continue;
+            uint32_t end = n;  // the class ends where the next smaller present class starts
+            for (uint32_t k2 = 2; k2 < k; ++k2)
+                if (fk[k2] < n)
+                    end = std::min(end, fk[k2]);
+            fc.n[k] = end - fk[k];
+            fc.hoff[k] = words;
+            words += (fc.n[k] + 31) / 32;
+            e = cudaMemcpyAsync(dk + k, ix->j_small.p + fk[k], 8, cudaMemcpyDeviceToHost, st);
+        }
+        if (e == cudaSuccess && words) e = ix->j_fheads.ensure(words);
+        for (uint32_t k = 2; e == cudaSuccess && k <= flat_max; ++k) {
+            if (!fc.n[k])
+                continue;
+            k_flat_heads<<<(fc.n[k] + 255) / 256, 256, 0, st>>>(heads, fk[k], fc.n[k], ix->j_fheads.p + fc.hoff[k]);
+            count_launch();
+        }
+    }
     uint32_t last_pos = 0, last_head = 0;
     if (e == cudaSuccess) e = cudaMemcpyAsync(&last_pos, cpos + n - 1, 4, cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(&last_head, cheads + n - 1, 4, cudaMemcpyDeviceToHost, st);
@@ -1513,7 +1696,8 @@ cudaError_t set_major_plan(kssdgpu_index *ix, uint32_t n, cudaStream_t st)
             order = sval2;
         }
         if (e == cudaSuccess) {
-            k_set_permute<<<grid_for(nchunks), 256, 0, st>>>(order, nchunks, chunks0, ix->j_chunks.p, npairs);
+            k_set_permute<<<grid_for(nchunks), 256, 0, st>>>(order, nchunks, chunks0, ix->j_chunks.p, npairs,
+                                                             flat_max);
             count_launch();
             size_t b = tb;
             e = cub::DeviceScan::ExclusiveSum(tmp, b, npairs, ioff, nchunks, st);
@@ -1529,7 +1713,7 @@ cudaError_t set_major_plan(kssdgpu_index *ix, uint32_t n, cudaStream_t st)
         e = cudaErrorMemoryAllocation;  // more join items than one 32-bit launch index covers
     if (e == cudaSuccess) e = ix->j_items.ensure(nitems);
     if (e == cudaSuccess) {
-        k_set_items<<<grid_for(nchunks), 256, 0, st>>>(ix->j_chunks.p, ioff, nchunks, ix->j_items.p);
+        k_set_items<<<grid_for(nchunks), 256, 0, st>>>(ix->j_chunks.p, ioff, nchunks, flat_max, ix->j_items.p);
         count_launch();
         e = cudaStreamSynchronize(st);
     }
@@ -1537,60 +1721,61 @@ cudaError_t set_major_plan(kssdgpu_index *ix, uint32_t n, cudaStream_t st)
     if (e == cudaSuccess) {
         ix->j_nchunks = nchunks;
         ix->j_nitems = (uint32_t)nitems;
+        for (uint32_t k = 2; k <= kFlatMax; ++k)
+            fc.off[k] = (uint32_t)dk[k];
+        ix->j_flat = fc;
     }
     return e;
 }
 
-// Autotuner of the set-major join: every candidate (groups per chunk, chunk order)
-// is planned and timed on scratch counters (CUDA events, best of three after one
-// warm-up run; the scratch is zeroed once: accumulating into nonzero counters
+// Autotuner of the set-major join: candidate plans (largest flat group size, then
+// groups per chunk and chunk order at the best flat size) are built and timed on
+// scratch counters (CUDA events, best of three after one warm-up run, each run after
+// a write of twice the L2 size so that the postings come from HBM as in a one-shot
+// call; the scratch counters are zeroed once: accumulating into nonzero counters
 // costs the same); the fastest stays.  Runs once per index, on request
 // (kssdgpu_self_plan_tune) or at plan time with KSSDGPU_TUNE=1; keeps the defaults
-// when a knob is pinned by its environment variable or when the scratch counters
-// would take more than a quarter of the free device memory.
+// when a knob is pinned by its environment variable or when the scratch would take
+// more than a quarter of the free device memory.
 cudaError_t tune_join(kssdgpu_index *ix, uint32_t n, cudaStream_t st)
 {
     ix->j_tuned = true;
-    const bool pinned = std::getenv("KSSDGPU_JOIN_CHUNK") || std::getenv("KSSDGPU_JOIN_SORT");
+    const bool pinned = std::getenv("KSSDGPU_JOIN_CHUNK") || std::getenv("KSSDGPU_JOIN_SORT") ||
+                        std::getenv("KSSDGPU_JOIN_FLAT");
     if (pinned || n == 0)
         return n ? set_major_plan(ix, n, st) : cudaSuccess;
     const size_t cells = std::max<size_t>((size_t)ix->nref * (ix->nref - 1) / 2, 1);
+    int l2 = 0;
+    cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, ix->device);
+    const size_t flush_b = std::max<size_t>(2 * (size_t)std::max(l2, 0), 64u << 20);
     size_t free_b = 0, total_b = 0;
     cudaError_t e = cudaMemGetInfo(&free_b, &total_b);
-    if (e != cudaSuccess || cells * 16 > free_b / 4)
+    if (e != cudaSuccess || cells * 16 + flush_b > free_b / 4)
         return set_major_plan(ix, n, st);
     unsigned long long *oc = nullptr, *oo = nullptr;
+    void *flush = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     e = cudaMalloc(&oc, cells * 8);
     if (e == cudaSuccess) e = cudaMalloc(&oo, cells * 8);
+    if (e == cudaSuccess) e = cudaMalloc(&flush, flush_b);
     if (e == cudaSuccess) e = cudaEventCreate(&ev0);
     if (e == cudaSuccess) e = cudaEventCreate(&ev1);
-    // chunk order: largest first for every size; plan order once, at the default size
-    static const struct { uint32_t size; bool sorted; } kCands[] = {
-        {8, true}, {16, true}, {32, true}, {64, true}, {128, true}, {32, false}};
-    float best = 1e30f;
-    uint32_t best_size = ix->j_chunk_size;
-    bool best_sort = ix->j_sort_chunks;
-    int tried = 0;
     if (e == cudaSuccess) e = cudaMemsetAsync(oc, 0, cells * 8, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(oo, 0, cells * 8, st);
-    for (const auto &cand : kCands) {
-        if (e != cudaSuccess)
-            break;
-        const uint32_t cs = cand.size;
-        const int srt = cand.sorted ? 1 : 0;
+    float best = 1e30f;
+    uint32_t best_size = ix->j_chunk_size, best_flat = ix->j_flat_max;
+    bool best_sort = ix->j_sort_chunks;
+    int tried = 0;
+    auto time_plan = [&](uint32_t cs, bool srt, uint32_t flat) {
         ix->j_chunk_size = cs;
-        ix->j_sort_chunks = srt != 0;
+        ix->j_sort_chunks = srt;
+        ix->j_flat_max = flat;
         e = set_major_plan(ix, n, st);
         float t_min = 1e30f;
         for (int r = 0; r < 4 && e == cudaSuccess; ++r) {
-            e = cudaEventRecord(ev0, st);
-            if (e == cudaSuccess && ix->j_nitems) {
-                k_self_sets<<<(ix->j_nitems + 255) / 256, 256, 0, st>>>(ix->j_items.p, ix->j_nitems, ix->j_post.p,
-                                                                        oc, oo);
-                count_launch();
-                e = cudaGetLastError();
-            }
+            e = cudaMemsetAsync(flush, r, flush_b, st);
+            if (e == cudaSuccess) e = cudaEventRecord(ev0, st);
+            if (e == cudaSuccess) e = launch_sets(ix, oc, oo, st);
             if (e == cudaSuccess) e = cudaEventRecord(ev1, st);
             if (e == cudaSuccess) e = cudaEventSynchronize(ev1);
             float ms = 0;
@@ -1599,22 +1784,35 @@ cudaError_t tune_join(kssdgpu_index *ix, uint32_t n, cudaStream_t st)
                 t_min = std::min(t_min, ms);
         }
         if (e != cudaSuccess)
-            break;
+            return;
         ++tried;
         if (t_min < best) {
             best = t_min;
             best_size = cs;
-            best_sort = srt != 0;
+            best_sort = srt;
+            best_flat = flat;
         }
-    }
+    };
+    // the flat size at 32 groups per chunk, largest chunks first; then the chunk
+    // size (largest first) and the plan order at the best flat size
+    for (uint32_t flat = kFlatMax; flat >= 1 && e == cudaSuccess; --flat)
+        time_plan(32, true, flat);
+    static const struct { uint32_t size; bool sorted; } kChunkCands[] = {
+        {8, true}, {16, true}, {64, true}, {128, true}, {32, false}};
+    const uint32_t flat_at = best_flat;
+    for (const auto &cand : kChunkCands)
+        if (e == cudaSuccess)
+            time_plan(cand.size, cand.sorted, flat_at);
     cudaFree(oc);
     cudaFree(oo);
+    cudaFree(flush);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (e != cudaSuccess)
         return e;
     ix->j_chunk_size = best_size;
     ix->j_sort_chunks = best_sort;
+    ix->j_flat_max = best_flat;
     ix->j_tune_tried = tried;
     ix->j_tune_ms = best;
     return set_major_plan(ix, n, st);
@@ -1722,11 +1920,7 @@ int self_lower_dev_impl(kssdgpu_index *ix, unsigned flags, unsigned long long *o
             CUDA_TRY(cudaMemsetAsync(oo, 0, words * 8, st));
         }
     }
-    if (ix->j_nitems) {
-        k_self_sets<<<(ix->j_nitems + 255) / 256, 256, 0, st>>>(ix->j_items.p, ix->j_nitems, ix->j_post.p, oc,
-                                                                oo);
-        count_launch();
-    }
+    CUDA_TRY(launch_sets(ix, oc, oo, st));
     if (ix->j_n[1]) {
         k_self_big<<<(unsigned)(((uint64_t)ix->j_n[1] * 32 + 255) / 256), 256, 0, st>>>(ix->j_big.p, ix->j_n[1], ix->post,
                                                                                        oc, oo);
@@ -1980,6 +2174,7 @@ void kssdgpu_index_free(kssdgpu_index_t *ix)
     ix->j_post.release();
     ix->j_chunks.release();
     ix->j_items.release();
+    ix->j_fheads.release();
     ix->j_big.release();
     ix->j_conf.release();
     delete ix;
@@ -2267,7 +2462,8 @@ int kssdgpu_self_plan_info(kssdgpu_index_t *ix, uint64_t *groups, uint64_t *post
     return KSSDGPU_OK;
 }
 
-int kssdgpu_self_plan_tune(kssdgpu_index_t *ix, uint32_t *chunk_groups, int *sorted, int *candidates, float *join_ms)
+int kssdgpu_self_plan_tune(kssdgpu_index_t *ix, uint32_t *chunk_groups, int *sorted, uint32_t *flat_groups,
+                           int *candidates, float *join_ms)
 {
     if (!ix)
         return fail(KSSDGPU_ERR_ARG, "null index");
@@ -2283,6 +2479,7 @@ int kssdgpu_self_plan_tune(kssdgpu_index_t *ix, uint32_t *chunk_groups, int *sor
     }
     if (chunk_groups) *chunk_groups = ix->j_chunk_size;
     if (sorted) *sorted = ix->j_sort_chunks ? 1 : 0;
+    if (flat_groups) *flat_groups = ix->j_flat_max;
     if (candidates) *candidates = ix->j_tune_tried;
     if (join_ms) *join_ms = ix->j_tune_ms;
     return KSSDGPU_OK;

@@ -72,7 +72,7 @@ def gpu_lib() -> C.CDLL:
                                            C.POINTER(_CountTuning)]
         lib.kssdgpu_self_lower.argtypes = [vp, C.c_uint, vp, vp]
         lib.kssdgpu_self_lower_dev.argtypes = [vp, C.c_uint, vp, vp, vp]
-        lib.kssdgpu_self_plan_tune.argtypes = [vp, C.POINTER(C.c_uint32), C.POINTER(C.c_int),
+        lib.kssdgpu_self_plan_tune.argtypes = [vp, C.POINTER(C.c_uint32), C.POINTER(C.c_int), C.POINTER(C.c_uint32),
                                                  C.POINTER(C.c_int), C.POINTER(C.c_float)]
         lib.kssdgpu_self_plan_info.argtypes = [vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
                                                C.POINTER(C.c_uint64)]
@@ -413,9 +413,11 @@ class Index:
 
     def self_plan_tune(self):
         """Autotune the self-join plan (once per index); returns the setting in use."""
-        c, so, n, ms = C.c_uint32(), C.c_int(), C.c_int(), C.c_float()
-        _check(gpu_lib().kssdgpu_self_plan_tune(self._h, C.byref(c), C.byref(so), C.byref(n), C.byref(ms)))
-        return dict(chunk_groups=c.value, sorted=bool(so.value), candidates=n.value, join_ms=ms.value)
+        c, so, f, n, ms = C.c_uint32(), C.c_int(), C.c_uint32(), C.c_int(), C.c_float()
+        _check(gpu_lib().kssdgpu_self_plan_tune(self._h, C.byref(c), C.byref(so), C.byref(f), C.byref(n),
+                                                C.byref(ms)))
+        return dict(chunk_groups=c.value, sorted=bool(so.value), flat_groups=f.value, candidates=n.value,
+                    join_ms=ms.value)
 
     def self_plan_info(self):
         g, p, q = C.c_uint64(), C.c_uint64(), C.c_uint64()

@@ -118,6 +118,46 @@ def test_synthetic_genomes_block_and_self():
     np.testing.assert_array_equal(got[1], want[1])
 
 
+def _clustered_sketch():
+    # tight clusters: many contexts shared by exactly 2..4 genomes, in runs of the same
+    # gid list that cross warp (32-group) boundaries and end in partial warps
+    return kssdgpu.synth(n_samples=120, n_clusters=30, len_median=3e5, len_min=1e5, len_max=1e6,
+                         size_dist=kssdgpu.SIZE_LOGNORMAL, sub_lo=0.001, sub_hi=0.05)
+
+
+@pytest.mark.parametrize("flat,chunk,srt", [(1, 32, 1), (2, 32, 1), (3, 32, 1), (4, 32, 1), (4, 1, 1), (4, 7, 0),
+                                            (2, 255, 1), (3, 16, 0)])
+def test_self_join_plan_settings(monkeypatch, flat, chunk, srt):
+    """Every plan setting (largest flat group size, groups per chunk, chunk order)
+    gives the oracle's self-join counters."""
+    monkeypatch.setenv("KSSDGPU_JOIN_FLAT", str(flat))
+    monkeypatch.setenv("KSSDGPU_JOIN_CHUNK", str(chunk))
+    monkeypatch.setenv("KSSDGPU_JOIN_SORT", str(srt))
+    sk = _clustered_sketch()
+    rec = oracle.build_index(sk.keys, sk.offs)
+    idx = kssdgpu.Index.from_records(rec, sk.n)
+    want = oracle.self_lower_all(rec, sk.keys, sk.offs)
+    got = idx.self_lower()
+    np.testing.assert_array_equal(got[0], want[0])
+    np.testing.assert_array_equal(got[1], want[1])
+    t = idx.self_plan_tune()  # pinned by the environment: defaults kept, nothing timed
+    assert (t["flat_groups"], t["chunk_groups"], t["sorted"], t["candidates"]) == (flat, chunk, bool(srt), 0)
+
+
+def test_self_join_autotuner_keeps_counts(monkeypatch):
+    for v in ("KSSDGPU_JOIN_FLAT", "KSSDGPU_JOIN_CHUNK", "KSSDGPU_JOIN_SORT"):
+        monkeypatch.delenv(v, raising=False)
+    sk = _clustered_sketch()
+    rec = oracle.build_index(sk.keys, sk.offs)
+    idx = kssdgpu.Index.from_records(rec, sk.n)
+    t = idx.self_plan_tune()
+    assert t["candidates"] == 9 and 1 <= t["flat_groups"] <= 4 and t["join_ms"] > 0
+    want = oracle.self_lower_all(rec, sk.keys, sk.offs)
+    got = idx.self_lower()
+    np.testing.assert_array_equal(got[0], want[0])
+    np.testing.assert_array_equal(got[1], want[1])
+
+
 def test_read_sets_with_conflicts():
     ref = kssdgpu.synth(n_samples=40, n_clusters=8, len_median=2e5, len_min=1e5, len_max=1e6)
     reads = kssdgpu.synth(n_samples=6, n_clusters=8, role=kssdgpu.ROLE_READS, sample_seed=5,
