@@ -668,9 +668,31 @@ __device__ __forceinline__ void join_pair(uint64_t pi, uint64_t pj, unsigned lon
 }
 
 // Zero two 16-byte aligned arrays of `words` 8-byte counters.
-__global__ void __launch_bounds__(256) k_zero_pair(unsigned long long *__restrict__ a, unsigned long long *__restrict__ b,
-                                                   size_t words)
+// Programmatic dependent launch of the self join after the zero fill: the fill lets
+// the join's grid launch at once, and the join waits for the fill's completion (and
+// its stores) only before its first atomic, so the join's loads overlap the fill.
+#ifndef KSSD_JOIN_PDL
+#define KSSD_JOIN_PDL 1
+#endif
+__device__ __forceinline__ void pdl_launch_dependents()
 {
+#if KSSD_JOIN_PDL
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+#endif
+}
+__device__ __forceinline__ void pdl_wait_primary()
+{
+#if KSSD_JOIN_PDL
+    asm volatile("griddepcontrol.wait;" ::: "memory");  // no-op without a programmatic dependency
+#endif
+}
+
+// One wave (8 blocks of 256 per SM, all resident at once), so that the dependent
+// join's blocks never take the slots of fill blocks still waiting to start.
+__global__ void __launch_bounds__(256, 8) k_zero_pair(unsigned long long *__restrict__ a, unsigned long long *__restrict__ b,
+                                                      size_t words)
+{
+    pdl_launch_dependents();
     const size_t n16 = words / 2;
     const size_t stride = (size_t)gridDim.x * blockDim.x;
     ulonglong2 *a2 = reinterpret_cast<ulonglong2 *>(a), *b2 = reinterpret_cast<ulonglong2 *>(b);
@@ -855,6 +877,7 @@ __device__ __forceinline__ void self_set_item(uint32_t t, const unsigned long lo
         sect += d;
     }
     const size_t cell = lower_cell(gj, gi);
+    pdl_wait_primary();
     atomicAdd(oc + cell, (unsigned long long)m | ((unsigned long long)mut2 << 32));
     if (dobj)
         atomicAdd(oo + cell, (unsigned long long)dobj | ((unsigned long long)sect << 32));
@@ -864,48 +887,78 @@ __device__ __forceinline__ void self_set_item(uint32_t t, const unsigned long lo
 // consecutive groups (a warp reads 32 x K postings, contiguous).  Groups of one run
 // share their K(K-1)/2 counter cells; per pair, a warp sums each run's increments by
 // a segmented reduction toward the run's first lane (run heads from the plan, bit =
-// lane) and that lane adds them with one atomic per counter word.  Threads of a warp
-// exit together (the shuffles span the full warp).
+// lane) and that lane adds them with one atomic per counter word.  A warp takes
+// kFlatRounds(K) consecutive rounds of 32 groups and issues all their loads first, so
+// that each thread keeps several postings in flight.  Threads of a warp exit together
+// (the shuffles span the full warp).
+__host__ __device__ constexpr uint32_t kFlatRounds(int k) { return k == 2 ? 3 : 1; }
+#ifndef KSSD_FLAT_REDUX
+#define KSSD_FLAT_REDUX 1
+#endif
+
 template <int K>
-__device__ __forceinline__ void self_flat_group(uint32_t t, const uint64_t *__restrict__ pk, uint32_t nk,
-                                                const uint32_t *__restrict__ hk, unsigned long long *__restrict__ oc,
-                                                unsigned long long *__restrict__ oo)
+__device__ __forceinline__ void self_flat_groups(uint32_t t, const uint64_t *__restrict__ pk, uint32_t nk,
+                                                 const uint32_t *__restrict__ hk, unsigned long long *__restrict__ oc,
+                                                 unsigned long long *__restrict__ oo)
 {
-    const uint32_t lane = t & 31, base = t - lane;
-    if (base >= nk)
+    constexpr uint32_t R = kFlatRounds(K);
+    const uint32_t lane = t & 31, w0 = (t >> 5) * R;  // the warp's first 32-group word
+    if ((size_t)w0 * 32 >= nk)
         return;
-    const uint32_t nv = min(nk - base, 32u);
-    const bool act = lane < nv;
-    uint64_t p[K];
+    uint64_t p[R][K];
+    uint32_t hw[R];
 #pragma unroll
-    for (int x = 0; x < K; ++x)
-        p[x] = act ? __ldg(pk + (size_t)K * t + x) : 0;
-    // segments: the plan's run heads, lane 0, and every inactive lane on its own
-    const uint32_t valid = nv == 32 ? 0xFFFFFFFFu : (1u << nv) - 1;
-    const uint32_t heads = __ldg(hk + (t >> 5)) | 1u | ~valid;
-    const uint32_t above = lane == 31 ? 0u : heads & (0xFFFFFFFFu << (lane + 1));
-    const uint32_t end = above ? (uint32_t)__ffs(above) - 1 : 32u;
-    const bool lead = act && ((heads >> lane) & 1u);
-    const uint32_t m = end - lane;
+    for (uint32_t r = 0; r < R; ++r) {
+        const size_t g = (size_t)(w0 + r) * 32 + lane;
+        const bool act = g < nk;
 #pragma unroll
-    for (int j = 1; j < K; ++j) {
+        for (int x = 0; x < K; ++x)
+            p[r][x] = act ? __ldg(pk + (size_t)K * g + x) : 0;
+        hw[r] = (size_t)(w0 + r) * 32 < nk ? __ldg(hk + w0 + r) : 0u;
+    }
 #pragma unroll
-        for (int i = 0; i < j; ++i) {
-            const uint32_t d = (uint32_t)min(kMinInit, dna_pop((uint32_t)p[i] ^ (uint32_t)p[j]));
-            // sect (9 bits: at most 32 x 12) | dobj << 9 (6 bits) | mut2 << 15 (6 bits)
-            uint32_t v = act ? d | (uint32_t)(d > 0) << 9 | (uint32_t)(d > 1) << 15 : 0;
+    for (uint32_t r = 0; r < R; ++r) {
+        const size_t base = (size_t)(w0 + r) * 32;
+        if (base >= nk)
+            break;  // the same for the whole warp
+        const uint32_t nv = (uint32_t)min((size_t)32, nk - base);
+        const bool act = lane < nv;
+        // segments: the plan's run heads, lane 0, and every inactive lane on its own
+        const uint32_t valid = nv == 32 ? 0xFFFFFFFFu : (1u << nv) - 1;
+        const uint32_t heads = hw[r] | 1u | ~valid;
+        const uint32_t above = lane == 31 ? 0u : heads & (0xFFFFFFFFu << (lane + 1));
+        const uint32_t end = above ? (uint32_t)__ffs(above) - 1 : 32u;
+        const bool lead = act && ((heads >> lane) & 1u);
+        const uint32_t m = end - lane;
+        if (r == 0)
+            pdl_wait_primary();
 #pragma unroll
-            for (uint32_t off = 1; off < 32; off <<= 1) {
-                const uint32_t x = __shfl_down_sync(0xFFFFFFFFu, v, off);
-                if (lane + off < end)
-                    v += x;
-            }
-            if (lead) {
-                const uint32_t sect = v & 511u, dobj = (v >> 9) & 63u, mut2 = v >> 15;
-                const size_t cell = lower_cell((uint32_t)(p[j] >> 32), (uint32_t)(p[i] >> 32));
-                atomicAdd(oc + cell, (unsigned long long)m | ((unsigned long long)mut2 << 32));
-                if (dobj)
-                    atomicAdd(oo + cell, (unsigned long long)dobj | ((unsigned long long)sect << 32));
+        for (int j = 1; j < K; ++j) {
+#pragma unroll
+            for (int i = 0; i < j; ++i) {
+                const uint32_t d = (uint32_t)min(kMinInit, dna_pop((uint32_t)p[r][i] ^ (uint32_t)p[r][j]));
+                // sect (9 bits: at most 32 x 12) | dobj << 9 (6 bits) | mut2 << 15 (6 bits)
+                uint32_t v = act ? d | (uint32_t)(d > 0) << 9 | (uint32_t)(d > 1) << 15 : 0;
+#if KSSD_FLAT_REDUX
+                if (heads == 1u) {
+                    v = __reduce_add_sync(0xFFFFFFFFu, v);  // one run over the whole warp
+                } else
+#endif
+                {
+#pragma unroll
+                    for (uint32_t off = 1; off < 32; off <<= 1) {
+                        const uint32_t x = __shfl_down_sync(0xFFFFFFFFu, v, off);
+                        if (lane + off < end)
+                            v += x;
+                    }
+                }
+                if (lead) {
+                    const uint32_t sect = v & 511u, dobj = (v >> 9) & 63u, mut2 = v >> 15;
+                    const size_t cell = lower_cell((uint32_t)(p[r][j] >> 32), (uint32_t)(p[r][i] >> 32));
+                    atomicAdd(oc + cell, (unsigned long long)m | ((unsigned long long)mut2 << 32));
+                    if (dobj)
+                        atomicAdd(oo + cell, (unsigned long long)dobj | ((unsigned long long)sect << 32));
+                }
             }
         }
     }
@@ -930,7 +983,7 @@ __device__ __forceinline__ bool flat_class_block(const FlatClasses &fc, const ui
     const uint32_t b = blockIdx.x - fc.block0[K];
     if (b >= fc.nblocks[K])
         return false;
-    self_flat_group<K>(b * blockDim.x + threadIdx.x, jp + fc.off[K], fc.n[K], fheads + fc.hoff[K], oc, oo);
+    self_flat_groups<K>(b * blockDim.x + threadIdx.x, jp + fc.off[K], fc.n[K], fheads + fc.hoff[K], oc, oo);
     return true;
 }
 
@@ -1120,6 +1173,7 @@ struct kssdgpu_index {
     int *err = nullptr;
     unsigned int *work = nullptr;
     int sms = 148;
+    int l2_bytes = 0;
     // host-API staging
     DevBuf<uint64_t> s_keys, s_offs;
     DevBuf<unsigned long long> s_out;
@@ -1220,6 +1274,7 @@ int new_index(int nref, int obj_bits, int device, uint64_t n, kssdgpu_index **ou
     ix->obj_bits = obj_bits;
     ix->n = n;
     cudaDeviceGetAttribute(&ix->sms, cudaDevAttrMultiProcessorCount, device);
+    cudaDeviceGetAttribute(&ix->l2_bytes, cudaDevAttrL2CacheSize, device);
     cudaError_t e = cudaMalloc(&ix->err, sizeof(int));
     if (e == cudaSuccess)
         e = cudaMalloc(&ix->work, sizeof(unsigned int));
@@ -1578,21 +1633,36 @@ uint32_t env_u32(const char *name, uint32_t def, uint32_t lo, uint32_t hi)
 
 // One launch of the set-major join: the plan's (chunk, pair) items, then its flat
 // classes, largest size first.
-cudaError_t launch_sets(kssdgpu_index *ix, unsigned long long *oc, unsigned long long *oo, cudaStream_t st)
+cudaError_t launch_sets(kssdgpu_index *ix, unsigned long long *oc, unsigned long long *oo, cudaStream_t st,
+                        bool after_zero = false)
 {
     FlatClasses fc = ix->j_flat;
     const uint32_t sb = (ix->j_nitems + 255) / 256;
     uint32_t nb = sb;
     for (uint32_t k = kFlatMax; k >= 2; --k) {
         fc.block0[k] = nb;
-        fc.nblocks[k] = (fc.n[k] + 255) / 256;
+        const uint32_t per_block = 256 * kFlatRounds((int)k);  // groups per block
+        fc.nblocks[k] = (uint32_t)(((uint64_t)fc.n[k] + per_block - 1) / per_block);
         nb += fc.nblocks[k];
     }
     if (!nb)
         return cudaSuccess;
-    k_self_sets<<<nb, 256, 0, st>>>(ix->j_items.p, ix->j_nitems, sb, ix->j_post.p, fc, ix->j_fheads.p, oc, oo);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(nb);
+    cfg.blockDim = dim3(256);
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    if (after_zero && KSSD_JOIN_PDL) {
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+    }
+    const cudaError_t e = cudaLaunchKernelEx(&cfg, k_self_sets, (const unsigned long long *)ix->j_items.p, ix->j_nitems,
+                                             sb, (const uint64_t *)ix->j_post.p, fc, (const uint32_t *)ix->j_fheads.p,
+                                             oc, oo);
     count_launch();
-    return cudaGetLastError();
+    return e != cudaSuccess ? e : cudaGetLastError();
 }
 
 cudaError_t set_major_plan(kssdgpu_index *ix, uint32_t n, cudaStream_t st)
@@ -1908,6 +1978,12 @@ int self_lower_dev_impl(kssdgpu_index *ix, unsigned flags, unsigned long long *o
     if (rc)
         return rc;
     const size_t cells = (size_t)ix->nref * (ix->nref - 1) / 2;
+    // The join launches programmatically after k_zero_pair when the fill stays in L2:
+    // hiding the join's launch and first loads under a fill of a few microseconds
+    // shortens the 2,000-genome step by 4 us (of 32); after fills of hundreds of
+    // microseconds (20,000 genomes: 3.2 GB) it measured 22 us slower, so there the
+    // launches stay serialized.
+    bool after_fill = false;
     if (!(flags & KSSDGPU_NO_ZERO)) {
         const size_t words = std::max<size_t>(cells, 1);
         if ((((uintptr_t)oc | (uintptr_t)oo) & 15) == 0) {
@@ -1915,12 +1991,13 @@ int self_lower_dev_impl(kssdgpu_index *ix, unsigned flags, unsigned long long *o
             k_zero_pair<<<ix->sms * 8, 256, 0, st>>>(oc, oo, words);
             count_launch();
             CUDA_TRY(cudaGetLastError());
+            after_fill = cells * 16 <= (size_t)ix->l2_bytes;
         } else {
             CUDA_TRY(cudaMemsetAsync(oc, 0, words * 8, st));
             CUDA_TRY(cudaMemsetAsync(oo, 0, words * 8, st));
         }
     }
-    CUDA_TRY(launch_sets(ix, oc, oo, st));
+    CUDA_TRY(launch_sets(ix, oc, oo, st, after_fill));
     if (ix->j_n[1]) {
         k_self_big<<<(unsigned)(((uint64_t)ix->j_n[1] * 32 + 255) / 256), 256, 0, st>>>(ix->j_big.p, ix->j_n[1], ix->post,
                                                                                        oc, oo);

@@ -158,6 +158,34 @@ def test_self_join_autotuner_keeps_counts(monkeypatch):
     np.testing.assert_array_equal(got[1], want[1])
 
 
+@pytest.mark.parametrize("misalign", [0, 8])
+def test_self_lower_dev_overwrites_stale_counters(misalign):
+    """kssdgpu_self_lower_dev zero-fills the device counters before the join adds into
+    them (the join may start under the fill's tail and waits for it before its first
+    atomic): counters full of stale values come out equal to the oracle's, repeatedly.
+    An 8-byte offset takes the memset path instead of the 16-byte fill kernel."""
+    import torch
+    sk = kssdgpu.synth(n_samples=400, n_clusters=40, len_median=3e5, len_min=1e5, len_max=1e6,
+                       size_dist=kssdgpu.SIZE_LOGNORMAL, sub_lo=0.001, sub_hi=0.1)
+    rec = oracle.build_index(sk.keys, sk.offs)
+    idx = kssdgpu.Index.from_records(rec, sk.n)
+    want = oracle.self_lower_all(rec, sk.keys, sk.offs)
+    cells = sk.n * (sk.n - 1) // 2
+    w = misalign // 8
+    buf_c = torch.empty(cells + 1, dtype=torch.int64, device="cuda")
+    buf_o = torch.empty(cells + 1, dtype=torch.int64, device="cuda")
+    d_c, d_o = buf_c[w:w + cells], buf_o[w:w + cells]
+    for rep in range(3):
+        buf_c.fill_(0x5A5A5A5A5A5A5A5A - rep)
+        buf_o.fill_(-1 - rep)
+        idx.self_lower_dev(d_c, d_o)
+        torch.cuda.synchronize()
+        got_c = d_c.cpu().numpy().view(np.uint32).reshape(-1, 2)
+        got_o = d_o.cpu().numpy().view(np.uint32).reshape(-1, 2)
+        np.testing.assert_array_equal(got_c, want[0])
+        np.testing.assert_array_equal(got_o, want[1])
+
+
 def test_read_sets_with_conflicts():
     ref = kssdgpu.synth(n_samples=40, n_clusters=8, len_median=2e5, len_min=1e5, len_max=1e6)
     reads = kssdgpu.synth(n_samples=6, n_clusters=8, role=kssdgpu.ROLE_READS, sample_seed=5,
