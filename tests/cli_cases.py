@@ -40,9 +40,13 @@ FIXTURES = {
                    sample_seed=31, ref_sample_seed=11, ref_samples=120, cov_lo=5, cov_hi=20, err_lo=0.001,
                    err_hi=0.005, name_prefix="reads"),
 }
-INDEXED = {"refs120i", "refs120im", "refs40i"}  # with sortedcomb_ctxgid64obj32 written up front
+INDEXED = {"refs120i", "refs120im", "refs40i", "refs40c9i"}  # with sortedcomb_ctxgid64obj32 written up front
 WITH_META = {"refs120im", "refs40m"}  # with lcofiles.infilemeta (per-sample input metadata)
 WITH_COUNTS = {"reads6a", "reads1a"}  # sketched with k-mer counts: comblco.a
+# sketched at 9 or 10 codens (k = 26 / 29): 36- / 40-bit contexts, 16- / 18-bit objects
+# (the reference reads the object width of every sketch from its lcofiles.stat)
+CODENS = {"refs40c9": (9, 26), "refs40c9i": (9, 26), "qry8c9": (9, 26), "qry50c9": (9, 26),
+          "refs40c10": (10, 29), "qry8c10": (10, 29)}
 
 
 def synth_counts(sk, seed):
@@ -156,6 +160,12 @@ CASES = [
                                    "--estimate-coverage"], {}),
     ("reads_coverage_no_counts", ["ani", "-r", "{refs120i}", "--qraw", "{reads6}", "-n", "0.8",
                                   "--estimate-coverage"], {}),
+    # sketches of 9 and 10 codens: narrower objects (p_dist divides by the object width)
+    ("codens9_memeff_detail", ["ani", "-r", "{refs40c9i}", "-q", "{qry50c9}", "-n", "0.5"], {}),
+    ("codens9_stream_pdist", ["ani", "-r", "{refs40c9}", "-q", "{qry8c9}", "--metric", "p_dist", "-n", "0.3"], {}),
+    ("codens9_self_matrix", ["ani", "-q", "{refs40c9i}", "--format", "matrix", "--values", "ani"], {}),
+    ("codens10_stream_detail", ["ani", "-r", "{refs40c10}", "-q", "{qry8c10}", "-n", "0.5", "-v"], {}),
+    ("codens10_matrix_triangle", ["matrix", "--format", "triangle", "{refs40c10}"], {}),
 ]
 
 
@@ -168,10 +178,14 @@ def make_fixture(root: str, name: str) -> str:
     while base not in FIXTURES:
         base = base[:-1]
     spec = dict(FIXTURES[base])
+    coden_len, klen = CODENS.get(name, (11, 32))
+    if name in CODENS:
+        spec.update(ctx_bits=4 * coden_len, obj_bits=2 * klen - 4 * coden_len, klen=klen)
     sk = kssdgpu.synth(**spec)
     meta = synth_meta(sk, len(name)) if name in WITH_META else None
     counts = synth_counts(sk, len(name)) if name in WITH_COUNTS else None
-    kssdgpu.write_sketch_dir(path, sk, with_index=name in INDEXED, meta=meta, abundance=counts)
+    kssdgpu.write_sketch_dir(path, sk, coden_len=coden_len, klen=klen, with_index=name in INDEXED, meta=meta,
+                             abundance=counts)
     return path
 
 
