@@ -6,9 +6,14 @@
 namespace kssd {
 
 constexpr int kGidBits = 20;
-// Initial value of the per-context minimum object difference: NUM_CODENS + 1 with
-// the reference's default NUM_CODENS = 11 (src/command_ani.h:547,684).
-constexpr int kMinInit = 12;
+// Initial value (and cap) of the per-context minimum object difference: NUM_CODENS + 1
+// (src/command_ani.h:287,535,694); the reference's default build has NUM_CODENS = 11,
+// its 9- and 10-coden builds (-DNUM_CODENS) cap at 10 and 11.
+#ifndef KSSD_NUM_CODENS
+#define KSSD_NUM_CODENS 11
+#endif
+static_assert(KSSD_NUM_CODENS >= 9 && KSSD_NUM_CODENS <= 11, "the reference builds 9, 10 or 11 codens");
+constexpr int kMinInit = KSSD_NUM_CODENS + 1;
 constexpr unsigned long long kEmptyCtx = ~0ull;      // contexts are at most 44 bits
 constexpr unsigned long long kInlineBit = 1ull << 62;  // slot holds its only posting
 

@@ -14,8 +14,35 @@
 #define KSSD_NAIVE_TAU (0.01)
 
 /* ---------------------------------------------------------------- model coefficients
- * Trained constants of the reference's default NUM_CODENS = 11 build
- * (src/model_ani.h:9-205); they must be identical for identical output. */
+ * Trained constants of the reference's builds (src/model_ani.h:9-205): the default
+ * NUM_CODENS = 11 set, or the set its 9- and 10-coden builds share; they must be
+ * identical for identical output.  The AF model's constants are the same for all. */
+#ifndef KSSD_NUM_CODENS
+#define KSSD_NUM_CODENS 11
+#endif
+#if KSSD_NUM_CODENS != 9 && KSSD_NUM_CODENS != 10 && KSSD_NUM_CODENS != 11
+#error "the reference builds 9, 10 or 11 codens"
+#endif
+#if KSSD_NUM_CODENS < 11
+static const double k_denom[12] = {1.0090536851341, 1.0013604061893, 1.03540226374509, 1.04270754727088,
+                                   1.0108940845453, 1.0010797461052, 0.98914550652945, 1.01536320288592,
+                                   1.0061957741437, 0.9957814716168, 0.98352379677340, 1.00951820561544};
+static const double k_denom95[12] = {1.0196821174688, 0.9817771341602, 1.04637038371202, 1.02441485561367,
+                                     1.0163855061091, 0.9824051281495, 1.04908985213703, 1.01102197270052,
+                                     1.0074050784795, 1.0018402553389, 0.94654127396428, 0.94051319172603};
+static const double k_coef[17] = {-0.587100397752123, -7.93027271403258e-08, 4.98481429879899e-06,
+                                  -1.63903694463017e-05, -4.93356600478016e-06, -14843.5350131617,
+                                  306478.144745683,  -290254.345158429, -1781.00695309133,
+                                  -1091.99589131905, 327.6575530681,    47395.255680747,
+                                  47798.7112013701,  -35574.6303634354, -45398.423188085,
+                                  -46461.4920783106, 35045.3583333325};
+static const double k_coef95[17] = {10.7394186800999,  -2.92835943410177e-08, 1.66112325940088e-05,
+                                    -3.48757817098253e-05, -1.82725607919882e-05, 3151.11534599359,
+                                    -1300.37794535582, -1824.96575177919, -21820.9227396359,
+                                    -30943.09511694,   10100.3465983902,  25441.8492675468,
+                                    35763.8363380932,  -3901.01958522226, -3669.6748819999,
+                                    -4909.59256464219, -5653.59698386914};
+#else
 static const double k_denom[12] = {1.0178887, 1.0135146, 1.0302181, 1.1205122, 1.0136223, 0.9803396,
                                    1.0021964, 0.9839395, 0.9988935, 0.9690589, 0.9888171, 0.9817371};
 static const double k_denom95[12] = {1.0145656, 1.2708196, 1.2169829, 0.3904416, 0.8147527, 1.3389150,
@@ -32,6 +59,7 @@ static const double k_coef95[17] = {-1.69173585242774, -3.64716315423252e-08, 2.
                                     212.734805232395,  208.388739816682,  -0.27860125939004,
                                     2.27065806912198,  -10.2977013026837, -250.681324281127,
                                     -403.751360812353, -137.96628693833};
+#endif
 static const double k_af_denom[15] = {2.36775520439829,  2.17036643548818,  -0.0977124271437818,
                                       -0.251063182363729, 2.19491057829433,  1.41850238263675,
                                       2.15224961402778,  -2.18587619877498, -2.21943802445092,
@@ -44,9 +72,14 @@ static const double k_af_coef[21] = {0.127498260534708, -1.51730137145957e-06, 9
                                      -86.3482066935661, 2.16630645286942,  -0.674746089642152,
                                      48.1147600903939,  3.39101087242059,  -15.5481688297158,
                                      -26.7068442368566, 18.5142668221724,  20.4430437567379};
-/* naive model for NUM_CODENS = 11 (src/command_ani.h:214-220) */
+/* naive model (src/command_ani.h:212-218) */
+#if KSSD_NUM_CODENS < 11
+static const double k_naive_scale = 0.1557143;
+static const double k_naive_intercept = 9.961e-5;
+#else
 static const double k_naive_scale = 0.1544286;
 static const double k_naive_intercept = 7.133e-4;
+#endif
 
 static const char *const k_metric_names[9] = {"BestDist", "RecalDist", "CtxMoE", "Naive", "MashD",
                                               "AafD",     "MashD_if_far", "AafD_if_far", "p_dist"};
@@ -167,6 +200,12 @@ static double clamp01(double x) { return x < 0.0 ? 0.0 : (x > 1.0 ? 1.0 : x); }
 double kssd_hgb_predict_ani(double raw_ani, double ref_af, unsigned xny, unsigned n_diff_obj,
                             unsigned n_diff_obj_section, unsigned n_mut2_ctx, int drfold)
 {
+#if KSSD_NUM_CODENS < 11
+    /* the 9- and 10-coden builds carry no calibration model: raw ANI
+     * (src/model_refaf_hgb.h, its #else branch) */
+    (void)ref_af; (void)xny; (void)n_diff_obj; (void)n_diff_obj_section; (void)n_mut2_ctx; (void)drfold;
+    return raw_ani;
+#endif
     if (xny == 0)
         return raw_ani;
     raw_ani = clamp01(raw_ani);

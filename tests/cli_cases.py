@@ -169,6 +169,21 @@ CASES = [
 ]
 
 
+# Cases run by the 9- and 10-coden builds (build/codens9, build/codens10) against the
+# reference compiled the same way (-DNUM_CODENS=9 / 10: the other lm3ways and naive
+# model coefficients, no calibration model, object-difference cap 10 / 11), on
+# sketches of 9 / 10 codens and of the default 11.
+CODENS_BUILD_CASES = [
+    ("memeff_detail", ["ani", "-r", "{refs40c9i}", "-q", "{qry50c9}", "-n", "0.5"]),
+    ("stream_detail_naive", ["ani", "-r", "{refs40c10}", "-q", "{qry8c10}", "-n", "0.5", "-v"]),
+    ("stream_detail_moe", ["ani", "-r", "{refs40c9}", "-q", "{qry8c9}", "-s", "3", "-n", "0.5"]),
+    ("self_matrix", ["ani", "-q", "{refs40c9i}", "--format", "matrix", "--values", "ani"]),
+    ("matrix_full", ["matrix", "--format", "full", "{refs40c10}"]),
+    ("memeff_detail_11codens", ["ani", "-r", "{refs120}", "-q", "{qry30}", "-n", "0.8"]),
+    ("self_triangle_11codens", ["ani", "-q", "{refs40}", "--format", "triangle", "--values", "ani"]),
+]
+
+
 def make_fixture(root: str, name: str) -> str:
     """Writes fixture `name` under root (idempotent) and returns its directory."""
     path = os.path.join(root, name)

@@ -8,6 +8,9 @@ counts_*.json : fixture samples + every row of `ani --unique-ctx-report` (the
                 reference's full per-cell counters, src/command_ani.c:462-492)
 cli/*.out.gz  : the reference CLI's stdout for every case of tests/cli_cases.py
                 (seeded synthetic sketch directories, regenerated on demand)
+cli_codens/c{9,10}_*.out.gz : the reference CLI compiled for 9 / 10 codens
+                (`make -C oracle ref-codens`) on the CODENS_BUILD_CASES of
+                tests/cli_cases.py (`python tests/golden/make_golden.py codens` alone)
 """
 import csv
 import io
@@ -96,7 +99,30 @@ def cli_cases():
         shutil.rmtree(root)
 
 
+def codens_cases():
+    """stdout of the reference CLI compiled for 9 and 10 codens (oracle/_ref/kssd3a_c9,
+    kssd3a_c10: `make -C oracle ref-codens`) for every CODENS_BUILD_CASES case."""
+    import gzip
+    from cli_cases import CODENS_BUILD_CASES, materialize, with_threads
+    out_dir = os.path.join(HERE, "cli_codens")
+    os.makedirs(out_dir, exist_ok=True)
+    root = tempfile.mkdtemp(prefix="golden-codens-")
+    try:
+        for c in (9, 10):
+            for name, argv in CODENS_BUILD_CASES:
+                a = materialize(root, argv, f"ref_c{c}_" + name)
+                e = dict(os.environ, OMP_NUM_THREADS="4")
+                r = subprocess.run([f"{REF}_c{c}", *with_threads(a)], capture_output=True, env=e, check=True)
+                with gzip.GzipFile(os.path.join(out_dir, f"c{c}_{name}.out.gz"), "wb", mtime=0) as f:
+                    f.write(r.stdout)
+                print(f"c{c}", name, len(r.stdout), "bytes")
+    finally:
+        shutil.rmtree(root)
+
+
 def main():
+    if sys.argv[1:] == ["codens"]:
+        return codens_cases()
     if not os.path.exists(REF):
         sys.exit(f"{REF} missing: run `make -C oracle ref` first")
     counts_case("s0", 0, 4, 2, 35, 256, False)
@@ -105,6 +131,7 @@ def main():
     counts_case("s3", 3, 12, 6, 60, 1 << 20, True)
     counts_case("s4", 4, 30, 10, 400, 1 << 20, False)
     cli_cases()
+    codens_cases()
 
 
 if __name__ == "__main__":
