@@ -752,8 +752,11 @@ __global__ void k_set_chunk_heads(const uint32_t *__restrict__ runs_incl, const 
 }
 
 // chunk records {offset of the first group's postings, m | k << 32} and pair counts
+// Sort key of a chunk: (descending group count, then size) when sorted, else the size
+// alone (plan order within a size); chunks of equal (count, size) end up adjacent,
+// as the item tiles need.
 __global__ void k_set_chunks(const uint32_t *__restrict__ cheads, const uint32_t *__restrict__ cpos, uint32_t n,
-                             uint32_t csize, const unsigned long long *__restrict__ desc,
+                             uint32_t csize, int by_count, const unsigned long long *__restrict__ desc,
                              ulonglong2 *__restrict__ chunks, uint32_t *__restrict__ skey, uint32_t *__restrict__ sval)
 {
     for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
@@ -767,7 +770,7 @@ __global__ void k_set_chunks(const uint32_t *__restrict__ cheads, const uint32_t
         const unsigned long long d = desc[t];
         const uint32_t k = (uint32_t)(d >> 32);
         chunks[c] = make_ulonglong2((unsigned long long)(uint32_t)d, (unsigned long long)(e - t) | ((unsigned long long)k << 32));
-        skey[c] = csize - (e - t);  // ascending key = descending group count
+        skey[c] = (by_count ? (csize - (e - t)) << 6 : 0u) | k;  // csize < 256, k <= 32: 14 bits
         sval[c] = c;
     }
 }
@@ -776,16 +779,12 @@ __global__ void k_set_chunks(const uint32_t *__restrict__ cheads, const uint32_t
 // instead of as (chunk, pair) items; the plan chooses the largest flat size.
 constexpr uint32_t kFlatMax = 4;
 
-// chunks in sorted order, with their pair counts (none for chunks of flat-joined sizes)
+// chunks in sorted order
 __global__ void k_set_permute(const uint32_t *__restrict__ order, uint32_t nchunks, const ulonglong2 *__restrict__ in,
-                              ulonglong2 *__restrict__ out, uint32_t *__restrict__ npairs, uint32_t flat_max)
+                              ulonglong2 *__restrict__ out)
 {
-    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < nchunks; c += gridDim.x * blockDim.x) {
-        const ulonglong2 ch = in[order[c]];
-        const uint32_t k = (uint32_t)(ch.y >> 32);
-        out[c] = ch;
-        npairs[c] = k <= flat_max ? 0 : k * (k - 1) / 2;
-    }
+    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < nchunks; c += gridDim.x * blockDim.x)
+        out[c] = in[order[c]];
 }
 
 // first sorted small group of every size 2..flat_max (the groups are sorted by size,
@@ -811,38 +810,114 @@ __global__ void k_flat_heads(const uint32_t *__restrict__ heads, uint32_t first,
         out[t >> 5] = b;
 }
 
-// Self-contained join items: offset of the chunk's first group in the compact
-// postings (34 bits) | m << 34 (8) | k << 42 (6) | i << 48 (5) | j << 53 (5).
+// Self-contained join items: first word of the chunk's tile in the tiled postings
+// (34 bits) | m << 34 (8) | k << 42 (6) | i << 48 (5) | j << 53 (5) | slot << 58 (5),
+// slot = the chunk's place in its tile.  The all-zero word (m = 0) is an empty lane.
 __host__ __device__ __forceinline__ unsigned long long set_item(uint64_t off, uint32_t m, uint32_t k, uint32_t i,
-                                                                uint32_t j)
+                                                                uint32_t j, uint32_t slot)
 {
     return off | ((unsigned long long)m << 34) | ((unsigned long long)k << 42) | ((unsigned long long)i << 48) |
-           ((unsigned long long)j << 53);
+           ((unsigned long long)j << 53) | ((unsigned long long)slot << 58);
 }
 constexpr uint64_t kSetItemMaxOffset = 1ull << 34;
 
-// items[item_off[c] + p] for the chunk's pairs (i < j); chunks of flat-joined sizes
-// have none
-__global__ void k_set_items(const ulonglong2 *__restrict__ chunks, const uint32_t *__restrict__ item_off, uint32_t nchunks,
-                            uint32_t flat_max, unsigned long long *__restrict__ items)
+// Item tiles.  Chunks of equal group count m and size k are packed C at a time into
+// a tile whose postings are stored row-interleaved: row x of chunk 0, row x of chunk
+// 1, ..., then row x + 1 (word (x * C + slot) * k + posting).  C = 32 / P chunks with
+// P = k(k-1)/2 items each fill one warp, so the warp's loads of one row touch one or
+// two 128-byte lines instead of one line per chunk; a chunk with P > 32 items is a
+// tile of its own over whole warps.
+__host__ __device__ __forceinline__ uint32_t tile_chunks(uint32_t k)
+{
+    const uint32_t p = k * (k - 1) / 2;
+    return p >= 1 && p <= 32 ? 32 / p : 1;
+}
+__host__ __device__ __forceinline__ uint32_t tile_lanes(uint32_t k)
+{
+    const uint32_t p = k * (k - 1) / 2;
+    return p <= 32 ? 32 : (p + 31) / 32 * 32;
+}
+
+// heads of the runs of tiled chunks with equal (m, k) in the sorted chunk order
+__global__ void k_tile_class_heads(const ulonglong2 *__restrict__ chunks, uint32_t nchunks, uint32_t flat_max,
+                                   uint32_t *__restrict__ heads)
+{
+    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < nchunks; c += gridDim.x * blockDim.x) {
+        const unsigned long long y = chunks[c].y;
+        const uint32_t k = (uint32_t)(y >> 32);
+        heads[c] = k > flat_max && (c == 0 || chunks[c - 1].y != y);
+    }
+}
+
+// each chunk's slot in its tile; tile heads carry the tile's words and lanes
+__global__ void k_tile_slots(const ulonglong2 *__restrict__ chunks, uint32_t nchunks, uint32_t flat_max,
+                             const uint32_t *__restrict__ cls_incl, const uint32_t *__restrict__ cls_first,
+                             uint32_t *__restrict__ slot, unsigned long long *__restrict__ words,
+                             uint32_t *__restrict__ lanes)
+{
+    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < nchunks; c += gridDim.x * blockDim.x) {
+        const unsigned long long y = chunks[c].y;
+        const uint32_t m = (uint32_t)y, k = (uint32_t)(y >> 32);
+        uint32_t sl = 0;
+        unsigned long long wd = 0;
+        uint32_t ln = 0;
+        if (k > flat_max) {
+            const uint32_t cap = tile_chunks(k);
+            sl = (c - cls_first[cls_incl[c] - 1]) % cap;
+            if (sl == 0) {
+                wd = (unsigned long long)m * cap * k;
+                ln = tile_lanes(k);
+            }
+        }
+        slot[c] = sl;
+        words[c] = wd;
+        lanes[c] = ln;
+    }
+}
+
+// postings of every tiled chunk into its tile, row-interleaved
+__global__ void k_tile_scatter(const ulonglong2 *__restrict__ chunks, uint32_t nchunks, uint32_t flat_max,
+                               const uint32_t *__restrict__ slot, const unsigned long long *__restrict__ word0,
+                               const uint64_t *__restrict__ jp, uint64_t *__restrict__ jt)
 {
     for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < nchunks; c += gridDim.x * blockDim.x) {
         const ulonglong2 ch = chunks[c];
         const uint32_t m = (uint32_t)ch.y, k = (uint32_t)(ch.y >> 32);
         if (k <= flat_max)
             continue;
-        uint32_t o = item_off[c];
+        const uint32_t sl = slot[c], cap = tile_chunks(k);
+        const uint64_t base = word0[c - sl];
+        for (uint32_t x = 0; x < m; ++x)
+            for (uint32_t i = 0; i < k; ++i)
+                jt[base + ((uint64_t)x * cap + sl) * k + i] = jp[ch.x + (uint64_t)x * k + i];
+    }
+}
+
+// Items of every tiled chunk: pair p (i < j, p = j(j-1)/2 + i) of the chunk in slot
+// sl of its tile is lane lane0 + sl * P + p of the tile's lanes; unused lanes stay 0.
+__global__ void k_set_items(const ulonglong2 *__restrict__ chunks, uint32_t nchunks, uint32_t flat_max,
+                            const uint32_t *__restrict__ slot, const unsigned long long *__restrict__ word0,
+                            const uint32_t *__restrict__ lane0, unsigned long long *__restrict__ items)
+{
+    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < nchunks; c += gridDim.x * blockDim.x) {
+        const ulonglong2 ch = chunks[c];
+        const uint32_t m = (uint32_t)ch.y, k = (uint32_t)(ch.y >> 32);
+        if (k <= flat_max)
+            continue;
+        const uint32_t sl = slot[c], np = k * (k - 1) / 2;
+        const uint64_t w0 = word0[c - sl];
+        uint32_t o = lane0[c - sl] + sl * np;
         for (uint32_t j = 1; j < k; ++j)
             for (uint32_t i = 0; i < j; ++i)
-                items[o++] = set_item(ch.x, m, k, i, j);
+                items[o++] = set_item(w0, m, k, i, j, sl);
     }
 }
 
 // The set-major join: one thread per (chunk, pair) item.  The m groups of the chunk
 // share their gid list, so the pair's counter cell is the same for all of them:
 // sum num_ctx (= m), mut2, diff_obj and section over the groups, then one atomic
-// per counter word.  The chunk's postings (m x k, contiguous) are read by all its
-// items, from L1.
+// per counter word.  The items of a tile (one warp) read the same row of its
+// row-interleaved postings together, from one or two lines.
 #ifndef KSSD_SET_UNROLL
 #define KSSD_SET_UNROLL 4
 #endif
@@ -851,7 +926,7 @@ __global__ void k_set_items(const ulonglong2 *__restrict__ chunks, const uint32_
 #endif
 constexpr int kSetUnroll = KSSD_SET_UNROLL;
 __device__ __forceinline__ void self_set_item(uint32_t t, const unsigned long long *__restrict__ items, uint32_t nitems,
-                                              const uint64_t *__restrict__ jp, unsigned long long *__restrict__ oc,
+                                              const uint64_t *__restrict__ jt, unsigned long long *__restrict__ oc,
                                               unsigned long long *__restrict__ oo)
 {
     if (t >= nitems)
@@ -859,18 +934,21 @@ __device__ __forceinline__ void self_set_item(uint32_t t, const unsigned long lo
     const unsigned long long it = __ldg(items + t);
     const uint64_t off = it & (kSetItemMaxOffset - 1);
     const uint32_t m = (uint32_t)(it >> 34) & 0xFFu, k = (uint32_t)(it >> 42) & 0x3Fu;
+    if (m == 0)
+        return;  // an empty lane of a tile
     const uint32_t i = (uint32_t)(it >> 48) & 0x1Fu, j = (uint32_t)(it >> 53) & 0x1Fu;
-    const uint64_t *g = jp + off;
-    // the first group's postings give the gids (high words) and its objects
+    const uint32_t slot = (uint32_t)(it >> 58) & 0x1Fu, stride = tile_chunks(k) * k;  // words per tile row
+    // the chunk's first row gives the gids (high words) and its objects
+    const uint64_t *g = jt + off + slot * k;
     const uint64_t pi0 = __ldg(g + i), pj0 = __ldg(g + j);
     const uint32_t gi = (uint32_t)(pi0 >> 32), gj = (uint32_t)(pj0 >> 32);
     uint32_t d = (uint32_t)min(kMinInit, dna_pop((uint32_t)pi0 ^ (uint32_t)pj0));
     uint32_t mut2 = d > 1, dobj = d > 0, sect = d;
-    // low (object) words of the other groups' postings
+    // low (object) words of the other rows' postings
     const uint32_t *w = reinterpret_cast<const uint32_t *>(g);
 #pragma unroll kSetUnroll
     for (uint32_t x = 1; x < m; ++x) {
-        const uint32_t oi = __ldg(w + 2 * (x * k + i)), oj = __ldg(w + 2 * (x * k + j));
+        const uint32_t oi = __ldg(w + 2 * (x * stride + i)), oj = __ldg(w + 2 * (x * stride + j));
         d = (uint32_t)min(kMinInit, dna_pop(oi ^ oj));
         mut2 += d > 1;
         dobj += d > 0;
@@ -990,13 +1068,14 @@ __device__ __forceinline__ bool flat_class_block(const FlatClasses &fc, const ui
 // The join launch: the first set_blocks blocks run the (chunk, pair) items, the rest
 // the flat classes (largest size first), so that the latter fill the former's tail.
 __global__ void __launch_bounds__(256, KSSD_SET_MINB) k_self_sets(const unsigned long long *__restrict__ items, uint32_t nitems,
-                                                   uint32_t set_blocks, const uint64_t *__restrict__ jp,
+                                                   uint32_t set_blocks, const uint64_t *__restrict__ jt,
+                                                   const uint64_t *__restrict__ jp,
                                                    const FlatClasses fc, const uint32_t *__restrict__ fheads,
                                                    unsigned long long *__restrict__ oc,
                                                    unsigned long long *__restrict__ oo)
 {
     if (blockIdx.x < set_blocks) {
-        self_set_item(blockIdx.x * blockDim.x + threadIdx.x, items, nitems, jp, oc, oo);
+        self_set_item(blockIdx.x * blockDim.x + threadIdx.x, items, nitems, jt, oc, oo);
         return;
     }
     static_assert(kFlatMax == 4, "one dispatch per flat class");
@@ -1194,7 +1273,8 @@ struct kssdgpu_index {
     DevBuf<unsigned long long> j_small, j_big, j_conf;
     DevBuf<uint64_t> j_post;
     DevBuf<ulonglong2> j_chunks;            // set-major chunks of the small groups
-    DevBuf<unsigned long long> j_items;     // (chunk, pair) work items
+    DevBuf<unsigned long long> j_items;     // (chunk, pair) work items, tile by tile (one warp each)
+    DevBuf<uint64_t> j_tile;                // postings of the item chunks, row-interleaved by tile
     uint32_t j_nchunks = 0, j_nitems = 0;
     uint32_t j_chunk_size = 32;             // groups per set-major chunk (1..255)
     bool j_sort_chunks = true;              // chunks ordered by group count, largest first
@@ -1659,8 +1739,8 @@ cudaError_t launch_sets(kssdgpu_index *ix, unsigned long long *oc, unsigned long
         cfg.numAttrs = 1;
     }
     const cudaError_t e = cudaLaunchKernelEx(&cfg, k_self_sets, (const unsigned long long *)ix->j_items.p, ix->j_nitems,
-                                             sb, (const uint64_t *)ix->j_post.p, fc, (const uint32_t *)ix->j_fheads.p,
-                                             oc, oo);
+                                             sb, (const uint64_t *)ix->j_tile.p, (const uint64_t *)ix->j_post.p, fc,
+                                             (const uint32_t *)ix->j_fheads.p, oc, oo);
     count_launch();
     return e != cudaSuccess ? e : cudaGetLastError();
 }
@@ -1675,14 +1755,15 @@ cudaError_t set_major_plan(kssdgpu_index *ix, uint32_t n, cudaStream_t st)
     uint32_t *heads = nullptr, *runs = nullptr, *first = nullptr, *cheads = nullptr, *cpos = nullptr;
     uint32_t *skey = nullptr, *skey2 = nullptr, *sval = nullptr, *sval2 = nullptr, *npairs = nullptr, *ioff = nullptr;
     uint32_t *f2d = nullptr;
+    unsigned long long *twords = nullptr, *tword0 = nullptr;
     ulonglong2 *chunks0 = nullptr;
     void *tmp = nullptr;
     auto cleanup = [&]() {
         cudaFree(heads); cudaFree(runs); cudaFree(first); cudaFree(cheads); cudaFree(cpos);
         cudaFree(skey); cudaFree(skey2); cudaFree(sval); cudaFree(sval2); cudaFree(npairs); cudaFree(ioff);
-        cudaFree(f2d); cudaFree(chunks0); cudaFree(tmp);
+        cudaFree(f2d); cudaFree(twords); cudaFree(tword0); cudaFree(chunks0); cudaFree(tmp);
     };
-    size_t tb1 = 0, tb2 = 0, tb3 = 0;
+    size_t tb1 = 0, tb2 = 0, tb3 = 0, tb4 = 0;
     cudaError_t e = cudaMalloc(&heads, (size_t)n * 4);
     if (e == cudaSuccess) e = cudaMalloc(&f2d, (kFlatMax + 1) * 4);
     if (e == cudaSuccess) e = cudaMalloc(&runs, (size_t)n * 4);
@@ -1696,10 +1777,13 @@ cudaError_t set_major_plan(kssdgpu_index *ix, uint32_t n, cudaStream_t st)
     if (e == cudaSuccess) e = cudaMalloc(&npairs, (size_t)n * 4);
     if (e == cudaSuccess) e = cudaMalloc(&ioff, (size_t)n * 4);
     if (e == cudaSuccess) e = cudaMalloc(&chunks0, (size_t)n * sizeof(ulonglong2));
+    if (e == cudaSuccess) e = cudaMalloc(&twords, (size_t)n * 8);
+    if (e == cudaSuccess) e = cudaMalloc(&tword0, (size_t)n * 8);
+    if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(nullptr, tb4, twords, tword0, n, st);
     if (e == cudaSuccess) e = cub::DeviceScan::InclusiveSum(nullptr, tb1, heads, runs, n, st);
     if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(nullptr, tb2, cheads, cpos, n, st);
     if (e == cudaSuccess) e = cub::DeviceRadixSort::SortPairs(nullptr, tb3, skey, skey2, sval, sval2, n, 0, 16, st);
-    const size_t tb = std::max<size_t>(std::max(std::max(tb1, tb2), tb3), 1);
+    const size_t tb = std::max<size_t>(std::max(std::max(tb1, tb2), std::max(tb3, tb4)), 1);
     if (e == cudaSuccess) e = cudaMalloc(&tmp, tb);
     if (e == cudaSuccess) {
         k_set_heads<<<grid_for(n), 256, 0, st>>>(ix->j_small.p, n, ix->j_post.p, heads);
@@ -1756,35 +1840,59 @@ cudaError_t set_major_plan(kssdgpu_index *ix, uint32_t n, cudaStream_t st)
     const uint32_t nchunks = last_pos + last_head;
     if (e == cudaSuccess) e = ix->j_chunks.ensure(nchunks);
     if (e == cudaSuccess) {
-        k_set_chunks<<<grid_for(n), 256, 0, st>>>(cheads, cpos, n, csize, ix->j_small.p, chunks0, skey, sval);
+        k_set_chunks<<<grid_for(n), 256, 0, st>>>(cheads, cpos, n, csize, ix->j_sort_chunks ? 1 : 0, ix->j_small.p,
+                                                  chunks0, skey, sval);
         count_launch();
-        const uint32_t *order = sval;
-        if (ix->j_sort_chunks) {
-            size_t b = tb;
-            e = cub::DeviceRadixSort::SortPairs(tmp, b, skey, skey2, sval, sval2, nchunks, 0, 16, st);
-            count_launch(4);
-            order = sval2;
-        }
-        if (e == cudaSuccess) {
-            k_set_permute<<<grid_for(nchunks), 256, 0, st>>>(order, nchunks, chunks0, ix->j_chunks.p, npairs,
-                                                             flat_max);
-            count_launch();
-            size_t b = tb;
-            e = cub::DeviceScan::ExclusiveSum(tmp, b, npairs, ioff, nchunks, st);
-            count_launch(2);
-        }
+        size_t b = tb;
+        e = cub::DeviceRadixSort::SortPairs(tmp, b, skey, skey2, sval, sval2, nchunks, 0, 16, st);
+        count_launch(4);
     }
-    uint32_t last_off = 0, last_np = 0;
-    if (e == cudaSuccess) e = cudaMemcpyAsync(&last_off, ioff + nchunks - 1, 4, cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(&last_np, npairs + nchunks - 1, 4, cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    const uint64_t nitems = (uint64_t)last_off + last_np;
-    if (e == cudaSuccess && nitems >= (1ull << 32))
-        e = cudaErrorMemoryAllocation;  // more join items than one 32-bit launch index covers
-    if (e == cudaSuccess) e = ix->j_items.ensure(nitems);
+    // Tiles of the item chunks (sizes above flat_max): runs of equal (m, k) in the
+    // sorted order are cut into tiles of tile_chunks(k) chunks.  The scratch arrays of
+    // the chunk build are free again: heads = class heads, runs = class numbers,
+    // first = class starts, cheads = slots, npairs = tile lanes, ioff = first lanes.
+    uint32_t *slot = cheads, *tlanes = npairs, *tlane0 = ioff;
     if (e == cudaSuccess) {
-        k_set_items<<<grid_for(nchunks), 256, 0, st>>>(ix->j_chunks.p, ioff, nchunks, flat_max, ix->j_items.p);
-        count_launch();
+        k_set_permute<<<grid_for(nchunks), 256, 0, st>>>(sval2, nchunks, chunks0, ix->j_chunks.p);
+        k_tile_class_heads<<<grid_for(nchunks), 256, 0, st>>>(ix->j_chunks.p, nchunks, flat_max, heads);
+        count_launch(2);
+        size_t b = tb;
+        e = cub::DeviceScan::InclusiveSum(tmp, b, heads, runs, nchunks, st);
+        count_launch(2);
+    }
+    if (e == cudaSuccess) {
+        k_set_run_first<<<grid_for(nchunks), 256, 0, st>>>(heads, runs, nchunks, first);
+        k_tile_slots<<<grid_for(nchunks), 256, 0, st>>>(ix->j_chunks.p, nchunks, flat_max, runs, first, slot, twords,
+                                                        tlanes);
+        count_launch(2);
+        size_t b = tb;
+        e = cub::DeviceScan::ExclusiveSum(tmp, b, twords, tword0, nchunks, st);
+        count_launch(2);
+    }
+    if (e == cudaSuccess) {
+        size_t b = tb;
+        e = cub::DeviceScan::ExclusiveSum(tmp, b, tlanes, tlane0, nchunks, st);
+        count_launch(2);
+    }
+    unsigned long long last_w0 = 0, last_w = 0;
+    uint32_t last_l0 = 0, last_l = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&last_w0, tword0 + nchunks - 1, 8, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&last_w, twords + nchunks - 1, 8, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&last_l0, tlane0 + nchunks - 1, 4, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&last_l, tlanes + nchunks - 1, 4, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    const uint64_t nitems = (uint64_t)last_l0 + last_l, tile_words = last_w0 + last_w;
+    if (e == cudaSuccess && (nitems >= (1ull << 32) || tile_words >= kSetItemMaxOffset))
+        e = cudaErrorMemoryAllocation;  // beyond the 32-bit launch index or the item word's offset field
+    if (e == cudaSuccess) e = ix->j_items.ensure(nitems);
+    if (e == cudaSuccess) e = ix->j_tile.ensure(tile_words);
+    if (e == cudaSuccess && nitems) e = cudaMemsetAsync(ix->j_items.p, 0, nitems * 8, st);  // empty lanes
+    if (e == cudaSuccess) {
+        k_tile_scatter<<<grid_for(nchunks), 256, 0, st>>>(ix->j_chunks.p, nchunks, flat_max, slot, tword0,
+                                                          ix->j_post.p, ix->j_tile.p);
+        k_set_items<<<grid_for(nchunks), 256, 0, st>>>(ix->j_chunks.p, nchunks, flat_max, slot, tword0, tlane0,
+                                                       ix->j_items.p);
+        count_launch(2);
         e = cudaStreamSynchronize(st);
     }
     cleanup();
@@ -2251,6 +2359,7 @@ void kssdgpu_index_free(kssdgpu_index_t *ix)
     ix->j_post.release();
     ix->j_chunks.release();
     ix->j_items.release();
+    ix->j_tile.release();
     ix->j_fheads.release();
     ix->j_big.release();
     ix->j_conf.release();
