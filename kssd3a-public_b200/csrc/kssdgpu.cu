@@ -1700,7 +1700,7 @@ int count_host_impl(kssdgpu_index *ix, const uint64_t *qkeys, const uint64_t *qo
 // Runs of equal gid lists among the n sorted small groups -> chunks -> (chunk, pair)
 // items (j_chunks, j_items); the per-group descriptors are released afterwards.
 // Plan knobs, overridable for tuning: KSSDGPU_JOIN_CHUNK (groups per chunk, 1..255)
-// , KSSDGPU_JOIN_SORT (0: chunks in plan order) and KSSDGPU_JOIN_FLAT (largest group
+// , KSSDGPU_JOIN_SORT (0: chunks by size only, plan order within a size) and KSSDGPU_JOIN_FLAT (largest group
 // size joined flat, 1..4; 1: every small group as chunk items).
 uint32_t env_u32(const char *name, uint32_t def, uint32_t lo, uint32_t hi)
 {
@@ -1972,7 +1972,7 @@ cudaError_t tune_join(kssdgpu_index *ix, uint32_t n, cudaStream_t st)
         }
     };
     // the flat size at 32 groups per chunk, largest chunks first; then the chunk
-    // size (largest first) and the plan order at the best flat size
+    // size (largest first) and the size-only order at the best flat size
     for (uint32_t flat = kFlatMax; flat >= 1 && e == cudaSuccess; --flat)
         time_plan(32, true, flat);
     static const struct { uint32_t size; bool sorted; } kChunkCands[] = {
