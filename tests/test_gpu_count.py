@@ -118,22 +118,28 @@ def test_synthetic_genomes_block_and_self():
     np.testing.assert_array_equal(got[1], want[1])
 
 
-def _clustered_sketch():
-    # tight clusters: many contexts shared by exactly 2..4 genomes, in runs of the same
-    # gid list that cross warp (32-group) boundaries and end in partial warps
-    return kssdgpu.synth(n_samples=120, n_clusters=30, len_median=3e5, len_min=1e5, len_max=1e6,
-                         size_dist=kssdgpu.SIZE_LOGNORMAL, sub_lo=0.001, sub_hi=0.05)
+def _clustered_sketch(kind="pairs"):
+    if kind == "pairs":
+        # tight clusters: many contexts shared by exactly 2..4 genomes, in runs of the
+        # same gid list that cross warp (32-group) boundaries and end in partial warps
+        return kssdgpu.synth(n_samples=120, n_clusters=30, len_median=3e5, len_min=1e5, len_max=1e6,
+                             size_dist=kssdgpu.SIZE_LOGNORMAL, sub_lo=0.001, sub_hi=0.05)
+    # three wide clusters: contexts shared by 5..23 genomes (tiles of one chunk whose
+    # 36..253 items span several warps)
+    return kssdgpu.synth(n_samples=90, n_clusters=3, len_median=2e5, len_min=1e5, len_max=6e5,
+                         size_dist=kssdgpu.SIZE_LOGNORMAL, sub_lo=0.001, sub_hi=0.08)
 
 
+@pytest.mark.parametrize("kind", ["pairs", "wide"])
 @pytest.mark.parametrize("flat,chunk,srt", [(1, 32, 1), (2, 32, 1), (3, 32, 1), (4, 32, 1), (4, 1, 1), (4, 7, 0),
                                             (2, 255, 1), (3, 16, 0)])
-def test_self_join_plan_settings(monkeypatch, flat, chunk, srt):
+def test_self_join_plan_settings(monkeypatch, flat, chunk, srt, kind):
     """Every plan setting (largest flat group size, groups per chunk, chunk order)
     gives the oracle's self-join counters."""
     monkeypatch.setenv("KSSDGPU_JOIN_FLAT", str(flat))
     monkeypatch.setenv("KSSDGPU_JOIN_CHUNK", str(chunk))
     monkeypatch.setenv("KSSDGPU_JOIN_SORT", str(srt))
-    sk = _clustered_sketch()
+    sk = _clustered_sketch(kind)
     rec = oracle.build_index(sk.keys, sk.offs)
     idx = kssdgpu.Index.from_records(rec, sk.n)
     want = oracle.self_lower_all(rec, sk.keys, sk.offs)
