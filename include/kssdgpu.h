@@ -208,18 +208,18 @@ int kssdgpu_self_plan_info(kssdgpu_index_t *idx, uint64_t *groups, uint64_t *pos
 
 /*
  * Autotune the self-join plan (once per index; builds the plan first if needed):
- * every candidate setting is planned and timed on scratch counters (after an L2
- * flush) and the fastest is kept.  Reports the setting in use: groups per
+ * every candidate setting is planned and timed as a whole step (zero fill + join) on
+ * scratch counters, after an L2 flush, and the fastest is kept.  Reports the setting in use: groups per
  * set-major chunk, whether chunks run largest first, the largest group size joined
  * flat (one thread per group; 1: none), how many candidates were timed (0: defaults
  * kept, e.g. when a setting is pinned by KSSDGPU_JOIN_CHUNK / KSSDGPU_JOIN_SORT /
- * KSSDGPU_JOIN_FLAT or the scratch would not fit) and the chosen candidate's join
+ * KSSDGPU_JOIN_FLAT or the scratch would not fit) and the chosen candidate's step
  * time in ms.  Without this call the plan uses the defaults (32 groups, largest
- * first, two-genome groups flat) unless KSSDGPU_TUNE=1.  Synchronizes the device.  No
+ * first, every size as tiled items) unless KSSDGPU_TUNE=1.  Synchronizes the device.  No
  * reference counterpart (the CPU path has no tunables).  Any out pointer may be NULL.
  */
 int kssdgpu_self_plan_tune(kssdgpu_index_t *idx, uint32_t *chunk_groups, int *sorted, uint32_t *flat_groups,
-                           int *candidates, float *join_ms);
+                           int *candidates, float *step_ms);
 
 /*
  * Plain baseline kernel with device inputs: one launch per query (h_qry_offs is a

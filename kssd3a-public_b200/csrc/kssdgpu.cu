@@ -1278,7 +1278,7 @@ struct kssdgpu_index {
     uint32_t j_nchunks = 0, j_nitems = 0;
     uint32_t j_chunk_size = 32;             // groups per set-major chunk (1..255)
     bool j_sort_chunks = true;              // chunks ordered by group count, largest first
-    uint32_t j_flat_max = 2;                // small groups of up to this many genomes joined flat (1: none)
+    uint32_t j_flat_max = 1;                // small groups of up to this many genomes joined flat (1: none)
     FlatClasses j_flat{};                   // the flat classes of the plan
     DevBuf<uint32_t> j_fheads;              // their run heads, one word per 32 groups
     bool j_tuned = false;                   // the autotuner ran for this index
@@ -1745,6 +1745,35 @@ cudaError_t launch_sets(kssdgpu_index *ix, unsigned long long *oc, unsigned long
     return e != cudaSuccess ? e : cudaGetLastError();
 }
 
+// One step of the self join on counters oc / oo: zero fill (when `zero`), then the
+// set-major launch.  The join launches programmatically after k_zero_pair when the
+// fill stays in L2: hiding the join's launch and first loads under a fill of a few
+// microseconds shortens the 2,000-genome step by 4 us (of 32); after fills of hundreds
+// of microseconds (20,000 genomes: 3.2 GB) it measured 22 us slower, so there the
+// launches stay serialized.
+cudaError_t join_step(kssdgpu_index *ix, bool zero, unsigned long long *oc, unsigned long long *oo, cudaStream_t st)
+{
+    const size_t cells = (size_t)ix->nref * (ix->nref - 1) / 2;
+    bool after_fill = false;
+    if (zero) {
+        const size_t words = std::max<size_t>(cells, 1);
+        cudaError_t e;
+        if ((((uintptr_t)oc | (uintptr_t)oo) & 15) == 0) {
+            // both counter arrays in one launch, 16-byte stores
+            k_zero_pair<<<ix->sms * 8, 256, 0, st>>>(oc, oo, words);
+            count_launch();
+            e = cudaGetLastError();
+            after_fill = cells * 16 <= (size_t)ix->l2_bytes;
+        } else {
+            e = cudaMemsetAsync(oc, 0, words * 8, st);
+            if (e == cudaSuccess) e = cudaMemsetAsync(oo, 0, words * 8, st);
+        }
+        if (e != cudaSuccess)
+            return e;
+    }
+    return launch_sets(ix, oc, oo, st, after_fill);
+}
+
 cudaError_t set_major_plan(kssdgpu_index *ix, uint32_t n, cudaStream_t st)
 {
     ix->j_chunk_size = env_u32("KSSDGPU_JOIN_CHUNK", ix->j_chunk_size, 1, 255);
@@ -1907,11 +1936,11 @@ cudaError_t set_major_plan(kssdgpu_index *ix, uint32_t n, cudaStream_t st)
 }
 
 // Autotuner of the set-major join: candidate plans (largest flat group size, then
-// groups per chunk and chunk order at the best flat size) are built and timed on
-// scratch counters (CUDA events, best of three after one warm-up run, each run after
-// a write of twice the L2 size so that the postings come from HBM as in a one-shot
-// call; the scratch counters are zeroed once: accumulating into nonzero counters
-// costs the same); the fastest stays.  Runs once per index, on request
+// groups per chunk and chunk order at the best flat size) are built and each timed
+// as a whole step on scratch counters, zero fill and join (CUDA events, best of three
+// after one warm-up run, each run after a write of twice the L2 size so that the
+// postings come from HBM as in a one-shot call; the fill is timed because the join
+// overlaps it); the fastest stays.  Runs once per index, on request
 // (kssdgpu_self_plan_tune) or at plan time with KSSDGPU_TUNE=1; keeps the defaults
 // when a knob is pinned by its environment variable or when the scratch would take
 // more than a quarter of the free device memory.
@@ -1938,8 +1967,6 @@ cudaError_t tune_join(kssdgpu_index *ix, uint32_t n, cudaStream_t st)
     if (e == cudaSuccess) e = cudaMalloc(&flush, flush_b);
     if (e == cudaSuccess) e = cudaEventCreate(&ev0);
     if (e == cudaSuccess) e = cudaEventCreate(&ev1);
-    if (e == cudaSuccess) e = cudaMemsetAsync(oc, 0, cells * 8, st);
-    if (e == cudaSuccess) e = cudaMemsetAsync(oo, 0, cells * 8, st);
     float best = 1e30f;
     uint32_t best_size = ix->j_chunk_size, best_flat = ix->j_flat_max;
     bool best_sort = ix->j_sort_chunks;
@@ -1953,7 +1980,7 @@ cudaError_t tune_join(kssdgpu_index *ix, uint32_t n, cudaStream_t st)
         for (int r = 0; r < 4 && e == cudaSuccess; ++r) {
             e = cudaMemsetAsync(flush, r, flush_b, st);
             if (e == cudaSuccess) e = cudaEventRecord(ev0, st);
-            if (e == cudaSuccess) e = launch_sets(ix, oc, oo, st);
+            if (e == cudaSuccess) e = join_step(ix, true, oc, oo, st);
             if (e == cudaSuccess) e = cudaEventRecord(ev1, st);
             if (e == cudaSuccess) e = cudaEventSynchronize(ev1);
             float ms = 0;
@@ -2085,27 +2112,7 @@ int self_lower_dev_impl(kssdgpu_index *ix, unsigned flags, unsigned long long *o
     int rc = self_plan(ix, st);
     if (rc)
         return rc;
-    const size_t cells = (size_t)ix->nref * (ix->nref - 1) / 2;
-    // The join launches programmatically after k_zero_pair when the fill stays in L2:
-    // hiding the join's launch and first loads under a fill of a few microseconds
-    // shortens the 2,000-genome step by 4 us (of 32); after fills of hundreds of
-    // microseconds (20,000 genomes: 3.2 GB) it measured 22 us slower, so there the
-    // launches stay serialized.
-    bool after_fill = false;
-    if (!(flags & KSSDGPU_NO_ZERO)) {
-        const size_t words = std::max<size_t>(cells, 1);
-        if ((((uintptr_t)oc | (uintptr_t)oo) & 15) == 0) {
-            // both counter arrays in one launch, 16-byte stores
-            k_zero_pair<<<ix->sms * 8, 256, 0, st>>>(oc, oo, words);
-            count_launch();
-            CUDA_TRY(cudaGetLastError());
-            after_fill = cells * 16 <= (size_t)ix->l2_bytes;
-        } else {
-            CUDA_TRY(cudaMemsetAsync(oc, 0, words * 8, st));
-            CUDA_TRY(cudaMemsetAsync(oo, 0, words * 8, st));
-        }
-    }
-    CUDA_TRY(launch_sets(ix, oc, oo, st, after_fill));
+    CUDA_TRY(join_step(ix, !(flags & KSSDGPU_NO_ZERO), oc, oo, st));
     if (ix->j_n[1]) {
         k_self_big<<<(unsigned)(((uint64_t)ix->j_n[1] * 32 + 255) / 256), 256, 0, st>>>(ix->j_big.p, ix->j_n[1], ix->post,
                                                                                        oc, oo);
@@ -2649,7 +2656,7 @@ int kssdgpu_self_plan_info(kssdgpu_index_t *ix, uint64_t *groups, uint64_t *post
 }
 
 int kssdgpu_self_plan_tune(kssdgpu_index_t *ix, uint32_t *chunk_groups, int *sorted, uint32_t *flat_groups,
-                           int *candidates, float *join_ms)
+                           int *candidates, float *step_ms)
 {
     if (!ix)
         return fail(KSSDGPU_ERR_ARG, "null index");
@@ -2667,7 +2674,7 @@ int kssdgpu_self_plan_tune(kssdgpu_index_t *ix, uint32_t *chunk_groups, int *sor
     if (sorted) *sorted = ix->j_sort_chunks ? 1 : 0;
     if (flat_groups) *flat_groups = ix->j_flat_max;
     if (candidates) *candidates = ix->j_tune_tried;
-    if (join_ms) *join_ms = ix->j_tune_ms;
+    if (step_ms) *step_ms = ix->j_tune_ms;
     return KSSDGPU_OK;
 }
 

@@ -417,7 +417,7 @@ class Index:
         _check(gpu_lib().kssdgpu_self_plan_tune(self._h, C.byref(c), C.byref(so), C.byref(f), C.byref(n),
                                                 C.byref(ms)))
         return dict(chunk_groups=c.value, sorted=bool(so.value), flat_groups=f.value, candidates=n.value,
-                    join_ms=ms.value)
+                    step_ms=ms.value)
 
     def self_plan_info(self):
         g, p, q = C.c_uint64(), C.c_uint64(), C.c_uint64()

@@ -157,7 +157,7 @@ def test_self_join_autotuner_keeps_counts(monkeypatch):
     rec = oracle.build_index(sk.keys, sk.offs)
     idx = kssdgpu.Index.from_records(rec, sk.n)
     t = idx.self_plan_tune()
-    assert t["candidates"] == 9 and 1 <= t["flat_groups"] <= 4 and t["join_ms"] > 0
+    assert t["candidates"] == 9 and 1 <= t["flat_groups"] <= 4 and t["step_ms"] > 0
     want = oracle.self_lower_all(rec, sk.keys, sk.offs)
     got = idx.self_lower()
     np.testing.assert_array_equal(got[0], want[0])
