@@ -195,7 +195,11 @@ int kssdgpu_self_lower(kssdgpu_index_t *idx, unsigned flags, kssdgpu_ctx_mut2_t 
  */
 int kssdgpu_self_votes(kssdgpu_index_t *idx, const uint64_t *keys, const uint64_t *offs, uint32_t max_ctx_freq,
                        uint32_t sample_step, uint32_t *votes, uint32_t *first);
-/* Device form of kssdgpu_self_lower (outputs in HBM, stream-ordered). */
+/* Device form of kssdgpu_self_lower (outputs in HBM, stream-ordered).  Where the
+ * dense counters outgrow L2 the join adds into per-index compact counters while the
+ * zero fill runs on an internal stream that waits for the caller's earlier work; the
+ * call's last operation on `stream` waits for both.  Calls on one index that overlap
+ * on the GPU share those compact counters: order them on one stream. */
 int kssdgpu_self_lower_dev(kssdgpu_index_t *idx, unsigned flags, kssdgpu_ctx_mut2_t *d_ctx_lower,
                            kssdgpu_obj_section_t *d_obj_lower, void *stream);
 

@@ -913,6 +913,73 @@ __global__ void k_set_items(const ulonglong2 *__restrict__ chunks, uint32_t nchu
     }
 }
 
+// Compact counters.  Every item's counter cell is known when the plan is built, and
+// the touched cells are few (a genome shares contexts with a handful of others), so
+// the join can add into one compact slot per touched cell (L2-resident) while the
+// dense zero fill runs beside it on another stream; a scatter then adds the compact
+// counters into the dense arrays.  Cell of every item lane (empty lanes sort last):
+__global__ void k_item_cells(const unsigned long long *__restrict__ items, uint32_t nitems,
+                             const uint64_t *__restrict__ jt, unsigned long long *__restrict__ cell,
+                             uint32_t *__restrict__ lane)
+{
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nitems; t += gridDim.x * blockDim.x) {
+        const unsigned long long it = items[t];
+        const uint32_t m = (uint32_t)(it >> 34) & 0xFFu, k = (uint32_t)(it >> 42) & 0x3Fu;
+        unsigned long long c = ~0ull;
+        if (m) {
+            const uint32_t i = (uint32_t)(it >> 48) & 0x1Fu, j = (uint32_t)(it >> 53) & 0x1Fu;
+            const uint32_t slot = (uint32_t)(it >> 58) & 0x1Fu;
+            const uint64_t *g = jt + (it & (kSetItemMaxOffset - 1)) + slot * k;
+            const uint32_t gi = (uint32_t)(g[i] >> 32), gj = (uint32_t)(g[j] >> 32);
+            c = lower_cell(gj, gi);
+        }
+        cell[t] = c;
+        lane[t] = t;
+    }
+}
+
+// heads of the distinct touched cells in the sorted cell list
+__global__ void k_touched_heads(const unsigned long long *__restrict__ cell, uint32_t n, uint32_t *__restrict__ heads)
+{
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x)
+        heads[s] = cell[s] != ~0ull && (s == 0 || cell[s] != cell[s - 1]);
+}
+
+// Compact slot layout: slot s holds its ctx word at s * kCompactStride and its obj
+// word right after it (20,000 genomes: strides of 2 / 4 / 16 words measured a 153 /
+// 156 / 161 us join).
+#ifndef KSSD_COMPACT_STRIDE
+#define KSSD_COMPACT_STRIDE 2
+#endif
+constexpr uint32_t kCompactStride = KSSD_COMPACT_STRIDE;
+
+// each item lane's compact slot (as the word offset of its ctx word), and the dense
+// cell of every slot
+__global__ void k_touched_slots(const unsigned long long *__restrict__ cell, const uint32_t *__restrict__ lane,
+                                const uint32_t *__restrict__ heads, const uint32_t *__restrict__ incl, uint32_t n,
+                                uint32_t *__restrict__ islot, unsigned long long *__restrict__ touched)
+{
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+        if (cell[s] == ~0ull)
+            continue;
+        islot[lane[s]] = (incl[s] - 1) * kCompactStride;
+        if (heads[s])
+            touched[incl[s] - 1] = cell[s];
+    }
+}
+
+// dense counters += compact counters (distinct cells: no two threads share one)
+__global__ void k_scatter_touched(const unsigned long long *__restrict__ touched, uint32_t n,
+                                  const unsigned long long *__restrict__ acc, unsigned long long *__restrict__ oc,
+                                  unsigned long long *__restrict__ oo)
+{
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+        const size_t c = touched[s];
+        oc[c] += acc[(size_t)s * kCompactStride];
+        oo[c] += acc[(size_t)s * kCompactStride + 1];
+    }
+}
+
 // The set-major join: one thread per (chunk, pair) item.  The m groups of the chunk
 // share their gid list, so the pair's counter cell is the same for all of them:
 // sum num_ctx (= m), mut2, diff_obj and section over the groups, then one atomic
@@ -926,7 +993,8 @@ __global__ void k_set_items(const ulonglong2 *__restrict__ chunks, uint32_t nchu
 #endif
 constexpr int kSetUnroll = KSSD_SET_UNROLL;
 __device__ __forceinline__ void self_set_item(uint32_t t, const unsigned long long *__restrict__ items, uint32_t nitems,
-                                              const uint64_t *__restrict__ jt, unsigned long long *__restrict__ oc,
+                                              const uint64_t *__restrict__ jt, const uint32_t *__restrict__ islot,
+                                              unsigned long long *__restrict__ oc,
                                               unsigned long long *__restrict__ oo)
 {
     if (t >= nitems)
@@ -954,7 +1022,7 @@ __device__ __forceinline__ void self_set_item(uint32_t t, const unsigned long lo
         dobj += d > 0;
         sect += d;
     }
-    const size_t cell = lower_cell(gj, gi);
+    const size_t cell = islot ? (size_t)__ldg(islot + t) : lower_cell(gj, gi);  // compact slot or dense cell
     pdl_wait_primary();
     atomicAdd(oc + cell, (unsigned long long)m | ((unsigned long long)mut2 << 32));
     if (dobj)
@@ -1069,13 +1137,14 @@ __device__ __forceinline__ bool flat_class_block(const FlatClasses &fc, const ui
 // the flat classes (largest size first), so that the latter fill the former's tail.
 __global__ void __launch_bounds__(256, KSSD_SET_MINB) k_self_sets(const unsigned long long *__restrict__ items, uint32_t nitems,
                                                    uint32_t set_blocks, const uint64_t *__restrict__ jt,
+                                                   const uint32_t *__restrict__ islot,
                                                    const uint64_t *__restrict__ jp,
                                                    const FlatClasses fc, const uint32_t *__restrict__ fheads,
                                                    unsigned long long *__restrict__ oc,
                                                    unsigned long long *__restrict__ oo)
 {
     if (blockIdx.x < set_blocks) {
-        self_set_item(blockIdx.x * blockDim.x + threadIdx.x, items, nitems, jt, oc, oo);
+        self_set_item(blockIdx.x * blockDim.x + threadIdx.x, items, nitems, jt, islot, oc, oo);
         return;
     }
     static_assert(kFlatMax == 4, "one dispatch per flat class");
@@ -1275,6 +1344,14 @@ struct kssdgpu_index {
     DevBuf<ulonglong2> j_chunks;            // set-major chunks of the small groups
     DevBuf<unsigned long long> j_items;     // (chunk, pair) work items, tile by tile (one warp each)
     DevBuf<uint64_t> j_tile;                // postings of the item chunks, row-interleaved by tile
+    bool j_compact_ok = true;               // compact counters allowed (KSSDGPU_JOIN_COMPACT=0: never)
+    bool j_compact = false;                 // the plan adds into compact slots of the touched cells
+    uint32_t j_ntouched = 0;                // touched lower cells
+    DevBuf<uint32_t> j_islot;               // compact slot of every item lane
+    DevBuf<unsigned long long> j_touched;   // dense cell of every compact slot
+    DevBuf<unsigned long long> j_cacc;      // compact counters, kCompactStride words per slot
+    cudaStream_t j_fill_st = nullptr;       // the dense zero fill beside a compact join
+    cudaEvent_t j_fill_ev[2] = {nullptr, nullptr};
     uint32_t j_nchunks = 0, j_nitems = 0;
     uint32_t j_chunk_size = 32;             // groups per set-major chunk (1..255)
     bool j_sort_chunks = true;              // chunks ordered by group count, largest first
@@ -1700,8 +1777,9 @@ int count_host_impl(kssdgpu_index *ix, const uint64_t *qkeys, const uint64_t *qo
 // Runs of equal gid lists among the n sorted small groups -> chunks -> (chunk, pair)
 // items (j_chunks, j_items); the per-group descriptors are released afterwards.
 // Plan knobs, overridable for tuning: KSSDGPU_JOIN_CHUNK (groups per chunk, 1..255)
-// , KSSDGPU_JOIN_SORT (0: chunks by size only, plan order within a size) and KSSDGPU_JOIN_FLAT (largest group
-// size joined flat, 1..4; 1: every small group as chunk items).
+// , KSSDGPU_JOIN_SORT (0: chunks by size only, plan order within a size), KSSDGPU_JOIN_FLAT (largest group
+// size joined flat, 1..4; 1: every small group as chunk items) and KSSDGPU_JOIN_COMPACT (0: the
+// join always adds into the dense counters; 2: compact slots whenever possible).
 uint32_t env_u32(const char *name, uint32_t def, uint32_t lo, uint32_t hi)
 {
     const char *v = std::getenv(name);
@@ -1714,7 +1792,7 @@ uint32_t env_u32(const char *name, uint32_t def, uint32_t lo, uint32_t hi)
 // One launch of the set-major join: the plan's (chunk, pair) items, then its flat
 // classes, largest size first.
 cudaError_t launch_sets(kssdgpu_index *ix, unsigned long long *oc, unsigned long long *oo, cudaStream_t st,
-                        bool after_zero = false)
+                        bool after_zero = false, bool compact = false)
 {
     FlatClasses fc = ix->j_flat;
     const uint32_t sb = (ix->j_nitems + 255) / 256;
@@ -1739,8 +1817,10 @@ cudaError_t launch_sets(kssdgpu_index *ix, unsigned long long *oc, unsigned long
         cfg.numAttrs = 1;
     }
     const cudaError_t e = cudaLaunchKernelEx(&cfg, k_self_sets, (const unsigned long long *)ix->j_items.p, ix->j_nitems,
-                                             sb, (const uint64_t *)ix->j_tile.p, (const uint64_t *)ix->j_post.p, fc,
-                                             (const uint32_t *)ix->j_fheads.p, oc, oo);
+                                             sb, (const uint64_t *)ix->j_tile.p,
+                                             compact ? (const uint32_t *)ix->j_islot.p : (const uint32_t *)nullptr,
+                                             (const uint64_t *)ix->j_post.p, fc, (const uint32_t *)ix->j_fheads.p, oc,
+                                             oo);
     count_launch();
     return e != cudaSuccess ? e : cudaGetLastError();
 }
@@ -1754,6 +1834,41 @@ cudaError_t launch_sets(kssdgpu_index *ix, unsigned long long *oc, unsigned long
 cudaError_t join_step(kssdgpu_index *ix, bool zero, unsigned long long *oc, unsigned long long *oo, cudaStream_t st)
 {
     const size_t cells = (size_t)ix->nref * (ix->nref - 1) / 2;
+    if (ix->j_compact && ix->j_ntouched) {
+        // compact counters: the fill (on j_fill_st, after the caller's earlier work)
+        // runs beside the join; the scatter waits for both
+        const uint32_t T = ix->j_ntouched;
+        cudaError_t e = cudaSuccess;
+        if (zero) {
+            if (!ix->j_fill_st) e = cudaStreamCreateWithFlags(&ix->j_fill_st, cudaStreamNonBlocking);
+            for (int i = 0; i < 2 && e == cudaSuccess; ++i)
+                if (!ix->j_fill_ev[i]) e = cudaEventCreateWithFlags(&ix->j_fill_ev[i], cudaEventDisableTiming);
+            if (e == cudaSuccess) e = cudaEventRecord(ix->j_fill_ev[0], st);
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(ix->j_fill_st, ix->j_fill_ev[0], 0);
+            const size_t words = std::max<size_t>(cells, 1);
+            if (e == cudaSuccess) {
+                if ((((uintptr_t)oc | (uintptr_t)oo) & 15) == 0) {
+                    k_zero_pair<<<ix->sms * 8, 256, 0, ix->j_fill_st>>>(oc, oo, words);
+                    count_launch();
+                    e = cudaGetLastError();
+                } else {
+                    e = cudaMemsetAsync(oc, 0, words * 8, ix->j_fill_st);
+                    if (e == cudaSuccess) e = cudaMemsetAsync(oo, 0, words * 8, ix->j_fill_st);
+                }
+            }
+            if (e == cudaSuccess) e = cudaEventRecord(ix->j_fill_ev[1], ix->j_fill_st);
+        }
+        unsigned long long *acc = ix->j_cacc.p;
+        if (e == cudaSuccess) e = cudaMemsetAsync(acc, 0, (size_t)T * kCompactStride * 8, st);
+        if (e == cudaSuccess) e = launch_sets(ix, acc, acc + 1, st, false, true);
+        if (e == cudaSuccess && zero) e = cudaStreamWaitEvent(st, ix->j_fill_ev[1], 0);
+        if (e == cudaSuccess) {
+            k_scatter_touched<<<grid_for(T), 256, 0, st>>>(ix->j_touched.p, T, acc, oc, oo);
+            count_launch();
+            e = cudaGetLastError();
+        }
+        return e;
+    }
     bool after_fill = false;
     if (zero) {
         const size_t words = std::max<size_t>(cells, 1);
@@ -1772,6 +1887,59 @@ cudaError_t join_step(kssdgpu_index *ix, bool zero, unsigned long long *oc, unsi
             return e;
     }
     return launch_sets(ix, oc, oo, st, after_fill);
+}
+
+// Compact slots of a plan of items: the item lanes' cells, sorted; one slot per
+// distinct cell (T of them); every lane's slot and every slot's cell.
+cudaError_t build_compact(kssdgpu_index *ix, uint32_t nitems, uint32_t *ntouched, cudaStream_t st)
+{
+    unsigned long long *k1 = nullptr, *k2 = nullptr;
+    uint32_t *v1 = nullptr, *v2 = nullptr, *hd = nullptr, *inc = nullptr;
+    void *tmp = nullptr;
+    auto cleanup = [&]() {
+        cudaFree(k1); cudaFree(k2); cudaFree(v1); cudaFree(v2); cudaFree(hd); cudaFree(inc); cudaFree(tmp);
+    };
+    size_t tb1 = 0, tb2 = 0;
+    cudaError_t e = cudaMalloc(&k1, (size_t)nitems * 8);
+    if (e == cudaSuccess) e = cudaMalloc(&k2, (size_t)nitems * 8);
+    if (e == cudaSuccess) e = cudaMalloc(&v1, (size_t)nitems * 4);
+    if (e == cudaSuccess) e = cudaMalloc(&v2, (size_t)nitems * 4);
+    if (e == cudaSuccess) e = cudaMalloc(&hd, (size_t)nitems * 4);
+    if (e == cudaSuccess) e = cudaMalloc(&inc, (size_t)nitems * 4);
+    if (e == cudaSuccess) e = cub::DeviceRadixSort::SortPairs(nullptr, tb1, k1, k2, v1, v2, nitems, 0, 64, st);
+    if (e == cudaSuccess) e = cub::DeviceScan::InclusiveSum(nullptr, tb2, hd, inc, nitems, st);
+    const size_t tb = std::max<size_t>(std::max(tb1, tb2), 1);
+    if (e == cudaSuccess) e = cudaMalloc(&tmp, tb);
+    if (e == cudaSuccess) {
+        k_item_cells<<<grid_for(nitems), 256, 0, st>>>(ix->j_items.p, nitems, ix->j_tile.p, k1, v1);
+        count_launch();
+        size_t b = tb;
+        e = cub::DeviceRadixSort::SortPairs(tmp, b, k1, k2, v1, v2, nitems, 0, 64, st);
+        count_launch(8);
+    }
+    if (e == cudaSuccess) {
+        k_touched_heads<<<grid_for(nitems), 256, 0, st>>>(k2, nitems, hd);
+        count_launch();
+        size_t b = tb;
+        e = cub::DeviceScan::InclusiveSum(tmp, b, hd, inc, nitems, st);
+        count_launch(2);
+    }
+    uint32_t T = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&T, inc + nitems - 1, 4, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e == cudaSuccess) e = ix->j_islot.ensure(nitems);
+    if (e == cudaSuccess) e = ix->j_touched.ensure(T);
+    if (e == cudaSuccess && (uint64_t)T * kCompactStride >= (1ull << 32))
+        e = cudaErrorMemoryAllocation;  // slot word offsets are 32-bit
+    if (e == cudaSuccess) e = ix->j_cacc.ensure((size_t)T * kCompactStride);
+    if (e == cudaSuccess) {
+        k_touched_slots<<<grid_for(nitems), 256, 0, st>>>(k2, v2, hd, inc, nitems, ix->j_islot.p, ix->j_touched.p);
+        count_launch();
+        e = cudaStreamSynchronize(st);
+    }
+    cleanup();
+    *ntouched = e == cudaSuccess ? T : 0;
+    return e;
 }
 
 cudaError_t set_major_plan(kssdgpu_index *ix, uint32_t n, cudaStream_t st)
@@ -1924,8 +2092,26 @@ cudaError_t set_major_plan(kssdgpu_index *ix, uint32_t n, cudaStream_t st)
         count_launch(2);
         e = cudaStreamSynchronize(st);
     }
+    // Compact counters for plans of items only (the flat path adds into dense cells),
+    // while the touched cells are at most half of the lower triangle, and only where
+    // the dense counters outgrow L2: there the fill takes hundreds of microseconds and
+    // running it beside the join pays (20,000 genomes: step 0.65 vs 0.73 ms); a fill
+    // that fits in L2 overlaps the join through the dependent launch instead, and the
+    // compact path's extra memset and scatter launches cost more than they save there
+    // (2,000 genomes: 34.8 vs 25.6 us).  KSSDGPU_JOIN_COMPACT=2 forces it (tests).
+    const uint32_t compact_env = env_u32("KSSDGPU_JOIN_COMPACT", 1, 0, 2);
+    ix->j_compact_ok = compact_env != 0;
+    const bool big_fill = (uint64_t)ix->nref * (ix->nref - 1) / 2 * 16 > (uint64_t)ix->l2_bytes || compact_env == 2;
+    bool compact = false;
+    uint32_t ntouched = 0;
+    if (e == cudaSuccess && ix->j_compact_ok && big_fill && flat_max < 2 && nitems) {
+        e = build_compact(ix, (uint32_t)nitems, &ntouched, st);
+        compact = e == cudaSuccess && ntouched && 2 * (uint64_t)ntouched <= (uint64_t)ix->nref * (ix->nref - 1) / 2;
+    }
     cleanup();
     if (e == cudaSuccess) {
+        ix->j_compact = compact;
+        ix->j_ntouched = compact ? ntouched : 0;
         ix->j_nchunks = nchunks;
         ix->j_nitems = (uint32_t)nitems;
         for (uint32_t k = 2; k <= kFlatMax; ++k)
@@ -2367,6 +2553,14 @@ void kssdgpu_index_free(kssdgpu_index_t *ix)
     ix->j_chunks.release();
     ix->j_items.release();
     ix->j_tile.release();
+    ix->j_islot.release();
+    ix->j_touched.release();
+    ix->j_cacc.release();
+    if (ix->j_fill_st)
+        cudaStreamDestroy(ix->j_fill_st);
+    for (cudaEvent_t e : ix->j_fill_ev)
+        if (e)
+            cudaEventDestroy(e);
     ix->j_fheads.release();
     ix->j_big.release();
     ix->j_conf.release();

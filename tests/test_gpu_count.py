@@ -150,6 +150,35 @@ def test_self_join_plan_settings(monkeypatch, flat, chunk, srt, kind):
     assert (t["flat_groups"], t["chunk_groups"], t["sorted"], t["candidates"]) == (flat, chunk, bool(srt), 0)
 
 
+@pytest.mark.parametrize("kind", ["pairs", "wide"])
+@pytest.mark.parametrize("compact", [0, 2])
+def test_self_join_compact_counters(monkeypatch, kind, compact):
+    """Plans of items only add into compact slots of the touched cells while the dense
+    fill runs on a second stream, then scatter (by default only where the dense
+    counters outgrow L2; KSSDGPU_JOIN_COMPACT=2 forces it here); with
+    KSSDGPU_JOIN_COMPACT=0 they add into the dense cells.  Both give the oracle's
+    counters, overwrite stale device counters, and accumulate with KSSDGPU_NO_ZERO."""
+    import torch
+    monkeypatch.setenv("KSSDGPU_JOIN_FLAT", "1")
+    monkeypatch.setenv("KSSDGPU_JOIN_COMPACT", str(compact))
+    sk = _clustered_sketch(kind)
+    rec = oracle.build_index(sk.keys, sk.offs)
+    idx = kssdgpu.Index.from_records(rec, sk.n)
+    want = oracle.self_lower_all(rec, sk.keys, sk.offs)
+    cells = sk.n * (sk.n - 1) // 2
+    d_c = torch.full((cells,), 0x3C3C3C3C3C3C3C3C, dtype=torch.int64, device="cuda")
+    d_o = torch.full((cells,), -7, dtype=torch.int64, device="cuda")
+    for _ in range(2):
+        idx.self_lower_dev(d_c, d_o)
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(d_c.cpu().numpy().view(np.uint32).reshape(-1, 2), want[0])
+        np.testing.assert_array_equal(d_o.cpu().numpy().view(np.uint32).reshape(-1, 2), want[1])
+    idx.self_lower_dev(d_c, d_o, flags=kssdgpu.NO_ZERO)  # adds a second copy of every count
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(d_c.cpu().numpy().view(np.uint32).reshape(-1, 2), 2 * want[0])
+    np.testing.assert_array_equal(d_o.cpu().numpy().view(np.uint32).reshape(-1, 2), 2 * want[1])
+
+
 def test_self_join_autotuner_keeps_counts(monkeypatch):
     for v in ("KSSDGPU_JOIN_FLAT", "KSSDGPU_JOIN_CHUNK", "KSSDGPU_JOIN_SORT"):
         monkeypatch.delenv(v, raising=False)
