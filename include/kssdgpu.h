@@ -90,6 +90,11 @@ int kssdgpu_index_from_sketch(const uint64_t *keys, const uint64_t *offs, int nr
 
 void kssdgpu_index_free(kssdgpu_index_t *idx);
 
+/* Calls on one index handle share its per-index device scratch (plans, work lists,
+ * compact counters): do not make them from several host threads at once, and do
+ * not let them overlap on the GPU (order them on one stream).  Different handles are
+ * independent; the server (kssdgpu_server_*) serialises its own calls. */
+
 /* Facts of a built index: records, unique contexts, references, object bits. */
 int kssdgpu_index_info(const kssdgpu_index_t *idx, uint64_t *records, uint64_t *contexts,
                        int *nref, int *obj_bits);
