@@ -11,11 +11,19 @@ full matrix): the lower triangle of shared-context counters for every pair;
 genome-pairs = n^2 matrix cells per step.
 
 Arms:
-  ours (default)   value: device-resident step (self join over the resident index,
-                   counters zeroed and rebuilt each step); e2e: the reference-facing
-                   C-ABI call kssdgpu_count_lower with pinned HOST buffers (query keys
-                   H2D, dense counters D2H) every step; plus the plain one-query-per-
-                   launch kernel and the batched persistent probe kernel beside it.
+  ours (default)   value: one self step from the resident index per timed step --
+                   zero fill of the dense lower triangle plus the one-pass scan join
+                   (every context group's bounds read, every shared context joined;
+                   nothing cached between steps); e2e: the reference-facing C-ABI call
+                   kssdgpu_count_lower with HOST buffers (query keys H2D, dense
+                   counters D2H) every step, pinned in one call, and as the reference's
+                   drivers call it (64-query blocks, pageable buffers); beside it the
+                   batched probe kernel, the plain one-query-per-launch kernel, the
+                   cached-plan join, and (unless --no-extra) the 20,000-genome
+                   all-vs-all, a 10,000-query x 20,000-reference block, 40 read sets
+                   with unique contexts and a short serving sweep against the resident
+                   20,000-genome index, each with parity against the reference's own
+                   counting function on a sample.
   reference        the reference's own count_ctx_obj_frm_comb_sketch_section_lower
                    (compiled from its sources into oracle/_ref) over blocks of 64
                    queries with all host threads; rank 0 only.
@@ -26,6 +34,7 @@ from __future__ import annotations
 import argparse
 import json
 import os
+import random
 import subprocess
 import sys
 import threading
@@ -41,13 +50,13 @@ WORKLOAD = dict(name="self-ani-matrix-2000-genomes", n_samples=2000, n_clusters=
 BLOCK = 64  # the reference's self-matrix query block (src/command_ani.c:1498-1531)
 
 
-def make_workload(n: int):
+def make_workload(n: int, lib=None):
     import kssdgpu
     w = dict(WORKLOAD)
-    return kssdgpu.synth(n_samples=n, n_clusters=max(1, n // 10), size_dist=kssdgpu.SIZE_LOGNORMAL,
+    return kssdgpu.synth(lib=lib, n_samples=n, n_clusters=max(1, n // 10), size_dist=kssdgpu.SIZE_LOGNORMAL,
                          len_median=w["len_median"], len_sigma=w["len_sigma"], len_min=w["len_min"],
                          len_max=w["len_max"], sub_lo=w["sub_lo"], sub_hi=w["sub_hi"], seed=w["seed"],
-                         sample_seed=w["seed"])
+                         sample_seed=w["seed"], threads=os.cpu_count() or 8)
 
 
 def cpu_count_lower_blocks(sk, rec, blocks, threads, use_ref):
@@ -137,12 +146,107 @@ def replica_value(world, units, seconds):
     return world * units / seconds
 
 
+def probe_model_bytes(n_keys, postings_walked, cells):
+    """The per-query probe model of the counting kernels: 8 B per query key, 12 B per
+    index posting walked (the reference's ctxgidobj_t record), 16 B per counter cell."""
+    return 8 * n_keys + 12 * postings_walked + 16 * cells
+
+
+def scan_join_bytes(contexts, shared_postings, touched):
+    """Distinct bytes of the one-pass scan join: every context group's bounds (4 B per
+    group + 1), the postings of groups of >= 2 (8 B each) and the touched counter cells
+    read and written once (2 x 16 B)."""
+    return 4 * (contexts + 1) + 8 * shared_postings + 2 * 16 * touched
+
+
+def lower_equals_dense(lower_c, lower_o, dense_c, dense_o, n, rows=1024):
+    """Packed lower triangle == the strictly-lower part of the dense [n][n] counters
+    (compared in row blocks on the device)."""
+    import torch
+    dc, do = dense_c.view(n, n), dense_o.view(n, n)
+    for a in range(0, n, rows):
+        b = min(n, a + rows)
+        r = torch.arange(a, b, device=dc.device).unsqueeze(1)
+        c = torch.arange(0, b, device=dc.device).unsqueeze(0)
+        m = c < r
+        lo, hi = a * (a - 1) // 2 if a else 0, b * (b - 1) // 2
+        if not (torch.equal(dc[a:b, :b][m], lower_c[lo:hi]) and torch.equal(do[a:b, :b][m], lower_o[lo:hi])):
+            return False
+    return True
+
+
+class Timer:
+    """CUDA-event timing on one stream, an L2 flush (a 256 MB write, above the 126 MB
+    L2) before every timed call."""
+
+    def __init__(self, stream, device):
+        import torch
+        self.torch = torch
+        self.stream = stream
+        self.flush = torch.empty(256 << 20, dtype=torch.uint8, device=device)
+
+    def __call__(self, fn, steps, warmup, pre=None, flush_l2=True):
+        torch = self.torch
+        for _ in range(warmup):
+            if pre:
+                pre()
+            fn()
+        torch.cuda.synchronize()
+        tot = []
+        for _ in range(steps):
+            if flush_l2:
+                self.flush.fill_(1)
+            if pre:
+                pre()
+            s = torch.cuda.Event(enable_timing=True)
+            e = torch.cuda.Event(enable_timing=True)
+            s.record(self.stream)
+            fn()
+            e.record(self.stream)
+            e.synchronize()
+            tot.append(s.elapsed_time(e))
+        torch.cuda.synchronize()
+        return float(np.mean(tot))  # ms
+
+
+def density_histogram(d_lc, sizes, n, tile=128):
+    """Shared-context density of the all-vs-all matrix per 128 x 128 genome tile, in
+    gid order and with the genomes grouped by cluster (the best case for a dense
+    tile): credits / (tile cells x mean sketch size), i.e. the fraction of a dense
+    int8 context-by-genome GEMM's multiply-adds that land on a shared context."""
+    import torch
+    num_ctx = (d_lc & 0xFFFFFFFF).to(torch.float64)
+    full = torch.zeros(n, n, dtype=torch.float64, device=d_lc.device)
+    tri = torch.tril_indices(n, n, -1, device=d_lc.device)
+    full[tri[0], tri[1]] = num_ctx
+    full = full + full.T
+    mean_size = float(np.mean(sizes))
+    out = {}
+    for name, order in (("gid_order", torch.arange(n, device=d_lc.device)),
+                        ("cluster_order", torch.argsort(torch.arange(n, device=d_lc.device) % max(1, n // 10),
+                                                        stable=True))):
+        m = full[order][:, order]
+        nt = (n + tile - 1) // tile
+        pad = nt * tile - n
+        m = torch.nn.functional.pad(m, (0, pad, 0, pad))
+        t = m.view(nt, tile, nt, tile).sum(dim=(1, 3)) / (tile * tile * mean_size)
+        t = t[torch.triu_indices(nt, nt, 0, device=t.device).unbind(0)]
+        edges = [0, 1e-6, 1e-5, 1e-4, 1e-3, 1e-2, 0.1, 1.0]
+        hist = [int(((t >= lo) & (t < hi)).sum().item()) for lo, hi in zip(edges[:-1], edges[1:])]
+        out[name] = {"tiles": int(t.numel()), "max": float(t.max().item()), "mean": float(t.mean().item()),
+                     "bins": edges, "counts": hist}
+    return out
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return 0
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import kssdgpu
     import oracle
-    sk = make_workload(args.genomes)
+    # the generator built into the oracle's own library (the product's host library
+    # stays unmapped in this process)
+    sk = make_workload(args.genomes, lib=kssdgpu.bind_synth(oracle.workload_lib()))
     rec = oracle.build_index(sk.keys, sk.offs)
     use_ref = oracle.ref_available()
     threads = os.cpu_count() or 1
@@ -165,15 +269,268 @@ def run_reference(args, rank, world):
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * float(np.mean(times)), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-        "config": {"workload": WORKLOAD["name"], "genomes": sk.n, "entries": int(sk.offs[-1]),
-                   "path": "count_ctx_obj_frm_comb_sketch_section_lower, 64-query blocks",
-                   "blocks_per_step": per_step},
+        "config": {"workload": WORKLOAD["name"], "genomes": sk.n, "entries": int(sk.offs[-1])},
+        "path": "count_ctx_obj_frm_comb_sketch_section_lower, 64-query blocks (-O3 -flto -fopenmp build)",
+        "blocks_per_step": per_step,
         "cpu_baseline": {"value": value, "unit": "genome-pairs/s", "cores": threads, "kind": kind,
                          "sample": f"{per_step} of {nblocks} 64-query blocks per step, rotating"},
         "e2e": {"value": value, "unit": "genome-pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
     return 0
+
+
+def leg_north_star(args, timer, dev, stream, peak):
+    """The 20,000-genome all-vs-all: the self step (fill + scan join) vs the batched
+    probe kernel vs the plain per-query kernel on the same counters (parity checked on
+    the device), and the cached-plan join (first call = plan + join)."""
+    import torch
+    import kssdgpu
+    n = args.ns_genomes
+    t0 = time.perf_counter()
+    sk = make_workload(n)
+    gen_s = time.perf_counter() - t0
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    idx = kssdgpu.Index.from_sketch(sk, device=dev.index or 0)
+    torch.cuda.synchronize()
+    build_s = time.perf_counter() - t0
+    info = idx.info()
+    facts = idx.self_plan_info()
+    cells = n * (n - 1) // 2
+    lc = torch.zeros(cells, dtype=torch.int64, device=dev)
+    lo = torch.zeros_like(lc)
+    step = lambda: idx.self_lower_dev(lc, lo, stream=stream)  # noqa: E731
+    ms_step = timer(step, max(3, args.steps // 2), 3)
+    touched = int(torch.count_nonzero(lc).item())
+    ms_scan = timer(lambda: idx.self_lower_dev(lc, lo, flags=kssdgpu.NO_ZERO, stream=stream), max(3, args.steps // 2),
+                    2, pre=lambda: (lc.zero_(), lo.zero_()))
+    # cached-plan join: the first call builds the plan (host-timed), later calls only join
+    l2c, l2o = torch.zeros_like(lc), torch.zeros_like(lc)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    idx.self_lower_dev(l2c, l2o, flags=kssdgpu.SELF_PLAN, stream=stream)
+    torch.cuda.synchronize()
+    plan_first_ms = 1e3 * (time.perf_counter() - t0)
+    ms_cached = timer(lambda: idx.self_lower_dev(l2c, l2o, flags=kssdgpu.SELF_PLAN, stream=stream), 3, 1)
+    step()
+    torch.cuda.synchronize()
+    same_plan = bool(torch.equal(lc, l2c) and torch.equal(lo, l2o))
+    del l2c, l2o
+    d_keys = torch.from_numpy(sk.keys.view(np.int64)).to(dev)
+    d_offs = torch.from_numpy(sk.offs.view(np.int64)).to(dev)
+    dc = torch.zeros(n * n, dtype=torch.int64, device=dev)
+    do = torch.zeros_like(dc)
+    probe = lambda: idx.count_block_dev(d_keys, d_offs, n, dc, do, lower=True, stream=stream)  # noqa: E731
+    ms_probe = timer(probe, 3, 1)
+    same_probe = lower_equals_dense(lc, lo, dc, do, n)
+    ms_plain = timer(lambda: idx.count_plain_dev(d_keys, d_offs, sk.offs, dc, do, lower=True, stream=stream), 1, 1)
+    same_plain = lower_equals_dense(lc, lo, dc, do, n)
+    scan_bytes = scan_join_bytes(info["contexts"], facts["postings"], touched)
+    step_bytes = scan_bytes + 16 * cells
+    model = probe_model_bytes(int(sk.offs[-1]), facts["pairs"], cells)
+    out = {
+        "workload": f"self-ani-matrix-{n}-genomes", "genomes": n, "entries": int(sk.offs[-1]),
+        "unique_contexts": info["contexts"], "generate_s": gen_s, "index_build_s": build_s,
+        "self_step": {"ms": ms_step, "genome_pairs_s": n * n / (ms_step / 1e3),
+                      "what": "zero fill of the dense lower triangle + one-pass scan join, nothing cached",
+                      "roofline": {"bound": "hbm", "bytes": step_bytes, "achieved": step_bytes / ms_step / 1e6,
+                                   "frac": step_bytes / ms_step / 1e6 / peak},
+                      "probe_model_frac": model / ms_step / 1e6 / peak},
+        "scan_join_alone": {"ms": ms_scan, "bytes": scan_bytes, "frac": scan_bytes / ms_scan / 1e6 / peak},
+        "batched_probe": {"ms": ms_probe, "genome_pairs_s": n * n / (ms_probe / 1e3),
+                          "contexts_probed_per_s": int(sk.offs[-1]) / (ms_probe / 1e3),
+                          "probe_model_frac": model / ms_probe / 1e6 / peak},
+        "plain_per_query": {"ms": ms_plain, "launches": n},
+        "batched_vs_plain": ms_plain / ms_probe, "self_step_vs_plain": ms_plain / ms_step,
+        "cached_plan_join": {"first_call_ms": plan_first_ms, "join_ms": ms_cached},
+        "parity": {"scan_eq_probe": same_probe, "scan_eq_plain": same_plain, "scan_eq_cached_plan": same_plan},
+        "touched_cells": touched,
+    }
+    del dc, do, lc, lo
+    return out, idx, sk
+
+
+def leg_rect(args, timer, dev, stream, peak, idx, ref):
+    """A 10,000-query x 20,000-reference block (queries of log-uniform 50 kbp-12 Mbp
+    from the references' cluster ancestors): one batched launch vs the plain kernel,
+    and the counters of a query sample against the reference's own counting function."""
+    import torch
+    import kssdgpu
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    nr, nq = ref.n, args.rect_queries
+    qry = kssdgpu.synth(n_samples=nq, n_clusters=max(1, nr // 10), role=kssdgpu.ROLE_OWNLEN,
+                        size_dist=kssdgpu.SIZE_LOGNORMAL, len_median=4e6, len_sigma=0.37, len_min=1e6, len_max=12e6,
+                        own_len_min=5e4, own_len_max=12e6, sub_lo=0.001, sub_hi=0.2, seed=WORKLOAD["seed"],
+                        sample_seed=WORKLOAD["seed"] + 11, threads=os.cpu_count() or 8)
+    dk = torch.from_numpy(qry.keys.view(np.int64)).to(dev)
+    do = torch.from_numpy(qry.offs.view(np.int64)).to(dev)
+    cells = nq * nr
+    dc = torch.zeros(cells, dtype=torch.int64, device=dev)
+    dob = torch.zeros_like(dc)
+    ms_b = timer(lambda: idx.count_block_dev(dk, do, nq, dc, dob, stream=stream), 3, 2)
+    shared = int((dc & 0xFFFFFFFF).sum().item())
+    ms_p = timer(lambda: idx.count_plain_dev(dk, do, qry.offs, dc, dob, stream=stream), 1, 0)
+    qkeys = int(qry.offs[-1])
+    model = probe_model_bytes(qkeys, shared, cells)
+    rec, _ = idx.export()
+    sample = list(range(0, nq, max(1, nq // args.parity_queries)))[:args.parity_queries]
+    skeys = np.concatenate([qry.keys[int(qry.offs[q]):int(qry.offs[q + 1])] for q in sample])
+    soffs = np.concatenate([[0], np.cumsum([int(qry.offs[q + 1] - qry.offs[q]) for q in sample])]).astype(np.uint64)
+    t0 = time.perf_counter()
+    c, o = oracle.count_block(rec, nr, skeys, soffs, threads=os.cpu_count() or 1, ref=oracle.ref_available())
+    cpu_s = time.perf_counter() - t0
+    rows = torch.tensor(sample, device=dev)
+    same = bool(np.array_equal(c.view(np.int64).reshape(len(sample), nr), dc.view(nq, nr)[rows].cpu().numpy()) and
+                np.array_equal(o.view(np.int64).reshape(len(sample), nr), dob.view(nq, nr)[rows].cpu().numpy()))
+    del rec, dc, dob
+    return {"workload": f"rect-{nq}x{nr}", "query_keys": qkeys, "ms": ms_b, "genome_pairs_s": cells / (ms_b / 1e3),
+            "contexts_probed_per_s": qkeys / (ms_b / 1e3),
+            "roofline_probe_model": {"bytes": model, "achieved": model / ms_b / 1e6, "frac": model / ms_b / 1e6 / peak},
+            "plain_per_query": {"ms": ms_p, "launches": nq}, "batched_vs_plain": ms_p / ms_b,
+            "parity": {"queries": len(sample), "counts_match_reference": same,
+                       "checker": "reference count_ctx_obj_frm_comb_sketch_section_with_unique"
+                       if oracle.ref_available() else "oracle"},
+            "cpu_baseline": {"value": len(sample) * nr / cpu_s, "unit": "genome-pairs/s", "cores": os.cpu_count(),
+                             "kind": "reference" if oracle.ref_available() else "port",
+                             "sample": f"{len(sample)} queries"}}
+
+
+def leg_reads(args, timer, dev, stream, idx, ref):
+    """40 read sets (1-5 genomes of the reference set at 5-50x, 0.1-1% errors,
+    conflicts kept) against the 20,000-genome index with unique contexts (`ani --qraw
+    ... --unique-ctx --anicut 0.95`): batched vs plain, and the counters of a sample
+    against the reference's own counting function."""
+    import torch
+    import kssdgpu
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    nr, nq = ref.n, args.reads_samples
+    qry = kssdgpu.synth(n_samples=nq, n_clusters=max(1, nr // 10), role=kssdgpu.ROLE_READS,
+                        size_dist=kssdgpu.SIZE_LOGNORMAL, len_median=4e6, len_sigma=0.37, len_min=1e6, len_max=12e6,
+                        sub_lo=0.001, sub_hi=0.2, seed=WORKLOAD["seed"], sample_seed=WORKLOAD["seed"] + 12,
+                        ref_sample_seed=WORKLOAD["seed"], ref_samples=nr, cov_lo=5, cov_hi=50, err_lo=0.001,
+                        err_hi=0.01, threads=os.cpu_count() or 8)
+    dk = torch.from_numpy(qry.keys.view(np.int64)).to(dev)
+    do = torch.from_numpy(qry.offs.view(np.int64)).to(dev)
+    cells = nq * nr
+    outs = [torch.zeros(cells, dtype=torch.int64, device=dev) for _ in range(4)]
+    flags = kssdgpu.UNIQUE
+    ms_b = timer(lambda: idx.count_block_dev(dk, do, nq, *outs, flags=flags, stream=stream), 3, 2)
+    ms_p = timer(lambda: idx.count_plain_dev(dk, do, qry.offs, *outs, flags=flags, stream=stream), 1, 0)
+    rec, _ = idx.export()
+    sample = list(range(0, nq, max(1, nq // 8)))[:8]
+    skeys = np.concatenate([qry.keys[int(qry.offs[q]):int(qry.offs[q + 1])] for q in sample])
+    soffs = np.concatenate([[0], np.cumsum([int(qry.offs[q + 1] - qry.offs[q]) for q in sample])]).astype(np.uint64)
+    want = oracle.count_block(rec, nr, skeys, soffs, unique=True, threads=os.cpu_count() or 1,
+                              ref=oracle.ref_available())
+    rows = torch.tensor(sample, device=dev)
+    same = all(bool(np.array_equal(w.view(np.int64).reshape(len(sample), nr), o.view(nq, nr)[rows].cpu().numpy()))
+               for w, o in zip(want, outs))
+    del rec, outs
+    qkeys = int(qry.offs[-1])
+    return {"workload": f"reads-{nq}x{nr}-unique-ctx", "read_sets": nq, "query_keys": qkeys, "ms": ms_b,
+            "genome_pairs_s": cells / (ms_b / 1e3), "contexts_probed_per_s": qkeys / (ms_b / 1e3),
+            "plain_per_query": {"ms": ms_p, "launches": nq}, "batched_vs_plain": ms_p / ms_b,
+            "parity": {"read_sets": len(sample), "counts_match_reference": same}}
+
+
+def _pct(xs, p):
+    xs = sorted(xs)
+    return float(xs[min(len(xs) - 1, int(p * (len(xs) - 1) + 0.5))]) if xs else None
+
+
+def serve_sweep(idx, nref, rates, seconds, seed, pool_assemblies=256, pool_reads=64, max_batch_queries=64):
+    """Poisson arrivals at each rate for `seconds`: 80% assemblies (0.5-12 Mbp, from the
+    references' cluster ancestors) and 20% read sets (1-5 genomes at 5-100x, 0.1-1%
+    errors); latency = submit -> hits on the host, measured by the server.  Returns
+    (per-rate results, pool facts, server facts)."""
+    import kssdgpu
+    asm = kssdgpu.synth(n_samples=pool_assemblies, n_clusters=max(1, nref // 10), role=kssdgpu.ROLE_OWNLEN,
+                        size_dist=kssdgpu.SIZE_LOGNORMAL, len_median=4e6, len_sigma=0.37, len_min=1e6, len_max=12e6,
+                        own_len_min=5e5, own_len_max=12e6, sub_lo=0.001, sub_hi=0.2, seed=seed, sample_seed=seed + 1)
+    reads = kssdgpu.synth(n_samples=pool_reads, n_clusters=max(1, nref // 10), role=kssdgpu.ROLE_READS,
+                          size_dist=kssdgpu.SIZE_LOGNORMAL, len_median=4e6, len_sigma=0.37, len_min=1e6,
+                          len_max=12e6, sub_lo=0.001, sub_hi=0.2, seed=seed, sample_seed=seed + 2,
+                          ref_sample_seed=seed, ref_samples=nref, cov_lo=5, cov_hi=100, err_lo=0.001, err_hi=0.01)
+    pool = [("assembly", asm.keys[asm.offs[i]:asm.offs[i + 1]]) for i in range(asm.n)]
+    pool_r = [("reads", reads.keys[reads.offs[i]:reads.offs[i + 1]]) for i in range(reads.n)]
+    max_keys = max(len(k) for _, k in pool + pool_r)
+    srv = kssdgpu.Server(idx, max_batch_queries=max_batch_queries, max_batch_keys=max(1 << 24, 2 * max_keys),
+                         max_hits=1 << 22)
+    for _, k in pool[:32] + pool_r[:8]:  # warm-up
+        srv.result(srv.submit(k))
+    rng = random.Random(seed)
+    results = []
+    old_si = sys.getswitchinterval()
+    sys.setswitchinterval(2e-4)  # the pacing loop must not hold the interpreter lock for 5 ms
+    try:
+        for rate in rates:
+            srv.reset_stats()
+            nreq = max(1, int(rate * seconds))
+            t = 0.0
+            plan = []
+            for _ in range(nreq):
+                t += rng.expovariate(rate)
+                plan.append((t, pool[rng.randrange(len(pool))] if rng.random() < 0.8 else
+                             pool_r[rng.randrange(len(pool_r))]))
+            got, tickets = [], []
+            cond = threading.Condition()
+            done_submitting = [False]
+
+            def collector():
+                i = 0
+                while i < nreq:
+                    with cond:
+                        while i >= len(tickets):
+                            cond.wait(timeout=1.0)
+                            if i >= len(tickets) and done_submitting[0]:
+                                return
+                        kind, tk = tickets[i]
+                    hits, lat = srv.result(tk, timeout_ms=120000)
+                    got.append((kind, lat, len(hits)))
+                    i += 1
+
+            th = threading.Thread(target=collector)
+            th.start()
+            start = time.perf_counter()
+            for at, (kind, keys) in plan:
+                gap = at - (time.perf_counter() - start)
+                if gap > 1e-3:
+                    time.sleep(gap - 5e-4)
+                while time.perf_counter() - start < at:
+                    pass
+                tk = srv.submit(keys)
+                with cond:
+                    tickets.append((kind, tk))
+                    cond.notify()
+            with cond:
+                done_submitting[0] = True
+                cond.notify()
+            th.join()
+            wall = time.perf_counter() - start
+            st = srv.stats()
+            lat_a = [x[1] for x in got if x[0] == "assembly"]
+            lat_r = [x[1] for x in got if x[0] == "reads"]
+            lat = [x[1] for x in got]
+            results.append({
+                "rate_req_s": rate, "requests": nreq, "wall_s": wall, "throughput_req_s": nreq / wall,
+                "genome_pairs_s": nreq * nref / wall, "p50_ms": _pct(lat, 0.5), "p99_ms": _pct(lat, 0.99),
+                "assembly_p50_ms": _pct(lat_a, 0.5), "assembly_p99_ms": _pct(lat_a, 0.99),
+                "reads_p50_ms": _pct(lat_r, 0.5), "reads_p99_ms": _pct(lat_r, 0.99),
+                "max_ms": max(lat) if lat else None, "batches": st["batches"], "max_inflight": st["max_inflight"],
+                "overlapped_batches": st["overlapped_batches"], "splits": st["splits"],
+                "mean_hits": float(np.mean([x[2] for x in got])) if got else 0.0})
+    finally:
+        sys.setswitchinterval(old_si)
+    pool_facts = {"assemblies": len(pool), "read_sets": len(pool_r), "max_keys": max_keys,
+                  "mean_assembly_keys": float(np.mean([len(k) for _, k in pool])),
+                  "mean_reads_keys": float(np.mean([len(k) for _, k in pool_r]))}
+    srv_facts = {"reserved_bytes": srv.stats()["reserved_bytes"], "slots": srv.stats()["slots"],
+                 "max_batch_queries": max_batch_queries}
+    srv.close()
+    return results, pool_facts, srv_facts
 
 
 def run_ours(args, rank, world, local_rank):
@@ -185,6 +542,8 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     stream = torch.cuda.current_stream()
+    timer = Timer(stream, dev)
+    peak, peak_kind = measured_peak_hbm()
 
     sk = make_workload(args.genomes)
     n = sk.n
@@ -194,14 +553,7 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.synchronize()
     index_ms = 1e3 * (time.perf_counter() - t0)
     info = idx.info()
-    t0 = time.perf_counter()
-    plan = idx.self_plan_info()  # first call builds the join plan (once per index)
-    torch.cuda.synchronize()
-    plan["plan_ms"] = 1e3 * (time.perf_counter() - t0)
-    t0 = time.perf_counter()
-    plan["tuning"] = idx.self_plan_tune()  # the autotuner picks the plan's chunking
-    plan["tuning"]["tune_ms"] = 1e3 * (time.perf_counter() - t0)
-    plan["index_build_ms"] = index_ms
+    facts = idx.self_plan_info()  # shared context groups, their postings and pairs (one pass; no plan)
 
     d_keys = torch.from_numpy(sk.keys.view(np.int64)).to(dev)
     d_offs = torch.from_numpy(sk.offs.view(np.int64)).to(dev)
@@ -210,7 +562,6 @@ def run_ours(args, rank, world, local_rank):
     d_lo = torch.zeros(lower_cells, dtype=torch.int64, device=dev)
     d_c = torch.zeros(n * n, dtype=torch.int64, device=dev)
     d_o = torch.zeros(n * n, dtype=torch.int64, device=dev)
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
 
     def self_step(flags=0):
         idx.self_lower_dev(d_lc, d_lo, flags=flags, stream=stream)
@@ -221,58 +572,39 @@ def run_ours(args, rank, world, local_rank):
     def plain_step():
         idx.count_plain_dev(d_keys, d_offs, sk.offs, d_c, d_o, lower=True, stream=stream)
 
-    # ---- parity on the benchmark's own inputs: self join == batched probe == plain
+    # ---- parity on the benchmark's own inputs: scan join == batched probe == plain == cached-plan join
     probe_step()
     idx.sync(stream)
-    tri = torch.tril_indices(n, n, -1, device=dev)
-    dense_c = d_c.view(n, n)[tri[0], tri[1]].clone()
-    dense_o = d_o.view(n, n)[tri[0], tri[1]].clone()
     self_step()
     idx.sync(stream)
-    ok_join = bool(torch.equal(dense_c, d_lc) and torch.equal(dense_o, d_lo))
+    ok_probe = lower_equals_dense(d_lc, d_lo, d_c, d_o, n)
     plain_step()
     idx.sync(stream)
-    ok_plain = bool(torch.equal(d_c.view(n, n)[tri[0], tri[1]], dense_c) and
-                    torch.equal(d_o.view(n, n)[tri[0], tri[1]], dense_o))
-    if not (ok_join and ok_plain):
-        raise SystemExit(f"parity failure on the bench workload: join={ok_join} plain={ok_plain}")
-    del tri
+    ok_plain = lower_equals_dense(d_lc, d_lo, d_c, d_o, n)
+    p_c, p_o = torch.zeros_like(d_lc), torch.zeros_like(d_lo)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    idx.self_lower_dev(p_c, p_o, flags=kssdgpu.SELF_PLAN, stream=stream)  # first call builds the plan
+    torch.cuda.synchronize()
+    plan_first_ms = 1e3 * (time.perf_counter() - t0)
+    ok_plan = bool(torch.equal(p_c, d_lc) and torch.equal(p_o, d_lo))
+    if not (ok_probe and ok_plain and ok_plan):
+        raise SystemExit(f"parity failure on the bench workload: probe={ok_probe} plain={ok_plain} plan={ok_plan}")
     # lower-triangle cells that share at least one context (every credit adds num_ctx += 1)
     touched = int(torch.count_nonzero(d_lc).item())
+    density = density_histogram(d_lc, np.diff(sk.offs.astype(np.int64)), n)
 
-    def timed(fn, steps, warmup, flush_l2=True, pre=None):
-        for _ in range(warmup):
-            if pre:
-                pre()
-            fn()
-        torch.cuda.synchronize()
-        tot = 0.0
-        for _ in range(steps):
-            if flush_l2:
-                flush.fill_(1)
-            if pre:
-                pre()
-            s = torch.cuda.Event(enable_timing=True)
-            e = torch.cuda.Event(enable_timing=True)
-            s.record(stream)
-            fn()
-            e.record(stream)
-            e.synchronize()
-            tot += s.elapsed_time(e)
-        idx.sync(stream)
-        return tot / steps  # ms
-
-    # ---- headline: timed region bracketed by barrier + synchronize, max over ranks
+    # ---- headline: one self step per timed step, bracketed by barrier + synchronize, max over ranks
     launches0 = kssdgpu.launch_count()
     self_step()
     torch.cuda.synchronize()
     launches_per_step = kssdgpu.launch_count() - launches0
     with ClockSampler(local_rank) as clocks:
-        # the steps take milliseconds: keep the GPU on this workload until the sampler
-        # has readings, then run the timed region inside the same sampling window
+        # the steps take tens of microseconds: keep the GPU on this workload until the
+        # sampler has readings, then run the timed region inside the same sampling window
         t_end = time.time() + 1.5
         while time.time() < t_end or len(clocks.samples) < 3:
-            for _ in range(50):
+            for _ in range(200):
                 self_step()
             torch.cuda.synchronize()
             if time.time() > t_end + 10:
@@ -280,7 +612,7 @@ def run_ours(args, rank, world, local_rank):
         if dist:
             dist.barrier()
         torch.cuda.synchronize()
-        ms_step = timed(self_step, args.steps, args.warmup)
+        ms_step = timer(self_step, args.steps, args.warmup)
         torch.cuda.synchronize()
         if dist:
             dist.barrier()
@@ -288,40 +620,36 @@ def run_ours(args, rank, world, local_rank):
     launches_timed = launches_per_step * args.steps
     value = replica_value(world, n * n, ms_step / 1e3)
 
-    # ---- dominant kernel alone (join kernels, counters zeroed outside the events)
+    # ---- the dominant kernel alone: the scan join, counters zeroed outside the events
     zero = lambda: (d_lc.zero_(), d_lo.zero_())  # noqa: E731
-    ms_join = timed(lambda: self_step(kssdgpu.NO_ZERO), args.steps, 2, pre=zero)
-    peak, peak_kind = measured_peak_hbm()
-    # algorithmic bytes of one join launch: each listed group's (begin,k) word and its
-    # postings read once, each touched lower-triangle cell (16 B of counters) read and
-    # written once; the step adds the 16 B/cell zero fill of the dense lower triangle
-    join_bytes = 8 * plan["groups"] + 8 * plan["postings"] + 2 * 16 * touched
-    step_bytes = join_bytes + 16 * lower_cells
-    achieved = join_bytes / (ms_join / 1e3) / 1e9
+    ms_scan = timer(lambda: self_step(kssdgpu.NO_ZERO), args.steps, 2, pre=zero)
+    scan_bytes = scan_join_bytes(info["contexts"], facts["postings"], touched)
+    step_bytes = scan_bytes + 16 * lower_cells
+    model_bytes = probe_model_bytes(int(sk.offs[-1]), facts["pairs"], lower_cells)
+    achieved = scan_bytes / (ms_scan / 1e3) / 1e9
     traffic = None
-    tfile = os.path.join(ROOT, "profiles", "k_self_sets_traffic.json")
+    tfile = os.path.join(ROOT, "profiles", "k_self_scan_traffic.json")
     if os.path.exists(tfile):
         try:
             t = json.load(open(tfile))
-            if t.get("workload_genomes") == n:  # the ncu capture of this workload's join launch
+            if t.get("workload_genomes") == n:  # the ncu capture of this workload's scan-join launch
                 traffic = t.get("bytes_per_launch")
         except Exception:
             traffic = None
 
-    # ---- plain one-query-per-launch and batched probe kernels (same counters)
+    # ---- batched probe, plain per-query kernel and cached-plan join on the same workload
     probe_tuning = idx.count_tune(d_keys, d_offs, n, d_c, d_o, lower=True)  # accumulator mode / chunk size
-    ms_probe = timed(probe_step, max(3, args.steps // 2), 2)
-    ms_plain = timed(plain_step, 3, 1)
-    # per-query probe model bytes: 8|q| + 12 * postings walked + 16 per output cell
-    probe_model_bytes = None
+    ms_probe = timer(probe_step, max(3, args.steps // 2), 2)
+    ms_plain = timer(plain_step, 3, 1)
+    ms_plan_join = timer(lambda: idx.self_lower_dev(p_c, p_o, flags=kssdgpu.SELF_PLAN, stream=stream), 5, 2)
+    del p_c, p_o
 
-    # ---- e2e through the host-buffer C ABI (pinned host inputs and outputs)
+    # ---- e2e through the host-buffer C ABI
+    lib = kssdgpu.gpu_lib()
     h_keys = torch.from_numpy(sk.keys.view(np.int64)).pin_memory()
-    h_offs_t = torch.from_numpy(sk.offs.view(np.int64)).pin_memory()
+    h_offs_np = np.ascontiguousarray(sk.offs, dtype=np.uint64)
     h_ctx = torch.empty(n * n * 2, dtype=torch.int32).pin_memory()
     h_obj = torch.empty(n * n * 2, dtype=torch.int32).pin_memory()
-    lib = kssdgpu.gpu_lib()
-    h_offs_np = h_offs_t.numpy().view(np.uint64)
 
     def e2e_call():
         rc = lib.kssdgpu_count_lower(idx.handle, h_keys.data_ptr(), h_offs_np, n, 0, 0, h_ctx.data_ptr(),
@@ -329,22 +657,43 @@ def run_ours(args, rank, world, local_rank):
         if rc:
             raise kssdgpu.KssdGpuError(rc, lib.kssdgpu_last_error().decode())
 
-    for _ in range(2):
-        e2e_call()
-    e2e_times = []
-    for _ in range(max(3, args.steps // 2)):
-        flush.fill_(1)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        e2e_call()
-        e2e_times.append(time.perf_counter() - t0)
-    e2e_s = float(np.median(e2e_times))
-    e2e_s = max_over_ranks(dist, e2e_s, dev)
+    def e2e_time(call, reps):
+        call()
+        ts = []
+        for _ in range(reps):
+            timer.flush.fill_(1)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            call()
+            ts.append(time.perf_counter() - t0)
+        return float(np.median(ts))
+
+    e2e_s = max_over_ranks(dist, e2e_time(e2e_call, max(3, args.steps // 2)), dev)
     e2e_value = replica_value(world, n * n, e2e_s)
-    h2d = int(sk.keys.nbytes + sk.offs.nbytes + 4 * n)
+    h2d = int(sk.keys.nbytes + sk.offs.nbytes)
     d2h = int(n * n * 16)
-    # the e2e counters equal the device-resident ones
     e2e_ok = bool(np.array_equal(h_ctx.numpy().view(np.int64), d_c.cpu().numpy()))
+    # as the reference's drivers call it: 64-query blocks, pageable (malloc'd) buffers
+    # (src/command_ani.c:1698 in comb_sortedsketch64_indexed_self_full)
+    blk_ctx = np.empty((BLOCK, n, 2), dtype=np.uint32)
+    blk_obj = np.empty((BLOCK, n, 2), dtype=np.uint32)
+    blk_ok = [True]
+
+    def e2e_blocks(check=False):
+        for off in range(0, n, BLOCK):
+            nb = min(BLOCK, n - off)
+            qo = np.ascontiguousarray(sk.offs[off: off + nb + 1])
+            qk = sk.keys[int(qo[0]): int(qo[-1])]
+            rc = lib.kssdgpu_count_lower(idx.handle, qk.ctypes.data, qo, nb, off, 0, blk_ctx.ctypes.data,
+                                         blk_obj.ctypes.data)
+            if rc:
+                raise kssdgpu.KssdGpuError(rc, lib.kssdgpu_last_error().decode())
+            if check:
+                want = h_ctx.numpy().view(np.uint32).reshape(n, n, 2)[off: off + nb]
+                blk_ok[0] &= bool(np.array_equal(blk_ctx[:nb], want))
+
+    e2e_blocks(check=True)
+    blocks_s = max_over_ranks(dist, e2e_time(e2e_blocks, 3), dev)
 
     # ---- CPU baseline: the reference's counting function on host cores (rank 0, N=1)
     cpu = None
@@ -370,6 +719,24 @@ def run_ours(args, rank, world, local_rank):
                "kind": "reference" if use_ref else "port",
                "sample": f"{len(blocks)} of {nblocks} 64-query blocks (count_lower), spread over the matrix",
                "counts_match_gpu": bool(same)}
+        del rec
+
+    # ---- the north-star and config legs against a resident 20,000-genome index
+    extra = {}
+    if rank == 0 and not args.no_extra:
+        del d_c, d_o
+        torch.cuda.empty_cache()
+        ns, ns_idx, ns_sk = leg_north_star(args, timer, dev, stream, peak)
+        extra["all_vs_all_20k"] = ns
+        extra["rect_config3"] = leg_rect(args, timer, dev, stream, peak, ns_idx, ns_sk)
+        extra["reads_config4"] = leg_reads(args, timer, dev, stream, ns_idx, ns_sk)
+        rates = [float(x) for x in args.serve_rates.split(",")] if args.serve_rates else []
+        if rates:
+            res, pool, srvf = serve_sweep(ns_idx, ns_sk.n, rates, args.serve_seconds, WORKLOAD["seed"] + 5)
+            extra["serve"] = {"index_genomes": ns_sk.n, "note": "resident 20,000-genome index (not 50,000: the "
+                              "default run stays within minutes; --workload serve runs the 50,000-genome index)",
+                              "pool": pool, "server": srvf, "rates": res}
+        ns_idx.close()
 
     if rank == 0:
         line = {
@@ -378,55 +745,66 @@ def run_ours(args, rank, world, local_rank):
             "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
             "config": {"workload": WORKLOAD["name"], "genomes": n, "entries": int(sk.offs[-1]),
                        "unique_contexts": info["contexts"], "matrix_cells": n * n,
-                       "lower_pairs": lower_cells, "path": "self join (kssdgpu_self_lower_dev)",
+                       "lower_pairs": lower_cells,
+                       "path": "self step from the resident index: zero fill + one-pass scan join "
+                               "(kssdgpu_self_lower_dev), nothing cached between steps",
                        "l2": "flushed (256 MB write) before every timed step",
                        "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
             "e2e": {"value": e2e_value, "unit": "genome-pairs/s", "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h, "call": "kssdgpu_count_lower (host buffers, pinned)",
+                    "d2h_bytes_per_step": d2h, "call": "kssdgpu_count_lower, one call, pinned host buffers",
                     "ms_per_step": 1e3 * e2e_s, "counts_match_device": e2e_ok},
+            "e2e_reference_blocks": {"value": replica_value(world, n * n, blocks_s), "unit": "genome-pairs/s",
+                                     "ms_per_step": 1e3 * blocks_s, "h2d_bytes_per_step": h2d,
+                                     "d2h_bytes_per_step": d2h, "counts_match_one_call": blk_ok[0],
+                                     "call": "kssdgpu_count_lower per 64-query block, pageable host buffers "
+                                             "(as the reference's drivers call the counting function)"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                         "kernel": "k_self_sets (set-major self join)", "ms_per_launch": ms_join,
-                         "algorithmic_bytes": join_bytes, "touched_cells": touched},
+                         "kernel": "k_self_scan (one-pass scan join)", "ms_per_launch": ms_scan,
+                         "algorithmic_bytes": scan_bytes,
+                         "bytes_model": "4 B per context group + 1 (bounds) + 8 B per posting of a group of >= 2 "
+                                        "+ 2 x 16 B per touched lower cell",
+                         "touched_cells": touched, "shared_groups": facts["groups"],
+                         "shared_postings": facts["postings"], "pairs": facts["pairs"]},
             "step_roofline": {"bound": "hbm", "algorithmic_bytes": step_bytes,
                               "achieved": step_bytes / (ms_step / 1e3) / 1e9,
                               "frac": step_bytes / (ms_step / 1e3) / 1e9 / peak,
-                              "what": "zero fill of the dense lower triangle + self join"},
+                              "what": "zero fill of the dense lower triangle (16 B per cell) + scan join",
+                              "probe_model_bytes": model_bytes,
+                              "probe_model_frac": model_bytes / (ms_step / 1e3) / 1e9 / peak},
             "kernels": {
                 "batched_probe": {"ms": ms_probe, "value": world * n * n / (ms_probe / 1e3),
                                   "contexts_probed_per_s": world * int(sk.offs[-1]) / (ms_probe / 1e3),
+                                  "probe_model_bytes": model_bytes,
+                                  "probe_model_frac": model_bytes / (ms_probe / 1e3) / 1e9 / peak,
                                   "tuning": probe_tuning},
                 "plain_per_query": {"ms": ms_plain, "value": world * n * n / (ms_plain / 1e3), "launches": n},
-                "self_join_vs_plain": ms_plain / ms_step, "batched_probe_vs_plain": ms_plain / ms_probe,
+                "cached_plan_join": {"ms": ms_plan_join, "first_call_ms": plan_first_ms,
+                                     "what": "KSSDGPU_SELF_PLAN: set-major plan built by the first call and kept"},
+                "self_step_vs_plain": ms_plain / ms_step, "batched_probe_vs_plain": ms_plain / ms_probe,
+                "self_step_vs_batched_probe": ms_probe / ms_step,
             },
-            "join_plan": plan,
+            "index_build_ms": index_ms,
+            "density_per_128_tile": density,
             "gpu_launches": int(launches_timed),
             "clocks": clocks.summary(),
             "cpu_baseline": cpu,
         }
+        line.update(extra)
         print(json.dumps(line), flush=True)
     idx.close()
     return 0
 
 
-def _pct(xs, p):
-    xs = sorted(xs)
-    return float(xs[min(len(xs) - 1, int(p * (len(xs) - 1) + 0.5))]) if xs else None
-
-
 def run_serve(args, rank):
-    """Serving: a resident index of --serve-refs genomes (the self-matrix generator,
-    10 genomes per cluster), Poisson arrivals at each rate for --serve-seconds, 80%
-    assemblies (0.5-12 Mbp, from the same cluster ancestors) and 20% read sets (1-5
-    genomes at 5-100x, 0.1-1% errors, conflicts kept); latency = submit -> hits on the
-    host, measured by the server."""
-    import random
+    """Serving alone: a resident index of --serve-refs genomes (the self-matrix
+    generator, 10 genomes per cluster), Poisson arrivals at each rate."""
     import torch
     import kssdgpu
     if rank != 0:
         return 0
     n = args.serve_refs
-    seed = 20261203 + 5
+    seed = WORKLOAD["seed"] + 5
     t0 = time.perf_counter()
     ref = kssdgpu.synth(n_samples=n, n_clusters=max(1, n // 10), size_dist=kssdgpu.SIZE_LOGNORMAL, len_median=4e6,
                         len_sigma=0.37, len_min=1e6, len_max=12e6, sub_lo=0.001, sub_hi=0.2, seed=seed,
@@ -439,277 +817,12 @@ def run_serve(args, rank):
     torch.cuda.synchronize()
     build_s = time.perf_counter() - t0
     del ref
-    asm = kssdgpu.synth(n_samples=256, n_clusters=max(1, n // 10), role=kssdgpu.ROLE_OWNLEN,
-                        size_dist=kssdgpu.SIZE_LOGNORMAL, len_median=4e6, len_sigma=0.37, len_min=1e6, len_max=12e6,
-                        own_len_min=5e5, own_len_max=12e6, sub_lo=0.001, sub_hi=0.2, seed=seed, sample_seed=seed + 1)
-    reads = kssdgpu.synth(n_samples=64, n_clusters=max(1, n // 10), role=kssdgpu.ROLE_READS,
-                          size_dist=kssdgpu.SIZE_LOGNORMAL, len_median=4e6, len_sigma=0.37, len_min=1e6,
-                          len_max=12e6, sub_lo=0.001, sub_hi=0.2, seed=seed, sample_seed=seed + 2,
-                          ref_sample_seed=seed, ref_samples=n, cov_lo=5, cov_hi=100, err_lo=0.001, err_hi=0.01)
-    pool = [("assembly", asm.keys[asm.offs[i]:asm.offs[i + 1]]) for i in range(asm.n)]
-    pool_reads = [("reads", reads.keys[reads.offs[i]:reads.offs[i + 1]]) for i in range(reads.n)]
-    max_keys = max(len(k) for _, k in pool + pool_reads)
-    srv = kssdgpu.Server(idx, max_batch_queries=64, max_batch_keys=max(1 << 24, 2 * max_keys), max_hits=1 << 22)
-    for _, k in pool[:32] + pool_reads[:8]:  # warm-up
-        srv.result(srv.submit(k))
-    rng = random.Random(seed)
-    results = []
-    sys.setswitchinterval(2e-4)  # the pacing loop must not hold the interpreter lock for 5 ms
-    for rate in [float(x) for x in args.serve_rates.split(",")]:
-        srv.reset_stats()
-        nreq = max(1, int(rate * args.serve_seconds))
-        t = 0.0
-        plan = []
-        for _ in range(nreq):
-            t += rng.expovariate(rate)
-            plan.append((t, pool[rng.randrange(len(pool))] if rng.random() < 0.8 else
-                         pool_reads[rng.randrange(len(pool_reads))]))
-        got = []
-        tickets = []
-        cond = threading.Condition()
-
-        def collector():
-            i = 0
-            while True:
-                with cond:
-                    while i >= len(tickets):
-                        cond.wait(timeout=1.0)
-                        if i >= len(tickets) and done_submitting[0]:
-                            return
-                    kind, tk = tickets[i]
-                hits, lat = srv.result(tk, timeout_ms=120000)
-                got.append((kind, lat, len(hits)))
-                i += 1
-                if i == nreq:
-                    return
-
-        done_submitting = [False]
-        th = threading.Thread(target=collector)
-        th.start()
-        start = time.perf_counter()
-        for at, (kind, keys) in plan:
-            gap = at - (time.perf_counter() - start)
-            if gap > 1e-3:
-                time.sleep(gap - 5e-4)
-            while time.perf_counter() - start < at:
-                pass
-            tk = srv.submit(keys)
-            with cond:
-                tickets.append((kind, tk))
-                cond.notify()
-        with cond:
-            done_submitting[0] = True
-            cond.notify()
-        th.join()
-        wall = time.perf_counter() - start
-        st = srv.stats()
-        lat_a = [x[1] for x in got if x[0] == "assembly"]
-        lat_r = [x[1] for x in got if x[0] == "reads"]
-        lat = [x[1] for x in got]
-        results.append({
-            "rate_req_s": rate, "requests": nreq, "wall_s": wall, "throughput_req_s": nreq / wall,
-            "genome_pairs_s": nreq * n / wall, "p50_ms": _pct(lat, 0.5), "p99_ms": _pct(lat, 0.99),
-            "assembly_p50_ms": _pct(lat_a, 0.5), "assembly_p99_ms": _pct(lat_a, 0.99),
-            "reads_p50_ms": _pct(lat_r, 0.5), "reads_p99_ms": _pct(lat_r, 0.99), "max_ms": max(lat) if lat else None,
-            "batches": st["batches"], "max_inflight": st["max_inflight"],
-            "overlapped_batches": st["overlapped_batches"], "mean_hits": float(np.mean([x[2] for x in got]))})
-        print(json.dumps({"partial": results[-1]}), file=sys.stderr, flush=True)
+    rates = [float(x) for x in args.serve_rates.split(",")]
+    res, pool, srvf = serve_sweep(idx, n, rates, args.serve_seconds, seed)
     line = {"metric": "serve p50/p99 ms", "workload": f"serve-{n}-genome-index", "unit": "ms",
-            "higher_is_better": False, "data": "synthetic", "index": {"genomes": n, "entries": entries,
-            "generate_s": gen_s, "device_build_s": build_s}, "pool": {"assemblies": len(pool),
-            "read_sets": len(pool_reads), "max_keys": max_keys,
-            "mean_assembly_keys": float(np.mean([len(k) for _, k in pool])),
-            "mean_reads_keys": float(np.mean([len(k) for _, k in pool_reads]))},
-            "server": {"reserved_bytes": srv.stats()["reserved_bytes"], "max_batch_queries": 64},
-            "rates": results}
-    print(json.dumps(line), flush=True)
-    srv.close()
-    idx.close()
-    return 0
-
-
-def run_rect(args, rank):
-    """Uneven batch: --rect-queries genomes of log-uniform 50 kbp-12 Mbp against a
-    --rect-refs genome index (2,000 clusters at the default sizes): one persistent
-    batched launch (also replayed from a CUDA graph) vs the plain per-query kernel,
-    with the reference's own counting function timed on a query sample."""
-    import torch
-    import kssdgpu
-    if rank != 0:
-        return 0
-    nr, nq = args.rect_refs, args.rect_queries
-    seed = 20261203 + 3
-    clusters = max(1, nr // 10)
-    ref = kssdgpu.synth(n_samples=nr, n_clusters=clusters, size_dist=kssdgpu.SIZE_LOGNORMAL, len_median=4e6,
-                        len_sigma=0.37, len_min=1e6, len_max=12e6, sub_lo=0.001, sub_hi=0.2, seed=seed,
-                        sample_seed=seed, threads=os.cpu_count() or 8)
-    qry = kssdgpu.synth(n_samples=nq, n_clusters=clusters, role=kssdgpu.ROLE_OWNLEN, size_dist=kssdgpu.SIZE_LOGNORMAL,
-                        len_median=4e6, len_sigma=0.37, len_min=1e6, len_max=12e6, own_len_min=5e4,
-                        own_len_max=12e6, sub_lo=0.001, sub_hi=0.2, seed=seed, sample_seed=seed + 1,
-                        threads=os.cpu_count() or 8)
-    idx = kssdgpu.Index.from_sketch(ref)
-    dev = torch.device("cuda", 0)
-    stream = torch.cuda.current_stream()
-    dk = torch.from_numpy(qry.keys.view(np.int64)).to(dev)
-    do = torch.from_numpy(qry.offs.view(np.int64)).to(dev)
-    cells = nq * nr
-    dc = torch.zeros(cells, dtype=torch.int64, device=dev)
-    dob = torch.zeros(cells, dtype=torch.int64, device=dev)
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
-
-    def batched():
-        idx.count_block_dev(dk, do, nq, dc, dob, stream=stream)
-
-    def timed(fn, steps, warm):
-        for _ in range(warm):
-            fn()
-        torch.cuda.synchronize()
-        tot = 0.0
-        for _ in range(steps):
-            flush.fill_(1)
-            s = torch.cuda.Event(enable_timing=True)
-            e = torch.cuda.Event(enable_timing=True)
-            s.record(stream)
-            fn()
-            e.record(stream)
-            e.synchronize()
-            tot += s.elapsed_time(e)
-        idx.sync(stream)
-        return tot / steps
-
-    tuning = idx.count_tune(dk, do, nq, dc, dob)
-    ms_b = timed(batched, args.steps, args.warmup)
-    checksum = int(dc.sum().item())
-    shared = int((dc & 0xFFFFFFFF).sum().item())  # = postings walked (conflict-free references)
-    # the same launch sequence captured once into a CUDA graph and replayed
-    graph_ms = None
-    try:
-        g = torch.cuda.CUDAGraph()
-        side = torch.cuda.Stream()
-        side.wait_stream(stream)
-        with torch.cuda.stream(side):
-            with torch.cuda.graph(g, stream=side):
-                idx.count_block_dev(dk, do, nq, dc, dob, stream=side)
-        stream.wait_stream(side)
-        graph_ms = timed(lambda: g.replay(), args.steps, 2)
-        assert int(dc.sum().item()) == checksum
-    except Exception as exc:  # capture support depends on the driver; report instead of failing
-        graph_ms = f"capture failed: {exc}"
-    ms_p = timed(lambda: idx.count_plain_dev(dk, do, qry.offs, dc, dob, stream=stream), 1, 1)
-    assert int(dc.sum().item()) == checksum
-    qkeys = int(qry.offs[-1])
-    probe_bytes = 8 * qkeys + 12 * shared + 16 * cells
-    peak, kind = measured_peak_hbm()
-    # the reference's counting function on a sample of queries (host cores)
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle
-    rec, _ = idx.export()
-    sample = list(range(0, nq, max(1, nq // 48)))[:48]
-    skeys = np.concatenate([qry.keys[int(qry.offs[q]):int(qry.offs[q + 1])] for q in sample])
-    soffs = np.concatenate([[0], np.cumsum([int(qry.offs[q + 1] - qry.offs[q]) for q in sample])]).astype(np.uint64)
-    t0 = time.perf_counter()
-    c, _ = oracle.count_block(rec, nr, skeys, soffs, threads=os.cpu_count() or 1, ref=oracle.ref_available())
-    cpu_s = time.perf_counter() - t0
-    hc = dc.view(nq, nr)[torch.tensor(sample, device=dev)].cpu().numpy()
-    same = bool(np.array_equal(c[:, :, 0].astype(np.int64) | (c[:, :, 1].astype(np.int64) << 32), hc))
-    line = {"metric": "ANI genome-pairs/s", "workload": f"rect-{nq}x{nr}", "unit": "genome-pairs/s",
-            "value": cells / (ms_b / 1e3), "ms_per_step": ms_b, "steps": args.steps, "data": "synthetic",
-            "config": {"queries": nq, "refs": nr, "query_keys": qkeys, "ref_entries": int(ref.offs[-1]),
-                       "accumulators": "global (reference row exceeds shared memory)" if nr * 16 > 112 * 1024
-                       else "shared"},
-            "graph_replay_ms": graph_ms, "contexts_probed_per_s": qkeys / (ms_b / 1e3), "tuning": tuning,
-            "plain_per_query": {"ms": ms_p, "value": cells / (ms_p / 1e3), "launches": nq},
-            "batched_vs_plain": ms_p / ms_b,
-            "roofline_probe_model": {"bound": "hbm", "bytes": probe_bytes,
-                                     "achieved": probe_bytes / (ms_b / 1e3) / 1e9, "peak": peak,
-                                     "frac": probe_bytes / (ms_b / 1e3) / 1e9 / peak, "peak_kind": kind},
-            "cpu_baseline": {"value": len(sample) * nr / cpu_s, "unit": "genome-pairs/s",
-                             "cores": os.cpu_count(), "kind": "reference" if oracle.ref_available() else "port",
-                             "sample": f"{len(sample)} queries", "counts_match_gpu": same}}
-    print(json.dumps(line), flush=True)
-    idx.close()
-    return 0
-
-
-def run_reads(args, rank):
-    """Read sets: --reads-samples samples, each a mix of 1-5 genomes of a --rect-refs
-    genome reference at 5-50x with 0.1-1% substitution errors (conflicts kept, as
-    `sketch --asone --conflict -A`), counted against the reference index with unique
-    contexts (`ani --qraw ... --unique-ctx`): one batched launch, key-range chunks
-    built on the device, vs the plain per-query kernel; the reference's own counting
-    function timed on a sample."""
-    import torch
-    import kssdgpu
-    if rank != 0:
-        return 0
-    nr, nq = args.rect_refs, args.reads_samples
-    seed = 20261203 + 4
-    clusters = max(1, nr // 10)
-    ref = kssdgpu.synth(n_samples=nr, n_clusters=clusters, size_dist=kssdgpu.SIZE_LOGNORMAL, len_median=4e6,
-                        len_sigma=0.37, len_min=1e6, len_max=12e6, sub_lo=0.001, sub_hi=0.2, seed=seed,
-                        sample_seed=seed, threads=os.cpu_count() or 8)
-    qry = kssdgpu.synth(n_samples=nq, n_clusters=clusters, role=kssdgpu.ROLE_READS, size_dist=kssdgpu.SIZE_LOGNORMAL,
-                        len_median=4e6, len_sigma=0.37, len_min=1e6, len_max=12e6, sub_lo=0.001, sub_hi=0.2,
-                        seed=seed, sample_seed=seed + 1, ref_sample_seed=seed, ref_samples=nr, cov_lo=5, cov_hi=50,
-                        err_lo=0.001, err_hi=0.01, threads=os.cpu_count() or 8)
-    idx = kssdgpu.Index.from_sketch(ref)
-    dev = torch.device("cuda", 0)
-    stream = torch.cuda.current_stream()
-    dk = torch.from_numpy(qry.keys.view(np.int64)).to(dev)
-    do = torch.from_numpy(qry.offs.view(np.int64)).to(dev)
-    cells = nq * nr
-    outs = [torch.zeros(cells, dtype=torch.int64, device=dev) for _ in range(4)]
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
-    flags = kssdgpu.UNIQUE
-
-    def timed(fn, steps, warm):
-        for _ in range(warm):
-            fn()
-        torch.cuda.synchronize()
-        tot = 0.0
-        for _ in range(steps):
-            flush.fill_(1)
-            s = torch.cuda.Event(enable_timing=True)
-            e = torch.cuda.Event(enable_timing=True)
-            s.record(stream)
-            fn()
-            e.record(stream)
-            e.synchronize()
-            tot += s.elapsed_time(e)
-        idx.sync(stream)
-        return tot / steps
-
-    tuning = idx.count_tune(dk, do, nq, *outs, flags=flags)
-    ms_b = timed(lambda: idx.count_block_dev(dk, do, nq, *outs, flags=flags, stream=stream), args.steps,
-                 args.warmup)
-    sums = [int(o.sum().item()) for o in outs]
-    ms_p = timed(lambda: idx.count_plain_dev(dk, do, qry.offs, *outs, flags=flags, stream=stream), 1, 1)
-    assert [int(o.sum().item()) for o in outs] == sums
-    qkeys = int(qry.offs[-1])
-    # the reference's counting function (with unique contexts) on a sample of read sets
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle
-    rec, _ = idx.export()
-    sample = list(range(0, nq, max(1, nq // 8)))[:8]
-    skeys = np.concatenate([qry.keys[int(qry.offs[q]):int(qry.offs[q + 1])] for q in sample])
-    soffs = np.concatenate([[0], np.cumsum([int(qry.offs[q + 1] - qry.offs[q]) for q in sample])]).astype(np.uint64)
-    t0 = time.perf_counter()
-    want = oracle.count_block(rec, nr, skeys, soffs, unique=True, threads=os.cpu_count() or 1,
-                              ref=oracle.ref_available())
-    cpu_s = time.perf_counter() - t0
-    rows = torch.tensor(sample, device=dev)
-    same = all(bool(np.array_equal(w[:, :, 0].astype(np.int64) | (w[:, :, 1].astype(np.int64) << 32),
-                                   o.view(nq, nr)[rows].cpu().numpy())) for w, o in zip(want, outs))
-    line = {"metric": "ANI genome-pairs/s", "workload": f"reads-{nq}x{nr}-unique-ctx", "unit": "genome-pairs/s",
-            "value": cells / (ms_b / 1e3), "ms_per_step": ms_b, "steps": args.steps, "data": "synthetic",
-            "contexts_probed_per_s": qkeys / (ms_b / 1e3), "tuning": tuning,
-            "config": {"read_sets": nq, "refs": nr, "query_keys": qkeys, "ref_entries": int(ref.offs[-1]),
-                       "mean_keys_per_read_set": qkeys / nq, "flags": "unique contexts, conflicts kept"},
-            "plain_per_query": {"ms": ms_p, "value": cells / (ms_p / 1e3), "launches": nq},
-            "batched_vs_plain": ms_p / ms_b,
-            "cpu_baseline": {"value": len(sample) * nr / cpu_s, "unit": "genome-pairs/s",
-                             "cores": os.cpu_count(), "kind": "reference" if oracle.ref_available() else "port",
-                             "sample": f"{len(sample)} read sets", "counts_match_gpu": same}}
+            "higher_is_better": False, "data": "synthetic",
+            "index": {"genomes": n, "entries": entries, "generate_s": gen_s, "device_build_s": build_s},
+            "pool": pool, "server": srvf, "rates": res}
     print(json.dumps(line), flush=True)
     idx.close()
     return 0
@@ -725,16 +838,17 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline sample budget")
     ap.add_argument("--cpu-step-seconds", type=float, default=8.0, help="reference arm: seconds per step")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", choices=["self", "serve", "rect", "reads"], default="self",
-                    help="self: the headline self matrix (default); serve: Poisson arrivals against a resident "
-                         "index (p50/p99); rect: uneven queries against a larger index, one batched launch; "
-                         "reads: read sets with unique-context counting against the larger index")
-    ap.add_argument("--reads-samples", type=int, default=40)
-    ap.add_argument("--serve-refs", type=int, default=50000, help="serve: resident index size (genomes)")
-    ap.add_argument("--serve-rates", default="100,300,1000,3000,5000,10000,20000", help="serve: arrival rates (req/s)")
-    ap.add_argument("--serve-seconds", type=float, default=3.0, help="serve: arrival window per rate")
-    ap.add_argument("--rect-refs", type=int, default=20000)
+    ap.add_argument("--no-extra", action="store_true", help="skip the 20,000-genome legs")
+    ap.add_argument("--workload", choices=["self", "serve"], default="self",
+                    help="self: the headline self matrix and its legs (default); serve: Poisson arrivals against "
+                         "a resident --serve-refs genome index (p50/p99)")
+    ap.add_argument("--ns-genomes", type=int, default=20000, help="genomes of the all-vs-all leg and its index")
     ap.add_argument("--rect-queries", type=int, default=10000)
+    ap.add_argument("--reads-samples", type=int, default=40)
+    ap.add_argument("--parity-queries", type=int, default=48)
+    ap.add_argument("--serve-refs", type=int, default=50000, help="serve workload: resident index size (genomes)")
+    ap.add_argument("--serve-rates", default="1000,5000", help="arrival rates (req/s) of the serving sweep")
+    ap.add_argument("--serve-seconds", type=float, default=1.5, help="arrival window per rate")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -745,10 +859,6 @@ def main():
         return run_reference(args, rank, world)
     if args.workload == "serve":
         return run_serve(args, rank)
-    if args.workload == "rect":
-        return run_rect(args, rank)
-    if args.workload == "reads":
-        return run_reads(args, rank)
     if world > 1:
         import datetime
         import torch

@@ -47,6 +47,8 @@ extern "C" {
 #define KSSDGPU_NO_ZERO 0x10u       /* device calls: outputs were zeroed by the caller (skip memset) */
 #define KSSDGPU_SMEM_ACC 0x20u      /* force shared-memory accumulator rows (KSSDGPU_ERR_CAPACITY when a
                                        row of the index's references does not fit) */
+#define KSSDGPU_SELF_PLAN 0x40u     /* self lower triangle: join over the index's cached set-major plan
+                                       (built and kept on first use) instead of the one-pass scan */
 
 /* Counter cells, identical in layout to the reference's ctx_mut2_t / obj_section_t. */
 typedef struct kssdgpu_ctx_mut2 {
@@ -176,6 +178,32 @@ int kssdgpu_count_tune(kssdgpu_index_t *idx, const uint64_t *d_qry_keys, const u
                        kssdgpu_count_tuning_t *out);
 
 /*
+ * Detail-mode count with the candidate filter fused behind it on the device: the
+ * counting of kssdgpu_count_block on the block, then the pre-filter of the reference's
+ * detail branch (src/command_ani.h:585-609) over the block's counters in HBM, so only
+ * candidate cells are copied back.  A cell (i, j) is a candidate when
+ *   num_ctx >= ctxcut, qry_ctx_count[i] > 0, ref_ctx_count[j] > 0,
+ *   max(num_ctx / qry_ctx_count[i], num_ctx / ref_ctx_count[j]) >= afcut, and
+ *   its naive ANI >= anicut - 1e-9, the naive ANI being the float
+ *   1 - diff_obj / num_ctx / 7 or, with KSSDGPU_UNIQUE, 1 - naive distance of the
+ *   unique counters when they cover >= 5% of the reference, else of the full ones
+ *   (FP64 with the device's pow).
+ * The 1e-9 margin keeps every cell the reference keeps: the caller re-applies the
+ * exact ANI test with its own libm to the candidates before ranking them.  Outputs:
+ *   hits      the candidates, ascending (query, ref); query = index in the block;
+ *             all eight counters (unique ones zero without KSSDGPU_UNIQUE)
+ *   row_offs  nq + 1 entries: query i's candidates are hits[row_offs[i] .. row_offs[i+1])
+ * More than hits_cap candidates: KSSDGPU_ERR_CAPACITY with row_offs filled (the size
+ * the caller needs).  flags: KSSDGPU_IGNORECONFLICT, KSSDGPU_UNIQUE, accumulator flags.
+ * No reference counterpart as an entry point: it fuses a6's counting with its detail
+ * filter so the dense block stays on the device.
+ */
+typedef struct kssdgpu_hit kssdgpu_hit_t;
+int kssdgpu_count_detail(kssdgpu_index_t *idx, const uint64_t *qry_keys, const uint64_t *qry_offs, int nq,
+                         unsigned flags, const uint32_t *qry_ctx_count, const uint32_t *ref_ctx_count, int ctxcut,
+                         float afcut, float anicut, kssdgpu_hit_t *hits, uint64_t hits_cap, uint64_t *row_offs);
+
+/*
  * Whole self lower triangle in one pass (the counting behind
  * comb_sortedsketch64_indexed_self_full / _triangle, src/command_ani.c:1657-1842,
  * and matrix_write_indexed_self_matrix, src/command_matrix.c:439-619), valid when
@@ -200,8 +228,15 @@ int kssdgpu_self_lower(kssdgpu_index_t *idx, unsigned flags, kssdgpu_ctx_mut2_t 
  */
 int kssdgpu_self_votes(kssdgpu_index_t *idx, const uint64_t *keys, const uint64_t *offs, uint32_t max_ctx_freq,
                        uint32_t sample_step, uint32_t *votes, uint32_t *first);
-/* Device form of kssdgpu_self_lower (outputs in HBM, stream-ordered).  Where the
- * dense counters outgrow L2 the join adds into per-index compact counters while the
+/* Device form of kssdgpu_self_lower (outputs in HBM, stream-ordered).
+ *
+ * Default: one pass over the whole index per call, nothing cached -- the dense lower
+ * triangle is zero-filled (unless KSSDGPU_NO_ZERO) and a persistent scan reads every
+ * context group's bounds, and joins each group of >= 2 postings as it finds it.
+ *
+ * With KSSDGPU_SELF_PLAN: the first call builds a set-major plan of the index's
+ * shared contexts (kept on the handle; later calls only join over it).  Where the
+ * dense counters outgrow L2 that join adds into per-index compact counters while the
  * zero fill runs on an internal stream that waits for the caller's earlier work; the
  * call's last operation on `stream` waits for both.  Calls on one index that overlap
  * on the GPU share those compact counters: order them on one stream. */
@@ -209,14 +244,14 @@ int kssdgpu_self_lower_dev(kssdgpu_index_t *idx, unsigned flags, kssdgpu_ctx_mut
                            kssdgpu_obj_section_t *d_obj_lower, void *stream);
 
 /*
- * Facts of the self-join plan (built on first use): context groups holding >= 2
- * postings (listed groups), postings inside them, and the reference-run pairs the
- * join credits.  These size the join's algorithmic bytes.
+ * Facts of the self join, from one pass over the index (no plan is built): context
+ * groups holding >= 2 postings, postings inside them, and their posting pairs
+ * (k(k-1)/2 per group of k).  These size the join's algorithmic bytes.
  */
 int kssdgpu_self_plan_info(kssdgpu_index_t *idx, uint64_t *groups, uint64_t *postings, uint64_t *pairs);
 
 /*
- * Autotune the self-join plan (once per index; builds the plan first if needed):
+ * Autotune the KSSDGPU_SELF_PLAN join's plan (once per index; builds the plan first if needed):
  * every candidate setting is planned and timed as a whole step (zero fill + join) on
  * scratch counters, after an L2 flush, and the fastest is kept.  Reports the setting in use: groups per
  * set-major chunk, whether chunks run largest first, the largest group size joined
@@ -246,12 +281,16 @@ int kssdgpu_count_plain_dev(kssdgpu_index_t *idx, const uint64_t *d_qry_keys, co
  * For callers that must not allocate device memory during a count: a serving
  * loop that reserved all device memory up front for its admission budget, or an
  * embedding application whose own allocator owns the device and forbids other
- * allocations.  The call runs the batched persistent counting kernel with its
- * scratch (work counter, error word, and the largest-first query order it builds
- * on the device) in a static device array of this library instead of memory from
- * cudaMalloc; it calls no cudaMalloc, cudaFree or allocating library routine.
- * The index (built earlier) and all inputs and outputs are the caller's device
- * buffers, as for kssdgpu_count_block_dev.
+ * allocations.  The call runs the batched persistent counting kernel, in the
+ * accumulator mode kssdgpu_count_block_dev would use (global rows split into
+ * key-range chunks, so a large query spreads over all SMs, unless shared-memory rows
+ * are forced or were chosen by kssdgpu_count_tune), with its scratch (work counter
+ * and the chunk prefix or largest-first query order it builds on the device) in a
+ * static device array of this library instead of memory from cudaMalloc; it calls
+ * no cudaMalloc, cudaFree or allocating library routine.  The index (built earlier)
+ * and all inputs and outputs are the caller's device buffers, as for
+ * kssdgpu_count_block_dev; errors found on the device (query keys out of order) are
+ * reported by the next kssdgpu_sync(idx, stream).
  *
  * Limits and rules:
  *   - at most KSSDGPU_NOALLOC_MAX_QUERIES queries per call; more returns
@@ -259,7 +298,8 @@ int kssdgpu_count_plain_dev(kssdgpu_index_t *idx, const uint64_t *d_qry_keys, co
  *   - the array is KSSDGPU_NOALLOC_SCRATCH_BYTES, held by every GPU that loads the
  *     library until the process exits;
  *   - the first call on a device looks up the array's device address (set-up);
- *     make that first call before any stream capture;
+ *     make that first call before any stream capture; after a cudaDeviceReset,
+ *     call kssdgpu_init(device) first so that the address is looked up again;
  *   - every call shares the one array (it keeps the last call's contents and is
  *     cleared where needed on each call), so calls that overlap on the GPU (other
  *     streams, other threads) race: serialise them.
@@ -276,9 +316,15 @@ int kssdgpu_count_block_noalloc(kssdgpu_index_t *idx, const uint64_t *d_qry_keys
  * reference has no server: its per-request equivalent is one `kssd3a ani -r R -q one`
  * run).  Each request is one query sample; its result is the list of nonzero counter
  * cells kssdgpu_count_block gives for that query alone, sorted by reference id.
- * Device memory for two batch slots is reserved at creation (the admission budget):
- * a slot admits the oldest queued requests up to max_batch_queries queries and
- * max_batch_keys keys, and the two slots' batches overlap on the device.
+ *
+ * Admission by device memory: at creation the server reserves as many batch slots as
+ * device_budget bytes hold (at most `slots`); each slot admits the oldest queued
+ * requests up to max_batch_queries queries and max_batch_keys keys, and every slot's
+ * batch runs beside the others on the device, so requests arriving while batches run
+ * join the next free slot.  A batch whose nonzero cells overflow max_hits is split:
+ * its requests re-run one per batch, and only a request that overflows alone fails
+ * (KSSDGPU_ERR_CAPACITY).  Query keys that do not ascend are rejected at submit
+ * (KSSDGPU_ERR_UNSORTED).
  */
 typedef struct kssdgpu_hit {
     uint32_t query; /* 0 in results (each request is one query) */
@@ -290,13 +336,17 @@ typedef struct kssdgpu_hit {
 typedef struct kssdgpu_server_config {
     int max_batch_queries;   /* queries per batch slot */
     uint64_t max_batch_keys; /* keys per batch slot (larger single queries are rejected) */
-    uint64_t max_hits;       /* nonzero cells per batch (0: batch queries x references) */
+    uint64_t max_hits;       /* nonzero cells per batch (0: min(batch queries x references, 2^22)) */
     unsigned flags;          /* KSSDGPU_IGNORECONFLICT | KSSDGPU_UNIQUE */
+    int slots;               /* most batch slots in flight (0: 4) */
+    uint64_t device_budget;  /* device bytes the slots may reserve (0: half of the free memory) */
 } kssdgpu_server_config_t;
 
 typedef struct kssdgpu_server_stats {
     uint64_t completed, batches, pending, max_inflight, overlapped_batches, reserved_bytes;
     double p50_ms, p99_ms, max_ms, mean_ms; /* submit -> result latency */
+    uint64_t slots;          /* batch slots reserved (the budget's share) */
+    uint64_t splits;         /* batches split after overflowing max_hits */
 } kssdgpu_server_stats_t;
 
 typedef struct kssdgpu_server kssdgpu_server_t;

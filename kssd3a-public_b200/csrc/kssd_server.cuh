@@ -1,17 +1,20 @@
 // Continuous-batching query server over a resident index (part of the kssdgpu.cu
 // translation unit: it launches the batched counting kernel defined there).
 //
-// Requests are single query samples (sorted comblco keys).  submit() copies the keys
-// into the request and queues it.  A worker thread owns two device slots whose
-// buffers are reserved when the server is created (the admission budget): a slot
-// takes the oldest queued requests up to its query and key capacity, uploads them
-// from pinned staging, runs the batched counting kernel with global accumulators
-// over dense [query][reference] rows, compacts the nonzero cells into sparse hits
-// on the device (re-zeroing the rows for the next batch) and copies the hits back.
-// While one slot's batch runs, the other admits and launches the next one, so
-// requests that arrive while work is on the GPU join the next free slot and both
-// batches overlap on the device.  Every request's hits are the nonzero counter
-// cells of kssdgpu_count_block for that query alone, sorted by reference id.
+// Requests are single query samples (sorted comblco keys).  submit() checks and
+// copies the keys into the request and queues it.  A worker thread owns a pool of
+// device slots whose buffers are reserved when the server is created: as many slots
+// as the configured device-memory budget holds (at most the configured count), so
+// the budget bounds the work in flight.  A free slot admits the oldest queued
+// requests up to its query and key capacity, uploads them from pinned staging, runs
+// the batched counting kernel with global accumulators over dense
+// [query][reference] rows, compacts the nonzero cells into sparse hits on the device
+// (re-zeroing the rows for the next batch) and copies the hits back.  Requests that
+// arrive while batches run are admitted into the next free slot at once, so several
+// batches overlap on the device.  A batch whose hits overflow the hit capacity is
+// split: its requests go back to the front of the queue and run one per batch; only
+// a request that overflows alone fails.  Every request's hits are the nonzero
+// counter cells of kssdgpu_count_block for that query alone, sorted by reference id.
 #pragma once
 
 #include <chrono>
@@ -71,6 +74,7 @@ struct ServerRequest {
     int status = KSSDGPU_OK;
     std::string error;
     bool done = false;
+    bool solo = false;  // re-run alone after its batch overflowed the hit capacity
 };
 
 double now_ms()
@@ -99,7 +103,8 @@ struct kssdgpu_server {
     kssdgpu_index *ix = nullptr;
     kssdgpu_server_config_t cfg{};
     unsigned hit_cap = 0;
-    ServerSlot slots[2];
+    std::vector<ServerSlot> slots;
+    uint64_t slot_bytes = 0;  // device memory reserved per slot
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
     std::deque<std::shared_ptr<ServerRequest>> pending;
@@ -109,7 +114,7 @@ struct kssdgpu_server {
     std::thread worker;
     // statistics (under mu)
     std::vector<double> latencies;
-    uint64_t batches = 0, queries = 0, max_inflight = 0, overlapped = 0;
+    uint64_t batches = 0, queries = 0, max_inflight = 0, overlapped = 0, splits = 0;
     int fatal = KSSDGPU_OK;
     std::string fatal_msg;
 };
@@ -120,6 +125,23 @@ namespace {
 size_t server_item_cap(const kssdgpu_server_config_t &c)
 {
     return (size_t)(c.max_batch_keys / kChunkKeys) + (size_t)c.max_batch_queries + 1;
+}
+
+// Device bytes one slot reserves: keys, offsets, work items, dense counter rows
+// (twice with unique contexts), hits and two counters.
+uint64_t server_slot_bytes(const kssdgpu_server_config_t &c, int nref, unsigned hit_cap)
+{
+    const uint64_t cells = (uint64_t)c.max_batch_queries * (uint64_t)nref;
+    return c.max_batch_keys * 8 + ((uint64_t)c.max_batch_queries + 1) * 8 + server_item_cap(c) * sizeof(WorkItem) +
+           cells * 16 * ((c.flags & KSSDGPU_UNIQUE) ? 2 : 1) + (uint64_t)hit_cap * sizeof(kssdgpu_hit_t) + 8;
+}
+
+bool any_busy(const kssdgpu_server *s)
+{
+    for (const auto &sl : s->slots)
+        if (sl.busy)
+            return true;
+    return false;
 }
 
 int server_slot_alloc(kssdgpu_server *s, ServerSlot &sl)
@@ -240,9 +262,26 @@ int server_finish(kssdgpu_server *s, ServerSlot &sl)
     const unsigned n = *sl.h_count;
     int status = KSSDGPU_OK;
     std::string msg;
+    if (n > s->hit_cap && sl.batch.size() > 1) {
+        // split: the requests go back to the front of the queue, in order, to run
+        // alone (the compaction re-zeroed every row, so the slot is clean)
+        {
+            std::lock_guard<std::mutex> lock(s->mu);
+            for (auto it = sl.batch.rbegin(); it != sl.batch.rend(); ++it) {
+                (*it)->solo = true;
+                s->pending.push_front(*it);
+            }
+            s->splits++;
+        }
+        sl.batch.clear();
+        sl.busy = false;
+        s->cv_work.notify_one();
+        return KSSDGPU_OK;
+    }
     if (n > s->hit_cap) {
         status = KSSDGPU_ERR_CAPACITY;
-        msg = "batch produced more nonzero cells than the server's hit capacity";
+        msg = "query produced more nonzero cells (" + std::to_string(n) + ") than the server's hit capacity (" +
+              std::to_string(s->hit_cap) + ")";
     } else if (n) {
         const cudaError_t e = cudaMemcpyAsync(sl.h_hits, sl.d_hits, (size_t)n * sizeof(kssdgpu_hit_t),
                                               cudaMemcpyDeviceToHost, sl.st);
@@ -303,16 +342,22 @@ void server_loop(kssdgpu_server *s)
                 uint64_t keys = 0;
                 while (!s->pending.empty() && sl.batch.size() < (size_t)s->cfg.max_batch_queries &&
                        keys + s->pending.front()->keys.size() <= s->cfg.max_batch_keys) {
+                    const bool solo = s->pending.front()->solo;
+                    if (solo && !sl.batch.empty())
+                        break;  // a split request runs in a batch of its own
                     keys += s->pending.front()->keys.size();
                     sl.batch.push_back(std::move(s->pending.front()));
                     s->pending.pop_front();
+                    if (solo)
+                        break;
                 }
                 if (!sl.batch.empty()) {
-                    const bool other_busy = s->slots[0].busy || s->slots[1].busy;
-                    if (other_busy)
+                    uint64_t inflight = sl.batch.size();
+                    for (const auto &o : s->slots)
+                        if (o.busy)
+                            inflight += o.batch.size();
+                    if (any_busy(s))
                         s->overlapped++;
-                    const uint64_t inflight = sl.batch.size() + (s->slots[0].busy ? s->slots[0].batch.size() : 0) +
-                                              (s->slots[1].busy ? s->slots[1].batch.size() : 0);
                     s->max_inflight = std::max<uint64_t>(s->max_inflight, inflight);
                 }
             }
@@ -336,10 +381,10 @@ void server_loop(kssdgpu_server *s)
             progressed = true;
         }
         std::unique_lock<std::mutex> lock(s->mu);
-        if (s->stop && s->pending.empty() && !s->slots[0].busy && !s->slots[1].busy)
+        if (s->stop && s->pending.empty() && !any_busy(s))
             break;
         if (!progressed) {
-            if (s->slots[0].busy || s->slots[1].busy) {
+            if (any_busy(s)) {
                 lock.unlock();
                 std::this_thread::sleep_for(std::chrono::microseconds(20));
             } else {
@@ -358,14 +403,29 @@ int kssdgpu_server_create(kssdgpu_index_t *ix, const kssdgpu_server_config_t *cf
 {
     if (!ix || !cfg || !out)
         return fail(KSSDGPU_ERR_ARG, "null argument");
-    if (cfg->max_batch_queries <= 0 || cfg->max_batch_keys == 0)
-        return fail(KSSDGPU_ERR_ARG, "server batch capacity must be positive");
+    if (cfg->max_batch_queries <= 0 || cfg->max_batch_keys == 0 || cfg->slots < 0)
+        return fail(KSSDGPU_ERR_ARG, "server batch capacity and slot count must be positive");
     CUDA_TRY(cudaSetDevice(ix->device));
+    const uint64_t dense = (uint64_t)cfg->max_batch_queries * (uint64_t)ix->nref;
+    const unsigned hit_cap = (unsigned)std::min<uint64_t>(dense, cfg->max_hits ? cfg->max_hits : (1ull << 22));
+    const uint64_t per_slot = server_slot_bytes(*cfg, ix->nref, hit_cap);
+    uint64_t budget = cfg->device_budget;
+    if (!budget) {
+        size_t free_b = 0, total_b = 0;
+        CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
+        budget = free_b / 2;
+    }
+    const uint64_t fit = budget / std::max<uint64_t>(per_slot, 1);
+    const int want = cfg->slots ? cfg->slots : 4;
+    if (fit < 1)
+        return fail(KSSDGPU_ERR_CAPACITY, "one server slot needs " + std::to_string(per_slot) +
+                                              " bytes of device memory, above the budget of " + std::to_string(budget));
     auto *s = new kssdgpu_server();
     s->ix = ix;
     s->cfg = *cfg;
-    const uint64_t dense = (uint64_t)cfg->max_batch_queries * (uint64_t)ix->nref;
-    s->hit_cap = (unsigned)std::min<uint64_t>(dense, cfg->max_hits ? cfg->max_hits : (1ull << 22));
+    s->hit_cap = hit_cap;
+    s->slot_bytes = per_slot;
+    s->slots.resize((size_t)std::min<uint64_t>((uint64_t)want, fit));
     for (auto &sl : s->slots) {
         const int rc = server_slot_alloc(s, sl);
         if (rc) {
@@ -387,6 +447,9 @@ int kssdgpu_server_submit(kssdgpu_server_t *s, const uint64_t *keys, uint64_t n_
     if (n_keys > s->cfg.max_batch_keys)
         return fail(KSSDGPU_ERR_CAPACITY, "query has more keys than a server slot admits (" +
                                               std::to_string(s->cfg.max_batch_keys) + ")");
+    for (uint64_t i = 1; i < n_keys; ++i)
+        if (keys[i - 1] > keys[i])
+            return fail(KSSDGPU_ERR_UNSORTED, "query keys are not sorted ascending (position " + std::to_string(i) + ")");
     auto r = std::make_shared<ServerRequest>();
     r->keys.assign(keys, keys + n_keys);
     {
@@ -466,10 +529,9 @@ int kssdgpu_server_stats(kssdgpu_server_t *s, kssdgpu_server_stats_t *out)
         out->mean_ms += x;
     if (!l.empty())
         out->mean_ms /= (double)l.size();
-    out->reserved_bytes = 0;
-    const size_t cells = (size_t)s->cfg.max_batch_queries * s->ix->nref;
-    out->reserved_bytes = 2 * (s->cfg.max_batch_keys * 8 + cells * 16 * ((s->cfg.flags & KSSDGPU_UNIQUE) ? 2 : 1) +
-                               (size_t)s->hit_cap * sizeof(kssdgpu_hit_t));
+    out->reserved_bytes = s->slot_bytes * s->slots.size();
+    out->slots = s->slots.size();
+    out->splits = s->splits;
     return KSSDGPU_OK;
 }
 
@@ -479,7 +541,7 @@ int kssdgpu_server_reset_stats(kssdgpu_server_t *s)
         return fail(KSSDGPU_ERR_ARG, "null server");
     std::lock_guard<std::mutex> lock(s->mu);
     s->latencies.clear();
-    s->batches = s->queries = s->max_inflight = s->overlapped = 0;
+    s->batches = s->queries = s->max_inflight = s->overlapped = s->splits = 0;
     return KSSDGPU_OK;
 }
 

@@ -364,7 +364,10 @@ __device__ __forceinline__ void process_entry(const CountParams &P, uint64_t i, 
 {
     const uint64_t key = __ldg(P.qkeys + i);
     const uint64_t ctx = key >> P.obj_bits;
-    if (i > b && (__ldg(P.qkeys + i - 1) >> P.obj_bits) == ctx)
+    const uint64_t prev = i > b ? __ldg(P.qkeys + i - 1) : 0;
+    if (prev > key)
+        atomicMax(P.err, (int)kDevUnsorted);  // a sample's keys must ascend (comblco order)
+    if (i > b && (prev >> P.obj_bits) == ctx)
         return;
     int s = 1;
     while (i + s < e && (__ldg(P.qkeys + i + s) >> P.obj_bits) == ctx)
@@ -401,7 +404,10 @@ __device__ __forceinline__ void process_query(const CountParams &P, uint64_t b, 
             if (i < ce) {
                 const uint64_t key = __ldg(P.qkeys + i);
                 ctx[u] = key >> P.obj_bits;
-                if (!(i > b && (__ldg(P.qkeys + i - 1) >> P.obj_bits) == ctx[u])) {
+                const uint64_t prev = i > b ? __ldg(P.qkeys + i - 1) : 0;
+                if (prev > key)
+                    atomicMax(P.err, (int)kDevUnsorted);  // a sample's keys must ascend (comblco order)
+                if (!(i > b && (prev >> P.obj_bits) == ctx[u])) {
                     int run = 1;
                     while (i + run < e && (__ldg(P.qkeys + i + run) >> P.obj_bits) == ctx[u])
                         ++run;
@@ -1212,6 +1218,188 @@ __global__ void k_self_conflict_groups(const unsigned long long *__restrict__ li
     }
 }
 
+// ------------------------------------------------------------------ self lower triangle: one-pass scan join
+//
+// The self step from the resident index alone, with nothing prepared beforehand: a
+// persistent grid streams the context-group boundaries (gbeg) tile by tile, queues
+// every group of >= 2 postings in shared memory and joins the queue at once -- one
+// thread per group of at most kScanLaneMax postings, the whole CTA for a larger one.
+// Every pair of gid runs of a group credits cell (higher gid, lower gid) with the
+// minimum object difference over the two runs' cross product (the higher gid's run is
+// the query run of count_lower at that context, src/command_ani.h:694-716);
+// --ignoreconflict skips reference (lower-gid) runs of several objects.
+
+constexpr uint32_t kScanThreads = 256;
+constexpr uint32_t kScanPerThread = 16;
+constexpr uint32_t kScanTile = kScanThreads * kScanPerThread;  // groups per tile (16 KB of gbeg)
+constexpr uint32_t kScanLaneMax = 32;                          // larger groups: the whole CTA
+
+__device__ __forceinline__ void credit_lower(unsigned long long *__restrict__ oc, unsigned long long *__restrict__ oo,
+                                             uint32_t qg, uint32_t rg, int d)
+{
+    const size_t cell = lower_cell(qg, rg);
+    atomicAdd(oc + cell, inc_ctx(d));
+    if (d)
+        atomicAdd(oo + cell, inc_obj(d));
+}
+
+// Query run [qb, qe) of gid qg against every reference run of [b, qb).
+__device__ __forceinline__ void join_query_run(const uint64_t *__restrict__ post, uint32_t b, uint32_t qb,
+                                               uint32_t qe, uint32_t qg, int ignoreconflict,
+                                               unsigned long long *__restrict__ oc, unsigned long long *__restrict__ oo)
+{
+    const uint32_t q0 = (uint32_t)__ldg(post + qb);
+    for (uint32_t rb = b; rb < qb;) {
+        const uint64_t r0 = __ldg(post + rb);
+        const uint32_t rg = (uint32_t)(r0 >> 32);
+        uint32_t re = rb + 1;
+        while (re < qb && (uint32_t)(__ldg(post + re) >> 32) == rg)
+            ++re;
+        if (!(ignoreconflict && re - rb > 1)) {
+            int d = kMinInit;
+            for (uint32_t x = qb; x < qe && d; ++x) {
+                const uint32_t qo = x == qb ? q0 : (uint32_t)__ldg(post + x);
+                for (uint32_t y = rb; y < re && d; ++y)
+                    d = min(d, dna_pop(qo ^ (uint32_t)__ldg(post + y)));
+            }
+            credit_lower(oc, oo, qg, rg, d);
+        }
+        rb = re;
+    }
+}
+
+// All run pairs of group [b, b + k) on one thread.
+__device__ __forceinline__ void join_group_lane(const uint64_t *__restrict__ post, uint32_t b, uint32_t k,
+                                                int ignoreconflict, unsigned long long *__restrict__ oc,
+                                                unsigned long long *__restrict__ oo)
+{
+    const uint32_t e = b + k;
+    const uint32_t g0 = (uint32_t)(__ldg(post + b) >> 32);
+    uint32_t qb = b + 1;
+    while (qb < e && (uint32_t)(__ldg(post + qb) >> 32) == g0)
+        ++qb;
+    while (qb < e) {
+        const uint32_t qg = (uint32_t)(__ldg(post + qb) >> 32);
+        uint32_t qe = qb + 1;
+        while (qe < e && (uint32_t)(__ldg(post + qe) >> 32) == qg)
+            ++qe;
+        join_query_run(post, b, qb, qe, qg, ignoreconflict, oc, oo);
+        qb = qe;
+    }
+}
+
+// All run pairs of group [b, b + k) on the whole CTA: thread t takes the query runs
+// starting at b + t, b + t + T, ...
+__device__ __forceinline__ void join_group_cta(const uint64_t *__restrict__ post, uint32_t b, uint32_t k,
+                                               int ignoreconflict, unsigned long long *__restrict__ oc,
+                                               unsigned long long *__restrict__ oo)
+{
+    const uint32_t e = b + k;
+    for (uint32_t x = b + 1 + threadIdx.x; x < e; x += blockDim.x) {
+        const uint32_t qg = (uint32_t)(__ldg(post + x) >> 32);
+        if ((uint32_t)(__ldg(post + x - 1) >> 32) == qg)
+            continue;  // not the first posting of its run
+        uint32_t qe = x + 1;
+        while (qe < e && (uint32_t)(__ldg(post + qe) >> 32) == qg)
+            ++qe;
+        join_query_run(post, b, x, qe, qg, ignoreconflict, oc, oo);
+    }
+}
+
+// Warp-aggregated append to a shared-memory counter; returns this lane's slot.
+__device__ __forceinline__ uint32_t smem_slot(uint32_t *counter, bool want, unsigned lane)
+{
+    const unsigned m = __ballot_sync(0xffffffffu, want);
+    uint32_t base = 0;
+    if (m && lane == (unsigned)(__ffs(m) - 1))
+        base = atomicAdd(counter, (uint32_t)__popc(m));
+    base = __shfl_sync(0xffffffffu, base, m ? __ffs(m) - 1 : 0);
+    return base + (uint32_t)__popc(m & ((1u << lane) - 1u));
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_self_scan(const uint32_t *__restrict__ gbeg, uint64_t u,
+                                                            const uint64_t *__restrict__ post, int ignoreconflict,
+                                                            unsigned long long *__restrict__ oc,
+                                                            unsigned long long *__restrict__ oo)
+{
+    // groups of 2..kScanLaneMax postings from the front, larger ones from the back
+    __shared__ unsigned long long queue[kScanTile];
+    __shared__ uint32_t n_lane, n_cta;
+    const unsigned lane = threadIdx.x & 31;
+    const uint64_t ntiles = (u + kScanTile - 1) / kScanTile;
+    bool waited = false;
+    for (uint64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        if (threadIdx.x == 0) {
+            n_lane = 0;
+            n_cta = 0;
+        }
+        __syncthreads();
+        const uint64_t base = t * kScanTile;
+        uint32_t beg[kScanPerThread], cnt[kScanPerThread];
+#pragma unroll
+        for (uint32_t j = 0; j < kScanPerThread; ++j) {
+            const uint64_t g = base + j * kScanThreads + threadIdx.x;
+            beg[j] = 0;
+            cnt[j] = 0;
+            if (g < u) {
+                beg[j] = __ldg(gbeg + g);
+                cnt[j] = __ldg(gbeg + g + 1);
+            }
+        }
+#pragma unroll
+        for (uint32_t j = 0; j < kScanPerThread; ++j) {
+            const uint32_t k = cnt[j] - beg[j];
+            const unsigned long long item = (unsigned long long)beg[j] | ((unsigned long long)k << 32);
+            const bool small = k >= 2 && k <= kScanLaneMax, large = k > kScanLaneMax;
+            const uint32_t s = smem_slot(&n_lane, small, lane);
+            if (small)
+                queue[s] = item;
+            const uint32_t l = smem_slot(&n_cta, large, lane);
+            if (large)
+                queue[kScanTile - 1 - l] = item;
+        }
+        __syncthreads();
+        if (!waited) {
+            pdl_wait_primary();  // the counters' zero fill has finished (no-op without a dependency)
+            waited = true;
+        }
+        const uint32_t nl = n_lane, nc = n_cta;
+        for (uint32_t i = threadIdx.x; i < nl; i += kScanThreads) {
+            const unsigned long long item = queue[i];
+            join_group_lane(post, (uint32_t)item, (uint32_t)(item >> 32), ignoreconflict, oc, oo);
+        }
+        for (uint32_t i = 0; i < nc; ++i) {
+            const unsigned long long item = queue[kScanTile - 1 - i];
+            join_group_cta(post, (uint32_t)item, (uint32_t)(item >> 32), ignoreconflict, oc, oo);
+        }
+        __syncthreads();  // the queue is refilled by the next tile
+    }
+}
+
+// Facts of the self join: groups of >= 2 postings, postings in them, their pairs.
+__global__ void k_self_stats(const uint32_t *__restrict__ gbeg, uint64_t u, unsigned long long *__restrict__ tot)
+{
+    unsigned long long g2 = 0, p2 = 0, pairs = 0;
+    for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < u; g += (uint64_t)gridDim.x * blockDim.x) {
+        const unsigned long long k = gbeg[g + 1] - gbeg[g];
+        if (k >= 2) {
+            ++g2;
+            p2 += k;
+            pairs += k * (k - 1) / 2;
+        }
+    }
+    for (int o = 16; o; o >>= 1) {
+        g2 += __shfl_down_sync(0xffffffffu, g2, o);
+        p2 += __shfl_down_sync(0xffffffffu, p2, o);
+        pairs += __shfl_down_sync(0xffffffffu, pairs, o);
+    }
+    if ((threadIdx.x & 31) == 0 && g2) {
+        atomicAdd(tot + 0, g2);
+        atomicAdd(tot + 1, p2);
+        atomicAdd(tot + 2, pairs);
+    }
+}
+
 // ------------------------------------------------------------------ sparse-scan candidate votes
 
 // Candidate nomination of the indexed sparse scan (src/pairwise_graph.c:1195-1246):
@@ -1328,6 +1516,9 @@ struct kssdgpu_index {
     DevBuf<int> s_order;
     DevBuf<WorkItem> s_items;
     DevBuf<uint32_t> s_prefix, s_counts;    // device-built chunk prefix of a query block
+    DevBuf<uint32_t> s_qcnt, s_rcnt, s_dcount;  // detail filter: sketch sizes, candidates per row
+    DevBuf<uint64_t> s_dprefix;             // detail filter: candidate offsets per row
+    DevBuf<kssdgpu_hit_t> s_hits;           // detail filter: the candidates
     cudaStream_t pipe_st[3] = {nullptr, nullptr, nullptr};  // host-buffer pipeline: H2D, count, D2H
     std::vector<cudaEvent_t> pipe_ev;
     // batched-count setting (kssdgpu_count_tune): shared-memory rows where they fit, or
@@ -1364,6 +1555,7 @@ struct kssdgpu_index {
     uint32_t j_n[3] = {0, 0, 0};
     unsigned long long j_postings = 0, j_pairs = 0;
     bool j_ready = false;
+    int scan_grid = 0;                      // CTAs of the one-pass scan join (resident per SM x SMs)
 };
 
 namespace {
@@ -1454,6 +1646,10 @@ int check_dev_err(kssdgpu_index *ix, cudaStream_t st)
     CUDA_TRY(cudaStreamSynchronize(st));
     if (herr) {
         cudaMemsetAsync(ix->err, 0, sizeof(int), st);
+        if (herr == kDevUnsorted)
+            return fail(KSSDGPU_ERR_UNSORTED, "query keys are not sorted ascending within a sample");
+        if (herr == kDevGid)
+            return fail(KSSDGPU_ERR_GID, "record gid is not below the reference count");
         return fail(KSSDGPU_ERR_TIMEOUT, "device probe loop exceeded its bound");
     }
     return KSSDGPU_OK;
@@ -1772,6 +1968,174 @@ int count_host_impl(kssdgpu_index *ix, const uint64_t *qkeys, const uint64_t *qo
         CUDA_TRY(cudaMemcpyAsync(uobj, uo, cells * 8, cudaMemcpyDeviceToHost, st));
     }
     return check_dev_err(ix, st);
+}
+
+// ------------------------------------------------------------------ detail-mode candidate filter
+//
+// The pre-filter of the reference's detail branch (src/command_ani.h:585-609), fused
+// behind the count on the device so that only candidate cells cross to the host.
+// A cell (i, j) of the dense block is a candidate when num_ctx >= ctxcut, both
+// sketch sizes are nonzero, max(num_ctx / qry_size, num_ctx / ref_size) >= afcut (all
+// exact: integer and IEEE double division), and its naive ANI reaches anicut minus a
+// margin: float 1 - diff_obj / num_ctx / 7 (IEEE float, exact), or with unique
+// contexts 1 - naive_dist of the unique or full counters (the 5% rule of
+// src/command_ani.h:437-440) in FP64 with the device's pow.  The margin makes the
+// device set a superset of the reference's: the host re-applies the exact test (its
+// own libm) to the candidates only.
+struct DetailFilter {
+    const uint32_t *qcnt;   // sketch sizes of the block's queries
+    const uint32_t *rcnt;   // sketch sizes of the references
+    uint32_t ctxcut;
+    double afcut;
+    double ani_lo;          // anicut minus the margin
+    int unique;
+};
+constexpr double kDetailMargin = 1e-9;  // far above pow's few-ulp difference, far below a printed digit
+
+// get_naive_dist (src/command_ani.h:202-224) in FP64 on the device
+__device__ __forceinline__ double naive_dist_dev(uint32_t xny, uint32_t diff, uint32_t sect)
+{
+    if (xny == 0)
+        return 1.0;
+    const double eps = 1e-8;  // EPSILON, src/model_ani.h:224
+    const double ratio = ((double)sect + eps) / ((double)diff + eps);
+    const double dist0 = (double)diff / (double)(xny + diff);
+    const double final_dist = 1.0 - pow(1.0 - dist0, ratio);
+    if (final_dist <= 0.0)
+        return 0.0;
+#if KSSD_NUM_CODENS < 11
+    const double scale = 0.1557143, intercept = 9.961e-5;
+#else
+    const double scale = 0.1544286, intercept = 7.133e-4;
+#endif
+    const double w = fmin(final_dist / 0.01, 1.0);  // NAIVE_DIST_INTERCEPT_RAMP_TAU
+    return final_dist * scale + intercept * w;
+}
+
+__device__ __forceinline__ bool detail_candidate(const DetailFilter &F, int i, int j, unsigned long long c,
+                                                 unsigned long long o, unsigned long long uc, unsigned long long uo)
+{
+    const uint32_t shared = (uint32_t)c;
+    if (shared < F.ctxcut)
+        return false;
+    const uint32_t qs = F.qcnt[i], rs = F.rcnt[j];
+    if (rs == 0 || qs == 0)
+        return false;
+    const double afq = (double)shared / (double)qs, afr = (double)shared / (double)rs;
+    if ((afq > afr ? afq : afr) < F.afcut)
+        return false;
+    double ani;
+    if (F.unique) {
+        const bool use_u = (uint64_t)(uint32_t)uc * 20 >= (uint64_t)rs;  // rs > 0 here
+        const unsigned long long xc = use_u ? uc : c, xo = use_u ? uo : o;
+        ani = 1.0 - naive_dist_dev((uint32_t)xc, (uint32_t)xo, (uint32_t)(xo >> 32));
+    } else {
+        const float dist = __fdiv_rn(__fdiv_rn(__uint2float_rn((uint32_t)o), __uint2float_rn(shared)), 7.0f);
+        ani = (double)__fsub_rn(1.0f, dist);
+    }
+    return ani >= F.ani_lo;
+}
+
+// Candidates per query row (one CTA per row).
+__global__ void __launch_bounds__(256) k_detail_count(const unsigned long long *__restrict__ oc,
+                                                      const unsigned long long *__restrict__ oo,
+                                                      const unsigned long long *__restrict__ uc,
+                                                      const unsigned long long *__restrict__ uo, int nq, int nref,
+                                                      DetailFilter F, uint32_t *__restrict__ counts)
+{
+    __shared__ uint32_t total;
+    for (int q = blockIdx.x; q < nq; q += gridDim.x) {
+        if (threadIdx.x == 0)
+            total = 0;
+        __syncthreads();
+        const size_t row = (size_t)q * nref;
+        uint32_t mine = 0;
+        for (int j = threadIdx.x; j < nref; j += blockDim.x)
+            mine += detail_candidate(F, q, j, oc[row + j], oo[row + j], uc ? uc[row + j] : 0ull,
+                                     uo ? uo[row + j] : 0ull);
+        for (int o = 16; o; o >>= 1)
+            mine += __shfl_down_sync(0xffffffffu, mine, o);
+        if ((threadIdx.x & 31) == 0 && mine)
+            atomicAdd(&total, mine);
+        __syncthreads();
+        if (threadIdx.x == 0)
+            counts[q] = total;
+        __syncthreads();
+    }
+}
+
+// The candidates of each row in ascending reference order at prefix[q] (one CTA per
+// row, an ordered compaction 256 cells at a time).
+__global__ void __launch_bounds__(256) k_detail_write(const unsigned long long *__restrict__ oc,
+                                                      const unsigned long long *__restrict__ oo,
+                                                      const unsigned long long *__restrict__ uc,
+                                                      const unsigned long long *__restrict__ uo, int nq, int nref,
+                                                      DetailFilter F, const uint64_t *__restrict__ prefix,
+                                                      kssdgpu_hit_t *__restrict__ hits)
+{
+    using Scan = cub::BlockScan<uint32_t, 256>;
+    __shared__ typename Scan::TempStorage tmp;
+    for (int q = blockIdx.x; q < nq; q += gridDim.x) {
+        const size_t row = (size_t)q * nref;
+        uint64_t at = prefix[q];
+        for (int j0 = 0; j0 < nref; j0 += 256) {
+            const int j = j0 + (int)threadIdx.x;
+            unsigned long long c = 0, o = 0, u = 0, v = 0;
+            bool keep = false;
+            if (j < nref) {
+                c = oc[row + j];
+                o = oo[row + j];
+                u = uc ? uc[row + j] : 0ull;
+                v = uo ? uo[row + j] : 0ull;
+                keep = detail_candidate(F, q, j, c, o, u, v);
+            }
+            uint32_t pos, sum;
+            Scan(tmp).ExclusiveSum(keep ? 1u : 0u, pos, sum);
+            if (keep) {
+                kssdgpu_hit_t h;
+                h.query = (uint32_t)q;
+                h.ref = (uint32_t)j;
+                h.num_ctx = (uint32_t)c;
+                h.num_mut2_ctx = (uint32_t)(c >> 32);
+                h.diff_obj = (uint32_t)o;
+                h.diff_obj_section = (uint32_t)(o >> 32);
+                h.u_num_ctx = (uint32_t)u;
+                h.u_num_mut2_ctx = (uint32_t)(u >> 32);
+                h.u_diff_obj = (uint32_t)v;
+                h.u_diff_obj_section = (uint32_t)(v >> 32);
+                hits[at + pos] = h;
+            }
+            at += sum;
+            __syncthreads();  // the scan storage is reused
+        }
+    }
+}
+
+// prefix[0] = 0, prefix[q + 1] = prefix[q] + counts[q] (one CTA)
+__global__ void __launch_bounds__(1024) k_detail_prefix(const uint32_t *__restrict__ counts, int nq,
+                                                        uint64_t *__restrict__ prefix)
+{
+    __shared__ unsigned long long part[1024];
+    const int per = (nq + 1023) / 1024;
+    const int q0 = min(nq, (int)threadIdx.x * per), q1 = min(nq, q0 + per);
+    unsigned long long sum = 0;
+    for (int q = q0; q < q1; ++q)
+        sum += counts[q];
+    part[threadIdx.x] = sum;
+    __syncthreads();
+    for (int o = 1; o < 1024; o <<= 1) {
+        const unsigned long long v = threadIdx.x >= (unsigned)o ? part[threadIdx.x - o] : 0ull;
+        __syncthreads();
+        part[threadIdx.x] += v;
+        __syncthreads();
+    }
+    unsigned long long run = threadIdx.x ? part[threadIdx.x - 1] : 0ull;
+    if (threadIdx.x == 0)
+        prefix[0] = 0;
+    for (int q = q0; q < q1; ++q) {
+        run += counts[q];
+        prefix[q + 1] = run;
+    }
 }
 
 // Runs of equal gid lists among the n sorted small groups -> chunks -> (chunk, pair)
@@ -2293,8 +2657,57 @@ int self_plan(kssdgpu_index *ix, cudaStream_t st)
     return KSSDGPU_OK;
 }
 
+// The one-pass self step: zero fill of the dense lower triangle (unless NO_ZERO), then
+// the scan join over the whole index.  When the fill stays in L2 the scan launches
+// programmatically after it and waits for it only before its first atomic, so its
+// first tiles' gbeg loads overlap the fill.
+int self_scan_impl(kssdgpu_index *ix, unsigned flags, unsigned long long *oc, unsigned long long *oo, cudaStream_t st)
+{
+    const size_t cells = (size_t)ix->nref * (ix->nref - 1) / 2;
+    if (!cells)
+        return KSSDGPU_OK;
+    bool after_fill = false;
+    if (!(flags & KSSDGPU_NO_ZERO)) {
+        if ((((uintptr_t)oc | (uintptr_t)oo) & 15) == 0) {
+            k_zero_pair<<<ix->sms * 8, 256, 0, st>>>(oc, oo, cells);
+            count_launch();
+            CUDA_TRY(cudaGetLastError());
+            after_fill = cells * 16 <= (size_t)ix->l2_bytes;
+        } else {
+            CUDA_TRY(cudaMemsetAsync(oc, 0, cells * 8, st));
+            CUDA_TRY(cudaMemsetAsync(oo, 0, cells * 8, st));
+        }
+    }
+    if (!ix->u)
+        return KSSDGPU_OK;
+    if (!ix->scan_grid) {
+        int per_sm = 0;
+        CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_self_scan, kScanThreads, 0));
+        ix->scan_grid = std::max(1, per_sm) * ix->sms;
+    }
+    const uint64_t ntiles = (ix->u + kScanTile - 1) / kScanTile;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)std::min<uint64_t>(ntiles, (uint64_t)ix->scan_grid));
+    cfg.blockDim = dim3(kScanThreads);
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    if (after_fill && KSSD_JOIN_PDL) {
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+    }
+    CUDA_TRY(cudaLaunchKernelEx(&cfg, k_self_scan, (const uint32_t *)ix->gbeg, ix->u, (const uint64_t *)ix->post,
+                                (flags & KSSDGPU_IGNORECONFLICT) ? 1 : 0, oc, oo));
+    count_launch();
+    CUDA_TRY(cudaGetLastError());
+    return KSSDGPU_OK;
+}
+
 int self_lower_dev_impl(kssdgpu_index *ix, unsigned flags, unsigned long long *oc, unsigned long long *oo, cudaStream_t st)
 {
+    if (!(flags & KSSDGPU_SELF_PLAN))
+        return self_scan_impl(ix, flags, oc, oo, st);
     int rc = self_plan(ix, st);
     if (rc)
         return rc;
@@ -2320,12 +2733,14 @@ int self_lower_dev_impl(kssdgpu_index *ix, unsigned flags, unsigned long long *o
 // Scratch of kssdgpu_count_block_noalloc, in the library's own static device
 // memory so that a call needs no cudaMalloc.  Layout (32-bit words):
 //   [0]       work counter of the persistent kernel
-//   [1]       error word
-//   [2, 34)   histogram of query size classes
-//   [34, 66)  scatter cursors of the size classes
-//   [128, ..) query order, largest size class first (KSSDGPU_NOALLOC_MAX_QUERIES ints)
-// The first 128 words are cleared at the start of every call; the order is fully
-// rewritten by every call before it is read.
+//   [2, 34)   histogram of query size classes          (shared-memory rows)
+//   [34, 66)  scatter cursors of the size classes      (shared-memory rows)
+//   [128, ..) query order, largest size class first    (shared-memory rows), or
+//   [127, ..) key-range chunk prefix, nq + 1 words      (global rows)
+// The first 128 words are cleared at the start of every call; the order or the
+// prefix is fully rewritten by every call before it is read.  Errors found on the
+// device (query keys out of order) go to the index's own error word, which
+// kssdgpu_sync reports.
 static __device__ __align__(256) unsigned int g_noalloc_scratch[KSSDGPU_NOALLOC_SCRATCH_BYTES / 4];
 
 namespace {
@@ -2366,6 +2781,34 @@ __global__ void k_noalloc_scatter(const uint64_t *__restrict__ offs, int nq, uns
         order[atomicAdd(scr + 34 + size_class(offs, q), 1u)] = q;
 }
 
+// prefix[0] = 0, prefix[q + 1] = prefix[q] + ceil(size(q) / chunk): the key-range
+// chunks of the global-row kernel, in one CTA (nq <= KSSDGPU_NOALLOC_MAX_QUERIES).
+__global__ void __launch_bounds__(1024) k_noalloc_prefix(const uint64_t *__restrict__ offs, int nq, uint32_t chunk,
+                                                         unsigned int *__restrict__ prefix)
+{
+    __shared__ unsigned int part[1024];
+    const int per = (nq + 1023) / 1024;
+    const int q0 = min(nq, (int)threadIdx.x * per), q1 = min(nq, q0 + per);
+    unsigned int sum = 0;
+    for (int q = q0; q < q1; ++q)
+        sum += (unsigned int)((offs[q + 1] - offs[q] + chunk - 1) / chunk);
+    part[threadIdx.x] = sum;
+    __syncthreads();
+    for (int o = 1; o < 1024; o <<= 1) {
+        const unsigned int v = threadIdx.x >= (unsigned)o ? part[threadIdx.x - o] : 0u;
+        __syncthreads();
+        part[threadIdx.x] += v;
+        __syncthreads();
+    }
+    unsigned int run = threadIdx.x ? part[threadIdx.x - 1] : 0u;
+    if (threadIdx.x == 0)
+        prefix[0] = 0;
+    for (int q = q0; q < q1; ++q) {
+        run += (unsigned int)((offs[q + 1] - offs[q] + chunk - 1) / chunk);
+        prefix[q + 1] = run;
+    }
+}
+
 std::mutex g_noalloc_mu;
 unsigned int *g_noalloc_addr[64] = {};
 
@@ -2399,6 +2842,12 @@ int kssdgpu_init(int device)
 {
     CUDA_TRY(cudaSetDevice(device));
     CUDA_TRY(cudaFree(nullptr));
+    if (device >= 0 && device < 64) {
+        // a fresh context (e.g. after the caller's cudaDeviceReset) may hold the
+        // no-allocation scratch elsewhere: look its address up again on next use
+        std::lock_guard<std::mutex> lock(g_noalloc_mu);
+        g_noalloc_addr[device] = nullptr;
+    }
     return KSSDGPU_OK;
 }
 
@@ -2790,11 +3239,23 @@ int kssdgpu_count_block_noalloc(kssdgpu_index_t *ix, const uint64_t *d_qry_keys,
     CUDA_TRY(cudaMemsetAsync(scr, 0, kNoallocHeaderWords * sizeof(unsigned int), st));
     if (nq == 0)
         return KSSDGPU_OK;
+    // the accumulator mode of kssdgpu_count_block_dev: global rows in key-range chunks
+    // unless shared-memory rows are forced or were chosen by the count autotuner
+    if ((flags & KSSDGPU_SMEM_ACC) && !(flags & KSSDGPU_GLOBAL_ACC) && !smem_row_fits(ix, flags))
+        return fail(KSSDGPU_ERR_CAPACITY, "shared-memory accumulator rows requested, but a row of " +
+                                              std::to_string(ix->nref) + " references does not fit");
+    const bool use_smem = uses_smem_row(ix, flags);
     const int grid = std::min((nq + 255) / 256, ix->sms * 8);
-    k_noalloc_hist<<<grid, 256, 0, st>>>(d_qry_offs, nq, scr);
-    k_noalloc_scan<<<1, 32, 0, st>>>(scr);
-    k_noalloc_scatter<<<grid, 256, 0, st>>>(d_qry_offs, nq, scr);
-    count_launch(3);
+    if (use_smem) {
+        k_noalloc_hist<<<grid, 256, 0, st>>>(d_qry_offs, nq, scr);
+        k_noalloc_scan<<<1, 32, 0, st>>>(scr);
+        k_noalloc_scatter<<<grid, 256, 0, st>>>(d_qry_offs, nq, scr);
+        count_launch(3);
+    } else {
+        k_noalloc_prefix<<<1, 1024, 0, st>>>(d_qry_offs, nq, ix->count_chunk_keys, scr + kNoallocHeaderWords - 1);
+        count_launch();
+    }
+    CUDA_TRY(cudaGetLastError());
     CountParams P{};
     P.table = ix->table;
     P.mask = ix->mask;
@@ -2811,11 +3272,12 @@ int kssdgpu_count_block_noalloc(kssdgpu_index_t *ix, const uint64_t *d_qry_keys,
     P.out_uctx = reinterpret_cast<unsigned long long *>(d_uctx);
     P.out_uobj = reinterpret_cast<unsigned long long *>(d_uobj);
     P.work = scr;
-    P.err = reinterpret_cast<int *>(scr + 1);
-    P.order = reinterpret_cast<const int *>(scr + kNoallocHeaderWords);
+    P.err = ix->err;
+    P.order = use_smem ? reinterpret_cast<const int *>(scr + kNoallocHeaderWords) : nullptr;
+    P.chunk_prefix = use_smem ? nullptr : scr + kNoallocHeaderWords - 1;
+    P.chunk_keys = ix->count_chunk_keys;
     const size_t cells = (size_t)nq * ix->nref;
     const size_t smem = (size_t)ix->nref * sizeof(unsigned long long) * (unique ? 4 : 2);
-    const bool use_smem = !(flags & KSSDGPU_GLOBAL_ACC) && smem <= kSmemRowLimit;
     if (!use_smem && !(flags & KSSDGPU_NO_ZERO)) {
         CUDA_TRY(cudaMemsetAsync(d_ctx, 0, cells * 8, st));
         CUDA_TRY(cudaMemsetAsync(d_obj, 0, cells * 8, st));
@@ -2835,17 +3297,116 @@ int kssdgpu_count_block_noalloc(kssdgpu_index_t *ix, const uint64_t *d_qry_keys,
     return unique ? launch_batched<false, true, false>(ix, P, 0, st) : launch_batched<false, false, false>(ix, P, 0, st);
 }
 
+int kssdgpu_count_detail(kssdgpu_index_t *ix, const uint64_t *qry_keys, const uint64_t *qry_offs, int nq,
+                         unsigned flags, const uint32_t *qry_ctx_count, const uint32_t *ref_ctx_count, int ctxcut,
+                         float afcut, float anicut, kssdgpu_hit_t *hits, uint64_t hits_cap, uint64_t *row_offs)
+{
+    if (!ix || nq < 0 || !row_offs || (nq > 0 && (!qry_offs || !qry_ctx_count || !ref_ctx_count)))
+        return fail(KSSDGPU_ERR_ARG, "invalid detail count arguments");
+    if (flags & (KSSDGPU_PLAIN | KSSDGPU_NO_ZERO | KSSDGPU_SELF_PLAN))
+        return fail(KSSDGPU_ERR_ARG, "the detail count takes KSSDGPU_IGNORECONFLICT, KSSDGPU_UNIQUE and the "
+                                     "accumulator flags only");
+    row_offs[0] = 0;
+    if (nq == 0)
+        return KSSDGPU_OK;
+    CUDA_TRY(cudaSetDevice(ix->device));
+    const uint64_t nkeys = qry_offs[nq] - qry_offs[0];
+    if (nkeys && !qry_keys)
+        return fail(KSSDGPU_ERR_ARG, "null query keys");
+    std::vector<uint64_t> sizes(nq);
+    for (int i = 0; i < nq; ++i) {
+        if (qry_offs[i + 1] < qry_offs[i])
+            return fail(KSSDGPU_ERR_ARG, "query offsets are not monotone");
+        sizes[i] = qry_offs[i + 1] - qry_offs[i];
+    }
+    const bool unique = (flags & KSSDGPU_UNIQUE) != 0;
+    std::vector<int> order(nq);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return sizes[a] > sizes[b]; });
+    std::vector<WorkItem> items;
+    if (!uses_smem_row(ix, flags))
+        build_chunks(qry_offs, nq, order.data(), ix->count_chunk_keys, items);
+    const int nref = ix->nref;
+    const size_t cells = (size_t)nq * nref;
+    CUDA_TRY(ix->s_keys.ensure(nkeys));
+    CUDA_TRY(ix->s_offs.ensure((size_t)nq + 1));
+    CUDA_TRY(ix->s_out.ensure(cells * (unique ? 4 : 2)));
+    CUDA_TRY(ix->s_order.ensure((size_t)nq));
+    CUDA_TRY(ix->s_items.ensure(items.size()));
+    CUDA_TRY(ix->s_qcnt.ensure((size_t)nq));
+    CUDA_TRY(ix->s_rcnt.ensure((size_t)nref));
+    CUDA_TRY(ix->s_dcount.ensure((size_t)nq));
+    CUDA_TRY(ix->s_dprefix.ensure((size_t)nq + 1));
+    cudaStream_t st = 0;
+    if (nkeys)
+        CUDA_TRY(cudaMemcpyAsync(ix->s_keys.p, qry_keys, nkeys * 8, cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaMemcpyAsync(ix->s_offs.p, qry_offs, ((size_t)nq + 1) * 8, cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaMemcpyAsync(ix->s_order.p, order.data(), (size_t)nq * sizeof(int), cudaMemcpyHostToDevice, st));
+    if (!items.empty())
+        CUDA_TRY(cudaMemcpyAsync(ix->s_items.p, items.data(), items.size() * sizeof(WorkItem), cudaMemcpyHostToDevice,
+                                 st));
+    CUDA_TRY(cudaMemcpyAsync(ix->s_qcnt.p, qry_ctx_count, (size_t)nq * 4, cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaMemcpyAsync(ix->s_rcnt.p, ref_ctx_count, (size_t)nref * 4, cudaMemcpyHostToDevice, st));
+    unsigned long long *oc = ix->s_out.p, *oo = oc + cells;
+    unsigned long long *uc = unique ? oo + cells : nullptr, *uo = unique ? uc + cells : nullptr;
+    int rc = count_dev_impl(ix, ix->s_keys.p, ix->s_offs.p, nq, 0, false, flags, oc, oo, uc, uo, ix->s_order.p, &sizes,
+                            st, items.empty() ? nullptr : ix->s_items.p, (int)items.size());
+    if (rc)
+        return rc;
+    DetailFilter F;
+    F.qcnt = ix->s_qcnt.p;
+    F.rcnt = ix->s_rcnt.p;
+    F.ctxcut = (uint32_t)ctxcut;
+    F.afcut = (double)afcut;
+    F.ani_lo = (double)anicut - kDetailMargin;
+    F.unique = unique ? 1 : 0;
+    const int grid = std::min(nq, ix->sms * 8);
+    k_detail_count<<<grid, 256, 0, st>>>(oc, oo, uc, uo, nq, nref, F, ix->s_dcount.p);
+    k_detail_prefix<<<1, 1024, 0, st>>>(ix->s_dcount.p, nq, ix->s_dprefix.p);
+    count_launch(2);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemcpyAsync(row_offs, ix->s_dprefix.p, ((size_t)nq + 1) * 8, cudaMemcpyDeviceToHost, st));
+    rc = check_dev_err(ix, st);  // synchronizes: row_offs is on the host now
+    if (rc)
+        return rc;
+    const uint64_t total = row_offs[nq];
+    if (total > hits_cap)
+        return fail(KSSDGPU_ERR_CAPACITY, "detail count: " + std::to_string(total) +
+                                              " candidate cells exceed the hit buffer of " + std::to_string(hits_cap) +
+                                              " (row_offs holds the sizes)");
+    if (!total)
+        return KSSDGPU_OK;
+    if (!hits)
+        return fail(KSSDGPU_ERR_ARG, "null hit buffer");
+    CUDA_TRY(ix->s_hits.ensure(total));
+    k_detail_write<<<grid, 256, 0, st>>>(oc, oo, uc, uo, nq, nref, F, ix->s_dprefix.p, ix->s_hits.p);
+    count_launch();
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemcpyAsync(hits, ix->s_hits.p, total * sizeof(kssdgpu_hit_t), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    return KSSDGPU_OK;
+}
+
 int kssdgpu_self_plan_info(kssdgpu_index_t *ix, uint64_t *groups, uint64_t *postings, uint64_t *pairs)
 {
     if (!ix)
         return fail(KSSDGPU_ERR_ARG, "null index");
     CUDA_TRY(cudaSetDevice(ix->device));
-    int rc = self_plan(ix, 0);
-    if (rc)
-        return rc;
-    if (groups) *groups = (uint64_t)ix->j_n[0] + ix->j_n[1] + ix->j_n[2];
-    if (postings) *postings = ix->j_postings;
-    if (pairs) *pairs = ix->j_pairs;
+    unsigned long long *d = nullptr, h[3] = {0, 0, 0};
+    CUDA_TRY(cudaMalloc(&d, sizeof h));
+    cudaError_t e = cudaMemset(d, 0, sizeof h);
+    if (e == cudaSuccess && ix->u) {
+        k_self_stats<<<grid_for(ix->u), 256>>>(ix->gbeg, ix->u, d);
+        count_launch();
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(h, d, sizeof h, cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess)
+        return fail(KSSDGPU_ERR_CUDA, std::string("self-join facts: ") + cudaGetErrorString(e));
+    if (groups) *groups = h[0];
+    if (postings) *postings = h[1];
+    if (pairs) *pairs = h[2];
     return KSSDGPU_OK;
 }
 

@@ -56,4 +56,6 @@ def main(path):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src/model_refaf_hgb.h")
+    if len(sys.argv) != 2:
+        sys.exit("usage: gen_hgb_table.py <reference src/model_refaf_hgb.h>")
+    main(sys.argv[1])

@@ -622,6 +622,60 @@ static double naive_of(const kssdgpu_ctx_mut2_t *c, const kssdgpu_obj_section_t 
     return kssd_naive_dist(&f);
 }
 
+/* The counters of one (query, reference) cell. */
+typedef struct cell {
+    kssdgpu_ctx_mut2_t c, uc;
+    kssdgpu_obj_section_t o, uo;
+} cell_t;
+
+/* Candidates of a detail block from kssdgpu_count_detail: the device applies the
+ * pre-filter of src/command_ani.h:585-609 with a margin below anicut, so only these
+ * cells (ascending (query, ref)) cross to the host; the host re-applies the exact test. */
+typedef struct detail_hits {
+    kssdgpu_hit_t *hits;
+    uint64_t *row_offs; /* nb + 1 */
+} detail_hits_t;
+
+static detail_hits_t detail_candidates(kssdgpu_index_t *ix, const kssd_sketch_t *q, int q0, int nb, unsigned flags,
+                                       const uint32_t *qcnt_block, const uint32_t *rcnt, const kssd_ani_opt_t *o)
+{
+    detail_hits_t d = {0};
+    d.row_offs = malloc(((size_t)nb + 1) * sizeof(uint64_t));
+    uint64_t cap = (uint64_t)nb * 64;
+    d.hits = malloc(cap * sizeof(kssdgpu_hit_t) + 1);
+    if (!d.row_offs || !d.hits)
+        err(EXIT_FAILURE, "OOM detail candidates");
+    const uint64_t *keys = q->keys + (q->offs[q0] - q->offs[0]);
+    int rc = kssdgpu_count_detail(ix, keys, q->offs + q0, nb, flags, qcnt_block, rcnt, o->ctxcut, o->afcut, o->anicut,
+                                  d.hits, cap, d.row_offs);
+    if (rc == KSSDGPU_ERR_CAPACITY) {
+        /* more candidates than the first guess: the call reported how many */
+        cap = d.row_offs[nb];
+        free(d.hits);
+        d.hits = malloc(cap * sizeof(kssdgpu_hit_t) + 1);
+        if (!d.hits)
+            err(EXIT_FAILURE, "OOM detail candidates");
+        rc = kssdgpu_count_detail(ix, keys, q->offs + q0, nb, flags, qcnt_block, rcnt, o->ctxcut, o->afcut,
+                                  o->anicut, d.hits, cap, d.row_offs);
+    }
+    gpu_check(rc, "device counting (detail candidates)");
+    return d;
+}
+
+static cell_t cell_of_hit(const kssdgpu_hit_t *h)
+{
+    cell_t x;
+    x.c.num_ctx = h->num_ctx;
+    x.c.num_mut2_ctx = h->num_mut2_ctx;
+    x.o.diff_obj = h->diff_obj;
+    x.o.diff_obj_section = h->diff_obj_section;
+    x.uc.num_ctx = h->u_num_ctx;
+    x.uc.num_mut2_ctx = h->u_num_mut2_ctx;
+    x.uo.diff_obj = h->u_diff_obj;
+    x.uo.diff_obj_section = h->u_diff_obj_section;
+    return x;
+}
+
 /* query blocks sized so that four counter blocks stay within ~2 GB of host memory */
 static int block_for(int nref, int nq)
 {
@@ -909,9 +963,17 @@ static int run_mem_eff(void)
     const unsigned flags = (o->ignoreconflict ? KSSDGPU_IGNORECONFLICT : 0) | (count_unique ? KSSDGPU_UNIQUE : 0);
     const int ntop = o->ntop > 0 ? o->ntop : R;
     const int B = block_for(R, qry->n);
+    /* detail mode keeps the dense counters on the device and takes only its candidates;
+     * the unique-context report prints every cell, so it takes the dense block */
+    const bool sparse = !o->fmt && !report;
     for (int q0 = 0; q0 < qry->n; q0 += B) {
         const int nb = qry->n - q0 < B ? qry->n - q0 : B;
-        counts_t c = count_queries(ix, R, qry, q0, nb, flags);
+        counts_t c = {0};
+        detail_hits_t dh = {0};
+        if (sparse)
+            dh = detail_candidates(ix, qry, q0, nb, flags, qcnt + q0, rcnt, o);
+        else
+            c = count_queries(ix, R, qry, q0, nb, flags);
         if (report) {
             kssd_buf_t rb = {0};
             print_unique_block(&rb, R, q0, nb, rcnt, qcnt, uref, &c, ref->names, qry->names);
@@ -924,30 +986,42 @@ static int run_mem_eff(void)
             const int qg = q0 + i;
             const size_t a_size = (size_t)(qry->offs[qg + 1] - qry->offs[qg]);
             kssd_buf_t *b = &rows[i];
-            const kssdgpu_ctx_mut2_t *cx = c.ctx + (size_t)i * R;
-            const kssdgpu_obj_section_t *ob = c.obj + (size_t)i * R;
+            const kssdgpu_ctx_mut2_t *cx = c.ctx ? c.ctx + (size_t)i * R : NULL;
+            const kssdgpu_obj_section_t *ob = c.obj ? c.obj + (size_t)i * R : NULL;
             const kssdgpu_ctx_mut2_t *ucx = c.uctx ? c.uctx + (size_t)i * R : NULL;
             const kssdgpu_obj_section_t *uob = c.uobj ? c.uobj + (size_t)i * R : NULL;
+            /* this query's cells: the dense row, or its device candidates (ascending ref) */
+            const kssdgpu_hit_t *hq = sparse ? dh.hits + dh.row_offs[i] : NULL;
+            const int hn = sparse ? (int)(dh.row_offs[i + 1] - dh.row_offs[i]) : 0;
+            cell_t *cells = sparse ? malloc((size_t)(hn ? hn : 1) * sizeof(cell_t)) : NULL;
+            for (int k = 0; k < hn; ++k)
+                cells[k] = cell_of_hit(&hq[k]);
             uint32_t *ids = NULL;
             int out_n = 0;
             if (!o->fmt) {
                 /* detail candidates and ranking, src/command_ani.h:577-621 */
                 if (a_size) {
-                    idani_t *cand = malloc((size_t)R * sizeof(idani_t) + 8);
-                    urank_t *ranks = o->unique_ctx ? malloc((size_t)R * sizeof(urank_t) + 16) : NULL;
+                    const int span = sparse ? hn : R;
+                    idani_t *cand = malloc((size_t)span * sizeof(idani_t) + 8);
+                    urank_t *ranks = o->unique_ctx ? malloc((size_t)span * sizeof(urank_t) + 16) : NULL;
                     int m = 0;
-                    for (int j = 0; j < R; ++j) {
-                        const uint32_t shared = cx[j].num_ctx;
+                    for (int k = 0; k < span; ++k) {
+                        const int j = sparse ? (int)hq[k].ref : k;
+                        const kssdgpu_ctx_mut2_t *cj = sparse ? &cells[k].c : &cx[j];
+                        const kssdgpu_obj_section_t *oj = sparse ? &cells[k].o : &ob[j];
+                        const uint32_t shared = cj->num_ctx;
                         if (shared < (uint32_t)o->ctxcut)
                             continue;
                         if (rcnt[j] == 0 || qcnt[qg] == 0 ||
                             !kssd_af_pass(o, (double)shared / (double)qcnt[qg], (double)shared / (double)rcnt[j]))
                             continue;
-                        float dist = (float)ob[j].diff_obj / cx[j].num_ctx / 7;
+                        float dist = (float)oj->diff_obj / cj->num_ctx / 7;
                         double ani = (float)(1 - dist);
                         if (ranks) {
-                            const bool use_u = kssd_use_unique_context(ucx[j].num_ctx, rcnt[j]);
-                            ani = 1.0 - (use_u ? naive_of(&ucx[j], &uob[j]) : naive_of(&cx[j], &ob[j]));
+                            const kssdgpu_ctx_mut2_t *ucj = sparse ? &cells[k].uc : &ucx[j];
+                            const kssdgpu_obj_section_t *uoj = sparse ? &cells[k].uo : &uob[j];
+                            const bool use_u = kssd_use_unique_context(ucj->num_ctx, rcnt[j]);
+                            ani = 1.0 - (use_u ? naive_of(ucj, uoj) : naive_of(cj, oj));
                         }
                         if (ani < o->anicut)
                             continue;
@@ -982,7 +1056,27 @@ static int run_mem_eff(void)
             size_t cov_n = 0;
             for (int n = 0; n < loop; ++n) {
                 const int j = o->fmt ? n : (int)ids[n];
-                kssd_features_t f = feat_of(&cx[j], &ob[j]);
+                cell_t cl = {0};
+                if (sparse) {
+                    /* the candidate of reference j (candidates ascend by ref) */
+                    int lo = 0, hi = hn - 1;
+                    while (lo < hi) {
+                        const int mid = (lo + hi) >> 1;
+                        if ((int)hq[mid].ref < j)
+                            lo = mid + 1;
+                        else
+                            hi = mid;
+                    }
+                    cl = cells[lo];
+                } else {
+                    cl.c = cx[j];
+                    cl.o = ob[j];
+                    if (ucx) {
+                        cl.uc = ucx[j];
+                        cl.uo = uob[j];
+                    }
+                }
+                kssd_features_t f = feat_of(&cl.c, &cl.o);
                 const int rsize = (int)rcnt[j];
                 if (qsize == 0 || rsize == 0) {
                     if (o->fmt)
@@ -999,8 +1093,8 @@ static int run_mem_eff(void)
                 kssd_row_t row = kssd_make_row((uint32_t)j, &f, o, (uint32_t)qsize, (uint32_t)rsize, af_q, bq, af_r, br,
                                                qry->meta ? &qry->meta[qg] : NULL, ref->meta ? &ref->meta[j] : NULL);
                 if (o->unique_ctx) {
-                    row.unique_ctx_selected = kssd_use_unique_context(ucx[j].num_ctx, rcnt[j]);
-                    row.naive_dist = row.unique_ctx_selected ? naive_of(&ucx[j], &uob[j]) : naive_of(&cx[j], &ob[j]);
+                    row.unique_ctx_selected = kssd_use_unique_context(cl.uc.num_ctx, rcnt[j]);
+                    row.naive_dist = row.unique_ctx_selected ? naive_of(&cl.uc, &cl.uo) : naive_of(&cl.c, &cl.o);
                     kssd_finalize_row(&row, o);
                 }
                 const double metric = o->s < 0 ? row.selected_ani : row.metric;
@@ -1025,6 +1119,7 @@ static int run_mem_eff(void)
             if (o->fmt)
                 kssd_buf_putc(b, '\n');
             free(ids);
+            free(cells);
         }
         for (int i = 0; i < nb; ++i) {
             write_buf(out, &rows[i]);
@@ -1032,6 +1127,8 @@ static int run_mem_eff(void)
         }
         free(rows);
         free_counts(&c);
+        free(dh.hits);
+        free(dh.row_offs);
     }
     if (report && fclose(report) != 0)
         err(errno, "Cannot finish unique-context report");

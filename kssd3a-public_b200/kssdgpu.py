@@ -24,6 +24,7 @@ PLAIN = 0x4
 GLOBAL_ACC = 0x8
 NO_ZERO = 0x10
 SMEM_ACC = 0x20
+SELF_PLAN = 0x40
 
 _u64p = np.ctypeslib.ndpointer(dtype=np.uint64, flags="C_CONTIGUOUS")
 _u32p = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
@@ -64,6 +65,8 @@ def gpu_lib() -> C.CDLL:
         lib.kssdgpu_index_ref_ctx_counts.argtypes = [vp, C.c_int, C.c_int, vp, vp]
         lib.kssdgpu_count_block.argtypes = [vp, vp, _u64p, C.c_int, C.c_uint, vp, vp, vp, vp]
         lib.kssdgpu_count_lower.argtypes = [vp, vp, _u64p, C.c_int, C.c_int, C.c_uint, vp, vp]
+        lib.kssdgpu_count_detail.argtypes = [vp, vp, _u64p, C.c_int, C.c_uint, _u32p, _u32p, C.c_int, C.c_float,
+                                             C.c_float, vp, C.c_uint64, _u64p]
         lib.kssdgpu_count_block_dev.argtypes = [vp, vp, vp, C.c_int, C.c_int, C.c_int, C.c_uint,
                                                 vp, vp, vp, vp, vp]
         lib.kssdgpu_sync.argtypes = [vp, vp]
@@ -93,7 +96,7 @@ def gpu_lib() -> C.CDLL:
 
 class _ServerConfig(C.Structure):
     _fields_ = [("max_batch_queries", C.c_int), ("max_batch_keys", C.c_uint64), ("max_hits", C.c_uint64),
-                ("flags", C.c_uint)]
+                ("flags", C.c_uint), ("slots", C.c_int), ("device_budget", C.c_uint64)]
 
 
 class _CountTuning(C.Structure):
@@ -103,7 +106,8 @@ class _CountTuning(C.Structure):
 class _ServerStats(C.Structure):
     _fields_ = [("completed", C.c_uint64), ("batches", C.c_uint64), ("pending", C.c_uint64),
                 ("max_inflight", C.c_uint64), ("overlapped_batches", C.c_uint64), ("reserved_bytes", C.c_uint64),
-                ("p50_ms", C.c_double), ("p99_ms", C.c_double), ("max_ms", C.c_double), ("mean_ms", C.c_double)]
+                ("p50_ms", C.c_double), ("p99_ms", C.c_double), ("max_ms", C.c_double), ("mean_ms", C.c_double),
+                ("slots", C.c_uint64), ("splits", C.c_uint64)]
 
 
 HIT_DTYPE = np.dtype([("query", "<u4"), ("ref", "<u4"), ("num_ctx", "<u4"), ("num_mut2_ctx", "<u4"),
@@ -136,14 +140,20 @@ def host_lib() -> C.CDLL:
     if _host is None:
         lib = _load("libkssdhost.so")
         lib.kssd_host_last_error.restype = C.c_char_p
-        lib.kssd_synth_default.argtypes = [C.POINTER(_SynthCfg)]
-        lib.kssd_synth_default.restype = None
-        lib.kssd_synth_generate.argtypes = [C.POINTER(_SynthCfg)]
-        lib.kssd_synth_generate.restype = C.POINTER(_SynthOut)
-        lib.kssd_synth_free.argtypes = [C.POINTER(_SynthOut)]
-        lib.kssd_synth_free.restype = None
+        bind_synth(lib)
         _host = lib
     return _host
+
+
+def bind_synth(lib: C.CDLL) -> C.CDLL:
+    """Declares the generator's entry points (host/kssd_synth.h) on a loaded library."""
+    lib.kssd_synth_default.argtypes = [C.POINTER(_SynthCfg)]
+    lib.kssd_synth_default.restype = None
+    lib.kssd_synth_generate.argtypes = [C.POINTER(_SynthCfg)]
+    lib.kssd_synth_generate.restype = C.POINTER(_SynthOut)
+    lib.kssd_synth_free.argtypes = [C.POINTER(_SynthOut)]
+    lib.kssd_synth_free.restype = None
+    return lib
 
 
 def _check(rc: int):
@@ -177,10 +187,12 @@ class Sketch:
         return len(self.offs) - 1
 
 
-def synth(**kw) -> Sketch:
-    """Generate a synthetic sketch (see host/kssd_synth.h for the model and fields)."""
+def synth(lib: C.CDLL | None = None, **kw) -> Sketch:
+    """Generate a synthetic sketch (see host/kssd_synth.h for the model and fields).
+    lib: another build of the same generator, declared with bind_synth (default: the
+    host library)."""
     prefix = kw.pop("name_prefix", None)
-    lib = host_lib()
+    lib = lib or host_lib()
     cfg = _SynthCfg()
     lib.kssd_synth_default(C.byref(cfg))
     for k, v in kw.items():
@@ -368,6 +380,25 @@ class Index:
                                              qry_gid_offset, flags, ctx.ctypes.data, obj.ctypes.data))
         return ctx, obj
 
+    def count_detail(self, qkeys: np.ndarray, qoffs: np.ndarray, qry_ctx_count, ref_ctx_count, flags: int = 0,
+                     ctxcut: int = 3, afcut: float = 0.5, anicut: float = 0.95, cap: int = 1 << 20):
+        """Detail-mode candidates filtered on the device: (hits HIT_DTYPE array ascending
+        (query, ref), row_offs [nq + 1])."""
+        nq = len(qoffs) - 1
+        qk = np.ascontiguousarray(qkeys, dtype=np.uint64)
+        qo = np.ascontiguousarray(qoffs, dtype=np.uint64)
+        qc = np.ascontiguousarray(qry_ctx_count, dtype=np.uint32)
+        rc_ = np.ascontiguousarray(ref_ctx_count, dtype=np.uint32)
+        row_offs = np.zeros(nq + 1, dtype=np.uint64)
+        hits = np.zeros(max(cap, 1), dtype=HIT_DTYPE)
+        rc = gpu_lib().kssdgpu_count_detail(self._h, qk.ctypes.data if len(qk) else None, qo, nq, flags, qc, rc_,
+                                            ctxcut, afcut, anicut, hits.ctypes.data, cap, row_offs)
+        if rc == 7 and row_offs[-1] > cap:  # more candidates than the guess: the call reported how many
+            return self.count_detail(qkeys, qoffs, qry_ctx_count, ref_ctx_count, flags, ctxcut, afcut, anicut,
+                                     int(row_offs[-1]))
+        _check(rc)
+        return hits[: int(row_offs[-1])], row_offs
+
     def self_lower(self, flags: int = 0):
         """Packed lower triangle: arrays [nref*(nref-1)/2, 2] of (num_ctx, mut2) and (diff_obj, section)."""
         cells = self.nref * (self.nref - 1) // 2
@@ -434,9 +465,10 @@ class Index:
 class Server:
     """Continuous-batching query server over a resident Index (libkssdgpu kssdgpu_server_*)."""
 
-    def __init__(self, index: Index, max_batch_queries=256, max_batch_keys=1 << 26, max_hits=0, flags=0):
+    def __init__(self, index: Index, max_batch_queries=256, max_batch_keys=1 << 26, max_hits=0, flags=0, slots=0,
+                 device_budget=0):
         self.index = index  # keep the index alive
-        cfg = _ServerConfig(max_batch_queries, max_batch_keys, max_hits, flags)
+        cfg = _ServerConfig(max_batch_queries, max_batch_keys, max_hits, flags, slots, device_budget)
         h = C.c_void_p()
         _check(gpu_lib().kssdgpu_server_create(index.handle, C.byref(cfg), C.byref(h)))
         self._h = h

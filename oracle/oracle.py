@@ -51,6 +51,21 @@ def oracle_lib() -> C.CDLL:
     return _orc
 
 
+_work = None
+
+
+def workload_lib() -> C.CDLL:
+    """oracle/libworkload.so: the seeded synthetic-sketch generator built on its own
+    (declare its entry points with kssdgpu.bind_synth before use)."""
+    global _work
+    if _work is None:
+        path = os.path.join(HERE, "libworkload.so")
+        if not os.path.exists(path):
+            raise ImportError(f"{path} missing: run `make -C {HERE}`")
+        _work = C.CDLL(path)
+    return _work
+
+
 def ref_available() -> bool:
     return os.path.exists(os.path.join(REF_DIR, "refharness.so")) and os.path.exists(REF_BIN)
 

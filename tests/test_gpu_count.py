@@ -67,17 +67,52 @@ def test_count_lower_blocks(case, flags):
             np.testing.assert_array_equal(g, w)
 
 
+SELF_PATHS = [0, kssdgpu.SELF_PLAN]  # one-pass scan join (default), cached set-major plan
+
+
 @pytest.mark.parametrize("case", CASES[::3])
 @pytest.mark.parametrize("ign", [False, True])
-def test_self_lower_join(case, ign):
+@pytest.mark.parametrize("path", SELF_PATHS)
+def test_self_lower_join(case, ign, path):
     rk, ro, _, _ = _fixture(*case)
     rec = oracle.build_index(rk, ro)
     nref = len(ro) - 1
     idx = kssdgpu.Index.from_records(rec, nref)
-    got = idx.self_lower(kssdgpu.IGNORECONFLICT if ign else 0)
+    got = idx.self_lower((kssdgpu.IGNORECONFLICT if ign else 0) | path)
     want = oracle.self_lower_all(rec, rk, ro, ignoreconflict=ign)
     np.testing.assert_array_equal(got[0], want[0])
     np.testing.assert_array_equal(got[1], want[1])
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2])
+@pytest.mark.parametrize("conflict", [False, True])
+@pytest.mark.parametrize("ign", [False, True])
+def test_self_scan_large_groups(seed, conflict, ign):
+    """Context groups of more than 32 postings (the scan join's whole-CTA path), with and
+    without multi-object gid runs, mixed with small groups and empty samples."""
+    rng = np.random.default_rng(100 + seed)
+    refs = random_samples(rng, 70, 60, 12, 64 if conflict else 1 << 20, conflict)
+    refs += random_samples(rng, 30, 40, 5000, 1 << 20, conflict)
+    rk, ro = samples_to_sketch(refs)
+    rec = oracle.build_index(rk, ro)
+    nref = len(ro) - 1
+    idx = kssdgpu.Index.from_records(rec, nref)
+    assert idx.self_plan_info()["postings"] > 0
+    want = oracle.self_lower_all(rec, rk, ro, ignoreconflict=ign)
+    for path in SELF_PATHS:
+        got = idx.self_lower((kssdgpu.IGNORECONFLICT if ign else 0) | path)
+        np.testing.assert_array_equal(got[0], want[0])
+        np.testing.assert_array_equal(got[1], want[1])
+
+
+def test_self_plan_info_counts_groups():
+    rk, ro, _, _ = _fixture(*CASES[12])
+    rec = oracle.build_index(rk, ro)
+    idx = kssdgpu.Index.from_records(rec, len(ro) - 1)
+    ctx = (np.frombuffer(rec.tobytes(), dtype=np.dtype([("cg", "<u8"), ("obj", "<u4")]))["cg"] >> np.uint64(20))
+    _, k = np.unique(ctx, return_counts=True)
+    k = k[k >= 2].astype(np.int64)
+    assert idx.self_plan_info() == dict(groups=len(k), postings=int(k.sum()), pairs=int((k * (k - 1) // 2).sum()))
 
 
 @pytest.mark.parametrize("case", CASES[::4])
@@ -112,10 +147,11 @@ def test_synthetic_genomes_block_and_self():
     for g, w in zip(got, want):
         np.testing.assert_array_equal(g, w)
     assert want[0][:, :, 0].sum() > 0
-    got = idx.self_lower()
     want = oracle.self_lower_all(rec, sk.keys, sk.offs)
-    np.testing.assert_array_equal(got[0], want[0])
-    np.testing.assert_array_equal(got[1], want[1])
+    for path in SELF_PATHS:
+        got = idx.self_lower(path)
+        np.testing.assert_array_equal(got[0], want[0])
+        np.testing.assert_array_equal(got[1], want[1])
 
 
 def _clustered_sketch(kind="pairs"):
@@ -143,7 +179,7 @@ def test_self_join_plan_settings(monkeypatch, flat, chunk, srt, kind):
     rec = oracle.build_index(sk.keys, sk.offs)
     idx = kssdgpu.Index.from_records(rec, sk.n)
     want = oracle.self_lower_all(rec, sk.keys, sk.offs)
-    got = idx.self_lower()
+    got = idx.self_lower(kssdgpu.SELF_PLAN)
     np.testing.assert_array_equal(got[0], want[0])
     np.testing.assert_array_equal(got[1], want[1])
     t = idx.self_plan_tune()  # pinned by the environment: defaults kept, nothing timed
@@ -169,11 +205,11 @@ def test_self_join_compact_counters(monkeypatch, kind, compact):
     d_c = torch.full((cells,), 0x3C3C3C3C3C3C3C3C, dtype=torch.int64, device="cuda")
     d_o = torch.full((cells,), -7, dtype=torch.int64, device="cuda")
     for _ in range(2):
-        idx.self_lower_dev(d_c, d_o)
+        idx.self_lower_dev(d_c, d_o, flags=kssdgpu.SELF_PLAN)
         torch.cuda.synchronize()
         np.testing.assert_array_equal(d_c.cpu().numpy().view(np.uint32).reshape(-1, 2), want[0])
         np.testing.assert_array_equal(d_o.cpu().numpy().view(np.uint32).reshape(-1, 2), want[1])
-    idx.self_lower_dev(d_c, d_o, flags=kssdgpu.NO_ZERO)  # adds a second copy of every count
+    idx.self_lower_dev(d_c, d_o, flags=kssdgpu.NO_ZERO | kssdgpu.SELF_PLAN)  # adds a second copy of every count
     torch.cuda.synchronize()
     np.testing.assert_array_equal(d_c.cpu().numpy().view(np.uint32).reshape(-1, 2), 2 * want[0])
     np.testing.assert_array_equal(d_o.cpu().numpy().view(np.uint32).reshape(-1, 2), 2 * want[1])
@@ -188,13 +224,14 @@ def test_self_join_autotuner_keeps_counts(monkeypatch):
     t = idx.self_plan_tune()
     assert t["candidates"] == 9 and 1 <= t["flat_groups"] <= 4 and t["step_ms"] > 0
     want = oracle.self_lower_all(rec, sk.keys, sk.offs)
-    got = idx.self_lower()
+    got = idx.self_lower(kssdgpu.SELF_PLAN)
     np.testing.assert_array_equal(got[0], want[0])
     np.testing.assert_array_equal(got[1], want[1])
 
 
 @pytest.mark.parametrize("misalign", [0, 8])
-def test_self_lower_dev_overwrites_stale_counters(misalign):
+@pytest.mark.parametrize("path", SELF_PATHS)
+def test_self_lower_dev_overwrites_stale_counters(misalign, path):
     """kssdgpu_self_lower_dev zero-fills the device counters before the join adds into
     them (the join may start under the fill's tail and waits for it before its first
     atomic): counters full of stale values come out equal to the oracle's, repeatedly.
@@ -213,7 +250,7 @@ def test_self_lower_dev_overwrites_stale_counters(misalign):
     for rep in range(3):
         buf_c.fill_(0x5A5A5A5A5A5A5A5A - rep)
         buf_o.fill_(-1 - rep)
-        idx.self_lower_dev(d_c, d_o)
+        idx.self_lower_dev(d_c, d_o, flags=path)
         torch.cuda.synchronize()
         got_c = d_c.cpu().numpy().view(np.uint32).reshape(-1, 2)
         got_o = d_o.cpu().numpy().view(np.uint32).reshape(-1, 2)
@@ -429,3 +466,73 @@ def test_pinned_host_buffers_pipeline(mode):
     assert rc == 0, lib.kssdgpu_last_error()
     for g, w in zip(outs, want):
         np.testing.assert_array_equal(g.numpy().view(np.uint32).reshape(n, n, 2), w)
+
+
+def _naive_ani(xny, diff, sect):
+    """1 - get_naive_dist (src/command_ani.h:202-224), numpy FP64."""
+    xny, diff, sect = (np.asarray(v, dtype=np.float64) for v in (xny, diff, sect))
+    with np.errstate(divide="ignore", invalid="ignore"):
+        ratio = (sect + 1e-8) / (diff + 1e-8)
+        dist0 = diff / (xny + diff)
+        fd = 1 - np.power(1 - dist0, ratio)
+    w = np.minimum(fd / 0.01, 1.0)
+    d = np.where(fd <= 0, 0.0, fd * 0.1544286 + 7.133e-4 * w)
+    return 1 - np.where(xny == 0, 1.0, d)
+
+
+@pytest.mark.parametrize("flags", [0, kssdgpu.UNIQUE, kssdgpu.UNIQUE | kssdgpu.IGNORECONFLICT])
+@pytest.mark.parametrize("cuts", [(3, 0.5, 0.95), (1, 0.0, 0.0), (5, 0.3, 0.85)])
+def test_count_detail_candidates(flags, cuts):
+    """kssdgpu_count_detail keeps every cell the reference's detail pre-filter keeps
+    (the candidates are a superset within the 1e-9 ANI margin), in ascending (query,
+    ref) order with the dense block's counters."""
+    ctxcut, afcut, anicut = cuts
+    ref = kssdgpu.synth(n_samples=150, n_clusters=15, len_median=3e5, len_min=1e5, len_max=1e6,
+                        size_dist=kssdgpu.SIZE_LOGNORMAL, sub_lo=0.001, sub_hi=0.08, seed=51, sample_seed=51)
+    qry = kssdgpu.synth(n_samples=30, n_clusters=15, role=kssdgpu.ROLE_OWNLEN, len_median=3e5, len_min=1e5,
+                        len_max=1e6, size_dist=kssdgpu.SIZE_LOGNORMAL, own_len_min=5e4, own_len_max=1.2e6,
+                        seed=51, sample_seed=52)
+    rec = oracle.build_index(ref.keys, ref.offs)
+    idx = kssdgpu.Index.from_records(rec, ref.n)
+    rcnt = np.diff(ref.offs).astype(np.uint32)
+    qcnt = np.diff(qry.offs).astype(np.uint32)
+    hits, roffs = idx.count_detail(qry.keys, qry.offs, qcnt, rcnt, flags, ctxcut, afcut, anicut, cap=64)
+    dense = oracle.count_block(rec, ref.n, qry.keys, qry.offs, unique=True,
+                               ignoreconflict=bool(flags & kssdgpu.IGNORECONFLICT))
+    c, o, uc, uo = (x.astype(np.int64) for x in dense)
+    shared = c[:, :, 0]
+    with np.errstate(divide="ignore", invalid="ignore"):
+        af = np.maximum(shared / qcnt[:, None].astype(np.float64), shared / rcnt[None, :].astype(np.float64))
+        if flags & kssdgpu.UNIQUE:
+            use_u = uc[:, :, 0] * 20 >= rcnt[None, :]
+            ani = np.where(use_u, _naive_ani(uc[:, :, 0], uo[:, :, 0], uo[:, :, 1]),
+                           _naive_ani(c[:, :, 0], o[:, :, 0], o[:, :, 1]))
+        else:
+            dist = (o[:, :, 0].astype(np.float32) / shared.astype(np.float32)) / np.float32(7)
+            ani = (np.float32(1) - dist).astype(np.float64)
+    base = (shared >= ctxcut) & (qcnt[:, None] > 0) & (rcnt[None, :] > 0) & (af >= np.float64(np.float32(afcut)))
+    exact = base & (ani >= np.float64(np.float32(anicut)))
+    loose = base & (ani >= np.float64(np.float32(anicut)) - 1e-9)
+    got = np.zeros_like(exact)
+    got[hits["query"], hits["ref"]] = True
+    assert (exact <= got).all() and (got <= loose).all()
+    assert exact.sum() > 0
+    assert np.all(np.diff(hits["query"].astype(np.int64) * ref.n + hits["ref"]) > 0)
+    np.testing.assert_array_equal(roffs, np.concatenate([[0], np.cumsum(got.sum(axis=1))]))
+    q, r = hits["query"], hits["ref"]
+    np.testing.assert_array_equal(hits["num_ctx"], dense[0][q, r, 0])
+    np.testing.assert_array_equal(hits["num_mut2_ctx"], dense[0][q, r, 1])
+    np.testing.assert_array_equal(hits["diff_obj"], dense[1][q, r, 0])
+    np.testing.assert_array_equal(hits["diff_obj_section"], dense[1][q, r, 1])
+    if flags & kssdgpu.UNIQUE:
+        np.testing.assert_array_equal(hits["u_num_ctx"], dense[2][q, r, 0])
+        np.testing.assert_array_equal(hits["u_diff_obj_section"], dense[3][q, r, 1])
+    if oracle.ref_available():
+        # the reference's own detail pre-filter keeps exactly the exact set
+        _, npass, ranked = oracle.count_detail_ref(rec, ref.n, qry.keys, qry.offs, rcnt, qcnt,
+                                                   ignoreconflict=bool(flags & kssdgpu.IGNORECONFLICT),
+                                                   unique=bool(flags & kssdgpu.UNIQUE), ctxcut=ctxcut, afcut=afcut,
+                                                   anicut=anicut, ntop=ref.n)
+        for i in range(qry.n):
+            ids = set(ranked.reshape(qry.n, ref.n)[i, :npass[i]].tolist())
+            assert ids == set(np.flatnonzero(exact[i]).tolist())

@@ -1,6 +1,7 @@
 """The continuous-batching server (kssdgpu_server_*): every request's hits equal the
-nonzero counter cells kssdgpu_count_block gives for that query alone, whether the
-request ran alone or shared batches with concurrent arrivals."""
+nonzero counter cells the oracle gives for that query alone, whether the request ran
+alone or shared batches with concurrent arrivals; batches that overflow the hit
+capacity are split and re-run; admission follows the device-memory budget."""
 import random
 import threading
 import time
@@ -9,6 +10,7 @@ import numpy as np
 import pytest
 
 import kssdgpu
+import oracle
 
 pytestmark = pytest.mark.gpu
 
@@ -28,9 +30,11 @@ def _workload():
     return ref, queries
 
 
-def _expected(idx, q, flags):
+def _expected(rec, nref, q, flags):
+    """Nonzero cells of the oracle's counters for query q alone."""
     offs = np.array([0, len(q)], dtype=np.uint64)
-    out = idx.count_block(q, offs, flags)
+    out = oracle.count_block(rec, nref, q, offs, ignoreconflict=bool(flags & kssdgpu.IGNORECONFLICT),
+                             unique=bool(flags & kssdgpu.UNIQUE))
     ctx, obj = out[0][0], out[1][0]
     nz = np.nonzero(ctx[:, 0])[0]
     if flags & kssdgpu.UNIQUE:
@@ -56,7 +60,8 @@ def _as_rows(hits, flags):
 def test_results_identical_alone_and_in_the_mix(flags):
     ref, queries = _workload()
     idx = kssdgpu.Index.from_sketch(ref)
-    want = [_expected(idx, q, flags) for q in queries]
+    rec = oracle.build_index(ref.keys, ref.offs)
+    want = [_expected(rec, ref.n, q, flags) for q in queries]
     assert sum(len(w) for w in want) > 0
     srv = kssdgpu.Server(idx, max_batch_queries=16, max_batch_keys=1 << 22, flags=flags)
     try:
@@ -114,7 +119,66 @@ def test_oversized_query_is_rejected():
         small = min((q for q in queries if len(q)), key=len)
         if len(small) <= 1000:
             hits, _ = srv.result(srv.submit(small))
-            assert _as_rows(hits, 0) == _expected(idx, small, 0)
+            assert _as_rows(hits, 0) == _expected(oracle.build_index(ref.keys, ref.offs), ref.n, small, 0)
+        bad = np.array(big[:50][::-1])  # descending keys
+        with pytest.raises(kssdgpu.KssdGpuError) as e:
+            srv.submit(bad)
+        assert e.value.code == 3
     finally:
         srv.close()
+        idx.close()
+
+
+def test_hit_overflow_splits_the_batch():
+    """A batch whose nonzero cells exceed max_hits re-runs its requests one per batch:
+    each request that fits alone gets its full result; one that overflows alone fails
+    with KSSDGPU_ERR_CAPACITY, and the server keeps serving."""
+    ref, queries = _workload()
+    idx = kssdgpu.Index.from_sketch(ref)
+    rec = oracle.build_index(ref.keys, ref.offs)
+    want = [_expected(rec, ref.n, q, 0) for q in queries]
+    cap = max(len(w) for w in want if len(w) < 60) if any(len(w) < 60 for w in want) else 0
+    assert cap > 0
+    srv = kssdgpu.Server(idx, max_batch_queries=8, max_batch_keys=1 << 22, max_hits=cap, slots=1)
+    try:
+        tickets = [srv.submit(q) for q in queries]  # queued together: batches of up to 8
+        for q, w, t in zip(queries, want, tickets):
+            if len(w) <= cap:
+                hits, _ = srv.result(t, timeout_ms=60000)
+                assert _as_rows(hits, 0) == w
+            else:
+                with pytest.raises(kssdgpu.KssdGpuError) as e:
+                    srv.result(t, timeout_ms=60000)
+                assert e.value.code == 7
+        st = srv.stats()
+        assert st["splits"] > 0 and st["slots"] == 1
+        small = [i for i, w in enumerate(want) if 0 < len(w) <= cap][0]
+        hits, _ = srv.result(srv.submit(queries[small]))
+        assert _as_rows(hits, 0) == want[small]
+    finally:
+        srv.close()
+        idx.close()
+
+
+def test_admission_by_device_budget():
+    """The slot count follows the device-memory budget; a budget below one slot is refused."""
+    ref, queries = _workload()
+    idx = kssdgpu.Index.from_sketch(ref)
+    try:
+        one = kssdgpu.Server(idx, max_batch_queries=4, max_batch_keys=1 << 20, slots=8)
+        per_slot = one.stats()["reserved_bytes"] // one.stats()["slots"]
+        assert one.stats()["slots"] == 8
+        one.close()
+        srv = kssdgpu.Server(idx, max_batch_queries=4, max_batch_keys=1 << 20, slots=8, device_budget=3 * per_slot)
+        assert srv.stats()["slots"] == 3
+        rec = oracle.build_index(ref.keys, ref.offs)
+        ts = [srv.submit(q) for q in queries]
+        for q, t in zip(queries, ts):
+            hits, _ = srv.result(t, timeout_ms=60000)
+            assert _as_rows(hits, 0) == _expected(rec, ref.n, q, 0)
+        srv.close()
+        with pytest.raises(kssdgpu.KssdGpuError) as e:
+            kssdgpu.Server(idx, max_batch_queries=4, max_batch_keys=1 << 20, device_budget=per_slot - 1)
+        assert e.value.code == 7
+    finally:
         idx.close()

@@ -173,3 +173,15 @@ def test_reference_index_build_matches_oracle(tmp_path):
     assert ref_rec.tobytes() == rec.tobytes()
     ref_bits = np.fromfile(os.path.join(d, "sortedcomb_ctxgid64obj32.unique_bits"), dtype=np.uint8)
     np.testing.assert_array_equal(ref_bits, oracle.unique_bits(rec))
+
+
+def test_workload_generator_builds_agree():
+    """The generator built into oracle/libworkload.so (used by the timed reference arm)
+    yields the same sketches as the product's host library."""
+    import kssdgpu
+    kw = dict(n_samples=60, n_clusters=6, size_dist=kssdgpu.SIZE_LOGNORMAL, len_median=4e5, len_min=1e5,
+              len_max=1.2e6, sub_lo=0.001, sub_hi=0.2, seed=77, sample_seed=78)
+    a = kssdgpu.synth(**kw)
+    b = kssdgpu.synth(lib=kssdgpu.bind_synth(oracle.workload_lib()), **kw)
+    np.testing.assert_array_equal(a.offs, b.offs)
+    np.testing.assert_array_equal(a.keys, b.keys)

@@ -51,13 +51,14 @@ def _workload():
     return ref, qry, reads
 
 
-@pytest.mark.parametrize("case", ["block", "block_unique", "reads_ignoreconflict", "lower", "global_acc"])
+@pytest.mark.parametrize("case", ["block", "block_unique", "reads_ignoreconflict", "lower", "global_acc",
+                                  "smem_acc", "lower_offset"])
 def test_noalloc_matches_existing_entry_point_twice(case):
     import torch
     ref, qry, reads = _workload()
     idx = kssdgpu.Index.from_sketch(ref)
     dev = torch.device("cuda", 0)
-    flags, lower, q = 0, False, qry
+    flags, lower, q, off = 0, False, qry, 0
     if case == "block_unique":
         flags = kssdgpu.UNIQUE
     elif case == "reads_ignoreconflict":
@@ -66,23 +67,31 @@ def test_noalloc_matches_existing_entry_point_twice(case):
         lower, q = True, ref
     elif case == "global_acc":
         flags = kssdgpu.GLOBAL_ACC | kssdgpu.UNIQUE
+    elif case == "smem_acc":
+        flags = kssdgpu.SMEM_ACC | kssdgpu.UNIQUE
+    elif case == "lower_offset":
+        # a block of the reference's own samples past the first: gids below 50 + i count
+        lower, off = True, 50
+        q = kssdgpu.Sketch(keys=ref.keys[int(ref.offs[off]):int(ref.offs[off + 40])],
+                           offs=np.ascontiguousarray(ref.offs[off:off + 41]), names=[])
     nq, nref = q.n, ref.n
     d_keys = torch.from_numpy(q.keys.view(np.int64)).to(dev)
     d_offs = torch.from_numpy(q.offs.view(np.int64)).to(dev)
     nout = 4 if flags & kssdgpu.UNIQUE else 2
     want = [torch.zeros(nq * nref, dtype=torch.int64, device=dev) for _ in range(nout)]
-    idx.count_block_dev(d_keys, d_offs, nq, *want, flags=flags, lower=lower)
+    idx.count_block_dev(d_keys, d_offs, nq, *want, flags=flags, lower=lower, qry_gid_offset=off)
     idx.sync()
     for call in range(2):  # two calls in a row share the one scratch array
         got = [torch.full((nq * nref,), -1, dtype=torch.int64, device=dev) for _ in range(nout)]
-        _noalloc(idx, d_keys, d_offs, nq, got, flags=flags, lower=lower)
+        _noalloc(idx, d_keys, d_offs, nq, got, flags=flags, lower=lower, qgid_offset=off)
         for g, w in zip(got, want):
             assert torch.equal(g, w), f"call {call + 1} differs from kssdgpu_count_block_dev"
+    idx.sync()  # no error recorded on the device
     assert int((want[0] & 0xFFFFFFFF).sum()) > 0
     # and both equal the oracle
     rec, _ = idx.export()
     if lower:
-        o = oracle.count_lower(rec, nref, 0, q.keys, q.offs)
+        o = oracle.count_lower(rec, nref, off, q.keys, q.offs)
     else:
         o = oracle.count_block(rec, nref, q.keys, q.offs, unique=bool(flags & kssdgpu.UNIQUE),
                                ignoreconflict=bool(flags & kssdgpu.IGNORECONFLICT))
@@ -104,4 +113,55 @@ def test_noalloc_rejects_more_queries_than_its_scratch_holds():
                                          0, out.data_ptr(), out.data_ptr(), None, None, None)
     assert rc == ERR_CAPACITY
     assert b"maximum" in lib.kssdgpu_last_error()
+    idx.close()
+
+
+def test_noalloc_empty_block_and_unsorted_keys():
+    """nq = 0 launches nothing and leaves the outputs untouched; query keys out of order
+    are recorded on the device and reported by the next kssdgpu_sync."""
+    import torch
+    ref, qry, _ = _workload()
+    idx = kssdgpu.Index.from_sketch(ref)
+    dev = torch.device("cuda", 0)
+    d_keys = torch.from_numpy(qry.keys.view(np.int64)).to(dev)
+    d_offs = torch.from_numpy(qry.offs.view(np.int64)).to(dev)
+    out = [torch.full((qry.n * ref.n,), 7, dtype=torch.int64, device=dev) for _ in range(2)]
+    _noalloc(idx, d_keys, d_offs, 0, out)
+    assert all(bool((o == 7).all()) for o in out)
+    bad = d_keys.clone()
+    a, b = int(qry.offs[3]), int(qry.offs[4])
+    assert b - a > 2
+    bad[a:b] = torch.flip(bad[a:b], [0])
+    _noalloc(idx, bad, d_offs, qry.n, out)
+    with pytest.raises(kssdgpu.KssdGpuError) as e:
+        idx.sync()
+    assert e.value.code == 3  # KSSDGPU_ERR_UNSORTED
+    idx.sync()  # reported once, then cleared
+    idx.close()
+
+
+def test_noalloc_at_the_query_limit():
+    """KSSDGPU_NOALLOC_MAX_QUERIES queries of a few keys each (the chunk prefix fills the
+    scratch to its last word) give the counters of kssdgpu_count_block_dev."""
+    import torch
+    ref, qry, _ = _workload()
+    idx = kssdgpu.Index.from_sketch(ref)
+    dev = torch.device("cuda", 0)
+    rng = np.random.default_rng(5)
+    sizes = rng.integers(0, 4, size=MAX_QUERIES)
+    offs = np.concatenate([[0], np.cumsum(sizes)]).astype(np.uint64)
+    src = rng.integers(0, qry.n, size=MAX_QUERIES)
+    keys = np.concatenate([np.sort(rng.choice(qry.keys[int(qry.offs[q]):int(qry.offs[q + 1])], size=k, replace=False))
+                           for q, k in zip(src, sizes) if k]).astype(np.uint64)
+    d_keys = torch.from_numpy(keys.view(np.int64)).to(dev)
+    d_offs = torch.from_numpy(offs.view(np.int64)).to(dev)
+    cells = MAX_QUERIES * ref.n
+    want = [torch.zeros(cells, dtype=torch.int64, device=dev) for _ in range(2)]
+    idx.count_block_dev(d_keys, d_offs, MAX_QUERIES, *want)
+    idx.sync()
+    got = [torch.full((cells,), -1, dtype=torch.int64, device=dev) for _ in range(2)]
+    _noalloc(idx, d_keys, d_offs, MAX_QUERIES, got)
+    idx.sync()
+    assert all(torch.equal(g, w) for g, w in zip(got, want))
+    assert int((want[0] & 0xFFFFFFFF).sum()) > 0
     idx.close()
