@@ -129,6 +129,14 @@ def measured_peak_hbm():
         return 6650.0, "fallback"
 
 
+def measured_peak_bf16_tflops():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["bf16_tflops"])
+    except Exception:
+        return 1590.0
+
+
 def max_over_ranks(dist, x, device):
     """The largest of x over all ranks (x itself without a process group): every
     rank's timed region ends with the slowest one."""
@@ -436,6 +444,93 @@ def leg_reads(args, timer, dev, stream, idx, ref):
             "parity": {"read_sets": len(sample), "counts_match_reference": same}}
 
 
+def leg_dense(args, timer, dev, stream, peak_tc):
+    """One species: --dense-genomes genomes of one cluster at 0.1-2% substitutions (most
+    contexts shared by most genomes): the dense tensor-core self join vs the one-pass
+    scan on the same counters."""
+    import torch
+    import kssdgpu
+    n = args.dense_genomes
+    sk = kssdgpu.synth(n_samples=n, n_clusters=1, size_dist=kssdgpu.SIZE_LOGNORMAL, len_median=4e6, len_sigma=0.2,
+                       len_min=2e6, len_max=8e6, sub_lo=0.001, sub_hi=0.02, seed=WORKLOAD["seed"] + 21,
+                       sample_seed=WORKLOAD["seed"] + 21, threads=os.cpu_count() or 8)
+    idx = kssdgpu.Index.from_sketch(sk)
+    facts = idx.self_plan_info()
+    path, density = idx.self_choice()
+    cells = n * (n - 1) // 2
+    a_c = torch.zeros(cells, dtype=torch.int64, device=dev)
+    a_o = torch.zeros_like(a_c)
+    b_c, b_o = torch.zeros_like(a_c), torch.zeros_like(a_c)
+    ms_dense = timer(lambda: idx.self_lower_dev(a_c, a_o, flags=kssdgpu.SELF_DENSE, stream=stream), 3, 1)
+    alleles = idx.dense_alleles()
+    ms_scan = timer(lambda: idx.self_lower_dev(b_c, b_o, flags=kssdgpu.SELF_SCAN, stream=stream), 3, 1)
+    same = bool(torch.equal(a_c, b_c) and torch.equal(a_o, b_o))
+    kpad = (alleles + 127) // 128 * 128
+    ops = 2 * n * 4 * n * kpad  # int8 multiply-adds x 2 of the GEMM
+    idx.close()
+    return {"workload": f"one-species-{n}-genomes", "genomes": n, "entries": int(sk.offs[-1]),
+            "shared_postings": facts["postings"], "pairs": facts["pairs"], "alleles": alleles,
+            "density": density, "default_path": ["scan", "dense", "plan"][path],
+            "dense_step_ms": ms_dense, "scan_step_ms": ms_scan, "dense_vs_scan": ms_scan / ms_dense,
+            "genome_pairs_s": n * n / (ms_dense / 1e3),
+            "tensor": {"bound": "tensor", "int8_ops": ops, "achieved_tops": ops / ms_dense / 1e9,
+                       "peak_tops": peak_tc, "frac_of_step": ops / ms_dense / 1e9 / peak_tc,
+                       "what": "GEMM int8 ops over the whole dense step (allele build + GEMM + epilogue)"},
+            "parity": {"dense_eq_scan": same}}
+
+
+def leg_config1(args):
+    """64 genomes of 1 Mbp (8 clusters x 8 members, 0.5-5% substitutions, 0.1% indels) as
+    FASTA, sketched by the reference's own sketcher; bin/kssd3a and the reference CLI on
+    the dispatcher's small-n paths: bytes compared, wall times beside."""
+    import shutil
+    import tempfile
+    import fasta_synth
+    import kssdgpu
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    if not oracle.ref_available():
+        return {"skipped": "reference build absent"}
+    ours = os.path.join(ROOT, "kssd3a-public_b200", "bin", "kssd3a")
+    root = tempfile.mkdtemp(prefix="kssd_cfg1_")
+    try:
+        paths = fasta_synth.write_genomes(os.path.join(root, "fa"))
+        thr = str(os.cpu_count() or 8)
+        plain, indexed = os.path.join(root, "refs"), os.path.join(root, "refsi")
+        for d in (plain, indexed):
+            subprocess.run([oracle.REF_BIN, "sketch", "-p", thr, "-o", d, *paths], check=True, capture_output=True)
+        subprocess.run([oracle.REF_BIN, "sketch", "-i", indexed], check=True, capture_output=True)
+        cases = {"detail_hash": ["ani", "-p", thr, "-r", plain, "-q", plain],
+                 "detail_mem_eff": ["ani", "-p", thr, "-r", indexed, "-q", indexed],
+                 "matrix_direct": ["ani", "-p", thr, "-r", plain, "-q", plain, "--format", "matrix"],
+                 "self_ani_matrix": ["ani", "-p", thr, "-q", indexed, "--format", "matrix", "--values", "ani"],
+                 "matrix_cmd": ["matrix", "-p", thr, "-q", plain]}
+        out = {}
+        env = {k: v for k, v in os.environ.items() if not k.startswith("KSSD3A_")}
+        for name, argv in cases.items():
+            t0 = time.perf_counter()
+            a = subprocess.run([ours, *argv], capture_output=True, env=env)
+            t1 = time.perf_counter()
+            b = subprocess.run([oracle.REF_BIN, *argv], capture_output=True, env=env)
+            t2 = time.perf_counter()
+            out[name] = {"bytes_equal": a.returncode == 0 and a.stdout == b.stdout, "lines": len(b.stdout.splitlines()),
+                         "ours_s": t1 - t0, "reference_s": t2 - t1}
+        sk = kssdgpu.read_sketch_dir(plain)
+        syn = kssdgpu.synth(n_samples=64, n_clusters=8, size_dist=kssdgpu.SIZE_FIXED, len_median=1e6, len_min=1e6,
+                            len_max=1e6, sub_lo=0.005, sub_hi=0.05, indel_rate=0.001, seed=5, sample_seed=5)
+        hist = {}
+        for name, x in (("reference_sketcher_on_fasta", sk), ("sketch_space_generator", syn)):
+            _, k = np.unique(x.keys >> np.uint64(20), return_counts=True)
+            h = np.bincount(np.minimum(k, 9), minlength=10)[1:]
+            hist[name] = {"entries": int(len(x.keys)), "contexts": int(len(k)),
+                          "postings_per_context": float(len(x.keys) / len(k)),
+                          "fraction_of_contexts_with_k_postings_1_to_9plus": (h / len(k)).round(4).tolist()}
+        return {"workload": "64 x 1 Mbp FASTA genomes, 8 clusters x 8, sketched by the reference sketcher",
+                "entries": int(len(sk.keys)), "cases": out, "postings_per_context": hist}
+    finally:
+        shutil.rmtree(root, ignore_errors=True)
+
+
 def _pct(xs, p):
     xs = sorted(xs)
     return float(xs[min(len(xs) - 1, int(p * (len(xs) - 1) + 0.5))]) if xs else None
@@ -544,6 +639,7 @@ def run_ours(args, rank, world, local_rank):
     stream = torch.cuda.current_stream()
     timer = Timer(stream, dev)
     peak, peak_kind = measured_peak_hbm()
+    peak_tc = 2 * measured_peak_bf16_tflops()  # int8 dense rate = 2 x bf16 on these tensor cores
 
     sk = make_workload(args.genomes)
     n = sk.n
@@ -737,6 +833,8 @@ def run_ours(args, rank, world, local_rank):
                               "default run stays within minutes; --workload serve runs the 50,000-genome index)",
                               "pool": pool, "server": srvf, "rates": res}
         ns_idx.close()
+        extra["dense_one_species"] = leg_dense(args, timer, dev, stream, peak_tc)
+        extra["config1_fasta"] = leg_config1(args)
 
     if rank == 0:
         line = {
@@ -846,6 +944,7 @@ def main():
     ap.add_argument("--rect-queries", type=int, default=10000)
     ap.add_argument("--reads-samples", type=int, default=40)
     ap.add_argument("--parity-queries", type=int, default=48)
+    ap.add_argument("--dense-genomes", type=int, default=1024, help="genomes of the one-species dense leg")
     ap.add_argument("--serve-refs", type=int, default=50000, help="serve workload: resident index size (genomes)")
     ap.add_argument("--serve-rates", default="1000,5000", help="arrival rates (req/s) of the serving sweep")
     ap.add_argument("--serve-seconds", type=float, default=1.5, help="arrival window per rate")

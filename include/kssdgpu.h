@@ -49,6 +49,9 @@ extern "C" {
                                        row of the index's references does not fit) */
 #define KSSDGPU_SELF_PLAN 0x40u     /* self lower triangle: join over the index's cached set-major plan
                                        (built and kept on first use) instead of the one-pass scan */
+#define KSSDGPU_SELF_SCAN 0x80u     /* self lower triangle: the one-pass scan join, whatever the density */
+#define KSSDGPU_SELF_DENSE 0x100u   /* self lower triangle: the dense tensor-core join, whatever the
+                                       density (conflict-free indexes only) */
 
 /* Counter cells, identical in layout to the reference's ctx_mut2_t / obj_section_t. */
 typedef struct kssdgpu_ctx_mut2 {
@@ -230,9 +233,16 @@ int kssdgpu_self_votes(kssdgpu_index_t *idx, const uint64_t *keys, const uint64_
                        uint32_t sample_step, uint32_t *votes, uint32_t *first);
 /* Device form of kssdgpu_self_lower (outputs in HBM, stream-ordered).
  *
- * Default: one pass over the whole index per call, nothing cached -- the dense lower
- * triangle is zero-filled (unless KSSDGPU_NO_ZERO) and a persistent scan reads every
- * context group's bounds, and joins each group of >= 2 postings as it finds it.
+ * Default: nothing cached between calls; the join follows the index's density
+ * (kssdgpu_self_choice).  The one-pass scan (KSSDGPU_SELF_SCAN) zero-fills the packed
+ * lower triangle (unless KSSDGPU_NO_ZERO), reads every context group's bounds and
+ * joins each group of >= 2 postings as it finds it.  The dense join
+ * (KSSDGPU_SELF_DENSE) lists the shared contexts, sorts their postings into alleles
+ * (distinct objects per context), builds two int8 operand matrices and computes all
+ * four counters of every pair with one exact int8 GEMM on the tensor cores (int32
+ * accumulation), then writes every cell of the triangle; it needs a conflict-free
+ * index (KSSDGPU_ERR_ARG otherwise) and synchronizes the stream once (for the
+ * allele count).
  *
  * With KSSDGPU_SELF_PLAN: the first call builds a set-major plan of the index's
  * shared contexts (kept on the handle; later calls only join over it).  Where the
@@ -249,6 +259,24 @@ int kssdgpu_self_lower_dev(kssdgpu_index_t *idx, unsigned flags, kssdgpu_ctx_mut
  * (k(k-1)/2 per group of k).  These size the join's algorithmic bytes.
  */
 int kssdgpu_self_plan_info(kssdgpu_index_t *idx, uint64_t *groups, uint64_t *postings, uint64_t *pairs);
+
+/*
+ * Which join kssdgpu_self_lower(_dev) takes for these flags (KSSDGPU_PATH_*), and the
+ * index's shared-context density: pairs of postings of shared contexts / (nref^2 x
+ * alleles of shared contexts), the ratio of the scan's counter updates to the dense
+ * GEMM's multiply-adds up to a constant (the allele count -- distinct objects per
+ * shared context -- is estimated at index build from up to 65,536 sampled context
+ * groups).  Without a path flag the dense tensor-core join is taken when the index is
+ * conflict-free, the density is at least 1/2048 and its operands fit in half of the
+ * free device memory; else the one-pass scan.  No reference counterpart.
+ */
+#define KSSDGPU_PATH_SCAN 0
+#define KSSDGPU_PATH_DENSE 1
+#define KSSDGPU_PATH_PLAN 2
+int kssdgpu_self_choice(kssdgpu_index_t *idx, unsigned flags, int *path, double *density);
+/* Allele rows (distinct objects of the shared contexts: the GEMM's K before padding to
+ * 128) of the last dense self join on this index; 0 before one ran. */
+int kssdgpu_self_dense_alleles(kssdgpu_index_t *idx, uint64_t *alleles);
 
 /*
  * Autotune the KSSDGPU_SELF_PLAN join's plan (once per index; builds the plan first if needed):

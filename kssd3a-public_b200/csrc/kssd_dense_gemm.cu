@@ -1,0 +1,76 @@
+// Exact int8 x int8 -> int32 GEMM on the sm_100a tensor cores (tcgen05.mma with the
+// accumulator in TMEM, operands staged into shared memory by TMA), through CUTLASS's
+// sm100 collective mainloop and epilogue.  Used by the dense self join of
+// libkssdgpu: D[M][N] = A[M][K] * B[N][K]^T with both operands K-major (row-major A,
+// column-major B), int32 D row-major.  One CTA per 128 x 128 tile, no thread-block
+// cluster (no multicast loads).
+#include "cutlass/cutlass.h"
+#include "cute/tensor.hpp"
+#include "cutlass/epilogue/collective/collective_builder.hpp"
+#include "cutlass/gemm/collective/collective_builder.hpp"
+#include "cutlass/gemm/device/gemm_universal_adapter.h"
+#include "cutlass/gemm/dispatch_policy.hpp"
+#include "cutlass/gemm/kernel/gemm_universal.hpp"
+#include "cutlass/util/packed_stride.hpp"
+
+#include <cstdint>
+
+namespace {
+
+using namespace cute;
+
+using TileShape = Shape<_128, _128, _128>;
+using ClusterShape = Shape<_1, _1, _1>;
+using Epilogue = typename cutlass::epilogue::collective::CollectiveBuilder<
+    cutlass::arch::Sm100, cutlass::arch::OpClassTensorOp, TileShape, ClusterShape,
+    cutlass::epilogue::collective::EpilogueTileAuto, int32_t, int32_t, int32_t, cutlass::layout::RowMajor, 4,
+    int32_t, cutlass::layout::RowMajor, 4, cutlass::epilogue::collective::EpilogueScheduleAuto>::CollectiveOp;
+using Mainloop = typename cutlass::gemm::collective::CollectiveBuilder<
+    cutlass::arch::Sm100, cutlass::arch::OpClassTensorOp, int8_t, cutlass::layout::RowMajor, 16, int8_t,
+    cutlass::layout::ColumnMajor, 16, int32_t, TileShape, ClusterShape,
+    cutlass::gemm::collective::StageCountAutoCarveout<static_cast<int>(sizeof(typename Epilogue::SharedStorage))>,
+    cutlass::gemm::KernelTmaWarpSpecialized1SmSm100>::CollectiveOp;
+using Kernel = cutlass::gemm::kernel::GemmUniversal<Shape<int, int, int, int>, Mainloop, Epilogue, void>;
+using Gemm = cutlass::gemm::device::GemmUniversalAdapter<Kernel>;
+
+typename Gemm::Arguments make_args(const int8_t *A, const int8_t *B, int32_t *D, int M, int N, int K)
+{
+    using SA = typename Gemm::GemmKernel::StrideA;
+    using SB = typename Gemm::GemmKernel::StrideB;
+    using SC = typename Gemm::GemmKernel::StrideC;
+    using SD = typename Gemm::GemmKernel::StrideD;
+    const SA sa = cutlass::make_cute_packed_stride(SA{}, cute::make_shape(M, K, 1));
+    const SB sb = cutlass::make_cute_packed_stride(SB{}, cute::make_shape(N, K, 1));
+    const SC sc = cutlass::make_cute_packed_stride(SC{}, cute::make_shape(M, N, 1));
+    const SD sd = cutlass::make_cute_packed_stride(SD{}, cute::make_shape(M, N, 1));
+    return typename Gemm::Arguments{cutlass::gemm::GemmUniversalMode::kGemm, {M, N, K, 1}, {A, sa, B, sb},
+                                    {{1, 0}, D, sc, D, sd}};
+}
+
+}  // namespace
+
+namespace kssd {
+
+// Bytes of device workspace the GEMM of this shape needs (0 or more).
+size_t dense_gemm_s8_workspace(int M, int N, int K)
+{
+    return Gemm::get_workspace_size(make_args(nullptr, nullptr, nullptr, M, N, K));
+}
+
+// D = A * B^T; K a multiple of 16, rows 16-byte aligned.  Returns 0, or 1 when the
+// shape is not supported, 2 when the launch failed.
+int dense_gemm_s8(const int8_t *A, const int8_t *B, int32_t *D, int M, int N, int K, void *workspace,
+                  cudaStream_t st)
+{
+    const auto args = make_args(A, B, D, M, N, K);
+    Gemm gemm;
+    if (gemm.can_implement(args) != cutlass::Status::kSuccess)
+        return 1;
+    if (gemm.initialize(args, workspace, st) != cutlass::Status::kSuccess)
+        return 2;
+    if (gemm.run(st) != cutlass::Status::kSuccess)
+        return 2;
+    return 0;
+}
+
+}  // namespace kssd

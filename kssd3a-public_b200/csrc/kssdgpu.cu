@@ -26,6 +26,11 @@
 
 using namespace kssd;
 
+namespace kssd {
+size_t dense_gemm_s8_workspace(int M, int N, int K);
+int dense_gemm_s8(const int8_t *A, const int8_t *B, int32_t *D, int M, int N, int K, void *workspace, cudaStream_t st);
+}  // namespace kssd
+
 namespace {
 
 thread_local std::string g_last_error;
@@ -1376,27 +1381,191 @@ __global__ void __launch_bounds__(kScanThreads) k_self_scan(const uint32_t *__re
     }
 }
 
-// Facts of the self join: groups of >= 2 postings, postings in them, their pairs.
-__global__ void k_self_stats(const uint32_t *__restrict__ gbeg, uint64_t u, unsigned long long *__restrict__ tot)
+// Facts of the self join: groups of >= 2 postings, postings in them, their pairs,
+// and whether any gid holds several objects of one context (a conflict).
+__global__ void k_self_stats(const uint32_t *__restrict__ gbeg, uint64_t u, const uint64_t *__restrict__ post,
+                             unsigned long long *__restrict__ tot)
 {
-    unsigned long long g2 = 0, p2 = 0, pairs = 0;
+    unsigned long long g2 = 0, p2 = 0, pairs = 0, conf = 0;
     for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < u; g += (uint64_t)gridDim.x * blockDim.x) {
-        const unsigned long long k = gbeg[g + 1] - gbeg[g];
+        const uint32_t b = gbeg[g];
+        const unsigned long long k = gbeg[g + 1] - b;
         if (k >= 2) {
             ++g2;
             p2 += k;
             pairs += k * (k - 1) / 2;
+            uint32_t prev = (uint32_t)(post[b] >> 32);
+            for (uint32_t i = 1; i < k && !conf; ++i) {
+                const uint32_t gid = (uint32_t)(post[b + i] >> 32);
+                conf |= gid == prev;
+                prev = gid;
+            }
         }
     }
     for (int o = 16; o; o >>= 1) {
         g2 += __shfl_down_sync(0xffffffffu, g2, o);
         p2 += __shfl_down_sync(0xffffffffu, p2, o);
         pairs += __shfl_down_sync(0xffffffffu, pairs, o);
+        conf |= __shfl_down_sync(0xffffffffu, conf, o);
     }
-    if ((threadIdx.x & 31) == 0 && g2) {
+    if ((threadIdx.x & 31) == 0 && (g2 || conf)) {
         atomicAdd(tot + 0, g2);
         atomicAdd(tot + 1, p2);
         atomicAdd(tot + 2, pairs);
+        if (conf)
+            atomicOr(tot + 3, 1ull);
+    }
+}
+
+// ------------------------------------------------------------------ dense self join (tensor cores)
+//
+// For a conflict-free index whose shared contexts are dense (many genomes of one
+// species: contexts held by most genomes), the four counters of every pair are one
+// exact int8 GEMM.  Rows are the alleles of the shared contexts -- the distinct
+// objects u seen at a context c among its postings.  With A'[q][(c,u)] = 1 when genome
+// q holds object u at c, and for every genome r holding c with object o_r, d = min(
+// dna_popcount(u ^ o_r), NUM_CODENS + 1):
+//     F[r][(c,u)] = 1,  F[n+r][(c,u)] = d >= 1,  F[2n+r][(c,u)] = d >= 2,  F[3n+r][(c,u)] = d
+// D = A' F^T gives, for q != r over their shared contexts, D[q][r] = num_ctx,
+// D[q][n+r] = diff_obj, D[q][2n+r] = num_mut2_ctx and D[q][3n+r] = diff_obj_section:
+// the counters of count_lower (src/command_ani.h:694-716; one object per gid run, so
+// the minimum over the run cross product is that one difference).
+
+// Alleles of a sample of the shared groups (groups g = i * stride, one warp each):
+// tot[0] += distinct objects, tot[1] += postings.  Scales the shared postings to the
+// dense join's allele count (its GEMM's K) for the density rule.
+__global__ void k_allele_sample(const uint32_t *__restrict__ gbeg, uint64_t u, uint64_t stride, uint32_t samples,
+                                const uint64_t *__restrict__ post, unsigned long long *__restrict__ tot)
+{
+    const uint32_t lane = threadIdx.x & 31;
+    for (uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < samples; i += (gridDim.x * blockDim.x) >> 5) {
+        const uint64_t g = (uint64_t)i * stride;
+        if (g >= u)
+            continue;
+        const uint32_t b = gbeg[g], k = gbeg[g + 1] - b;
+        if (k < 2)
+            continue;
+        uint32_t firsts = 0;
+        for (uint32_t j = lane; j < k; j += 32) {
+            const uint32_t o = (uint32_t)post[b + j];
+            bool first = true;
+            for (uint32_t t = 0; t < j && first; ++t)
+                first = (uint32_t)post[b + t] != o;
+            firsts += first;
+        }
+        for (int o = 16; o; o >>= 1)
+            firsts += __shfl_down_sync(0xffffffffu, firsts, o);
+        if (lane == 0) {
+            atomicAdd(tot + 0, (unsigned long long)firsts);
+            atomicAdd(tot + 1, (unsigned long long)k);
+        }
+    }
+}
+
+// Shared groups (>= 2 postings) as (begin | k << 32), appended in any order.
+__global__ void k_dense_list(const uint32_t *__restrict__ gbeg, uint64_t u, unsigned long long *__restrict__ list,
+                             unsigned int *__restrict__ n_list)
+{
+    const unsigned lane = threadIdx.x & 31;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t g0 = blockIdx.x * (uint64_t)blockDim.x; g0 < u; g0 += stride) {
+        const uint64_t g = g0 + threadIdx.x;
+        uint32_t b = 0, k = 0;
+        if (g < u) {
+            b = gbeg[g];
+            k = gbeg[g + 1] - b;
+        }
+        const bool want = k >= 2;
+        const uint32_t at = warp_slot(n_list, want, lane);
+        if (want)
+            list[at] = (unsigned long long)b | ((unsigned long long)k << 32);
+    }
+}
+
+// Sort records of the shared postings: key (list rank << 32 | object), value gid; one
+// warp per listed group.
+__global__ void k_dense_keys(const unsigned long long *__restrict__ list, uint32_t n_list,
+                             const uint32_t *__restrict__ poff, const uint64_t *__restrict__ post,
+                             unsigned long long *__restrict__ keys, uint32_t *__restrict__ vals)
+{
+    const uint32_t lane = threadIdx.x & 31;
+    for (uint32_t s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < n_list;
+         s += (gridDim.x * blockDim.x) >> 5) {
+        const unsigned long long item = list[s];
+        const uint32_t b = (uint32_t)item, k = (uint32_t)(item >> 32), o = poff[s];
+        for (uint32_t i = lane; i < k; i += 32) {
+            const uint64_t p = post[b + i];
+            keys[o + i] = ((unsigned long long)s << 32) | (uint32_t)p;
+            vals[o + i] = (uint32_t)(p >> 32);
+        }
+    }
+}
+
+__global__ void k_unpack_k(const unsigned long long *__restrict__ list, uint32_t n, uint32_t *__restrict__ k)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        k[i] = (uint32_t)(list[i] >> 32);
+}
+
+__global__ void k_dense_heads(const unsigned long long *__restrict__ keys, uint32_t n, uint32_t *__restrict__ heads)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        heads[i] = i == 0 || keys[i] != keys[i - 1];
+}
+
+// A'[gid][allele] = 1 for every sorted posting; the first posting of every allele.
+__global__ void k_dense_fill_a(const uint32_t *__restrict__ vals, const uint32_t *__restrict__ heads,
+                               const uint32_t *__restrict__ allele_incl, uint32_t n, size_t kpad,
+                               int8_t *__restrict__ A, uint32_t *__restrict__ first)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t a = allele_incl[i] - 1;
+        A[(size_t)vals[i] * kpad + a] = 1;
+        if (heads[i])
+            first[a] = i;
+    }
+}
+
+// The four feature rows of every allele (one warp per allele, lanes over the postings
+// of its context).
+__global__ void k_dense_fill_f(const unsigned long long *__restrict__ keys, const uint32_t *__restrict__ first,
+                               uint32_t n_alleles, const unsigned long long *__restrict__ list,
+                               const uint64_t *__restrict__ post, int nref, size_t kpad, int8_t *__restrict__ F)
+{
+    const uint32_t lane = threadIdx.x & 31;
+    for (uint32_t a = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; a < n_alleles;
+         a += (gridDim.x * blockDim.x) >> 5) {
+        const unsigned long long key = keys[first[a]];
+        const uint32_t s = (uint32_t)(key >> 32), obj = (uint32_t)key;
+        const unsigned long long item = list[s];
+        const uint32_t b = (uint32_t)item, k = (uint32_t)(item >> 32);
+        for (uint32_t i = lane; i < k; i += 32) {
+            const uint64_t p = post[b + i];
+            const size_t r = (size_t)(p >> 32);
+            const int d = min(kMinInit, dna_pop(obj ^ (uint32_t)p));
+            F[r * kpad + a] = 1;
+            F[(nref + r) * kpad + a] = (int8_t)(d >= 1);
+            F[(2 * (size_t)nref + r) * kpad + a] = (int8_t)(d >= 2);
+            F[(3 * (size_t)nref + r) * kpad + a] = (int8_t)d;
+        }
+    }
+}
+
+// Packed lower triangle from D (n x 4n): every cell written (zeros included).
+__global__ void k_dense_epilogue(const int32_t *__restrict__ D, int nref, size_t cells,
+                                 unsigned long long *__restrict__ oc, unsigned long long *__restrict__ oo)
+{
+    for (size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x; c < cells; c += (size_t)gridDim.x * blockDim.x) {
+        // row q: the largest q with q (q - 1) / 2 <= c
+        uint32_t q = (uint32_t)((1.0 + sqrt(1.0 + 8.0 * (double)c)) * 0.5);
+        while ((size_t)q * (q - 1) / 2 > c)
+            --q;
+        while ((size_t)(q + 1) * q / 2 <= c)
+            ++q;
+        const uint32_t r = (uint32_t)(c - (size_t)q * (q - 1) / 2);
+        const int32_t *row = D + (size_t)q * 4 * nref;
+        oc[c] = (unsigned long long)(uint32_t)row[r] | ((unsigned long long)(uint32_t)row[2 * nref + r] << 32);
+        oo[c] = (unsigned long long)(uint32_t)row[nref + r] | ((unsigned long long)(uint32_t)row[3 * nref + r] << 32);
     }
 }
 
@@ -1556,6 +1725,18 @@ struct kssdgpu_index {
     unsigned long long j_postings = 0, j_pairs = 0;
     bool j_ready = false;
     int scan_grid = 0;                      // CTAs of the one-pass scan join (resident per SM x SMs)
+    // facts of the index, from one pass at build: shared groups (>= 2 postings), their
+    // postings and pairs, whether any gid run holds several objects (a conflict)
+    unsigned long long f_groups = 0, f_postings = 0, f_pairs = 0;
+    unsigned long long f_alleles = 0;       // distinct objects of the shared contexts (sampled estimate)
+    bool f_conflict = false;
+    // dense self join scratch
+    DevBuf<unsigned long long> d_list, d_keys, d_keys2;
+    DevBuf<uint32_t> d_poff, d_vals, d_vals2, d_heads, d_allele, d_first;
+    DevBuf<int8_t> d_a, d_f;
+    DevBuf<int32_t> d_d;
+    DevBuf<unsigned char> d_tmp, d_ws;
+    unsigned long long d_alleles = 0;       // alleles of the last dense join (its GEMM's K before padding)
 };
 
 namespace {
@@ -1596,6 +1777,49 @@ int finish_build(kssdgpu_index *ix, uint32_t *head, unsigned long long *ctx_of, 
     cudaFree(gidx);
     int herr = 0;
     CUDA_TRY(cudaMemcpy(&herr, ix->err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (!herr && ix->u) {
+        // facts of the shared contexts (sizes of the self joins; the dense path's conditions)
+        unsigned long long *d = nullptr, h[4] = {0, 0, 0, 0};
+        CUDA_TRY(cudaMalloc(&d, sizeof h));
+        cudaError_t e = cudaMemsetAsync(d, 0, sizeof h, st);
+        if (e == cudaSuccess) {
+            k_self_stats<<<grid_for(ix->u), 256, 0, st>>>(ix->gbeg, ix->u, ix->post, d);
+            count_launch();
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess) e = cudaMemcpyAsync(h, d, sizeof h, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        cudaFree(d);
+        if (e != cudaSuccess)
+            return fail(KSSDGPU_ERR_CUDA, std::string("index facts: ") + cudaGetErrorString(e));
+        ix->f_groups = h[0];
+        ix->f_postings = h[1];
+        ix->f_pairs = h[2];
+        ix->f_conflict = h[3] != 0;
+        // the dense join's allele count, estimated from up to 65,536 sampled groups
+        ix->f_alleles = ix->f_postings;
+        if (ix->f_groups) {
+            const uint32_t samples = (uint32_t)std::min<uint64_t>(ix->u, 65536);
+            const uint64_t stride = ix->u / samples;
+            unsigned long long *d2 = nullptr, h2[2] = {0, 0};
+            CUDA_TRY(cudaMalloc(&d2, sizeof h2));
+            e = cudaMemsetAsync(d2, 0, sizeof h2, st);
+            if (e == cudaSuccess) {
+                k_allele_sample<<<(samples * 32 + 255) / 256, 256, 0, st>>>(ix->gbeg, ix->u, stride, samples, ix->post,
+                                                                           d2);
+                count_launch();
+                e = cudaGetLastError();
+            }
+            if (e == cudaSuccess) e = cudaMemcpyAsync(h2, d2, sizeof h2, cudaMemcpyDeviceToHost, st);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+            cudaFree(d2);
+            if (e != cudaSuccess)
+                return fail(KSSDGPU_ERR_CUDA, std::string("index facts: ") + cudaGetErrorString(e));
+            if (h2[1])
+                ix->f_alleles = std::max<unsigned long long>(
+                    1, (unsigned long long)((double)ix->f_postings * (double)h2[0] / (double)h2[1]));
+        }
+    }
     if (herr == kDevUnsorted)
         return fail(KSSDGPU_ERR_UNSORTED, "index records are not sorted by (ctxgid, obj)");
     if (herr == kDevGid)
@@ -2704,8 +2928,147 @@ int self_scan_impl(kssdgpu_index *ix, unsigned flags, unsigned long long *oc, un
     return KSSDGPU_OK;
 }
 
+// Device bytes of a dense self join with K allele rows (A', F, D).
+uint64_t dense_bytes(const kssdgpu_index *ix, uint64_t kpad)
+{
+    return 5ull * (uint64_t)ix->nref * kpad + 16ull * (uint64_t)ix->nref * (uint64_t)ix->nref;
+}
+
+uint64_t round_up(uint64_t x, uint64_t m) { return (x + m - 1) / m * m; }
+
+// Dense self join (see k_dense_list): list the shared groups, sort their postings by
+// (group, object) to find the alleles, fill A' and F, one tensor-core GEMM, and the
+// packed lower triangle (every cell written, so no zero fill).  Conflict-free indexes
+// only; the GEMM's allele count bounds its memory (checked against free memory).
+int self_dense_impl(kssdgpu_index *ix, unsigned long long *oc, unsigned long long *oo, cudaStream_t st)
+{
+    const int n = ix->nref;
+    const size_t cells = (size_t)n * (n - 1) / 2;
+    if (ix->f_conflict)
+        return fail(KSSDGPU_ERR_ARG, "the dense self join needs a conflict-free index (a gid holds several objects "
+                                     "of one context)");
+    if (!cells)
+        return KSSDGPU_OK;
+    const uint32_t S = (uint32_t)ix->f_groups, P = (uint32_t)ix->f_postings;
+    if (ix->f_groups >= (1ull << 32) || ix->f_postings >= (1ull << 32))
+        return fail(KSSDGPU_ERR_CAPACITY, "dense self join: too many shared postings");
+    size_t free_b = 0, total_b = 0;
+    CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
+    if (!S) {
+        CUDA_TRY(cudaMemsetAsync(oc, 0, cells * 8, st));
+        CUDA_TRY(cudaMemsetAsync(oo, 0, cells * 8, st));
+        return KSSDGPU_OK;
+    }
+    CUDA_TRY(ix->d_list.ensure(S));
+    CUDA_TRY(ix->d_poff.ensure((size_t)S + 1));
+    CUDA_TRY(ix->d_keys.ensure(P));
+    CUDA_TRY(ix->d_keys2.ensure(P));
+    CUDA_TRY(ix->d_vals.ensure(P));
+    CUDA_TRY(ix->d_vals2.ensure(P));
+    CUDA_TRY(ix->d_heads.ensure(P));
+    CUDA_TRY(ix->d_allele.ensure(P));
+    CUDA_TRY(ix->d_first.ensure(P));
+    unsigned int *d_count = reinterpret_cast<unsigned int *>(ix->d_poff.p + S);  // the list's fill counter
+    int bits = 32;
+    while (bits < 64 && (1ull << (bits - 32)) < (unsigned long long)S)
+        ++bits;
+    size_t tb1 = 0, tb2 = 0, tb3 = 0;
+    CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, tb1, ix->d_heads.p, ix->d_poff.p, S, st));
+    CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, tb2, ix->d_keys.p, ix->d_keys2.p, ix->d_vals.p, ix->d_vals2.p, P, 0,
+                                             bits, st));
+    CUDA_TRY(cub::DeviceScan::InclusiveSum(nullptr, tb3, ix->d_heads.p, ix->d_allele.p, P, st));
+    CUDA_TRY(ix->d_tmp.ensure(std::max(tb1, std::max(tb2, tb3))));
+    // 1. the shared groups and their posting offsets
+    CUDA_TRY(cudaMemsetAsync(d_count, 0, sizeof(unsigned int), st));
+    k_dense_list<<<grid_for(ix->u), 256, 0, st>>>(ix->gbeg, ix->u, ix->d_list.p, d_count);
+    k_unpack_k<<<grid_for(S), 256, 0, st>>>(ix->d_list.p, S, ix->d_heads.p);
+    count_launch(2);
+    size_t tb = ix->d_tmp.cap;
+    CUDA_TRY(cub::DeviceScan::ExclusiveSum(ix->d_tmp.p, tb, ix->d_heads.p, ix->d_poff.p, S, st));
+    count_launch();
+    // 2. alleles: postings sorted by (group, object); runs of equal keys
+    k_dense_keys<<<std::min<uint64_t>(((uint64_t)S * 32 + 255) / 256, (uint64_t)ix->sms * 64), 256, 0, st>>>(
+        ix->d_list.p, S, ix->d_poff.p, ix->post, ix->d_keys.p, ix->d_vals.p);
+    count_launch();
+    tb = ix->d_tmp.cap;
+    CUDA_TRY(cub::DeviceRadixSort::SortPairs(ix->d_tmp.p, tb, ix->d_keys.p, ix->d_keys2.p, ix->d_vals.p, ix->d_vals2.p,
+                                             P, 0, bits, st));
+    count_launch(4);
+    k_dense_heads<<<grid_for(P), 256, 0, st>>>(ix->d_keys2.p, P, ix->d_heads.p);
+    count_launch();
+    tb = ix->d_tmp.cap;
+    CUDA_TRY(cub::DeviceScan::InclusiveSum(ix->d_tmp.p, tb, ix->d_heads.p, ix->d_allele.p, P, st));
+    count_launch();
+    uint32_t alleles = 0;
+    CUDA_TRY(cudaMemcpyAsync(&alleles, ix->d_allele.p + P - 1, 4, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    ix->d_alleles = alleles;
+    const uint64_t kpad = round_up(std::max<uint32_t>(alleles, 1), 128);
+    if (dense_bytes(ix, kpad) > free_b / 2)
+        return fail(KSSDGPU_ERR_NOMEM, "dense self join: operands of " + std::to_string(dense_bytes(ix, kpad)) +
+                                           " bytes exceed half of the free device memory");
+    // 3. operands
+    CUDA_TRY(ix->d_a.ensure((size_t)n * kpad));
+    CUDA_TRY(ix->d_f.ensure((size_t)4 * n * kpad));
+    CUDA_TRY(ix->d_d.ensure((size_t)4 * n * n));
+    CUDA_TRY(cudaMemsetAsync(ix->d_a.p, 0, (size_t)n * kpad, st));
+    CUDA_TRY(cudaMemsetAsync(ix->d_f.p, 0, (size_t)4 * n * kpad, st));
+    k_dense_fill_a<<<grid_for(P), 256, 0, st>>>(ix->d_vals2.p, ix->d_heads.p, ix->d_allele.p, P, kpad, ix->d_a.p,
+                                                ix->d_first.p);
+    k_dense_fill_f<<<std::min<uint64_t>(((uint64_t)alleles * 32 + 255) / 256, (uint64_t)ix->sms * 64), 256, 0, st>>>(
+        ix->d_keys2.p, ix->d_first.p, alleles, ix->d_list.p, ix->post, n, kpad, ix->d_f.p);
+    count_launch(2);
+    CUDA_TRY(cudaGetLastError());
+    // 4. D = A' F^T on the tensor cores
+    const size_t ws = kssd::dense_gemm_s8_workspace(n, 4 * n, (int)kpad);
+    CUDA_TRY(ix->d_ws.ensure(ws));
+    if (kpad > 0x7FFFFFFFull)
+        return fail(KSSDGPU_ERR_CAPACITY, "dense self join: allele count beyond the GEMM's 32-bit extent");
+    const int grc = kssd::dense_gemm_s8(ix->d_a.p, ix->d_f.p, ix->d_d.p, n, 4 * n, (int)kpad, ix->d_ws.p, st);
+    count_launch();
+    if (grc)
+        return fail(KSSDGPU_ERR_CUDA, grc == 1 ? "dense self join: GEMM shape not supported"
+                                               : "dense self join: GEMM launch failed");
+    CUDA_TRY(cudaGetLastError());
+    // 5. the packed lower triangle
+    k_dense_epilogue<<<grid_for(cells), 256, 0, st>>>(ix->d_d.p, n, cells, oc, oo);
+    count_launch();
+    CUDA_TRY(cudaGetLastError());
+    return KSSDGPU_OK;
+}
+
+// The density rule of the self join: the dense path does 4 n^2 K multiply-adds (K
+// alleles of the shared contexts), the scan one counter update per pair of postings of
+// a shared context.  density = pairs / (n^2 K); the dense join is taken when it is
+// above kDenseRatio, on a conflict-free index whose operands fit in half of the free
+// device memory.
+constexpr double kDenseRatio = 1.0 / 2048.0;
+
+double self_density(const kssdgpu_index *ix)
+{
+    const double n = (double)ix->nref, k = (double)std::max<unsigned long long>(ix->f_alleles, 1);
+    return (double)ix->f_pairs / (n * n * k);
+}
+
+bool dense_chosen(const kssdgpu_index *ix)
+{
+    if (ix->f_conflict || ix->f_pairs == 0 || ix->nref < 2 || self_density(ix) < kDenseRatio)
+        return false;
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    // the estimate's margin: operands for twice the sampled allele count
+    return dense_bytes(ix, round_up(2 * ix->f_alleles, 128)) <= free_b / 2;
+}
+
 int self_lower_dev_impl(kssdgpu_index *ix, unsigned flags, unsigned long long *oc, unsigned long long *oo, cudaStream_t st)
 {
+    if (flags & KSSDGPU_SELF_DENSE)
+        return self_dense_impl(ix, oc, oo, st);
+    if (!(flags & (KSSDGPU_SELF_PLAN | KSSDGPU_SELF_SCAN)) && !(flags & KSSDGPU_NO_ZERO) && dense_chosen(ix))
+        return self_dense_impl(ix, oc, oo, st);
     if (!(flags & KSSDGPU_SELF_PLAN))
         return self_scan_impl(ix, flags, oc, oo, st);
     int rc = self_plan(ix, st);
@@ -3391,22 +3754,35 @@ int kssdgpu_self_plan_info(kssdgpu_index_t *ix, uint64_t *groups, uint64_t *post
 {
     if (!ix)
         return fail(KSSDGPU_ERR_ARG, "null index");
+    if (groups) *groups = ix->f_groups;
+    if (postings) *postings = ix->f_postings;
+    if (pairs) *pairs = ix->f_pairs;
+    return KSSDGPU_OK;
+}
+
+int kssdgpu_self_dense_alleles(kssdgpu_index_t *ix, uint64_t *alleles)
+{
+    if (!ix || !alleles)
+        return fail(KSSDGPU_ERR_ARG, "null argument");
+    *alleles = ix->d_alleles;
+    return KSSDGPU_OK;
+}
+
+int kssdgpu_self_choice(kssdgpu_index_t *ix, unsigned flags, int *path, double *density)
+{
+    if (!ix || !path)
+        return fail(KSSDGPU_ERR_ARG, "null argument");
     CUDA_TRY(cudaSetDevice(ix->device));
-    unsigned long long *d = nullptr, h[3] = {0, 0, 0};
-    CUDA_TRY(cudaMalloc(&d, sizeof h));
-    cudaError_t e = cudaMemset(d, 0, sizeof h);
-    if (e == cudaSuccess && ix->u) {
-        k_self_stats<<<grid_for(ix->u), 256>>>(ix->gbeg, ix->u, d);
-        count_launch();
-        e = cudaGetLastError();
-    }
-    if (e == cudaSuccess) e = cudaMemcpy(h, d, sizeof h, cudaMemcpyDeviceToHost);
-    cudaFree(d);
-    if (e != cudaSuccess)
-        return fail(KSSDGPU_ERR_CUDA, std::string("self-join facts: ") + cudaGetErrorString(e));
-    if (groups) *groups = h[0];
-    if (postings) *postings = h[1];
-    if (pairs) *pairs = h[2];
+    if (density)
+        *density = self_density(ix);
+    if (flags & KSSDGPU_SELF_DENSE)
+        *path = KSSDGPU_PATH_DENSE;
+    else if (flags & KSSDGPU_SELF_PLAN)
+        *path = KSSDGPU_PATH_PLAN;
+    else if (!(flags & (KSSDGPU_SELF_SCAN | KSSDGPU_NO_ZERO)) && dense_chosen(ix))
+        *path = KSSDGPU_PATH_DENSE;
+    else
+        *path = KSSDGPU_PATH_SCAN;
     return KSSDGPU_OK;
 }
 

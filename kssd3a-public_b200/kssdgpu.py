@@ -25,6 +25,9 @@ GLOBAL_ACC = 0x8
 NO_ZERO = 0x10
 SMEM_ACC = 0x20
 SELF_PLAN = 0x40
+SELF_SCAN = 0x80
+SELF_DENSE = 0x100
+PATH_SCAN, PATH_DENSE, PATH_PLAN = 0, 1, 2
 
 _u64p = np.ctypeslib.ndpointer(dtype=np.uint64, flags="C_CONTIGUOUS")
 _u32p = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
@@ -75,6 +78,8 @@ def gpu_lib() -> C.CDLL:
                                            C.POINTER(_CountTuning)]
         lib.kssdgpu_self_lower.argtypes = [vp, C.c_uint, vp, vp]
         lib.kssdgpu_self_lower_dev.argtypes = [vp, C.c_uint, vp, vp, vp]
+        lib.kssdgpu_self_choice.argtypes = [vp, C.c_uint, C.POINTER(C.c_int), C.POINTER(C.c_double)]
+        lib.kssdgpu_self_dense_alleles.argtypes = [vp, C.POINTER(C.c_uint64)]
         lib.kssdgpu_self_plan_tune.argtypes = [vp, C.POINTER(C.c_uint32), C.POINTER(C.c_int), C.POINTER(C.c_uint32),
                                                  C.POINTER(C.c_int), C.POINTER(C.c_float)]
         lib.kssdgpu_self_plan_info.argtypes = [vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
@@ -449,6 +454,18 @@ class Index:
                                                 C.byref(ms)))
         return dict(chunk_groups=c.value, sorted=bool(so.value), flat_groups=f.value, candidates=n.value,
                     step_ms=ms.value)
+
+    def dense_alleles(self) -> int:
+        """Allele rows (the GEMM's K before padding) of the last dense self join."""
+        a = C.c_uint64()
+        _check(gpu_lib().kssdgpu_self_dense_alleles(self._h, C.byref(a)))
+        return a.value
+
+    def self_choice(self, flags: int = 0):
+        """(path the self join takes for these flags: PATH_*, the index's shared-context density)."""
+        p, d = C.c_int(), C.c_double()
+        _check(gpu_lib().kssdgpu_self_choice(self._h, flags, C.byref(p), C.byref(d)))
+        return p.value, d.value
 
     def self_plan_info(self):
         g, p, q = C.c_uint64(), C.c_uint64(), C.c_uint64()

@@ -67,7 +67,7 @@ def test_count_lower_blocks(case, flags):
             np.testing.assert_array_equal(g, w)
 
 
-SELF_PATHS = [0, kssdgpu.SELF_PLAN]  # one-pass scan join (default), cached set-major plan
+SELF_PATHS = [0, kssdgpu.SELF_SCAN, kssdgpu.SELF_PLAN]  # by density (default), one-pass scan, cached plan
 
 
 @pytest.mark.parametrize("case", CASES[::3])
@@ -536,3 +536,63 @@ def test_count_detail_candidates(flags, cuts):
         for i in range(qry.n):
             ids = set(ranked.reshape(qry.n, ref.n)[i, :npass[i]].tolist())
             assert ids == set(np.flatnonzero(exact[i]).tolist())
+
+
+def _wide_cluster(n=160, seed=61, sub_hi=0.01):
+    """One species: every genome a member of one cluster at 0.1-1% substitutions, so most
+    contexts are shared by most genomes (dense incidence)."""
+    return kssdgpu.synth(n_samples=n, n_clusters=1, len_median=4e5, len_min=2e5, len_max=8e5,
+                         size_dist=kssdgpu.SIZE_LOGNORMAL, sub_lo=0.001, sub_hi=sub_hi, seed=seed, sample_seed=seed)
+
+
+@pytest.mark.parametrize("n,seed,sub_hi", [(160, 61, 0.01), (300, 62, 0.03), (129, 63, 0.2), (2, 64, 0.01)])
+def test_self_dense_join_matches_oracle(n, seed, sub_hi):
+    """The dense tensor-core self join (alleles of the shared contexts, one int8 GEMM)
+    gives the oracle's counters; on a dense index the default path chooses it."""
+    sk = _wide_cluster(n, seed, sub_hi)
+    rec = oracle.build_index(sk.keys, sk.offs)
+    idx = kssdgpu.Index.from_records(rec, sk.n)
+    want = oracle.self_lower_all(rec, sk.keys, sk.offs)
+    for flags in (kssdgpu.SELF_DENSE, 0, kssdgpu.SELF_SCAN):
+        got = idx.self_lower(flags)
+        np.testing.assert_array_equal(got[0], want[0])
+        np.testing.assert_array_equal(got[1], want[1])
+    path, density = idx.self_choice()
+    if sub_hi <= 0.03 and n >= 100:
+        assert path == kssdgpu.PATH_DENSE and density >= 1 / 2048
+    assert idx.self_choice(kssdgpu.SELF_SCAN)[0] == kssdgpu.PATH_SCAN
+
+
+@pytest.mark.parametrize("case", [c for c in CASES if not c[5]])
+def test_self_dense_join_on_sparse_fixtures(case):
+    """Forced on sparse conflict-free fixtures (empty samples, contexts of one genome)."""
+    rk, ro, _, _ = _fixture(*case)
+    rec = oracle.build_index(rk, ro)
+    idx = kssdgpu.Index.from_records(rec, len(ro) - 1)
+    want = oracle.self_lower_all(rec, rk, ro)
+    got = idx.self_lower(kssdgpu.SELF_DENSE)
+    np.testing.assert_array_equal(got[0], want[0])
+    np.testing.assert_array_equal(got[1], want[1])
+    assert idx.self_choice()[0] == kssdgpu.PATH_SCAN  # sparse: the scan
+
+
+def test_self_dense_join_wide_objects_and_conflicts():
+    """32-bit objects (differences capped at NUM_CODENS + 1) through the dense join; an
+    index with conflicts refuses it and the default path falls back to the scan."""
+    rng = np.random.default_rng(9)
+    samples = [[(c, int(rng.integers(0, 1 << 32))) for c in range(40) if rng.random() < 0.8] for _ in range(50)]
+    rk, ro = samples_to_sketch(samples, obj_bits=32)
+    rec = oracle.build_index(rk, ro, obj_bits=32)
+    idx = kssdgpu.Index.from_records(rec, 50, obj_bits=32)
+    want = oracle.self_lower_all(rec, rk, ro, obj_bits=32)
+    got = idx.self_lower(kssdgpu.SELF_DENSE)
+    np.testing.assert_array_equal(got[0], want[0])
+    np.testing.assert_array_equal(got[1], want[1])
+    assert want[1][:, 1].max() > 0
+    rk, ro, _, _ = _fixture(*CASES[0])  # conflicts
+    rec = oracle.build_index(rk, ro)
+    idx = kssdgpu.Index.from_records(rec, len(ro) - 1)
+    with pytest.raises(kssdgpu.KssdGpuError) as e:
+        idx.self_lower(kssdgpu.SELF_DENSE)
+    assert e.value.code == 1
+    assert idx.self_choice()[0] == kssdgpu.PATH_SCAN
