@@ -819,7 +819,7 @@ def run_ours(args, rank, world, local_rank):
 
     # ---- the north-star and config legs against a resident 20,000-genome index
     extra = {}
-    if rank == 0 and not args.no_extra:
+    if rank == 0 and world == 1 and not args.no_extra:
         del d_c, d_o
         torch.cuda.empty_cache()
         ns, ns_idx, ns_sk = leg_north_star(args, timer, dev, stream, peak)
