@@ -1,9 +1,9 @@
 // Exact int8 x int8 -> int32 GEMM on the sm_100a tensor cores (tcgen05.mma with the
 // accumulator in TMEM, operands staged into shared memory by TMA), through CUTLASS's
 // sm100 collective mainloop and epilogue.  Used by the dense self join of
-// libkssdgpu: D[M][N] = A[M][K] * B[N][K]^T with both operands K-major (row-major A,
-// column-major B), int32 D row-major.  One CTA per 128 x 128 tile, no thread-block
-// cluster (no multicast loads).
+// libkssdgpu: D[M][N] = sum_k A[k][m] B[k][n] with both operands MN-major (stored
+// K x M and K x N, rows contiguous over M and N), int32 D row-major.  One CTA per
+// 128 x 128 tile, no thread-block cluster (no multicast loads).
 #include "cutlass/cutlass.h"
 #include "cute/tensor.hpp"
 #include "cutlass/epilogue/collective/collective_builder.hpp"
@@ -26,8 +26,8 @@ using Epilogue = typename cutlass::epilogue::collective::CollectiveBuilder<
     cutlass::epilogue::collective::EpilogueTileAuto, int32_t, int32_t, int32_t, cutlass::layout::RowMajor, 4,
     int32_t, cutlass::layout::RowMajor, 4, cutlass::epilogue::collective::EpilogueScheduleAuto>::CollectiveOp;
 using Mainloop = typename cutlass::gemm::collective::CollectiveBuilder<
-    cutlass::arch::Sm100, cutlass::arch::OpClassTensorOp, int8_t, cutlass::layout::RowMajor, 16, int8_t,
-    cutlass::layout::ColumnMajor, 16, int32_t, TileShape, ClusterShape,
+    cutlass::arch::Sm100, cutlass::arch::OpClassTensorOp, int8_t, cutlass::layout::ColumnMajor, 16, int8_t,
+    cutlass::layout::RowMajor, 16, int32_t, TileShape, ClusterShape,
     cutlass::gemm::collective::StageCountAutoCarveout<static_cast<int>(sizeof(typename Epilogue::SharedStorage))>,
     cutlass::gemm::KernelTmaWarpSpecialized1SmSm100>::CollectiveOp;
 using Kernel = cutlass::gemm::kernel::GemmUniversal<Shape<int, int, int, int>, Mainloop, Epilogue, void>;
@@ -57,8 +57,9 @@ size_t dense_gemm_s8_workspace(int M, int N, int K)
     return Gemm::get_workspace_size(make_args(nullptr, nullptr, nullptr, M, N, K));
 }
 
-// D = A * B^T; K a multiple of 16, rows 16-byte aligned.  Returns 0, or 1 when the
-// shape is not supported, 2 when the launch failed.
+// D = A^T B for A stored K x M and B stored K x N; M and N multiples of 16 (16-byte
+// aligned rows).  Returns 0, or 1 when the shape is not supported, 2 when the launch
+// failed.
 int dense_gemm_s8(const int8_t *A, const int8_t *B, int32_t *D, int M, int N, int K, void *workspace,
                   cudaStream_t st)
 {

@@ -1482,77 +1482,130 @@ __global__ void k_dense_list(const uint32_t *__restrict__ gbeg, uint64_t u, unsi
     }
 }
 
-// Sort records of the shared postings: key (list rank << 32 | object), value gid; one
-// warp per listed group.
-__global__ void k_dense_keys(const unsigned long long *__restrict__ list, uint32_t n_list,
-                             const uint32_t *__restrict__ poff, const uint64_t *__restrict__ post,
-                             unsigned long long *__restrict__ keys, uint32_t *__restrict__ vals)
+// Largest shared group the dense join handles (its postings are sorted in shared
+// memory), which also bounds the references: the dense join needs nref <= this.
+constexpr uint32_t kDenseMaxGroup = 4096;
+constexpr int kDenseThreads = 256;
+
+// Sorts the group's postings (object << 32 | gid) ascending in shared memory (bitonic
+// over the next power of two, padded with ~0) and returns that power of two.
+__device__ uint32_t dense_sort_group(const uint64_t *__restrict__ post, uint32_t b, uint32_t k,
+                                     unsigned long long *__restrict__ v)
 {
-    const uint32_t lane = threadIdx.x & 31;
-    for (uint32_t s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < n_list;
-         s += (gridDim.x * blockDim.x) >> 5) {
-        const unsigned long long item = list[s];
-        const uint32_t b = (uint32_t)item, k = (uint32_t)(item >> 32), o = poff[s];
-        for (uint32_t i = lane; i < k; i += 32) {
-            const uint64_t p = post[b + i];
-            keys[o + i] = ((unsigned long long)s << 32) | (uint32_t)p;
-            vals[o + i] = (uint32_t)(p >> 32);
+    uint32_t m = 1;
+    while (m < k)
+        m <<= 1;
+    for (uint32_t j = threadIdx.x; j < m; j += blockDim.x) {
+        if (j < k) {
+            const uint64_t p = post[b + j];
+            v[j] = ((unsigned long long)(uint32_t)p << 32) | (p >> 32);
+        } else {
+            v[j] = ~0ull;
         }
     }
-}
-
-__global__ void k_unpack_k(const unsigned long long *__restrict__ list, uint32_t n, uint32_t *__restrict__ k)
-{
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-        k[i] = (uint32_t)(list[i] >> 32);
-}
-
-__global__ void k_dense_heads(const unsigned long long *__restrict__ keys, uint32_t n, uint32_t *__restrict__ heads)
-{
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-        heads[i] = i == 0 || keys[i] != keys[i - 1];
-}
-
-// A'[gid][allele] = 1 for every sorted posting; the first posting of every allele.
-__global__ void k_dense_fill_a(const uint32_t *__restrict__ vals, const uint32_t *__restrict__ heads,
-                               const uint32_t *__restrict__ allele_incl, uint32_t n, size_t kpad,
-                               int8_t *__restrict__ A, uint32_t *__restrict__ first)
-{
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const uint32_t a = allele_incl[i] - 1;
-        A[(size_t)vals[i] * kpad + a] = 1;
-        if (heads[i])
-            first[a] = i;
+    __syncthreads();
+    for (uint32_t size = 2; size <= m; size <<= 1) {
+        for (uint32_t stride = size >> 1; stride; stride >>= 1) {
+            for (uint32_t t = threadIdx.x; t < m / 2; t += blockDim.x) {
+                const uint32_t lo = 2 * t - (t & (stride - 1)), hi = lo + stride;
+                const bool up = (lo & size) == 0;
+                const unsigned long long x = v[lo], y = v[hi];
+                if ((x > y) == up) {
+                    v[lo] = y;
+                    v[hi] = x;
+                }
+            }
+            __syncthreads();
+        }
     }
+    return m;
 }
 
-// The four feature rows of every allele (one warp per allele, lanes over the postings
-// of its context).
-__global__ void k_dense_fill_f(const unsigned long long *__restrict__ keys, const uint32_t *__restrict__ first,
-                               uint32_t n_alleles, const unsigned long long *__restrict__ list,
-                               const uint64_t *__restrict__ post, int nref, size_t kpad, int8_t *__restrict__ F)
+// Alleles (distinct objects) of every listed shared group: one CTA per group.
+__global__ void __launch_bounds__(kDenseThreads) k_dense_alleles(const unsigned long long *__restrict__ list,
+                                                                 uint32_t n_list, const uint64_t *__restrict__ post,
+                                                                 uint32_t *__restrict__ alleles)
 {
-    const uint32_t lane = threadIdx.x & 31;
-    for (uint32_t a = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; a < n_alleles;
-         a += (gridDim.x * blockDim.x) >> 5) {
-        const unsigned long long key = keys[first[a]];
-        const uint32_t s = (uint32_t)(key >> 32), obj = (uint32_t)key;
+    extern __shared__ unsigned long long dsm[];
+    __shared__ uint32_t heads;
+    for (uint32_t s = blockIdx.x; s < n_list; s += gridDim.x) {
         const unsigned long long item = list[s];
         const uint32_t b = (uint32_t)item, k = (uint32_t)(item >> 32);
-        for (uint32_t i = lane; i < k; i += 32) {
-            const uint64_t p = post[b + i];
-            const size_t r = (size_t)(p >> 32);
-            const int d = min(kMinInit, dna_pop(obj ^ (uint32_t)p));
-            F[r * kpad + a] = 1;
-            F[(nref + r) * kpad + a] = (int8_t)(d >= 1);
-            F[(2 * (size_t)nref + r) * kpad + a] = (int8_t)(d >= 2);
-            F[(3 * (size_t)nref + r) * kpad + a] = (int8_t)d;
+        if (threadIdx.x == 0)
+            heads = 0;
+        dense_sort_group(post, b, k, dsm);  // ends with a barrier
+        uint32_t mine = 0;
+        for (uint32_t j = threadIdx.x; j < k; j += blockDim.x)
+            mine += j == 0 || (dsm[j] >> 32) != (dsm[j - 1] >> 32);
+        atomicAdd(&heads, mine);
+        __syncthreads();
+        if (threadIdx.x == 0)
+            alleles[s] = heads;
+        __syncthreads();
+    }
+}
+
+// The operand rows of every allele, written whole (allele-major: a row runs over the
+// genomes, so the GEMM takes both operands MN-major): A'[a][q] = 1 where genome q holds
+// the allele; F[a][x * npad + r] for every genome r at the allele's context, x = 0..3:
+// 1, d >= 1, d >= 2, d = min(dna_popcount(u ^ o_r), NUM_CODENS + 1).  One CTA per group:
+// its postings sorted by object (runs = alleles), each allele row built in shared
+// memory and stored with 16-byte writes.
+__global__ void __launch_bounds__(kDenseThreads) k_dense_rows(const unsigned long long *__restrict__ list,
+                                                              uint32_t n_list, const uint32_t *__restrict__ abase,
+                                                              const uint64_t *__restrict__ post, uint32_t npad,
+                                                              int8_t *__restrict__ A, int8_t *__restrict__ F)
+{
+    extern __shared__ unsigned long long dsm[];
+    int8_t *row = reinterpret_cast<int8_t *>(dsm + kDenseMaxGroup);  // npad (A) + 4 npad (F) bytes
+    __shared__ uint32_t run_b, run_e;
+    for (uint32_t s = blockIdx.x; s < n_list; s += gridDim.x) {
+        const unsigned long long item = list[s];
+        const uint32_t b = (uint32_t)item, k = (uint32_t)(item >> 32);
+        dense_sort_group(post, b, k, dsm);
+        uint32_t a = abase[s];
+        for (uint32_t start = 0; start < k;) {
+            // the run of equal objects beginning at `start`
+            if (threadIdx.x == 0) {
+                uint32_t e = start + 1;
+                while (e < k && (dsm[e] >> 32) == (dsm[start] >> 32))
+                    ++e;
+                run_b = start;
+                run_e = e;
+            }
+            uint4 *r4 = reinterpret_cast<uint4 *>(row);
+            for (uint32_t w = threadIdx.x; w < 5 * npad / 16; w += blockDim.x)
+                r4[w] = make_uint4(0u, 0u, 0u, 0u);
+            __syncthreads();
+            const uint32_t rb = run_b, re = run_e;
+            const uint32_t u = (uint32_t)(dsm[rb] >> 32);
+            for (uint32_t j = threadIdx.x; j < k; j += blockDim.x) {
+                const uint32_t o = (uint32_t)(dsm[j] >> 32), r = (uint32_t)dsm[j];
+                const int d = min(kMinInit, dna_pop(u ^ o));
+                if (j >= rb && j < re)
+                    row[r] = 1;
+                int8_t *f = row + npad;
+                f[r] = 1;
+                f[npad + r] = (int8_t)(d >= 1);
+                f[2 * npad + r] = (int8_t)(d >= 2);
+                f[3 * npad + r] = (int8_t)d;
+            }
+            __syncthreads();
+            uint4 *ga = reinterpret_cast<uint4 *>(A + (size_t)a * npad);
+            uint4 *gf = reinterpret_cast<uint4 *>(F + (size_t)a * 4 * npad);
+            for (uint32_t w = threadIdx.x; w < npad / 16; w += blockDim.x)
+                ga[w] = r4[w];
+            for (uint32_t w = threadIdx.x; w < 4 * npad / 16; w += blockDim.x)
+                gf[w] = r4[npad / 16 + w];
+            __syncthreads();
+            start = re;
+            ++a;
         }
     }
 }
 
-// Packed lower triangle from D (n x 4n): every cell written (zeros included).
-__global__ void k_dense_epilogue(const int32_t *__restrict__ D, int nref, size_t cells,
+// Packed lower triangle from D (npad x 4 npad): every cell written (zeros included).
+__global__ void k_dense_epilogue(const int32_t *__restrict__ D, uint32_t npad, size_t cells,
                                  unsigned long long *__restrict__ oc, unsigned long long *__restrict__ oo)
 {
     for (size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x; c < cells; c += (size_t)gridDim.x * blockDim.x) {
@@ -1563,9 +1616,9 @@ __global__ void k_dense_epilogue(const int32_t *__restrict__ D, int nref, size_t
         while ((size_t)(q + 1) * q / 2 <= c)
             ++q;
         const uint32_t r = (uint32_t)(c - (size_t)q * (q - 1) / 2);
-        const int32_t *row = D + (size_t)q * 4 * nref;
-        oc[c] = (unsigned long long)(uint32_t)row[r] | ((unsigned long long)(uint32_t)row[2 * nref + r] << 32);
-        oo[c] = (unsigned long long)(uint32_t)row[nref + r] | ((unsigned long long)(uint32_t)row[3 * nref + r] << 32);
+        const int32_t *d = D + (size_t)q * 4 * npad;
+        oc[c] = (unsigned long long)(uint32_t)d[r] | ((unsigned long long)(uint32_t)d[2 * npad + r] << 32);
+        oo[c] = (unsigned long long)(uint32_t)d[npad + r] | ((unsigned long long)(uint32_t)d[3 * npad + r] << 32);
     }
 }
 
@@ -1731,8 +1784,8 @@ struct kssdgpu_index {
     unsigned long long f_alleles = 0;       // distinct objects of the shared contexts (sampled estimate)
     bool f_conflict = false;
     // dense self join scratch
-    DevBuf<unsigned long long> d_list, d_keys, d_keys2;
-    DevBuf<uint32_t> d_poff, d_vals, d_vals2, d_heads, d_allele, d_first;
+    DevBuf<unsigned long long> d_list;
+    DevBuf<uint32_t> d_poff, d_allele;
     DevBuf<int8_t> d_a, d_f;
     DevBuf<int32_t> d_d;
     DevBuf<unsigned char> d_tmp, d_ws;
@@ -2929,17 +2982,20 @@ int self_scan_impl(kssdgpu_index *ix, unsigned flags, unsigned long long *oc, un
 }
 
 // Device bytes of a dense self join with K allele rows (A', F, D).
+uint64_t dense_npad(const kssdgpu_index *ix) { return ((uint64_t)ix->nref + 15) / 16 * 16; }
 uint64_t dense_bytes(const kssdgpu_index *ix, uint64_t kpad)
 {
-    return 5ull * (uint64_t)ix->nref * kpad + 16ull * (uint64_t)ix->nref * (uint64_t)ix->nref;
+    const uint64_t np = dense_npad(ix);
+    return 5ull * np * kpad + 16ull * np * np;
 }
 
 uint64_t round_up(uint64_t x, uint64_t m) { return (x + m - 1) / m * m; }
 
-// Dense self join (see k_dense_list): list the shared groups, sort their postings by
-// (group, object) to find the alleles, fill A' and F, one tensor-core GEMM, and the
-// packed lower triangle (every cell written, so no zero fill).  Conflict-free indexes
-// only; the GEMM's allele count bounds its memory (checked against free memory).
+// Dense self join (see k_dense_list): list the shared groups, count their alleles
+// (distinct objects, from a sort of each group's postings in shared memory), build
+// every allele's operand rows, one tensor-core GEMM, and the packed lower triangle
+// (every cell written, so no zero fill).  Conflict-free indexes of at most
+// kDenseMaxGroup references only; the operands must fit in half of the free memory.
 int self_dense_impl(kssdgpu_index *ix, unsigned long long *oc, unsigned long long *oo, cudaStream_t st)
 {
     const int n = ix->nref;
@@ -2947,91 +3003,76 @@ int self_dense_impl(kssdgpu_index *ix, unsigned long long *oc, unsigned long lon
     if (ix->f_conflict)
         return fail(KSSDGPU_ERR_ARG, "the dense self join needs a conflict-free index (a gid holds several objects "
                                      "of one context)");
+    if ((uint32_t)n > kDenseMaxGroup)
+        return fail(KSSDGPU_ERR_CAPACITY, "the dense self join takes at most " + std::to_string(kDenseMaxGroup) +
+                                              " references");
     if (!cells)
         return KSSDGPU_OK;
-    const uint32_t S = (uint32_t)ix->f_groups, P = (uint32_t)ix->f_postings;
-    if (ix->f_groups >= (1ull << 32) || ix->f_postings >= (1ull << 32))
-        return fail(KSSDGPU_ERR_CAPACITY, "dense self join: too many shared postings");
-    size_t free_b = 0, total_b = 0;
-    CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
+    if (ix->f_groups >= (1ull << 31))
+        return fail(KSSDGPU_ERR_CAPACITY, "dense self join: too many shared contexts");
+    const uint32_t S = (uint32_t)ix->f_groups;
     if (!S) {
         CUDA_TRY(cudaMemsetAsync(oc, 0, cells * 8, st));
         CUDA_TRY(cudaMemsetAsync(oo, 0, cells * 8, st));
         return KSSDGPU_OK;
     }
+    const uint32_t npad = (uint32_t)dense_npad(ix);
+    const size_t sort_smem = kDenseMaxGroup * sizeof(unsigned long long);
+    const size_t rows_smem = sort_smem + 5 * (size_t)npad;
+    CUDA_TRY(cudaFuncSetAttribute(k_dense_alleles, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sort_smem));
+    CUDA_TRY(cudaFuncSetAttribute(k_dense_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rows_smem));
     CUDA_TRY(ix->d_list.ensure(S));
-    CUDA_TRY(ix->d_poff.ensure((size_t)S + 1));
-    CUDA_TRY(ix->d_keys.ensure(P));
-    CUDA_TRY(ix->d_keys2.ensure(P));
-    CUDA_TRY(ix->d_vals.ensure(P));
-    CUDA_TRY(ix->d_vals2.ensure(P));
-    CUDA_TRY(ix->d_heads.ensure(P));
-    CUDA_TRY(ix->d_allele.ensure(P));
-    CUDA_TRY(ix->d_first.ensure(P));
-    unsigned int *d_count = reinterpret_cast<unsigned int *>(ix->d_poff.p + S);  // the list's fill counter
-    int bits = 32;
-    while (bits < 64 && (1ull << (bits - 32)) < (unsigned long long)S)
-        ++bits;
-    size_t tb1 = 0, tb2 = 0, tb3 = 0;
-    CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, tb1, ix->d_heads.p, ix->d_poff.p, S, st));
-    CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, tb2, ix->d_keys.p, ix->d_keys2.p, ix->d_vals.p, ix->d_vals2.p, P, 0,
-                                             bits, st));
-    CUDA_TRY(cub::DeviceScan::InclusiveSum(nullptr, tb3, ix->d_heads.p, ix->d_allele.p, P, st));
-    CUDA_TRY(ix->d_tmp.ensure(std::max(tb1, std::max(tb2, tb3))));
-    // 1. the shared groups and their posting offsets
+    CUDA_TRY(ix->d_poff.ensure((size_t)S + 1));   // alleles per group, then the fill counter
+    CUDA_TRY(ix->d_allele.ensure((size_t)S + 1)); // first allele row of every group
+    unsigned int *d_count = reinterpret_cast<unsigned int *>(ix->d_poff.p + S);
+    size_t tb = 0;
+    CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, tb, ix->d_poff.p, ix->d_allele.p, (int)S + 1, st));
+    CUDA_TRY(ix->d_tmp.ensure(tb));
+    // 1. the shared groups, their allele counts and first allele rows
     CUDA_TRY(cudaMemsetAsync(d_count, 0, sizeof(unsigned int), st));
     k_dense_list<<<grid_for(ix->u), 256, 0, st>>>(ix->gbeg, ix->u, ix->d_list.p, d_count);
-    k_unpack_k<<<grid_for(S), 256, 0, st>>>(ix->d_list.p, S, ix->d_heads.p);
-    count_launch(2);
-    size_t tb = ix->d_tmp.cap;
-    CUDA_TRY(cub::DeviceScan::ExclusiveSum(ix->d_tmp.p, tb, ix->d_heads.p, ix->d_poff.p, S, st));
-    count_launch();
-    // 2. alleles: postings sorted by (group, object); runs of equal keys
-    k_dense_keys<<<std::min<uint64_t>(((uint64_t)S * 32 + 255) / 256, (uint64_t)ix->sms * 64), 256, 0, st>>>(
-        ix->d_list.p, S, ix->d_poff.p, ix->post, ix->d_keys.p, ix->d_vals.p);
-    count_launch();
+    const int grid = ix->sms * 4;
+    k_dense_alleles<<<grid, kDenseThreads, sort_smem, st>>>(ix->d_list.p, S, ix->post, ix->d_poff.p);
+    CUDA_TRY(cudaMemsetAsync(d_count, 0, sizeof(unsigned int), st));  // poff[S] = 0: the scan's last term
     tb = ix->d_tmp.cap;
-    CUDA_TRY(cub::DeviceRadixSort::SortPairs(ix->d_tmp.p, tb, ix->d_keys.p, ix->d_keys2.p, ix->d_vals.p, ix->d_vals2.p,
-                                             P, 0, bits, st));
+    CUDA_TRY(cub::DeviceScan::ExclusiveSum(ix->d_tmp.p, tb, ix->d_poff.p, ix->d_allele.p, (int)S + 1, st));
     count_launch(4);
-    k_dense_heads<<<grid_for(P), 256, 0, st>>>(ix->d_keys2.p, P, ix->d_heads.p);
-    count_launch();
-    tb = ix->d_tmp.cap;
-    CUDA_TRY(cub::DeviceScan::InclusiveSum(ix->d_tmp.p, tb, ix->d_heads.p, ix->d_allele.p, P, st));
-    count_launch();
     uint32_t alleles = 0;
-    CUDA_TRY(cudaMemcpyAsync(&alleles, ix->d_allele.p + P - 1, 4, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaMemcpyAsync(&alleles, ix->d_allele.p + S, 4, cudaMemcpyDeviceToHost, st));
     CUDA_TRY(cudaStreamSynchronize(st));
     ix->d_alleles = alleles;
     const uint64_t kpad = round_up(std::max<uint32_t>(alleles, 1), 128);
+    size_t free_b = 0, total_b = 0;
+    CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
     if (dense_bytes(ix, kpad) > free_b / 2)
         return fail(KSSDGPU_ERR_NOMEM, "dense self join: operands of " + std::to_string(dense_bytes(ix, kpad)) +
                                            " bytes exceed half of the free device memory");
-    // 3. operands
-    CUDA_TRY(ix->d_a.ensure((size_t)n * kpad));
-    CUDA_TRY(ix->d_f.ensure((size_t)4 * n * kpad));
-    CUDA_TRY(ix->d_d.ensure((size_t)4 * n * n));
-    CUDA_TRY(cudaMemsetAsync(ix->d_a.p, 0, (size_t)n * kpad, st));
-    CUDA_TRY(cudaMemsetAsync(ix->d_f.p, 0, (size_t)4 * n * kpad, st));
-    k_dense_fill_a<<<grid_for(P), 256, 0, st>>>(ix->d_vals2.p, ix->d_heads.p, ix->d_allele.p, P, kpad, ix->d_a.p,
-                                                ix->d_first.p);
-    k_dense_fill_f<<<std::min<uint64_t>(((uint64_t)alleles * 32 + 255) / 256, (uint64_t)ix->sms * 64), 256, 0, st>>>(
-        ix->d_keys2.p, ix->d_first.p, alleles, ix->d_list.p, ix->post, n, kpad, ix->d_f.p);
-    count_launch(2);
-    CUDA_TRY(cudaGetLastError());
-    // 4. D = A' F^T on the tensor cores
-    const size_t ws = kssd::dense_gemm_s8_workspace(n, 4 * n, (int)kpad);
-    CUDA_TRY(ix->d_ws.ensure(ws));
     if (kpad > 0x7FFFFFFFull)
         return fail(KSSDGPU_ERR_CAPACITY, "dense self join: allele count beyond the GEMM's 32-bit extent");
-    const int grc = kssd::dense_gemm_s8(ix->d_a.p, ix->d_f.p, ix->d_d.p, n, 4 * n, (int)kpad, ix->d_ws.p, st);
+    // 2. operands, allele-major; the padding rows past the last allele are zero
+    CUDA_TRY(ix->d_a.ensure((size_t)npad * kpad));
+    CUDA_TRY(ix->d_f.ensure((size_t)4 * npad * kpad));
+    CUDA_TRY(ix->d_d.ensure((size_t)4 * npad * npad));
+    if (kpad > alleles) {
+        CUDA_TRY(cudaMemsetAsync(ix->d_a.p + (size_t)alleles * npad, 0, (size_t)(kpad - alleles) * npad, st));
+        CUDA_TRY(cudaMemsetAsync(ix->d_f.p + (size_t)alleles * 4 * npad, 0, (size_t)(kpad - alleles) * 4 * npad, st));
+    }
+    k_dense_rows<<<grid, kDenseThreads, rows_smem, st>>>(ix->d_list.p, S, ix->d_allele.p, ix->post, npad, ix->d_a.p,
+                                                         ix->d_f.p);
+    count_launch();
+    CUDA_TRY(cudaGetLastError());
+    // 3. D = A' F^T on the tensor cores (both operands MN-major)
+    const size_t ws = kssd::dense_gemm_s8_workspace((int)npad, (int)(4 * npad), (int)kpad);
+    CUDA_TRY(ix->d_ws.ensure(ws));
+    const int grc = kssd::dense_gemm_s8(ix->d_a.p, ix->d_f.p, ix->d_d.p, (int)npad, (int)(4 * npad), (int)kpad,
+                                        ix->d_ws.p, st);
     count_launch();
     if (grc)
         return fail(KSSDGPU_ERR_CUDA, grc == 1 ? "dense self join: GEMM shape not supported"
                                                : "dense self join: GEMM launch failed");
     CUDA_TRY(cudaGetLastError());
-    // 5. the packed lower triangle
-    k_dense_epilogue<<<grid_for(cells), 256, 0, st>>>(ix->d_d.p, n, cells, oc, oo);
+    // 4. the packed lower triangle
+    k_dense_epilogue<<<grid_for(cells), 256, 0, st>>>(ix->d_d.p, npad, cells, oc, oo);
     count_launch();
     CUDA_TRY(cudaGetLastError());
     return KSSDGPU_OK;
@@ -3052,7 +3093,8 @@ double self_density(const kssdgpu_index *ix)
 
 bool dense_chosen(const kssdgpu_index *ix)
 {
-    if (ix->f_conflict || ix->f_pairs == 0 || ix->nref < 2 || self_density(ix) < kDenseRatio)
+    if (ix->f_conflict || ix->f_pairs == 0 || ix->nref < 2 || (uint32_t)ix->nref > kDenseMaxGroup ||
+        self_density(ix) < kDenseRatio)
         return false;
     size_t free_b = 0, total_b = 0;
     if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
