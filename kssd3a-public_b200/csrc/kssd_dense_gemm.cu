@@ -3,7 +3,7 @@
 // sm100 collective mainloop and epilogue.  Used by the dense self join of
 // libkssdgpu: D[M][N] = sum_k A[k][m] B[k][n] with both operands MN-major (stored
 // K x M and K x N, rows contiguous over M and N), int32 D row-major.  One CTA per
-// 128 x 128 tile, no thread-block cluster (no multicast loads).
+// 128 x 128 tile, no thread-block cluster (no multicast loads), stream-K scheduling.
 #include "cutlass/cutlass.h"
 #include "cute/tensor.hpp"
 #include "cutlass/epilogue/collective/collective_builder.hpp"
@@ -30,7 +30,10 @@ using Mainloop = typename cutlass::gemm::collective::CollectiveBuilder<
     cutlass::layout::RowMajor, 16, int32_t, TileShape, ClusterShape,
     cutlass::gemm::collective::StageCountAutoCarveout<static_cast<int>(sizeof(typename Epilogue::SharedStorage))>,
     cutlass::gemm::KernelTmaWarpSpecialized1SmSm100>::CollectiveOp;
-using Kernel = cutlass::gemm::kernel::GemmUniversal<Shape<int, int, int, int>, Mainloop, Epilogue, void>;
+// stream-K: the output has few 128 x 128 tiles (n x 4n for n of hundreds to thousands of
+// genomes) against a deep K, so the K loop of each tile is split across SMs
+using Kernel =
+    cutlass::gemm::kernel::GemmUniversal<Shape<int, int, int, int>, Mainloop, Epilogue, cutlass::gemm::StreamKScheduler>;
 using Gemm = cutlass::gemm::device::GemmUniversalAdapter<Kernel>;
 
 typename Gemm::Arguments make_args(const int8_t *A, const int8_t *B, int32_t *D, int M, int N, int K)

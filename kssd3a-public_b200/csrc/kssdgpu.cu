@@ -1311,34 +1311,44 @@ __device__ __forceinline__ void join_group_cta(const uint64_t *__restrict__ post
     }
 }
 
-// Warp-aggregated append to a shared-memory counter; returns this lane's slot.
-__device__ __forceinline__ uint32_t smem_slot(uint32_t *counter, bool want, unsigned lane)
+// Shared memory of k_self_scan: the tile's queue of shared groups, and (PAIRS) the
+// exclusive prefix of the small groups' pair counts.
+struct ScanSmem {
+    unsigned long long queue[kScanTile];  // groups of 2..kScanLaneMax from the front, larger from the back
+    uint32_t prefix[kScanTile];
+};
+
+// The pair (i < j) of rank t among the k(k-1)/2 pairs of a group: j(j-1)/2 <= t.
+__device__ __forceinline__ void pair_of_rank(uint32_t t, uint32_t &i, uint32_t &j)
 {
-    const unsigned m = __ballot_sync(0xffffffffu, want);
-    uint32_t base = 0;
-    if (m && lane == (unsigned)(__ffs(m) - 1))
-        base = atomicAdd(counter, (uint32_t)__popc(m));
-    base = __shfl_sync(0xffffffffu, base, m ? __ffs(m) - 1 : 0);
-    return base + (uint32_t)__popc(m & ((1u << lane) - 1u));
+    j = (uint32_t)((1.0f + sqrtf(1.0f + 8.0f * (float)t)) * 0.5f);
+    while (j * (j - 1) / 2 > t)
+        --j;
+    while ((j + 1) * j / 2 <= t)
+        ++j;
+    i = t - j * (j - 1) / 2;
 }
 
+// Per tile: every thread loads 16 group bounds (coalesced, all in flight), block scans
+// place its shared groups in the queue.  PAIRS (a conflict-free index: one object per
+// gid run): the small groups' pairs are then dealt out evenly, thread t taking a
+// contiguous range of the tile's pair ranks, so every lane runs the same short
+// sequence per pair and no thread walks a whole large group while the others wait;
+// with conflicts every thread walks whole groups (run cross products).  Groups of more
+// than kScanLaneMax postings are taken by the whole CTA.
+template <bool PAIRS>
 __global__ void __launch_bounds__(kScanThreads) k_self_scan(const uint32_t *__restrict__ gbeg, uint64_t u,
                                                             const uint64_t *__restrict__ post, int ignoreconflict,
                                                             unsigned long long *__restrict__ oc,
                                                             unsigned long long *__restrict__ oo)
 {
-    // groups of 2..kScanLaneMax postings from the front, larger ones from the back
-    __shared__ unsigned long long queue[kScanTile];
-    __shared__ uint32_t n_lane, n_cta;
-    const unsigned lane = threadIdx.x & 31;
+    extern __shared__ __align__(16) unsigned char scan_smem[];
+    ScanSmem &S = *reinterpret_cast<ScanSmem *>(scan_smem);
+    using Scan = cub::BlockScan<uint32_t, kScanThreads>;
+    __shared__ typename Scan::TempStorage scan_tmp;
     const uint64_t ntiles = (u + kScanTile - 1) / kScanTile;
     bool waited = false;
     for (uint64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
-        if (threadIdx.x == 0) {
-            n_lane = 0;
-            n_cta = 0;
-        }
-        __syncthreads();
         const uint64_t base = t * kScanTile;
         uint32_t beg[kScanPerThread], cnt[kScanPerThread];
 #pragma unroll
@@ -1351,33 +1361,81 @@ __global__ void __launch_bounds__(kScanThreads) k_self_scan(const uint32_t *__re
                 cnt[j] = __ldg(gbeg + g + 1);
             }
         }
+        // this thread's small / large shared groups (low / high 16 bits) and small pairs
+        uint32_t mine = 0, my_pairs = 0;
 #pragma unroll
         for (uint32_t j = 0; j < kScanPerThread; ++j) {
             const uint32_t k = cnt[j] - beg[j];
+            cnt[j] = k;
+            const bool small = k >= 2 && k <= kScanLaneMax;
+            mine += small ? 1u : (k > kScanLaneMax ? 0x10000u : 0u);
+            my_pairs += small ? k * (k - 1) / 2 : 0u;
+        }
+        uint32_t off, tot, poff, ptot;
+        Scan(scan_tmp).ExclusiveSum(mine, off, tot);
+        __syncthreads();
+        if (PAIRS)
+            Scan(scan_tmp).ExclusiveSum(my_pairs, poff, ptot);
+        uint32_t sl = off & 0xFFFFu, ll = off >> 16;
+#pragma unroll
+        for (uint32_t j = 0; j < kScanPerThread; ++j) {
+            const uint32_t k = cnt[j];
             const unsigned long long item = (unsigned long long)beg[j] | ((unsigned long long)k << 32);
-            const bool small = k >= 2 && k <= kScanLaneMax, large = k > kScanLaneMax;
-            const uint32_t s = smem_slot(&n_lane, small, lane);
-            if (small)
-                queue[s] = item;
-            const uint32_t l = smem_slot(&n_cta, large, lane);
-            if (large)
-                queue[kScanTile - 1 - l] = item;
+            if (k >= 2 && k <= kScanLaneMax) {
+                S.queue[sl] = item;
+                if (PAIRS) {
+                    S.prefix[sl] = poff;
+                    poff += k * (k - 1) / 2;
+                }
+                ++sl;
+            } else if (k > kScanLaneMax) {
+                S.queue[kScanTile - 1 - ll] = item;
+                ++ll;
+            }
         }
         __syncthreads();
+        const uint32_t nl = tot & 0xFFFFu, nc = tot >> 16;
         if (!waited) {
             pdl_wait_primary();  // the counters' zero fill has finished (no-op without a dependency)
             waited = true;
         }
-        const uint32_t nl = n_lane, nc = n_cta;
-        for (uint32_t i = threadIdx.x; i < nl; i += kScanThreads) {
-            const unsigned long long item = queue[i];
-            join_group_lane(post, (uint32_t)item, (uint32_t)(item >> 32), ignoreconflict, oc, oo);
+        if (PAIRS) {
+            const uint32_t total = ptot;
+            const uint32_t p0 = (uint32_t)((uint64_t)total * threadIdx.x / kScanThreads);
+            const uint32_t p1 = (uint32_t)((uint64_t)total * (threadIdx.x + 1) / kScanThreads);
+            if (p0 < p1) {
+                // the group holding pair rank p0: the last q < nl with prefix[q] <= p0
+                uint32_t lo = 0, hi = nl - 1;
+                while (lo < hi) {
+                    const uint32_t mid = (lo + hi + 1) >> 1;
+                    if (S.prefix[mid] <= p0)
+                        lo = mid;
+                    else
+                        hi = mid - 1;
+                }
+                uint32_t q = lo;
+                for (uint32_t pr = p0; pr < p1; ++pr) {
+                    while (q + 1 < nl && S.prefix[q + 1] <= pr)
+                        ++q;
+                    const unsigned long long item = S.queue[q];
+                    uint32_t i, j;
+                    pair_of_rank(pr - S.prefix[q], i, j);
+                    const uint64_t pi = __ldg(post + (uint32_t)item + i), pj = __ldg(post + (uint32_t)item + j);
+                    const int d = min(kMinInit, dna_pop((uint32_t)pi ^ (uint32_t)pj));
+                    credit_lower(oc, oo, (uint32_t)(pj >> 32), (uint32_t)(pi >> 32), d);
+                }
+            }
+        } else {
+            for (uint32_t i = threadIdx.x; i < nl; i += kScanThreads) {
+                const unsigned long long item = S.queue[i];
+                join_group_lane(post, (uint32_t)item, (uint32_t)(item >> 32), ignoreconflict, oc, oo);
+            }
         }
         for (uint32_t i = 0; i < nc; ++i) {
-            const unsigned long long item = queue[kScanTile - 1 - i];
+            const unsigned long long item = S.queue[kScanTile - 1 - i];
             join_group_cta(post, (uint32_t)item, (uint32_t)(item >> 32), ignoreconflict, oc, oo);
         }
-        __syncthreads();  // the queue is refilled by the next tile
+        __syncthreads();  // the queue and the scan storage are reused by the next tile
     }
 }
 
@@ -1545,62 +1603,82 @@ __global__ void __launch_bounds__(kDenseThreads) k_dense_alleles(const unsigned 
     }
 }
 
+// Byte offset of the row buffers in k_dense_rows' shared memory (after the sorted
+// postings and the allele starts).
+constexpr size_t kDenseRowsOffset = kDenseMaxGroup * 8 + (kDenseMaxGroup + 16) * 4;
+constexpr size_t kDenseRowBudget = 160 * 1024;  // shared memory for row buffers
+
 // The operand rows of every allele, written whole (allele-major: a row runs over the
 // genomes, so the GEMM takes both operands MN-major): A'[a][q] = 1 where genome q holds
 // the allele; F[a][x * npad + r] for every genome r at the allele's context, x = 0..3:
 // 1, d >= 1, d >= 2, d = min(dna_popcount(u ^ o_r), NUM_CODENS + 1).  One CTA per group:
-// its postings sorted by object (runs = alleles), each allele row built in shared
-// memory and stored with 16-byte writes.
+// its postings sorted by object (runs = alleles, their starts from a block scan), then
+// each of nbuf warps builds one allele's rows at a time in its own shared-memory
+// buffer and stores them with 16-byte writes.
 __global__ void __launch_bounds__(kDenseThreads) k_dense_rows(const unsigned long long *__restrict__ list,
                                                               uint32_t n_list, const uint32_t *__restrict__ abase,
                                                               const uint64_t *__restrict__ post, uint32_t npad,
-                                                              int8_t *__restrict__ A, int8_t *__restrict__ F)
+                                                              uint32_t nbuf, int8_t *__restrict__ A,
+                                                              int8_t *__restrict__ F)
 {
     extern __shared__ unsigned long long dsm[];
-    int8_t *row = reinterpret_cast<int8_t *>(dsm + kDenseMaxGroup);  // npad (A) + 4 npad (F) bytes
-    __shared__ uint32_t run_b, run_e;
+    uint32_t *start = reinterpret_cast<uint32_t *>(dsm + kDenseMaxGroup);
+    int8_t *rows = reinterpret_cast<int8_t *>(dsm) + kDenseRowsOffset;
+    constexpr uint32_t kPer = kDenseMaxGroup / kDenseThreads;
+    using Scan = cub::BlockScan<uint32_t, kDenseThreads>;
+    __shared__ typename Scan::TempStorage scan_tmp;
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (uint32_t s = blockIdx.x; s < n_list; s += gridDim.x) {
         const unsigned long long item = list[s];
         const uint32_t b = (uint32_t)item, k = (uint32_t)(item >> 32);
         dense_sort_group(post, b, k, dsm);
-        uint32_t a = abase[s];
-        for (uint32_t start = 0; start < k;) {
-            // the run of equal objects beginning at `start`
-            if (threadIdx.x == 0) {
-                uint32_t e = start + 1;
-                while (e < k && (dsm[e] >> 32) == (dsm[start] >> 32))
-                    ++e;
-                run_b = start;
-                run_e = e;
-            }
-            uint4 *r4 = reinterpret_cast<uint4 *>(row);
-            for (uint32_t w = threadIdx.x; w < 5 * npad / 16; w += blockDim.x)
-                r4[w] = make_uint4(0u, 0u, 0u, 0u);
-            __syncthreads();
-            const uint32_t rb = run_b, re = run_e;
-            const uint32_t u = (uint32_t)(dsm[rb] >> 32);
-            for (uint32_t j = threadIdx.x; j < k; j += blockDim.x) {
-                const uint32_t o = (uint32_t)(dsm[j] >> 32), r = (uint32_t)dsm[j];
-                const int d = min(kMinInit, dna_pop(u ^ o));
-                if (j >= rb && j < re)
-                    row[r] = 1;
-                int8_t *f = row + npad;
-                f[r] = 1;
-                f[npad + r] = (int8_t)(d >= 1);
-                f[2 * npad + r] = (int8_t)(d >= 2);
-                f[3 * npad + r] = (int8_t)d;
-            }
-            __syncthreads();
-            uint4 *ga = reinterpret_cast<uint4 *>(A + (size_t)a * npad);
-            uint4 *gf = reinterpret_cast<uint4 *>(F + (size_t)a * 4 * npad);
-            for (uint32_t w = threadIdx.x; w < npad / 16; w += blockDim.x)
-                ga[w] = r4[w];
-            for (uint32_t w = threadIdx.x; w < 4 * npad / 16; w += blockDim.x)
-                gf[w] = r4[npad / 16 + w];
-            __syncthreads();
-            start = re;
-            ++a;
+        // allele starts: the positions where the object changes
+        uint32_t h[kPer], pos[kPer], m = 0;
+#pragma unroll
+        for (uint32_t i = 0; i < kPer; ++i) {
+            const uint32_t j = threadIdx.x * kPer + i;
+            h[i] = j < k && (j == 0 || (dsm[j] >> 32) != (dsm[j - 1] >> 32));
         }
+        Scan(scan_tmp).ExclusiveSum(h, pos, m);
+#pragma unroll
+        for (uint32_t i = 0; i < kPer; ++i)
+            if (h[i])
+                start[pos[i]] = threadIdx.x * kPer + i;
+        if (threadIdx.x == 0)
+            start[m] = k;
+        __syncthreads();
+        const uint32_t a0 = abase[s];
+        if (warp < nbuf) {
+            int8_t *row = rows + (size_t)warp * 5 * npad;
+            uint4 *r4 = reinterpret_cast<uint4 *>(row);
+            for (uint32_t a = warp; a < m; a += nbuf) {
+                for (uint32_t w = lane; w < 5 * npad / 16; w += 32)
+                    r4[w] = make_uint4(0u, 0u, 0u, 0u);
+                __syncwarp();
+                const uint32_t rb = start[a], re = start[a + 1];
+                const uint32_t u = (uint32_t)(dsm[rb] >> 32);
+                int8_t *f = row + npad;
+                for (uint32_t j = lane; j < k; j += 32) {
+                    const uint32_t o = (uint32_t)(dsm[j] >> 32), r = (uint32_t)dsm[j];
+                    const int d = min(kMinInit, dna_pop(u ^ o));
+                    if (j >= rb && j < re)
+                        row[r] = 1;
+                    f[r] = 1;
+                    f[npad + r] = (int8_t)(d >= 1);
+                    f[2 * npad + r] = (int8_t)(d >= 2);
+                    f[3 * npad + r] = (int8_t)d;
+                }
+                __syncwarp();
+                uint4 *ga = reinterpret_cast<uint4 *>(A + (size_t)(a0 + a) * npad);
+                uint4 *gf = reinterpret_cast<uint4 *>(F + (size_t)(a0 + a) * 4 * npad);
+                for (uint32_t w = lane; w < npad / 16; w += 32)
+                    ga[w] = r4[w];
+                for (uint32_t w = lane; w < 4 * npad / 16; w += 32)
+                    gf[w] = r4[npad / 16 + w];
+                __syncwarp();
+            }
+        }
+        __syncthreads();  // the sorted postings and the starts are reused by the next group
     }
 }
 
@@ -2957,15 +3035,22 @@ int self_scan_impl(kssdgpu_index *ix, unsigned flags, unsigned long long *oc, un
     }
     if (!ix->u)
         return KSSDGPU_OK;
+    // a conflict-free index deals out pairs; with conflicts threads walk whole groups
+    const bool pairs = !ix->f_conflict;
+    auto kern = pairs ? k_self_scan<true> : k_self_scan<false>;
+    const size_t smem = sizeof(ScanSmem);
     if (!ix->scan_grid) {
+        CUDA_TRY(cudaFuncSetAttribute(k_self_scan<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        CUDA_TRY(cudaFuncSetAttribute(k_self_scan<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         int per_sm = 0;
-        CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_self_scan, kScanThreads, 0));
+        CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_self_scan<true>, kScanThreads, smem));
         ix->scan_grid = std::max(1, per_sm) * ix->sms;
     }
     const uint64_t ntiles = (ix->u + kScanTile - 1) / kScanTile;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)std::min<uint64_t>(ntiles, (uint64_t)ix->scan_grid));
     cfg.blockDim = dim3(kScanThreads);
+    cfg.dynamicSmemBytes = smem;
     cfg.stream = st;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
@@ -2974,7 +3059,7 @@ int self_scan_impl(kssdgpu_index *ix, unsigned flags, unsigned long long *oc, un
         cfg.attrs = attr;
         cfg.numAttrs = 1;
     }
-    CUDA_TRY(cudaLaunchKernelEx(&cfg, k_self_scan, (const uint32_t *)ix->gbeg, ix->u, (const uint64_t *)ix->post,
+    CUDA_TRY(cudaLaunchKernelEx(&cfg, kern, (const uint32_t *)ix->gbeg, ix->u, (const uint64_t *)ix->post,
                                 (flags & KSSDGPU_IGNORECONFLICT) ? 1 : 0, oc, oo));
     count_launch();
     CUDA_TRY(cudaGetLastError());
@@ -3018,7 +3103,8 @@ int self_dense_impl(kssdgpu_index *ix, unsigned long long *oc, unsigned long lon
     }
     const uint32_t npad = (uint32_t)dense_npad(ix);
     const size_t sort_smem = kDenseMaxGroup * sizeof(unsigned long long);
-    const size_t rows_smem = sort_smem + 5 * (size_t)npad;
+    const uint32_t nbuf = (uint32_t)std::max<size_t>(1, std::min<size_t>(8, kDenseRowBudget / (5 * (size_t)npad)));
+    const size_t rows_smem = kDenseRowsOffset + (size_t)nbuf * 5 * npad;
     CUDA_TRY(cudaFuncSetAttribute(k_dense_alleles, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sort_smem));
     CUDA_TRY(cudaFuncSetAttribute(k_dense_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rows_smem));
     CUDA_TRY(ix->d_list.ensure(S));
@@ -3057,8 +3143,8 @@ int self_dense_impl(kssdgpu_index *ix, unsigned long long *oc, unsigned long lon
         CUDA_TRY(cudaMemsetAsync(ix->d_a.p + (size_t)alleles * npad, 0, (size_t)(kpad - alleles) * npad, st));
         CUDA_TRY(cudaMemsetAsync(ix->d_f.p + (size_t)alleles * 4 * npad, 0, (size_t)(kpad - alleles) * 4 * npad, st));
     }
-    k_dense_rows<<<grid, kDenseThreads, rows_smem, st>>>(ix->d_list.p, S, ix->d_allele.p, ix->post, npad, ix->d_a.p,
-                                                         ix->d_f.p);
+    k_dense_rows<<<grid, kDenseThreads, rows_smem, st>>>(ix->d_list.p, S, ix->d_allele.p, ix->post, npad, nbuf,
+                                                         ix->d_a.p, ix->d_f.p);
     count_launch();
     CUDA_TRY(cudaGetLastError());
     // 3. D = A' F^T on the tensor cores (both operands MN-major)
