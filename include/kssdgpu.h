@@ -163,17 +163,20 @@ int kssdgpu_sync(kssdgpu_index_t *idx, void *stream);
  * kssdgpu_count_block_dev; flags select unique/ignoreconflict, lower selects the
  * triangle form): shared-memory accumulator rows (where a row fits) and global rows
  * in key-range chunks of 1,024 / 4,096 / 16,384 entries are each timed with CUDA
- * events (best of three after a warm-up) on the legacy stream, and the fastest
- * becomes the index's setting for later batched counts without KSSDGPU_SMEM_ACC /
- * KSSDGPU_GLOBAL_ACC.  Synchronizes the device; the outputs hold the block's counters
- * afterwards.  Without a call: global rows in 4,096-entry chunks.  No reference
- * counterpart (the CPU path has no tunables).
+ * events (best of three after a warm-up) on the legacy stream, then the best of them
+ * with the index's context membership filter toggled (a filter of about 8 bits per
+ * context, at most 64 MB, built with the index: a query context it rules out needs no
+ * table probe); the fastest becomes the index's setting for later batched counts
+ * without KSSDGPU_SMEM_ACC / KSSDGPU_GLOBAL_ACC.  Synchronizes the device; the outputs
+ * hold the block's counters afterwards.  Without a call: global rows in 4,096-entry
+ * chunks, filter on.  No reference counterpart (the CPU path has no tunables).
  */
 typedef struct kssdgpu_count_tuning {
     int smem_rows;        /* 1: shared-memory accumulator rows; 0: global rows in chunks */
     uint32_t chunk_keys;  /* entries per key-range chunk of the global-row mode */
     int candidates;       /* settings timed */
     float ms;             /* the chosen setting's time on the block */
+    int filter;           /* 1: query contexts pass the index's membership filter before a table probe */
 } kssdgpu_count_tuning_t;
 int kssdgpu_count_tune(kssdgpu_index_t *idx, const uint64_t *d_qry_keys, const uint64_t *d_qry_offs, int nq,
                        int qry_gid_offset, int lower, unsigned flags, kssdgpu_ctx_mut2_t *d_ctx,

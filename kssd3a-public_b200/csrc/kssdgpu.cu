@@ -253,6 +253,8 @@ struct CountParams {
                                    // chunks [prefix[q], prefix[q+1]) (nq + 1 words), may be null
     uint32_t chunk_keys;           // entries per chunk in that mode
     int *err;
+    const uint4 *bloom;            // membership filter of the index's contexts, may be null
+    uint32_t bloom_mask;           // its 32-byte blocks - 1
 };
 
 
@@ -384,6 +386,52 @@ __device__ __forceinline__ void process_entry(const CountParams &P, uint64_t i, 
     credit_context<LOWER, UNIQUE>(P, i, s, payload, single, qgid, objmask, acc, uacc);
 }
 
+// Membership filter of an index's contexts: 32-byte blocks (a power of two of them, at
+// most 64 MB so that it stays in L2 beside the working set), each context setting 4
+// bits in one 16-byte half of its block.  A query context whose bits are not all set
+// is not in the index and needs no table probe: for queries of other genomes most
+// contexts are absent (a 10,000 x 20,000 block: 88%), and each absent context would
+// otherwise cost a random table line from HBM.
+struct BloomBits {
+    uint32_t block, half, p[4];
+};
+__device__ __forceinline__ BloomBits bloom_bits(unsigned long long ctx, uint32_t mask)
+{
+    const unsigned long long h = mix64(mix64(ctx) ^ 0x243F6A8885A308D3ull);
+    BloomBits b;
+    b.block = (uint32_t)h & mask;
+    b.half = (uint32_t)(h >> 32) & 1u;
+    b.p[0] = (uint32_t)(h >> 33) & 127u;
+    b.p[1] = (uint32_t)(h >> 40) & 127u;
+    b.p[2] = (uint32_t)(h >> 47) & 127u;
+    b.p[3] = (uint32_t)(h >> 54) & 127u;
+    return b;
+}
+
+__device__ __forceinline__ bool bloom_may_hold(const uint4 *__restrict__ f, uint32_t mask, unsigned long long ctx)
+{
+    const BloomBits b = bloom_bits(ctx, mask);
+    const uint4 w = __ldg(f + 2 * (size_t)b.block + b.half);
+    const uint32_t words[4] = {w.x, w.y, w.z, w.w};
+    bool all = true;
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+        all &= (words[b.p[i] >> 5] >> (b.p[i] & 31)) & 1u;
+    return all;
+}
+
+__global__ void k_bloom_insert(const unsigned long long *__restrict__ gkey, uint64_t u, uint32_t mask,
+                               uint32_t *__restrict__ f)
+{
+    for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < u; g += (uint64_t)gridDim.x * blockDim.x) {
+        const BloomBits b = bloom_bits(gkey[g], mask);
+        uint32_t *half = f + (2 * (size_t)b.block + b.half) * 4;
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+            atomicOr(half + (b.p[i] >> 5), 1u << (b.p[i] & 31));
+    }
+}
+
 // Entries b + t, b + t + T, ... of one query, kProbeBatch per thread at a time:
 // their first hash slots are loaded back to back so several random lines are in
 // flight per thread, then each probe is resolved (rarely a second slot) and credited.
@@ -412,7 +460,8 @@ __device__ __forceinline__ void process_query(const CountParams &P, uint64_t b, 
                 const uint64_t prev = i > b ? __ldg(P.qkeys + i - 1) : 0;
                 if (prev > key)
                     atomicMax(P.err, (int)kDevUnsorted);  // a sample's keys must ascend (comblco order)
-                if (!(i > b && (prev >> P.obj_bits) == ctx[u])) {
+                if (!(i > b && (prev >> P.obj_bits) == ctx[u]) &&
+                    (!P.bloom || bloom_may_hold(P.bloom, P.bloom_mask, ctx[u]))) {
                     int run = 1;
                     while (i + run < e && (__ldg(P.qkeys + i + run) >> P.obj_bits) == ctx[u])
                         ++run;
@@ -1235,8 +1284,16 @@ __global__ void k_self_conflict_groups(const unsigned long long *__restrict__ li
 // --ignoreconflict skips reference (lower-gid) runs of several objects.
 
 constexpr uint32_t kScanThreads = 256;
-constexpr uint32_t kScanPerThread = 16;
-constexpr uint32_t kScanTile = kScanThreads * kScanPerThread;  // groups per tile (16 KB of gbeg)
+#ifndef KSSD_SCAN_PER_THREAD
+#define KSSD_SCAN_PER_THREAD 8
+#endif
+#ifndef KSSD_SCAN_CACHE
+#define KSSD_SCAN_CACHE 1
+#endif
+constexpr uint32_t kScanPerThread = KSSD_SCAN_PER_THREAD;
+constexpr uint32_t kScanTile = kScanThreads * kScanPerThread;  // groups per tile (4 B of gbeg each)
+constexpr uint32_t kCellCache = KSSD_SCAN_CACHE ? 2048 : 1;     // counter cache slots per CTA (pairs mode)
+constexpr uint32_t kCellEmpty = 0xFFFFFFFFu;
 constexpr uint32_t kScanLaneMax = 32;                          // larger groups: the whole CTA
 
 __device__ __forceinline__ void credit_lower(unsigned long long *__restrict__ oc, unsigned long long *__restrict__ oo,
@@ -1316,7 +1373,35 @@ __device__ __forceinline__ void join_group_cta(const uint64_t *__restrict__ post
 struct ScanSmem {
     unsigned long long queue[kScanTile];  // groups of 2..kScanLaneMax from the front, larger from the back
     uint32_t prefix[kScanTile];
+    // pairs mode: a per-CTA cache of counter cells (claimed by the first credit that hashes
+    // to a free slot, never evicted, added into the triangle when the CTA ends): hot cells
+    // -- pairs of close genomes take a credit from most of their contexts -- add in shared
+    // memory instead of contending in L2
+    uint32_t cell[kCellCache];
+    uint32_t nc[kCellCache], m2[kCellCache], dobj[kCellCache], sect[kCellCache];  // 32-bit: native shared atomics
 };
+
+// One credit through the CTA's cell cache (cells below 2^32 only; the caller checks).
+__device__ __forceinline__ void credit_cached(ScanSmem &S, unsigned long long *__restrict__ oc,
+                                              unsigned long long *__restrict__ oo, uint32_t qg, uint32_t rg, int d)
+{
+    const uint32_t cell = (uint32_t)lower_cell(qg, rg);
+    const uint32_t slot = kCellCache > 1 ? (cell * 2654435761u) >> (32 - 11) : 0u;  // kCellCache = 2^11
+    uint32_t key = S.cell[slot];
+    if (key == kCellEmpty)
+        key = atomicCAS(&S.cell[slot], kCellEmpty, cell) == kCellEmpty ? cell : S.cell[slot];
+    if (key == cell) {
+        atomicAdd(&S.nc[slot], 1u);
+        if (d) {
+            atomicAdd(&S.dobj[slot], 1u);
+            atomicAdd(&S.sect[slot], (uint32_t)d);
+            if (d > 1)
+                atomicAdd(&S.m2[slot], 1u);
+        }
+    } else {
+        credit_lower(oc, oo, qg, rg, d);
+    }
+}
 
 // The pair (i < j) of rank t among the k(k-1)/2 pairs of a group: j(j-1)/2 <= t.
 __device__ __forceinline__ void pair_of_rank(uint32_t t, uint32_t &i, uint32_t &j)
@@ -1337,9 +1422,9 @@ __device__ __forceinline__ void pair_of_rank(uint32_t t, uint32_t &i, uint32_t &
 // with conflicts every thread walks whole groups (run cross products).  Groups of more
 // than kScanLaneMax postings are taken by the whole CTA.
 template <bool PAIRS>
-__global__ void __launch_bounds__(kScanThreads) k_self_scan(const uint32_t *__restrict__ gbeg, uint64_t u,
+__global__ void __launch_bounds__(kScanThreads, 3) k_self_scan(const uint32_t *__restrict__ gbeg, uint64_t u,
                                                             const uint64_t *__restrict__ post, int ignoreconflict,
-                                                            unsigned long long *__restrict__ oc,
+                                                            bool use_cache, unsigned long long *__restrict__ oc,
                                                             unsigned long long *__restrict__ oo)
 {
     extern __shared__ __align__(16) unsigned char scan_smem[];
@@ -1348,6 +1433,13 @@ __global__ void __launch_bounds__(kScanThreads) k_self_scan(const uint32_t *__re
     __shared__ typename Scan::TempStorage scan_tmp;
     const uint64_t ntiles = (u + kScanTile - 1) / kScanTile;
     bool waited = false;
+    const bool cache = PAIRS && KSSD_SCAN_CACHE && use_cache;
+    if (cache) {
+        for (uint32_t i = threadIdx.x; i < kCellCache; i += kScanThreads) {
+            S.cell[i] = kCellEmpty;
+            S.nc[i] = S.m2[i] = S.dobj[i] = S.sect[i] = 0;
+        }
+    }
     for (uint64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
         const uint64_t base = t * kScanTile;
         uint32_t beg[kScanPerThread], cnt[kScanPerThread];
@@ -1422,7 +1514,10 @@ __global__ void __launch_bounds__(kScanThreads) k_self_scan(const uint32_t *__re
                     pair_of_rank(pr - S.prefix[q], i, j);
                     const uint64_t pi = __ldg(post + (uint32_t)item + i), pj = __ldg(post + (uint32_t)item + j);
                     const int d = min(kMinInit, dna_pop((uint32_t)pi ^ (uint32_t)pj));
-                    credit_lower(oc, oo, (uint32_t)(pj >> 32), (uint32_t)(pi >> 32), d);
+                    if (cache)
+                        credit_cached(S, oc, oo, (uint32_t)(pj >> 32), (uint32_t)(pi >> 32), d);
+                    else
+                        credit_lower(oc, oo, (uint32_t)(pj >> 32), (uint32_t)(pi >> 32), d);
                 }
             }
         } else {
@@ -1436,6 +1531,18 @@ __global__ void __launch_bounds__(kScanThreads) k_self_scan(const uint32_t *__re
             join_group_cta(post, (uint32_t)item, (uint32_t)(item >> 32), ignoreconflict, oc, oo);
         }
         __syncthreads();  // the queue and the scan storage are reused by the next tile
+    }
+    if (cache && waited) {
+        // the cached cells into the triangle (only CTAs that took a tile waited for the fill
+        // and can hold claimed cells)
+        for (uint32_t i = threadIdx.x; i < kCellCache; i += kScanThreads) {
+            const uint32_t cell = S.cell[i];
+            if (cell == kCellEmpty)
+                continue;
+            atomicAdd(oc + cell, (unsigned long long)S.nc[i] | ((unsigned long long)S.m2[i] << 32));
+            if (S.dobj[i])
+                atomicAdd(oo + cell, (unsigned long long)S.dobj[i] | ((unsigned long long)S.sect[i] << 32));
+        }
     }
 }
 
@@ -1805,6 +1912,9 @@ struct kssdgpu_index {
     unsigned long long *gkey = nullptr;
     uint32_t *gbeg = nullptr;
     Slot *table = nullptr;
+    uint4 *bloom = nullptr;                 // membership filter of the contexts (see bloom_may_hold)
+    uint32_t bloom_mask = 0;
+    bool count_filter = true;               // batched counts consult the filter (kssdgpu_count_tune may turn it off)
     uint32_t mask = 0;
     int *err = nullptr;
     unsigned int *work = nullptr;
@@ -1903,6 +2013,18 @@ int finish_build(kssdgpu_index *ix, uint32_t *head, unsigned long long *ctx_of, 
     k_table_insert<<<grid_for(ix->u), 256, 0, st>>>(ix->gkey, ix->gbeg, ix->u, ix->post, ix->table, ix->mask,
                                                      ix->err);
     count_launch();
+    // the contexts' membership filter: about 8 bits per context, at most 64 MB
+    if (ix->u) {
+        uint64_t blocks = 1;
+        while (blocks * 256 < ix->u * 8 && blocks * 32 < (64ull << 20))
+            blocks <<= 1;
+        ix->bloom_mask = (uint32_t)(blocks - 1);
+        CUDA_TRY(cudaMalloc(&ix->bloom, blocks * 32));
+        CUDA_TRY(cudaMemsetAsync(ix->bloom, 0, blocks * 32, st));
+        k_bloom_insert<<<grid_for(ix->u), 256, 0, st>>>(ix->gkey, ix->u, ix->bloom_mask,
+                                                         reinterpret_cast<uint32_t *>(ix->bloom));
+        count_launch();
+    }
     CUDA_TRY(cudaStreamSynchronize(st));
     cudaFree(tmp);
     cudaFree(gidx);
@@ -2105,6 +2227,8 @@ int count_dev_impl(kssdgpu_index *ix, const uint64_t *d_keys, const uint64_t *d_
     P.work = ix->work;
     P.order = d_order;
     P.err = ix->err;
+    P.bloom = ix->count_filter ? ix->bloom : nullptr;
+    P.bloom_mask = ix->bloom_mask;
     const size_t cells = (size_t)nq * ix->nref;
     if (nq == 0)
         return KSSDGPU_OK;
@@ -3059,8 +3183,13 @@ int self_scan_impl(kssdgpu_index *ix, unsigned flags, unsigned long long *oc, un
         cfg.attrs = attr;
         cfg.numAttrs = 1;
     }
+    // The cell cache holds 32-bit cell numbers (triangles of at most 92,681 genomes) and
+    // pays where the counters outgrow L2: 20,000 genomes 2.78 ms per step with it vs 2.98
+    // without; with the counters in L2 its shared-memory adds cost more than they save
+    // (2,000 genomes: 0.19 vs 0.15 ms).
+    const bool use_cache = cells < (size_t)kCellEmpty && cells * 16 > (size_t)ix->l2_bytes;
     CUDA_TRY(cudaLaunchKernelEx(&cfg, kern, (const uint32_t *)ix->gbeg, ix->u, (const uint64_t *)ix->post,
-                                (flags & KSSDGPU_IGNORECONFLICT) ? 1 : 0, oc, oo));
+                                (flags & KSSDGPU_IGNORECONFLICT) ? 1 : 0, use_cache, oc, oo));
     count_launch();
     CUDA_TRY(cudaGetLastError());
     return KSSDGPU_OK;
@@ -3472,6 +3601,7 @@ void kssdgpu_index_free(kssdgpu_index_t *ix)
     cudaFree(ix->gkey);
     cudaFree(ix->gbeg);
     cudaFree(ix->table);
+    cudaFree(ix->bloom);
     cudaFree(ix->err);
     cudaFree(ix->work);
     ix->s_keys.release();
@@ -3666,6 +3796,45 @@ int kssdgpu_count_tune(kssdgpu_index_t *ix, const uint64_t *d_qry_keys, const ui
             pick = c;
         }
     }
+    // then the best setting without (or with) the membership filter
+    bool filter = ix->count_filter;
+    if (rc == KSSDGPU_OK && ix->bloom) {
+        ix->count_smem = pick.smem;
+        ix->count_chunk_keys = pick.chunk;
+        ix->count_filter = !filter;
+        const unsigned f = base | (pick.smem ? KSSDGPU_SMEM_ACC : KSSDGPU_GLOBAL_ACC);
+        float t_min = 1e30f;
+        for (int r = 0; r < 4 && rc == KSSDGPU_OK; ++r) {
+            ce = cudaEventRecord(ev0, 0);
+            if (ce == cudaSuccess) {
+                rc = count_dev_impl(ix, d_qry_keys, d_qry_offs, nq, qry_gid_offset, lower != 0, f,
+                                    reinterpret_cast<unsigned long long *>(d_ctx),
+                                    reinterpret_cast<unsigned long long *>(d_obj),
+                                    reinterpret_cast<unsigned long long *>(d_uctx),
+                                    reinterpret_cast<unsigned long long *>(d_uobj), nullptr, nullptr, 0);
+                if (rc)
+                    break;
+            }
+            if (ce == cudaSuccess) ce = cudaEventRecord(ev1, 0);
+            if (ce == cudaSuccess) ce = cudaEventSynchronize(ev1);
+            float ms = 0;
+            if (ce == cudaSuccess) ce = cudaEventElapsedTime(&ms, ev0, ev1);
+            if (ce != cudaSuccess) {
+                rc = fail(KSSDGPU_ERR_CUDA, cudaGetErrorString(ce));
+                break;
+            }
+            if (r > 0)
+                t_min = std::min(t_min, ms);
+        }
+        if (rc == KSSDGPU_OK) {
+            ++tried;
+            if (t_min < best) {
+                best = t_min;
+                filter = !filter;
+            }
+        }
+        ix->count_filter = filter;
+    }
     cudaEventDestroy(ev0);
     cudaEventDestroy(ev1);
     if (rc) {
@@ -3682,6 +3851,7 @@ int kssdgpu_count_tune(kssdgpu_index_t *ix, const uint64_t *d_qry_keys, const ui
         out->chunk_keys = pick.chunk;
         out->candidates = tried;
         out->ms = best;
+        out->filter = ix->count_filter && ix->bloom ? 1 : 0;
     }
     return check_dev_err(ix, 0);
 }
@@ -3764,6 +3934,8 @@ int kssdgpu_count_block_noalloc(kssdgpu_index_t *ix, const uint64_t *d_qry_keys,
     P.out_uobj = reinterpret_cast<unsigned long long *>(d_uobj);
     P.work = scr;
     P.err = ix->err;
+    P.bloom = ix->count_filter ? ix->bloom : nullptr;
+    P.bloom_mask = ix->bloom_mask;
     P.order = use_smem ? reinterpret_cast<const int *>(scr + kNoallocHeaderWords) : nullptr;
     P.chunk_prefix = use_smem ? nullptr : scr + kNoallocHeaderWords - 1;
     P.chunk_keys = ix->count_chunk_keys;

@@ -105,7 +105,8 @@ class _ServerConfig(C.Structure):
 
 
 class _CountTuning(C.Structure):
-    _fields_ = [("smem_rows", C.c_int), ("chunk_keys", C.c_uint32), ("candidates", C.c_int), ("ms", C.c_float)]
+    _fields_ = [("smem_rows", C.c_int), ("chunk_keys", C.c_uint32), ("candidates", C.c_int), ("ms", C.c_float),
+                ("filter", C.c_int)]
 
 
 class _ServerStats(C.Structure):

@@ -596,3 +596,17 @@ def test_self_dense_join_wide_objects_and_conflicts():
         idx.self_lower(kssdgpu.SELF_DENSE)
     assert e.value.code == 1
     assert idx.self_choice()[0] == kssdgpu.PATH_SCAN
+
+
+def test_self_scan_with_counters_beyond_l2():
+    """6,000 small genomes: the packed triangle (18M cells, 288 MB) outgrows L2, so the scan
+    join adds through its per-CTA cell cache; the counters still equal the oracle's."""
+    sk = kssdgpu.synth(n_samples=6000, n_clusters=600, len_median=8e4, len_min=5e4, len_max=1.5e5,
+                       size_dist=kssdgpu.SIZE_LOGNORMAL, sub_lo=0.001, sub_hi=0.1, seed=71, sample_seed=71)
+    rec = oracle.build_index(sk.keys, sk.offs)
+    idx = kssdgpu.Index.from_records(rec, sk.n)
+    want = oracle.self_lower_all(rec, sk.keys, sk.offs)
+    got = idx.self_lower(kssdgpu.SELF_SCAN)
+    np.testing.assert_array_equal(got[0], want[0])
+    np.testing.assert_array_equal(got[1], want[1])
+    assert want[0][:, 0].sum() > 0
