@@ -408,10 +408,23 @@ __device__ __forceinline__ BloomBits bloom_bits(unsigned long long ctx, uint32_t
     return b;
 }
 
+// Filter loads ask L2 to keep their lines (evict_last), so that the streamed query
+// keys and the random table lines do not push the filter out of L2.
+__device__ __forceinline__ uint4 ld_keep_l2(const uint4 *p)
+{
+    uint4 r;
+    unsigned long long pol;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+    asm volatile("ld.global.nc.L2::cache_hint.v4.u32 {%0, %1, %2, %3}, [%4], %5;"
+                 : "=r"(r.x), "=r"(r.y), "=r"(r.z), "=r"(r.w)
+                 : "l"(p), "l"(pol));
+    return r;
+}
+
 __device__ __forceinline__ bool bloom_may_hold(const uint4 *__restrict__ f, uint32_t mask, unsigned long long ctx)
 {
     const BloomBits b = bloom_bits(ctx, mask);
-    const uint4 w = __ldg(f + 2 * (size_t)b.block + b.half);
+    const uint4 w = ld_keep_l2(f + 2 * (size_t)b.block + b.half);
     const uint32_t words[4] = {w.x, w.y, w.z, w.w};
     bool all = true;
 #pragma unroll

@@ -397,7 +397,9 @@ def test_count_autotuner_keeps_counts():
     do = torch.from_numpy(qry.offs.view(np.int64)).to(dev)
     outs = [torch.zeros(qry.n * ref.n, dtype=torch.int64, device=dev) for _ in range(4)]
     t = idx.count_tune(dk, do, qry.n, *outs, flags=kssdgpu.UNIQUE)
-    assert t["candidates"] == 4 and t["chunk_keys"] in (1024, 4096, 16384) and t["ms"] > 0
+    # 4 accumulator settings, then the best of them with the membership filter toggled
+    assert t["candidates"] == 5 and t["chunk_keys"] in (1024, 4096, 16384) and t["ms"] > 0
+    assert t["filter"] in (0, 1)
     for _ in range(2):
         got = [o.cpu().numpy().view(np.uint32).reshape(qry.n, ref.n, 2) for o in outs]
         for g, w in zip(got, want):
