@@ -504,6 +504,51 @@ def leg_dense(args, timer, dev, stream, peak_tc):
             "parity": {"dense_eq_scan": same}}
 
 
+def leg_cli_2k(args, sk):
+    """The drop-in CLI end to end on the headline workload: `kssd3a ani -p P -q DIR --format
+    matrix --values ani -o FILE` (indexed self full matrix, 36 MB of TSV) with bin/kssd3a and
+    with the reference CLI on the same sketch directory (index file present, warm page
+    cache): wall times and byte equality of the outputs."""
+    import hashlib
+    import shutil
+    import tempfile
+    import kssdgpu
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    if not oracle.ref_available():
+        return {"skipped": "reference build absent"}
+    ours = os.path.join(ROOT, "kssd3a-public_b200", "bin", "kssd3a")
+    root = tempfile.mkdtemp(prefix="kssd_cli2k_")
+    try:
+        d = os.path.join(root, "refs")
+        kssdgpu.write_sketch_dir(d, sk)
+        rec = oracle.build_index(sk.keys, sk.offs)
+        rec.tofile(os.path.join(d, "sortedcomb_ctxgid64obj32"))
+        oracle.unique_bits(rec).tofile(os.path.join(d, "sortedcomb_ctxgid64obj32.unique_bits"))
+        del rec
+        thr = str(os.cpu_count() or 8)
+        env = {k: v for k, v in os.environ.items() if not k.startswith("KSSD3A_")}
+        out = {}
+        for name, binary in (("ours", ours), ("reference", oracle.REF_BIN)):
+            dst = os.path.join(root, name + ".tsv")
+            argv = [binary, "ani", "-p", thr, "-q", d, "--format", "matrix", "--values", "ani", "-o", dst]
+            subprocess.run(argv, check=True, capture_output=True, env=env)  # warm page cache and context
+            ts = []
+            for _ in range(3):
+                t0 = time.perf_counter()
+                subprocess.run(argv, check=True, capture_output=True, env=env)
+                ts.append(time.perf_counter() - t0)
+            out[name] = {"wall_s_median_of_3": float(np.median(ts)),
+                         "sha256": hashlib.sha256(open(dst, "rb").read()).hexdigest(),
+                         "bytes": os.path.getsize(dst)}
+        return {"command": "kssd3a ani -p P -q DIR --format matrix --values ani -o FILE", "genomes": sk.n,
+                "threads": int(thr), "ours": out["ours"], "reference": out["reference"],
+                "bytes_equal": out["ours"]["sha256"] == out["reference"]["sha256"],
+                "speedup": out["reference"]["wall_s_median_of_3"] / out["ours"]["wall_s_median_of_3"]}
+    finally:
+        shutil.rmtree(root, ignore_errors=True)
+
+
 def leg_config1(args):
     """64 genomes of 1 Mbp (8 clusters x 8 members, 0.5-5% substitutions, 0.1% indels) as
     FASTA, sketched by the reference's own sketcher; bin/kssd3a and the reference CLI on
@@ -878,6 +923,7 @@ def run_ours(args, rank, world, local_rank):
                               "pool": pool, "server": srvf, "rates": res}
         ns_idx.close()
         extra["dense_one_species"] = leg_dense(args, timer, dev, stream, peak_tc)
+        extra["cli_2k"] = leg_cli_2k(args, sk)
         extra["config1_fasta"] = leg_config1(args)
 
     if rank == 0:
