@@ -340,3 +340,126 @@ void orc_self_votes(const void *records, size_t len, const uint64_t *keys, const
         }
     }
 }
+
+/* ---------------------------------------------------------------- sketching (FASTA/FASTQ)
+ * The reference's sketch of one genome (src/command_sketch.c:3913-3949 per record, then
+ * :4156-4188 sort + dedup and src/kssdlib_sort.c:388-406 conflict removal), restated
+ * with a portable bit-extract.  Masks: src/sketch_rearrange.c:7-39 and
+ * src/sketch_rearrange.h:109-122 (coden pattern). */
+
+void orc_sketch_masks(int coden_len, int klen, int hclen, int holen, uint64_t *ctxmask, uint64_t *tupmask,
+                      int *obj_bits)
+{
+    uint64_t cm = 0;
+    int ctx_bits;
+    if (coden_len > 0) {
+        /* per coden: 4 context bits over 2 object bits (0b111100), the 11th coden one
+         * final 4-bit context group */
+        for (int i = 0; i < coden_len; ++i) {
+            cm = (cm << 6) | 0x3Cu;
+            if (i == 10) {
+                cm = (cm << 4) | 0xFu;
+                break;
+            }
+        }
+        ctx_bits = 4 * coden_len;
+    } else {
+        const int iolen = klen - 2 * (hclen + holen);
+        const uint64_t hc = hclen ? (~0ull >> (64 - 2 * hclen)) : 0;
+        cm = (hc << (2 * (holen + hclen + iolen))) | (hc << (2 * holen));
+        ctx_bits = 4 * hclen;
+    }
+    *ctxmask = cm;
+    *tupmask = klen ? (~0ull >> (64 - 2 * klen)) : 0;
+    *obj_bits = 2 * klen - ctx_bits;
+}
+
+static uint64_t orc_pext(uint64_t x, uint64_t mask)
+{
+    uint64_t r = 0;
+    int k = 0;
+    for (int b = 0; b < 64; ++b)
+        if ((mask >> b) & 1u)
+            r |= ((x >> b) & 1u) << k++;
+    return r;
+}
+
+/* SplitMix64 finalizer (Steele, Lea, Flood 2014), the sketch's context hash (src/kssdlib_hash.h:16-21) */
+static uint64_t orc_splitmix64(uint64_t x)
+{
+    x += 0x9e3779b97f4a7c15ull;
+    x = (x ^ (x >> 30)) * 0xbf58476d1ce4e5b9ull;
+    x = (x ^ (x >> 27)) * 0x94d049bb133111ebull;
+    return x ^ (x >> 31);
+}
+
+static int orc_base(unsigned char c)
+{
+    switch (c) {
+    case 'A': case 'a': return 0;
+    case 'C': case 'c': return 1;
+    case 'G': case 'g': return 2;
+    case 'T': case 't': return 3;
+    default: return -1;
+    }
+}
+
+static int u64_cmp(const void *a, const void *b)
+{
+    const uint64_t x = *(const uint64_t *)a, y = *(const uint64_t *)b;
+    return x < y ? -1 : x > y;
+}
+
+size_t orc_sketch_records(const char *seq, const uint64_t *rec_offs, int nrec, int klen, uint64_t ctxmask,
+                          uint64_t tupmask, int obj_bits, uint32_t filter, int conflict, uint64_t *out, size_t cap)
+{
+    size_t n = 0;
+    const int len_mv = 2 * klen - 2;
+    const uint64_t objmask = tupmask & ~ctxmask;
+    for (int r = 0; r < nrec; ++r) {
+        const uint64_t b = rec_offs[r], e = rec_offs[r + 1];
+        if (e - b < (uint64_t)klen)
+            continue;
+        uint64_t tuple = 0, crv = 0;
+        int run = 0;
+        for (uint64_t p = b; p < e; ++p) {
+            const int v = orc_base((unsigned char)seq[p]);
+            if (v < 0) {
+                run = 0;
+                tuple = crv = 0;
+                continue;
+            }
+            tuple = (tuple << 2) | (uint64_t)v;
+            crv = (crv >> 2) | ((uint64_t)(v ^ 3) << len_mv);
+            if (++run < klen)
+                continue;
+            const uint64_t tc = tuple & ctxmask, rc = crv & ctxmask;
+            const int fwd = tc < rc;
+            const uint64_t uctx = fwd ? tc : rc;
+            if ((uint32_t)orc_splitmix64(uctx) > filter)
+                continue;
+            const uint64_t ut = (fwd ? tuple : crv) & tupmask;
+            if (n == cap)
+                return (size_t)-1;
+            out[n++] = (orc_pext(ut, ctxmask) << obj_bits) | orc_pext(ut, objmask);
+        }
+    }
+    qsort(out, n, sizeof(uint64_t), u64_cmp);
+    size_t m = 0;
+    for (size_t i = 0; i < n; ++i)
+        if (i == 0 || out[i] != out[m - 1])
+            out[m++] = out[i];
+    if (conflict)
+        return m;
+    /* drop every context that holds more than one object */
+    size_t w = 0;
+    for (size_t i = 0; i < m;) {
+        size_t j = i + 1;
+        while (j < m && (out[j] >> obj_bits) == (out[i] >> obj_bits))
+            ++j;
+        if (j - i == 1)
+            out[w++] = out[i];
+        i = j;
+    }
+    return w;
+}

@@ -52,6 +52,16 @@ void orc_pair_features(const uint64_t *a, size_t n, const uint64_t *b, size_t m,
 int orc_dna_popcount(uint32_t x);
 void orc_self_votes(const void *records, size_t len, const uint64_t *keys, const uint64_t *offs, int nsamples,
                     int obj_bits, uint32_t max_freq, uint32_t step, uint32_t *votes, uint32_t *first);
+/* Sketch parameters -> context mask, k-mer mask, object width (src/sketch_rearrange.c:7-39). */
+void orc_sketch_masks(int coden_len, int klen, int hclen, int holen, uint64_t *ctxmask, uint64_t *tupmask,
+                      int *obj_bits);
+/* One genome's sketch from its records' sequence bytes seq[rec_offs[r]..rec_offs[r+1]): canonical
+ * context per k-mer, kept when (uint32) splitmix64(ctx) <= filter, ctx << obj_bits | obj, sorted,
+ * deduplicated, and without conflict the contexts holding several objects removed
+ * (src/command_sketch.c:3913-3949, :4156-4188; src/kssdlib_sort.c:388-406).
+ * Returns the key count, or (size_t)-1 when cap is too small. */
+size_t orc_sketch_records(const char *seq, const uint64_t *rec_offs, int nrec, int klen, uint64_t ctxmask,
+                          uint64_t tupmask, int obj_bits, uint32_t filter, int conflict, uint64_t *out, size_t cap);
 
 #ifdef __cplusplus
 }

@@ -47,6 +47,11 @@ def oracle_lib() -> C.CDLL:
         lib.orc_dna_popcount.argtypes = [C.c_uint32]
         lib.orc_self_votes.argtypes = [_vp, C.c_size_t, _u64p, _u64p, C.c_int, C.c_int, C.c_uint32, C.c_uint32,
                                        _u32p, _u32p]
+        lib.orc_sketch_masks.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_uint64),
+                                         C.POINTER(C.c_uint64), C.POINTER(C.c_int)]
+        lib.orc_sketch_records.argtypes = [C.c_char_p, _u64p, C.c_int, C.c_int, C.c_uint64, C.c_uint64, C.c_int,
+                                           C.c_uint32, C.c_int, _vp, C.c_size_t]
+        lib.orc_sketch_records.restype = C.c_size_t
         _orc = lib
     return _orc
 
@@ -214,3 +219,22 @@ def self_votes(rec, keys, offs, obj_bits=20, max_freq=256, step=1):
     oracle_lib().orc_self_votes(_rptr(rec), len(rec), _qk(keys), np.ascontiguousarray(offs, np.uint64), n, obj_bits,
                                 max_freq, step, votes, first)
     return votes[:cells], first[:cells]
+
+
+def sketch_masks(coden_len=11, klen=32, hclen=0, holen=0):
+    """(context mask, k-mer mask, object bits) of the sketch parameters."""
+    cm, tm, ob = C.c_uint64(), C.c_uint64(), C.c_int()
+    oracle_lib().orc_sketch_masks(coden_len, klen, hclen, holen, C.byref(cm), C.byref(tm), C.byref(ob))
+    return cm.value, tm.value, ob.value
+
+
+def sketch_records(records, klen=32, coden_len=11, hclen=0, holen=0, drfold=8, conflict=False):
+    """One sample's sketch keys from its records' sequence bytes (the reference's sketcher,
+    restated in liboracle)."""
+    cm, tm, ob = sketch_masks(coden_len, klen, hclen, holen)
+    seq = b"".join(records)
+    offs = np.cumsum([0] + [len(r) for r in records]).astype(np.uint64)
+    out = np.zeros(max(len(seq), 1), dtype=np.uint64)
+    n = oracle_lib().orc_sketch_records(seq, offs, len(records), klen, cm, tm, ob, 0xFFFFFFFF >> drfold,
+                                        1 if conflict else 0, out.ctypes.data, len(out))
+    return out[:n].copy()

@@ -43,3 +43,38 @@ def mutate_from(rng, base, rate, obj_bits=OBJ_BITS):
                 o ^= int(rng.integers(1, 4)) << (2 * b)
         out.append((c, o))
     return out
+
+
+def read_fastx_records(path):
+    """Sequence records of a FASTA/FASTQ file (gzip or plain) with the reference's parser
+    rules (klib kseq as vendored by the reference): a record starts at '>' or '@';
+    sequence lines run to the next line starting with '>', '+' or '@'; line ends are
+    '\\n' with one trailing '\\r' removed; empty lines are skipped; FASTQ quality lines
+    are consumed by length."""
+    import gzip
+    with open(path, "rb") as f:
+        data = f.read()
+    if data[:2] == b"\x1f\x8b":
+        data = gzip.decompress(data)
+    lines = data.split(b"\n")
+    if lines and lines[-1] == b"":
+        lines.pop()
+    recs, i = [], 0
+    while i < len(lines) and not lines[i][:1] in (b">", b"@"):
+        i += 1
+    while i < len(lines):
+        i += 1  # header
+        seq = []
+        while i < len(lines) and lines[i][:1] not in (b">", b"+", b"@"):
+            if lines[i]:
+                seq.append(lines[i][:-1] if lines[i].endswith(b"\r") else lines[i])
+            i += 1
+        s = b"".join(seq)
+        if i < len(lines) and lines[i][:1] == b"+":
+            i += 1
+            q = 0
+            while i < len(lines) and q < len(s):
+                q += len(lines[i].rstrip(b"\r"))
+                i += 1
+        recs.append(s)
+    return recs
