@@ -105,6 +105,17 @@ int kssdgpu_index_info(const kssdgpu_index_t *idx, uint64_t *records, uint64_t *
                        int *nref, int *obj_bits);
 
 /*
+ * Rebuilds the index's context membership filter (built with the index) with
+ * key-range stripes of at most max_stripe_bytes each (0: the default of 16 MB; at most
+ * 256 stripes; at least 8 bits per context) and reports the stripe count and the
+ * filter's bytes (either may be NULL).  A batched count with the filter on walks the
+ * query keys stripe by stripe when there are several, so that the stripe in use stays
+ * in L2.  Synchronizes the device; not to be called while a server runs on the
+ * index.  No reference counterpart (the CPU path has no filter).
+ */
+int kssdgpu_index_filter(kssdgpu_index_t *idx, uint64_t max_stripe_bytes, int *stripes, uint64_t *bytes);
+
+/*
  * Copies the index back as reference-layout records (12-byte packed, sorted) and
  * its unique-object bitset ((n+7)/8 bytes; src/command_sketch.c:856-914).  Either
  * output may be NULL.
@@ -161,15 +172,18 @@ int kssdgpu_sync(kssdgpu_index_t *idx, void *stream);
 /*
  * Autotune the batched count of this index on a representative block (arguments as
  * kssdgpu_count_block_dev; flags select unique/ignoreconflict, lower selects the
- * triangle form): shared-memory accumulator rows (where a row fits) and global rows
- * in key-range chunks of 1,024 / 4,096 / 16,384 entries are each timed with CUDA
- * events (best of three after a warm-up) on the legacy stream, then the best of them
- * with the index's context membership filter toggled (a filter of about 8 bits per
- * context, at most 64 MB, built with the index: a query context it rules out needs no
- * table probe); the fastest becomes the index's setting for later batched counts
- * without KSSDGPU_SMEM_ACC / KSSDGPU_GLOBAL_ACC.  Synchronizes the device; the outputs
- * hold the block's counters afterwards.  Without a call: global rows in 4,096-entry
- * chunks, filter on.  No reference counterpart (the CPU path has no tunables).
+ * triangle form): shared-memory accumulator rows (where a row fits), global rows in
+ * key-range chunks of 1,024 / 4,096 / 16,384 entries and (with several filter stripes)
+ * global rows stripe by stripe are each timed with CUDA events (best of three after a
+ * warm-up) on the legacy stream, then the best of them
+ * with the index's context membership filter toggled (at least 8 bits per context
+ * in key-range stripes of at most 16 MB, built with the index: a query context it
+ * rules out needs no table probe; with several stripes and global rows the count runs
+ * stripe by stripe, see kssdgpu_index_filter); the fastest becomes the index's
+ * setting for later batched counts without KSSDGPU_SMEM_ACC / KSSDGPU_GLOBAL_ACC.
+ * Synchronizes the device; the outputs hold the block's counters afterwards.  Without
+ * a call: global rows (in 4,096-entry chunks, or stripe by stripe), filter on.  No
+ * reference counterpart (the CPU path has no tunables).
  */
 typedef struct kssdgpu_count_tuning {
     int smem_rows;        /* 1: shared-memory accumulator rows; 0: global rows in chunks */
@@ -177,6 +191,7 @@ typedef struct kssdgpu_count_tuning {
     int candidates;       /* settings timed */
     float ms;             /* the chosen setting's time on the block */
     int filter;           /* 1: query contexts pass the index's membership filter before a table probe */
+    int striped;          /* 1: global rows run stripe by stripe over the filter's key-range stripes */
 } kssdgpu_count_tuning_t;
 int kssdgpu_count_tune(kssdgpu_index_t *idx, const uint64_t *d_qry_keys, const uint64_t *d_qry_offs, int nq,
                        int qry_gid_offset, int lower, unsigned flags, kssdgpu_ctx_mut2_t *d_ctx,
@@ -394,6 +409,39 @@ int kssdgpu_server_stats(kssdgpu_server_t *srv, kssdgpu_server_stats_t *out);
 int kssdgpu_server_reset_stats(kssdgpu_server_t *srv);
 /* Finishes queued and running batches, then frees the server (not the index). */
 void kssdgpu_server_destroy(kssdgpu_server_t *srv);
+
+/*
+ * Sketching of sequence (FASTA/FASTQ records) on the device, as the reference's
+ * `kssd3a sketch` (src/command_sketch.c:3913-3949, :4156-4188; src/kssdlib_sort.c:388-406):
+ * every k-mer of a record made of A/C/G/T (either case) takes its canonical context
+ * (the smaller of the forward and reverse-complement contexts, the reverse on a tie),
+ * is kept when the 32-bit SplitMix64 hash of the context is <= UINT32_MAX >> drfold, and
+ * becomes ctx << obj_bits | obj; per sample the keys are sorted and deduplicated and,
+ * unless conflict is set, contexts holding more than one object are dropped.
+ */
+typedef struct kssdgpu_sketch_params {
+    int klen;       /* k-mer length, 1..32 (32 with the 11-coden pattern) */
+    int coden_len;  /* > 0: the coden context pattern of this many codens; 0: hclen/holen layout */
+    int hclen;      /* half context length (coden_len == 0) */
+    int holen;      /* half outer object length (coden_len == 0) */
+    int drfold;     /* k-mer space downsampling 1/2^drfold, 0..32 */
+    int conflict;   /* 1: keep contexts that hold several objects */
+} kssdgpu_sketch_params_t;
+/* Context mask, k-mer mask and object width of the parameters (src/sketch_rearrange.c:7-39). */
+int kssdgpu_sketch_masks(const kssdgpu_sketch_params_t *p, uint64_t *ctxmask, uint64_t *tupmask, int *obj_bits);
+/* The sketch method id stored in lcofiles.stat (src/command_sketch.h:49-52, :769-772). */
+uint32_t kssdgpu_sketch_hash_id(const kssdgpu_sketch_params_t *p);
+/*
+ * seq: the records' sequence bytes back to back (< 4 GiB per call); record r is
+ * seq[rec_offs[r] .. rec_offs[r+1]) (rec_offs[0] = 0, rec_offs[nrec] = seq_len); sample s
+ * is records samp_recs[s] .. samp_recs[s+1] (samp_recs[0] = 0, samp_recs[nsamples] = nrec).
+ * Writes sample s's keys to keys[offs[s] .. offs[s+1]) (offs: nsamples + 1 words).  With
+ * fewer than offs[nsamples] keys of room the call returns KSSDGPU_ERR_CAPACITY with offs
+ * filled.  Runs on the current device; synchronous.
+ */
+int kssdgpu_sketch(const char *seq, uint64_t seq_len, const uint64_t *rec_offs, uint64_t nrec,
+                   const uint64_t *samp_recs, int nsamples, const kssdgpu_sketch_params_t *p, uint64_t *keys,
+                   uint64_t keys_cap, uint64_t *offs);
 
 /* Number of kernels launched by this library so far in this process. */
 uint64_t kssdgpu_launch_count(void);

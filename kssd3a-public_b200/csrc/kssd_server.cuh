@@ -244,6 +244,8 @@ int server_launch(kssdgpu_server *s, ServerSlot &sl)
     P.err = s->ix->err;
     P.bloom = s->ix->count_filter ? s->ix->bloom : nullptr;
     P.bloom_mask = s->ix->bloom_mask;
+    P.bloom_stripes = s->ix->bloom_stripes;
+    P.bloom_bounds = s->ix->bloom_bounds;
     int rc = (s->cfg.flags & KSSDGPU_UNIQUE) ? launch_batched<false, true, false>(s->ix, P, 0, sl.st)
                                              : launch_batched<false, false, false>(s->ix, P, 0, sl.st);
     if (rc)

@@ -13,6 +13,7 @@
 #include "kssd_dev.cuh"
 
 #include <cub/cub.cuh>
+#include <cub/device/device_segmented_sort.cuh>
 
 #include <algorithm>
 #include <atomic>
@@ -229,6 +230,17 @@ struct WorkItem {
     uint64_t b, e;
 };
 constexpr uint64_t kChunkKeys = 4096;
+// filter stripes: at most this many bytes each (one stripe stays in L2 beside the
+// streamed keys and the table lines), at most kMaxStripes of them
+#ifndef KSSD_STRIPE_MB
+#define KSSD_STRIPE_MB 16
+#endif
+constexpr uint64_t kStripeBytes = (uint64_t)KSSD_STRIPE_MB << 20;
+constexpr int kMaxStripes = 256;
+// stripe-major work: chunks of at least kStripeChunk entries, at most kStripeItemsMax
+// chunks beyond one per (stripe, query)
+constexpr uint64_t kStripeChunk = 256;
+constexpr uint64_t kStripeItemsMax = 1ull << 20;
 
 struct CountParams {
     const Slot *table;
@@ -254,7 +266,10 @@ struct CountParams {
     uint32_t chunk_keys;           // entries per chunk in that mode
     int *err;
     const uint4 *bloom;            // membership filter of the index's contexts, may be null
-    uint32_t bloom_mask;           // its 32-byte blocks - 1
+    uint32_t bloom_mask;           // 32-byte blocks of one stripe of it - 1
+    int bloom_stripes;             // its key-range stripes (a power of two)
+    const unsigned long long *bloom_bounds;  // first context of each stripe (stripes + 1 words)
+    const uint32_t *nitems_dev;    // stripe-major mode: count of P.items (built on the device), may be null
 };
 
 
@@ -386,12 +401,16 @@ __device__ __forceinline__ void process_entry(const CountParams &P, uint64_t i, 
     credit_context<LOWER, UNIQUE>(P, i, s, payload, single, qgid, objmask, acc, uacc);
 }
 
-// Membership filter of an index's contexts: 32-byte blocks (a power of two of them, at
-// most 64 MB so that it stays in L2 beside the working set), each context setting 4
-// bits in one 16-byte half of its block.  A query context whose bits are not all set
-// is not in the index and needs no table probe: for queries of other genomes most
-// contexts are absent (a 10,000 x 20,000 block: 88%), and each absent context would
-// otherwise cost a random table line from HBM.
+// Membership filter of an index's contexts, cut into key-range stripes: stripe s holds
+// the contexts of [bounds[s], bounds[s+1]) (quantiles of the sorted contexts, so every
+// stripe holds U / S of them) in a power of two of 32-byte blocks, at most 16 MB per
+// stripe and at least 8 bits per context; each context sets 4 bits in one 16-byte half
+// of its block.  A query context whose bits are not all set is not in the index and
+// needs no table probe: for queries of other genomes most contexts are absent (a
+// 10,000 x 20,000 block: 88%), and each absent context would otherwise cost a random
+// table line from HBM.  A filter read at random as a whole does not stay in L2 once it
+// is tens of MB; a count that walks the query keys stripe by stripe keeps only the
+// current stripe's part hot (k_count_striped).
 struct BloomBits {
     uint32_t block, half, p[4];
 };
@@ -408,6 +427,17 @@ __device__ __forceinline__ BloomBits bloom_bits(unsigned long long ctx, uint32_t
     return b;
 }
 
+// stripe of a context: the largest s < S with bounds[s] <= ctx (bounds[0] = 0)
+__device__ __forceinline__ uint32_t stripe_of(const unsigned long long *__restrict__ bounds, int S,
+                                              unsigned long long ctx)
+{
+    uint32_t lo = 0;
+    for (uint32_t step = (uint32_t)S >> 1; step; step >>= 1)
+        if (__ldg(bounds + lo + step) <= ctx)
+            lo += step;
+    return lo;
+}
+
 // Filter loads ask L2 to keep their lines (evict_last), so that the streamed query
 // keys and the random table lines do not push the filter out of L2.
 __device__ __forceinline__ uint4 ld_keep_l2(const uint4 *p)
@@ -421,27 +451,88 @@ __device__ __forceinline__ uint4 ld_keep_l2(const uint4 *p)
     return r;
 }
 
+// f: the context's stripe of the filter
 __device__ __forceinline__ bool bloom_may_hold(const uint4 *__restrict__ f, uint32_t mask, unsigned long long ctx)
 {
     const BloomBits b = bloom_bits(ctx, mask);
     const uint4 w = ld_keep_l2(f + 2 * (size_t)b.block + b.half);
-    const uint32_t words[4] = {w.x, w.y, w.z, w.w};
     bool all = true;
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
-        all &= (words[b.p[i] >> 5] >> (b.p[i] & 31)) & 1u;
+    for (int i = 0; i < 4; ++i) {
+        const uint32_t p = b.p[i];  // word by selects (a dynamically indexed array would live in local memory)
+        const uint32_t word = (p & 64) ? ((p & 32) ? w.w : w.z) : ((p & 32) ? w.y : w.x);
+        all &= (word >> (p & 31)) & 1u;
+    }
     return all;
 }
 
-__global__ void k_bloom_insert(const unsigned long long *__restrict__ gkey, uint64_t u, uint32_t mask,
-                               uint32_t *__restrict__ f)
+// The filter as one kernel sees it: a whole filter whose stripe is found per context,
+// or (stripes == 1) the one stripe the caller works in.
+struct FilterView {
+    const uint4 *f;
+    uint32_t mask;
+    int stripes;
+    const unsigned long long *bounds;
+    __device__ __forceinline__ bool may_hold(unsigned long long ctx) const
+    {
+        if (!f)
+            return true;
+        const uint4 *base = f;
+        if (stripes > 1)
+            base += 2 * ((size_t)mask + 1) * stripe_of(bounds, stripes, ctx);
+        return bloom_may_hold(base, mask, ctx);
+    }
+};
+
+__global__ void k_bloom_insert(const unsigned long long *__restrict__ gkey, uint64_t u, uint32_t mask, int stripes,
+                               const unsigned long long *__restrict__ bounds, uint32_t *__restrict__ f)
 {
     for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < u; g += (uint64_t)gridDim.x * blockDim.x) {
-        const BloomBits b = bloom_bits(gkey[g], mask);
-        uint32_t *half = f + (2 * (size_t)b.block + b.half) * 4;
+        const unsigned long long ctx = gkey[g];
+        const BloomBits b = bloom_bits(ctx, mask);
+        const size_t blk = (size_t)(stripes > 1 ? stripe_of(bounds, stripes, ctx) : 0) * ((size_t)mask + 1) + b.block;
+        uint32_t *half = f + (2 * blk + b.half) * 4;
 #pragma unroll
         for (int i = 0; i < 4; ++i)
             atomicOr(half + (b.p[i] >> 5), 1u << (b.p[i] & 31));
+    }
+}
+
+// bounds[s] = first context of stripe s: 0, then gkey[s * U / S], then ~0 (S + 1 words)
+__global__ void k_stripe_bounds(const unsigned long long *__restrict__ gkey, uint64_t u, int stripes,
+                                unsigned long long *__restrict__ bounds)
+{
+    for (int s = threadIdx.x; s <= stripes; s += blockDim.x)
+        bounds[s] = s == 0 ? 0ull : s == stripes ? ~0ull : gkey[(uint64_t)s * u / (uint64_t)stripes];
+}
+
+// spos[q * (S + 1) + s]: the first entry of query q whose context is >= bounds[s]
+// (absolute offsets; s = 0 and s = S are the query's own bounds).  Keys ascend within
+// a query, so each is one binary search.
+__global__ void k_stripe_pos(const uint64_t *__restrict__ qkeys, const uint64_t *__restrict__ qoffs, int nq,
+                             int stripes, const unsigned long long *__restrict__ bounds, int obj_bits,
+                             uint64_t *__restrict__ spos)
+{
+    const uint64_t base = qoffs[0];
+    const uint64_t n = (uint64_t)nq * (stripes + 1);
+    for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < n; t += (uint64_t)gridDim.x * blockDim.x) {
+        const int q = (int)(t / (uint64_t)(stripes + 1)), s = (int)(t % (uint64_t)(stripes + 1));
+        uint64_t lo = qoffs[q], hi = qoffs[q + 1];
+        if (s == stripes) {
+            spos[t] = hi;
+            continue;
+        }
+        if (s > 0) {
+            const unsigned long long bound = bounds[s];
+            while (lo < hi) {
+                const uint64_t mid = lo + ((hi - lo) >> 1);
+                if ((__ldg(qkeys + (mid - base)) >> obj_bits) < bound)
+                    lo = mid + 1;
+                else
+                    hi = mid;
+            }
+        }
+        spos[t] = lo;
     }
 }
 
@@ -453,12 +544,13 @@ __global__ void k_bloom_insert(const unsigned long long *__restrict__ gkey, uint
 #endif
 constexpr int kProbeBatch = KSSD_PROBE_BATCH;
 
+// Threads t0, t0 + T, ... of the caller's group take the entries; fv is the filter.
 template <bool LOWER, bool UNIQUE, class Acc>
 __device__ __forceinline__ void process_query(const CountParams &P, uint64_t b, uint64_t e, uint64_t cb, uint64_t ce,
-                                              int qgid, uint64_t objmask, const Acc &acc, const Acc &uacc)
+                                              int qgid, uint64_t objmask, const Acc &acc, const Acc &uacc,
+                                              const FilterView &fv, uint64_t t0, uint64_t T)
 {
-    const uint64_t T = blockDim.x;
-    for (uint64_t base = cb + threadIdx.x; base < ce; base += T * kProbeBatch) {
+    for (uint64_t base = cb + t0; base < ce; base += T * kProbeBatch) {
         unsigned long long ctx[kProbeBatch];
         uint32_t slot[kProbeBatch];
         int s[kProbeBatch];
@@ -473,8 +565,7 @@ __device__ __forceinline__ void process_query(const CountParams &P, uint64_t b, 
                 const uint64_t prev = i > b ? __ldg(P.qkeys + i - 1) : 0;
                 if (prev > key)
                     atomicMax(P.err, (int)kDevUnsorted);  // a sample's keys must ascend (comblco order)
-                if (!(i > b && (prev >> P.obj_bits) == ctx[u]) &&
-                    (!P.bloom || bloom_may_hold(P.bloom, P.bloom_mask, ctx[u]))) {
+                if (!(i > b && (prev >> P.obj_bits) == ctx[u]) && fv.may_hold(ctx[u])) {
                     int run = 1;
                     while (i + run < e && (__ldg(P.qkeys + i + run) >> P.obj_bits) == ctx[u])
                         ++run;
@@ -524,6 +615,7 @@ __global__ void __launch_bounds__(512) k_count_batched(CountParams P)
     const uint64_t objmask = (P.obj_bits >= 64) ? ~0ull : ((1ull << P.obj_bits) - 1);
     const uint64_t base = P.qoffs[0];
     const int nref = P.nref;
+    const FilterView fv{P.bloom, P.bloom_mask, P.bloom_stripes, P.bloom_bounds};
     for (;;) {
         if (threadIdx.x == 0)
             s_item = (int)atomicAdd(P.work, 1u);
@@ -562,7 +654,7 @@ __global__ void __launch_bounds__(512) k_count_batched(CountParams P)
         if (SMEM) {
             const SmemAcc acc{row0, row0 + nref, row0 + 2 * nref, row0 + 3 * nref};
             const SmemAcc uacc{row1, row1 + nref, row1 + 2 * nref, row1 + 3 * nref};
-            process_query<LOWER, UNIQUE>(P, b, e, b, e, qgid, objmask, acc, uacc);
+            process_query<LOWER, UNIQUE>(P, b, e, b, e, qgid, objmask, acc, uacc, fv, threadIdx.x, blockDim.x);
         } else {
             const GlobalAcc acc{P.out_ctx + row, P.out_obj + row};
             const GlobalAcc uacc{UNIQUE ? P.out_uctx + row : nullptr, UNIQUE ? P.out_uobj + row : nullptr};
@@ -574,7 +666,7 @@ __global__ void __launch_bounds__(512) k_count_batched(CountParams P)
                 cb = b + (uint64_t)(it - (int)P.chunk_prefix[q]) * P.chunk_keys;
                 ce = min(e, cb + (uint64_t)P.chunk_keys);
             }
-            process_query<LOWER, UNIQUE>(P, b, e, cb, ce, qgid, objmask, acc, uacc);
+            process_query<LOWER, UNIQUE>(P, b, e, cb, ce, qgid, objmask, acc, uacc, fv, threadIdx.x, blockDim.x);
         }
         __syncthreads();
         if (SMEM) {
@@ -589,6 +681,94 @@ __global__ void __launch_bounds__(512) k_count_batched(CountParams P)
             }
         }
         __syncthreads();
+    }
+}
+
+// Stripe-major global-row kernel: the work items are chunks of one query's entries
+// whose contexts fall in one filter stripe, listed stripe by stripe (k_stripe_expand),
+// so that at any time the SMs probe one stripe of the filter and it stays in L2 while
+// the query keys stream past.  Each warp takes kStripeGrab chunks at a time from the
+// work counter; its lanes stride over a chunk's entries.  Counters go to the zeroed
+// global rows with atomics, as in the chunked mode.
+constexpr uint32_t kStripeGrab = 2;
+
+template <bool LOWER, bool UNIQUE>
+__global__ void __launch_bounds__(512) k_count_striped(CountParams P)
+{
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t objmask = (P.obj_bits >= 64) ? ~0ull : ((1ull << P.obj_bits) - 1);
+    const uint64_t base = P.qoffs[0];
+    const uint32_t nitems = *P.nitems_dev;
+    const size_t stripe_words = 2 * ((size_t)P.bloom_mask + 1);  // uint4 per stripe
+    for (;;) {
+        uint32_t it0 = 0;
+        if (lane == 0)
+            it0 = atomicAdd(P.work, kStripeGrab);
+        it0 = __shfl_sync(0xFFFFFFFFu, it0, 0);
+        if (it0 >= nitems)
+            break;
+        const uint32_t it1 = min(nitems, it0 + kStripeGrab);
+        for (uint32_t it = it0; it < it1; ++it) {
+            const WorkItem w = P.items[it];
+            const int q = (int)w.q;
+            const uint64_t b = P.qoffs[q] - base, e = P.qoffs[q + 1] - base;
+            const size_t row = (size_t)q * P.nref;
+            const GlobalAcc acc{P.out_ctx + row, P.out_obj + row};
+            const GlobalAcc uacc{UNIQUE ? P.out_uctx + row : nullptr, UNIQUE ? P.out_uobj + row : nullptr};
+            const FilterView fv{P.bloom + stripe_words * w.pad, P.bloom_mask, 1, nullptr};
+            process_query<LOWER, UNIQUE>(P, b, e, w.b, w.e, P.qgid_offset + q, objmask, acc, uacc, fv, lane, 32);
+        }
+    }
+}
+
+// chunk size of the stripe-major items: kStripeChunk entries, more for blocks so large
+// that the chunks would exceed kStripeItemsMax
+__device__ __forceinline__ uint64_t stripe_chunk(const uint64_t *__restrict__ qoffs, int nq)
+{
+    const uint64_t total = qoffs[nq] - qoffs[0];
+    return max(kStripeChunk, (total + kStripeItemsMax - 1) / kStripeItemsMax);
+}
+
+// cnt[s * nq + q]: chunks of query q's entries in stripe s (cnt[S * nq] = 0, so that an
+// exclusive scan leaves the chunk total there).  Offsets that decrease come only from
+// keys out of order: the block is refused (err) and the range counts nothing, so the
+// chunks never outgrow their buffer.
+__global__ void k_stripe_counts(const uint64_t *__restrict__ spos, const uint64_t *__restrict__ qoffs, int nq,
+                                int stripes, uint32_t *__restrict__ cnt, int *__restrict__ err)
+{
+    const uint64_t ck = stripe_chunk(qoffs, nq);
+    const uint64_t n = (uint64_t)stripes * nq;
+    for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t <= n; t += (uint64_t)gridDim.x * blockDim.x) {
+        if (t == n) {
+            cnt[n] = 0;
+            continue;
+        }
+        const int st = (int)(t / (uint64_t)nq), q = (int)(t % (uint64_t)nq);
+        const uint64_t *sp = spos + (size_t)q * (stripes + 1) + st;
+        if (sp[1] < sp[0]) {
+            atomicMax(err, (int)kDevUnsorted);
+            cnt[t] = 0;
+            continue;
+        }
+        cnt[t] = (uint32_t)((sp[1] - sp[0] + ck - 1) / ck);
+    }
+}
+
+// the chunks themselves, at their scanned offsets: {query, stripe, begin, end} with
+// offsets relative to the block's first entry
+__global__ void k_stripe_expand(const uint64_t *__restrict__ spos, const uint64_t *__restrict__ qoffs, int nq,
+                                int stripes, const uint32_t *__restrict__ pre, WorkItem *__restrict__ items)
+{
+    const uint64_t ck = stripe_chunk(qoffs, nq);
+    const uint64_t base = qoffs[0];
+    const uint64_t n = (uint64_t)stripes * nq;
+    for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < n; t += (uint64_t)gridDim.x * blockDim.x) {
+        const int st = (int)(t / (uint64_t)nq), q = (int)(t % (uint64_t)nq);
+        const uint64_t *sp = spos + (size_t)q * (stripes + 1) + st;
+        const uint64_t b = sp[0] - base, e = sp[1] - base;
+        uint32_t o = pre[t];
+        for (uint64_t c = b; c < e && o < pre[t + 1]; c += ck)
+            items[o++] = WorkItem{(uint32_t)q, (uint32_t)st, c, min(e, c + ck)};
     }
 }
 
@@ -1903,6 +2083,179 @@ struct DevBuf {
     }
 };
 
+// ------------------------------------------------------------------ sketching (FASTA/FASTQ)
+// The reference's sketch of sequence (src/command_sketch.c:3913-3949): every k-mer of a
+// record whose bases are all A/C/G/T (either case) takes the canonical context (the
+// smaller of the forward and reverse-complement contexts under the context mask, the
+// reverse on a tie), is kept when the 32-bit hash of that context is <= UINT32_MAX >>
+// drfold, and becomes ctx << obj_bits | obj by extracting the mask's bits of the k-mer
+// on the chosen strand.  Per sample: sort, dedup, and without conflict mode the contexts
+// holding several objects dropped (src/command_sketch.c:4156-4188, src/kssdlib_sort.c:388-406).
+struct SketchGeom {
+    unsigned long long ctxmask, tupmask;
+    int klen, obj_bits;
+    uint32_t filter;
+};
+
+// SplitMix64 finalizer (Steele, Lea, Flood 2014): the sketch's context hash (the
+// reference's mix64 in src/kssdlib_hash.h, which the sketch files' hash_id names)
+__host__ __device__ __forceinline__ unsigned long long splitmix64(unsigned long long x)
+{
+    x += 0x9e3779b97f4a7c15ull;
+    x = (x ^ (x >> 30)) * 0xbf58476d1ce4e5b9ull;
+    x = (x ^ (x >> 27)) * 0x94d049bb133111ebull;
+    return x ^ (x >> 31);
+}
+
+// bits of x under mask m, packed from the low end (BMI2 pext)
+__device__ __forceinline__ unsigned long long extract_bits(unsigned long long x, unsigned long long m)
+{
+    unsigned long long r = 0;
+    int k = 0;
+    while (m) {
+        const int b = __ffsll((long long)m) - 1;
+        r |= ((x >> b) & 1ull) << k++;
+        m &= m - 1;
+    }
+    return r;
+}
+
+// 2-bit code of a base, -1 for anything but A/C/G/T in either case
+__device__ __forceinline__ int base_code(unsigned char c)
+{
+    switch (c | 0x20) {
+    case 'a': return 0;
+    case 'c': return 1;
+    case 'g': return 2;
+    case 't': return 3;
+    default: return -1;
+    }
+}
+
+constexpr int kSketchThreads = 256;
+constexpr int kSketchSpan = 64;                               // k-mer end positions per thread
+constexpr int kSketchTile = kSketchThreads * kSketchSpan;     // bytes per CTA
+constexpr int kSketchHalo = 32;                               // >= klen - 1 bytes before the tile
+
+// largest i in [0, n) with a[i] <= v (a[0] <= v)
+__device__ __forceinline__ uint64_t last_le(const uint64_t *__restrict__ a, uint64_t n, uint64_t v)
+{
+    uint64_t lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const uint64_t mid = (lo + hi + 1) >> 1;
+        if (__ldg(a + mid) <= v)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
+// Pass 1 (WRITE = false): kept k-mers per thread (counts) and per sample; pass 2: the
+// keys, each thread's at out[pos[thread] ...] (byte order, so grouped by sample).
+// Records rec_offs[r]..rec_offs[r+1] of seq; sample s = records samp_recs[s]..samp_recs[s+1].
+template <bool WRITE>
+__global__ void __launch_bounds__(kSketchThreads) k_sketch_scan(
+    const unsigned char *__restrict__ seq, uint64_t n, const uint64_t *__restrict__ rec_offs, uint64_t nrec,
+    const uint64_t *__restrict__ samp_recs, int nsamples, SketchGeom g, uint32_t *__restrict__ counts,
+    uint32_t *__restrict__ samp_counts, const uint32_t *__restrict__ pos, unsigned long long *__restrict__ out)
+{
+    __shared__ unsigned char tile[kSketchHalo + kSketchTile];
+    const uint64_t t0 = (uint64_t)blockIdx.x * kSketchTile;
+    // stage the tile and its halo (coalesced bytes; the tile start is 32-byte aligned)
+    for (int i = threadIdx.x; i < kSketchHalo + kSketchTile; i += kSketchThreads) {
+        const int64_t p = (int64_t)t0 - kSketchHalo + i;
+        tile[i] = (p >= 0 && (uint64_t)p < n) ? seq[p] : (unsigned char)'N';
+    }
+    __syncthreads();
+    const uint64_t gt = (uint64_t)blockIdx.x * kSketchThreads + threadIdx.x;
+    const uint64_t p0 = gt * kSketchSpan;
+    uint32_t kept = 0;
+    if (p0 < n && nrec) {
+        const uint64_t p1 = min(n, p0 + kSketchSpan);
+        const int len_mv = 2 * g.klen - 2;
+        uint64_t r = last_le(rec_offs, nrec + 1, p0);   // record holding p0 (or the last empty one before)
+        uint64_t rs = __ldg(rec_offs + r), re = r < nrec ? __ldg(rec_offs + r + 1) : rs;
+        uint64_t p = p0 >= rs + (uint64_t)(g.klen - 1) ? p0 - (g.klen - 1) : rs;
+        unsigned long long tuple = 0, crv = 0;
+        int run = 0;
+        uint32_t wi = 0;
+        const uint32_t wbase = WRITE ? pos[gt] : 0;
+        for (; p < p1; ++p) {
+            while (p >= re && r < nrec) {  // next record: the k-mer state starts over
+                ++r;
+                rs = re;
+                re = r < nrec ? __ldg(rec_offs + r + 1) : rs;
+                run = 0;
+                tuple = crv = 0;
+            }
+            if (r >= nrec)
+                break;
+            const int v = base_code(tile[kSketchHalo + (int64_t)(p - t0)]);
+            if (v < 0) {
+                run = 0;
+                tuple = crv = 0;
+                continue;
+            }
+            tuple = (tuple << 2) | (unsigned long long)v;
+            crv = (crv >> 2) | ((unsigned long long)(v ^ 3) << len_mv);
+            if (++run < g.klen || p < p0)
+                continue;
+            const unsigned long long tc = tuple & g.ctxmask, rc = crv & g.ctxmask;
+            const bool fwd = tc < rc;
+            const unsigned long long uctx = fwd ? tc : rc;
+            if ((uint32_t)splitmix64(uctx) > g.filter)
+                continue;
+            if (WRITE) {
+                const unsigned long long ut = (fwd ? tuple : crv) & g.tupmask;
+                out[wbase + wi++] = (extract_bits(ut, g.ctxmask) << g.obj_bits) |
+                                    extract_bits(ut, g.tupmask & ~g.ctxmask);
+            } else {
+                ++kept;
+                const int sm = (int)last_le(samp_recs, (uint64_t)nsamples + 1, r);
+                atomicAdd(samp_counts + min(sm, nsamples - 1), 1u);
+            }
+        }
+    }
+    if (!WRITE && gt < (n + kSketchSpan - 1) / kSketchSpan)
+        counts[gt] = kept;
+}
+
+// keep[i]: key i of its sample's sorted run is the first of its duplicates and (without
+// conflict mode) the only object of its context; kept keys counted per sample
+__global__ void k_sketch_keep(const unsigned long long *__restrict__ k, uint64_t n, const uint32_t *__restrict__ seg,
+                              int nsamples, int obj_bits, int conflict, uint8_t *__restrict__ keep,
+                              uint32_t *__restrict__ kept)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        // sample of key i: the last segment starting at or before i that is not empty
+        int lo = 0, hi = nsamples - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (seg[mid] <= i)
+                lo = mid;
+            else
+                hi = mid - 1;
+        }
+        const uint64_t b = seg[lo], e = seg[lo + 1];
+        const unsigned long long x = k[i];
+        bool ok = i == b || k[i - 1] != x;
+        if (ok && !conflict) {
+            const unsigned long long c = x >> obj_bits;
+            if (i > b && (k[i - 1] >> obj_bits) == c)
+                ok = false;
+            uint64_t j = i + 1;
+            while (ok && j < e && k[j] == x)
+                ++j;
+            if (ok && j < e && (k[j] >> obj_bits) == c)
+                ok = false;
+        }
+        keep[i] = ok ? 1 : 0;
+        if (ok)
+            atomicAdd(kept + lo, 1u);
+    }
+}
+
 int grid_for(uint64_t n, int block = 256)
 {
     uint64_t g = (n + block - 1) / block;
@@ -1926,7 +2279,13 @@ struct kssdgpu_index {
     uint32_t *gbeg = nullptr;
     Slot *table = nullptr;
     uint4 *bloom = nullptr;                 // membership filter of the contexts (see bloom_may_hold)
-    uint32_t bloom_mask = 0;
+    uint32_t bloom_mask = 0;                // 32-byte blocks per stripe - 1
+    int bloom_stripes = 1;                  // key-range stripes of the filter
+    unsigned long long *bloom_bounds = nullptr;  // first context of each stripe (stripes + 1 words)
+    DevBuf<uint64_t> s_spos;                // stripe-major count: entry offsets per (query, stripe)
+    DevBuf<uint32_t> s_scnt, s_spre;        // stripe-major count: chunks per (stripe, query), their offsets
+    DevBuf<WorkItem> s_sitems;              // stripe-major count: the chunks
+    bool count_striped = true;              // with several filter stripes, global rows run stripe-major
     bool count_filter = true;               // batched counts consult the filter (kssdgpu_count_tune may turn it off)
     uint32_t mask = 0;
     int *err = nullptr;
@@ -1995,6 +2354,45 @@ struct kssdgpu_index {
 
 namespace {
 
+
+// The contexts' membership filter: key-range stripes of U / S contexts each, a power of
+// two of 32-byte blocks per stripe giving at least 8 bits per context, S the smallest
+// power of two (at most kMaxStripes) that keeps a stripe within stripe_bytes.
+int build_filter(kssdgpu_index *ix, uint64_t stripe_bytes, cudaStream_t st)
+{
+    cudaFree(ix->bloom);
+    cudaFree(ix->bloom_bounds);
+    ix->bloom = nullptr;
+    ix->bloom_bounds = nullptr;
+    ix->bloom_stripes = 1;
+    ix->bloom_mask = 0;
+    if (!ix->u)
+        return KSSDGPU_OK;
+    int stripes = 1;
+    uint64_t blocks = 1;
+    for (;;) {
+        const uint64_t per = (ix->u + stripes - 1) / stripes;
+        blocks = 1;
+        while (blocks * 256 < per * 8)
+            blocks <<= 1;
+        if (blocks * 32 <= stripe_bytes || stripes >= kMaxStripes)
+            break;
+        stripes <<= 1;
+    }
+    const size_t fbytes = (size_t)stripes * blocks * 32;
+    CUDA_TRY(cudaMalloc(&ix->bloom, fbytes));
+    CUDA_TRY(cudaMalloc(&ix->bloom_bounds, (size_t)(stripes + 1) * sizeof(unsigned long long)));
+    ix->bloom_stripes = stripes;
+    ix->bloom_mask = (uint32_t)(blocks - 1);
+    CUDA_TRY(cudaMemsetAsync(ix->bloom, 0, fbytes, st));
+    k_stripe_bounds<<<1, 256, 0, st>>>(ix->gkey, ix->u, stripes, ix->bloom_bounds);
+    k_bloom_insert<<<grid_for(ix->u), 256, 0, st>>>(ix->gkey, ix->u, ix->bloom_mask, stripes, ix->bloom_bounds,
+                                                     reinterpret_cast<uint32_t *>(ix->bloom));
+    count_launch(2);
+    CUDA_TRY(cudaGetLastError());
+    return KSSDGPU_OK;
+}
+
 int finish_build(kssdgpu_index *ix, uint32_t *head, unsigned long long *ctx_of, cudaStream_t st)
 {
     const uint64_t n = ix->n;
@@ -2026,17 +2424,10 @@ int finish_build(kssdgpu_index *ix, uint32_t *head, unsigned long long *ctx_of, 
     k_table_insert<<<grid_for(ix->u), 256, 0, st>>>(ix->gkey, ix->gbeg, ix->u, ix->post, ix->table, ix->mask,
                                                      ix->err);
     count_launch();
-    // the contexts' membership filter: about 8 bits per context, at most 64 MB
     if (ix->u) {
-        uint64_t blocks = 1;
-        while (blocks * 256 < ix->u * 8 && blocks * 32 < (64ull << 20))
-            blocks <<= 1;
-        ix->bloom_mask = (uint32_t)(blocks - 1);
-        CUDA_TRY(cudaMalloc(&ix->bloom, blocks * 32));
-        CUDA_TRY(cudaMemsetAsync(ix->bloom, 0, blocks * 32, st));
-        k_bloom_insert<<<grid_for(ix->u), 256, 0, st>>>(ix->gkey, ix->u, ix->bloom_mask,
-                                                         reinterpret_cast<uint32_t *>(ix->bloom));
-        count_launch();
+        const int frc = build_filter(ix, kStripeBytes, st);
+        if (frc)
+            return frc;
     }
     CUDA_TRY(cudaStreamSynchronize(st));
     cudaFree(tmp);
@@ -2168,6 +2559,20 @@ int launch_batched(kssdgpu_index *ix, const CountParams &P, size_t smem, cudaStr
 }
 
 template <bool LOWER, bool UNIQUE>
+int launch_striped(kssdgpu_index *ix, const CountParams &P, cudaStream_t st)
+{
+    auto kern = k_count_striped<LOWER, UNIQUE>;
+    int per_sm = 0;
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 512, 0));
+    const int grid = ix->sms * std::max(per_sm, 1);  // persistent: the item count stays on the device
+    CUDA_TRY(cudaMemsetAsync(P.work, 0, sizeof(unsigned int), st));
+    kern<<<grid, 512, 0, st>>>(P);
+    count_launch();
+    CUDA_TRY(cudaGetLastError());
+    return KSSDGPU_OK;
+}
+
+template <bool LOWER, bool UNIQUE>
 int launch_plain(kssdgpu_index *ix, const CountParams &P, const std::vector<uint64_t> &sizes, cudaStream_t st)
 {
     for (int q = 0; q < P.nq; ++q) {
@@ -2242,6 +2647,8 @@ int count_dev_impl(kssdgpu_index *ix, const uint64_t *d_keys, const uint64_t *d_
     P.err = ix->err;
     P.bloom = ix->count_filter ? ix->bloom : nullptr;
     P.bloom_mask = ix->bloom_mask;
+    P.bloom_stripes = ix->bloom_stripes;
+    P.bloom_bounds = ix->bloom_bounds;
     const size_t cells = (size_t)nq * ix->nref;
     if (nq == 0)
         return KSSDGPU_OK;
@@ -2252,7 +2659,30 @@ int count_dev_impl(kssdgpu_index *ix, const uint64_t *d_keys, const uint64_t *d_
                                               std::to_string(ix->nref) + " references does not fit");
     const bool use_smem = uses_smem_row(ix, flags);
     P.chunk_keys = ix->count_chunk_keys;
-    if (!use_smem && d_items) {
+    // stripe-major items when the filter is on and striped (global rows)
+    const bool striped = !use_smem && !plain && !d_items && P.bloom && ix->count_striped && ix->bloom_stripes > 1 &&
+                         (uint64_t)nq * (uint64_t)ix->bloom_stripes < (1ull << 30);
+    if (striped) {
+        // per (query, stripe): entry offsets, chunk counts, their scan, the chunks
+        const int S = ix->bloom_stripes;
+        const size_t npos = (size_t)nq * (S + 1), nsq = (size_t)nq * S;
+        CUDA_TRY(ix->s_spos.ensure(npos));
+        CUDA_TRY(ix->s_scnt.ensure(nsq + 1));
+        CUDA_TRY(ix->s_spre.ensure(nsq + 1));
+        CUDA_TRY(ix->s_sitems.ensure(nsq + kStripeItemsMax));
+        size_t tb = 0;
+        CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, tb, ix->s_scnt.p, ix->s_spre.p, (int64_t)nsq + 1, st));
+        CUDA_TRY(ix->s_cubtmp.ensure(tb));
+        k_stripe_pos<<<grid_for(npos), 256, 0, st>>>(d_keys, d_offs, nq, S, ix->bloom_bounds, ix->obj_bits,
+                                                      ix->s_spos.p);
+        k_stripe_counts<<<grid_for(nsq + 1), 256, 0, st>>>(ix->s_spos.p, d_offs, nq, S, ix->s_scnt.p, ix->err);
+        CUDA_TRY(cub::DeviceScan::ExclusiveSum(ix->s_cubtmp.p, tb, ix->s_scnt.p, ix->s_spre.p, (int64_t)nsq + 1, st));
+        k_stripe_expand<<<grid_for(nsq), 256, 0, st>>>(ix->s_spos.p, d_offs, nq, S, ix->s_spre.p, ix->s_sitems.p);
+        count_launch(4);
+        P.items = ix->s_sitems.p;
+        P.nitems_dev = ix->s_spre.p + nsq;
+        P.order = nullptr;
+    } else if (!use_smem && d_items) {
         P.items = d_items;
         P.nitems = nitems;
     } else if (!use_smem && !plain && nq > 0) {
@@ -2289,6 +2719,11 @@ int count_dev_impl(kssdgpu_index *ix, const uint64_t *d_keys, const uint64_t *d_
             return launch_batched<true, false, true>(ix, P, smem, st);
         return unique ? launch_batched<false, true, true>(ix, P, smem, st)
                       : launch_batched<false, false, true>(ix, P, smem, st);
+    }
+    if (striped) {
+        if (lower)
+            return launch_striped<true, false>(ix, P, st);
+        return unique ? launch_striped<false, true>(ix, P, st) : launch_striped<false, false>(ix, P, st);
     }
     if (lower)
         return launch_batched<true, false, false>(ix, P, 0, st);
@@ -3486,6 +3921,187 @@ int kssdgpu_init(int device)
 
 uint64_t kssdgpu_launch_count(void) { return g_launches.load(); }
 
+int kssdgpu_sketch_masks(const kssdgpu_sketch_params_t *p, uint64_t *ctxmask, uint64_t *tupmask, int *obj_bits)
+{
+    if (!p || p->klen < 1 || p->klen > 32)
+        return fail(KSSDGPU_ERR_ARG, "sketch k-mer length must be 1..32");
+    uint64_t cm = 0;
+    int ctx_bits;
+    if (p->coden_len > 0) {
+        // per coden 4 context bits above 2 object bits; the 11th coden adds a last 4-bit
+        // context group (src/sketch_rearrange.h:109-122)
+        for (int i = 0; i < p->coden_len; ++i) {
+            cm = (cm << 6) | 0x3Cull;
+            if (i == 10) {
+                cm = (cm << 4) | 0xFull;
+                break;
+            }
+        }
+        ctx_bits = 4 * p->coden_len;
+    } else {
+        const int iolen = p->klen - 2 * (p->hclen + p->holen);
+        if (p->hclen < 0 || p->holen < 0 || iolen < 0)
+            return fail(KSSDGPU_ERR_ARG, "invalid context/object lengths for the k-mer length");
+        const uint64_t hc = p->hclen ? (~0ull >> (64 - 2 * p->hclen)) : 0;
+        cm = (hc << (2 * (p->holen + p->hclen + iolen))) | (hc << (2 * p->holen));
+        ctx_bits = 4 * p->hclen;
+    }
+    const uint64_t tm = ~0ull >> (64 - 2 * p->klen);
+    if ((cm & ~tm) || 2 * p->klen - ctx_bits < 0)
+        return fail(KSSDGPU_ERR_ARG, "context pattern wider than the k-mer");
+    if (ctxmask) *ctxmask = cm;
+    if (tupmask) *tupmask = tm;
+    if (obj_bits) *obj_bits = 2 * p->klen - ctx_bits;
+    return KSSDGPU_OK;
+}
+
+uint32_t kssdgpu_sketch_hash_id(const kssdgpu_sketch_params_t *p)
+{
+    // the sketch files' method id (src/command_sketch.h:49-52): hashes of the layout
+    // parameters and the filter, xor-folded with that of a fixed tag
+    if (!p)
+        return 0;
+    const uint64_t filter = 0xFFFFFFFFu >> (p->drfold < 0 ? 0 : p->drfold > 31 ? 31 : p->drfold);
+    uint64_t v[5];
+    if (p->coden_len > 0) {
+        v[0] = (uint64_t)p->coden_len; v[1] = 0; v[2] = 0;
+    } else {
+        v[0] = (uint64_t)p->hclen; v[1] = (uint64_t)p->holen; v[2] = (uint64_t)(p->klen - 2 * (p->hclen + p->holen));
+    }
+    v[3] = (uint64_t)p->drfold;
+    v[4] = filter;
+    uint32_t h = (uint32_t)splitmix64(31415926ull);
+    for (int i = 0; i < 5; ++i)
+        h ^= (uint32_t)splitmix64(v[i]);
+    return h;
+}
+
+int kssdgpu_sketch(const char *seq, uint64_t seq_len, const uint64_t *rec_offs, uint64_t nrec,
+                   const uint64_t *samp_recs, int nsamples, const kssdgpu_sketch_params_t *p, uint64_t *keys,
+                   uint64_t keys_cap, uint64_t *offs)
+{
+    if (!p || !offs || nsamples < 0 || (nrec && !rec_offs) || (nsamples && !samp_recs) || (seq_len && !seq))
+        return fail(KSSDGPU_ERR_ARG, "invalid sketch arguments");
+    uint64_t cm = 0, tm = 0;
+    int ob = 0;
+    int rc = kssdgpu_sketch_masks(p, &cm, &tm, &ob);
+    if (rc)
+        return rc;
+    if (p->drfold < 0 || p->drfold > 32)
+        return fail(KSSDGPU_ERR_ARG, "sketch drfold must be 0..32");
+    if (seq_len >= (1ull << 32))
+        return fail(KSSDGPU_ERR_CAPACITY, "sketch at most 4 GiB of sequence per call");
+    // records tile the sequence; samples tile the records
+    if (nrec && (rec_offs[0] != 0 || rec_offs[nrec] != seq_len))
+        return fail(KSSDGPU_ERR_ARG, "record offsets must run from 0 to the sequence length");
+    if (!nrec && seq_len)
+        return fail(KSSDGPU_ERR_ARG, "sequence bytes without records");
+    for (uint64_t r = 0; r < nrec; ++r)
+        if (rec_offs[r + 1] < rec_offs[r])
+            return fail(KSSDGPU_ERR_ARG, "record offsets must not decrease");
+    if (nsamples && (samp_recs[0] != 0 || samp_recs[nsamples] != nrec))
+        return fail(KSSDGPU_ERR_ARG, "sample record ranges must run from 0 to the record count");
+    for (int s = 0; s < nsamples; ++s)
+        if (samp_recs[s + 1] < samp_recs[s])
+            return fail(KSSDGPU_ERR_ARG, "sample record ranges must not decrease");
+    for (int s = 0; s <= nsamples; ++s)
+        offs[s] = 0;
+    if (!nsamples || !seq_len)
+        return KSSDGPU_OK;
+    SketchGeom g;
+    g.ctxmask = cm;
+    g.tupmask = tm;
+    g.klen = p->klen;
+    g.obj_bits = ob;
+    g.filter = p->drfold >= 32 ? 0u : (0xFFFFFFFFu >> p->drfold);
+    cudaStream_t st = nullptr;
+    const uint64_t nthreads = (seq_len + kSketchSpan - 1) / kSketchSpan;
+    const uint64_t nblocks = (seq_len + kSketchTile - 1) / kSketchTile;
+    // device buffers (freed on every path)
+    struct Bufs {
+        unsigned char *seq = nullptr;
+        uint64_t *rec = nullptr, *samp = nullptr;
+        uint32_t *counts = nullptr, *pos = nullptr, *scounts = nullptr, *seg = nullptr, *kept = nullptr;
+        unsigned long long *k0 = nullptr, *k1 = nullptr;
+        uint8_t *keep = nullptr;
+        void *tmp = nullptr;
+        int *nsel = nullptr;
+        ~Bufs()
+        {
+            cudaFree(seq); cudaFree(rec); cudaFree(samp); cudaFree(counts); cudaFree(pos); cudaFree(scounts);
+            cudaFree(seg); cudaFree(kept); cudaFree(k0); cudaFree(k1); cudaFree(keep); cudaFree(tmp); cudaFree(nsel);
+        }
+    } b;
+    CUDA_TRY(cudaMalloc(&b.seq, seq_len));
+    CUDA_TRY(cudaMalloc(&b.rec, (nrec + 1) * sizeof(uint64_t)));
+    CUDA_TRY(cudaMalloc(&b.samp, ((size_t)nsamples + 1) * sizeof(uint64_t)));
+    CUDA_TRY(cudaMalloc(&b.counts, nthreads * sizeof(uint32_t)));
+    CUDA_TRY(cudaMalloc(&b.pos, (nthreads + 1) * sizeof(uint32_t)));
+    CUDA_TRY(cudaMalloc(&b.scounts, ((size_t)nsamples + 1) * sizeof(uint32_t)));
+    CUDA_TRY(cudaMalloc(&b.seg, ((size_t)nsamples + 1) * sizeof(uint32_t)));
+    CUDA_TRY(cudaMalloc(&b.kept, ((size_t)nsamples + 1) * sizeof(uint32_t)));
+    CUDA_TRY(cudaMemcpyAsync(b.seq, seq, seq_len, cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaMemcpyAsync(b.rec, rec_offs, (nrec + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaMemcpyAsync(b.samp, samp_recs, ((size_t)nsamples + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaMemsetAsync(b.scounts, 0, ((size_t)nsamples + 1) * sizeof(uint32_t), st));
+    CUDA_TRY(cudaMemsetAsync(b.kept, 0, ((size_t)nsamples + 1) * sizeof(uint32_t), st));
+    k_sketch_scan<false><<<(unsigned)nblocks, kSketchThreads, 0, st>>>(b.seq, seq_len, b.rec, nrec, b.samp, nsamples, g,
+                                                                       b.counts, b.scounts, nullptr, nullptr);
+    count_launch();
+    CUDA_TRY(cudaGetLastError());
+    // thread offsets and sample segments: exclusive sums (the totals land in the last word)
+    size_t tb0 = 0, tb1 = 0, tb2 = 0, tb3 = 0;
+    CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, tb0, b.counts, b.pos, (int64_t)nthreads, st));
+    CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, tb1, b.scounts, b.seg, nsamples + 1, st));
+    CUDA_TRY(cudaMalloc(&b.tmp, std::max(tb0, tb1)));
+    CUDA_TRY(cub::DeviceScan::ExclusiveSum(b.tmp, tb0, b.counts, b.pos, (int64_t)nthreads, st));
+    CUDA_TRY(cub::DeviceScan::ExclusiveSum(b.tmp, tb1, b.scounts, b.seg, nsamples + 1, st));
+    count_launch(2);
+    uint32_t total = 0;
+    CUDA_TRY(cudaMemcpyAsync(&total, b.seg + nsamples, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    if (total == 0)
+        return KSSDGPU_OK;
+    CUDA_TRY(cudaMalloc(&b.k0, (size_t)total * sizeof(unsigned long long)));
+    CUDA_TRY(cudaMalloc(&b.k1, (size_t)total * sizeof(unsigned long long)));
+    CUDA_TRY(cudaMalloc(&b.keep, total));
+    CUDA_TRY(cudaMalloc(&b.nsel, sizeof(int)));
+    k_sketch_scan<true><<<(unsigned)nblocks, kSketchThreads, 0, st>>>(b.seq, seq_len, b.rec, nrec, b.samp, nsamples, g,
+                                                                      nullptr, nullptr, b.pos, b.k0);
+    count_launch();
+    CUDA_TRY(cudaGetLastError());
+    // sort each sample's keys, mark the kept ones, compact
+    CUDA_TRY(cub::DeviceSegmentedSort::SortKeys(nullptr, tb2, b.k0, b.k1, (int64_t)total, nsamples, b.seg,
+                                                b.seg + 1, st));
+    CUDA_TRY(cub::DeviceSelect::Flagged(nullptr, tb3, b.k1, b.keep, b.k0, b.nsel, (int64_t)total, st));
+    if (std::max(tb2, tb3) > std::max(tb0, tb1)) {
+        cudaFree(b.tmp);
+        b.tmp = nullptr;
+        CUDA_TRY(cudaMalloc(&b.tmp, std::max(tb2, tb3)));
+    }
+    CUDA_TRY(cub::DeviceSegmentedSort::SortKeys(b.tmp, tb2, b.k0, b.k1, (int64_t)total, nsamples, b.seg, b.seg + 1,
+                                                st));
+    k_sketch_keep<<<grid_for(total), 256, 0, st>>>(b.k1, total, b.seg, nsamples, ob, p->conflict ? 1 : 0, b.keep,
+                                                   b.kept);
+    CUDA_TRY(cub::DeviceSelect::Flagged(b.tmp, tb3, b.k1, b.keep, b.k0, b.nsel, (int64_t)total, st));
+    count_launch(3);
+    int nsel = 0;
+    std::vector<uint32_t> kept((size_t)nsamples);
+    CUDA_TRY(cudaMemcpyAsync(&nsel, b.nsel, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaMemcpyAsync(kept.data(), b.kept, (size_t)nsamples * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    for (int s = 0; s < nsamples; ++s)
+        offs[s + 1] = offs[s] + kept[s];
+    if (offs[nsamples] != (uint64_t)nsel)
+        return fail(KSSDGPU_ERR_CUDA, "sketch compaction count mismatch");
+    if ((uint64_t)nsel > keys_cap || (nsel && !keys))
+        return fail(KSSDGPU_ERR_CAPACITY, "sketch output needs " + std::to_string(nsel) + " keys (offs holds them)");
+    if (nsel)
+        CUDA_TRY(cudaMemcpy(keys, b.k0, (size_t)nsel * sizeof(uint64_t), cudaMemcpyDeviceToHost));
+    return KSSDGPU_OK;
+}
+
+
 int kssdgpu_index_from_records(const void *records12, uint64_t n, int nref, int obj_bits, int device,
                                kssdgpu_index_t **out)
 {
@@ -3615,6 +4231,7 @@ void kssdgpu_index_free(kssdgpu_index_t *ix)
     cudaFree(ix->gbeg);
     cudaFree(ix->table);
     cudaFree(ix->bloom);
+    cudaFree(ix->bloom_bounds);
     cudaFree(ix->err);
     cudaFree(ix->work);
     ix->s_keys.release();
@@ -3623,6 +4240,10 @@ void kssdgpu_index_free(kssdgpu_index_t *ix)
     ix->s_order.release();
     ix->s_items.release();
     ix->s_prefix.release();
+    ix->s_spos.release();
+    ix->s_scnt.release();
+    ix->s_spre.release();
+    ix->s_sitems.release();
     for (int i = 0; i < 3; ++i)
         if (ix->pipe_st[i])
             cudaStreamDestroy(ix->pipe_st[i]);
@@ -3658,6 +4279,26 @@ int kssdgpu_index_info(const kssdgpu_index_t *ix, uint64_t *records, uint64_t *c
     if (contexts) *contexts = ix->u;
     if (nref) *nref = ix->nref;
     if (obj_bits) *obj_bits = ix->obj_bits;
+    return KSSDGPU_OK;
+}
+
+int kssdgpu_index_filter(kssdgpu_index_t *ix, uint64_t max_stripe_bytes, int *stripes, uint64_t *bytes)
+{
+    if (!ix)
+        return fail(KSSDGPU_ERR_ARG, "null index");
+    if (max_stripe_bytes && max_stripe_bytes < 32)
+        return fail(KSSDGPU_ERR_ARG, "a filter stripe holds at least one 32-byte block");
+    CUDA_TRY(cudaSetDevice(ix->device));
+    cudaStream_t st = nullptr;
+    CUDA_TRY(cudaDeviceSynchronize());
+    int rc = build_filter(ix, max_stripe_bytes ? max_stripe_bytes : kStripeBytes, st);
+    if (rc)
+        return rc;
+    CUDA_TRY(cudaStreamSynchronize(st));
+    if (stripes)
+        *stripes = ix->bloom ? ix->bloom_stripes : 0;
+    if (bytes)
+        *bytes = ix->bloom ? (uint64_t)ix->bloom_stripes * ((uint64_t)ix->bloom_mask + 1) * 32 : 0;
     return KSSDGPU_OK;
 }
 
@@ -3759,10 +4400,15 @@ int kssdgpu_count_tune(kssdgpu_index_t *ix, const uint64_t *d_qry_keys, const ui
     struct Cand {
         bool smem;
         uint32_t chunk;
+        bool striped;
     };
-    std::vector<Cand> cands = {{false, 1024}, {false, 4096}, {false, 16384}};
+    // with the filter on: global rows in key-range chunks, global rows stripe by stripe
+    // (several filter stripes), shared rows (where a row fits)
+    std::vector<Cand> cands = {{false, 1024, false}, {false, 4096, false}, {false, 16384, false}};
+    if (ix->bloom && ix->bloom_stripes > 1)
+        cands.push_back({false, 4096, true});
     if (smem_row_fits(ix, base))
-        cands.push_back({true, 4096});
+        cands.push_back({true, 4096, false});
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     CUDA_TRY(cudaEventCreate(&ev0));
     cudaError_t ce = cudaEventCreate(&ev1);
@@ -3770,15 +4416,17 @@ int kssdgpu_count_tune(kssdgpu_index_t *ix, const uint64_t *d_qry_keys, const ui
         cudaEventDestroy(ev0);
         return fail(KSSDGPU_ERR_CUDA, cudaGetErrorString(ce));
     }
-    const bool keep_smem = ix->count_smem;
+    const bool keep_smem = ix->count_smem, keep_striped = ix->count_striped, keep_filter = ix->count_filter;
     const uint32_t keep_chunk = ix->count_chunk_keys;
-    float best = 1e30f;
-    Cand pick = {keep_smem, keep_chunk};
     int rc = KSSDGPU_OK, tried = 0;
-    for (const Cand &c : cands) {
+    // best of three timed runs after a warm-up, CUDA events on the legacy stream
+    auto time_setting = [&](const Cand &c, bool filter, float &t_min) {
+        ix->count_smem = c.smem;
         ix->count_chunk_keys = c.chunk;
+        ix->count_striped = c.striped;
+        ix->count_filter = filter;
         const unsigned f = base | (c.smem ? KSSDGPU_SMEM_ACC : KSSDGPU_GLOBAL_ACC);
-        float t_min = 1e30f;
+        t_min = 1e30f;
         for (int r = 0; r < 4 && rc == KSSDGPU_OK; ++r) {
             ce = cudaEventRecord(ev0, 0);
             if (ce == cudaSuccess) {
@@ -3801,60 +4449,43 @@ int kssdgpu_count_tune(kssdgpu_index_t *ix, const uint64_t *d_qry_keys, const ui
             if (r > 0)
                 t_min = std::min(t_min, ms);
         }
+        if (rc == KSSDGPU_OK)
+            ++tried;
+    };
+    float best = 1e30f;
+    Cand pick = {keep_smem, keep_chunk, keep_striped};
+    const bool filter_on = ix->bloom != nullptr;
+    for (const Cand &c : cands) {
+        float t = 0;
+        time_setting(c, filter_on, t);
         if (rc)
             break;
-        ++tried;
-        if (t_min < best) {
-            best = t_min;
+        if (t < best) {
+            best = t;
             pick = c;
         }
     }
-    // then the best setting without (or with) the membership filter
-    bool filter = ix->count_filter;
-    if (rc == KSSDGPU_OK && ix->bloom) {
-        ix->count_smem = pick.smem;
-        ix->count_chunk_keys = pick.chunk;
-        ix->count_filter = !filter;
-        const unsigned f = base | (pick.smem ? KSSDGPU_SMEM_ACC : KSSDGPU_GLOBAL_ACC);
-        float t_min = 1e30f;
-        for (int r = 0; r < 4 && rc == KSSDGPU_OK; ++r) {
-            ce = cudaEventRecord(ev0, 0);
-            if (ce == cudaSuccess) {
-                rc = count_dev_impl(ix, d_qry_keys, d_qry_offs, nq, qry_gid_offset, lower != 0, f,
-                                    reinterpret_cast<unsigned long long *>(d_ctx),
-                                    reinterpret_cast<unsigned long long *>(d_obj),
-                                    reinterpret_cast<unsigned long long *>(d_uctx),
-                                    reinterpret_cast<unsigned long long *>(d_uobj), nullptr, nullptr, 0);
-                if (rc)
-                    break;
-            }
-            if (ce == cudaSuccess) ce = cudaEventRecord(ev1, 0);
-            if (ce == cudaSuccess) ce = cudaEventSynchronize(ev1);
-            float ms = 0;
-            if (ce == cudaSuccess) ce = cudaEventElapsedTime(&ms, ev0, ev1);
-            if (ce != cudaSuccess) {
-                rc = fail(KSSDGPU_ERR_CUDA, cudaGetErrorString(ce));
-                break;
-            }
-            if (r > 0)
-                t_min = std::min(t_min, ms);
+    // then the best setting without the membership filter
+    bool filter = filter_on;
+    if (rc == KSSDGPU_OK && filter_on) {
+        float t = 0;
+        time_setting(pick, false, t);
+        if (rc == KSSDGPU_OK && t < best) {
+            best = t;
+            filter = false;
         }
-        if (rc == KSSDGPU_OK) {
-            ++tried;
-            if (t_min < best) {
-                best = t_min;
-                filter = !filter;
-            }
-        }
-        ix->count_filter = filter;
     }
     cudaEventDestroy(ev0);
     cudaEventDestroy(ev1);
     if (rc) {
         ix->count_smem = keep_smem;
         ix->count_chunk_keys = keep_chunk;
+        ix->count_striped = keep_striped;
+        ix->count_filter = keep_filter;
         return rc;
     }
+    ix->count_filter = filter;
+    ix->count_striped = pick.striped;
     ix->count_smem = pick.smem;
     ix->count_chunk_keys = pick.chunk;
     ix->count_tune_tried = tried;
@@ -3865,6 +4496,7 @@ int kssdgpu_count_tune(kssdgpu_index_t *ix, const uint64_t *d_qry_keys, const ui
         out->candidates = tried;
         out->ms = best;
         out->filter = ix->count_filter && ix->bloom ? 1 : 0;
+        out->striped = out->filter && ix->count_striped && ix->bloom_stripes > 1 && !pick.smem ? 1 : 0;
     }
     return check_dev_err(ix, 0);
 }
@@ -3949,6 +4581,8 @@ int kssdgpu_count_block_noalloc(kssdgpu_index_t *ix, const uint64_t *d_qry_keys,
     P.err = ix->err;
     P.bloom = ix->count_filter ? ix->bloom : nullptr;
     P.bloom_mask = ix->bloom_mask;
+    P.bloom_stripes = ix->bloom_stripes;
+    P.bloom_bounds = ix->bloom_bounds;
     P.order = use_smem ? reinterpret_cast<const int *>(scr + kNoallocHeaderWords) : nullptr;
     P.chunk_prefix = use_smem ? nullptr : scr + kNoallocHeaderWords - 1;
     P.chunk_keys = ix->count_chunk_keys;

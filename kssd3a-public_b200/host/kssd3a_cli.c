@@ -14,7 +14,9 @@
  *   multi-query stream          src/command_ani.c:2792-3015
  *   no-index hash detail        src/command_ani.c:3837-4000
  *
- * Inputs are sketch directories; FASTA/FASTQ inputs need a sketcher and are rejected.
+ * Inputs are sketch directories, or FASTA/FASTQ files and directories of them, which
+ * are sketched on the GPU first (auto ANI, src/command_ani_wrapper.c:842-1046,1275-1502;
+ * host/kssd_autosketch.c).
  */
 #define _GNU_SOURCE
 #include <argp.h>
@@ -35,6 +37,8 @@
 
 #include "kssd_epilogue.h"
 #include "kssd_format.h"
+#include "kssd_autosketch.h"
+#include "kssd_fastx.h"
 #include "kssdgpu.h"
 
 #define PATHLEN KSSD_PATHLEN
@@ -51,7 +55,7 @@ typedef struct cli {
     bool sketch_coden;
     int sketch_hclen, sketch_holen, sketch_iolen, sketch_drfold, sketch_kmerocrs, sketch_ncap;
     double sketch_npercentile;
-    bool sketch_split_mfa;
+    bool sketch_split_mfa, sketch_abundance, sketch_anno, sketch_conflict, sketch_asone, sketch_reads_qc;
     int nrem;
     char **rem;
 } cli_t;
@@ -71,8 +75,8 @@ static struct argp_option k_opts[] = {
     {"ref", 'r', "<SKETCH>", 0, "Reference sketch directory.", 1},
     {"query", 'q', "<SKETCH>", 0, "Query sketch directory.", 1},
     {"qraw", 'x', "<SKETCH>", 0, "Raw-read query sketch directory; enables naive ANI mode.", 1},
-    {"reflist", 779, "<FILE>", 0, "Reference path list for auto ANI (needs a sketcher; not in this build).", 1},
-    {"qrylist", 780, "<FILE>", 0, "Query path list for auto ANI (needs a sketcher; not in this build).", 1},
+    {"reflist", 779, "<FILE>", 0, "Reference FASTA/FASTQ/sketch path list for auto ANI.", 1},
+    {"qrylist", 780, "<FILE>", 0, "Query FASTA/FASTQ/sketch path list for auto ANI.", 1},
     {"index", 'i', "<FILE>", OPTION_HIDDEN, "Reserved; currently unused.", 2},
     {0, 0, 0, 0, "ANI mode and conflict handling:", 2},
     {"naive", 'v', 0, 0, "Use naive distance/ANI calculation.", 2},
@@ -105,7 +109,7 @@ static struct argp_option k_opts[] = {
     {"top", 'N', "<INT>", 0, "Report at most top N references per query. [all]", 4},
     {0, 0, 0, 0, "Execution:", 5},
     {"threads", 'p', "<INT>", 0, "Number of host threads for the epilogue.", 5},
-    {0, 0, 0, 0, "Direct FASTA/FASTQ input mode (needs a sketcher; not in this build):", 6},
+    {0, 0, 0, 0, "Direct FASTA/FASTQ input mode:", 6},
     {"pair", 777, 0, 0, "Treat positional inputs as reference then query inputs.", 6},
     {"pipecmd", O_PIPECMD, "<cmd>", 0, "Stream each raw input through command.", 6},
     {"use_coden_ctxobj", O_USE_CODEN, 0, 0, "Use the coden context-object pattern. [default]", 7},
@@ -208,8 +212,15 @@ static error_t parse_ani(int key, char *arg, struct argp_state *st)
     case O_LSTKMER: g.sketch_kmerocrs = parse_int_range(st, "--LstKmerOcrs", arg, 1, 65536); break;
     case O_NPERCENTILE: g.sketch_npercentile = parse_double_range(st, "--npercentile", arg, 0.0, 1.0); break;
     case O_NCAP: g.sketch_ncap = parse_int_range(st, "--ncap", arg, 0, 65536); break;
-    case O_READSQC: if (g.sketch_kmerocrs < 2) g.sketch_kmerocrs = 2; break;
-    case O_ABUNDANCE: case O_ANNO: case O_CONFLICT: case O_ASONE: break;
+    case O_READSQC:
+        g.sketch_reads_qc = true;
+        if (g.sketch_kmerocrs < 2)
+            g.sketch_kmerocrs = 2;
+        break;
+    case O_ABUNDANCE: g.sketch_abundance = true; break;
+    case O_ANNO: g.sketch_anno = true; break;
+    case O_CONFLICT: g.sketch_conflict = true; break;
+    case O_ASONE: g.sketch_asone = true; break;
     case O_SPLITMFA: g.sketch_split_mfa = true; break;
     case O_PIPECMD: copy_path(st, "--pipecmd", g.pipecmd, arg); break;
     case O_RAW_OUTPUT: o->raw_output = true; break;
@@ -1765,6 +1776,320 @@ static int run_sketch_ani(void)
     return run_detail_scan(DETAIL_HASH);
 }
 
+/* ------------------------------------------------------------------ auto ANI on sequence inputs
+ * FASTA/FASTQ inputs are sketched (on the GPU) into temporary sketch directories with
+ * the parameters of the first sketch input, or the auto-sketch defaults, then merged
+ * per side and counted like sketch inputs (src/command_ani_wrapper.c:842-1046,
+ * 1275-1502). */
+
+typedef struct path_list {
+    char **v;
+    int n, cap;
+} path_list_t;
+
+static void plist_push(path_list_t *l, const char *p)
+{
+    if (l->n == l->cap) {
+        l->cap = l->cap ? 2 * l->cap : 8;
+        l->v = realloc(l->v, (size_t)l->cap * sizeof(char *));
+        if (!l->v)
+            err(errno, "%s(): OOM path vector", "path_vec_push");
+    }
+    l->v[l->n] = strdup(p);
+    if (!l->v[l->n])
+        err(errno, "%s(): OOM path copy", "path_vec_push");
+    l->n++;
+}
+
+static void read_path_list(const char *list_path, path_list_t *out, const char *option_name)
+{
+    FILE *list = fopen(list_path, "r");
+    if (!list)
+        err(errno, "can't open %s file %s", option_name, list_path);
+    char *line = malloc(4096);
+    int line_no = 0;
+    while (fgets(line, 4096, list) != NULL) {
+        line_no++;
+        size_t len = strlen(line);
+        if (len == 4095 && line[len - 1] != '\n' && line[len - 1] != '\r')
+            errx(EXIT_FAILURE, "%s file %s line %d exceeds maximum line length %d", option_name, list_path, line_no,
+                 4095);
+        char *start = line;
+        while (isspace((unsigned char)*start))
+            start++;
+        char *end = start + strlen(start);
+        while (end > start && isspace((unsigned char)end[-1]))
+            end--;
+        *end = 0;
+        if (!start[0])
+            continue;
+        if (strlen(start) >= PATHLEN)
+            errx(EXIT_FAILURE, "%s file %s line %d path exceeds maximum length %d", option_name, list_path, line_no,
+                 PATHLEN - 1);
+        plist_push(out, start);
+    }
+    if (ferror(list))
+        err(errno, "failed while reading %s file %s", option_name, list_path);
+    free(line);
+    fclose(list);
+    if (out->n < 1)
+        errx(EXIT_FAILURE, "%s file %s has no input paths", option_name, list_path);
+}
+
+static kssd_sketch_stat_t read_sketch_stat_or_die(const char *dir)
+{
+    kssd_sketch_stat_t st;
+    if (kssd_read_stat(dir, &st))
+        err(EINVAL, "%s(): %s", "read_lco_sketch_stat", kssd_host_last_error());
+    return st;
+}
+
+static void validate_supported_auto_stat(const kssd_sketch_stat_t *st)
+{
+    /* src/command_ani_wrapper.c:918-949 */
+    if (st->drfold < 0 || st->drfold > 32)
+        errx(EXIT_FAILURE, "unsupported sketch drfold %d in first auto ANI sketch", st->drfold);
+    if (st->klen > 32)
+        errx(EXIT_FAILURE, "first auto ANI sketch has unsupported klen=%d; expected at most 32", st->klen);
+    if (st->coden_len > 0) {
+        if (st->coden_len != KSSD_NUM_CODENS)
+            errx(EXIT_FAILURE, "first auto ANI sketch uses coden_len=%d, but this binary was built with NUM_CODENS=%d",
+                 st->coden_len, KSSD_NUM_CODENS);
+        const int expected = KSSD_NUM_CODENS < 11 ? 3 * KSSD_NUM_CODENS + 1 : 32;
+        if (st->klen != expected)
+            errx(EXIT_FAILURE, "first auto ANI sketch klen=%d is not compatible with coden_len=%d in this binary",
+                 st->klen, st->coden_len);
+    } else if (st->klen - 2 * (st->hclen + st->holen) < 0) {
+        errx(EXIT_FAILURE, "first auto ANI sketch has invalid manual context-object lengths: klen=%d hclen=%d holen=%d",
+             st->klen, st->hclen, st->holen);
+    }
+}
+
+static bool same_auto_stat(const kssd_sketch_stat_t *a, const kssd_sketch_stat_t *b)
+{
+    return a->hash_id == b->hash_id && a->koc == b->koc && a->conflict == b->conflict &&
+           a->coden_len == b->coden_len && a->klen == b->klen && a->hclen == b->hclen && a->holen == b->holen &&
+           a->drfold == b->drfold;
+}
+
+static void validate_auto_inputs(const path_list_t *in, const kssd_sketch_stat_t *t)
+{
+    for (int i = 0; i < in->n; ++i) {
+        if (!is_sketch_dir(in->v[i]))
+            continue;
+        kssd_sketch_stat_t st = read_sketch_stat_or_die(in->v[i]);
+        if (!same_auto_stat(t, &st))
+            errx(EXIT_FAILURE,
+                 "%s sketch parameters do not match first auto ANI sketch "
+                 "(hash_id %u/%u, koc %d/%d, conflict %d/%d, coden_len %d/%d, "
+                 "klen %d/%d, hclen %d/%d, holen %d/%d, drfold %d/%d)",
+                 in->v[i], st.hash_id, t->hash_id, st.koc, t->koc, st.conflict, t->conflict, st.coden_len,
+                 t->coden_len, st.klen, t->klen, st.hclen, t->hclen, st.holen, t->holen, st.drfold, t->drfold);
+    }
+}
+
+static kssd_sketch_stat_t default_auto_stat(void)
+{
+    return kssd_default_auto_stat(g.sketch_coden, g.sketch_hclen, g.sketch_holen, g.sketch_iolen, g.sketch_drfold,
+                                  g.sketch_conflict, g.sketch_abundance);
+}
+
+static kssd_sketch_stat_t select_auto_template(const path_list_t *ref, const path_list_t *qry)
+{
+    const path_list_t *sides[2] = {ref, qry};
+    for (int s = 0; s < 2; ++s)
+        for (int i = 0; i < sides[s]->n; ++i)
+            if (is_sketch_dir(sides[s]->v[i])) {
+                kssd_sketch_stat_t st = read_sketch_stat_or_die(sides[s]->v[i]);
+                validate_supported_auto_stat(&st);
+                return st;
+            }
+    kssd_sketch_stat_t st = default_auto_stat();
+    validate_supported_auto_stat(&st);
+    return st;
+}
+
+/* Sketch options whose sketches need k-mer counts, read statistics, per-record
+ * genomes or piped streams: not part of this build's sketcher. */
+static void reject_unbuilt_sketch_options(const kssd_sketch_stat_t *t)
+{
+    const char *what = NULL;
+    if (g.pipecmd[0])
+        what = "--pipecmd";
+    else if (g.sketch_split_mfa)
+        what = "--splitmfa";
+    else if (t->koc)
+        what = "abundance (counting) sketches";
+    else if (g.sketch_reads_qc)
+        what = "--readsQC";
+    else if (g.sketch_npercentile > 0.0)
+        what = "--npercentile";
+    else if (g.sketch_ncap > 0)
+        what = "--ncap";
+    else if (g.sketch_kmerocrs > 1)
+        what = "--LstKmerOcrs above 1";
+    if (what)
+        errx(EXIT_FAILURE, "sequence inputs with %s are not supported by this build's sketcher; sketch them with "
+                           "`kssd3a sketch` and pass the sketch directories", what);
+}
+
+static void sketch_arg_to_dir(const char *input, const kssd_sketch_stat_t *t, const char *outdir)
+{
+    reject_unbuilt_sketch_options(t);
+    kssd_autosketch_opt_t ao;
+    memset(&ao, 0, sizeof ao);
+    ao.tmpl = *t;
+    ao.asone = g.sketch_asone;
+    ao.anno = g.sketch_anno;
+    ao.threads = g.o.p > 0 ? g.o.p : 1;
+    kssd_autosketch_to_dir(input, &ao, outdir);
+}
+
+static void prepare_side(const path_list_t *inputs, path_list_t *sketches, const char *prefix,
+                         const kssd_sketch_stat_t *t, const char *tmp_root)
+{
+    for (int i = 0; i < inputs->n; ++i) {
+        if (is_sketch_dir(inputs->v[i])) {
+            plist_push(sketches, inputs->v[i]);
+            continue;
+        }
+        char outdir[2 * PATHLEN];
+        int w = snprintf(outdir, sizeof outdir, "%s/%sseq_%d", tmp_root, prefix, i);
+        if (w < 0 || (size_t)w >= sizeof outdir)
+            errx(EXIT_FAILURE, "auto ANI temporary output path is too long for %s", inputs->v[i]);
+        sketch_arg_to_dir(inputs->v[i], t, outdir);
+        plist_push(sketches, outdir);
+    }
+}
+
+static void merge_side(const path_list_t *sketches, const char *outdir, char *dst, const char *label)
+{
+    const char *src = sketches->n == 1 ? sketches->v[0] : outdir;
+    if (strlen(src) >= PATHLEN)
+        errx(EXIT_FAILURE, "%s path is too long; maximum supported length is %d bytes", label, PATHLEN - 1);
+    if (sketches->n > 1)
+        kssd_merge_sketch_dirs(sketches->v, sketches->n, outdir);
+    memcpy(dst, src, strlen(src) + 1);
+}
+
+static int count_stdin(const path_list_t *l)
+{
+    int c = 0;
+    for (int i = 0; i < l->n; ++i)
+        c += !strcmp(l->v[i], "-");
+    return c;
+}
+
+static bool query_side_unassembled(const path_list_t *qry)
+{
+    for (int i = 0; i < qry->n; ++i) {
+        const char *p = qry->v[i];
+        if (is_sketch_dir(p))
+            continue;
+        if (strcmp(p, "-") && kssd_fastx_fmt(p) == KSSD_FMT_FASTQ)
+            return true;
+        if (g.sketch_conflict && (!strcmp(p, "-") || g.pipecmd[0]))
+            return true;
+    }
+    return false;
+}
+
+static char g_tmp_root[PATHLEN];
+
+static void remove_tmp_root(void)
+{
+    if (g_tmp_root[0])
+        kssd_remove_tree(g_tmp_root);
+}
+
+static const char *make_tmp_root(const char *pattern)
+{
+    snprintf(g_tmp_root, sizeof g_tmp_root, "%s", pattern);
+    if (!mkdtemp(g_tmp_root))
+        err(errno, "%s(): mkdtemp", "run_auto_ani_from_sides");
+    atexit(remove_tmp_root);
+    return g_tmp_root;
+}
+
+static int run_auto_ani_from_sides(const path_list_t *ref, const path_list_t *qry)
+{
+    if (ref->n < 1)
+        errx(EXIT_FAILURE, "auto ANI requires at least one reference input");
+    if (qry->n < 1)
+        errx(EXIT_FAILURE, "auto ANI requires at least one query input");
+    if (count_stdin(ref) + count_stdin(qry) > 1)
+        errx(EXIT_FAILURE, "stdin input '-' can be used only once in auto ANI");
+    kssd_sketch_stat_t t = select_auto_template(ref, qry);
+    validate_auto_inputs(ref, &t);
+    validate_auto_inputs(qry, &t);
+    const char *root = make_tmp_root("/tmp/kssd3a_ani_auto_XXXXXX");
+    path_list_t rs = {0}, qs = {0};
+    prepare_side(ref, &rs, "ref", &t, root);
+    prepare_side(qry, &qs, "qry", &t, root);
+    char rm[2 * PATHLEN], qm[2 * PATHLEN];
+    snprintf(rm, sizeof rm, "%s/ref_merged", root);
+    snprintf(qm, sizeof qm, "%s/qry_merged", root);
+    merge_side(&rs, rm, g.refdir, "auto ANI reference sketch");
+    merge_side(&qs, qm, g.qrydir, "auto ANI query sketch");
+    if (query_side_unassembled(qry)) {
+        g.o.unassembled = true;
+        g.o.v = true;
+    }
+    return run_sketch_ani();
+}
+
+static int run_auto_positional_ani(void)
+{
+    if (g.nrem < 2)
+        errx(EXIT_FAILURE, "auto ANI requires one reference input followed by at least one query input");
+    path_list_t ref = {0}, qry = {0};
+    plist_push(&ref, g.rem[0]);
+    for (int i = 1; i < g.nrem; ++i)
+        plist_push(&qry, g.rem[i]);
+    return run_auto_ani_from_sides(&ref, &qry);
+}
+
+static int run_auto_list_ani(void)
+{
+    path_list_t ref = {0}, qry = {0};
+    read_path_list(g.reflist, &ref, "--reflist");
+    read_path_list(g.qrylist, &qry, "--qrylist");
+    return run_auto_ani_from_sides(&ref, &qry);
+}
+
+static int run_direct_query_sequence_ani(bool force_raw, const char *option_name)
+{
+    /* src/command_ani_wrapper.c:1443-1502 */
+    if (!is_sketch_dir(g.refdir))
+        errx(EXIT_FAILURE,
+             "%s sequence input requires -r/--ref to be a sketch directory; "
+             "for direct reference sequence input use positional auto ANI",
+             option_name);
+    struct stat st;
+    if (stat(g.qrydir, &st) == 0 && S_ISDIR(st.st_mode))
+        errx(EXIT_FAILURE, "%s input '%s' is a directory but not a valid sketch", option_name, g.qrydir);
+    kssd_sketch_stat_t t = read_sketch_stat_or_die(g.refdir);
+    validate_supported_auto_stat(&t);
+    if (force_raw || g.sketch_conflict)
+        t.conflict = true;
+    const char *root = make_tmp_root("/tmp/kssd3a_ani_query_XXXXXX");
+    char out[2 * PATHLEN];
+    int w = snprintf(out, sizeof out, "%s/qry_seq", root);
+    if (w < 0 || (size_t)w >= sizeof out)
+        errx(EXIT_FAILURE, "temporary %s sketch output path is too long", option_name);
+    char input[PATHLEN];
+    snprintf(input, sizeof input, "%s", g.qrydir);
+    sketch_arg_to_dir(input, &t, out);
+    if (strlen(out) >= sizeof g.qrydir)
+        errx(EXIT_FAILURE, "temporary query sketch path is too long; maximum supported length is %zu bytes",
+             sizeof g.qrydir - 1);
+    memcpy(g.qrydir, out, strlen(out) + 1);
+    g.o.unassembled = force_raw;
+    if (force_raw)
+        g.o.v = true;
+    return run_sketch_ani();
+}
+
 static int cmd_ani(int argc, char **argv)
 {
     memset(&g, 0, sizeof g);
@@ -1778,14 +2103,17 @@ static int cmd_ani(int argc, char **argv)
     g.o.estimate_coverage = g.estimate_coverage;
     if (g.o.p < 1)
         g.o.p = 1;
-    if (g.reflist[0] || g.qrylist[0] || g.pair)
-        errx(EXIT_FAILURE, "FASTA/FASTQ and list inputs need the sketcher, which this build does not include; "
-                           "sketch with `kssd3a sketch` first");
-    if (!is_sketch_dir(g.qrydir))
-        errx(EXIT_FAILURE, "%s is not a sketch directory; FASTA/FASTQ inputs need the sketcher, which this build "
-                           "does not include", g.qrydir);
     start_gpu_warmup();
-    run_sketch_ani();
+    /* src/command_ani_wrapper.c:1519-1530 */
+    if (g.reflist[0] || g.qrylist[0])
+        run_auto_list_ani();
+    else if (g.qrydir[0]) {
+        if (!is_sketch_dir(g.qrydir))
+            run_direct_query_sequence_ani(g.o.unassembled, g.o.unassembled ? "--qraw" : "-q/--query");
+        else
+            run_sketch_ani();
+    } else if (g.nrem >= 2)
+        run_auto_positional_ani();
     return 0;
 }
 

@@ -29,6 +29,8 @@ static void set_err(const char *fmt, ...)
     va_end(ap);
 }
 
+void kssd_host_set_error(const char *msg) { snprintf(g_err, sizeof g_err, "%s", msg); }
+
 bool kssd_file_exists(const char *dir, const char *name)
 {
     char p[4096];

@@ -70,6 +70,7 @@ typedef struct kssd_sketch {
 
 /* Last error message of the host library (thread-local). */
 const char *kssd_host_last_error(void);
+void kssd_host_set_error(const char *msg);
 
 /* Loads a sketch directory.  flags: 1 = annotations, 2 = infile meta.
  * Returns NULL on error (message via kssd_host_last_error). */

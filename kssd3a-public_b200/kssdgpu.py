@@ -65,6 +65,7 @@ def gpu_lib() -> C.CDLL:
         lib.kssdgpu_index_info.argtypes = [vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
                                            C.POINTER(C.c_int), C.POINTER(C.c_int)]
         lib.kssdgpu_index_export.argtypes = [vp, vp, vp]
+        lib.kssdgpu_index_filter.argtypes = [vp, C.c_uint64, C.POINTER(C.c_int), C.POINTER(C.c_uint64)]
         lib.kssdgpu_index_ref_ctx_counts.argtypes = [vp, C.c_int, C.c_int, vp, vp]
         lib.kssdgpu_count_block.argtypes = [vp, vp, _u64p, C.c_int, C.c_uint, vp, vp, vp, vp]
         lib.kssdgpu_count_lower.argtypes = [vp, vp, _u64p, C.c_int, C.c_int, C.c_uint, vp, vp]
@@ -95,8 +96,42 @@ def gpu_lib() -> C.CDLL:
         lib.kssdgpu_server_reset_stats.argtypes = [vp]
         lib.kssdgpu_server_destroy.argtypes = [vp]
         lib.kssdgpu_server_destroy.restype = None
+        lib.kssdgpu_sketch.argtypes = [C.c_char_p, C.c_uint64, _u64p, C.c_uint64, _u64p, C.c_int,
+                                       C.POINTER(_SketchParams), vp, C.c_uint64, _u64p]
+        lib.kssdgpu_sketch_hash_id.argtypes = [C.POINTER(_SketchParams)]
+        lib.kssdgpu_sketch_hash_id.restype = C.c_uint32
         _gpu = lib
     return _gpu
+
+
+class _SketchParams(C.Structure):
+    _fields_ = [("klen", C.c_int), ("coden_len", C.c_int), ("hclen", C.c_int), ("holen", C.c_int),
+                ("drfold", C.c_int), ("conflict", C.c_int)]
+
+
+def sketch(samples, klen=32, coden_len=11, hclen=0, holen=0, drfold=8, conflict=False):
+    """Sketches on the device: samples is a list of samples, each a list of records'
+    sequence bytes.  Returns (keys, offs) in the comblco / comblco.index layout."""
+    recs = [r for smp in samples for r in smp]
+    seq = b"".join(recs)
+    rec_offs = np.cumsum([0] + [len(r) for r in recs]).astype(np.uint64)
+    samp = np.cumsum([0] + [len(smp) for smp in samples]).astype(np.uint64)
+    prm = _SketchParams(klen, coden_len, hclen, holen, drfold, 1 if conflict else 0)
+    offs = np.zeros(len(samples) + 1, dtype=np.uint64)
+    cap = max(1, len(seq) // max(1, 1 << min(drfold, 8)) + 1024)
+    keys = np.zeros(cap, dtype=np.uint64)
+    rc = gpu_lib().kssdgpu_sketch(seq, len(seq), rec_offs, len(recs), samp, len(samples), C.byref(prm),
+                                  keys.ctypes.data, cap, offs)
+    if rc == 7:  # capacity: offs holds the sizes
+        keys = np.zeros(int(offs[-1]), dtype=np.uint64)
+        rc = gpu_lib().kssdgpu_sketch(seq, len(seq), rec_offs, len(recs), samp, len(samples), C.byref(prm),
+                                      keys.ctypes.data if len(keys) else None, len(keys), offs)
+    _check(rc)
+    return keys[:int(offs[-1])].copy(), offs
+
+
+def sketch_hash_id(klen=32, coden_len=11, hclen=0, holen=0, drfold=8):
+    return gpu_lib().kssdgpu_sketch_hash_id(C.byref(_SketchParams(klen, coden_len, hclen, holen, drfold, 0)))
 
 
 class _ServerConfig(C.Structure):
@@ -106,7 +141,7 @@ class _ServerConfig(C.Structure):
 
 class _CountTuning(C.Structure):
     _fields_ = [("smem_rows", C.c_int), ("chunk_keys", C.c_uint32), ("candidates", C.c_int), ("ms", C.c_float),
-                ("filter", C.c_int)]
+                ("filter", C.c_int), ("striped", C.c_int)]
 
 
 class _ServerStats(C.Structure):
@@ -350,6 +385,13 @@ class Index:
         r, u, n, o = C.c_uint64(), C.c_uint64(), C.c_int(), C.c_int()
         _check(gpu_lib().kssdgpu_index_info(self._h, C.byref(r), C.byref(u), C.byref(n), C.byref(o)))
         return dict(records=r.value, contexts=u.value, nref=n.value, obj_bits=o.value)
+
+    def filter(self, max_stripe_bytes: int = 0):
+        """Rebuild the context membership filter with key-range stripes of at most
+        max_stripe_bytes (0: the default); returns its stripe count and bytes."""
+        n, b = C.c_int(), C.c_uint64()
+        _check(gpu_lib().kssdgpu_index_filter(self._h, max_stripe_bytes, C.byref(n), C.byref(b)))
+        return dict(stripes=n.value, bytes=b.value)
 
     def export(self):
         info = self.info()

@@ -380,6 +380,56 @@ def test_chunked_global_rows_with_runs_across_chunks():
             assert not g[1].any()
 
 
+@pytest.mark.parametrize("stripe_bytes", [0, 32, 2048, 1 << 16])
+def test_striped_filter_counts(stripe_bytes):
+    """The context membership filter cut into key-range stripes (down to one 32-byte
+    block per stripe, up to 256 stripes): block, unique, ignoreconflict and lower
+    counts, stripe-major (global rows) and with the stripe found per key (shared rows),
+    equal the oracle's counters; the filter admits every context of the index."""
+    import torch
+    ref = kssdgpu.synth(n_samples=64, n_clusters=8, len_median=3e5, len_min=1e5, len_max=1e6,
+                        size_dist=kssdgpu.SIZE_LOGNORMAL, sub_lo=0.001, sub_hi=0.1, seed=15, sample_seed=15)
+    qry = kssdgpu.synth(n_samples=24, n_clusters=8, role=kssdgpu.ROLE_OWNLEN, len_median=3e5, len_min=1e5,
+                        len_max=1e6, size_dist=kssdgpu.SIZE_LOGNORMAL, own_len_min=5e4, own_len_max=2e6,
+                        seed=15, sample_seed=16)
+    rec = oracle.build_index(ref.keys, ref.offs)
+    idx = kssdgpu.Index.from_records(rec, ref.n)
+    f = idx.filter(stripe_bytes)
+    ctxs = idx.info()["contexts"]
+    if stripe_bytes and ctxs > stripe_bytes:
+        assert 1 < f["stripes"] <= 256
+    per_ctx_bits = f["bytes"] * 8 / ctxs
+    assert per_ctx_bits >= 8
+    # the index's own samples as queries: every context is present and must pass
+    self_want = oracle.count_block(rec, ref.n, ref.keys, ref.offs)
+    for g, w in zip(idx.count_block(ref.keys, ref.offs, kssdgpu.GLOBAL_ACC), self_want):
+        np.testing.assert_array_equal(g, w)
+    for flags in (0, kssdgpu.UNIQUE, kssdgpu.UNIQUE | kssdgpu.IGNORECONFLICT):
+        want = oracle.count_block(rec, ref.n, qry.keys, qry.offs, unique=bool(flags & kssdgpu.UNIQUE),
+                                  ignoreconflict=bool(flags & kssdgpu.IGNORECONFLICT))
+        for acc in (kssdgpu.GLOBAL_ACC, kssdgpu.SMEM_ACC):
+            got = idx.count_block(qry.keys, qry.offs, flags | acc)
+            for g, w in zip(got, want):
+                np.testing.assert_array_equal(g, w)
+    want = oracle.count_lower(rec, ref.n, 0, ref.keys, ref.offs)
+    for acc in (kssdgpu.GLOBAL_ACC, kssdgpu.SMEM_ACC):
+        got = idx.count_lower(ref.keys, ref.offs, 0, acc)
+        for g, w in zip(got, want):
+            np.testing.assert_array_equal(g, w)
+    # device buffers, default accumulator, twice (the stripe offsets are scratch)
+    dev = torch.device("cuda", 0)
+    dk = torch.from_numpy(qry.keys.view(np.int64)).to(dev)
+    do = torch.from_numpy(qry.offs.view(np.int64)).to(dev)
+    want = oracle.count_block(rec, ref.n, qry.keys, qry.offs)
+    for _ in range(2):
+        outs = [torch.full((qry.n * ref.n,), -1, dtype=torch.int64, device=dev) for _ in range(2)]
+        idx.count_block_dev(dk, do, qry.n, *outs)
+        idx.sync()
+        for o, w in zip(outs, want):
+            np.testing.assert_array_equal(o.cpu().numpy().view(np.uint32).reshape(qry.n, ref.n, 2), w)
+    idx.close()
+
+
 def test_count_autotuner_keeps_counts():
     """kssdgpu_count_tune times the accumulator settings on a block; its outputs and
     every later count (under the chosen setting) equal the oracle's counters."""

@@ -56,10 +56,12 @@ def _as_rows(hits, flags):
     return [tuple(int(h[c]) for c in cols) for h in hits]
 
 
-@pytest.mark.parametrize("flags", [0, kssdgpu.UNIQUE | kssdgpu.IGNORECONFLICT])
-def test_results_identical_alone_and_in_the_mix(flags):
+@pytest.mark.parametrize("flags,stripe_bytes", [(0, 0), (kssdgpu.UNIQUE | kssdgpu.IGNORECONFLICT, 0), (0, 256)])
+def test_results_identical_alone_and_in_the_mix(flags, stripe_bytes):
     ref, queries = _workload()
     idx = kssdgpu.Index.from_sketch(ref)
+    if stripe_bytes:  # a filter of many key-range stripes: each context's stripe found per key
+        assert idx.filter(stripe_bytes)["stripes"] > 1
     rec = oracle.build_index(ref.keys, ref.offs)
     want = [_expected(rec, ref.n, q, flags) for q in queries]
     assert sum(len(w) for w in want) > 0

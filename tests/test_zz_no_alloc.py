@@ -52,13 +52,18 @@ def _workload():
 
 
 @pytest.mark.parametrize("case", ["block", "block_unique", "reads_ignoreconflict", "lower", "global_acc",
-                                  "smem_acc", "lower_offset"])
+                                  "smem_acc", "lower_offset", "striped_block_unique", "striped_lower"])
 def test_noalloc_matches_existing_entry_point_twice(case):
     import torch
     ref, qry, reads = _workload()
     idx = kssdgpu.Index.from_sketch(ref)
     dev = torch.device("cuda", 0)
     flags, lower, q, off = 0, False, qry, 0
+    if case.startswith("striped_"):
+        # a filter of many key-range stripes: the existing entry point counts stripe by
+        # stripe, the no-allocation one finds each context's stripe per key
+        assert idx.filter(512)["stripes"] > 1
+        case = case[len("striped_"):]
     if case == "block_unique":
         flags = kssdgpu.UNIQUE
     elif case == "reads_ignoreconflict":
