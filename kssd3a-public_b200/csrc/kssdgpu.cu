@@ -1480,12 +1480,8 @@ constexpr uint32_t kScanThreads = 256;
 #ifndef KSSD_SCAN_PER_THREAD
 #define KSSD_SCAN_PER_THREAD 8
 #endif
-#ifndef KSSD_SCAN_CACHE
-#define KSSD_SCAN_CACHE 1
-#endif
 constexpr uint32_t kScanPerThread = KSSD_SCAN_PER_THREAD;
 constexpr uint32_t kScanTile = kScanThreads * kScanPerThread;  // groups per tile (4 B of gbeg each)
-constexpr uint32_t kCellCache = KSSD_SCAN_CACHE ? 2048 : 1;     // counter cache slots per CTA (pairs mode)
 constexpr uint32_t kCellEmpty = 0xFFFFFFFFu;
 constexpr uint32_t kScanLaneMax = 32;                          // larger groups: the whole CTA
 
@@ -1566,33 +1562,70 @@ __device__ __forceinline__ void join_group_cta(const uint64_t *__restrict__ post
 struct ScanSmem {
     unsigned long long queue[kScanTile];  // groups of 2..kScanLaneMax from the front, larger from the back
     uint32_t prefix[kScanTile];
-    // pairs mode: a per-CTA cache of counter cells (claimed by the first credit that hashes
-    // to a free slot, never evicted, added into the triangle when the CTA ends): hot cells
-    // -- pairs of close genomes take a credit from most of their contexts -- add in shared
-    // memory instead of contending in L2
-    uint32_t cell[kCellCache];
-    uint32_t nc[kCellCache], m2[kCellCache], dobj[kCellCache], sect[kCellCache];  // 32-bit: native shared atomics
 };
 
-// One credit through the CTA's cell cache (cells below 2^32 only; the caller checks).
-__device__ __forceinline__ void credit_cached(ScanSmem &S, unsigned long long *__restrict__ oc,
+// Where the lower triangle spans far more memory than L2 (20,000 genomes: 3.2 GB), its
+// touched cells lie scattered over the whole span and every add into them is slow --
+// atomics onto a fixed set of addresses spread over 1.6 GB run at 38 G/s on a B200
+// against 130 G/s when the same addresses fit in 16 MB -- although the touched cells
+// themselves are few (20,000 genomes: 92,633).  The scan then adds into a compact
+// open-addressing table of touched cells instead (2^21 slots by default: a cell number
+// and its two counter words, 40 MB), claimed by the first credit of a cell that finds a
+// free slot among its first kCellTableProbes; a cell whose probes find no room goes to
+// the triangle directly.  Keys only go from empty to a cell while the join runs and
+// every credit of a cell probes the same sequence, so a cell lives in one slot or in the
+// triangle, never both; k_cell_table_flush adds the slots into the triangle after the
+// join and empties them for the next call.
+constexpr int kCellTableLog = 21;
+constexpr uint32_t kCellTableProbes = 8;
+
+struct CellTable {
+    uint32_t *key;            // cell number, kCellEmpty for a free slot (null: no table)
+    unsigned long long *acc;  // per slot: ctx word (num_mut2 << 32 | num_ctx), obj word (section << 32 | diff_obj)
+    int log;                  // 2^log slots
+};
+
+// One credit into the table, or into the triangle (no table, or no room).
+__device__ __forceinline__ void credit_global(const CellTable &T, unsigned long long *__restrict__ oc,
                                               unsigned long long *__restrict__ oo, uint32_t qg, uint32_t rg, int d)
 {
-    const uint32_t cell = (uint32_t)lower_cell(qg, rg);
-    const uint32_t slot = kCellCache > 1 ? (cell * 2654435761u) >> (32 - 11) : 0u;  // kCellCache = 2^11
-    uint32_t key = S.cell[slot];
-    if (key == kCellEmpty)
-        key = atomicCAS(&S.cell[slot], kCellEmpty, cell) == kCellEmpty ? cell : S.cell[slot];
-    if (key == cell) {
-        atomicAdd(&S.nc[slot], 1u);
-        if (d) {
-            atomicAdd(&S.dobj[slot], 1u);
-            atomicAdd(&S.sect[slot], (uint32_t)d);
-            if (d > 1)
-                atomicAdd(&S.m2[slot], 1u);
+    if (T.key) {
+        const uint32_t cell = (uint32_t)lower_cell(qg, rg);
+        const uint32_t mask = (1u << T.log) - 1;
+        uint32_t s = (cell * 2654435761u) >> (32 - T.log);
+        for (uint32_t p = 0; p < kCellTableProbes; ++p) {
+            uint32_t k = __ldcg(T.key + s);  // from L2: keys are claimed while the join runs
+            if (k == kCellEmpty) {
+                const uint32_t old = atomicCAS(T.key + s, kCellEmpty, cell);
+                k = old == kCellEmpty ? cell : old;
+            }
+            if (k == cell) {
+                atomicAdd(T.acc + 2 * (size_t)s, inc_ctx(d));
+                if (d)
+                    atomicAdd(T.acc + 2 * (size_t)s + 1, inc_obj(d));
+                return;
+            }
+            s = (s + 1) & mask;
         }
-    } else {
-        credit_lower(oc, oo, qg, rg, d);
+    }
+    credit_lower(oc, oo, qg, rg, d);
+}
+
+// The table's cells into the triangle (plain adds: a cell lives in one slot and the join
+// has finished), slots emptied for the next call.
+__global__ void k_cell_table_flush(uint32_t *__restrict__ key, unsigned long long *__restrict__ acc, uint32_t slots,
+                                   unsigned long long *__restrict__ oc, unsigned long long *__restrict__ oo)
+{
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < slots; s += gridDim.x * blockDim.x) {
+        const uint32_t cell = key[s];
+        if (cell == kCellEmpty)
+            continue;
+        const ulonglong2 a = reinterpret_cast<const ulonglong2 *>(acc)[s];
+        oc[cell] += a.x;
+        if (a.y)
+            oo[cell] += a.y;
+        key[s] = kCellEmpty;
+        reinterpret_cast<ulonglong2 *>(acc)[s] = make_ulonglong2(0, 0);
     }
 }
 
@@ -1607,65 +1640,106 @@ __device__ __forceinline__ void pair_of_rank(uint32_t t, uint32_t &i, uint32_t &
     i = t - j * (j - 1) / 2;
 }
 
-// Per tile: every thread loads 16 group bounds (coalesced, all in flight), block scans
-// place its shared groups in the queue.  PAIRS (a conflict-free index: one object per
-// gid run): the small groups' pairs are then dealt out evenly, thread t taking a
-// contiguous range of the tile's pair ranks, so every lane runs the same short
-// sequence per pair and no thread walks a whole large group while the others wait;
-// with conflicts every thread walks whole groups (run cross products).  Groups of more
-// than kScanLaneMax postings are taken by the whole CTA.
-template <bool PAIRS>
-__global__ void __launch_bounds__(kScanThreads, 3) k_self_scan(const uint32_t *__restrict__ gbeg, uint64_t u,
+// The same for the pairs of a large group (ranks up to 2^32, 64-bit arithmetic).
+__device__ __forceinline__ void pair_of_rank_wide(uint32_t t, uint32_t &i, uint32_t &j)
+{
+    uint64_t jj = (uint64_t)((1.0 + sqrt(1.0 + 8.0 * (double)t)) * 0.5);
+    while (jj * (jj - 1) / 2 > t)
+        --jj;
+    while ((jj + 1) * jj / 2 <= t)
+        ++jj;
+    j = (uint32_t)jj;
+    i = (uint32_t)(t - jj * (jj - 1) / 2);
+}
+
+// Bounds of this thread's groups of tile t: groups g0 .. g0 + kScanPerThread - 1
+// (contiguous per thread, so a warp reads one 1 KB span with 16-byte loads), the
+// kScanPerThread + 1 values gbeg[g0 ..]; past the end they repeat gbeg[u] (empty groups).
+__device__ __forceinline__ void scan_load_bounds(const uint32_t *__restrict__ gbeg, uint64_t u, uint64_t t,
+                                                 uint32_t (&bnd)[kScanPerThread + 1])
+{
+    const uint64_t g0 = t * kScanTile + (uint64_t)threadIdx.x * kScanPerThread;
+    if (g0 + kScanPerThread <= u) {
+        const uint4 *v = reinterpret_cast<const uint4 *>(gbeg + g0);
+#pragma unroll
+        for (uint32_t j = 0; j < kScanPerThread / 4; ++j) {
+            const uint4 w = __ldg(v + j);
+            bnd[4 * j] = w.x;
+            bnd[4 * j + 1] = w.y;
+            bnd[4 * j + 2] = w.z;
+            bnd[4 * j + 3] = w.w;
+        }
+        bnd[kScanPerThread] = __ldg(gbeg + g0 + kScanPerThread);
+    } else {
+#pragma unroll
+        for (uint32_t j = 0; j <= kScanPerThread; ++j)
+            bnd[j] = __ldg(gbeg + min(g0 + j, u));
+    }
+}
+
+// Per tile: every thread holds the bounds of kScanPerThread contiguous groups (loaded
+// while the previous tile was joined), one block scan places the tile's shared groups
+// in the queue.  PAIRS (a conflict-free index: one object per gid run): the small
+// groups' pairs are then dealt out evenly, thread t taking a contiguous range of the
+// tile's pair ranks and loading the postings of up to kScanPairBatch pairs before it
+// credits them, so every lane runs the same short sequence per pair and no thread
+// walks a whole large group while the others wait; with conflicts every thread walks
+// whole groups (run cross products).  Groups of more than kScanLaneMax postings are
+// taken by the whole CTA.
+#ifndef KSSD_SCAN_PAIR_BATCH
+#define KSSD_SCAN_PAIR_BATCH 4
+#endif
+constexpr uint32_t kScanPairBatch = KSSD_SCAN_PAIR_BATCH;
+static_assert(kScanPerThread % 4 == 0, "contiguous bounds are loaded 4 at a time");
+
+#ifndef KSSD_SCAN_MINB_L2
+#define KSSD_SCAN_MINB_L2 3
+#endif
+#ifndef KSSD_SCAN_MINB_BIG
+#define KSSD_SCAN_MINB_BIG 4
+#endif
+template <bool PAIRS, int MINB>
+__global__ void __launch_bounds__(kScanThreads, MINB) k_self_scan(const uint32_t *__restrict__ gbeg, uint64_t u,
                                                             const uint64_t *__restrict__ post, int ignoreconflict,
-                                                            bool use_cache, unsigned long long *__restrict__ oc,
+                                                            CellTable table,
+                                                            unsigned long long *__restrict__ oc,
                                                             unsigned long long *__restrict__ oo)
 {
     extern __shared__ __align__(16) unsigned char scan_smem[];
     ScanSmem &S = *reinterpret_cast<ScanSmem *>(scan_smem);
-    using Scan = cub::BlockScan<uint32_t, kScanThreads>;
+    using Scan = cub::BlockScan<unsigned long long, kScanThreads>;
     __shared__ typename Scan::TempStorage scan_tmp;
     const uint64_t ntiles = (u + kScanTile - 1) / kScanTile;
     bool waited = false;
-    const bool cache = PAIRS && KSSD_SCAN_CACHE && use_cache;
-    if (cache) {
-        for (uint32_t i = threadIdx.x; i < kCellCache; i += kScanThreads) {
-            S.cell[i] = kCellEmpty;
-            S.nc[i] = S.m2[i] = S.dobj[i] = S.sect[i] = 0;
-        }
-    }
+    uint32_t bnd[kScanPerThread + 1];
+    if (blockIdx.x < ntiles)
+        scan_load_bounds(gbeg, u, blockIdx.x, bnd);
     for (uint64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
-        const uint64_t base = t * kScanTile;
-        uint32_t beg[kScanPerThread], cnt[kScanPerThread];
+        // the next tile's bounds are in flight while this tile is joined
+        uint32_t nxt[kScanPerThread + 1];
+        if (t + gridDim.x < ntiles)
+            scan_load_bounds(gbeg, u, t + gridDim.x, nxt);
+        // this thread's small groups (bits 0-15), large groups (bits 16-31) and small
+        // pairs (bits 32-63): at most 2,048 x 2 groups and 2,048 x 496 pairs per tile,
+        // so one 64-bit scan carries all three without overflow between the fields
+        uint32_t cnt[kScanPerThread];
+        unsigned long long mine = 0;
 #pragma unroll
         for (uint32_t j = 0; j < kScanPerThread; ++j) {
-            const uint64_t g = base + j * kScanThreads + threadIdx.x;
-            beg[j] = 0;
-            cnt[j] = 0;
-            if (g < u) {
-                beg[j] = __ldg(gbeg + g);
-                cnt[j] = __ldg(gbeg + g + 1);
-            }
-        }
-        // this thread's small / large shared groups (low / high 16 bits) and small pairs
-        uint32_t mine = 0, my_pairs = 0;
-#pragma unroll
-        for (uint32_t j = 0; j < kScanPerThread; ++j) {
-            const uint32_t k = cnt[j] - beg[j];
+            const uint32_t k = bnd[j + 1] - bnd[j];
             cnt[j] = k;
             const bool small = k >= 2 && k <= kScanLaneMax;
-            mine += small ? 1u : (k > kScanLaneMax ? 0x10000u : 0u);
-            my_pairs += small ? k * (k - 1) / 2 : 0u;
+            mine += small ? (1ull | ((unsigned long long)(k * (k - 1) / 2) << 32))
+                          : (k > kScanLaneMax ? 0x10000ull : 0ull);
         }
-        uint32_t off, tot, poff, ptot;
+        unsigned long long off, tot;
         Scan(scan_tmp).ExclusiveSum(mine, off, tot);
-        __syncthreads();
-        if (PAIRS)
-            Scan(scan_tmp).ExclusiveSum(my_pairs, poff, ptot);
-        uint32_t sl = off & 0xFFFFu, ll = off >> 16;
+        uint32_t sl = (uint32_t)off & 0xFFFFu, ll = ((uint32_t)off >> 16) & 0xFFFFu;
+        uint32_t poff = (uint32_t)(off >> 32);
 #pragma unroll
         for (uint32_t j = 0; j < kScanPerThread; ++j) {
             const uint32_t k = cnt[j];
-            const unsigned long long item = (unsigned long long)beg[j] | ((unsigned long long)k << 32);
+            const unsigned long long item = (unsigned long long)bnd[j] | ((unsigned long long)k << 32);
             if (k >= 2 && k <= kScanLaneMax) {
                 S.queue[sl] = item;
                 if (PAIRS) {
@@ -1679,13 +1753,13 @@ __global__ void __launch_bounds__(kScanThreads, 3) k_self_scan(const uint32_t *_
             }
         }
         __syncthreads();
-        const uint32_t nl = tot & 0xFFFFu, nc = tot >> 16;
+        const uint32_t nl = (uint32_t)tot & 0xFFFFu, nc = ((uint32_t)tot >> 16) & 0xFFFFu;
         if (!waited) {
             pdl_wait_primary();  // the counters' zero fill has finished (no-op without a dependency)
             waited = true;
         }
         if (PAIRS) {
-            const uint32_t total = ptot;
+            const uint32_t total = (uint32_t)(tot >> 32);
             const uint32_t p0 = (uint32_t)((uint64_t)total * threadIdx.x / kScanThreads);
             const uint32_t p1 = (uint32_t)((uint64_t)total * (threadIdx.x + 1) / kScanThreads);
             if (p0 < p1) {
@@ -1699,18 +1773,27 @@ __global__ void __launch_bounds__(kScanThreads, 3) k_self_scan(const uint32_t *_
                         hi = mid - 1;
                 }
                 uint32_t q = lo;
-                for (uint32_t pr = p0; pr < p1; ++pr) {
-                    while (q + 1 < nl && S.prefix[q + 1] <= pr)
-                        ++q;
-                    const unsigned long long item = S.queue[q];
-                    uint32_t i, j;
-                    pair_of_rank(pr - S.prefix[q], i, j);
-                    const uint64_t pi = __ldg(post + (uint32_t)item + i), pj = __ldg(post + (uint32_t)item + j);
-                    const int d = min(kMinInit, dna_pop((uint32_t)pi ^ (uint32_t)pj));
-                    if (cache)
-                        credit_cached(S, oc, oo, (uint32_t)(pj >> 32), (uint32_t)(pi >> 32), d);
-                    else
-                        credit_lower(oc, oo, (uint32_t)(pj >> 32), (uint32_t)(pi >> 32), d);
+                for (uint32_t pr = p0; pr < p1; pr += kScanPairBatch) {
+                    uint64_t pi[kScanPairBatch], pj[kScanPairBatch];
+#pragma unroll
+                    for (uint32_t x = 0; x < kScanPairBatch; ++x) {
+                        if (pr + x < p1) {
+                            while (q + 1 < nl && S.prefix[q + 1] <= pr + x)
+                                ++q;
+                            const unsigned long long item = S.queue[q];
+                            uint32_t i, j;
+                            pair_of_rank(pr + x - S.prefix[q], i, j);
+                            pi[x] = __ldg(post + (uint32_t)item + i);
+                            pj[x] = __ldg(post + (uint32_t)item + j);
+                        }
+                    }
+#pragma unroll
+                    for (uint32_t x = 0; x < kScanPairBatch; ++x) {
+                        if (pr + x < p1) {
+                            const int d = min(kMinInit, dna_pop((uint32_t)pi[x] ^ (uint32_t)pj[x]));
+                            credit_global(table, oc, oo, (uint32_t)(pj[x] >> 32), (uint32_t)(pi[x] >> 32), d);
+                        }
+                    }
                 }
             }
         } else {
@@ -1721,21 +1804,25 @@ __global__ void __launch_bounds__(kScanThreads, 3) k_self_scan(const uint32_t *_
         }
         for (uint32_t i = 0; i < nc; ++i) {
             const unsigned long long item = S.queue[kScanTile - 1 - i];
-            join_group_cta(post, (uint32_t)item, (uint32_t)(item >> 32), ignoreconflict, oc, oo);
+            const uint32_t b = (uint32_t)item, k = (uint32_t)(item >> 32);
+            if (PAIRS && table.key) {
+                // one object per gid: the group's pairs dealt out over the CTA, into the table
+                const uint32_t np = (uint32_t)((uint64_t)k * (k - 1) / 2);  // k < 92,682 genomes
+                for (uint32_t pr = threadIdx.x; pr < np; pr += kScanThreads) {
+                    uint32_t x, y;
+                    pair_of_rank_wide(pr, x, y);
+                    const uint64_t px = __ldg(post + b + x), py = __ldg(post + b + y);
+                    credit_global(table, oc, oo, (uint32_t)(py >> 32), (uint32_t)(px >> 32),
+                                  min(kMinInit, dna_pop((uint32_t)px ^ (uint32_t)py)));
+                }
+            } else {
+                join_group_cta(post, b, k, ignoreconflict, oc, oo);
+            }
         }
         __syncthreads();  // the queue and the scan storage are reused by the next tile
-    }
-    if (cache && waited) {
-        // the cached cells into the triangle (only CTAs that took a tile waited for the fill
-        // and can hold claimed cells)
-        for (uint32_t i = threadIdx.x; i < kCellCache; i += kScanThreads) {
-            const uint32_t cell = S.cell[i];
-            if (cell == kCellEmpty)
-                continue;
-            atomicAdd(oc + cell, (unsigned long long)S.nc[i] | ((unsigned long long)S.m2[i] << 32));
-            if (S.dobj[i])
-                atomicAdd(oo + cell, (unsigned long long)S.dobj[i] | ((unsigned long long)S.sect[i] << 32));
-        }
+#pragma unroll
+        for (uint32_t j = 0; j <= kScanPerThread; ++j)
+            bnd[j] = nxt[j];
     }
 }
 
@@ -2337,7 +2424,10 @@ struct kssdgpu_index {
     uint32_t j_n[3] = {0, 0, 0};
     unsigned long long j_postings = 0, j_pairs = 0;
     bool j_ready = false;
-    int scan_grid = 0;                      // CTAs of the one-pass scan join (resident per SM x SMs)
+    int scan_grid[2] = {0, 0};              // CTAs of the one-pass scan join (resident per SM x SMs), per mode
+    DevBuf<uint32_t> c_key;                 // scan join: table of touched cells (empty between calls)
+    int c_log = kCellTableLog;              // its 2^c_log slots (KSSDGPU_CELL_TABLE_LOG, read at its allocation)
+    DevBuf<unsigned long long> c_acc;       // scan join: its counter words
     // facts of the index, from one pass at build: shared groups (>= 2 postings), their
     // postings and pairs, whether any gid run holds several objects (a conflict)
     unsigned long long f_groups = 0, f_postings = 0, f_pairs = 0;
@@ -3593,13 +3683,34 @@ int self_scan_impl(kssdgpu_index *ix, unsigned flags, unsigned long long *oc, un
     const size_t cells = (size_t)ix->nref * (ix->nref - 1) / 2;
     if (!cells)
         return KSSDGPU_OK;
+    // a conflict-free index deals out pairs; with conflicts threads walk whole groups
+    const bool pairs = !ix->f_conflict;
+    // Triangles larger than L2 (and of 32-bit cell numbers: at most 92,681 genomes) add
+    // through the table of touched cells (allocated on first use, kept empty between
+    // calls), with four CTAs per SM; with the counters in L2 the table's probes cost more
+    // than they save (2,000 genomes: 0.19 vs 0.14 ms per step) and the join adds into the
+    // triangle directly, three CTAs per SM.
+    const bool big = cells < (size_t)kCellEmpty && cells * 16 > (size_t)ix->l2_bytes;
+    CellTable table{nullptr, nullptr, 0};
+    if (ix->u && pairs && big) {
+        if (!ix->c_key.p || !ix->c_acc.p)
+            ix->c_log = (int)env_u32("KSSDGPU_CELL_TABLE_LOG", kCellTableLog, 4, 26);
+        const size_t slots = (size_t)1 << ix->c_log;
+        if (!ix->c_key.p || !ix->c_acc.p) {
+            CUDA_TRY(ix->c_key.ensure(slots));
+            CUDA_TRY(ix->c_acc.ensure(2 * slots));
+            CUDA_TRY(cudaMemsetAsync(ix->c_key.p, 0xFF, slots * 4, st));
+            CUDA_TRY(cudaMemsetAsync(ix->c_acc.p, 0, slots * 16, st));
+        }
+        table = CellTable{ix->c_key.p, ix->c_acc.p, ix->c_log};
+    }
     bool after_fill = false;
     if (!(flags & KSSDGPU_NO_ZERO)) {
         if ((((uintptr_t)oc | (uintptr_t)oo) & 15) == 0) {
             k_zero_pair<<<ix->sms * 8, 256, 0, st>>>(oc, oo, cells);
             count_launch();
-            CUDA_TRY(cudaGetLastError());
             after_fill = cells * 16 <= (size_t)ix->l2_bytes;
+            CUDA_TRY(cudaGetLastError());
         } else {
             CUDA_TRY(cudaMemsetAsync(oc, 0, cells * 8, st));
             CUDA_TRY(cudaMemsetAsync(oo, 0, cells * 8, st));
@@ -3607,20 +3718,19 @@ int self_scan_impl(kssdgpu_index *ix, unsigned flags, unsigned long long *oc, un
     }
     if (!ix->u)
         return KSSDGPU_OK;
-    // a conflict-free index deals out pairs; with conflicts threads walk whole groups
-    const bool pairs = !ix->f_conflict;
-    auto kern = pairs ? k_self_scan<true> : k_self_scan<false>;
+    const int mode = table.key ? 1 : 0;
+    auto kern = mode ? (pairs ? k_self_scan<true, KSSD_SCAN_MINB_BIG> : k_self_scan<false, KSSD_SCAN_MINB_BIG>)
+                     : (pairs ? k_self_scan<true, KSSD_SCAN_MINB_L2> : k_self_scan<false, KSSD_SCAN_MINB_L2>);
     const size_t smem = sizeof(ScanSmem);
-    if (!ix->scan_grid) {
-        CUDA_TRY(cudaFuncSetAttribute(k_self_scan<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        CUDA_TRY(cudaFuncSetAttribute(k_self_scan<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (!ix->scan_grid[mode]) {
+        CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         int per_sm = 0;
-        CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_self_scan<true>, kScanThreads, smem));
-        ix->scan_grid = std::max(1, per_sm) * ix->sms;
+        CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kScanThreads, smem));
+        ix->scan_grid[mode] = std::max(1, per_sm) * ix->sms;
     }
     const uint64_t ntiles = (ix->u + kScanTile - 1) / kScanTile;
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3((unsigned)std::min<uint64_t>(ntiles, (uint64_t)ix->scan_grid));
+    cfg.gridDim = dim3((unsigned)std::min<uint64_t>(ntiles, (uint64_t)ix->scan_grid[mode]));
     cfg.blockDim = dim3(kScanThreads);
     cfg.dynamicSmemBytes = smem;
     cfg.stream = st;
@@ -3631,15 +3741,15 @@ int self_scan_impl(kssdgpu_index *ix, unsigned flags, unsigned long long *oc, un
         cfg.attrs = attr;
         cfg.numAttrs = 1;
     }
-    // The cell cache holds 32-bit cell numbers (triangles of at most 92,681 genomes) and
-    // pays where the counters outgrow L2: 20,000 genomes 2.78 ms per step with it vs 2.98
-    // without; with the counters in L2 its shared-memory adds cost more than they save
-    // (2,000 genomes: 0.19 vs 0.15 ms).
-    const bool use_cache = cells < (size_t)kCellEmpty && cells * 16 > (size_t)ix->l2_bytes;
     CUDA_TRY(cudaLaunchKernelEx(&cfg, kern, (const uint32_t *)ix->gbeg, ix->u, (const uint64_t *)ix->post,
-                                (flags & KSSDGPU_IGNORECONFLICT) ? 1 : 0, use_cache, oc, oo));
+                                (flags & KSSDGPU_IGNORECONFLICT) ? 1 : 0, table, oc, oo));
     count_launch();
     CUDA_TRY(cudaGetLastError());
+    if (table.key) {
+        k_cell_table_flush<<<ix->sms * 4, 256, 0, st>>>(table.key, table.acc, 1u << table.log, oc, oo);
+        count_launch();
+        CUDA_TRY(cudaGetLastError());
+    }
     return KSSDGPU_OK;
 }
 
@@ -4253,6 +4363,8 @@ void kssdgpu_index_free(kssdgpu_index_t *ix)
     ix->s_counts.release();
     ix->s_cubtmp.release();
     ix->j_small.release();
+    ix->c_key.release();
+    ix->c_acc.release();
     ix->j_post.release();
     ix->j_chunks.release();
     ix->j_items.release();

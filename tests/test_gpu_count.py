@@ -650,15 +650,40 @@ def test_self_dense_join_wide_objects_and_conflicts():
     assert idx.self_choice()[0] == kssdgpu.PATH_SCAN
 
 
-def test_self_scan_with_counters_beyond_l2():
-    """6,000 small genomes: the packed triangle (18M cells, 288 MB) outgrows L2, so the scan
-    join adds through its per-CTA cell cache; the counters still equal the oracle's."""
-    sk = kssdgpu.synth(n_samples=6000, n_clusters=600, len_median=8e4, len_min=5e4, len_max=1.5e5,
-                       size_dist=kssdgpu.SIZE_LOGNORMAL, sub_lo=0.001, sub_hi=0.1, seed=71, sample_seed=71)
+@pytest.mark.parametrize("n,clusters,table_log", [(6000, 600, None), (4500, 50, None), (4500, 50, 4)])
+def test_self_scan_with_counters_beyond_l2(n, clusters, table_log, monkeypatch):
+    """Small genomes whose packed triangle (4,500 genomes: 10M cells, 162 MB) outgrows
+    L2: the scan join adds through the table of touched cells and flushes it into the
+    triangle.  Clusters of 90 genomes give context groups of more than 32 postings (dealt
+    out over the CTA, into the table); a table of 16 slots sends nearly every cell to the
+    triangle directly.  The counters equal the oracle's on two calls in a row (the flush
+    empties the table), and a NO_ZERO call adds onto the previous counters."""
+    import torch
+    if table_log is not None:
+        monkeypatch.setenv("KSSDGPU_CELL_TABLE_LOG", str(table_log))
+    sk = kssdgpu.synth(n_samples=n, n_clusters=clusters, len_median=8e4, len_min=5e4, len_max=1.5e5,
+                       size_dist=kssdgpu.SIZE_LOGNORMAL, sub_lo=0.001, sub_hi=0.1, seed=71 + clusters,
+                       sample_seed=71 + clusters)
     rec = oracle.build_index(sk.keys, sk.offs)
     idx = kssdgpu.Index.from_records(rec, sk.n)
     want = oracle.self_lower_all(rec, sk.keys, sk.offs)
-    got = idx.self_lower(kssdgpu.SELF_SCAN)
-    np.testing.assert_array_equal(got[0], want[0])
-    np.testing.assert_array_equal(got[1], want[1])
+    for _ in range(2):
+        got = idx.self_lower(kssdgpu.SELF_SCAN)
+        np.testing.assert_array_equal(got[0], want[0])
+        np.testing.assert_array_equal(got[1], want[1])
     assert want[0][:, 0].sum() > 0
+    if clusters == 50:
+        _, sizes = np.unique(rec["ctxgid"] >> 20, return_counts=True)
+        assert sizes.max() > 32  # groups of more than 32 postings are present
+    cells = n * (n - 1) // 2
+    dev = torch.device("cuda", 0)
+    lc = torch.zeros(cells, dtype=torch.int64, device=dev)
+    lo = torch.zeros_like(lc)
+    idx.self_lower_dev(lc, lo, flags=kssdgpu.SELF_SCAN)
+    idx.self_lower_dev(lc, lo, flags=kssdgpu.SELF_SCAN | kssdgpu.NO_ZERO)
+    idx.sync()
+    got_c = lc.cpu().numpy().view(np.uint32).reshape(cells, 2)
+    got_o = lo.cpu().numpy().view(np.uint32).reshape(cells, 2)
+    np.testing.assert_array_equal(got_c, 2 * want[0].reshape(cells, 2))
+    np.testing.assert_array_equal(got_o, 2 * want[1].reshape(cells, 2))
+    idx.close()
