@@ -1,6 +1,7 @@
 """Small, self-contained launches of the hot kernels for one-kernel ncu captures.
 
     python kssd3a-public_b200/profile_cases.py scan    # 2,000-genome self join, 3 scan-join steps
+    python kssd3a-public_b200/profile_cases.py scanbig # 5,000 small genomes: triangle beyond L2 (cell table)
     python kssd3a-public_b200/profile_cases.py dense   # 512-genome one-species dense join, 2 steps
     python kssd3a-public_b200/profile_cases.py rect    # 2,000 queries x 4,000 references, 4 batched counts
 
@@ -37,6 +38,24 @@ def case_scan(dev, st):
     for _ in range(3):
         idx.self_lower_dev(a, b, flags=kssdgpu.SELF_SCAN, stream=st)
     torch.cuda.synchronize()
+    idx.close()
+
+
+def case_scanbig(dev, st):
+    """5,000 genomes of 0.5-2 Mbp: the packed triangle (12.5M cells, 200 MB) is larger than
+    L2, so the scan join adds through its table of touched cells; about 1 GB on the device."""
+    n = 5000
+    sk = kssdgpu.synth(n_samples=n, n_clusters=n // 10, size_dist=kssdgpu.SIZE_LOGNORMAL, len_median=1e6,
+                       len_sigma=0.37, len_min=5e5, len_max=2e6, sub_lo=0.001, sub_hi=0.2, seed=20261203 + 2,
+                       sample_seed=20261203 + 2, threads=THREADS)
+    idx = kssdgpu.Index.from_sketch(sk)
+    cells = n * (n - 1) // 2
+    a = torch.zeros(cells, dtype=torch.int64, device=dev)
+    b = torch.zeros_like(a)
+    for _ in range(3):
+        idx.self_lower_dev(a, b, flags=kssdgpu.SELF_SCAN, stream=st)
+    torch.cuda.synchronize()
+    print("entries", int(sk.offs[-1]))
     idx.close()
 
 
@@ -77,10 +96,10 @@ def case_rect(dev, st):
 
 
 def main(argv):
-    cases = {"scan": case_scan, "dense": case_dense, "rect": case_rect}
+    cases = {"scan": case_scan, "scanbig": case_scanbig, "dense": case_dense, "rect": case_rect}
     which = argv[1] if len(argv) > 1 else ""
     if which not in cases:
-        print("usage: profile_cases.py scan|dense|rect", file=sys.stderr)
+        print("usage: profile_cases.py scan|scanbig|dense|rect", file=sys.stderr)
         return 64
     if not torch.cuda.is_available():
         print("profile_cases.py: needs a CUDA device", file=sys.stderr)
