@@ -272,6 +272,80 @@ int kssdgpu_self_lower_dev(kssdgpu_index_t *idx, unsigned flags, kssdgpu_ctx_mut
                            kssdgpu_obj_section_t *d_obj_lower, void *stream);
 
 /*
+ * Matrix values on the device: the FP64 epilogue that turns the counters of every
+ * cell of a packed lower triangle into the value a `kssd3a ani --format
+ * matrix|triangle` output prints for it -- the per-pair metric of
+ * ani_indexed_self_pair_metric / ani_matrix_pair_value (src/command_ani.c:1458-1496,
+ * 1627-1655): lm3ways distance (src/model_ani.h:285-305), naive and p distances
+ * (src/command_ani.h:202-232), Mash and AAF distances (src/command_matrix.c:26-33), the
+ * 160-tree calibration (src/model_refaf_hgb.h:7593-7628), the selected metric and the
+ * exception value (src/command_ani.c:1186-1379, 1448-1456).  Every + - * / is the
+ * reference's IEEE double operation in its order (no contraction), so a value built
+ * from them alone (lm3ways, the calibration trees, p_dist) is bit-identical to the
+ * reference's.  log, log1p and pow (CUDA's, whose last bits may differ from a host
+ * libm's) enter the Naive, Mash and AAF values and three calibration features; those
+ * values print the reference's six decimals, except where the difference could change
+ * what is printed: a calibration feature within 1e-9 (relative) of a tree threshold on
+ * the cell's path, or a Naive / Mash / AAF value within 1e-12 of a rounding boundary of
+ * its six printed decimals or of zero.  Such cells are not valued on the device: their
+ * value is a NaN and they are listed (cell, counters) for the caller to recompute on
+ * the host.
+ */
+typedef struct kssdgpu_metric_opt {
+    int s;              /* selected metric 1..9 (BestDist .. p_dist); negative: print 1 - distance */
+    int e;              /* exception value (no sketch on one side, failed AF gate) */
+    int v;              /* ANI from the naive model instead of lm3ways */
+    int unassembled;    /* --qraw query mode */
+    int unified_metric; /* --unified-metric */
+    int raw_output;     /* no calibration */
+    float afcut;        /* AF gate */
+    int drfold;         /* the sketch's drfold (model feature scale) */
+    int obj_bits;       /* object width (p_dist) */
+    int ctx_bits;       /* context width (Mash / AAF k = ctx_bits / 2) */
+    int zero_const;     /* cells with no shared context and both sketch sizes nonzero take zero_value */
+    double zero_value;
+    /* the calibration trees (the 11-coden build's model; the 9- and 10-coden builds have
+     * none): node records of 16 bytes {double x; int8 feature; uint8 flags (bit 0 leaf,
+     * bit 1 a NaN input goes left); uint16 left, right (relative to the tree's first
+     * node)}, the first node of every tree (hgb_trees + 1 offsets), the baseline */
+    const void *hgb_nodes;
+    uint32_t hgb_nodes_count;
+    const uint32_t *hgb_tree_begin;
+    uint32_t hgb_trees;
+    double hgb_baseline;
+} kssdgpu_metric_opt_t;
+
+/* A cell the caller values on the host: its lower-triangle number q*(q-1)/2 + r and its
+ * counters. */
+typedef struct kssdgpu_recheck {
+    uint64_t cell;
+    kssdgpu_ctx_mut2_t ctx;
+    kssdgpu_obj_section_t obj;
+} kssdgpu_recheck_t;
+
+/* Device form over any packed lower triangle of n samples: d_qcnt / d_rcnt are the
+ * samples' sketch sizes as query / as reference (n each), the counters d_ctx_lower /
+ * d_obj_lower (n(n-1)/2 each); writes d_value_lower (n(n-1)/2 doubles), the first
+ * recheck_cap listed cells to d_recheck and their number to *d_nrecheck (zeroed by the
+ * call).  Stream-ordered on `stream` of `device`; the calibration trees are copied to the
+ * device once per device and model. */
+int kssdgpu_lower_metric_dev(int device, const kssdgpu_metric_opt_t *opt, int n, const uint32_t *d_qcnt,
+                             const uint32_t *d_rcnt, const kssdgpu_ctx_mut2_t *d_ctx_lower,
+                             const kssdgpu_obj_section_t *d_obj_lower, double *d_value_lower,
+                             kssdgpu_recheck_t *d_recheck, uint64_t recheck_cap, uint64_t *d_nrecheck,
+                             void *stream);
+
+/* The self matrix of an index's own samples with its values from the device: the self
+ * join of kssdgpu_self_lower (flags alike), then the device epilogue above; host buffers
+ * (qcnt / rcnt: n sketch sizes; value_lower: n(n-1)/2 doubles; recheck: recheck_cap
+ * entries), synchronous.  *nrecheck = the listed cells; more than recheck_cap returns
+ * KSSDGPU_ERR_CAPACITY (the values of the other cells are written).  Moves 8 bytes per
+ * cell to the host instead of kssdgpu_self_lower's 16. */
+int kssdgpu_self_lower_metric(kssdgpu_index_t *idx, unsigned flags, const kssdgpu_metric_opt_t *opt,
+                              const uint32_t *qcnt, const uint32_t *rcnt, double *value_lower,
+                              kssdgpu_recheck_t *recheck, uint64_t recheck_cap, uint64_t *nrecheck);
+
+/*
  * Facts of the self join, from one pass over the index (no plan is built): context
  * groups holding >= 2 postings, postings inside them, and their posting pairs
  * (k(k-1)/2 per group of k).  These size the join's algorithmic bytes.

@@ -11,6 +11,7 @@
 // Counting semantics follow src/command_ani.h:463-721 (see walk_context below).
 #include "kssdgpu.h"
 #include "kssd_dev.cuh"
+#include "kssd_metric.cuh"
 
 #include <cub/cub.cuh>
 #include <cub/device/device_segmented_sort.cuh>
@@ -2425,6 +2426,9 @@ struct kssdgpu_index {
     unsigned long long j_postings = 0, j_pairs = 0;
     bool j_ready = false;
     int scan_grid[2] = {0, 0};              // CTAs of the one-pass scan join (resident per SM x SMs), per mode
+    DevBuf<double> m_val;                   // self matrix values (kssdgpu_self_lower_metric)
+    DevBuf<kssd::RecheckCell> m_recheck;    // cells the host values
+    DevBuf<unsigned long long> m_nrecheck;
     DevBuf<uint32_t> c_key;                 // scan join: table of touched cells (empty between calls)
     int c_log = kCellTableLog;              // its 2^c_log slots (KSSDGPU_CELL_TABLE_LOG, read at its allocation)
     DevBuf<unsigned long long> c_acc;       // scan join: its counter words
@@ -4012,6 +4016,69 @@ int noalloc_scratch(int device, unsigned int **out)
 
 // ------------------------------------------------------------------ C ABI
 
+// Device copies of the calibration trees, one per device, replaced when a call passes
+// another model.
+struct HgbDeviceModel {
+    const void *host_nodes = nullptr;
+    uint32_t nodes = 0, trees = 0;
+    kssd::HgbNode *d_nodes = nullptr;
+    uint32_t *d_begin = nullptr;
+};
+static std::mutex g_hgb_mu;
+static std::vector<HgbDeviceModel> g_hgb;
+
+static int metric_params(int device, const kssdgpu_metric_opt_t *o, kssd::MetricParams &P)
+{
+    if (!o)
+        return fail(KSSDGPU_ERR_ARG, "null metric options");
+    if (o->hgb_trees && (!o->hgb_nodes || !o->hgb_tree_begin || !o->hgb_nodes_count))
+        return fail(KSSDGPU_ERR_ARG, "calibration trees without their nodes");
+    P = kssd::MetricParams{};
+    P.s = o->s;
+    P.e = o->e;
+    P.v = o->v;
+    P.unassembled = o->unassembled;
+    P.unified_metric = o->unified_metric;
+    P.raw_output = o->raw_output;
+    P.afcut = o->afcut;
+    P.drfold = o->drfold;
+    P.obj_bits = o->obj_bits;
+    P.ctx_bits = o->ctx_bits;
+    P.zero_const = o->zero_const;
+    P.zero_value = o->zero_value;
+    P.baseline = o->hgb_baseline;
+    P.ntrees = (int)o->hgb_trees;
+    if (!o->hgb_trees)
+        return KSSDGPU_OK;
+    for (uint32_t t = 0; t < o->hgb_trees; ++t)
+        if (o->hgb_tree_begin[t] >= o->hgb_tree_begin[t + 1] || o->hgb_tree_begin[t + 1] > o->hgb_nodes_count)
+            return fail(KSSDGPU_ERR_ARG, "calibration tree offsets out of range");
+    std::lock_guard<std::mutex> lock(g_hgb_mu);
+    if ((int)g_hgb.size() <= device)
+        g_hgb.resize(device + 1);
+    HgbDeviceModel &m = g_hgb[device];
+    if (m.host_nodes != o->hgb_nodes || m.nodes != o->hgb_nodes_count || m.trees != o->hgb_trees) {
+        if (m.d_nodes)
+            cudaFree(m.d_nodes);
+        if (m.d_begin)
+            cudaFree(m.d_begin);
+        m = HgbDeviceModel{};
+        CUDA_TRY(cudaMalloc(&m.d_nodes, (size_t)o->hgb_nodes_count * sizeof(kssd::HgbNode)));
+        CUDA_TRY(cudaMalloc(&m.d_begin, ((size_t)o->hgb_trees + 1) * sizeof(uint32_t)));
+        CUDA_TRY(cudaMemcpy(m.d_nodes, o->hgb_nodes, (size_t)o->hgb_nodes_count * sizeof(kssd::HgbNode),
+                            cudaMemcpyHostToDevice));
+        CUDA_TRY(cudaMemcpy(m.d_begin, o->hgb_tree_begin, ((size_t)o->hgb_trees + 1) * sizeof(uint32_t),
+                            cudaMemcpyHostToDevice));
+        m.host_nodes = o->hgb_nodes;
+        m.nodes = o->hgb_nodes_count;
+        m.trees = o->hgb_trees;
+    }
+    P.nodes = m.d_nodes;
+    P.tree_begin = m.d_begin;
+    P.nnodes = m.nodes;
+    return KSSDGPU_OK;
+}
+
 extern "C" {
 
 const char *kssdgpu_last_error(void) { return g_last_error.c_str(); }
@@ -4365,6 +4432,9 @@ void kssdgpu_index_free(kssdgpu_index_t *ix)
     ix->j_small.release();
     ix->c_key.release();
     ix->c_acc.release();
+    ix->m_val.release();
+    ix->m_recheck.release();
+    ix->m_nrecheck.release();
     ix->j_post.release();
     ix->j_chunks.release();
     ix->j_items.release();
@@ -4947,6 +5017,80 @@ int kssdgpu_self_lower_dev(kssdgpu_index_t *ix, unsigned flags, kssdgpu_ctx_mut2
     CUDA_TRY(cudaSetDevice(ix->device));
     return self_lower_dev_impl(ix, flags, reinterpret_cast<unsigned long long *>(d_ctx_lower),
                                reinterpret_cast<unsigned long long *>(d_obj_lower), (cudaStream_t)stream);
+}
+
+int kssdgpu_lower_metric_dev(int device, const kssdgpu_metric_opt_t *opt, int n, const uint32_t *d_qcnt,
+                             const uint32_t *d_rcnt, const kssdgpu_ctx_mut2_t *d_ctx_lower,
+                             const kssdgpu_obj_section_t *d_obj_lower, double *d_value_lower,
+                             kssdgpu_recheck_t *d_recheck, uint64_t recheck_cap, uint64_t *d_nrecheck, void *stream)
+{
+    if (n < 0 || !d_nrecheck || (n > 1 && (!d_qcnt || !d_rcnt || !d_ctx_lower || !d_obj_lower || !d_value_lower)) ||
+        (recheck_cap && !d_recheck))
+        return fail(KSSDGPU_ERR_ARG, "null argument or negative size");
+    static_assert(sizeof(kssdgpu_recheck_t) == sizeof(kssd::RecheckCell), "recheck records are 24 bytes");
+    CUDA_TRY(cudaSetDevice(device));
+    kssd::MetricParams P;
+    int rc = metric_params(device, opt, P);
+    if (rc)
+        return rc;
+    int sms = 148;
+    CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    cudaStream_t st = (cudaStream_t)stream;
+    CUDA_TRY(cudaMemsetAsync(d_nrecheck, 0, sizeof(uint64_t), st));
+    CUDA_TRY(kssd::lower_metric_launch(P, n, reinterpret_cast<const unsigned long long *>(d_ctx_lower),
+                                       reinterpret_cast<const unsigned long long *>(d_obj_lower), d_qcnt, d_rcnt,
+                                       d_value_lower, reinterpret_cast<kssd::RecheckCell *>(d_recheck), recheck_cap,
+                                       reinterpret_cast<unsigned long long *>(d_nrecheck), sms, st));
+    count_launch(n > 1 ? 1 : 0);
+    return KSSDGPU_OK;
+}
+
+int kssdgpu_self_lower_metric(kssdgpu_index_t *ix, unsigned flags, const kssdgpu_metric_opt_t *opt,
+                              const uint32_t *qcnt, const uint32_t *rcnt, double *value_lower,
+                              kssdgpu_recheck_t *recheck, uint64_t recheck_cap, uint64_t *nrecheck)
+{
+    if (!ix || !qcnt || !rcnt || !value_lower || !nrecheck || (recheck_cap && !recheck))
+        return fail(KSSDGPU_ERR_ARG, "null argument");
+    CUDA_TRY(cudaSetDevice(ix->device));
+    const int n = ix->nref;
+    const size_t cells = (size_t)n * (n - 1) / 2;
+    *nrecheck = 0;
+    if (!cells)
+        return KSSDGPU_OK;
+    kssd::MetricParams P;
+    int rc = metric_params(ix->device, opt, P);
+    if (rc)
+        return rc;
+    cudaStream_t st = 0;
+    CUDA_TRY(ix->s_out.ensure(cells * 2));
+    CUDA_TRY(ix->m_val.ensure(cells));
+    CUDA_TRY(ix->m_recheck.ensure(std::max<uint64_t>(recheck_cap, 1)));
+    CUDA_TRY(ix->m_nrecheck.ensure(1));
+    CUDA_TRY(ix->s_qcnt.ensure((size_t)n));
+    CUDA_TRY(ix->s_rcnt.ensure((size_t)n));
+    CUDA_TRY(cudaMemcpyAsync(ix->s_qcnt.p, qcnt, (size_t)n * 4, cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaMemcpyAsync(ix->s_rcnt.p, rcnt, (size_t)n * 4, cudaMemcpyHostToDevice, st));
+    rc = self_lower_dev_impl(ix, flags, ix->s_out.p, ix->s_out.p + cells, st);
+    if (rc)
+        return rc;
+    CUDA_TRY(cudaMemsetAsync(ix->m_nrecheck.p, 0, sizeof(unsigned long long), st));
+    CUDA_TRY(kssd::lower_metric_launch(P, n, ix->s_out.p, ix->s_out.p + cells, ix->s_qcnt.p, ix->s_rcnt.p,
+                                       ix->m_val.p, ix->m_recheck.p, recheck_cap, ix->m_nrecheck.p, ix->sms, st));
+    count_launch();
+    CUDA_TRY(cudaMemcpyAsync(value_lower, ix->m_val.p, cells * 8, cudaMemcpyDeviceToHost, st));
+    unsigned long long nre = 0;
+    CUDA_TRY(cudaMemcpyAsync(&nre, ix->m_nrecheck.p, sizeof nre, cudaMemcpyDeviceToHost, st));
+    rc = check_dev_err(ix, st);  // synchronizes
+    if (rc)
+        return rc;
+    *nrecheck = nre;
+    const uint64_t listed = std::min<uint64_t>(nre, recheck_cap);
+    if (listed)
+        CUDA_TRY(cudaMemcpy(recheck, ix->m_recheck.p, listed * sizeof(kssdgpu_recheck_t), cudaMemcpyDeviceToHost));
+    if (nre > recheck_cap)
+        return fail(KSSDGPU_ERR_CAPACITY, std::to_string(nre) + " cells to value on the host, more than the " +
+                                              std::to_string(recheck_cap) + " the caller's list holds");
+    return KSSDGPU_OK;
 }
 
 }  // extern "C"

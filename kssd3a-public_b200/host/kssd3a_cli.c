@@ -37,6 +37,7 @@
 
 #include "kssd_epilogue.h"
 #include "kssd_format.h"
+#include "kssd_hgb.h"
 #include "kssd_autosketch.h"
 #include "kssd_fastx.h"
 #include "kssdgpu.h"
@@ -1294,6 +1295,17 @@ static void self_lower_counts(const kssd_sketch_t *s, const char *dir, bool inde
     *po = lo;
 }
 
+/* One self-matrix cell valued on the host (the zero-overlap constant, or the pair metric). */
+static double self_cell_metric(const kssd_sketch_t *s, const uint32_t *qcnt, const uint32_t *rcnt, int q, int r,
+                               const kssdgpu_ctx_mut2_t *c, const kssdgpu_obj_section_t *o, bool zero_const,
+                               double zero_metric)
+{
+    if (zero_const && c->num_ctx == 0 && qcnt[q] && rcnt[r])
+        return zero_metric;
+    kssd_features_t f = feat_of(c, o);
+    return kssd_pair_metric(&f, qcnt[q], rcnt[r], &g.o, s->meta ? &s->meta[q] : NULL, s->meta ? &s->meta[r] : NULL);
+}
+
 /* metric values of every lower pair (q > r), rows in parallel */
 static double *self_lower_metrics(const kssd_sketch_t *s, const kssdgpu_ctx_mut2_t *lc, const kssdgpu_obj_section_t *lo)
 {
@@ -1309,15 +1321,8 @@ static double *self_lower_metrics(const kssd_sketch_t *s, const kssdgpu_ctx_mut2
 #pragma omp parallel for schedule(dynamic, 16) num_threads(g.o.p)
     for (int q = 1; q < n; ++q) {
         const size_t base = (size_t)q * (q - 1) / 2;
-        for (int r = 0; r < q; ++r) {
-            if (zero_const && lc[base + r].num_ctx == 0 && qcnt[q] && rcnt[r]) {
-                m[base + r] = zero_metric;
-                continue;
-            }
-            kssd_features_t f = feat_of(&lc[base + r], &lo[base + r]);
-            m[base + r] = kssd_pair_metric(&f, qcnt[q], rcnt[r], &g.o, s->meta ? &s->meta[q] : NULL,
-                                           s->meta ? &s->meta[r] : NULL);
-        }
+        for (int r = 0; r < q; ++r)
+            m[base + r] = self_cell_metric(s, qcnt, rcnt, q, r, &lc[base + r], &lo[base + r], zero_const, zero_metric);
     }
     phase("epilogue (host FP64)");
     if (rcnt != qcnt)
@@ -1449,6 +1454,121 @@ static void print_self_lf(const kssd_sketch_t *s, const double *m, bool full)
     close_out(out);
 }
 
+/* The self matrix's values with the FP64 epilogue on the device (kssdgpu_self_lower_metric):
+ * 8 bytes per cell come back instead of 16 bytes of counters, and the few cells whose
+ * printed digits depend on how a libm rounds log / log1p / pow are recomputed here with
+ * the host's.  NULL when the device's list of those cells overflows (the caller then
+ * takes the counters path). */
+static double *self_values_on_device(const kssd_sketch_t *s, kssdgpu_index_t *ix, unsigned flags)
+{
+    const int n = s->n;
+    const size_t cells = (size_t)n * (n - 1) / 2;
+    uint32_t *qcnt = sample_ctx_counts(s, s->stat.conflict, false);
+    uint32_t *rcnt = g.o.ignoreconflict ? sample_ctx_counts(s, s->stat.conflict, true) : qcnt;
+    double zero_metric = 0;
+    const bool zero_const = kssd_zero_overlap_metric(&g.o, &zero_metric);
+    kssdgpu_metric_opt_t mo = {0};
+    mo.s = g.o.s;
+    mo.e = g.o.e;
+    mo.v = g.o.v;
+    mo.unassembled = g.o.unassembled;
+    mo.unified_metric = g.o.unified_metric;
+    mo.raw_output = g.o.raw_output;
+    mo.afcut = g.o.afcut;
+    mo.drfold = g.o.drfold;
+    mo.obj_bits = g.o.obj_bits;
+    mo.ctx_bits = g.o.ctx_bits;
+    mo.zero_const = zero_const;
+    mo.zero_value = zero_metric;
+    mo.hgb_nodes = kssd_hgb_nodes;
+    mo.hgb_nodes_count = KSSD_HGB_NODES;
+    mo.hgb_tree_begin = kssd_hgb_tree_begin;
+    mo.hgb_trees = KSSD_HGB_TREES;
+    mo.hgb_baseline = kssd_hgb_baseline;
+    double *m = malloc(cells * sizeof(double) + 8);
+    const uint64_t cap = 65536;
+    kssdgpu_recheck_t *re = malloc(cap * sizeof(*re));
+    if (!m || !re)
+        err(EXIT_FAILURE, "OOM matrix values");
+    /* map the pages on all cores before the device copy lands there */
+    const size_t bytes = cells * sizeof(double), piece = 8u << 20;
+    const size_t pieces = (bytes + piece - 1) / piece;
+#pragma omp parallel for schedule(dynamic, 1) num_threads(g.o.p)
+    for (size_t k = 0; k < pieces; ++k)
+        memset((char *)m + k * piece, 0, bytes - k * piece < piece ? bytes - k * piece : piece);
+    uint64_t nre = 0;
+    const int rc = kssdgpu_self_lower_metric(ix, flags, &mo, qcnt, rcnt, m, re, cap, &nre);
+    if (rc == KSSDGPU_ERR_CAPACITY) {
+        free(m);
+        m = NULL;
+    } else {
+        gpu_check(rc, "device self join and matrix values");
+        for (uint64_t i = 0; i < nre; ++i) {
+            const uint64_t cell = re[i].cell;
+            int q = (int)((1.0 + sqrt(1.0 + 8.0 * (double)cell)) / 2.0);
+            while ((uint64_t)q * (q - 1) / 2 > cell)
+                --q;
+            while ((uint64_t)(q + 1) * q / 2 <= cell)
+                ++q;
+            const int r = (int)(cell - (uint64_t)q * (q - 1) / 2);
+            m[cell] = self_cell_metric(s, qcnt, rcnt, q, r, &re[i].ctx, &re[i].obj, zero_const, zero_metric);
+        }
+    }
+    free(re);
+    if (rcnt != qcnt)
+        free(rcnt);
+    free(qcnt);
+    return m;
+}
+
+/* The self matrix's values: on the device where the index is the sketch's own (built
+ * from it, or an index file of the same records), else from counters valued on the host. */
+static double *self_lower_values(const kssd_sketch_t *s, const char *dir, bool index_file, bool forced_needs_file)
+{
+    const int n = s->n;
+    const size_t cells = (size_t)n * (n - 1) / 2;
+    const unsigned flags = g.o.ignoreconflict ? KSSDGPU_IGNORECONFLICT : 0;
+    if (cells && getenv("KSSDGPU_HOST_EPILOGUE") == NULL) {
+        kssdgpu_index_t *ix = NULL;
+        if (index_file) {
+            size_t nrec = 0;
+            kssd_index_rec_t *rec = kssd_index_load(dir, &nrec);
+            if (!rec)
+                errx(EXIT_FAILURE, "%s", kssd_host_last_error());
+            if (nrec != (size_t)(s->offs[n] - s->offs[0]))
+                errx(EINVAL, "load_self_sorted_index_or_build(): sorted index size mismatch");
+            phase("read index file");
+            const bool own = records_checksum(rec, nrec) == sketch_checksum(s);
+            phase("index/sketch checksum");
+            if (own) {
+                gpu_check(kssdgpu_index_from_records(rec, nrec, n, s->obj_bits, 0, &ix), "device index");
+                phase("device index from records");
+            }
+            free(rec);
+        } else {
+            if (forced_needs_file && force_ref_index())
+                errx(EXIT_FAILURE, "KSSD3A_FORCE_REF_INDEX requires reference index '%s/%s'", dir,
+                     "sortedcomb_ctxgid64obj32");
+            ix = gpu_index_of_sketch(s);
+            phase("device index from sketch");
+        }
+        if (ix) {
+            double *m = self_values_on_device(s, ix, flags);
+            kssdgpu_index_free(ix);
+            phase("self join + device epilogue + D2H");
+            if (m)
+                return m;
+        }
+    }
+    kssdgpu_ctx_mut2_t *lc = NULL;
+    kssdgpu_obj_section_t *lo = NULL;
+    self_lower_counts(s, dir, index_file, forced_needs_file, &lc, &lo);
+    double *m = self_lower_metrics(s, lc, lo);
+    free(lc);
+    free(lo);
+    return m;
+}
+
 /* kind: 0 indexed full (fixed6), 1 indexed triangle, 2 direct (full or triangle per fmt) */
 static int run_self(int kind)
 {
@@ -1468,12 +1588,7 @@ static int run_self(int kind)
     } else if (kind == 1) {
         index_file = kssd_file_exists(g.qrydir, "sortedcomb_ctxgid64obj32");
     }
-    kssdgpu_ctx_mut2_t *lc = NULL;
-    kssdgpu_obj_section_t *lo = NULL;
-    self_lower_counts(s, g.qrydir, index_file, kind != 2, &lc, &lo);
-    double *m = self_lower_metrics(s, lc, lo);
-    free(lc);
-    free(lo);
+    double *m = self_lower_values(s, g.qrydir, index_file, kind != 2);
     if (kind == 0)
         print_self_full_fixed6(s, m);
     else if (kind == 1)

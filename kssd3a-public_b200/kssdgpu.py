@@ -100,8 +100,46 @@ def gpu_lib() -> C.CDLL:
                                        C.POINTER(_SketchParams), vp, C.c_uint64, _u64p]
         lib.kssdgpu_sketch_hash_id.argtypes = [C.POINTER(_SketchParams)]
         lib.kssdgpu_sketch_hash_id.restype = C.c_uint32
+        lib.kssdgpu_lower_metric_dev.argtypes = [C.c_int, C.POINTER(MetricOpt), C.c_int, vp, vp, vp, vp, vp, vp,
+                                                 C.c_uint64, vp, vp]
+        lib.kssdgpu_self_lower_metric.argtypes = [vp, C.c_uint, C.POINTER(MetricOpt), _u32p, _u32p, vp, vp,
+                                                  C.c_uint64, C.POINTER(C.c_uint64)]
         _gpu = lib
     return _gpu
+
+
+class MetricOpt(C.Structure):
+    """kssdgpu_metric_opt_t: the options a matrix value reads, and the calibration trees."""
+    _fields_ = [("s", C.c_int), ("e", C.c_int), ("v", C.c_int), ("unassembled", C.c_int),
+                ("unified_metric", C.c_int), ("raw_output", C.c_int), ("afcut", C.c_float), ("drfold", C.c_int),
+                ("obj_bits", C.c_int), ("ctx_bits", C.c_int), ("zero_const", C.c_int), ("zero_value", C.c_double),
+                ("hgb_nodes", C.c_void_p), ("hgb_nodes_count", C.c_uint32), ("hgb_tree_begin", C.c_void_p),
+                ("hgb_trees", C.c_uint32), ("hgb_baseline", C.c_double)]
+
+
+RECHECK_DTYPE = np.dtype([("cell", "<u8"), ("num_ctx", "<u4"), ("num_mut2_ctx", "<u4"), ("diff_obj", "<u4"),
+                          ("diff_obj_section", "<u4")])
+
+
+def metric_opt(s=1, e=1, v=0, unassembled=0, unified_metric=0, raw_output=0, afcut=0.5, drfold=8, obj_bits=20,
+               ctx_bits=44, zero_const=0, zero_value=0.0) -> MetricOpt:
+    """Metric options with the calibration trees of the host library (its model tables)."""
+    host = host_lib()
+    trees, nodes = 160, 9760  # KSSD_HGB_TREES, KSSD_HGB_NODES
+    begin = (C.c_uint * (trees + 1)).in_dll(host, "kssd_hgb_tree_begin")
+    node_tab = (C.c_ubyte * (16 * nodes)).in_dll(host, "kssd_hgb_nodes")
+    base = C.c_double.in_dll(host, "kssd_hgb_baseline").value
+    return MetricOpt(s, e, v, unassembled, unified_metric, raw_output, afcut, drfold, obj_bits, ctx_bits, zero_const,
+                     zero_value, C.addressof(node_tab), nodes, C.addressof(begin), trees, base)
+
+
+def lower_metric_dev(opt: MetricOpt, n, d_qcnt, d_rcnt, d_lc, d_lo, d_val, d_recheck, cap, d_nrecheck, device=0,
+                     stream=None):
+    """kssdgpu_lower_metric_dev over device tensors (stream-ordered)."""
+    ptr = lambda t: None if t is None else t.data_ptr()  # noqa: E731
+    _check(gpu_lib().kssdgpu_lower_metric_dev(device, C.byref(opt), n, ptr(d_qcnt), ptr(d_rcnt), ptr(d_lc),
+                                              ptr(d_lo), ptr(d_val), ptr(d_recheck), cap, ptr(d_nrecheck),
+                                              None if stream is None else stream.cuda_stream))
 
 
 class _SketchParams(C.Structure):

@@ -170,3 +170,28 @@ def test_noalloc_at_the_query_limit():
     assert all(torch.equal(g, w) for g, w in zip(got, want))
     assert int((want[0] & 0xFFFFFFFF).sum()) > 0
     idx.close()
+
+
+def test_noalloc_with_no_queries_leaves_outputs_untouched():
+    """nq = 0 (an empty batch a serving loop may hand over) succeeds, launches nothing
+    that writes the outputs, and the next call still matches the existing entry point."""
+    import torch
+    ref, qry, _ = _workload()
+    idx = kssdgpu.Index.from_sketch(ref)
+    dev = torch.device("cuda", 0)
+    out = [torch.full((8,), -1, dtype=torch.int64, device=dev) for _ in range(2)]
+    d_offs = torch.zeros(1, dtype=torch.int64, device=dev)
+    d_keys = torch.zeros(1, dtype=torch.int64, device=dev)
+    _noalloc(idx, d_keys, d_offs, 0, out)
+    for o in out:
+        assert bool((o == -1).all())
+    d_keys = torch.from_numpy(qry.keys.view(np.int64)).to(dev)
+    d_offs = torch.from_numpy(qry.offs.view(np.int64)).to(dev)
+    want = [torch.zeros(qry.n * ref.n, dtype=torch.int64, device=dev) for _ in range(2)]
+    got = [torch.full((qry.n * ref.n,), -1, dtype=torch.int64, device=dev) for _ in range(2)]
+    idx.count_block_dev(d_keys, d_offs, qry.n, *want)
+    idx.sync()
+    _noalloc(idx, d_keys, d_offs, qry.n, got)
+    for g, w in zip(got, want):
+        assert torch.equal(g, w)
+    idx.close()
