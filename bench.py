@@ -915,13 +915,11 @@ def run_ours(args, rank, world, local_rank):
         extra["all_vs_all_20k"] = ns
         extra["rect_config3"] = leg_rect(args, timer, dev, stream, peak, ns_idx, ns_sk)
         extra["reads_config4"] = leg_reads(args, timer, dev, stream, ns_idx, ns_sk)
-        rates = [float(x) for x in args.serve_rates.split(",")] if args.serve_rates else []
-        if rates:
-            res, pool, srvf = serve_sweep(ns_idx, ns_sk.n, rates, args.serve_seconds, WORKLOAD["seed"] + 5)
-            extra["serve"] = {"index_genomes": ns_sk.n, "note": "resident 20,000-genome index (not 50,000: the "
-                              "default run stays within minutes; --workload serve runs the 50,000-genome index)",
-                              "pool": pool, "server": srvf, "rates": res}
         ns_idx.close()
+        del ns_sk
+        torch.cuda.empty_cache()
+        if args.serve_rates and args.serve_refs > 0:
+            extra["serve"] = serve_leg(args, args.serve_refs)
         extra["dense_one_species"] = leg_dense(args, timer, dev, stream, peak_tc)
         extra["cli_2k"] = leg_cli_2k(args, sk)
         extra["config1_fasta"] = leg_config1(args)
@@ -985,14 +983,11 @@ def run_ours(args, rank, world, local_rank):
     return 0
 
 
-def run_serve(args, rank):
-    """Serving alone: a resident index of --serve-refs genomes (the self-matrix
-    generator, 10 genomes per cluster), Poisson arrivals at each rate."""
+def serve_leg(args, n):
+    """A resident index of n genomes (the self-matrix generator, 10 genomes per cluster)
+    and the serving sweep against it."""
     import torch
     import kssdgpu
-    if rank != 0:
-        return 0
-    n = args.serve_refs
     seed = WORKLOAD["seed"] + 5
     t0 = time.perf_counter()
     ref = kssdgpu.synth(n_samples=n, n_clusters=max(1, n // 10), size_dist=kssdgpu.SIZE_LOGNORMAL, len_median=4e6,
@@ -1008,12 +1003,20 @@ def run_serve(args, rank):
     del ref
     rates = [float(x) for x in args.serve_rates.split(",")]
     res, pool, srvf = serve_sweep(idx, n, rates, args.serve_seconds, seed)
-    line = {"metric": "serve p50/p99 ms", "workload": f"serve-{n}-genome-index", "unit": "ms",
-            "higher_is_better": False, "data": "synthetic",
-            "index": {"genomes": n, "entries": entries, "generate_s": gen_s, "device_build_s": build_s},
-            "pool": pool, "server": srvf, "rates": res}
-    print(json.dumps(line), flush=True)
     idx.close()
+    return {"index": {"genomes": n, "entries": entries, "generate_s": gen_s, "device_build_s": build_s},
+            "pool": pool, "server": srvf, "rates": res}
+
+
+def run_serve(args, rank):
+    """Serving alone: a resident index of --serve-refs genomes, Poisson arrivals at each rate."""
+    if rank != 0:
+        return 0
+    leg = serve_leg(args, args.serve_refs)
+    line = {"metric": "serve p50/p99 ms", "workload": f"serve-{args.serve_refs}-genome-index", "unit": "ms",
+            "higher_is_better": False, "data": "synthetic"}
+    line.update(leg)
+    print(json.dumps(line), flush=True)
     return 0
 
 
@@ -1036,7 +1039,8 @@ def main():
     ap.add_argument("--reads-samples", type=int, default=40)
     ap.add_argument("--parity-queries", type=int, default=48)
     ap.add_argument("--dense-genomes", type=int, default=1024, help="genomes of the one-species dense leg")
-    ap.add_argument("--serve-refs", type=int, default=50000, help="serve workload: resident index size (genomes)")
+    ap.add_argument("--serve-refs", type=int, default=50000,
+                    help="resident index size (genomes) of the serving sweep (0: no sweep in the default run)")
     ap.add_argument("--serve-rates", default="1000,5000", help="arrival rates (req/s) of the serving sweep")
     ap.add_argument("--serve-seconds", type=float, default=1.5, help="arrival window per rate")
     args = ap.parse_args()

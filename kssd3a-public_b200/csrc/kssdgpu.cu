@@ -1560,9 +1560,11 @@ __device__ __forceinline__ void join_group_cta(const uint64_t *__restrict__ post
 
 // Shared memory of k_self_scan: the tile's queue of shared groups, and (PAIRS) the
 // exclusive prefix of the small groups' pair counts.
+constexpr uint32_t kScanPairRanks = kScanLaneMax * (kScanLaneMax - 1) / 2;  // pairs of the largest small group
 struct ScanSmem {
     unsigned long long queue[kScanTile];  // groups of 2..kScanLaneMax from the front, larger from the back
     uint32_t prefix[kScanTile];
+    unsigned short pair[kScanPairRanks];  // (i, j) of every pair rank of a small group: i | j << 8
 };
 
 // Where the lower triangle spans far more memory than L2 (20,000 genomes: 3.2 GB), its
@@ -1687,6 +1689,9 @@ __device__ __forceinline__ void scan_load_bounds(const uint32_t *__restrict__ gb
 // walks a whole large group while the others wait; with conflicts every thread walks
 // whole groups (run cross products).  Groups of more than kScanLaneMax postings are
 // taken by the whole CTA.
+#ifndef KSSD_SCAN_PAIR_TABLE
+#define KSSD_SCAN_PAIR_TABLE 1
+#endif
 #ifndef KSSD_SCAN_PAIR_BATCH
 #define KSSD_SCAN_PAIR_BATCH 4
 #endif
@@ -1712,6 +1717,16 @@ __global__ void __launch_bounds__(kScanThreads, MINB) k_self_scan(const uint32_t
     __shared__ typename Scan::TempStorage scan_tmp;
     const uint64_t ntiles = (u + kScanTile - 1) / kScanTile;
     bool waited = false;
+#if KSSD_SCAN_PAIR_TABLE
+    if (PAIRS) {
+        for (uint32_t t = threadIdx.x; t < kScanPairRanks; t += kScanThreads) {
+            uint32_t i, j;
+            pair_of_rank(t, i, j);
+            S.pair[t] = (unsigned short)(i | (j << 8));
+        }
+        // visible to every thread after the first tile's queue barrier
+    }
+#endif
     uint32_t bnd[kScanPerThread + 1];
     if (blockIdx.x < ntiles)
         scan_load_bounds(gbeg, u, blockIdx.x, bnd);
@@ -1783,7 +1798,13 @@ __global__ void __launch_bounds__(kScanThreads, MINB) k_self_scan(const uint32_t
                                 ++q;
                             const unsigned long long item = S.queue[q];
                             uint32_t i, j;
+#if KSSD_SCAN_PAIR_TABLE
+                            const uint32_t ij = S.pair[pr + x - S.prefix[q]];
+                            i = ij & 0xFFu;
+                            j = ij >> 8;
+#else
                             pair_of_rank(pr + x - S.prefix[q], i, j);
+#endif
                             pi[x] = __ldg(post + (uint32_t)item + i);
                             pj[x] = __ldg(post + (uint32_t)item + j);
                         }
