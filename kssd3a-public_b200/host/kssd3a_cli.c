@@ -1540,11 +1540,13 @@ static double *self_lower_values(const kssd_sketch_t *s, const char *dir, bool i
             phase("read index file");
             const bool own = records_checksum(rec, nrec) == sketch_checksum(s);
             phase("index/sketch checksum");
-            if (own) {
-                gpu_check(kssdgpu_index_from_records(rec, nrec, n, s->obj_bits, 0, &ix), "device index");
-                phase("device index from records");
-            }
             free(rec);
+            if (own) {
+                /* the file holds the sketch's own index: the device builds the same index from
+                 * the sketch's keys (2/3 of the file's bytes to move) */
+                ix = gpu_index_of_sketch(s);
+                phase("device index from sketch");
+            }
         } else {
             if (forced_needs_file && force_ref_index())
                 errx(EXIT_FAILURE, "KSSD3A_FORCE_REF_INDEX requires reference index '%s/%s'", dir,

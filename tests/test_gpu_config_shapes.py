@@ -111,6 +111,17 @@ def test_headline_2000_genome_ani_matrix_bytes(genomes2k):
     assert len(out.splitlines()) == 2001
 
 
+@pytest.mark.parametrize("fmt", ["matrix", "triangle"])
+def test_headline_2000_genome_matrix_to_file(genomes2k, tmp_path, fmt):
+    """-o FILE (a regular file: rows go out as positioned writes from all host threads)
+    gives the bytes the reference writes, also when the file already holds longer content."""
+    want = _run(oracle.REF_BIN, ["ani", "-p", THREADS, "-q", genomes2k, "--format", fmt, "--values", "ani"])
+    dst = tmp_path / "m.tsv"
+    dst.write_bytes(b"x" * (len(want) + 12345))
+    _run(OURS, ["ani", "-p", THREADS, "-q", genomes2k, "--format", fmt, "--values", "ani", "-o", str(dst)])
+    assert dst.read_bytes() == want
+
+
 def test_headline_2000_genome_detail_bytes(genomes2k):
     out = _same(["ani", "-p", THREADS, "-r", genomes2k, "-q", genomes2k])
     assert len(out.splitlines()) > 2000
