@@ -537,57 +537,100 @@ __global__ void k_stripe_pos(const uint64_t *__restrict__ qkeys, const uint64_t 
     }
 }
 
-// Entries b + t, b + t + T, ... of one query, kProbeBatch per thread at a time:
-// their first hash slots are loaded back to back so several random lines are in
-// flight per thread, then each probe is resolved (rarely a second slot) and credited.
-#ifndef KSSD_PROBE_BATCH
-#define KSSD_PROBE_BATCH 1
-#endif
-constexpr int kProbeBatch = KSSD_PROBE_BATCH;
+// A context group of at least kWarpWalk postings is walked by the whole warp: lanes load
+// consecutive postings (one coalesced line per 32 of them instead of one thread's
+// serial walk), the lane holding the first posting of a gid run takes the run's minimum
+// object difference and credits it, and a ballot counts the group's owners for the
+// unique-context rule.  Same credits as walk_context (src/command_ani.h:515-575): LOWER
+// stops at gid >= qgid, --ignoreconflict skips reference runs of several objects, the
+// sole owner is credited when its run counted.
+constexpr uint32_t kWarpWalk = 32;
 
-// Threads t0, t0 + T, ... of the caller's group take the entries; fv is the filter.
+template <bool LOWER, bool UNIQUE, class Acc>
+__device__ __forceinline__ void walk_context_warp(const uint64_t *__restrict__ post, uint32_t pb, uint32_t pe,
+                                                  const uint64_t *__restrict__ qrun, int s, uint64_t objmask,
+                                                  int qgid, int ignoreconflict, const Acc &acc, const Acc &uacc,
+                                                  uint32_t lane)
+{
+    const uint32_t q0 = (uint32_t)(__ldg(qrun) & objmask);
+    uint32_t owners = 0, sole_gid = 0;
+    int sole_d = 0;
+    bool sole_mine = false, sole_ok = false;
+    for (uint32_t p0 = pb; p0 < pe; p0 += 32) {
+        const uint32_t p = p0 + lane;
+        const bool in = p < pe;
+        const uint64_t w = in ? __ldg(post + p) : 0;
+        const uint32_t gid = (uint32_t)(w >> 32);
+        uint32_t pg = __shfl_up_sync(0xFFFFFFFFu, gid, 1);
+        if (lane == 0)
+            pg = p0 > pb ? (uint32_t)(__ldg(post + p0 - 1) >> 32) : 0xFFFFFFFFu;
+        const bool live = in && (!LOWER || (int)gid < qgid);
+        const bool head = live && gid != pg;
+        if (head) {
+            int d = min_diff_obj((uint32_t)w, q0, s, qrun, objmask, kMinInit);
+            uint32_t x = p + 1;
+            while (x < pe) {
+                const uint64_t w2 = __ldg(post + x);
+                if ((uint32_t)(w2 >> 32) != gid)
+                    break;
+                d = min_diff_obj((uint32_t)w2, q0, s, qrun, objmask, d);
+                ++x;
+            }
+            const bool counted = !(ignoreconflict && x - p > 1);
+            if (counted)
+                acc.add(gid, d);
+            sole_mine = true;
+            sole_gid = gid;
+            sole_d = d;
+            sole_ok = counted;
+        }
+        owners += __popc(__ballot_sync(0xFFFFFFFFu, head));
+        if (LOWER && __any_sync(0xFFFFFFFFu, in && (int)gid >= qgid))
+            break;  // postings ascend by gid: the rest are not below the query
+    }
+    if (UNIQUE && owners == 1 && sole_mine && sole_ok)
+        uacc.add(sole_gid, sole_d);
+}
+
+// Entries [cb, ce) of one query (whose entries are [b, e)), taken by the caller's
+// threads t0, t0 + T, ... (t0 % 32 = the lane, T a multiple of 32): every lane of a warp
+// takes one entry per round (the warp's rounds are the same for all its lanes).  Only the
+// first entry of a context run works (src/command_ani.h:498-505); the filter rules out
+// most absent contexts; one hash probe finds the context; the inline single posting is
+// credited at once, short groups are walked by their lane, long ones by the warp.
 template <bool LOWER, bool UNIQUE, class Acc>
 __device__ __forceinline__ void process_query(const CountParams &P, uint64_t b, uint64_t e, uint64_t cb, uint64_t ce,
                                               int qgid, uint64_t objmask, const Acc &acc, const Acc &uacc,
                                               const FilterView &fv, uint64_t t0, uint64_t T)
 {
-    for (uint64_t base = cb + t0; base < ce; base += T * kProbeBatch) {
-        unsigned long long ctx[kProbeBatch];
-        uint32_t slot[kProbeBatch];
-        int s[kProbeBatch];
-        ulonglong2 first[kProbeBatch];
-#pragma unroll
-        for (int u = 0; u < kProbeBatch; ++u) {
-            const uint64_t i = base + u * T;
-            s[u] = 0;
-            if (i < ce) {
-                const uint64_t key = __ldg(P.qkeys + i);
-                ctx[u] = key >> P.obj_bits;
-                const uint64_t prev = i > b ? __ldg(P.qkeys + i - 1) : 0;
-                if (prev > key)
-                    atomicMax(P.err, (int)kDevUnsorted);  // a sample's keys must ascend (comblco order)
-                if (!(i > b && (prev >> P.obj_bits) == ctx[u]) && fv.may_hold(ctx[u])) {
-                    int run = 1;
-                    while (i + run < e && (__ldg(P.qkeys + i + run) >> P.obj_bits) == ctx[u])
-                        ++run;
-                    s[u] = run;
-                    slot[u] = (uint32_t)mix64(ctx[u]) & P.mask;
-                }
+    const uint32_t lane = (uint32_t)(t0 & 31u);
+    for (uint64_t wb = cb + (t0 - lane); wb < ce; wb += T) {
+        const uint64_t i = wb + lane;
+        int s = 0;
+        unsigned long long ctx = 0;
+        uint32_t slot = 0;
+        if (i < ce) {
+            const uint64_t key = __ldg(P.qkeys + i);
+            ctx = key >> P.obj_bits;
+            const uint64_t prev = i > b ? __ldg(P.qkeys + i - 1) : 0;
+            if (prev > key)
+                atomicMax(P.err, (int)kDevUnsorted);  // a sample's keys must ascend (comblco order)
+            if (!(i > b && (prev >> P.obj_bits) == ctx) && fv.may_hold(ctx)) {
+                int run = 1;
+                while (i + run < e && (__ldg(P.qkeys + i + run) >> P.obj_bits) == ctx)
+                    ++run;
+                s = run;
+                slot = (uint32_t)mix64(ctx) & P.mask;
             }
         }
-#pragma unroll
-        for (int u = 0; u < kProbeBatch; ++u)
-            if (s[u])
-                first[u] = __ldg(reinterpret_cast<const ulonglong2 *>(P.table + slot[u]));
-#pragma unroll
-        for (int u = 0; u < kProbeBatch; ++u) {
-            if (!s[u])
-                continue;
-            ulonglong2 sl = first[u];
-            uint32_t at = slot[u];
+        bool wide = false;
+        uint32_t pb = 0, pc = 0;
+        if (s) {
+            ulonglong2 sl = __ldg(reinterpret_cast<const ulonglong2 *>(P.table + slot));
+            uint32_t at = slot;
             bool found = false;
             for (uint32_t probe = 0; probe <= P.mask; ++probe) {
-                if ((sl.x & ~kInlineBit) == ctx[u]) {
+                if ((sl.x & ~kInlineBit) == ctx) {
                     found = true;
                     break;
                 }
@@ -596,9 +639,24 @@ __device__ __forceinline__ void process_query(const CountParams &P, uint64_t b, 
                 at = (at + 1) & P.mask;
                 sl = __ldg(reinterpret_cast<const ulonglong2 *>(P.table + at));
             }
-            if (found)
-                credit_context<LOWER, UNIQUE>(P, base + u * T, s[u], sl.y, (sl.x & kInlineBit) != 0, qgid, objmask,
-                                              acc, uacc);
+            if (found) {
+                const bool single = (sl.x & kInlineBit) != 0;
+                pb = (uint32_t)sl.y;
+                pc = (uint32_t)(sl.y >> 32);
+                if (!single && pc >= kWarpWalk)
+                    wide = true;
+                else
+                    credit_context<LOWER, UNIQUE>(P, i, s, sl.y, single, qgid, objmask, acc, uacc);
+            }
+        }
+        // the warp walks its lanes' long groups together, one after another
+        for (unsigned m = __ballot_sync(0xFFFFFFFFu, wide); m; m &= m - 1) {
+            const int src = __ffs(m) - 1;
+            const uint32_t gb = __shfl_sync(0xFFFFFFFFu, pb, src), gc = __shfl_sync(0xFFFFFFFFu, pc, src);
+            const uint64_t gi = __shfl_sync(0xFFFFFFFFu, i, src);
+            const int gs = __shfl_sync(0xFFFFFFFFu, s, src);
+            walk_context_warp<LOWER, UNIQUE>(P.post, gb, gb + gc, P.qkeys + gi, gs, objmask, qgid, P.ignoreconflict,
+                                             acc, uacc, lane);
         }
     }
 }

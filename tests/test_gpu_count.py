@@ -687,3 +687,45 @@ def test_self_scan_with_counters_beyond_l2(n, clusters, table_log, monkeypatch):
     np.testing.assert_array_equal(got_c, 2 * want[0].reshape(cells, 2))
     np.testing.assert_array_equal(got_o, 2 * want[1].reshape(cells, 2))
     idx.close()
+
+@pytest.mark.parametrize("case", ["block", "block_unique", "lower", "reads_unique_ignoreconflict", "smem_unique",
+                                  "striped_unique", "striped_lower"])
+def test_batched_count_on_long_postings_lists(case):
+    """References of one species (contexts shared by up to 300 genomes): query contexts
+    whose groups hold 32 or more postings are walked by the whole warp (coalesced
+    postings, run heads by shuffle, owners by ballot); the counters equal the oracle's
+    for blocks, lower blocks, read sets with conflicts under --ignoreconflict, shared-
+    and global-memory rows and the stripe-major count."""
+    ref = _wide_cluster(300, 65, 0.03)
+    rec = oracle.build_index(ref.keys, ref.offs)
+    _, sizes = np.unique(rec["ctxgid"] >> 20, return_counts=True)
+    assert sizes.max() >= 200 and sizes[sizes >= 32].sum() > 0.5 * sizes.sum()  # most postings in long groups
+    idx = kssdgpu.Index.from_records(rec, ref.n)
+    flags, unique = 0, False
+    qry = kssdgpu.synth(n_samples=24, n_clusters=1, role=kssdgpu.ROLE_OWNLEN, len_median=4e5, len_min=2e5,
+                        len_max=8e5, size_dist=kssdgpu.SIZE_LOGNORMAL, sub_lo=0.001, sub_hi=0.03, seed=65,
+                        sample_seed=66, own_len_min=5e4, own_len_max=8e5)
+    if case.startswith("striped"):
+        assert idx.filter(4096)["stripes"] > 1
+    if case in ("block_unique", "smem_unique", "striped_unique"):
+        flags, unique = kssdgpu.UNIQUE, True
+    if case == "smem_unique":
+        flags |= kssdgpu.SMEM_ACC
+    if case == "reads_unique_ignoreconflict":
+        qry = kssdgpu.synth(n_samples=4, n_clusters=1, role=kssdgpu.ROLE_READS, sample_seed=67, ref_sample_seed=65,
+                            ref_samples=300, len_median=4e5, len_min=2e5, len_max=8e5, cov_lo=5, cov_hi=15)
+        flags, unique = kssdgpu.UNIQUE | kssdgpu.IGNORECONFLICT, True
+    if case in ("lower", "striped_lower"):
+        off = 100
+        qk = ref.keys[int(ref.offs[off]):int(ref.offs[off + 60])]
+        qo = np.ascontiguousarray(ref.offs[off:off + 61])
+        got = idx.count_lower(qk, qo, off, flags)
+        want = oracle.count_lower(rec, ref.n, off, qk, qo)
+    else:
+        got = idx.count_block(qry.keys, qry.offs, flags)
+        want = oracle.count_block(rec, ref.n, qry.keys, qry.offs, unique=unique,
+                                  ignoreconflict=bool(flags & kssdgpu.IGNORECONFLICT))
+    for g, w in zip(got, want):
+        np.testing.assert_array_equal(g, w)
+    assert want[0][:, :, 0].sum() > 0
+    idx.close()
