@@ -492,6 +492,35 @@ def leg_dense(args, timer, dev, stream, peak_tc):
     same = bool(torch.equal(a_c, b_c) and torch.equal(a_o, b_o))
     kpad = (alleles + 127) // 128 * 128
     ops = 2 * n * 4 * n * kpad  # int8 multiply-adds x 2 of the GEMM
+    del a_c, a_o, b_c, b_o
+    # the batched probe on the same dense index: 256 new members of the species against
+    # it (context groups of hundreds of postings, walked by whole warps), counters of a
+    # query sample against the oracle
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    qry = kssdgpu.synth(n_samples=256, n_clusters=1, role=kssdgpu.ROLE_OWNLEN, size_dist=kssdgpu.SIZE_LOGNORMAL,
+                        len_median=4e6, len_sigma=0.2, len_min=2e6, len_max=8e6, own_len_min=1e6, own_len_max=8e6,
+                        sub_lo=0.001, sub_hi=0.02, seed=WORKLOAD["seed"] + 21, sample_seed=WORKLOAD["seed"] + 22,
+                        threads=os.cpu_count() or 8)
+    dk = torch.from_numpy(qry.keys.view(np.int64)).to(dev)
+    do = torch.from_numpy(qry.offs.view(np.int64)).to(dev)
+    pc = torch.zeros(qry.n * n, dtype=torch.int64, device=dev)
+    po = torch.zeros_like(pc)
+    probe_tuning = idx.count_tune(dk, do, qry.n, pc, po)
+    ms_probe = timer(lambda: idx.count_block_dev(dk, do, qry.n, pc, po, stream=stream), 5, 2)
+    walked = int((pc & 0xFFFFFFFF).sum().item())  # one credit per (query context, reference gid run)
+    rec, _ = idx.export()
+    sample = list(range(0, qry.n, qry.n // 8))[:8]
+    skeys = np.concatenate([qry.keys[int(qry.offs[q]):int(qry.offs[q + 1])] for q in sample])
+    soffs = np.concatenate([[0], np.cumsum([int(qry.offs[q + 1] - qry.offs[q]) for q in sample])]).astype(np.uint64)
+    wc, wo = oracle.count_block(rec, n, skeys, soffs, threads=os.cpu_count() or 1, ref=oracle.ref_available())
+    rows = torch.tensor(sample, device=dev)
+    probe_same = bool(np.array_equal(wc.view(np.int64).reshape(len(sample), n), pc.view(qry.n, n)[rows].cpu().numpy())
+                      and np.array_equal(wo.view(np.int64).reshape(len(sample), n),
+                                         po.view(qry.n, n)[rows].cpu().numpy()))
+    qkeys = int(qry.offs[-1])
+    model = probe_model_bytes(qkeys, walked, qry.n * n)
+    del rec, pc, po, dk, do
     idx.close()
     return {"workload": f"one-species-{n}-genomes", "genomes": n, "entries": int(sk.offs[-1]),
             "shared_postings": facts["postings"], "pairs": facts["pairs"], "alleles": alleles,
@@ -501,7 +530,15 @@ def leg_dense(args, timer, dev, stream, peak_tc):
             "tensor": {"bound": "tensor", "int8_ops": ops, "achieved_tops": ops / ms_dense / 1e9,
                        "peak_tops": peak_tc, "frac_of_step": ops / ms_dense / 1e9 / peak_tc,
                        "what": "GEMM int8 ops over the whole dense step (allele build + GEMM + epilogue)"},
-            "parity": {"dense_eq_scan": same}}
+            "parity": {"dense_eq_scan": same},
+            "batched_probe_256_queries": {"ms": ms_probe, "query_keys": qkeys, "credits": walked,
+                                          "genome_pairs_s": qry.n * n / (ms_probe / 1e3),
+                                          "tuning": probe_tuning,
+                                          "roofline_probe_model": {"bytes": model, "frac": model / ms_probe / 1e6 /
+                                                                   measured_peak_hbm()[0]},
+                                          "counts_match_reference": probe_same,
+                                          "what": "kssdgpu_count_block_dev of 256 new members of the species: "
+                                                  "context groups of hundreds of postings walked by whole warps"}}
 
 
 def leg_cli_2k(args, sk):
