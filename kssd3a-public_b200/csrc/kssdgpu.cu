@@ -1742,11 +1742,12 @@ __device__ __forceinline__ void scan_load_bounds(const uint32_t *__restrict__ gb
 // while the previous tile was joined), one block scan places the tile's shared groups
 // in the queue.  PAIRS (a conflict-free index: one object per gid run): the small
 // groups' pairs are then dealt out evenly, thread t taking a contiguous range of the
-// tile's pair ranks and loading the postings of kScanPairBatch pairs (2: more only costs
-// registers and idle predicated slots at ~2 pairs per lane and tile) before it credits them, so every lane runs the same short sequence per pair and no thread
-// walks a whole large group while the others wait; with conflicts every thread walks
-// whole groups (run cross products).  Groups of more than kScanLaneMax postings are
-// taken by the whole CTA.
+// tile's pair ranks and loading the postings of kScanPairBatch pairs before it credits
+// them (2: more costs registers and idle predicated slots at ~2 pairs per lane and
+// tile), so every lane runs the same short sequence per pair and no thread walks a
+// whole large group while the others wait; with conflicts every thread walks whole
+// groups (run cross products).  Groups of more than kScanLaneMax postings are taken by
+// the whole CTA.
 #ifndef KSSD_SCAN_PAIR_TABLE
 #define KSSD_SCAN_PAIR_TABLE 1
 #endif
