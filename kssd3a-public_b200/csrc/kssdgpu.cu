@@ -1757,14 +1757,12 @@ __device__ __forceinline__ void scan_load_bounds(const uint32_t *__restrict__ gb
 constexpr uint32_t kScanPairBatch = KSSD_SCAN_PAIR_BATCH;
 static_assert(kScanPerThread % 4 == 0, "contiguous bounds are loaded 4 at a time");
 
-#ifndef KSSD_SCAN_MINB_L2
-#define KSSD_SCAN_MINB_L2 3
+// four CTAs per SM (64 registers): 2,000 genomes 0.112 vs 0.124 ms per join with three
+#ifndef KSSD_SCAN_MINB
+#define KSSD_SCAN_MINB 4
 #endif
-#ifndef KSSD_SCAN_MINB_BIG
-#define KSSD_SCAN_MINB_BIG 4
-#endif
-template <bool PAIRS, int MINB>
-__global__ void __launch_bounds__(kScanThreads, MINB) k_self_scan(const uint32_t *__restrict__ gbeg, uint64_t u,
+template <bool PAIRS>
+__global__ void __launch_bounds__(kScanThreads, KSSD_SCAN_MINB) k_self_scan(const uint32_t *__restrict__ gbeg, uint64_t u,
                                                             const uint64_t *__restrict__ post, int ignoreconflict,
                                                             CellTable table,
                                                             unsigned long long *__restrict__ oc,
@@ -2505,7 +2503,7 @@ struct kssdgpu_index {
     uint32_t j_n[3] = {0, 0, 0};
     unsigned long long j_postings = 0, j_pairs = 0;
     bool j_ready = false;
-    int scan_grid[2] = {0, 0};              // CTAs of the one-pass scan join (resident per SM x SMs), per mode
+    int scan_grid = 0;                      // CTAs of the one-pass scan join (resident per SM x SMs)
     DevBuf<double> m_val;                   // self matrix values (kssdgpu_self_lower_metric)
     DevBuf<kssd::RecheckCell> m_recheck;    // cells the host values
     DevBuf<unsigned long long> m_nrecheck;
@@ -3771,9 +3769,8 @@ int self_scan_impl(kssdgpu_index *ix, unsigned flags, unsigned long long *oc, un
     const bool pairs = !ix->f_conflict;
     // Triangles larger than L2 (and of 32-bit cell numbers: at most 92,681 genomes) add
     // through the table of touched cells (allocated on first use, kept empty between
-    // calls), with four CTAs per SM; with the counters in L2 the table's probes cost more
-    // than they save (2,000 genomes: 0.19 vs 0.14 ms per step) and the join adds into the
-    // triangle directly, three CTAs per SM.
+    // calls); with the counters in L2 the table's probes cost more than they save (2,000
+    // genomes: 0.19 vs 0.14 ms per step) and the join adds into the triangle directly.
     const bool big = cells < (size_t)kCellEmpty && cells * 16 > (size_t)ix->l2_bytes;
     CellTable table{nullptr, nullptr, 0};
     if (ix->u && pairs && big) {
@@ -3802,19 +3799,18 @@ int self_scan_impl(kssdgpu_index *ix, unsigned flags, unsigned long long *oc, un
     }
     if (!ix->u)
         return KSSDGPU_OK;
-    const int mode = table.key ? 1 : 0;
-    auto kern = mode ? (pairs ? k_self_scan<true, KSSD_SCAN_MINB_BIG> : k_self_scan<false, KSSD_SCAN_MINB_BIG>)
-                     : (pairs ? k_self_scan<true, KSSD_SCAN_MINB_L2> : k_self_scan<false, KSSD_SCAN_MINB_L2>);
+    auto kern = pairs ? k_self_scan<true> : k_self_scan<false>;
     const size_t smem = sizeof(ScanSmem);
-    if (!ix->scan_grid[mode]) {
-        CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (!ix->scan_grid) {
+        CUDA_TRY(cudaFuncSetAttribute(k_self_scan<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        CUDA_TRY(cudaFuncSetAttribute(k_self_scan<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         int per_sm = 0;
-        CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kScanThreads, smem));
-        ix->scan_grid[mode] = std::max(1, per_sm) * ix->sms;
+        CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_self_scan<true>, kScanThreads, smem));
+        ix->scan_grid = std::max(1, per_sm) * ix->sms;
     }
     const uint64_t ntiles = (ix->u + kScanTile - 1) / kScanTile;
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3((unsigned)std::min<uint64_t>(ntiles, (uint64_t)ix->scan_grid[mode]));
+    cfg.gridDim = dim3((unsigned)std::min<uint64_t>(ntiles, (uint64_t)ix->scan_grid));
     cfg.blockDim = dim3(kScanThreads);
     cfg.dynamicSmemBytes = smem;
     cfg.stream = st;
