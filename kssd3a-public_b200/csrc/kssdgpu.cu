@@ -2006,113 +2006,153 @@ __global__ void k_dense_list(const uint32_t *__restrict__ gbeg, uint64_t u, unsi
     }
 }
 
-// Largest shared group the dense join handles (its postings are sorted in shared
+// Largest shared group the dense join handles (its postings are held in shared
 // memory), which also bounds the references: the dense join needs nref <= this.
 constexpr uint32_t kDenseMaxGroup = 4096;
 constexpr int kDenseThreads = 256;
 
-// Sorts the group's postings (object << 32 | gid) ascending in shared memory (bitonic
-// over the next power of two, padded with ~0) and returns that power of two.
-__device__ uint32_t dense_sort_group(const uint64_t *__restrict__ post, uint32_t b, uint32_t k,
-                                     unsigned long long *__restrict__ v)
+// Shared memory of the dense kernels for groups of at most n postings (n = the index's
+// references): a hash of the group's objects (hcap = pow2 >= 2n slots: the object with a
+// valid bit, the slot's allele number), and per posting its object, gid and allele.
+struct DenseGroupSmem {
+    unsigned long long *hkey;  // hcap
+    unsigned short *hid;       // hcap
+    uint32_t *pobj, *aval;     // n: posting objects; allele values by number
+    unsigned short *pgid, *pall;  // n
+};
+__host__ __device__ __forceinline__ uint32_t dense_hcap(uint32_t n)
 {
-    uint32_t m = 1;
-    while (m < k)
-        m <<= 1;
-    for (uint32_t j = threadIdx.x; j < m; j += blockDim.x) {
-        if (j < k) {
-            const uint64_t p = post[b + j];
-            v[j] = ((unsigned long long)(uint32_t)p << 32) | (p >> 32);
-        } else {
-            v[j] = ~0ull;
+    uint32_t c = 64;
+    while (c < 2 * n)
+        c <<= 1;
+    return c;
+}
+__host__ __device__ __forceinline__ size_t dense_group_smem(uint32_t n)
+{
+    const uint32_t hcap = dense_hcap(n);
+    return (size_t)hcap * 10 + (size_t)n * 12 + 64;
+}
+__device__ __forceinline__ DenseGroupSmem dense_group_view(unsigned char *base, uint32_t n)
+{
+    const uint32_t hcap = dense_hcap(n);
+    DenseGroupSmem g;
+    g.hkey = reinterpret_cast<unsigned long long *>(base);
+    g.pobj = reinterpret_cast<uint32_t *>(g.hkey + hcap);
+    g.aval = g.pobj + n;
+    g.hid = reinterpret_cast<unsigned short *>(g.aval + n);
+    g.pgid = g.hid + hcap;
+    g.pall = g.pgid + n;
+    return g;
+}
+
+// The alleles of a group [b, b + k) (k <= n postings, one object per gid): its distinct
+// objects, numbered 0..m-1 by hash slot order; afterwards pobj / pgid / pall hold every
+// posting's object, gid and allele and aval[a] the object of allele a.  A few barriers
+// instead of a sort: every posting's object is inserted into the hash (CAS on an empty
+// slot, linear probing; 2k slots for at most k objects), each thread numbers the
+// occupied slots of its contiguous segment after one block scan of their counts.
+// Returns m; ends with a barrier.
+__device__ uint32_t dense_group_alleles(const uint64_t *__restrict__ post, uint32_t b, uint32_t k,
+                                        const DenseGroupSmem &g, uint32_t *scan_tot)
+{
+    using Scan = cub::BlockScan<uint32_t, kDenseThreads>;
+    __shared__ typename Scan::TempStorage scan_tmp;
+    const uint32_t hcap = dense_hcap(k), mask = hcap - 1;
+    int lg = 0;
+    while ((1u << lg) < hcap)
+        ++lg;
+    for (uint32_t i = threadIdx.x; i < hcap; i += kDenseThreads)
+        g.hkey[i] = 0;
+    __syncthreads();
+    for (uint32_t j = threadIdx.x; j < k; j += kDenseThreads) {
+        const uint64_t p = __ldg(post + b + j);
+        const uint32_t o = (uint32_t)p;
+        g.pobj[j] = o;
+        g.pgid[j] = (unsigned short)(p >> 32);
+        const unsigned long long key = (1ull << 32) | o;
+        uint32_t h = (o * 2654435761u) >> (32 - lg);
+        for (uint32_t probe = 0; probe < hcap; ++probe) {
+            const unsigned long long old = atomicCAS(&g.hkey[h], 0ull, key);
+            if (old == 0ull || old == key)
+                break;
+            h = (h + 1) & mask;
+        }
+        g.pall[j] = (unsigned short)h;  // the slot for now
+    }
+    __syncthreads();
+    const uint32_t seg = hcap / kDenseThreads, s0 = threadIdx.x * seg;  // hcap >= 64, a multiple of 256 or less
+    uint32_t mine = 0;
+    for (uint32_t i = 0; i < seg; ++i)
+        mine += g.hkey[s0 + i] != 0ull;
+    if (hcap < kDenseThreads)
+        mine = threadIdx.x < hcap ? (g.hkey[threadIdx.x] != 0ull) : 0u;
+    uint32_t first, m;
+    Scan(scan_tmp).ExclusiveSum(mine, first, m);
+    if (hcap < kDenseThreads) {
+        if (threadIdx.x < hcap && g.hkey[threadIdx.x]) {
+            g.hid[threadIdx.x] = (unsigned short)first;
+            g.aval[first] = (uint32_t)g.hkey[threadIdx.x];
+        }
+    } else {
+        for (uint32_t i = 0; i < seg; ++i) {
+            const unsigned long long key = g.hkey[s0 + i];
+            if (key) {
+                g.hid[s0 + i] = (unsigned short)first;
+                g.aval[first] = (uint32_t)key;
+                ++first;
+            }
         }
     }
     __syncthreads();
-    for (uint32_t size = 2; size <= m; size <<= 1) {
-        for (uint32_t stride = size >> 1; stride; stride >>= 1) {
-            for (uint32_t t = threadIdx.x; t < m / 2; t += blockDim.x) {
-                const uint32_t lo = 2 * t - (t & (stride - 1)), hi = lo + stride;
-                const bool up = (lo & size) == 0;
-                const unsigned long long x = v[lo], y = v[hi];
-                if ((x > y) == up) {
-                    v[lo] = y;
-                    v[hi] = x;
-                }
-            }
-            __syncthreads();
-        }
-    }
+    for (uint32_t j = threadIdx.x; j < k; j += kDenseThreads)
+        g.pall[j] = g.hid[g.pall[j]];
+    if (threadIdx.x == 0)
+        *scan_tot = m;
+    __syncthreads();
     return m;
 }
 
 // Alleles (distinct objects) of every listed shared group: one CTA per group.
 __global__ void __launch_bounds__(kDenseThreads) k_dense_alleles(const unsigned long long *__restrict__ list,
                                                                  uint32_t n_list, const uint64_t *__restrict__ post,
-                                                                 uint32_t *__restrict__ alleles)
+                                                                 uint32_t nref, uint32_t *__restrict__ alleles)
 {
-    extern __shared__ unsigned long long dsm[];
-    __shared__ uint32_t heads;
+    extern __shared__ __align__(16) unsigned char dsm[];
+    __shared__ uint32_t tot;
+    const DenseGroupSmem g = dense_group_view(dsm, nref);
     for (uint32_t s = blockIdx.x; s < n_list; s += gridDim.x) {
         const unsigned long long item = list[s];
-        const uint32_t b = (uint32_t)item, k = (uint32_t)(item >> 32);
+        const uint32_t m = dense_group_alleles(post, (uint32_t)item, (uint32_t)(item >> 32), g, &tot);
         if (threadIdx.x == 0)
-            heads = 0;
-        dense_sort_group(post, b, k, dsm);  // ends with a barrier
-        uint32_t mine = 0;
-        for (uint32_t j = threadIdx.x; j < k; j += blockDim.x)
-            mine += j == 0 || (dsm[j] >> 32) != (dsm[j - 1] >> 32);
-        atomicAdd(&heads, mine);
-        __syncthreads();
-        if (threadIdx.x == 0)
-            alleles[s] = heads;
-        __syncthreads();
+            alleles[s] = m;
     }
 }
 
-// Byte offset of the row buffers in k_dense_rows' shared memory (after the sorted
-// postings and the allele starts).
-constexpr size_t kDenseRowsOffset = kDenseMaxGroup * 8 + (kDenseMaxGroup + 16) * 4;
 constexpr size_t kDenseRowBudget = 160 * 1024;  // shared memory for row buffers
 
 // The operand rows of every allele, written whole (allele-major: a row runs over the
 // genomes, so the GEMM takes both operands MN-major): A'[a][q] = 1 where genome q holds
 // the allele; F[a][x * npad + r] for every genome r at the allele's context, x = 0..3:
 // 1, d >= 1, d >= 2, d = min(dna_popcount(u ^ o_r), NUM_CODENS + 1).  One CTA per group:
-// its postings sorted by object (runs = alleles, their starts from a block scan), then
-// each of nbuf warps builds one allele's rows at a time in its own shared-memory
-// buffer and stores them with 16-byte writes.
+// its alleles from the hash of its objects (numbered as in k_dense_alleles: the same
+// count, any order -- the GEMM sums over the alleles), then each of nbuf warps builds
+// one allele's rows at a time in its own shared-memory buffer and stores them with
+// 16-byte writes.
 __global__ void __launch_bounds__(kDenseThreads) k_dense_rows(const unsigned long long *__restrict__ list,
                                                               uint32_t n_list, const uint32_t *__restrict__ abase,
-                                                              const uint64_t *__restrict__ post, uint32_t npad,
-                                                              uint32_t nbuf, int8_t *__restrict__ A,
+                                                              const uint64_t *__restrict__ post, uint32_t nref,
+                                                              uint32_t npad, uint32_t nbuf, int8_t *__restrict__ A,
                                                               int8_t *__restrict__ F)
 {
-    extern __shared__ unsigned long long dsm[];
-    uint32_t *start = reinterpret_cast<uint32_t *>(dsm + kDenseMaxGroup);
-    int8_t *rows = reinterpret_cast<int8_t *>(dsm) + kDenseRowsOffset;
-    constexpr uint32_t kPer = kDenseMaxGroup / kDenseThreads;
-    using Scan = cub::BlockScan<uint32_t, kDenseThreads>;
-    __shared__ typename Scan::TempStorage scan_tmp;
+    extern __shared__ __align__(16) unsigned char dsm[];
+    __shared__ uint32_t tot;
+    const DenseGroupSmem g = dense_group_view(dsm, nref);
+    int8_t *rows = reinterpret_cast<int8_t *>(dsm) + (dense_group_smem(nref) + 15) / 16 * 16;
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (uint32_t s = blockIdx.x; s < n_list; s += gridDim.x) {
         const unsigned long long item = list[s];
-        const uint32_t b = (uint32_t)item, k = (uint32_t)(item >> 32);
-        dense_sort_group(post, b, k, dsm);
-        // allele starts: the positions where the object changes
-        uint32_t h[kPer], pos[kPer], m = 0;
-#pragma unroll
-        for (uint32_t i = 0; i < kPer; ++i) {
-            const uint32_t j = threadIdx.x * kPer + i;
-            h[i] = j < k && (j == 0 || (dsm[j] >> 32) != (dsm[j - 1] >> 32));
-        }
-        Scan(scan_tmp).ExclusiveSum(h, pos, m);
-#pragma unroll
-        for (uint32_t i = 0; i < kPer; ++i)
-            if (h[i])
-                start[pos[i]] = threadIdx.x * kPer + i;
-        if (threadIdx.x == 0)
-            start[m] = k;
-        __syncthreads();
+        const uint32_t k = (uint32_t)(item >> 32);
+        const uint32_t m = dense_group_alleles(post, (uint32_t)item, k, g, &tot);
         const uint32_t a0 = abase[s];
         if (warp < nbuf) {
             int8_t *row = rows + (size_t)warp * 5 * npad;
@@ -2121,13 +2161,12 @@ __global__ void __launch_bounds__(kDenseThreads) k_dense_rows(const unsigned lon
                 for (uint32_t w = lane; w < 5 * npad / 16; w += 32)
                     r4[w] = make_uint4(0u, 0u, 0u, 0u);
                 __syncwarp();
-                const uint32_t rb = start[a], re = start[a + 1];
-                const uint32_t u = (uint32_t)(dsm[rb] >> 32);
+                const uint32_t u = g.aval[a];
                 int8_t *f = row + npad;
                 for (uint32_t j = lane; j < k; j += 32) {
-                    const uint32_t o = (uint32_t)(dsm[j] >> 32), r = (uint32_t)dsm[j];
+                    const uint32_t o = g.pobj[j], r = g.pgid[j];
                     const int d = min(kMinInit, dna_pop(u ^ o));
-                    if (j >= rb && j < re)
+                    if (g.pall[j] == a)
                         row[r] = 1;
                     f[r] = 1;
                     f[npad + r] = (int8_t)(d >= 1);
@@ -2144,7 +2183,7 @@ __global__ void __launch_bounds__(kDenseThreads) k_dense_rows(const unsigned lon
                 __syncwarp();
             }
         }
-        __syncthreads();  // the sorted postings and the starts are reused by the next group
+        __syncthreads();  // the group's arrays are reused by the next group
     }
 }
 
@@ -3869,10 +3908,13 @@ int self_dense_impl(kssdgpu_index *ix, unsigned long long *oc, unsigned long lon
         return KSSDGPU_OK;
     }
     const uint32_t npad = (uint32_t)dense_npad(ix);
-    const size_t sort_smem = kDenseMaxGroup * sizeof(unsigned long long);
-    const uint32_t nbuf = (uint32_t)std::max<size_t>(1, std::min<size_t>(8, kDenseRowBudget / (5 * (size_t)npad)));
-    const size_t rows_smem = kDenseRowsOffset + (size_t)nbuf * 5 * npad;
-    CUDA_TRY(cudaFuncSetAttribute(k_dense_alleles, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sort_smem));
+    const size_t group_smem = dense_group_smem((uint32_t)n);
+    const size_t group_al = (group_smem + 15) / 16 * 16;
+    // row buffers in what is left of the 227 KB a CTA may hold (at most kDenseRowBudget)
+    const size_t row_room = std::min<size_t>(kDenseRowBudget, 232448 - 4096 - group_al);
+    const uint32_t nbuf = (uint32_t)std::max<size_t>(1, std::min<size_t>(8, row_room / (5 * (size_t)npad)));
+    const size_t rows_smem = group_al + (size_t)nbuf * 5 * npad;
+    CUDA_TRY(cudaFuncSetAttribute(k_dense_alleles, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)group_smem));
     CUDA_TRY(cudaFuncSetAttribute(k_dense_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rows_smem));
     CUDA_TRY(ix->d_list.ensure(S));
     CUDA_TRY(ix->d_poff.ensure((size_t)S + 1));   // alleles per group, then the fill counter
@@ -3885,7 +3927,7 @@ int self_dense_impl(kssdgpu_index *ix, unsigned long long *oc, unsigned long lon
     CUDA_TRY(cudaMemsetAsync(d_count, 0, sizeof(unsigned int), st));
     k_dense_list<<<grid_for(ix->u), 256, 0, st>>>(ix->gbeg, ix->u, ix->d_list.p, d_count);
     const int grid = ix->sms * 4;
-    k_dense_alleles<<<grid, kDenseThreads, sort_smem, st>>>(ix->d_list.p, S, ix->post, ix->d_poff.p);
+    k_dense_alleles<<<grid, kDenseThreads, group_smem, st>>>(ix->d_list.p, S, ix->post, (uint32_t)n, ix->d_poff.p);
     CUDA_TRY(cudaMemsetAsync(d_count, 0, sizeof(unsigned int), st));  // poff[S] = 0: the scan's last term
     tb = ix->d_tmp.cap;
     CUDA_TRY(cub::DeviceScan::ExclusiveSum(ix->d_tmp.p, tb, ix->d_poff.p, ix->d_allele.p, (int)S + 1, st));
@@ -3910,8 +3952,8 @@ int self_dense_impl(kssdgpu_index *ix, unsigned long long *oc, unsigned long lon
         CUDA_TRY(cudaMemsetAsync(ix->d_a.p + (size_t)alleles * npad, 0, (size_t)(kpad - alleles) * npad, st));
         CUDA_TRY(cudaMemsetAsync(ix->d_f.p + (size_t)alleles * 4 * npad, 0, (size_t)(kpad - alleles) * 4 * npad, st));
     }
-    k_dense_rows<<<grid, kDenseThreads, rows_smem, st>>>(ix->d_list.p, S, ix->d_allele.p, ix->post, npad, nbuf,
-                                                         ix->d_a.p, ix->d_f.p);
+    k_dense_rows<<<grid, kDenseThreads, rows_smem, st>>>(ix->d_list.p, S, ix->d_allele.p, ix->post, (uint32_t)n, npad,
+                                                         nbuf, ix->d_a.p, ix->d_f.p);
     count_launch();
     CUDA_TRY(cudaGetLastError());
     // 3. D = A' F^T on the tensor cores (both operands MN-major)
