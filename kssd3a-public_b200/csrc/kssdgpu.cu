@@ -2051,9 +2051,9 @@ __device__ __forceinline__ DenseGroupSmem dense_group_view(unsigned char *base, 
 // instead of a sort: every posting's object is inserted into the hash (CAS on an empty
 // slot, linear probing; 2k slots for at most k objects), each thread numbers the
 // occupied slots of its contiguous segment after one block scan of their counts.
-// Returns m; ends with a barrier.
+// Returns m (on every thread); ends with a barrier.
 __device__ uint32_t dense_group_alleles(const uint64_t *__restrict__ post, uint32_t b, uint32_t k,
-                                        const DenseGroupSmem &g, uint32_t *scan_tot)
+                                        const DenseGroupSmem &g)
 {
     using Scan = cub::BlockScan<uint32_t, kDenseThreads>;
     __shared__ typename Scan::TempStorage scan_tmp;
@@ -2106,8 +2106,6 @@ __device__ uint32_t dense_group_alleles(const uint64_t *__restrict__ post, uint3
     __syncthreads();
     for (uint32_t j = threadIdx.x; j < k; j += kDenseThreads)
         g.pall[j] = g.hid[g.pall[j]];
-    if (threadIdx.x == 0)
-        *scan_tot = m;
     __syncthreads();
     return m;
 }
@@ -2118,11 +2116,10 @@ __global__ void __launch_bounds__(kDenseThreads) k_dense_alleles(const unsigned 
                                                                  uint32_t nref, uint32_t *__restrict__ alleles)
 {
     extern __shared__ __align__(16) unsigned char dsm[];
-    __shared__ uint32_t tot;
     const DenseGroupSmem g = dense_group_view(dsm, nref);
     for (uint32_t s = blockIdx.x; s < n_list; s += gridDim.x) {
         const unsigned long long item = list[s];
-        const uint32_t m = dense_group_alleles(post, (uint32_t)item, (uint32_t)(item >> 32), g, &tot);
+        const uint32_t m = dense_group_alleles(post, (uint32_t)item, (uint32_t)(item >> 32), g);
         if (threadIdx.x == 0)
             alleles[s] = m;
     }
@@ -2145,14 +2142,13 @@ __global__ void __launch_bounds__(kDenseThreads) k_dense_rows(const unsigned lon
                                                               int8_t *__restrict__ F)
 {
     extern __shared__ __align__(16) unsigned char dsm[];
-    __shared__ uint32_t tot;
     const DenseGroupSmem g = dense_group_view(dsm, nref);
     int8_t *rows = reinterpret_cast<int8_t *>(dsm) + (dense_group_smem(nref) + 15) / 16 * 16;
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (uint32_t s = blockIdx.x; s < n_list; s += gridDim.x) {
         const unsigned long long item = list[s];
         const uint32_t k = (uint32_t)(item >> 32);
-        const uint32_t m = dense_group_alleles(post, (uint32_t)item, k, g, &tot);
+        const uint32_t m = dense_group_alleles(post, (uint32_t)item, k, g);
         const uint32_t a0 = abase[s];
         if (warp < nbuf) {
             int8_t *row = rows + (size_t)warp * 5 * npad;

@@ -94,6 +94,14 @@ CASES = [
     ("self_full_indexed_dist", ["ani", "-q", "{refs40}", "-m1"], {"KSSD3A_ANI_MATRIX_DIRECT_THRESHOLD": "0"}),
     ("self_triangle_direct", ["ani", "-q", "{refs40}", "-m2", "-d", "-s", "-1"], {}),
     ("self_triangle_indexed", ["ani", "-q", "{refs120}", "-m2"], {"KSSD3A_ANI_MATRIX_DIRECT_THRESHOLD": "0"}),
+    # self matrices whose values come from log / pow (Naive, Mash, AAF): the device's
+    # FP64 epilogue hands cells next to a rounding boundary to the host
+    ("self_full_indexed_naive_ani", ["ani", "-q", "{refs120}", "--format", "matrix", "-s", "-4"],
+     {"KSSD3A_ANI_MATRIX_DIRECT_THRESHOLD": "0"}),
+    ("self_full_mash", ["ani", "-q", "{refs120}", "--format", "matrix", "-s", "5"], {}),
+    ("self_triangle_aaf_ani", ["ani", "-q", "{refs40}", "-m2", "-s", "-6"], {}),
+    ("self_matrix_reads_ignoreconflict", ["ani", "-q", "{reads6}", "--format", "matrix", "--values", "ani",
+                                          "--ignoreconflict"], {}),
     ("reads_qraw", ["ani", "-r", "{refs120i}", "--qraw", "{reads6}", "-n", "0.8"], {}),
     ("reads_qraw_unique", ["ani", "-r", "{refs120i}", "--qraw", "{reads6}", "-n", "0.95", "--unique-ctx"], {}),
     ("reads_qraw_ignoreconflict", ["ani", "-r", "{refs120i}", "--qraw", "{reads6}", "-n", "0.5", "--ignoreconflict"],
