@@ -243,6 +243,15 @@ constexpr int kMaxStripes = 256;
 constexpr uint64_t kStripeChunk = 256;
 constexpr uint64_t kStripeItemsMax = 1ull << 20;
 
+// An open-addressing table of touched counter cells (see table_credit below).
+constexpr uint32_t kCellEmpty = 0xFFFFFFFFu;
+
+struct CellTable {
+    uint32_t *key;            // cell number, kCellEmpty for a free slot (null: no table)
+    unsigned long long *acc;  // per slot: ctx word (num_mut2 << 32 | num_ctx), obj word (section << 32 | diff_obj)
+    int log;                  // 2^log slots
+};
+
 struct CountParams {
     const Slot *table;
     uint32_t mask;
@@ -296,6 +305,48 @@ struct SmemAcc {
     }
 };
 
+// Where a counter array spans far more memory than L2 (the 20,000-genome lower
+// triangle: 3.2 GB), its touched cells lie scattered
+// over the whole span and every add into them is slow -- atomics onto a fixed set of
+// addresses spread over 1.6 GB run at 38 G/s on a B200 against 130 G/s when the same
+// addresses fit in 16 MB -- although the touched cells themselves are few (92,633).
+// The self join's scan then adds into a compact open-addressing table of touched cells
+// instead (2^21 slots by default: a cell
+// number and its two counter words, 40 MB), claimed by the first credit of a cell that
+// finds a free slot among its first kCellTableProbes; a cell whose probes find no room
+// goes to the array directly.  Keys only go from empty to a cell while a kernel runs and
+// every credit of a cell probes the same sequence, so a cell lives in one slot or in the
+// array, never both; k_cell_table_flush adds the slots into the array after the kernel
+// and empties them for the next call.
+constexpr int kCellTableLog = 21;
+constexpr uint32_t kCellTableProbes = 8;
+
+
+// One credit of difference d into the cell's slot; false when its probes find no room.
+__device__ __forceinline__ bool table_credit(const CellTable &T, uint32_t cell, int d)
+{
+    const uint32_t mask = (1u << T.log) - 1;
+    uint32_t s = (cell * 2654435761u) >> (32 - T.log);
+    for (uint32_t p = 0; p < kCellTableProbes; ++p) {
+        uint32_t k = __ldcg(T.key + s);  // from L2: keys are claimed while the kernel runs
+        if (k == kCellEmpty) {
+            const uint32_t old = atomicCAS(T.key + s, kCellEmpty, cell);
+            k = old == kCellEmpty ? cell : old;
+        }
+        if (k == cell) {
+            atomicAdd(T.acc + 2 * (size_t)s, inc_ctx(d));
+            if (d)
+                atomicAdd(T.acc + 2 * (size_t)s + 1, inc_obj(d));
+            return true;
+        }
+        s = (s + 1) & mask;
+    }
+    return false;
+}
+
+// A query's global counter row.  (Through the table of touched cells, the 10,000 x
+// 20,000 block's count measured 2.24 vs 2.18 ms: unlike the self join's, its credits'
+// cost is not the scattered addresses, and the key load per credit adds latency.)
 struct GlobalAcc {
     unsigned long long *c, *o;
     __device__ __forceinline__ void add(uint32_t gid, int d) const
@@ -1541,7 +1592,6 @@ constexpr uint32_t kScanThreads = 256;
 #endif
 constexpr uint32_t kScanPerThread = KSSD_SCAN_PER_THREAD;
 constexpr uint32_t kScanTile = kScanThreads * kScanPerThread;  // groups per tile (4 B of gbeg each)
-constexpr uint32_t kCellEmpty = 0xFFFFFFFFu;
 constexpr uint32_t kScanLaneMax = 32;                          // larger groups: the whole CTA
 
 __device__ __forceinline__ void credit_lower(unsigned long long *__restrict__ oc, unsigned long long *__restrict__ oo,
@@ -1625,50 +1675,12 @@ struct ScanSmem {
     unsigned short pair[kScanPairRanks];  // (i, j) of every pair rank of a small group: i | j << 8
 };
 
-// Where the lower triangle spans far more memory than L2 (20,000 genomes: 3.2 GB), its
-// touched cells lie scattered over the whole span and every add into them is slow --
-// atomics onto a fixed set of addresses spread over 1.6 GB run at 38 G/s on a B200
-// against 130 G/s when the same addresses fit in 16 MB -- although the touched cells
-// themselves are few (20,000 genomes: 92,633).  The scan then adds into a compact
-// open-addressing table of touched cells instead (2^21 slots by default: a cell number
-// and its two counter words, 40 MB), claimed by the first credit of a cell that finds a
-// free slot among its first kCellTableProbes; a cell whose probes find no room goes to
-// the triangle directly.  Keys only go from empty to a cell while the join runs and
-// every credit of a cell probes the same sequence, so a cell lives in one slot or in the
-// triangle, never both; k_cell_table_flush adds the slots into the triangle after the
-// join and empties them for the next call.
-constexpr int kCellTableLog = 21;
-constexpr uint32_t kCellTableProbes = 8;
-
-struct CellTable {
-    uint32_t *key;            // cell number, kCellEmpty for a free slot (null: no table)
-    unsigned long long *acc;  // per slot: ctx word (num_mut2 << 32 | num_ctx), obj word (section << 32 | diff_obj)
-    int log;                  // 2^log slots
-};
-
 // One credit into the table, or into the triangle (no table, or no room).
 __device__ __forceinline__ void credit_global(const CellTable &T, unsigned long long *__restrict__ oc,
                                               unsigned long long *__restrict__ oo, uint32_t qg, uint32_t rg, int d)
 {
-    if (T.key) {
-        const uint32_t cell = (uint32_t)lower_cell(qg, rg);
-        const uint32_t mask = (1u << T.log) - 1;
-        uint32_t s = (cell * 2654435761u) >> (32 - T.log);
-        for (uint32_t p = 0; p < kCellTableProbes; ++p) {
-            uint32_t k = __ldcg(T.key + s);  // from L2: keys are claimed while the join runs
-            if (k == kCellEmpty) {
-                const uint32_t old = atomicCAS(T.key + s, kCellEmpty, cell);
-                k = old == kCellEmpty ? cell : old;
-            }
-            if (k == cell) {
-                atomicAdd(T.acc + 2 * (size_t)s, inc_ctx(d));
-                if (d)
-                    atomicAdd(T.acc + 2 * (size_t)s + 1, inc_obj(d));
-                return;
-            }
-            s = (s + 1) & mask;
-        }
-    }
+    if (T.key && table_credit(T, (uint32_t)lower_cell(qg, rg), d))
+        return;
     credit_lower(oc, oo, qg, rg, d);
 }
 
@@ -2743,6 +2755,25 @@ int check_dev_err(kssdgpu_index *ix, cudaStream_t st)
     return KSSDGPU_OK;
 }
 
+uint32_t env_u32(const char *name, uint32_t def, uint32_t lo, uint32_t hi);
+
+// The index's table of touched cells (allocated on first use with 2^KSSDGPU_CELL_TABLE_LOG
+// slots, default 2^21; empty between calls: every kernel that fills it is followed by
+// k_cell_table_flush on the same stream).
+int cell_table(kssdgpu_index *ix, cudaStream_t st, CellTable &t)
+{
+    if (!ix->c_key.p || !ix->c_acc.p) {
+        ix->c_log = (int)env_u32("KSSDGPU_CELL_TABLE_LOG", kCellTableLog, 4, 26);
+        const size_t slots = (size_t)1 << ix->c_log;
+        CUDA_TRY(ix->c_key.ensure(slots));
+        CUDA_TRY(ix->c_acc.ensure(2 * slots));
+        CUDA_TRY(cudaMemsetAsync(ix->c_key.p, 0xFF, slots * 4, st));
+        CUDA_TRY(cudaMemsetAsync(ix->c_acc.p, 0, slots * 16, st));
+    }
+    t = CellTable{ix->c_key.p, ix->c_acc.p, ix->c_log};
+    return KSSDGPU_OK;
+}
+
 template <bool LOWER, bool UNIQUE, bool SMEM>
 int launch_batched(kssdgpu_index *ix, const CountParams &P, size_t smem, cudaStream_t st)
 {
@@ -3809,16 +3840,9 @@ int self_scan_impl(kssdgpu_index *ix, unsigned flags, unsigned long long *oc, un
     const bool big = cells < (size_t)kCellEmpty && cells * 16 > (size_t)ix->l2_bytes;
     CellTable table{nullptr, nullptr, 0};
     if (ix->u && pairs && big) {
-        if (!ix->c_key.p || !ix->c_acc.p)
-            ix->c_log = (int)env_u32("KSSDGPU_CELL_TABLE_LOG", kCellTableLog, 4, 26);
-        const size_t slots = (size_t)1 << ix->c_log;
-        if (!ix->c_key.p || !ix->c_acc.p) {
-            CUDA_TRY(ix->c_key.ensure(slots));
-            CUDA_TRY(ix->c_acc.ensure(2 * slots));
-            CUDA_TRY(cudaMemsetAsync(ix->c_key.p, 0xFF, slots * 4, st));
-            CUDA_TRY(cudaMemsetAsync(ix->c_acc.p, 0, slots * 16, st));
-        }
-        table = CellTable{ix->c_key.p, ix->c_acc.p, ix->c_log};
+        int rc = cell_table(ix, st, table);
+        if (rc)
+            return rc;
     }
     bool after_fill = false;
     if (!(flags & KSSDGPU_NO_ZERO)) {

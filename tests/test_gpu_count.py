@@ -729,3 +729,39 @@ def test_batched_count_on_long_postings_lists(case):
         np.testing.assert_array_equal(g, w)
     assert want[0][:, :, 0].sum() > 0
     idx.close()
+
+
+@pytest.mark.parametrize("case", ["block", "lower", "striped", "tiny_table"])
+def test_batched_count_beyond_l2(case, monkeypatch):
+    """A block of 2,500 queries x 4,000 references (10M counter cells, 160 MB: larger
+    than L2) through the global-row count, chunked and stripe-major, and as a lower
+    block; the table of touched cells shrunk to 16 slots must not matter (the count adds
+    into its rows directly).  Counters equal the oracle's, on two calls in a row."""
+    if case == "tiny_table":
+        monkeypatch.setenv("KSSDGPU_CELL_TABLE_LOG", "4")
+    ref = kssdgpu.synth(n_samples=4000, n_clusters=400, len_median=8e4, len_min=5e4, len_max=1.5e5,
+                        size_dist=kssdgpu.SIZE_LOGNORMAL, sub_lo=0.001, sub_hi=0.1, seed=81, sample_seed=81)
+    rec = oracle.build_index(ref.keys, ref.offs)
+    idx = kssdgpu.Index.from_records(rec, ref.n)
+    if case == "striped":
+        assert idx.filter(1 << 16)["stripes"] > 1
+    if case == "lower":
+        off = 1500
+        qk = ref.keys[int(ref.offs[off]):int(ref.offs[off + 2500])]
+        qo = np.ascontiguousarray(ref.offs[off:off + 2501])
+        want = oracle.count_lower(rec, ref.n, off, qk, qo)
+        for _ in range(2):
+            got = idx.count_lower(qk, qo, off, kssdgpu.GLOBAL_ACC)
+            for g, w in zip(got, want):
+                np.testing.assert_array_equal(g, w)
+    else:
+        qry = kssdgpu.synth(n_samples=2500, n_clusters=400, role=kssdgpu.ROLE_OWNLEN, len_median=8e4, len_min=5e4,
+                            len_max=1.5e5, size_dist=kssdgpu.SIZE_LOGNORMAL, sub_lo=0.001, sub_hi=0.1, seed=81,
+                            sample_seed=82, own_len_min=2e4, own_len_max=1.5e5)
+        want = oracle.count_block(rec, ref.n, qry.keys, qry.offs)
+        for _ in range(2):
+            got = idx.count_block(qry.keys, qry.offs, kssdgpu.GLOBAL_ACC)
+            for g, w in zip(got, want):
+                np.testing.assert_array_equal(g, w)
+    assert want[0][:, :, 0].sum() > 0
+    idx.close()
