@@ -4,6 +4,7 @@
     python kssd3a-public_b200/profile_cases.py scanbig # 5,000 small genomes: triangle beyond L2 (cell table)
     python kssd3a-public_b200/profile_cases.py dense   # 512-genome one-species dense join, 2 steps
     python kssd3a-public_b200/profile_cases.py rect    # 2,000 queries x 4,000 references, 4 batched counts
+    python kssd3a-public_b200/profile_cases.py denseprobe  # 128 queries x 512 one-species references, 3 counts
 
 Each case builds its index from a seeded synthetic sketch (the generators of the
 benchmark), runs a few launches of the kernel under study on cuda:0 and exits, so
@@ -74,6 +75,26 @@ def case_dense(dev, st):
     idx.close()
 
 
+def case_denseprobe(dev, st):
+    """The batched probe on a one-species index: 512 references and 128 new members of the
+    species (context groups of hundreds of postings, walked by whole warps)."""
+    ref = kssdgpu.synth(n_samples=512, n_clusters=1, size_dist=kssdgpu.SIZE_LOGNORMAL, len_median=4e6, len_sigma=0.2,
+                        len_min=2e6, len_max=8e6, sub_lo=0.001, sub_hi=0.02, seed=7, sample_seed=7, threads=THREADS)
+    qry = kssdgpu.synth(n_samples=128, n_clusters=1, role=kssdgpu.ROLE_OWNLEN, size_dist=kssdgpu.SIZE_LOGNORMAL,
+                        len_median=4e6, len_sigma=0.2, len_min=2e6, len_max=8e6, own_len_min=1e6, own_len_max=8e6,
+                        sub_lo=0.001, sub_hi=0.02, seed=7, sample_seed=8, threads=THREADS)
+    idx = kssdgpu.Index.from_sketch(ref)
+    dk = torch.from_numpy(qry.keys.view(np.int64)).to(dev)
+    do = torch.from_numpy(qry.offs.view(np.int64)).to(dev)
+    c = torch.zeros(qry.n * ref.n, dtype=torch.int64, device=dev)
+    o = torch.zeros_like(c)
+    for _ in range(3):
+        idx.count_block_dev(dk, do, qry.n, c, o, flags=kssdgpu.GLOBAL_ACC, stream=st)
+    torch.cuda.synchronize()
+    print("keys", int(qry.offs[-1]), "credits", int((c & 0xFFFFFFFF).sum().item()))
+    idx.close()
+
+
 def case_rect(dev, st):
     nr, nq = 4000, 2000
     ref = kssdgpu.synth(n_samples=nr, n_clusters=nr // 10, size_dist=kssdgpu.SIZE_LOGNORMAL, len_median=4e6,
@@ -96,10 +117,11 @@ def case_rect(dev, st):
 
 
 def main(argv):
-    cases = {"scan": case_scan, "scanbig": case_scanbig, "dense": case_dense, "rect": case_rect}
+    cases = {"scan": case_scan, "scanbig": case_scanbig, "dense": case_dense, "rect": case_rect,
+             "denseprobe": case_denseprobe}
     which = argv[1] if len(argv) > 1 else ""
     if which not in cases:
-        print("usage: profile_cases.py scan|scanbig|dense|rect", file=sys.stderr)
+        print("usage: profile_cases.py scan|scanbig|dense|rect|denseprobe", file=sys.stderr)
         return 64
     if not torch.cuda.is_available():
         print("profile_cases.py: needs a CUDA device", file=sys.stderr)
