@@ -2137,59 +2137,88 @@ __global__ void __launch_bounds__(kDenseThreads) k_dense_alleles(const unsigned 
     }
 }
 
-constexpr size_t kDenseRowBudget = 160 * 1024;  // shared memory for row buffers
+// Genome -> object map of one group for k_dense_rows: the object of genome r as a u32
+// word and a presence bit.  The words sit in 16-byte chunks (4 genomes) swizzled inside
+// blocks of 8 chunks (chunk c at c ^ ((c >> 3) & 7)), so that the 8 lanes of a quarter
+// warp, which read the chunks 4w + q of 8 consecutive w, hit 8 different bank groups.
+__host__ __device__ __forceinline__ uint32_t dense_gobj_words(uint32_t npad) { return (npad + 31) / 32 * 32; }
+__host__ __device__ __forceinline__ size_t dense_rows_smem(uint32_t nref, uint32_t npad)
+{
+    return (dense_group_smem(nref) + 15) / 16 * 16 + (size_t)dense_gobj_words(npad) * 4 +
+           (size_t)dense_gobj_words(npad) / 8;
+}
+__device__ __forceinline__ uint32_t dense_gobj_slot(uint32_t r)
+{
+    const uint32_t c = r >> 2;
+    return ((c ^ ((c >> 3) & 7u)) << 2) | (r & 3u);
+}
 
 // The operand rows of every allele, written whole (allele-major: a row runs over the
 // genomes, so the GEMM takes both operands MN-major): A'[a][q] = 1 where genome q holds
 // the allele; F[a][x * npad + r] for every genome r at the allele's context, x = 0..3:
 // 1, d >= 1, d >= 2, d = min(dna_popcount(u ^ o_r), NUM_CODENS + 1).  One CTA per group:
 // its alleles from the hash of its objects (numbered as in k_dense_alleles: the same
-// count, any order -- the GEMM sums over the alleles), then each of nbuf warps builds
-// one allele's rows at a time in its own shared-memory buffer and stores them with
-// 16-byte writes.
+// count, any order -- the GEMM sums over the alleles) and a genome -> object map; then
+// every thread of the CTA takes (allele, 16 genomes) pieces, consecutive threads on
+// consecutive genomes of one allele, and stores the piece's five 16-byte words (A' and
+// the four F rows) straight to the operands, zeros included.
 __global__ void __launch_bounds__(kDenseThreads) k_dense_rows(const unsigned long long *__restrict__ list,
                                                               uint32_t n_list, const uint32_t *__restrict__ abase,
                                                               const uint64_t *__restrict__ post, uint32_t nref,
-                                                              uint32_t npad, uint32_t nbuf, int8_t *__restrict__ A,
+                                                              uint32_t npad, int8_t *__restrict__ A,
                                                               int8_t *__restrict__ F)
 {
     extern __shared__ __align__(16) unsigned char dsm[];
     const DenseGroupSmem g = dense_group_view(dsm, nref);
-    int8_t *rows = reinterpret_cast<int8_t *>(dsm) + (dense_group_smem(nref) + 15) / 16 * 16;
-    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    uint32_t *gobj = reinterpret_cast<uint32_t *>(dsm + (dense_group_smem(nref) + 15) / 16 * 16);
+    uint32_t *gbit = gobj + dense_gobj_words(npad);
+    const uint32_t nchunk = npad / 16, nbit = dense_gobj_words(npad) / 32;
     for (uint32_t s = blockIdx.x; s < n_list; s += gridDim.x) {
         const unsigned long long item = list[s];
         const uint32_t k = (uint32_t)(item >> 32);
         const uint32_t m = dense_group_alleles(post, (uint32_t)item, k, g);
+        for (uint32_t i = threadIdx.x; i < nbit; i += kDenseThreads)
+            gbit[i] = 0u;
+        __syncthreads();
+        for (uint32_t j = threadIdx.x; j < k; j += kDenseThreads) {
+            const uint32_t r = g.pgid[j];
+            gobj[dense_gobj_slot(r)] = g.pobj[j];
+            atomicOr(&gbit[r >> 5], 1u << (r & 31u));
+        }
+        __syncthreads();
         const uint32_t a0 = abase[s];
-        if (warp < nbuf) {
-            int8_t *row = rows + (size_t)warp * 5 * npad;
-            uint4 *r4 = reinterpret_cast<uint4 *>(row);
-            for (uint32_t a = warp; a < m; a += nbuf) {
-                for (uint32_t w = lane; w < 5 * npad / 16; w += 32)
-                    r4[w] = make_uint4(0u, 0u, 0u, 0u);
-                __syncwarp();
-                const uint32_t u = g.aval[a];
-                int8_t *f = row + npad;
-                for (uint32_t j = lane; j < k; j += 32) {
-                    const uint32_t o = g.pobj[j], r = g.pgid[j];
-                    const int d = min(kMinInit, dna_pop(u ^ o));
-                    if (g.pall[j] == a)
-                        row[r] = 1;
-                    f[r] = 1;
-                    f[npad + r] = (int8_t)(d >= 1);
-                    f[2 * npad + r] = (int8_t)(d >= 2);
-                    f[3 * npad + r] = (int8_t)d;
+        for (uint32_t t = threadIdx.x; t < m * nchunk; t += kDenseThreads) {
+            const uint32_t a = t / nchunk, w = t - a * nchunk;
+            const uint32_t u = g.aval[a];
+            const uint32_t bits = (gbit[w >> 1] >> ((w & 1u) * 16)) & 0xFFFFu;
+            uint32_t av[4], f0[4], f1[4], f2[4], f3[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const uint32_t c = 4 * w + q;
+                const uint4 o4 = *reinterpret_cast<const uint4 *>(gobj + ((c ^ ((c >> 3) & 7u)) << 2));
+                const uint32_t ov[4] = {o4.x, o4.y, o4.z, o4.w};
+                av[q] = f0[q] = f1[q] = f2[q] = f3[q] = 0u;
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    if ((bits >> (4 * q + e)) & 1u) {
+                        const uint32_t o = ov[e];
+                        const uint32_t d = (uint32_t)min(kMinInit, dna_pop(u ^ o));
+                        const int sh = 8 * e;
+                        av[q] |= (uint32_t)(o == u) << sh;
+                        f0[q] |= 1u << sh;
+                        f1[q] |= (uint32_t)(d >= 1) << sh;
+                        f2[q] |= (uint32_t)(d >= 2) << sh;
+                        f3[q] |= d << sh;
+                    }
                 }
-                __syncwarp();
-                uint4 *ga = reinterpret_cast<uint4 *>(A + (size_t)(a0 + a) * npad);
-                uint4 *gf = reinterpret_cast<uint4 *>(F + (size_t)(a0 + a) * 4 * npad);
-                for (uint32_t w = lane; w < npad / 16; w += 32)
-                    ga[w] = r4[w];
-                for (uint32_t w = lane; w < 4 * npad / 16; w += 32)
-                    gf[w] = r4[npad / 16 + w];
-                __syncwarp();
             }
+            const size_t row = (size_t)(a0 + a);
+            reinterpret_cast<uint4 *>(A + row * npad)[w] = make_uint4(av[0], av[1], av[2], av[3]);
+            uint4 *fr = reinterpret_cast<uint4 *>(F + row * 4 * npad);
+            fr[w] = make_uint4(f0[0], f0[1], f0[2], f0[3]);
+            fr[nchunk + w] = make_uint4(f1[0], f1[1], f1[2], f1[3]);
+            fr[2 * nchunk + w] = make_uint4(f2[0], f2[1], f2[2], f2[3]);
+            fr[3 * nchunk + w] = make_uint4(f3[0], f3[1], f3[2], f3[3]);
         }
         __syncthreads();  // the group's arrays are reused by the next group
     }
@@ -3903,7 +3932,7 @@ uint64_t dense_bytes(const kssdgpu_index *ix, uint64_t kpad)
 uint64_t round_up(uint64_t x, uint64_t m) { return (x + m - 1) / m * m; }
 
 // Dense self join (see k_dense_list): list the shared groups, count their alleles
-// (distinct objects, from a sort of each group's postings in shared memory), build
+// (distinct objects, from a hash of each group's objects in shared memory), build
 // every allele's operand rows, one tensor-core GEMM, and the packed lower triangle
 // (every cell written, so no zero fill).  Conflict-free indexes of at most
 // kDenseMaxGroup references only; the operands must fit in half of the free memory.
@@ -3929,11 +3958,7 @@ int self_dense_impl(kssdgpu_index *ix, unsigned long long *oc, unsigned long lon
     }
     const uint32_t npad = (uint32_t)dense_npad(ix);
     const size_t group_smem = dense_group_smem((uint32_t)n);
-    const size_t group_al = (group_smem + 15) / 16 * 16;
-    // row buffers in what is left of the 227 KB a CTA may hold (at most kDenseRowBudget)
-    const size_t row_room = std::min<size_t>(kDenseRowBudget, 232448 - 4096 - group_al);
-    const uint32_t nbuf = (uint32_t)std::max<size_t>(1, std::min<size_t>(8, row_room / (5 * (size_t)npad)));
-    const size_t rows_smem = group_al + (size_t)nbuf * 5 * npad;
+    const size_t rows_smem = dense_rows_smem((uint32_t)n, npad);
     CUDA_TRY(cudaFuncSetAttribute(k_dense_alleles, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)group_smem));
     CUDA_TRY(cudaFuncSetAttribute(k_dense_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rows_smem));
     CUDA_TRY(ix->d_list.ensure(S));
@@ -3946,8 +3971,13 @@ int self_dense_impl(kssdgpu_index *ix, unsigned long long *oc, unsigned long lon
     // 1. the shared groups, their allele counts and first allele rows
     CUDA_TRY(cudaMemsetAsync(d_count, 0, sizeof(unsigned int), st));
     k_dense_list<<<grid_for(ix->u), 256, 0, st>>>(ix->gbeg, ix->u, ix->d_list.p, d_count);
-    const int grid = ix->sms * 4;
-    k_dense_alleles<<<grid, kDenseThreads, group_smem, st>>>(ix->d_list.p, S, ix->post, (uint32_t)n, ix->d_poff.p);
+    // persistent CTAs over the groups: as many as fit on an SM at once (the group's
+    // barriers and dependent loads leave one CTA mostly waiting)
+    int per_sm_al = 0, per_sm_rows = 0;
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_al, k_dense_alleles, kDenseThreads, group_smem));
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_rows, k_dense_rows, kDenseThreads, rows_smem));
+    const int grid_al = ix->sms * std::max(1, per_sm_al), grid = ix->sms * std::max(1, per_sm_rows);
+    k_dense_alleles<<<grid_al, kDenseThreads, group_smem, st>>>(ix->d_list.p, S, ix->post, (uint32_t)n, ix->d_poff.p);
     CUDA_TRY(cudaMemsetAsync(d_count, 0, sizeof(unsigned int), st));  // poff[S] = 0: the scan's last term
     tb = ix->d_tmp.cap;
     CUDA_TRY(cub::DeviceScan::ExclusiveSum(ix->d_tmp.p, tb, ix->d_poff.p, ix->d_allele.p, (int)S + 1, st));
@@ -3973,7 +4003,7 @@ int self_dense_impl(kssdgpu_index *ix, unsigned long long *oc, unsigned long lon
         CUDA_TRY(cudaMemsetAsync(ix->d_f.p + (size_t)alleles * 4 * npad, 0, (size_t)(kpad - alleles) * 4 * npad, st));
     }
     k_dense_rows<<<grid, kDenseThreads, rows_smem, st>>>(ix->d_list.p, S, ix->d_allele.p, ix->post, (uint32_t)n, npad,
-                                                         nbuf, ix->d_a.p, ix->d_f.p);
+                                                         ix->d_a.p, ix->d_f.p);
     count_launch();
     CUDA_TRY(cudaGetLastError());
     // 3. D = A' F^T on the tensor cores (both operands MN-major)
