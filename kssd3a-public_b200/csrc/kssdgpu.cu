@@ -2122,18 +2122,25 @@ __device__ uint32_t dense_group_alleles(const uint64_t *__restrict__ post, uint3
     return m;
 }
 
-// Alleles (distinct objects) of every listed shared group: one CTA per group.
+// Alleles (distinct objects) of every listed shared group: one CTA per group.  The
+// count goes to alleles[s]; the values, in allele-number order, to aval[b..b + m) where b
+// is the group's first posting (a group has at least as many postings as alleles).
 __global__ void __launch_bounds__(kDenseThreads) k_dense_alleles(const unsigned long long *__restrict__ list,
                                                                  uint32_t n_list, const uint64_t *__restrict__ post,
-                                                                 uint32_t nref, uint32_t *__restrict__ alleles)
+                                                                 uint32_t nref, uint32_t *__restrict__ alleles,
+                                                                 uint32_t *__restrict__ aval)
 {
     extern __shared__ __align__(16) unsigned char dsm[];
     const DenseGroupSmem g = dense_group_view(dsm, nref);
     for (uint32_t s = blockIdx.x; s < n_list; s += gridDim.x) {
         const unsigned long long item = list[s];
-        const uint32_t m = dense_group_alleles(post, (uint32_t)item, (uint32_t)(item >> 32), g);
+        const uint32_t b = (uint32_t)item;
+        const uint32_t m = dense_group_alleles(post, b, (uint32_t)(item >> 32), g);
         if (threadIdx.x == 0)
             alleles[s] = m;
+        // g.aval is rewritten only after two barriers of the next group's numbering
+        for (uint32_t i = threadIdx.x; i < m; i += kDenseThreads)
+            aval[b + i] = g.aval[i];
     }
 }
 
@@ -2142,10 +2149,9 @@ __global__ void __launch_bounds__(kDenseThreads) k_dense_alleles(const unsigned 
 // blocks of 8 chunks (chunk c at c ^ ((c >> 3) & 7)), so that the 8 lanes of a quarter
 // warp, which read the chunks 4w + q of 8 consecutive w, hit 8 different bank groups.
 __host__ __device__ __forceinline__ uint32_t dense_gobj_words(uint32_t npad) { return (npad + 31) / 32 * 32; }
-__host__ __device__ __forceinline__ size_t dense_rows_smem(uint32_t nref, uint32_t npad)
+__host__ __device__ __forceinline__ size_t dense_rows_smem(uint32_t npad)
 {
-    return (dense_group_smem(nref) + 15) / 16 * 16 + (size_t)dense_gobj_words(npad) * 4 +
-           (size_t)dense_gobj_words(npad) / 8;
+    return (size_t)dense_gobj_words(npad) * 4 + (size_t)dense_gobj_words(npad) / 8;
 }
 __device__ __forceinline__ uint32_t dense_gobj_slot(uint32_t r)
 {
@@ -2157,39 +2163,38 @@ __device__ __forceinline__ uint32_t dense_gobj_slot(uint32_t r)
 // genomes, so the GEMM takes both operands MN-major): A'[a][q] = 1 where genome q holds
 // the allele; F[a][x * npad + r] for every genome r at the allele's context, x = 0..3:
 // 1, d >= 1, d >= 2, d = min(dna_popcount(u ^ o_r), NUM_CODENS + 1).  One CTA per group:
-// its alleles from the hash of its objects (numbered as in k_dense_alleles: the same
-// count, any order -- the GEMM sums over the alleles) and a genome -> object map; then
-// every thread of the CTA takes (allele, 16 genomes) pieces, consecutive threads on
-// consecutive genomes of one allele, and stores the piece's five 16-byte words (A' and
-// the four F rows) straight to the operands, zeros included.
+// the group's alleles come from k_dense_alleles (values at the group's first posting,
+// rows from abase[s]); the CTA maps genome -> object from the postings, then every
+// thread takes (allele, 16 genomes) pieces, consecutive threads on consecutive genomes
+// of one allele, and stores the piece's five 16-byte words (A' and the four F rows)
+// straight to the operands, zeros included.
 __global__ void __launch_bounds__(kDenseThreads) k_dense_rows(const unsigned long long *__restrict__ list,
                                                               uint32_t n_list, const uint32_t *__restrict__ abase,
-                                                              const uint64_t *__restrict__ post, uint32_t nref,
-                                                              uint32_t npad, int8_t *__restrict__ A,
-                                                              int8_t *__restrict__ F)
+                                                              const uint32_t *__restrict__ aval,
+                                                              const uint64_t *__restrict__ post, uint32_t npad,
+                                                              int8_t *__restrict__ A, int8_t *__restrict__ F)
 {
     extern __shared__ __align__(16) unsigned char dsm[];
-    const DenseGroupSmem g = dense_group_view(dsm, nref);
-    uint32_t *gobj = reinterpret_cast<uint32_t *>(dsm + (dense_group_smem(nref) + 15) / 16 * 16);
+    uint32_t *gobj = reinterpret_cast<uint32_t *>(dsm);
     uint32_t *gbit = gobj + dense_gobj_words(npad);
     const uint32_t nchunk = npad / 16, nbit = dense_gobj_words(npad) / 32;
     for (uint32_t s = blockIdx.x; s < n_list; s += gridDim.x) {
         const unsigned long long item = list[s];
-        const uint32_t k = (uint32_t)(item >> 32);
-        const uint32_t m = dense_group_alleles(post, (uint32_t)item, k, g);
+        const uint32_t b = (uint32_t)item, k = (uint32_t)(item >> 32);
+        const uint32_t a0 = abase[s], m = abase[s + 1] - a0;
         for (uint32_t i = threadIdx.x; i < nbit; i += kDenseThreads)
             gbit[i] = 0u;
         __syncthreads();
         for (uint32_t j = threadIdx.x; j < k; j += kDenseThreads) {
-            const uint32_t r = g.pgid[j];
-            gobj[dense_gobj_slot(r)] = g.pobj[j];
+            const uint64_t p = __ldg(post + b + j);
+            const uint32_t r = (uint32_t)(p >> 32);
+            gobj[dense_gobj_slot(r)] = (uint32_t)p;
             atomicOr(&gbit[r >> 5], 1u << (r & 31u));
         }
         __syncthreads();
-        const uint32_t a0 = abase[s];
         for (uint32_t t = threadIdx.x; t < m * nchunk; t += kDenseThreads) {
             const uint32_t a = t / nchunk, w = t - a * nchunk;
-            const uint32_t u = g.aval[a];
+            const uint32_t u = __ldg(aval + b + a);
             const uint32_t bits = (gbit[w >> 1] >> ((w & 1u) * 16)) & 0xFFFFu;
             uint32_t av[4], f0[4], f1[4], f2[4], f3[4];
 #pragma unroll
@@ -2220,7 +2225,7 @@ __global__ void __launch_bounds__(kDenseThreads) k_dense_rows(const unsigned lon
             fr[2 * nchunk + w] = make_uint4(f2[0], f2[1], f2[2], f2[3]);
             fr[3 * nchunk + w] = make_uint4(f3[0], f3[1], f3[2], f3[3]);
         }
-        __syncthreads();  // the group's arrays are reused by the next group
+        __syncthreads();  // the map is reused by the next group
     }
 }
 
@@ -2594,6 +2599,7 @@ struct kssdgpu_index {
     // dense self join scratch
     DevBuf<unsigned long long> d_list;
     DevBuf<uint32_t> d_poff, d_allele;
+    DevBuf<uint32_t> d_aval;                // alleles of every listed group, at its first posting
     DevBuf<int8_t> d_a, d_f;
     DevBuf<int32_t> d_d;
     DevBuf<unsigned char> d_tmp, d_ws;
@@ -3958,12 +3964,13 @@ int self_dense_impl(kssdgpu_index *ix, unsigned long long *oc, unsigned long lon
     }
     const uint32_t npad = (uint32_t)dense_npad(ix);
     const size_t group_smem = dense_group_smem((uint32_t)n);
-    const size_t rows_smem = dense_rows_smem((uint32_t)n, npad);
+    const size_t rows_smem = dense_rows_smem(npad);
     CUDA_TRY(cudaFuncSetAttribute(k_dense_alleles, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)group_smem));
     CUDA_TRY(cudaFuncSetAttribute(k_dense_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rows_smem));
     CUDA_TRY(ix->d_list.ensure(S));
     CUDA_TRY(ix->d_poff.ensure((size_t)S + 1));   // alleles per group, then the fill counter
     CUDA_TRY(ix->d_allele.ensure((size_t)S + 1)); // first allele row of every group
+    CUDA_TRY(ix->d_aval.ensure(std::max<uint64_t>(ix->n, 1)));
     unsigned int *d_count = reinterpret_cast<unsigned int *>(ix->d_poff.p + S);
     size_t tb = 0;
     CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, tb, ix->d_poff.p, ix->d_allele.p, (int)S + 1, st));
@@ -3977,7 +3984,8 @@ int self_dense_impl(kssdgpu_index *ix, unsigned long long *oc, unsigned long lon
     CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_al, k_dense_alleles, kDenseThreads, group_smem));
     CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_rows, k_dense_rows, kDenseThreads, rows_smem));
     const int grid_al = ix->sms * std::max(1, per_sm_al), grid = ix->sms * std::max(1, per_sm_rows);
-    k_dense_alleles<<<grid_al, kDenseThreads, group_smem, st>>>(ix->d_list.p, S, ix->post, (uint32_t)n, ix->d_poff.p);
+    k_dense_alleles<<<grid_al, kDenseThreads, group_smem, st>>>(ix->d_list.p, S, ix->post, (uint32_t)n, ix->d_poff.p,
+                                                                ix->d_aval.p);
     CUDA_TRY(cudaMemsetAsync(d_count, 0, sizeof(unsigned int), st));  // poff[S] = 0: the scan's last term
     tb = ix->d_tmp.cap;
     CUDA_TRY(cub::DeviceScan::ExclusiveSum(ix->d_tmp.p, tb, ix->d_poff.p, ix->d_allele.p, (int)S + 1, st));
@@ -4002,8 +4010,8 @@ int self_dense_impl(kssdgpu_index *ix, unsigned long long *oc, unsigned long lon
         CUDA_TRY(cudaMemsetAsync(ix->d_a.p + (size_t)alleles * npad, 0, (size_t)(kpad - alleles) * npad, st));
         CUDA_TRY(cudaMemsetAsync(ix->d_f.p + (size_t)alleles * 4 * npad, 0, (size_t)(kpad - alleles) * 4 * npad, st));
     }
-    k_dense_rows<<<grid, kDenseThreads, rows_smem, st>>>(ix->d_list.p, S, ix->d_allele.p, ix->post, (uint32_t)n, npad,
-                                                         ix->d_a.p, ix->d_f.p);
+    k_dense_rows<<<grid, kDenseThreads, rows_smem, st>>>(ix->d_list.p, S, ix->d_allele.p, ix->d_aval.p, ix->post,
+                                                         npad, ix->d_a.p, ix->d_f.p);
     count_launch();
     CUDA_TRY(cudaGetLastError());
     // 3. D = A' F^T on the tensor cores (both operands MN-major)
