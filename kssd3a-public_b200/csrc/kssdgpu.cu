@@ -2201,21 +2201,21 @@ __global__ void __launch_bounds__(kDenseThreads) k_dense_rows(const unsigned lon
             for (int q = 0; q < 4; ++q) {
                 const uint32_t c = 4 * w + q;
                 const uint4 o4 = *reinterpret_cast<const uint4 *>(gobj + ((c ^ ((c >> 3) & 7u)) << 2));
-                const uint32_t ov[4] = {o4.x, o4.y, o4.z, o4.w};
-                av[q] = f0[q] = f1[q] = f2[q] = f3[q] = 0u;
-#pragma unroll
-                for (int e = 0; e < 4; ++e) {
-                    if ((bits >> (4 * q + e)) & 1u) {
-                        const uint32_t o = ov[e];
-                        const uint32_t d = (uint32_t)min(kMinInit, dna_pop(u ^ o));
-                        const int sh = 8 * e;
-                        av[q] |= (uint32_t)(o == u) << sh;
-                        f0[q] |= 1u << sh;
-                        f1[q] |= (uint32_t)(d >= 1) << sh;
-                        f2[q] |= (uint32_t)(d >= 2) << sh;
-                        f3[q] |= d << sh;
-                    }
-                }
+                // four genomes a word, one byte each: d (0..NUM_CODENS + 1, so < 128) of the
+                // present genomes, then the thresholds by bytewise adds into bit 7 (no carry
+                // leaves a byte); d = 0 exactly when the object is the allele's
+                const uint32_t pm = (((bits >> (4 * q)) & 0xFu) * 0x204081u) & 0x01010101u;  // bit i -> byte i
+                const uint32_t d0 = (uint32_t)min(kMinInit, dna_pop(u ^ o4.x));
+                const uint32_t d1 = (uint32_t)min(kMinInit, dna_pop(u ^ o4.y));
+                const uint32_t d2 = (uint32_t)min(kMinInit, dna_pop(u ^ o4.z));
+                const uint32_t d3 = (uint32_t)min(kMinInit, dna_pop(u ^ o4.w));
+                const uint32_t D = __byte_perm(__byte_perm(d0, d1, 0x0040u), __byte_perm(d2, d3, 0x0040u), 0x5410u) &
+                                   (pm * 0xFFu);
+                f0[q] = pm;
+                f1[q] = ((D + 0x7F7F7F7Fu) >> 7) & 0x01010101u;
+                f2[q] = ((D + 0x7E7E7E7Eu) >> 7) & 0x01010101u;
+                f3[q] = D;
+                av[q] = pm ^ f1[q];
             }
             const size_t row = (size_t)(a0 + a);
             reinterpret_cast<uint4 *>(A + row * npad)[w] = make_uint4(av[0], av[1], av[2], av[3]);
