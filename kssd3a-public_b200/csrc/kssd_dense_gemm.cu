@@ -49,16 +49,24 @@ using Kernel =
     cutlass::gemm::kernel::GemmUniversal<Shape<int, int, int, int>, Mainloop, Epilogue, cutlass::gemm::StreamKScheduler>;
 using Gemm = cutlass::gemm::device::GemmUniversalAdapter<Kernel>;
 
-typename Gemm::Arguments make_args(const int8_t *A, const int8_t *B, int32_t *D, int M, int N, int K)
+// lda / ldb: elements between consecutive k rows of A (K x M) and B (K x N); ldd:
+// elements between consecutive rows of D, so that a block of a larger matrix can be
+// one GEMM.
+typename Gemm::Arguments make_args(const int8_t *A, const int8_t *B, int32_t *D, int M, int N, int K, int64_t lda,
+                                   int64_t ldb, int64_t ldd)
 {
     using SA = typename Gemm::GemmKernel::StrideA;
     using SB = typename Gemm::GemmKernel::StrideB;
     using SC = typename Gemm::GemmKernel::StrideC;
     using SD = typename Gemm::GemmKernel::StrideD;
-    const SA sa = cutlass::make_cute_packed_stride(SA{}, cute::make_shape(M, K, 1));
-    const SB sb = cutlass::make_cute_packed_stride(SB{}, cute::make_shape(N, K, 1));
-    const SC sc = cutlass::make_cute_packed_stride(SC{}, cute::make_shape(M, N, 1));
-    const SD sd = cutlass::make_cute_packed_stride(SD{}, cute::make_shape(M, N, 1));
+    SA sa = cutlass::make_cute_packed_stride(SA{}, cute::make_shape(M, K, 1));
+    SB sb = cutlass::make_cute_packed_stride(SB{}, cute::make_shape(N, K, 1));
+    SC sc = cutlass::make_cute_packed_stride(SC{}, cute::make_shape(M, N, 1));
+    SD sd = cutlass::make_cute_packed_stride(SD{}, cute::make_shape(M, N, 1));
+    cute::get<1>(sa) = lda;  // A: (m, k) at m + k lda
+    cute::get<1>(sb) = ldb;  // B: (n, k) at n + k ldb
+    cute::get<0>(sc) = ldd;  // C (not read: beta = 0) and D: (m, n) at m ldd + n
+    cute::get<0>(sd) = ldd;
     typename Gemm::Arguments args{cutlass::gemm::GemmUniversalMode::kGemm, {M, N, K, 1}, {A, sa, B, sb},
                                   {{1, 0}, D, sc, D, sd}};
 #if KSSD_GEMM_SCHED
@@ -90,16 +98,17 @@ namespace kssd {
 // Bytes of device workspace the GEMM of this shape needs (0 or more).
 size_t dense_gemm_s8_workspace(int M, int N, int K)
 {
-    return Gemm::get_workspace_size(make_args(nullptr, nullptr, nullptr, M, N, K));
+    return Gemm::get_workspace_size(make_args(nullptr, nullptr, nullptr, M, N, K, M, N, N));
 }
 
-// D = A^T B for A stored K x M and B stored K x N; M and N multiples of 16 (16-byte
-// aligned rows).  Returns 0, or 1 when the shape is not supported, 2 when the launch
+// D = A^T B for A stored K x M (row stride lda) and B stored K x N (row stride ldb), D
+// row-major with row stride ldd; M, N, lda, ldb multiples of 16 and every base address
+// 16-byte aligned.  Returns 0, or 1 when the shape is not supported, 2 when the launch
 // failed.
-int dense_gemm_s8(const int8_t *A, const int8_t *B, int32_t *D, int M, int N, int K, void *workspace,
-                  cudaStream_t st)
+int dense_gemm_s8(const int8_t *A, const int8_t *B, int32_t *D, int M, int N, int K, int64_t lda, int64_t ldb,
+                  int64_t ldd, void *workspace, cudaStream_t st)
 {
-    const auto args = make_args(A, B, D, M, N, K);
+    const auto args = make_args(A, B, D, M, N, K, lda, ldb, ldd);
     Gemm gemm;
     if (gemm.can_implement(args) != cutlass::Status::kSuccess)
         return 1;

@@ -30,7 +30,8 @@ using namespace kssd;
 
 namespace kssd {
 size_t dense_gemm_s8_workspace(int M, int N, int K);
-int dense_gemm_s8(const int8_t *A, const int8_t *B, int32_t *D, int M, int N, int K, void *workspace, cudaStream_t st);
+int dense_gemm_s8(const int8_t *A, const int8_t *B, int32_t *D, int M, int N, int K, int64_t lda, int64_t ldb,
+                  int64_t ldd, void *workspace, cudaStream_t st);
 }  // namespace kssd
 
 namespace {
@@ -2021,6 +2022,9 @@ __global__ void k_dense_list(const uint32_t *__restrict__ gbeg, uint64_t u, unsi
 // Largest shared group the dense join handles (its postings are held in shared
 // memory), which also bounds the references: the dense join needs nref <= this.
 constexpr uint32_t kDenseMaxGroup = 4096;
+// From this many 128-genome blocks on, the dense join's GEMM runs per block below the
+// diagonal instead of over the whole square.
+constexpr uint64_t kDenseBlocks = 6;
 constexpr int kDenseThreads = 256;
 
 // Shared memory of the dense kernels for groups of at most n postings (n = the index's
@@ -2161,13 +2165,14 @@ __device__ __forceinline__ uint32_t dense_gobj_slot(uint32_t r)
 
 // The operand rows of every allele, written whole (allele-major: a row runs over the
 // genomes, so the GEMM takes both operands MN-major): A'[a][q] = 1 where genome q holds
-// the allele; F[a][x * npad + r] for every genome r at the allele's context, x = 0..3:
-// 1, d >= 1, d >= 2, d = min(dna_popcount(u ^ o_r), NUM_CODENS + 1).  One CTA per group:
+// the allele; F[a][4 r + x] for every genome r at the allele's context, x = 0..3:
+// 1, d >= 1, d >= 2, d = min(dna_popcount(u ^ o_r), NUM_CODENS + 1) (genome-major, so
+// that the columns of a block of genomes are one contiguous range).  One CTA per group:
 // the group's alleles come from k_dense_alleles (values at the group's first posting,
 // rows from abase[s]); the CTA maps genome -> object from the postings, then every
 // thread takes (allele, 16 genomes) pieces, consecutive threads on consecutive genomes
-// of one allele, and stores the piece's five 16-byte words (A' and the four F rows)
-// straight to the operands, zeros included.
+// of one allele, and stores the piece's 16-byte words (one of A', four of F) straight to
+// the operands, zeros included.
 __global__ void __launch_bounds__(kDenseThreads) k_dense_rows(const unsigned long long *__restrict__ list,
                                                               uint32_t n_list, const uint32_t *__restrict__ abase,
                                                               const uint32_t *__restrict__ aval,
@@ -2219,17 +2224,22 @@ __global__ void __launch_bounds__(kDenseThreads) k_dense_rows(const unsigned lon
             }
             const size_t row = (size_t)(a0 + a);
             reinterpret_cast<uint4 *>(A + row * npad)[w] = make_uint4(av[0], av[1], av[2], av[3]);
-            uint4 *fr = reinterpret_cast<uint4 *>(F + row * 4 * npad);
-            fr[w] = make_uint4(f0[0], f0[1], f0[2], f0[3]);
-            fr[nchunk + w] = make_uint4(f1[0], f1[1], f1[2], f1[3]);
-            fr[2 * nchunk + w] = make_uint4(f2[0], f2[1], f2[2], f2[3]);
-            fr[3 * nchunk + w] = make_uint4(f3[0], f3[1], f3[2], f3[3]);
+            uint4 *fr = reinterpret_cast<uint4 *>(F + row * 4 * npad) + 4 * w;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                // 4 x 4 byte transpose: word e = genome 4q + e's bytes x = 0..3
+                const uint32_t lo01 = __byte_perm(f0[q], f1[q], 0x5140u), hi01 = __byte_perm(f0[q], f1[q], 0x7362u);
+                const uint32_t lo23 = __byte_perm(f2[q], f3[q], 0x5140u), hi23 = __byte_perm(f2[q], f3[q], 0x7362u);
+                fr[q] = make_uint4(__byte_perm(lo01, lo23, 0x5410u), __byte_perm(lo01, lo23, 0x7632u),
+                                   __byte_perm(hi01, hi23, 0x5410u), __byte_perm(hi01, hi23, 0x7632u));
+            }
         }
         __syncthreads();  // the map is reused by the next group
     }
 }
 
-// Packed lower triangle from D (npad x 4 npad): every cell written (zeros included).
+// Packed lower triangle from D (npad x 4 npad, D[q][4 r + x]; with the blocked GEMM only
+// the blocks at or below the diagonal are computed): every cell written (zeros included).
 __global__ void k_dense_epilogue(const int32_t *__restrict__ D, uint32_t npad, size_t cells,
                                  unsigned long long *__restrict__ oc, unsigned long long *__restrict__ oo)
 {
@@ -2241,9 +2251,9 @@ __global__ void k_dense_epilogue(const int32_t *__restrict__ D, uint32_t npad, s
         while ((size_t)(q + 1) * q / 2 <= c)
             ++q;
         const uint32_t r = (uint32_t)(c - (size_t)q * (q - 1) / 2);
-        const int32_t *d = D + (size_t)q * 4 * npad;
-        oc[c] = (unsigned long long)(uint32_t)d[r] | ((unsigned long long)(uint32_t)d[2 * npad + r] << 32);
-        oo[c] = (unsigned long long)(uint32_t)d[npad + r] | ((unsigned long long)(uint32_t)d[3 * npad + r] << 32);
+        const int4 v = *reinterpret_cast<const int4 *>(D + (size_t)q * 4 * npad + 4 * (size_t)r);
+        oc[c] = (unsigned long long)(uint32_t)v.x | ((unsigned long long)(uint32_t)v.z << 32);
+        oo[c] = (unsigned long long)(uint32_t)v.y | ((unsigned long long)(uint32_t)v.w << 32);
     }
 }
 
@@ -4014,16 +4024,32 @@ int self_dense_impl(kssdgpu_index *ix, unsigned long long *oc, unsigned long lon
                                                          npad, ix->d_a.p, ix->d_f.p);
     count_launch();
     CUDA_TRY(cudaGetLastError());
-    // 3. D = A' F^T on the tensor cores (both operands MN-major)
-    const size_t ws = kssd::dense_gemm_s8_workspace((int)npad, (int)(4 * npad), (int)kpad);
+    // 3. D = A' F^T on the tensor cores (both operands MN-major).  The four counters are
+    // symmetric in (q, r) and only cells q > r are kept, so for every block of 128
+    // genomes r (512 columns of F) one GEMM covers the rows q >= the block's first:
+    // (B + 1) / 2B of the square's work for B blocks, F read once.  Below kDenseBlocks
+    // blocks one GEMM over the square is faster (one launch, fewer split-K partials:
+    // 512 genomes 0.78 vs 0.86 ms per join; 1,024 genomes 2.53 vs 2.34 ms, 2,048 genomes
+    // 11.3 vs 7.8 ms the other way).
+    const uint64_t nblk = (npad + 127) / 128;
+    const uint64_t bw = nblk >= kDenseBlocks ? 128 : npad;  // genomes r per GEMM
+    const uint64_t ngemm = (npad + bw - 1) / bw;
+    size_t ws = 0;
+    for (uint64_t j = 0; j < ngemm; ++j)
+        ws = std::max(ws, kssd::dense_gemm_s8_workspace((int)(npad - bw * j),
+                                                        (int)(4 * std::min<uint64_t>(bw, npad - bw * j)), (int)kpad));
     CUDA_TRY(ix->d_ws.ensure(ws));
-    const int grc = kssd::dense_gemm_s8(ix->d_a.p, ix->d_f.p, ix->d_d.p, (int)npad, (int)(4 * npad), (int)kpad,
-                                        ix->d_ws.p, st);
-    count_launch();
-    if (grc)
-        return fail(KSSDGPU_ERR_CUDA, grc == 1 ? "dense self join: GEMM shape not supported"
-                                               : "dense self join: GEMM launch failed");
-    CUDA_TRY(cudaGetLastError());
+    for (uint64_t j = 0; j < ngemm; ++j) {
+        const uint64_t m = npad - bw * j, nc = 4 * std::min<uint64_t>(bw, npad - bw * j);
+        const int grc = kssd::dense_gemm_s8(ix->d_a.p + bw * j, ix->d_f.p + 4 * bw * j,
+                                            ix->d_d.p + bw * j * 4 * npad + 4 * bw * j, (int)m, (int)nc, (int)kpad,
+                                            (int64_t)npad, (int64_t)(4 * npad), (int64_t)(4 * npad), ix->d_ws.p, st);
+        count_launch();
+        if (grc)
+            return fail(KSSDGPU_ERR_CUDA, grc == 1 ? "dense self join: GEMM shape not supported"
+                                                   : "dense self join: GEMM launch failed");
+        CUDA_TRY(cudaGetLastError());
+    }
     // 4. the packed lower triangle
     k_dense_epilogue<<<grid_for(cells), 256, 0, st>>>(ix->d_d.p, npad, cells, oc, oo);
     count_launch();

@@ -597,10 +597,12 @@ def _wide_cluster(n=160, seed=61, sub_hi=0.01):
                          size_dist=kssdgpu.SIZE_LOGNORMAL, sub_lo=0.001, sub_hi=sub_hi, seed=seed, sample_seed=seed)
 
 
-@pytest.mark.parametrize("n,seed,sub_hi", [(160, 61, 0.01), (300, 62, 0.03), (129, 63, 0.2), (2, 64, 0.01)])
+@pytest.mark.parametrize("n,seed,sub_hi", [(160, 61, 0.01), (300, 62, 0.03), (129, 63, 0.2), (2, 64, 0.01),
+                                            (700, 65, 0.01)])
 def test_self_dense_join_matches_oracle(n, seed, sub_hi):
-    """The dense tensor-core self join (alleles of the shared contexts, one int8 GEMM)
-    gives the oracle's counters; on a dense index the default path chooses it."""
+    """The dense tensor-core self join (alleles of the shared contexts, int8 GEMMs) gives
+    the oracle's counters; on a dense index the default path chooses it.  700 genomes
+    (6 blocks of 128, the last of 64) take the GEMM per block below the diagonal."""
     sk = _wide_cluster(n, seed, sub_hi)
     rec = oracle.build_index(sk.keys, sk.offs)
     idx = kssdgpu.Index.from_records(rec, sk.n)
