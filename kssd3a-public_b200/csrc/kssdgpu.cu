@@ -2149,9 +2149,9 @@ __global__ void __launch_bounds__(kDenseThreads) k_dense_alleles(const unsigned 
 }
 
 // Genome -> object map of one group for k_dense_rows: the object of genome r as a u32
-// word and a presence bit.  The words sit in 16-byte chunks (4 genomes) swizzled inside
-// blocks of 8 chunks (chunk c at c ^ ((c >> 3) & 7)), so that the 8 lanes of a quarter
-// warp, which read the chunks 4w + q of 8 consecutive w, hit 8 different bank groups.
+// word and a presence bit.  The words sit in 16-byte chunks (4 genomes), permuted inside
+// blocks of 8 chunks (chunk c at c ^ ((c >> 3) & 7)); the 8 lanes of a quarter warp read
+// 8 consecutive chunks, which stay on 8 different bank groups.
 __host__ __device__ __forceinline__ uint32_t dense_gobj_words(uint32_t npad) { return (npad + 31) / 32 * 32; }
 __host__ __device__ __forceinline__ size_t dense_rows_smem(uint32_t npad)
 {
@@ -2170,9 +2170,9 @@ __device__ __forceinline__ uint32_t dense_gobj_slot(uint32_t r)
 // that the columns of a block of genomes are one contiguous range).  One CTA per group:
 // the group's alleles come from k_dense_alleles (values at the group's first posting,
 // rows from abase[s]); the CTA maps genome -> object from the postings, then every
-// thread takes (allele, 16 genomes) pieces, consecutive threads on consecutive genomes
-// of one allele, and stores the piece's 16-byte words (one of A', four of F) straight to
-// the operands, zeros included.
+// thread takes (allele, 4 genomes) pieces, consecutive threads on consecutive genomes
+// of one allele, and stores the piece's 4 bytes of A' and 16 bytes of F straight to the
+// operands (a warp's stores of one allele are contiguous), zeros included.
 __global__ void __launch_bounds__(kDenseThreads) k_dense_rows(const unsigned long long *__restrict__ list,
                                                               uint32_t n_list, const uint32_t *__restrict__ abase,
                                                               const uint32_t *__restrict__ aval,
@@ -2182,7 +2182,7 @@ __global__ void __launch_bounds__(kDenseThreads) k_dense_rows(const unsigned lon
     extern __shared__ __align__(16) unsigned char dsm[];
     uint32_t *gobj = reinterpret_cast<uint32_t *>(dsm);
     uint32_t *gbit = gobj + dense_gobj_words(npad);
-    const uint32_t nchunk = npad / 16, nbit = dense_gobj_words(npad) / 32;
+    const uint32_t nquad = npad / 4, nbit = dense_gobj_words(npad) / 32;
     for (uint32_t s = blockIdx.x; s < n_list; s += gridDim.x) {
         const unsigned long long item = list[s];
         const uint32_t b = (uint32_t)item, k = (uint32_t)(item >> 32);
@@ -2197,42 +2197,30 @@ __global__ void __launch_bounds__(kDenseThreads) k_dense_rows(const unsigned lon
             atomicOr(&gbit[r >> 5], 1u << (r & 31u));
         }
         __syncthreads();
-        for (uint32_t t = threadIdx.x; t < m * nchunk; t += kDenseThreads) {
-            const uint32_t a = t / nchunk, w = t - a * nchunk;
+        for (uint32_t t = threadIdx.x; t < m * nquad; t += kDenseThreads) {
+            const uint32_t a = t / nquad, c = t - a * nquad;  // allele, genomes 4c..4c+3
             const uint32_t u = __ldg(aval + b + a);
-            const uint32_t bits = (gbit[w >> 1] >> ((w & 1u) * 16)) & 0xFFFFu;
-            uint32_t av[4], f0[4], f1[4], f2[4], f3[4];
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const uint32_t c = 4 * w + q;
-                const uint4 o4 = *reinterpret_cast<const uint4 *>(gobj + ((c ^ ((c >> 3) & 7u)) << 2));
-                // four genomes a word, one byte each: d (0..NUM_CODENS + 1, so < 128) of the
-                // present genomes, then the thresholds by bytewise adds into bit 7 (no carry
-                // leaves a byte); d = 0 exactly when the object is the allele's
-                const uint32_t pm = (((bits >> (4 * q)) & 0xFu) * 0x204081u) & 0x01010101u;  // bit i -> byte i
-                const uint32_t d0 = (uint32_t)min(kMinInit, dna_pop(u ^ o4.x));
-                const uint32_t d1 = (uint32_t)min(kMinInit, dna_pop(u ^ o4.y));
-                const uint32_t d2 = (uint32_t)min(kMinInit, dna_pop(u ^ o4.z));
-                const uint32_t d3 = (uint32_t)min(kMinInit, dna_pop(u ^ o4.w));
-                const uint32_t D = __byte_perm(__byte_perm(d0, d1, 0x0040u), __byte_perm(d2, d3, 0x0040u), 0x5410u) &
-                                   (pm * 0xFFu);
-                f0[q] = pm;
-                f1[q] = ((D + 0x7F7F7F7Fu) >> 7) & 0x01010101u;
-                f2[q] = ((D + 0x7E7E7E7Eu) >> 7) & 0x01010101u;
-                f3[q] = D;
-                av[q] = pm ^ f1[q];
-            }
+            const uint4 o4 = *reinterpret_cast<const uint4 *>(gobj + ((c ^ ((c >> 3) & 7u)) << 2));
+            // one byte a genome: d (0..NUM_CODENS + 1, so < 128) of the present genomes,
+            // then the thresholds by bytewise adds into bit 7 (no carry leaves a byte);
+            // d = 0 exactly when the object is the allele's
+            const uint32_t pm = (((gbit[c >> 3] >> ((c & 7u) * 4)) & 0xFu) * 0x204081u) & 0x01010101u;  // bit i -> byte i
+            const uint32_t d0 = (uint32_t)min(kMinInit, dna_pop(u ^ o4.x));
+            const uint32_t d1 = (uint32_t)min(kMinInit, dna_pop(u ^ o4.y));
+            const uint32_t d2 = (uint32_t)min(kMinInit, dna_pop(u ^ o4.z));
+            const uint32_t d3 = (uint32_t)min(kMinInit, dna_pop(u ^ o4.w));
+            const uint32_t D = __byte_perm(__byte_perm(d0, d1, 0x0040u), __byte_perm(d2, d3, 0x0040u), 0x5410u) &
+                               (pm * 0xFFu);
+            const uint32_t f1 = ((D + 0x7F7F7F7Fu) >> 7) & 0x01010101u;
+            const uint32_t f2 = ((D + 0x7E7E7E7Eu) >> 7) & 0x01010101u;
             const size_t row = (size_t)(a0 + a);
-            reinterpret_cast<uint4 *>(A + row * npad)[w] = make_uint4(av[0], av[1], av[2], av[3]);
-            uint4 *fr = reinterpret_cast<uint4 *>(F + row * 4 * npad) + 4 * w;
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                // 4 x 4 byte transpose: word e = genome 4q + e's bytes x = 0..3
-                const uint32_t lo01 = __byte_perm(f0[q], f1[q], 0x5140u), hi01 = __byte_perm(f0[q], f1[q], 0x7362u);
-                const uint32_t lo23 = __byte_perm(f2[q], f3[q], 0x5140u), hi23 = __byte_perm(f2[q], f3[q], 0x7362u);
-                fr[q] = make_uint4(__byte_perm(lo01, lo23, 0x5410u), __byte_perm(lo01, lo23, 0x7632u),
-                                   __byte_perm(hi01, hi23, 0x5410u), __byte_perm(hi01, hi23, 0x7632u));
-            }
+            reinterpret_cast<uint32_t *>(A + row * npad)[c] = pm ^ f1;
+            // 4 x 4 byte transpose of (present, d >= 1, d >= 2, d): word e = genome 4c + e
+            const uint32_t lo01 = __byte_perm(pm, f1, 0x5140u), hi01 = __byte_perm(pm, f1, 0x7362u);
+            const uint32_t lo23 = __byte_perm(f2, D, 0x5140u), hi23 = __byte_perm(f2, D, 0x7362u);
+            reinterpret_cast<uint4 *>(F + row * 4 * npad)[c] =
+                make_uint4(__byte_perm(lo01, lo23, 0x5410u), __byte_perm(lo01, lo23, 0x7632u),
+                           __byte_perm(hi01, hi23, 0x5410u), __byte_perm(hi01, hi23, 0x7632u));
         }
         __syncthreads();  // the map is reused by the next group
     }
