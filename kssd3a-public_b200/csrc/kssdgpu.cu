@@ -3937,7 +3937,8 @@ uint64_t round_up(uint64_t x, uint64_t m) { return (x + m - 1) / m * m; }
 
 // Dense self join (see k_dense_list): list the shared groups, count their alleles
 // (distinct objects, from a hash of each group's objects in shared memory), build
-// every allele's operand rows, one tensor-core GEMM, and the packed lower triangle
+// every allele's operand rows, the tensor-core GEMM (per block of genomes below the
+// diagonal from kDenseBlocks blocks on), and the packed lower triangle
 // (every cell written, so no zero fill).  Conflict-free indexes of at most
 // kDenseMaxGroup references only; the operands must fit in half of the free memory.
 int self_dense_impl(kssdgpu_index *ix, unsigned long long *oc, unsigned long long *oo, cudaStream_t st)
@@ -4045,7 +4046,7 @@ int self_dense_impl(kssdgpu_index *ix, unsigned long long *oc, unsigned long lon
     return KSSDGPU_OK;
 }
 
-// The density rule of the self join: the dense path does 4 n^2 K multiply-adds (K
+// The density rule of the self join: the dense path does at most 4 n^2 K multiply-adds (K
 // alleles of the shared contexts), the scan one counter update per pair of postings of
 // a shared context.  density = pairs / (n^2 K); the dense join is taken when it is
 // above kDenseRatio, on a conflict-free index whose operands fit in half of the free
