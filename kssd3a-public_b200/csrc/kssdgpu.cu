@@ -2027,14 +2027,12 @@ constexpr uint32_t kDenseMaxGroup = 4096;
 constexpr uint64_t kDenseBlocks = 6;
 constexpr int kDenseThreads = 256;
 
-// Shared memory of the dense kernels for groups of at most n postings (n = the index's
-// references): a hash of the group's objects (hcap = pow2 >= 2n slots: the object with a
-// valid bit, the slot's allele number), and per posting its object, gid and allele.
+// Shared memory of the allele numbering for groups of at most n postings (n = the
+// index's references): a hash of the group's objects (hcap = pow2 >= 2n slots: the
+// object with a valid bit) and the allele values by number.
 struct DenseGroupSmem {
     unsigned long long *hkey;  // hcap
-    unsigned short *hid;       // hcap
-    uint32_t *pobj, *aval;     // n: posting objects; allele values by number
-    unsigned short *pgid, *pall;  // n
+    uint32_t *aval;            // n: allele values by number
 };
 __host__ __device__ __forceinline__ uint32_t dense_hcap(uint32_t n)
 {
@@ -2045,29 +2043,22 @@ __host__ __device__ __forceinline__ uint32_t dense_hcap(uint32_t n)
 }
 __host__ __device__ __forceinline__ size_t dense_group_smem(uint32_t n)
 {
-    const uint32_t hcap = dense_hcap(n);
-    return (size_t)hcap * 10 + (size_t)n * 12 + 64;
+    return (size_t)dense_hcap(n) * 8 + (size_t)n * 4 + 64;
 }
 __device__ __forceinline__ DenseGroupSmem dense_group_view(unsigned char *base, uint32_t n)
 {
-    const uint32_t hcap = dense_hcap(n);
     DenseGroupSmem g;
     g.hkey = reinterpret_cast<unsigned long long *>(base);
-    g.pobj = reinterpret_cast<uint32_t *>(g.hkey + hcap);
-    g.aval = g.pobj + n;
-    g.hid = reinterpret_cast<unsigned short *>(g.aval + n);
-    g.pgid = g.hid + hcap;
-    g.pall = g.pgid + n;
+    g.aval = reinterpret_cast<uint32_t *>(g.hkey + dense_hcap(n));
     return g;
 }
 
 // The alleles of a group [b, b + k) (k <= n postings, one object per gid): its distinct
-// objects, numbered 0..m-1 by hash slot order; afterwards pobj / pgid / pall hold every
-// posting's object, gid and allele and aval[a] the object of allele a.  A few barriers
-// instead of a sort: every posting's object is inserted into the hash (CAS on an empty
-// slot, linear probing; 2k slots for at most k objects), each thread numbers the
-// occupied slots of its contiguous segment after one block scan of their counts.
-// Returns m (on every thread); ends with a barrier.
+// objects, numbered 0..m-1 by hash slot order; afterwards aval[a] holds the object of
+// allele a.  A few barriers instead of a sort: every posting's object is inserted into
+// the hash (CAS on an empty slot, linear probing; 2k slots for at most k objects), each
+// thread numbers the occupied slots of its contiguous segment after one block scan of
+// their counts.  Returns m (on every thread); ends with a barrier.
 __device__ uint32_t dense_group_alleles(const uint64_t *__restrict__ post, uint32_t b, uint32_t k,
                                         const DenseGroupSmem &g)
 {
@@ -2081,10 +2072,7 @@ __device__ uint32_t dense_group_alleles(const uint64_t *__restrict__ post, uint3
         g.hkey[i] = 0;
     __syncthreads();
     for (uint32_t j = threadIdx.x; j < k; j += kDenseThreads) {
-        const uint64_t p = __ldg(post + b + j);
-        const uint32_t o = (uint32_t)p;
-        g.pobj[j] = o;
-        g.pgid[j] = (unsigned short)(p >> 32);
+        const uint32_t o = (uint32_t)__ldg(post + b + j);
         const unsigned long long key = (1ull << 32) | o;
         uint32_t h = (o * 2654435761u) >> (32 - lg);
         for (uint32_t probe = 0; probe < hcap; ++probe) {
@@ -2093,7 +2081,6 @@ __device__ uint32_t dense_group_alleles(const uint64_t *__restrict__ post, uint3
                 break;
             h = (h + 1) & mask;
         }
-        g.pall[j] = (unsigned short)h;  // the slot for now
     }
     __syncthreads();
     const uint32_t seg = hcap / kDenseThreads, s0 = threadIdx.x * seg;  // hcap >= 64, a multiple of 256 or less
@@ -2105,23 +2092,15 @@ __device__ uint32_t dense_group_alleles(const uint64_t *__restrict__ post, uint3
     uint32_t first, m;
     Scan(scan_tmp).ExclusiveSum(mine, first, m);
     if (hcap < kDenseThreads) {
-        if (threadIdx.x < hcap && g.hkey[threadIdx.x]) {
-            g.hid[threadIdx.x] = (unsigned short)first;
+        if (threadIdx.x < hcap && g.hkey[threadIdx.x])
             g.aval[first] = (uint32_t)g.hkey[threadIdx.x];
-        }
     } else {
         for (uint32_t i = 0; i < seg; ++i) {
             const unsigned long long key = g.hkey[s0 + i];
-            if (key) {
-                g.hid[s0 + i] = (unsigned short)first;
-                g.aval[first] = (uint32_t)key;
-                ++first;
-            }
+            if (key)
+                g.aval[first++] = (uint32_t)key;
         }
     }
-    __syncthreads();
-    for (uint32_t j = threadIdx.x; j < k; j += kDenseThreads)
-        g.pall[j] = g.hid[g.pall[j]];
     __syncthreads();
     return m;
 }
